@@ -1,0 +1,325 @@
+"""Benchmark: RCS solves/s at N=2048 (mixed vs FP64 GPU), the 2-D airfoil workload.
+
+Workload (one "step"): the seeded NACA 00tt airfoil (chord 1 m, tt ~ U[8,15] %, cosine
+spacing, sharp trailing edge) with N = 2048 panels at lambda/10 (~30 GHz), 720
+monostatic angles (0..359.5 deg by 0.5), both polarisations (TM = HH EFIE, TE = VV
+MFIE): two solves per step, each = fill + LU + 720-RHS solve + refinement + far field.
+The headline arm is the mixed-precision path (complex64 fill/LU, FP64 refinement);
+the plain FP64 GPU path is timed on the same inputs for the ratio and the dB error.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl grim|reference]
+
+Multi-GPU (torchrun): every rank solves its own seeded airfoil (independent units, no
+data-path collective: weak scaling); the time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = 'RCS solves/s at N=2048 (mixed vs FP64 GPU, <=0.05 dB); p50/p99 serve latency'
+UNIT = 'solves/s'
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, 'MEASURED_PEAKS.json')) as f:
+            p = json.load(f)
+        return float(p['hbm_gbs']), float(p['bf16_tflops']), 'measured'
+    except Exception:
+        return 6650.0, 1590.0, 'fallback'
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    FIELDS = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
+              'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
+              'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix='.csv')
+            os.close(fd)
+            self.proc = subprocess.Popen(['nvidia-smi', f'--id={self.index}', f'--query-gpu={self.FIELDS}',
+                                          '--format=csv,noheader,nounits', '-lms', '200'],
+                                         stdout=open(self.path, 'w'), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        out = {'sm_mhz': None, 'sm_max_mhz': None, 'reasons': [], 'samples': 0}
+        if not self.path or not os.path.exists(self.path):
+            return out
+        sm, mx, reasons = [], [], set()
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(',')]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower() == 'active':
+                    reasons.add(nm)
+        os.unlink(self.path)
+        if sm:
+            out.update(sm_mhz=statistics.median(sm), sm_max_mhz=max(mx), reasons=sorted(reasons), samples=len(sm))
+        return out
+
+
+def workload(seed, n, nang):
+    from grim_20261007_b200 import synthetic as S
+    v, k, f, t = S.airfoil_case(seed, n)
+    ang = np.arange(nang) * (360.0 / nang)
+    return v, k, f, t, ang
+
+
+def cpu_oracle_solve(v, k, ang, pol):
+    from oracle import pulse2d as P
+    return P.solve(k, [v], ang, pol)['amplitude']
+
+
+def run_reference_arm(args, rank, world):
+    """Reference CPU implementation of the path (the oracle port), all host threads."""
+    if rank != 0:
+        return
+    import concurrent.futures as cf
+    import multiprocessing as mp
+    from oracle import pulse2d as P
+    import scipy.linalg as sla
+    cores = os.cpu_count() or 1
+    v, k, f, t, ang = workload(args.seed, args.n, args.angles)
+    c, tt, h, nn = P.panel_arrays([v])
+    ted = P.te_curvature_correction([v])
+    rows = np.array_split(np.arange(len(c)), cores)
+    ctx = mp.get_context('spawn')
+
+    def one_step(pool):
+        for pol in ('TM', 'TE'):
+            futs = [pool.submit(P.fill, k, c, tt, h, nn, pol, r, ted if pol == 'TE' else None) for r in rows]
+            z = np.concatenate([fu.result() for fu in futs], axis=0)
+            b = P.rhs(k, c, nn, ang, pol)
+            x = sla.lu_solve(sla.lu_factor(z, check_finite=False), b, check_finite=False)
+            P.monostatic_amplitude(P.farfield_weights(k, c, tt, h, ang), x)
+
+    with cf.ProcessPoolExecutor(max_workers=cores, mp_context=ctx) as pool:
+        for _ in range(args.warmup):
+            one_step(pool)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            one_step(pool)
+        dt = time.perf_counter() - t0
+    value = 2 * args.steps / dt
+    line = {
+        'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': world, 'steps': args.steps, 'warmup': args.warmup,
+        'ms_per_step': dt / args.steps * 1e3, 'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
+        'dtype': 'f64', 'data': 'synthetic (seeded NACA 00tt airfoil)', 'impl': 'reference',
+        'config': {'workload': f'2-D airfoil N={args.n}, {args.angles} angles, TM+TE, FP64 CPU oracle port',
+                   'n_panels': args.n, 'angles': args.angles, 'seed': args.seed},
+        'cpu_baseline': {'value': value, 'unit': UNIT, 'cores': cores, 'kind': 'port',
+                         'sample': f'full TM+TE solve of the workload per step ({args.steps} steps), fill split over '
+                                   f'{cores} spawned processes, LAPACK LU/solve'},
+        'e2e': {'value': value, 'unit': UNIT, 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=10)
+    ap.add_argument('--warmup', type=int, default=3)
+    ap.add_argument('--impl', default='grim', choices=['grim', 'reference'])
+    ap.add_argument('--n', type=int, default=2048)
+    ap.add_argument('--angles', type=int, default=720)
+    ap.add_argument('--seed', type=int, default=0)
+    ap.add_argument('--cpu-sample', type=int, default=1, help='oracle solves timed for cpu_baseline (0 = skip)')
+    args = ap.parse_args()
+
+    world = int(os.environ.get('WORLD_SIZE', '1'))
+    rank = int(os.environ.get('RANK', '0'))
+    local = int(os.environ.get('LOCAL_RANK', '0'))
+
+    if args.impl == 'reference':
+        run_reference_arm(args, rank, world)
+        return
+
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=120))
+
+    from grim_20261007_b200.device import context
+    from grim_20261007_b200.execution import linear_precision
+    from grim_20261007_b200.twod import geometry as geo, operators as ops
+    from grim_20261007_b200.twod.solver import solve_monostatic_rcs_2d
+    from grim_20261007_b200 import synthetic as S
+
+    ctx = context()
+    v, k, f, thick, ang = workload(args.seed + rank, args.n, args.angles)
+    geom = geo.panel_geometry([v])
+    bodies = {'TM': ops.DeviceBody(geom, None), 'TE': ops.DeviceBody(geom, geo.te_curvature_correction([v]))}
+    ang_dev = torch.as_tensor(ang, device='cuda')
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device='cuda')
+
+    def step(precision):
+        out = {}
+        for pol in ('TM', 'TE'):
+            out[pol] = ops.monostatic_solve(bodies[pol], k, ang, pol, precision=precision, angles_dev=ang_dev)
+        return out
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def timed(precision, steps, warmup):
+        for _ in range(warmup):
+            step(precision)
+        torch.cuda.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        times = []
+        launches0 = ctx.launches
+        last = None
+        for _ in range(steps):
+            flush.fill_(1.0)  # L2 flush (256 MiB write) outside the event window
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            last = step(precision)
+            e1.record()
+            times.append((e0, e1))
+        torch.cuda.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        launches = ctx.launches - launches0
+        ms = [a.elapsed_time(b) for a, b in times]
+        return ms, launches, last
+
+    # FP64 drop-in arm (ratio and accuracy reference)
+    ms64, _l64, out64 = timed('double', max(2, args.steps // 2), 1)
+    with ClockSampler(local) as clk:
+        ms32, launches32, out32 = timed('mixed', args.steps, args.warmup)
+    clocks = clk.summary()
+
+    tot = torch.tensor([sum(ms32), sum(ms64)], dtype=torch.float64, device='cuda')
+    if world > 1:
+        dist.all_reduce(tot, op=dist.ReduceOp.MAX)
+    total_ms32, total_ms64 = float(tot[0]), float(tot[1])
+    ms_step32 = total_ms32 / args.steps
+    ms_step64 = total_ms64 / max(2, args.steps // 2)
+    value = 2 * args.steps * world / (total_ms32 / 1e3)
+    fp64_value = 2 * world / (ms_step64 / 1e3)
+
+    # accuracy of the mixed arm vs the FP64 arm (dB where sigma is within 40 dB of its peak)
+    err_db = {}
+    for pol in ('TM', 'TE'):
+        a64 = out64[pol]['amplitude'].cpu().numpy()
+        a32 = out32[pol]['amplitude'].cpu().numpy()
+        s64 = ops.sigma_2d(a64, k)
+        s32 = ops.sigma_2d(a32, k)
+        db = ops.sigma_db(s64)
+        mask = db > db.max() - 40
+        err_db[pol] = float(np.max(np.abs(10 * np.log10(s32[mask] / s64[mask]))))
+    tele32 = {p: {kk: vv for kk, vv in out32[p]['telemetry'].items() if not hasattr(vv, 'cpu')} for p in ('TM', 'TE')}
+    tele64 = {p: {kk: vv for kk, vv in out64[p]['telemetry'].items() if not hasattr(vv, 'cpu')} for p in ('TM', 'TE')}
+    berr64 = max(float(out64[p]['telemetry']['backward_error_dev'].max()) for p in ('TM', 'TE'))
+
+    # end-to-end through the public API (host geometry in, host amplitudes out)
+    snap = S.snapshot_from_polygons([v])
+    with linear_precision('mixed'):
+        solve_monostatic_rcs_2d(snap, [f / 1e9], list(ang), geometry_units='meters', strict_quality_gate=False)
+        torch.cuda.synchronize()
+        barrier()
+        t0 = time.perf_counter()
+        e2e_steps = max(2, args.steps // 2)
+        for _ in range(e2e_steps):
+            solve_monostatic_rcs_2d(snap, [f / 1e9], list(ang), geometry_units='meters', strict_quality_gate=False)
+        torch.cuda.synchronize()
+        e2e_dt = time.perf_counter() - t0
+    e2e_t = torch.tensor([e2e_dt], dtype=torch.float64, device='cuda')
+    if world > 1:
+        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
+    e2e_value = 2 * e2e_steps * world / float(e2e_t[0])
+    h2d = 2 * (geom.nbytes + len(ang) * 8) + geom.shape[0] * 8
+    d2h = 2 * len(ang) * 16
+
+    # roofline of the dominant piece: the complex64 LU (8N^3/3 algorithmic flops per factorization)
+    n = args.n
+    lu_ms = statistics.median([tele32[p]['ms_factor'] for p in ('TM', 'TE')])
+    lu_tflops = 8.0 * n ** 3 / 3.0 / (lu_ms * 1e-3) / 1e12
+    hbm, bf16, src = _peaks()
+    roofline = {'bound': 'tensor', 'achieved': lu_tflops, 'peak': bf16, 'unit': 'TFLOP/s', 'frac': lu_tflops / bf16,
+                'traffic': None, 'kernel': 'complex64 getrf (whole factorization)', 'peak_source': src,
+                'flops_per_launch': 8.0 * n ** 3 / 3.0}
+
+    cpu_baseline = None
+    if rank == 0 and world == 1 and args.cpu_sample > 0:
+        t0 = time.perf_counter()
+        for _ in range(args.cpu_sample):
+            cpu_oracle_solve(v, k, ang, 'TM')
+        dt = time.perf_counter() - t0
+        cpu_baseline = {'value': args.cpu_sample / dt, 'unit': UNIT, 'cores': 1, 'kind': 'port',
+                        'sample': f'{args.cpu_sample} full TM solve(s) of the workload by the FP64 NumPy/SciPy oracle '
+                                  '(single-threaded SciPy Bessel fill, LAPACK LU)'}
+
+    if rank == 0:
+        line = {
+            'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': world, 'steps': args.steps,
+            'warmup': args.warmup, 'ms_per_step': ms_step32, 'higher_is_better': True, 'scaling': 'weak',
+            'vs_baseline': None, 'dtype': 'c64+f64', 'data': 'synthetic (seeded NACA 00tt airfoil)',
+            'config': {'workload': f'2-D airfoil N={n}, {args.angles} monostatic angles, TM+TE (2 solves/step), '
+                                   'mixed precision', 'n_panels': n, 'angles': args.angles, 'seed': args.seed,
+                       'frequency_ghz': f / 1e9, 'thickness': thick,
+                       'l2': 'flushed between steps (256 MiB write outside each step\'s event window)',
+                       'parallelism': f'replicas x{world}'},
+            'fp64_gpu': {'value': fp64_value, 'ms_per_step': ms_step64, 'max_backward_error': berr64},
+            'speedup_vs_fp64': value / fp64_value if fp64_value else None,
+            'max_db_error_vs_fp64': err_db,
+            'telemetry_mixed': tele32, 'telemetry_fp64': tele64,
+            'e2e': {'value': e2e_value, 'unit': UNIT, 'h2d_bytes_per_step': int(h2d), 'd2h_bytes_per_step': int(d2h),
+                    'path': 'solve_monostatic_rcs_2d (public API), linear_precision("mixed")'},
+            'gpu_launches': int(launches32),
+            'roofline': roofline,
+            'cpu_baseline': cpu_baseline,
+            'clocks': clocks,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == '__main__':
+    main()

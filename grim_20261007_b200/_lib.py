@@ -1,0 +1,123 @@
+"""ctypes binding of libgrimgpu.so (the C ABI declared in include/grimgpu.h).
+
+The product path has no CPU fallback: if the library is missing or the CUDA device
+is unusable, every entry point raises ``GrimError``.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, 'libgrimgpu.so')
+
+GRIM_OK = 0
+GRIM_ERR_ARGUMENT = 3
+GRIM_ERR_CUDA = 4
+GRIM_ERR_NOMEM = 5
+GRIM_ERR_SINGULAR = 6
+GRIM_ERR_NOT_CONVERGED = 7
+GRIM_ERR_NONFINITE = 8
+POL_TM, POL_TE = 0, 1
+PREC_FP64, PREC_MIXED = 0, 1
+
+c_int, c_int64, c_double, c_void_p, c_char_p = ctypes.c_int, ctypes.c_int64, ctypes.c_double, ctypes.c_void_p, ctypes.c_char_p
+c_size_t = ctypes.c_size_t
+P_int = ctypes.POINTER(ctypes.c_int)
+
+
+class GrimSolveInfo(ctypes.Structure):
+    _fields_ = [('backward_error', c_double), ('initial_backward_error', c_double), ('refinement_steps', c_int),
+                ('pivoted_panels', c_int), ('precision_mode', c_int), ('info', c_int), ('ms_factor', c_double),
+                ('ms_solve', c_double)]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class GrimError(RuntimeError):
+    def __init__(self, code, message):
+        super().__init__(message)
+        self.code = code
+
+
+class GrimMemoryError(GrimError, MemoryError):
+    pass
+
+
+class GrimNotConverged(GrimError):
+    pass
+
+
+# (name, restype, argtypes) for every symbol of include/grimgpu.h
+SIGNATURES = [
+    ('grim_create', c_int, [c_int, ctypes.POINTER(c_void_p)]),
+    ('grim_destroy', c_int, [c_void_p]),
+    ('grim_set_stream', c_int, [c_void_p, c_void_p]),
+    ('grim_get_stream', c_void_p, [c_void_p]),
+    ('grim_synchronize', c_int, [c_void_p]),
+    ('grim_last_error', c_char_p, []),
+    ('grim_device_name', c_int, [c_void_p, c_char_p, c_int]),
+    ('grim_version', c_int, []),
+    ('grim_launch_count', c_int64, [c_void_p]),
+    ('grim_release_workspace', c_int, [c_void_p]),
+    ('grim_fill2d', c_int, [c_void_p, c_int, c_int, c_void_p, c_void_p, c_double, c_void_p, c_int64, c_int]),
+    ('grim_rhs2d', c_int, [c_void_p, c_int, c_int, c_void_p, c_int, c_void_p, c_double, c_void_p, c_int64, c_int]),
+    ('grim_farfield2d', c_int, [c_void_p, c_int, c_void_p, c_int, c_void_p, c_double, c_void_p, c_int64, c_int, c_void_p]),
+    ('grim_zgetrf', c_int, [c_void_p, c_int, c_void_p, c_int64, c_void_p, P_int]),
+    ('grim_zgetrs', c_int, [c_void_p, c_int, c_int, c_void_p, c_int64, c_void_p, c_void_p, c_int64]),
+    ('grim_cgetrf', c_int, [c_void_p, c_int, c_void_p, c_int64, c_void_p, P_int]),
+    ('grim_cgetrs', c_int, [c_void_p, c_int, c_int, c_void_p, c_int64, c_void_p, c_void_p, c_int64]),
+    ('grim_backward_error', c_int, [c_void_p, c_int, c_int, c_void_p, c_int64, c_int, c_void_p, c_int64, c_void_p,
+                                    c_int64, c_void_p]),
+    ('grim_zgesv_mixed', c_int, [c_void_p, c_int, c_int, c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_int64,
+                                 c_int, c_double, c_int, P_int, ctypes.POINTER(GrimSolveInfo)]),
+    ('grim_zgesv_batched', c_int, [c_void_p, c_int, c_int, c_void_p, c_int, c_void_p, c_int, c_int, P_int]),
+    ('grim_last_solve_info', c_int, [c_void_p, ctypes.POINTER(GrimSolveInfo)]),
+    ('grim_mem_info', c_int, [c_void_p, ctypes.POINTER(c_size_t), ctypes.POINTER(c_size_t)]),
+]
+
+_lib = None
+_lock = threading.Lock()
+
+
+def header_symbols():
+    """Every function name declared in include/grimgpu.h (for export checks)."""
+    import re
+    path = os.path.join(os.path.dirname(_HERE), 'include', 'grimgpu.h')
+    text = open(path).read()
+    return sorted(set(re.findall(r'\b(grim_[a-z0-9_]+)\s*\(', text)))
+
+
+def load():
+    """Load libgrimgpu.so (no GPU needed) and bind every declared symbol."""
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        if not os.path.exists(LIB_PATH):
+            raise GrimError(GRIM_ERR_CUDA, f'libgrimgpu.so not built at {LIB_PATH}; run grim_20261007_b200/csrc/build.py')
+        lib = ctypes.CDLL(LIB_PATH)
+        for name, res, args in SIGNATURES:
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+        return lib
+
+
+def last_error():
+    msg = load().grim_last_error()
+    return msg.decode(errors='replace') if msg else ''
+
+
+def check(status, what=''):
+    if status == GRIM_OK:
+        return
+    msg = f'{what}: {last_error()}' if what else last_error()
+    if status == GRIM_ERR_NOMEM:
+        raise GrimMemoryError(status, msg)
+    if status == GRIM_ERR_NOT_CONVERGED:
+        raise GrimNotConverged(status, msg)
+    raise GrimError(status, msg)

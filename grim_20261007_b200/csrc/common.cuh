@@ -1,0 +1,150 @@
+// Shared device/host helpers for libgrimgpu: complex arithmetic on interleaved
+// pairs, the handle (context) structure, error reporting, workspace.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/grimgpu.h"
+
+// ---------------------------------------------------------------- complex math
+template <typename T> struct cplx_of;
+template <> struct cplx_of<double> { using type = double2; };
+template <> struct cplx_of<float> { using type = float2; };
+
+template <typename C> struct real_of;
+template <> struct real_of<double2> { using type = double; };
+template <> struct real_of<float2> { using type = float; };
+
+__host__ __device__ __forceinline__ double2 mk(double a, double b) { return make_double2(a, b); }
+__host__ __device__ __forceinline__ float2 mk(float a, float b) { return make_float2(a, b); }
+
+template <typename C> __host__ __device__ __forceinline__ C cadd(C a, C b) { return mk(a.x + b.x, a.y + b.y); }
+template <typename C> __host__ __device__ __forceinline__ C csub(C a, C b) { return mk(a.x - b.x, a.y - b.y); }
+template <typename C> __host__ __device__ __forceinline__ C cmul(C a, C b) {
+    return mk(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+// acc += a*b
+template <typename C> __host__ __device__ __forceinline__ void cfma(C &acc, C a, C b) {
+    acc.x = fma(a.x, b.x, acc.x);
+    acc.x = fma(-a.y, b.y, acc.x);
+    acc.y = fma(a.x, b.y, acc.y);
+    acc.y = fma(a.y, b.x, acc.y);
+}
+// acc -= a*b
+template <typename C> __host__ __device__ __forceinline__ void cfms(C &acc, C a, C b) {
+    acc.x = fma(-a.x, b.x, acc.x);
+    acc.x = fma(a.y, b.y, acc.x);
+    acc.y = fma(-a.x, b.y, acc.y);
+    acc.y = fma(-a.y, b.x, acc.y);
+}
+// a / b (Smith's algorithm, avoids overflow in |b|^2)
+template <typename C> __host__ __device__ __forceinline__ C cdiv(C a, C b) {
+    using R = typename real_of<C>::type;
+    R ar = a.x, ai = a.y, br = b.x, bi = b.y;
+    if (fabs(br) >= fabs(bi)) {
+        R r = bi / br, d = br + bi * r;
+        return mk((ar + ai * r) / d, (ai - ar * r) / d);
+    } else {
+        R r = br / bi, d = bi + br * r;
+        return mk((ar * r + ai) / d, (ai * r - ar) / d);
+    }
+}
+template <typename C> __host__ __device__ __forceinline__ typename real_of<C>::type cabs1(C a) {
+    return fabs(a.x) + fabs(a.y);
+}
+template <typename C> __host__ __device__ __forceinline__ C czero() { return mk((typename real_of<C>::type)0, (typename real_of<C>::type)0); }
+
+__device__ __forceinline__ double2 to_c64(float2 a) { return make_double2((double)a.x, (double)a.y); }
+__device__ __forceinline__ double2 to_c64(double2 a) { return a; }
+__device__ __forceinline__ float2 to_c32(double2 a) { return make_float2((float)a.x, (float)a.y); }
+__device__ __forceinline__ float2 to_c32(float2 a) { return a; }
+template <typename C> __device__ __forceinline__ C conv(double2 a);
+template <> __device__ __forceinline__ double2 conv<double2>(double2 a) { return a; }
+template <> __device__ __forceinline__ float2 conv<float2>(double2 a) { return to_c32(a); }
+
+// ---------------------------------------------------------------- error handling
+void grim_set_error(const std::string &msg);
+int grim_fail(int code, const std::string &msg);
+int grim_cuda_check(cudaError_t e, const char *what);
+
+#define GRIM_CHECK_CUDA(call)                                                     \
+    do {                                                                          \
+        cudaError_t _e = (call);                                                  \
+        if (_e != cudaSuccess) return grim_cuda_check(_e, #call);                 \
+    } while (0)
+
+#define GRIM_CHECK_LAUNCH(h, what)                                                \
+    do {                                                                          \
+        (h)->launches++;                                                          \
+        cudaError_t _e = cudaGetLastError();                                      \
+        if (_e != cudaSuccess) return grim_cuda_check(_e, what);                  \
+    } while (0)
+
+#define GRIM_TRY(call)                                                            \
+    do {                                                                          \
+        int _s = (call);                                                          \
+        if (_s != GRIM_OK) return _s;                                             \
+    } while (0)
+
+// ---------------------------------------------------------------- context
+struct grim_context {
+    int device = 0;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    int64_t launches = 0;
+    // named, grow-only device workspace buffers (stream-ordered allocations)
+    std::unordered_map<std::string, std::pair<void *, size_t>> ws;
+    grim_solve_info last{};
+    int sm_count = 148;
+};
+
+// Ensure a named workspace of at least `bytes` exists; returns its pointer in *out.
+int grim_workspace(grim_context *h, const char *name, size_t bytes, void **out);
+
+// Gauss-Legendre rules in constant memory, filled at context creation.
+// Orders 1..GRIM_MAX_GAUSS are stored at offset order*(order-1)/2.
+#define GRIM_MAX_GAUSS 32
+int grim_upload_gauss(void);
+
+// Scoped device guard
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+// Event-timed region on the handle stream.
+struct StreamTimer {
+    cudaEvent_t a = nullptr, b = nullptr;
+    cudaStream_t s;
+    explicit StreamTimer(cudaStream_t st) : s(st) {
+        cudaEventCreate(&a);
+        cudaEventCreate(&b);
+        cudaEventRecord(a, s);
+    }
+    double stop_ms() {
+        float ms = 0.f;
+        cudaEventRecord(b, s);
+        cudaEventSynchronize(b);
+        cudaEventElapsedTime(&ms, a, b);
+        return (double)ms;
+    }
+    ~StreamTimer() {
+        if (a) cudaEventDestroy(a);
+        if (b) cudaEventDestroy(b);
+    }
+};
+
+static inline int ceil_div(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }

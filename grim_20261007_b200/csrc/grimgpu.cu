@@ -1,0 +1,591 @@
+// libgrimgpu: C-ABI exports and host orchestration of the B200 RCS solve path.
+// One translation unit (constant-memory tables are shared by every kernel).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "fill2d.cuh"
+#include "hankel.cuh"
+#include "linalg.cuh"
+
+// ============================================================== errors
+static thread_local std::string g_last_error;
+
+void grim_set_error(const std::string &msg) { g_last_error = msg; }
+int grim_fail(int code, const std::string &msg) {
+    g_last_error = msg;
+    return code;
+}
+int grim_cuda_check(cudaError_t e, const char *what) {
+    g_last_error = std::string(what) + ": " + cudaGetErrorString(e);
+    return e == cudaErrorMemoryAllocation ? GRIM_ERR_NOMEM : GRIM_ERR_CUDA;
+}
+
+// ============================================================== tables
+// Gauss-Legendre nodes by Newton iteration on P_q (three-term recurrence), weights
+// 2 / ((1 - x^2) P_q'(x)^2).
+static void gauss_legendre(int q, double *x, double *w) {
+    for (int i = 0; i < q; ++i) {
+        double z = std::cos(M_PI * (i + 0.75) / (q + 0.5));
+        double dp = 1.0;
+        for (int it = 0; it < 100; ++it) {
+            double p0 = 1.0, p1 = z;
+            for (int l = 2; l <= q; ++l) {
+                const double p2 = ((2.0 * l - 1.0) * z * p1 - (l - 1.0) * p0) / l;
+                p0 = p1;
+                p1 = p2;
+            }
+            if (q == 1) { p1 = z; p0 = 1.0; }
+            dp = q * (z * p1 - p0) / (z * z - 1.0);
+            const double dz = p1 / dp;
+            z -= dz;
+            if (std::fabs(dz) < 1e-16) {
+                // one more polish step
+                p0 = 1.0; p1 = z;
+                for (int l = 2; l <= q; ++l) {
+                    const double p2 = ((2.0 * l - 1.0) * z * p1 - (l - 1.0) * p0) / l;
+                    p0 = p1;
+                    p1 = p2;
+                }
+                if (q == 1) { p1 = z; p0 = 1.0; }
+                dp = q * (z * p1 - p0) / (z * z - 1.0);
+                break;
+            }
+        }
+        // nodes ascending
+        x[q - 1 - i] = z;
+        w[q - 1 - i] = 2.0 / ((1.0 - z * z) * dp * dp);
+    }
+    if (q == 1) { x[0] = 0.0; w[0] = 2.0; }
+}
+
+static std::mutex g_table_mutex;
+static std::vector<int> g_tables_ready;  // per device
+
+static int upload_tables(int device) {
+    std::lock_guard<std::mutex> lk(g_table_mutex);
+    if ((int)g_tables_ready.size() <= device) g_tables_ready.resize(device + 1, 0);
+    if (g_tables_ready[device]) return GRIM_OK;
+    std::vector<double> gx(GRIM_MAX_GAUSS * (GRIM_MAX_GAUSS + 1) / 2), gw(gx.size());
+    for (int q = 1; q <= GRIM_MAX_GAUSS; ++q) gauss_legendre(q, &gx[q * (q - 1) / 2], &gw[q * (q - 1) / 2]);
+    GRIM_CHECK_CUDA(cudaMemcpyToSymbol(c_gl_x, gx.data(), gx.size() * sizeof(double)));
+    GRIM_CHECK_CUDA(cudaMemcpyToSymbol(c_gl_w, gw.data(), gw.size() * sizeof(double)));
+    float a0[GRIM_ASYM_TERMS], a1[GRIM_ASYM_TERMS];
+    double d0 = 1.0, d1 = 1.0;
+    for (int kk = 0; kk < GRIM_ASYM_TERMS; ++kk) {
+        if (kk > 0) {
+            const double odd = (2.0 * kk - 1.0) * (2.0 * kk - 1.0);
+            d0 *= (0.0 - odd) / (8.0 * kk);
+            d1 *= (4.0 - odd) / (8.0 * kk);
+        }
+        a0[kk] = (float)d0;
+        a1[kk] = (float)d1;
+    }
+    GRIM_CHECK_CUDA(cudaMemcpyToSymbol(c_asym_a0, a0, sizeof(a0)));
+    GRIM_CHECK_CUDA(cudaMemcpyToSymbol(c_asym_a1, a1, sizeof(a1)));
+    g_tables_ready[device] = 1;
+    return GRIM_OK;
+}
+
+int grim_upload_gauss(void) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    return upload_tables(dev);
+}
+
+// ============================================================== workspace
+int grim_workspace(grim_context *h, const char *name, size_t bytes, void **out) {
+    auto it = h->ws.find(name);
+    if (it != h->ws.end() && it->second.second >= bytes) {
+        *out = it->second.first;
+        return GRIM_OK;
+    }
+    if (it != h->ws.end()) {
+        GRIM_CHECK_CUDA(cudaFreeAsync(it->second.first, h->stream));
+        h->ws.erase(it);
+    }
+    void *p = nullptr;
+    const size_t want = std::max<size_t>(bytes, 256);
+    cudaError_t e = cudaMallocAsync(&p, want, h->stream);
+    if (e != cudaSuccess) return grim_cuda_check(e, "workspace allocation");
+    h->ws[name] = {p, want};
+    *out = p;
+    return GRIM_OK;
+}
+
+// ============================================================== context API
+extern "C" int grim_version(void) { return 1; }
+extern "C" const char *grim_last_error(void) { return g_last_error.c_str(); }
+
+extern "C" int grim_create(int device, grim_handle_t *out) {
+    if (!out) return grim_fail(GRIM_ERR_ARGUMENT, "grim_create: null output pointer");
+    int count = 0;
+    GRIM_CHECK_CUDA(cudaGetDeviceCount(&count));
+    if (device < 0 || device >= count) return grim_fail(GRIM_ERR_ARGUMENT, "grim_create: no such CUDA device");
+    DeviceGuard g(device);
+    auto *h = new grim_context();
+    h->device = device;
+    cudaError_t e = cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete h;
+        return grim_cuda_check(e, "cudaStreamCreate");
+    }
+    h->stream = h->own_stream;
+    cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, device);
+    int s = upload_tables(device);
+    if (s != GRIM_OK) {
+        cudaStreamDestroy(h->own_stream);
+        delete h;
+        return s;
+    }
+    *out = h;
+    return GRIM_OK;
+}
+
+extern "C" int grim_release_workspace(grim_handle_t h) {
+    if (!h) return grim_fail(GRIM_ERR_ARGUMENT, "null handle");
+    DeviceGuard g(h->device);
+    for (auto &kv : h->ws) cudaFreeAsync(kv.second.first, h->stream);
+    h->ws.clear();
+    GRIM_CHECK_CUDA(cudaStreamSynchronize(h->stream));
+    return GRIM_OK;
+}
+
+extern "C" int grim_destroy(grim_handle_t h) {
+    if (!h) return GRIM_OK;
+    DeviceGuard g(h->device);
+    grim_release_workspace(h);
+    if (h->own_stream) cudaStreamDestroy(h->own_stream);
+    delete h;
+    return GRIM_OK;
+}
+
+extern "C" int grim_set_stream(grim_handle_t h, void *stream) {
+    if (!h) return grim_fail(GRIM_ERR_ARGUMENT, "null handle");
+    h->stream = stream ? (cudaStream_t)stream : h->own_stream;
+    return GRIM_OK;
+}
+extern "C" void *grim_get_stream(grim_handle_t h) { return h ? (void *)h->stream : nullptr; }
+extern "C" int grim_synchronize(grim_handle_t h) {
+    if (!h) return grim_fail(GRIM_ERR_ARGUMENT, "null handle");
+    DeviceGuard g(h->device);
+    GRIM_CHECK_CUDA(cudaStreamSynchronize(h->stream));
+    return GRIM_OK;
+}
+extern "C" int64_t grim_launch_count(grim_handle_t h) { return h ? h->launches : 0; }
+extern "C" int grim_device_name(grim_handle_t h, char *buf, int len) {
+    if (!h || !buf || len <= 0) return grim_fail(GRIM_ERR_ARGUMENT, "grim_device_name: bad arguments");
+    cudaDeviceProp p;
+    GRIM_CHECK_CUDA(cudaGetDeviceProperties(&p, h->device));
+    std::snprintf(buf, (size_t)len, "%s", p.name);
+    return GRIM_OK;
+}
+extern "C" int grim_mem_info(grim_handle_t h, size_t *free_bytes, size_t *total_bytes) {
+    if (!h || !free_bytes || !total_bytes) return grim_fail(GRIM_ERR_ARGUMENT, "grim_mem_info: bad arguments");
+    DeviceGuard g(h->device);
+    GRIM_CHECK_CUDA(cudaMemGetInfo(free_bytes, total_bytes));
+    return GRIM_OK;
+}
+extern "C" int grim_last_solve_info(grim_handle_t h, grim_solve_info *out) {
+    if (!h || !out) return grim_fail(GRIM_ERR_ARGUMENT, "grim_last_solve_info: bad arguments");
+    *out = h->last;
+    return GRIM_OK;
+}
+
+// ============================================================== 2-D fill / rhs / far field
+extern "C" int grim_fill2d(grim_handle_t h, int pol, int n, const double *geom, const double *diag_extra, double k,
+                           void *Z, int64_t ldz, int out_complex64) {
+    if (!h || n <= 0 || !geom || !Z || ldz < n || !(k > 0) || (pol != GRIM_POL_TM && pol != GRIM_POL_TE))
+        return grim_fail(GRIM_ERR_ARGUMENT, "grim_fill2d: bad arguments");
+    DeviceGuard g(h->device);
+    dim3 grid(ceil_div(n, FILL_ROWS), ceil_div(n, FILL_COLS));
+    dim3 block(FILL_ROWS * FILL_WARPS);
+    if (out_complex64) {
+        if (pol == GRIM_POL_TM)
+            k_fill2d<GRIM_POL_TM, float2><<<grid, block, 0, h->stream>>>(n, geom, diag_extra, k, (float2 *)Z, ldz);
+        else
+            k_fill2d<GRIM_POL_TE, float2><<<grid, block, 0, h->stream>>>(n, geom, diag_extra, k, (float2 *)Z, ldz);
+    } else {
+        if (pol == GRIM_POL_TM)
+            k_fill2d<GRIM_POL_TM, double2><<<grid, block, 0, h->stream>>>(n, geom, diag_extra, k, (double2 *)Z, ldz);
+        else
+            k_fill2d<GRIM_POL_TE, double2><<<grid, block, 0, h->stream>>>(n, geom, diag_extra, k, (double2 *)Z, ldz);
+    }
+    GRIM_CHECK_LAUNCH(h, "k_fill2d");
+    return GRIM_OK;
+}
+
+extern "C" int grim_rhs2d(grim_handle_t h, int pol, int n, const double *geom, int nang, const double *angles_deg,
+                          double k, void *B, int64_t ldb, int out_complex64) {
+    if (!h || n <= 0 || nang <= 0 || !geom || !angles_deg || !B || ldb < n || nang > 65535 ||
+        (pol != GRIM_POL_TM && pol != GRIM_POL_TE))
+        return grim_fail(GRIM_ERR_ARGUMENT, "grim_rhs2d: bad arguments");
+    DeviceGuard g(h->device);
+    dim3 grid(ceil_div(n, 256), nang);
+    if (out_complex64) {
+        if (pol == GRIM_POL_TM) k_rhs2d<GRIM_POL_TM, float2><<<grid, 256, 0, h->stream>>>(n, geom, nang, angles_deg, k, (float2 *)B, ldb);
+        else k_rhs2d<GRIM_POL_TE, float2><<<grid, 256, 0, h->stream>>>(n, geom, nang, angles_deg, k, (float2 *)B, ldb);
+    } else {
+        if (pol == GRIM_POL_TM) k_rhs2d<GRIM_POL_TM, double2><<<grid, 256, 0, h->stream>>>(n, geom, nang, angles_deg, k, (double2 *)B, ldb);
+        else k_rhs2d<GRIM_POL_TE, double2><<<grid, 256, 0, h->stream>>>(n, geom, nang, angles_deg, k, (double2 *)B, ldb);
+    }
+    GRIM_CHECK_LAUNCH(h, "k_rhs2d");
+    return GRIM_OK;
+}
+
+extern "C" int grim_farfield2d(grim_handle_t h, int n, const double *geom, int nang, const double *angles_deg, double k,
+                               const void *X, int64_t ldx, int x_complex64, void *amp) {
+    if (!h || n <= 0 || nang <= 0 || !geom || !angles_deg || !X || !amp || ldx < n)
+        return grim_fail(GRIM_ERR_ARGUMENT, "grim_farfield2d: bad arguments");
+    DeviceGuard g(h->device);
+    if (x_complex64)
+        k_farfield2d<float2><<<nang, 256, 0, h->stream>>>(n, geom, nang, angles_deg, k, (const float2 *)X, ldx, (double2 *)amp);
+    else
+        k_farfield2d<double2><<<nang, 256, 0, h->stream>>>(n, geom, nang, angles_deg, k, (const double2 *)X, ldx, (double2 *)amp);
+    GRIM_CHECK_LAUNCH(h, "k_farfield2d");
+    return GRIM_OK;
+}
+
+// ============================================================== GEMM launcher
+template <typename ACC, typename TA, typename TB, typename TC, bool NEG, bool BETA>
+static int gemm(grim_context *h, int M, int N, int K, const TA *A, int64_t lda, const TB *B, int64_t ldb, TC *C,
+                int64_t ldc) {
+    if (M <= 0 || N <= 0) return GRIM_OK;
+    dim3 grid(ceil_div(M, GEMM_BM), ceil_div(N, GEMM_BN));
+    k_gemm<ACC, TA, TB, TC, NEG, BETA><<<grid, GEMM_THREADS, 0, h->stream>>>(M, N, K, A, lda, B, ldb, C, ldc);
+    GRIM_CHECK_LAUNCH(h, "k_gemm");
+    return GRIM_OK;
+}
+
+// ============================================================== getrf / getrs
+template <typename C>
+static int smem_opt_in() {
+    static bool done = false;
+    if (done) return GRIM_OK;
+    const int big = 3 * LU_NB * LU_NB * (int)sizeof(C);
+    GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_diag_lu<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_panel_fix<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_invert_blocks<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    const int strip = LU_NB * 32 * (int)sizeof(C);
+    GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_panel_l21<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, strip));
+    GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_row_update<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, strip));
+    GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_tri_apply<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, strip));
+    done = true;
+    return GRIM_OK;
+}
+
+// Device counters for one factorization: [0] info, [1] pivoted panels, [2..2+npan) cert, then swapped.
+template <typename C>
+static int getrf_impl(grim_context *h, int n, C *A, int64_t lda, int *ipiv, int *info_host) {
+    if (!h || n <= 0 || !A || lda < n || !ipiv) return grim_fail(GRIM_ERR_ARGUMENT, "getrf: bad arguments");
+    DeviceGuard g(h->device);
+    GRIM_TRY(smem_opt_in<C>());
+    const int nb = LU_NB;
+    const int npan = ceil_div(n, nb);
+    void *p_inv = nullptr, *p_backup = nullptr, *p_flags = nullptr;
+    GRIM_TRY(grim_workspace(h, "lu_inv", 2 * (size_t)LU_NB * LU_NB * sizeof(C), &p_inv));
+    GRIM_TRY(grim_workspace(h, "lu_backup", (size_t)n * nb * sizeof(C), &p_backup));
+    GRIM_TRY(grim_workspace(h, "lu_flags", (size_t)(2 + 2 * npan) * sizeof(int), &p_flags));
+    C *linv = (C *)p_inv, *uinv = linv + LU_NB * LU_NB, *backup = (C *)p_backup;
+    int *flags = (int *)p_flags;
+    int *d_info = flags, *d_pivoted = flags + 1, *cert = flags + 2, *swapped = flags + 2 + npan;
+    GRIM_CHECK_CUDA(cudaMemsetAsync(flags, 0, (size_t)(2 + 2 * npan) * sizeof(int), h->stream));
+    const size_t big = 3 * (size_t)LU_NB * LU_NB * sizeof(C);
+    const size_t strip = (size_t)LU_NB * 32 * sizeof(C);
+    for (int p = 0; p < npan; ++p) {
+        const int j = p * nb, nbj = std::min(nb, n - j);
+        k_diag_lu<C><<<1, 256, big, h->stream>>>(n, A, lda, j, nbj, linv, uinv, backup, cert + p, ipiv);
+        GRIM_CHECK_LAUNCH(h, "k_diag_lu");
+        const int below = n - j - nbj;
+        if (below > 0) {
+            k_panel_l21<C><<<ceil_div(below, 32), 256, strip, h->stream>>>(n, A, lda, j, nbj, uinv, backup, cert + p);
+            GRIM_CHECK_LAUNCH(h, "k_panel_l21");
+        }
+        k_panel_fix<C><<<1, 1024, big, h->stream>>>(n, A, lda, j, nbj, linv, uinv, backup, cert + p, swapped + p, ipiv,
+                                                   d_info, d_pivoted);
+        GRIM_CHECK_LAUNCH(h, "k_panel_fix");
+        const int right = n - j - nbj;
+        if (right > 0) {
+            k_row_update<C><<<ceil_div(right, 32), 256, strip, h->stream>>>(n, A, lda, j, nbj, linv, swapped + p, ipiv);
+            GRIM_CHECK_LAUNCH(h, "k_row_update");
+            GRIM_TRY((gemm<C, C, C, C, true, true>(h, below, right, nbj, A + (int64_t)j * lda + j + nbj, lda,
+                                                  A + (int64_t)(j + nbj) * lda + j, lda,
+                                                  A + (int64_t)(j + nbj) * lda + j + nbj, lda)));
+        }
+    }
+    k_laswp_left<C><<<ceil_div(n, 128), 128, 0, h->stream>>>(n, A, lda, nb, swapped, ipiv);
+    GRIM_CHECK_LAUNCH(h, "k_laswp_left");
+    int hostf[2] = {0, 0};
+    GRIM_CHECK_CUDA(cudaMemcpyAsync(hostf, flags, 2 * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    GRIM_CHECK_CUDA(cudaStreamSynchronize(h->stream));
+    if (info_host) *info_host = hostf[0];
+    h->last.pivoted_panels = hostf[1];
+    h->last.info = hostf[0];
+    return GRIM_OK;
+}
+
+template <typename C>
+static int getrs_impl(grim_context *h, int n, int nrhs, const C *LU, int64_t lda, const int *ipiv, C *B, int64_t ldb) {
+    if (!h || n <= 0 || nrhs <= 0 || !LU || !ipiv || !B || lda < n || ldb < n)
+        return grim_fail(GRIM_ERR_ARGUMENT, "getrs: bad arguments");
+    DeviceGuard g(h->device);
+    GRIM_TRY(smem_opt_in<C>());
+    const int nb = LU_NB, npan = ceil_div(n, nb);
+    void *p_inv = nullptr;
+    GRIM_TRY(grim_workspace(h, sizeof(C) == 16 ? "rs_inv64" : "rs_inv32", 2 * (size_t)npan * LU_NB * LU_NB * sizeof(C), &p_inv));
+    C *linv = (C *)p_inv, *uinv = linv + (size_t)npan * LU_NB * LU_NB;
+    const size_t big = 3 * (size_t)LU_NB * LU_NB * sizeof(C);
+    const size_t strip = (size_t)LU_NB * 32 * sizeof(C);
+    k_invert_blocks<C><<<npan, 256, big, h->stream>>>(n, LU, lda, nb, linv, uinv);
+    GRIM_CHECK_LAUNCH(h, "k_invert_blocks");
+    k_laswp_rhs<C><<<ceil_div(nrhs, 128), 128, 0, h->stream>>>(n, nrhs, B, ldb, ipiv);
+    GRIM_CHECK_LAUNCH(h, "k_laswp_rhs");
+    const int ctiles = ceil_div(nrhs, 32);
+    for (int p = 0; p < npan; ++p) {
+        const int j = p * nb, nbj = std::min(nb, n - j);
+        k_tri_apply<C><<<ctiles, 256, strip, h->stream>>>(nrhs, B, ldb, j, nbj, linv + (size_t)p * LU_NB * LU_NB);
+        GRIM_CHECK_LAUNCH(h, "k_tri_apply");
+        const int below = n - j - nbj;
+        if (below > 0)
+            GRIM_TRY((gemm<C, C, C, C, true, true>(h, below, nrhs, nbj, LU + (int64_t)j * lda + j + nbj, lda, B + j, ldb,
+                                                  B + j + nbj, ldb)));
+    }
+    for (int p = npan - 1; p >= 0; --p) {
+        const int j = p * nb, nbj = std::min(nb, n - j);
+        k_tri_apply<C><<<ctiles, 256, strip, h->stream>>>(nrhs, B, ldb, j, nbj, uinv + (size_t)p * LU_NB * LU_NB);
+        GRIM_CHECK_LAUNCH(h, "k_tri_apply");
+        if (j > 0)
+            GRIM_TRY((gemm<C, C, C, C, true, true>(h, j, nrhs, nbj, LU + (int64_t)j * lda, lda, B + j, ldb, B, ldb)));
+    }
+    return GRIM_OK;
+}
+
+extern "C" int grim_zgetrf(grim_handle_t h, int n, void *A, int64_t lda, int *ipiv, int *info) {
+    return getrf_impl<double2>(h, n, (double2 *)A, lda, ipiv, info);
+}
+extern "C" int grim_cgetrf(grim_handle_t h, int n, void *A, int64_t lda, int *ipiv, int *info) {
+    return getrf_impl<float2>(h, n, (float2 *)A, lda, ipiv, info);
+}
+extern "C" int grim_zgetrs(grim_handle_t h, int n, int nrhs, const void *LU, int64_t lda, const int *ipiv, void *B,
+                           int64_t ldb) {
+    return getrs_impl<double2>(h, n, nrhs, (const double2 *)LU, lda, ipiv, (double2 *)B, ldb);
+}
+extern "C" int grim_cgetrs(grim_handle_t h, int n, int nrhs, const void *LU, int64_t lda, const int *ipiv, void *B,
+                           int64_t ldb) {
+    return getrs_impl<float2>(h, n, nrhs, (const float2 *)LU, lda, ipiv, (float2 *)B, ldb);
+}
+
+// ============================================================== residual / backward error
+// R = B - A X (FP64 arithmetic; A complex128 or complex64), then per-column maxima and the
+// normwise backward error.  maxes_dev[0] = max berr, [1] = max relative residual.
+template <typename TA>
+static int residual_and_berr(grim_context *h, int n, int nrhs, const TA *A, int64_t lda, const double2 *X, int64_t ldx,
+                             const double2 *B, int64_t ldb, double2 *R, int64_t ldr, const double *anorm, double *berr,
+                             double *relres, double *maxes) {
+    GRIM_CHECK_CUDA(cudaMemcpy2DAsync(R, ldr * sizeof(double2), B, ldb * sizeof(double2), n * sizeof(double2), nrhs,
+                                      cudaMemcpyDeviceToDevice, h->stream));
+    GRIM_TRY((gemm<double2, TA, double2, double2, true, true>(h, n, nrhs, n, A, lda, X, ldx, R, ldr)));
+    void *p = nullptr;
+    GRIM_TRY(grim_workspace(h, "berr_absmax", (size_t)3 * nrhs * sizeof(double), &p));
+    k_col_absmax3<double2><<<nrhs, 256, 0, h->stream>>>(n, R, ldr, X, ldx, B, ldb, (double *)p);
+    GRIM_CHECK_LAUNCH(h, "k_col_absmax3");
+    k_berr_finish<<<1, 1024, 0, h->stream>>>(nrhs, (const double *)p, anorm, berr, relres, maxes);
+    GRIM_CHECK_LAUNCH(h, "k_berr_finish");
+    return GRIM_OK;
+}
+
+template <typename TA>
+static int inf_norm(grim_context *h, int n, const TA *A, int64_t lda, double *anorm_dev) {
+    void *p = nullptr;
+    GRIM_TRY(grim_workspace(h, "rowsum", (size_t)n * sizeof(double), &p));
+    k_row_abs_sum<TA><<<ceil_div(n, 128), 128, 0, h->stream>>>(n, A, lda, (double *)p);
+    GRIM_CHECK_LAUNCH(h, "k_row_abs_sum");
+    k_max_reduce<<<1, 1024, 0, h->stream>>>(n, (const double *)p, anorm_dev);
+    GRIM_CHECK_LAUNCH(h, "k_max_reduce");
+    return GRIM_OK;
+}
+
+extern "C" int grim_backward_error(grim_handle_t h, int n, int nrhs, const void *A, int64_t lda, int a_complex64,
+                                   const void *X, int64_t ldx, const void *B, int64_t ldb, double *berr_dev) {
+    if (!h || n <= 0 || nrhs <= 0 || !A || !X || !B || !berr_dev || lda < n || ldx < n || ldb < n)
+        return grim_fail(GRIM_ERR_ARGUMENT, "grim_backward_error: bad arguments");
+    DeviceGuard g(h->device);
+    void *pr = nullptr, *ps = nullptr;
+    GRIM_TRY(grim_workspace(h, "be_R", (size_t)n * nrhs * sizeof(double2), &pr));
+    GRIM_TRY(grim_workspace(h, "be_scalars", 8 * sizeof(double), &ps));
+    double *sc = (double *)ps;
+    if (a_complex64) {
+        GRIM_TRY(inf_norm(h, n, (const float2 *)A, lda, sc));
+        GRIM_TRY(residual_and_berr(h, n, nrhs, (const float2 *)A, lda, (const double2 *)X, ldx, (const double2 *)B, ldb,
+                                   (double2 *)pr, n, sc, berr_dev, nullptr, sc + 1));
+    } else {
+        GRIM_TRY(inf_norm(h, n, (const double2 *)A, lda, sc));
+        GRIM_TRY(residual_and_berr(h, n, nrhs, (const double2 *)A, lda, (const double2 *)X, ldx, (const double2 *)B, ldb,
+                                   (double2 *)pr, n, sc, berr_dev, nullptr, sc + 1));
+    }
+    return GRIM_OK;
+}
+
+// ============================================================== solve (FP64 or mixed)
+template <typename TA>
+static int mixed_refine(grim_context *h, int n, int nrhs, const TA *Ares, int64_t ldres, float2 *lu32, const int *ipiv,
+                        double2 *Bio, int64_t ldb, double tol, int max_iter, grim_solve_info *st) {
+    // Bio holds B on entry and X on exit.
+    void *pB = nullptr, *pX = nullptr, *pR = nullptr, *pR32 = nullptr, *pS = nullptr;
+    GRIM_TRY(grim_workspace(h, "mx_B", (size_t)n * nrhs * sizeof(double2), &pB));
+    GRIM_TRY(grim_workspace(h, "mx_X", (size_t)n * nrhs * sizeof(double2), &pX));
+    GRIM_TRY(grim_workspace(h, "mx_R", (size_t)n * nrhs * sizeof(double2), &pR));
+    GRIM_TRY(grim_workspace(h, "mx_R32", (size_t)n * nrhs * sizeof(float2), &pR32));
+    GRIM_TRY(grim_workspace(h, "mx_scalars", 16 * sizeof(double), &pS));
+    double2 *B0 = (double2 *)pB, *X = (double2 *)pX, *R = (double2 *)pR;
+    float2 *R32 = (float2 *)pR32;
+    double *sc = (double *)pS;  // [0] anorm, [1] max berr, [2] max relres
+    GRIM_CHECK_CUDA(cudaMemcpy2DAsync(B0, n * sizeof(double2), Bio, ldb * sizeof(double2), n * sizeof(double2), nrhs,
+                                      cudaMemcpyDeviceToDevice, h->stream));
+    GRIM_TRY(inf_norm(h, n, Ares, ldres, sc));
+    dim3 eg(ceil_div(n, 256), nrhs);
+    // x0 = solve32(b)
+    k_convert<float2, double2><<<eg, 256, 0, h->stream>>>(n, nrhs, B0, n, R32, n);
+    GRIM_CHECK_LAUNCH(h, "k_convert");
+    GRIM_TRY(getrs_impl<float2>(h, n, nrhs, lu32, n, ipiv, R32, n));
+    k_convert<double2, float2><<<eg, 256, 0, h->stream>>>(n, nrhs, R32, n, X, n);
+    GRIM_CHECK_LAUNCH(h, "k_convert");
+    double prev = INFINITY;
+    int steps = 0;
+    double berr = INFINITY, relres = INFINITY, first = -1.0;
+    int status = GRIM_OK;
+    for (int it = 0; it <= max_iter; ++it) {
+        GRIM_TRY(residual_and_berr(h, n, nrhs, Ares, ldres, X, n, B0, n, R, n, sc, nullptr, nullptr, sc + 1));
+        double hv[2];
+        GRIM_CHECK_CUDA(cudaMemcpyAsync(hv, sc + 1, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        GRIM_CHECK_CUDA(cudaStreamSynchronize(h->stream));
+        berr = hv[0];
+        relres = hv[1];
+        if (first < 0) first = berr;
+        if (std::isfinite(relres) && relres <= tol) break;
+        if (!std::isfinite(relres) || relres >= prev * 0.98) {
+            status = grim_fail(GRIM_ERR_NOT_CONVERGED, "mixed-precision refinement stalled; double LU required");
+            break;
+        }
+        if (it == max_iter) {
+            status = grim_fail(GRIM_ERR_NOT_CONVERGED, "mixed-precision refinement exceeded its correction limit");
+            break;
+        }
+        prev = relres;
+        k_convert<float2, double2><<<eg, 256, 0, h->stream>>>(n, nrhs, R, n, R32, n);
+        GRIM_CHECK_LAUNCH(h, "k_convert");
+        GRIM_TRY(getrs_impl<float2>(h, n, nrhs, lu32, n, ipiv, R32, n));
+        k_add_update<float2><<<eg, 256, 0, h->stream>>>(n, nrhs, X, n, R32, n);
+        GRIM_CHECK_LAUNCH(h, "k_add_update");
+        ++steps;
+    }
+    GRIM_CHECK_CUDA(cudaMemcpy2DAsync(Bio, ldb * sizeof(double2), X, n * sizeof(double2), n * sizeof(double2), nrhs,
+                                      cudaMemcpyDeviceToDevice, h->stream));
+    st->backward_error = berr;
+    st->initial_backward_error = first;
+    st->refinement_steps = steps;
+    return status;
+}
+
+extern "C" int grim_zgesv_mixed(grim_handle_t h, int n, int nrhs, const void *A, int64_t lda, const void *A32,
+                                int64_t lda32, void *B, int64_t ldb, int precision_mode, double tol, int max_iter,
+                                int *info, grim_solve_info *stats) {
+    if (!h || n <= 0 || nrhs <= 0 || !B || ldb < n || (!A && !A32) || (A && lda < n) || (A32 && lda32 < n) ||
+        (precision_mode != GRIM_PREC_FP64 && precision_mode != GRIM_PREC_MIXED))
+        return grim_fail(GRIM_ERR_ARGUMENT, "grim_zgesv_mixed: bad arguments");
+    if (precision_mode == GRIM_PREC_FP64 && !A)
+        return grim_fail(GRIM_ERR_ARGUMENT, "grim_zgesv_mixed: FP64 mode needs the complex128 matrix");
+    DeviceGuard g(h->device);
+    grim_solve_info st{};
+    st.precision_mode = precision_mode;
+    int linfo = 0;
+    void *pipiv = nullptr;
+    GRIM_TRY(grim_workspace(h, "sv_ipiv", (size_t)n * sizeof(int), &pipiv));
+    int *ipiv = (int *)pipiv;
+    if (precision_mode == GRIM_PREC_FP64) {
+        void *plu = nullptr;
+        GRIM_TRY(grim_workspace(h, "sv_lu64", (size_t)n * n * sizeof(double2), &plu));
+        double2 *lu = (double2 *)plu;
+        GRIM_CHECK_CUDA(cudaMemcpy2DAsync(lu, n * sizeof(double2), A, lda * sizeof(double2), n * sizeof(double2), n,
+                                          cudaMemcpyDeviceToDevice, h->stream));
+        StreamTimer tf(h->stream);
+        GRIM_TRY(getrf_impl<double2>(h, n, lu, n, ipiv, &linfo));
+        st.ms_factor = tf.stop_ms();
+        st.pivoted_panels = h->last.pivoted_panels;
+        if (linfo > 0) {
+            st.info = linfo;
+            h->last = st;
+            if (info) *info = linfo;
+            return grim_fail(GRIM_ERR_SINGULAR, "grim_zgesv_mixed: matrix is exactly singular");
+        }
+        StreamTimer ts(h->stream);
+        GRIM_TRY(getrs_impl<double2>(h, n, nrhs, lu, n, ipiv, (double2 *)B, ldb));
+        st.ms_solve = ts.stop_ms();
+        st.backward_error = -1.0;
+    } else {
+        void *plu = nullptr;
+        GRIM_TRY(grim_workspace(h, "sv_lu32", (size_t)n * n * sizeof(float2), &plu));
+        float2 *lu = (float2 *)plu;
+        if (A32) {
+            GRIM_CHECK_CUDA(cudaMemcpy2DAsync(lu, n * sizeof(float2), A32, lda32 * sizeof(float2), n * sizeof(float2), n,
+                                              cudaMemcpyDeviceToDevice, h->stream));
+        } else {
+            dim3 eg(ceil_div(n, 256), n);
+            k_convert<float2, double2><<<eg, 256, 0, h->stream>>>(n, n, (const double2 *)A, lda, lu, n);
+            GRIM_CHECK_LAUNCH(h, "k_convert");
+        }
+        StreamTimer tf(h->stream);
+        GRIM_TRY(getrf_impl<float2>(h, n, lu, n, ipiv, &linfo));
+        st.ms_factor = tf.stop_ms();
+        st.pivoted_panels = h->last.pivoted_panels;
+        if (linfo > 0) {
+            st.info = linfo;
+            h->last = st;
+            if (info) *info = linfo;
+            return grim_fail(GRIM_ERR_SINGULAR, "grim_zgesv_mixed: complex64 factor is exactly singular");
+        }
+        StreamTimer ts(h->stream);
+        int s;
+        if (A)
+            s = mixed_refine<double2>(h, n, nrhs, (const double2 *)A, lda, lu, ipiv, (double2 *)B, ldb, tol, max_iter, &st);
+        else
+            s = mixed_refine<float2>(h, n, nrhs, (const float2 *)A32, lda32, lu, ipiv, (double2 *)B, ldb, tol, max_iter, &st);
+        st.ms_solve = ts.stop_ms();
+        h->last = st;
+        if (stats) *stats = st;
+        if (info) *info = 0;
+        return s;
+    }
+    h->last = st;
+    if (stats) *stats = st;
+    if (info) *info = linfo;
+    return GRIM_OK;
+}
+
+// B1 drop-in with host buffers.
+extern "C" int grim_zgesv_batched(grim_handle_t h, int n, int nrhs, const double *A, int lda, double *B, int ldb,
+                                  int precision_mode, int *info) {
+    if (!h || n <= 0 || nrhs <= 0 || !A || !B || lda < n || ldb < n)
+        return grim_fail(GRIM_ERR_ARGUMENT, "grim_zgesv_batched: bad arguments");
+    DeviceGuard g(h->device);
+    void *pa = nullptr, *pb = nullptr;
+    GRIM_TRY(grim_workspace(h, "h_A", (size_t)n * n * sizeof(double2), &pa));
+    GRIM_TRY(grim_workspace(h, "h_B", (size_t)n * nrhs * sizeof(double2), &pb));
+    GRIM_CHECK_CUDA(cudaMemcpy2DAsync(pa, n * sizeof(double2), A, (size_t)lda * sizeof(double2), n * sizeof(double2), n,
+                                      cudaMemcpyHostToDevice, h->stream));
+    GRIM_CHECK_CUDA(cudaMemcpy2DAsync(pb, n * sizeof(double2), B, (size_t)ldb * sizeof(double2), n * sizeof(double2),
+                                      nrhs, cudaMemcpyHostToDevice, h->stream));
+    int s = grim_zgesv_mixed(h, n, nrhs, pa, n, nullptr, 0, pb, n, precision_mode, 2e-12, 10, info, nullptr);
+    if (s != GRIM_OK) return s;
+    GRIM_CHECK_CUDA(cudaMemcpy2DAsync(B, (size_t)ldb * sizeof(double2), pb, n * sizeof(double2), n * sizeof(double2),
+                                      nrhs, cudaMemcpyDeviceToHost, h->stream));
+    GRIM_CHECK_CUDA(cudaStreamSynchronize(h->stream));
+    return GRIM_OK;
+}

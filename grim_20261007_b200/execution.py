@@ -1,0 +1,48 @@
+"""Execution scopes and environment settings of the GPU solve path.
+
+Mirrors the reference's scoped options:
+* ``linear_precision('double'|'mixed')`` -- ``linalg/refined_lu.py:13-22``;
+* ``GHOST_DENSE_BACKEND`` in {cpu, auto, gpu} and ``GHOST_DENSE_GPU_MIN_N`` --
+  ``twod/solver.py:291-311``, ``twod/constants.py:25-28``.  This package is the GPU
+  backend, so ``cpu`` is accepted (for configuration compatibility) but still runs
+  on the GPU: there is no CPU fallback in this product.
+"""
+from __future__ import annotations
+
+import contextvars
+import os
+from contextlib import contextmanager
+
+DENSE_GPU_BACKEND_ENV = 'GHOST_DENSE_BACKEND'
+DENSE_GPU_MIN_N_ENV = 'GHOST_DENSE_GPU_MIN_N'
+DENSE_GPU_MIN_N_DEFAULT = 768
+
+_PRECISION = contextvars.ContextVar('grim_lu_precision', default='double')
+
+
+@contextmanager
+def linear_precision(value):
+    if value not in {'double', 'mixed'}:
+        raise ValueError('LU precision must be double or mixed.')
+    token = _PRECISION.set(value)
+    try:
+        yield
+    finally:
+        _PRECISION.reset(token)
+
+
+def requested_precision():
+    return _PRECISION.get()
+
+
+def requested_dense_backend():
+    backend = os.environ.get(DENSE_GPU_BACKEND_ENV, 'gpu').strip().lower()
+    if backend not in {'cpu', 'auto', 'gpu'}:
+        raise ValueError(f'{DENSE_GPU_BACKEND_ENV} must be cpu, auto, or gpu.')
+    try:
+        minimum_n = int(os.environ.get(DENSE_GPU_MIN_N_ENV, str(DENSE_GPU_MIN_N_DEFAULT)))
+    except (TypeError, ValueError):
+        raise ValueError(f'{DENSE_GPU_MIN_N_ENV} must be a positive integer.') from None
+    if minimum_n < 1:
+        raise ValueError(f'{DENSE_GPU_MIN_N_ENV} must be a positive integer.')
+    return backend, minimum_n

@@ -1,0 +1,379 @@
+"""2-D monostatic RCS on the GPU, behind the reference's solver entry points.
+
+Public API (same names, arguments and result-dict keys as the reference):
+
+* ``solve_monostatic_rcs_2d(geometry_snapshot, frequencies_ghz, elevations_deg, ...)``
+  -- ``twod/solver.py:3193``: both co-polarised channels (VV = TE, HH = TM), samples
+  VV first then HH (``_merge_co_polarized_2d_results`` ``:2778``);
+* ``solve_monostatic_rcs_2d_single_polarization(...)`` -- ``twod/solver.py:1988``;
+* ``_solve_dense_gpu(a_eval, rhs_eval) -> (x, device_name)`` -- ``twod/solver.py:355``,
+  the ``GHOST_DENSE_BACKEND=gpu`` hook (CuPy cuSOLVER there, libgrimgpu here);
+* ``_solve_dense_system(a_mat, rhs, ...)`` -- ``twod/solver.py:613-773``: GPU solve,
+  then the FP64 normwise backward-error gate (1e-12) with at most two refinement
+  steps, raising ``RuntimeError`` when the gate fails.
+
+Physics: pulse basis, point-matched TM EFIE and TE MFIE on the straight panels of
+closed PEC contours (see ``operators.py``).  The reference discretises with linear
+Galerkin elements and a combined S + gamma D potential, so results agree with it to
+discretisation error (hundredths of a dB at 20 panels per wavelength), and with the
+analytic Mie series for the circular cylinder.
+"""
+from __future__ import annotations
+
+import cmath
+import math
+import threading
+import time
+
+import numpy as np
+import torch
+
+from .. import _lib
+from ..device import context, ptr, require_cuda
+from ..execution import requested_dense_backend, requested_precision
+from . import geometry as geo
+from . import operators as ops
+
+C0 = 299_792_458.0
+ETA0 = 376.730313668
+EPS = 1e-12
+RCS_NORM_NUMERATOR = 0.25
+RCS_AMPLITUDE_CONVENTION = "A_physical_asymptotic = +j * B_stored"
+RCS_AMPLITUDE_VERSION = 2
+DENSE_LINEAR_BACKWARD_ERROR_MAX = 1.0e-12
+MAX_PANELS_DEFAULT = 20_000
+DEFAULT_PANELS_PER_WAVELENGTH = 20
+
+_DENSE_BACKEND_LOCAL = threading.local()
+
+
+# ------------------------------------------------------------------ telemetry
+def _reset_dense_backend_telemetry():
+    _DENSE_BACKEND_LOCAL.events = []
+
+
+def _record_dense_backend_event(**event):
+    events = getattr(_DENSE_BACKEND_LOCAL, 'events', None)
+    if events is None:
+        events = []
+        _DENSE_BACKEND_LOCAL.events = events
+    events.append(dict(event))
+
+
+def _dense_backend_summary():
+    events = list(getattr(_DENSE_BACKEND_LOCAL, 'events', []) or [])
+    used = sorted({str(e.get('used', 'gpu_grim')) for e in events})
+    devices = []
+    for e in events:
+        d = str(e.get('gpu_device', '') or '')
+        if d and d not in devices:
+            devices.append(d)
+    return {
+        'linear_backend': used[0] if len(used) == 1 else ('mixed' if used else 'gpu_grim'),
+        'dense_gpu_solve_count': sum(1 for e in events if str(e.get('used', '')).startswith('gpu')),
+        'dense_cpu_solve_count': 0,
+        'dense_factorization_count': sum(int(e.get('factorizations', 1)) for e in events),
+        'dense_rhs_batch_count': len(events),
+        'dense_rhs_column_count': sum(int(e.get('rhs_columns', 0)) for e in events),
+        'dense_max_rhs_columns': max([int(e.get('rhs_columns', 0)) for e in events] or [0]),
+        'dense_mixed_precision_solve_count': sum(1 for e in events if e.get('precision') == 'mixed'),
+        'dense_fallback_reasons': [],
+        'dense_gpu_fallback_reasons': [],
+        'dense_gpu_devices': devices,
+        'dense_largest_system': max([int(e.get('n', 0)) for e in events] or [0]),
+        'dense_pivoted_panels': sum(int(e.get('pivoted_panels', 0)) for e in events),
+    }
+
+
+# ------------------------------------------------------------------ dense hook (B1)
+def _solve_dense_gpu(a_eval, rhs_eval):
+    """GPU dense solve of A X = B for every RHS column; returns (x, device_name).
+
+    Same contract as the reference hook: inputs are borrowed NumPy arrays
+    (complex128, A n x n, B n or n x k), the solution is newly owned complex128 of
+    B's shape.  Raises ``MemoryError`` when the estimated device need exceeds 80% of
+    the free memory and ``RuntimeError`` on any device failure.
+    """
+    require_cuda()
+    a = np.asarray(a_eval, dtype=np.complex128)
+    b = np.asarray(rhs_eval, dtype=np.complex128)
+    if a.ndim != 2 or a.shape[0] != a.shape[1]:
+        raise ValueError('GPU dense solve needs a square matrix.')
+    vec = b.ndim == 1
+    b2 = b[:, None] if vec else b
+    if b2.shape[0] != a.shape[0]:
+        raise ValueError('Right-hand side height must match the matrix.')
+    ctx = context()
+    free, _total = ctx.mem_info()
+    required = int(4.0 * a.nbytes + 3.0 * b2.nbytes + 64.0 * 1024.0 ** 2)
+    if required > 0.8 * float(free):
+        raise MemoryError(
+            f'GPU dense solve needs an estimated {required / 1024.0 ** 3:.3f} GiB, exceeding 80% of the '
+            f'{float(free) / 1024.0 ** 3:.3f} GiB currently free.')
+    n, nrhs = a.shape[0], b2.shape[1]
+    a_f = np.asfortranarray(a)
+    x = np.array(b2, dtype=np.complex128, order='F', copy=True)
+    info = _lib.ctypes.c_int(0)
+    mode = _lib.PREC_MIXED if requested_precision() == 'mixed' else _lib.PREC_FP64
+    try:
+        torch.cuda.current_stream().synchronize()
+        status = ctx.lib.grim_zgesv_batched(ctx.h, n, nrhs, a_f.ctypes.data_as(_lib.c_void_p), n,
+                                            x.ctypes.data_as(_lib.c_void_p), n, mode, _lib.ctypes.byref(info))
+        _lib.check(status, 'grim_zgesv_batched')
+    except _lib.GrimMemoryError as exc:
+        raise MemoryError(str(exc)) from exc
+    except _lib.GrimError as exc:
+        raise RuntimeError(f'GPU dense solve failed: {exc}') from exc
+    st = _lib.GrimSolveInfo()
+    ctx.lib.grim_last_solve_info(ctx.h, _lib.ctypes.byref(st))
+    _DENSE_BACKEND_LOCAL.last_info = st.as_dict()
+    sol = x[:, 0].copy() if vec else np.ascontiguousarray(x) if b.flags.c_contiguous else x
+    return np.asarray(sol, dtype=np.complex128), ctx.device_name
+
+
+def matrix_inf_norm(a):
+    return float(np.max(np.sum(np.abs(a), axis=1))) if a.size else 0.0
+
+
+def _solve_dense_system(a_mat, rhs, condition_diagnostics=None, label='dense system', residual_diagnostics=None):
+    """GPU solve + the reference's FP64 backward-error gate (``twod/solver.py:613-773``)."""
+    import scipy.linalg as sla
+    a_eval = np.asarray(a_mat, dtype=np.complex128)
+    rhs_eval = np.asarray(rhs, dtype=np.complex128)
+    if not (np.all(np.isfinite(a_eval)) and np.all(np.isfinite(rhs_eval))):
+        raise FloatingPointError(f'{label} contains non-finite values.')
+    requested, _ = requested_dense_backend()
+    solution, device = _solve_dense_gpu(a_eval, rhs_eval)
+    matrix_inf = matrix_inf_norm(a_eval)
+
+    def backward_metrics(candidate):
+        x_columns = np.asarray(candidate, dtype=np.complex128)
+        b_columns = rhs_eval
+        if x_columns.ndim == 1:
+            x_columns = x_columns[:, None]
+            b_columns = b_columns[:, None]
+        residual = a_eval @ x_columns - b_columns
+        r = np.max(np.abs(residual), axis=0)
+        den = matrix_inf * np.max(np.abs(x_columns), axis=0) + np.max(np.abs(b_columns), axis=0)
+        err = np.divide(r, den, out=np.zeros_like(r), where=den > 0)
+        err[(den <= 0) & (r > 0)] = math.inf
+        return residual, float(np.max(err))
+
+    residual_matrix, berr = backward_metrics(solution)
+    steps = 0
+    lu = None
+    for _ in range(2):
+        if berr <= DENSE_LINEAR_BACKWARD_ERROR_MAX:
+            break
+        corr_rhs = -residual_matrix if np.asarray(solution).ndim > 1 else -residual_matrix[:, 0]
+        corr, _dev = _solve_dense_gpu(a_eval, corr_rhs)
+        cand = solution + corr
+        cand_res, cand_err = backward_metrics(cand)
+        if cand_err >= berr:
+            break
+        solution, residual_matrix, berr, steps = cand, cand_res, cand_err, steps + 1
+    if not math.isfinite(berr):
+        raise RuntimeError(f'{label} produced a non-finite normwise backward error.')
+    if berr > DENSE_LINEAR_BACKWARD_ERROR_MAX:
+        raise RuntimeError(f'{label} normwise backward error {berr:.6g} exceeds the release limit '
+                           f'{DENSE_LINEAR_BACKWARD_ERROR_MAX:.6g}.')
+    info = dict(getattr(_DENSE_BACKEND_LOCAL, 'last_info', {}) or {})
+    _record_dense_backend_event(requested=requested, used='gpu_grim', factorizations=1,
+                                rhs_columns=1 if rhs_eval.ndim == 1 else rhs_eval.shape[1], n=a_eval.shape[0],
+                                label=str(label), gpu_device=device, refinement_steps=steps,
+                                precision=requested_precision(), pivoted_panels=info.get('pivoted_panels', 0))
+    if condition_diagnostics is not None:
+        condition_diagnostics['linear_backward_error'] = berr
+        condition_diagnostics['linear_backward_error_limit'] = DENSE_LINEAR_BACKWARD_ERROR_MAX
+        condition_diagnostics['linear_refinement_steps'] = steps
+    if residual_diagnostics is not None:
+        b_columns = rhs_eval[:, None] if rhs_eval.ndim == 1 else rhs_eval
+        norm = np.linalg.norm(b_columns, axis=0)
+        residual_diagnostics['relative_residual'] = np.linalg.norm(residual_matrix, axis=0) / np.where(norm <= EPS, 1., norm)
+    return np.asarray(solution, dtype=np.complex128)
+
+
+# ------------------------------------------------------------------ RCS helpers
+def _rcs_sigma_from_amp(amp_vec, k_value):
+    amp = np.asarray(amp_vec, dtype=np.complex128)
+    if not np.all(np.isfinite(amp.real) & np.isfinite(amp.imag)):
+        raise FloatingPointError('Far-field amplitude contains non-finite value(s).')
+    k = float(k_value)
+    if not math.isfinite(k) or k <= 0.0:
+        raise ValueError(f'RCS normalization requires positive finite k; got {k_value!r}.')
+    return np.asarray(RCS_NORM_NUMERATOR / k * np.abs(amp) ** 2, dtype=float)
+
+
+def _rcs_db_from_sigma(sigma_linear, floor_linear=EPS):
+    s = np.asarray(sigma_linear, dtype=float)
+    if not np.all(np.isfinite(s)) or np.any(s < 0.0):
+        raise ValueError('Linear RCS must contain finite non-negative values.')
+    return np.asarray(10.0 * np.log10(np.maximum(s, float(floor_linear))), dtype=float)
+
+
+def _canonical_user_polarization_label(label):
+    text = str(label or '').strip().upper()
+    if text in {'TM', 'HH', 'H', 'HORIZONTAL'}:
+        return 'TM'
+    if text in {'TE', 'VV', 'V', 'VERTICAL'}:
+        return 'TE'
+    return text
+
+
+# ------------------------------------------------------------------ public solves
+def solve_monostatic_rcs_2d_single_polarization(
+        geometry_snapshot, frequencies_ghz, elevations_deg, polarization, geometry_units="inches",
+        material_base_dir=None, progress_callback=None, quality_thresholds=None, strict_quality_gate=True,
+        compute_condition_number=False, max_panels=MAX_PANELS_DEFAULT, mesh_reference_ghz=None,
+        rcs_normalization_mode="physical", cfie_alpha=0.0, abort_event=None, solver_method="auto",
+        _shared_discretization_cache=None):
+    """Single-polarization monostatic 2-D solve on the GPU (reference ``twod/solver.py:1988``).
+
+    Angle convention (coming-from): 0 deg arrives from the right, +90 deg from the top.
+    ``linear_precision('mixed')`` selects the mixed-precision path (complex64 fill and
+    LU, FP64 refinement); the default is the FP64 drop-in.
+    """
+    if not frequencies_ghz:
+        raise ValueError('At least one frequency is required.')
+    if not elevations_deg:
+        raise ValueError('At least one elevation angle is required.')
+    freqs = [float(f) for f in frequencies_ghz]
+    elevs = [float(e) for e in elevations_deg]
+    if any((not math.isfinite(f)) or f <= 0.0 for f in freqs):
+        raise ValueError('Frequencies must be positive finite GHz values.')
+    if any(not math.isfinite(e) for e in elevs):
+        raise ValueError('Elevation angles must all be finite.')
+    if not math.isfinite(float(cfie_alpha)) or float(cfie_alpha) != 0.0:
+        raise ValueError('cfie_alpha is not implemented by any active 2-D formulation; use cfie_alpha=0.')
+    if compute_condition_number:
+        raise NotImplementedError('Condition estimates run on the reference CPU path; the GPU path reports '
+                                  'backward errors instead.')
+    pol = _canonical_user_polarization_label(polarization)
+    if pol not in ('TM', 'TE'):
+        raise ValueError(f'Unknown polarization {polarization!r}.')
+    require_cuda()
+    _reset_dense_backend_telemetry()
+    precision = requested_precision()
+    samples = []
+    residuals = []
+    stage = {'operators': 0.0, 'linear_solve': 0.0, 'far_field': 0.0}
+    total_steps = len(freqs) * (len(elevs) + 1)
+    done = 0
+    angles = np.asarray(elevs, dtype=np.float64)
+    dev = torch.device('cuda', torch.cuda.current_device())
+    angles_dev = torch.as_tensor(angles, device=dev)
+    panel_counts = []
+    for f in freqs:
+        if abort_event is not None and abort_event.is_set():
+            raise InterruptedError('Solve canceled by user.')
+        k = 2.0 * math.pi * f * 1e9 / C0
+        wavelength = C0 / (f * 1e9)
+        mesh_lambda = C0 / (float(mesh_reference_ghz) * 1e9) if mesh_reference_ghz else wavelength
+        polys = geo.contours_from_snapshot(geometry_snapshot, geometry_units, mesh_lambda, max_panels)
+        geom = geo.panel_geometry(polys)
+        te_diag = geo.te_curvature_correction(polys) if pol == 'TE' else None
+        body = ops.DeviceBody(geom, te_diag, device=dev)
+        panel_counts.append(body.n)
+        t0 = time.perf_counter()
+        res = ops.monostatic_solve(body, k, angles, pol, precision=precision, angles_dev=angles_dev)
+        amp = res['amplitude'].cpu().numpy()
+        tele = res['telemetry']
+        berr = tele.get('backward_error_dev')
+        if berr is not None:
+            berr_h = berr.cpu().numpy()
+            if not np.all(np.isfinite(berr_h)):
+                raise RuntimeError('GPU solve produced a non-finite normwise backward error.')
+            if np.max(berr_h) > DENSE_LINEAR_BACKWARD_ERROR_MAX:
+                raise RuntimeError(f'GPU solve normwise backward error {np.max(berr_h):.6g} exceeds the release '
+                                   f'limit {DENSE_LINEAR_BACKWARD_ERROR_MAX:.6g}.')
+            resid = berr_h
+        else:
+            resid = np.full(len(elevs), float(tele.get('backward_error', 0.0)))
+        stage['linear_solve'] += time.perf_counter() - t0
+        _record_dense_backend_event(requested='gpu', used='gpu_grim', factorizations=1, rhs_columns=len(elevs),
+                                    n=body.n, label=f'{pol} pulse {f:g} GHz', gpu_device=context().device_name,
+                                    precision=precision, pivoted_panels=tele.get('pivoted_panels', 0),
+                                    refinement_steps=tele.get('refinement_steps', 0))
+        sig = _rcs_sigma_from_amp(amp, k)
+        sdb = _rcs_db_from_sigma(sig)
+        for idx, e in enumerate(elevs):
+            a = complex(amp[idx])
+            samples.append({
+                'frequency_ghz': f, 'theta_inc_deg': e, 'theta_scat_deg': e,
+                'rcs_linear': float(sig[idx]), 'rcs_db': float(sdb[idx]),
+                'rcs_amp_real': a.real, 'rcs_amp_imag': a.imag,
+                'rcs_amp_phase_deg': math.degrees(cmath.phase(a)),
+                'linear_residual': float(resid[idx]),
+            })
+            residuals.append(float(resid[idx]))
+            done += 1
+        if progress_callback is not None:
+            try:
+                progress_callback(done, total_steps, f'{pol} solved {f:g} GHz')
+            except Exception:
+                pass
+    metadata = {
+        'solver_method': 'direct',
+        'formulation': 'pulse_point_matched_efie' if pol == 'TM' else 'pulse_point_matched_mfie',
+        'precision': precision,
+        'device': context().device_name,
+        'panel_count_max': max(panel_counts),
+        'panel_count_min': min(panel_counts),
+        'residual_norm_max': max(residuals) if residuals else 0.0,
+        'runtime_profile': {'stage_seconds': stage},
+        'amplitude_version': RCS_AMPLITUDE_VERSION,
+        **_dense_backend_summary(),
+    }
+    metadata['quality_gate'] = {'passed': bool(max(residuals) <= (DENSE_LINEAR_BACKWARD_ERROR_MAX if precision == 'double'
+                                                                  else ops.MIXED_RCS_TOL * 10)),
+                                'reason': 'backward error gate'}
+    if strict_quality_gate and not metadata['quality_gate']['passed']:
+        raise ValueError('Quality gate failed: backward error gate')
+    return {
+        'solver': '2d_bie_mom_rcs',
+        'scattering_mode': 'monostatic',
+        'amplitude_convention': RCS_AMPLITUDE_CONVENTION,
+        'amplitude_version': RCS_AMPLITUDE_VERSION,
+        'polarization': pol,
+        'polarization_export': pol,
+        'samples': samples,
+        'metadata': metadata,
+    }
+
+
+_CO_POLARIZED_2D_CHANNELS = (('VV', 'TE'), ('HH', 'TM'))
+
+
+def solve_monostatic_rcs_2d(geometry_snapshot, frequencies_ghz, elevations_deg, geometry_units="inches",
+                            material_base_dir=None, progress_callback=None, quality_thresholds=None,
+                            strict_quality_gate=True, compute_condition_number=False, max_panels=MAX_PANELS_DEFAULT,
+                            mesh_reference_ghz=None, rcs_normalization_mode="physical", abort_event=None,
+                            solver_method="auto"):
+    """Both physical co-polarised channels (reference ``twod/solver.py:3193``): VV (TE) then HH (TM)."""
+    channels = {}
+    for export, pol in _CO_POLARIZED_2D_CHANNELS:
+        channels[export] = solve_monostatic_rcs_2d_single_polarization(
+            geometry_snapshot, frequencies_ghz, elevations_deg, pol, geometry_units=geometry_units,
+            material_base_dir=material_base_dir, progress_callback=progress_callback,
+            quality_thresholds=quality_thresholds, strict_quality_gate=strict_quality_gate,
+            compute_condition_number=compute_condition_number, max_panels=max_panels,
+            mesh_reference_ghz=mesh_reference_ghz, rcs_normalization_mode=rcs_normalization_mode,
+            abort_event=abort_event, solver_method=solver_method)
+    samples = []
+    for export, _pol in _CO_POLARIZED_2D_CHANNELS:
+        for s in channels[export]['samples']:
+            row = dict(s)
+            row['polarization'] = export
+            samples.append(row)
+    metadata = {'channels': {k: v['metadata'] for k, v in channels.items()},
+                'polarizations': [c[0] for c in _CO_POLARIZED_2D_CHANNELS]}
+    return {
+        'solver': '2d_bie_mom_rcs',
+        'scattering_mode': 'monostatic',
+        'amplitude_convention': RCS_AMPLITUDE_CONVENTION,
+        'amplitude_version': RCS_AMPLITUDE_VERSION,
+        'polarization': 'VV+HH',
+        'polarization_export': 'VV+HH',
+        'samples': samples,
+        'metadata': metadata,
+    }

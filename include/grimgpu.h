@@ -1,0 +1,140 @@
+/*
+ * grimgpu.h -- C ABI of the B200 method-of-moments RCS solve path (libgrimgpu.so).
+ *
+ * Plain C: opaque handles, plain pointers and sizes, integer status codes.  No
+ * PyTorch or C++ types cross this boundary.  Matrices are column-major (LAPACK
+ * order) with an explicit leading dimension; complex numbers are interleaved
+ * (re, im) pairs of double (complex128) or float (complex64).
+ *
+ * Pointer kinds: functions whose name ends in _host take host memory; every
+ * other function takes DEVICE memory of the handle's device and runs on the
+ * handle's stream (asynchronously unless stated).
+ *
+ * Reference interfaces replaced (paths inside tools/GHOST/ghost_backend/):
+ *   grim_zgesv_batched   twod/solver.py:355-392  _solve_dense_gpu(a_eval, rhs_eval)
+ *                        (the GHOST_DENSE_BACKEND=gpu hook; CuPy cp.linalg.solve there)
+ *   grim_zgetrf/zgetrs   linalg/dense.py:114-155,241  DenseFactor (scipy lu_factor / lu_solve)
+ *   grim_cgetrf/cgetrs   linalg/refined_lu.py:25-61   RefinedLU complex64 factor
+ *   grim_zgesv_mixed     linalg/refined_lu.py:25-61   RefinedLU (complex64 LU + FP64 refinement)
+ *   grim_fill2d          twod/operators.py:2087-2607  _assemble_multi (system-matrix fill)
+ *   grim_rhs2d           twod/assembly/kernels.py:223-294  incident_loads
+ *   grim_farfield2d      twod/assembly/kernels.py:163-219  farfield (matched monostatic)
+ *   grim_backward_error  twod/solver.py:695-720  backward_metrics (normwise backward error)
+ *   grim_bor_*           bor/solver.py:1769-1962,2558-2608  per-mode assembly, excitation, far field
+ *
+ * Status codes: 0 = success; any other value is an error and grim_last_error()
+ * returns a message for the calling thread.
+ */
+#ifndef GRIMGPU_H
+#define GRIMGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GRIM_OK 0
+#define GRIM_ERR_ARGUMENT 3      /* same meaning as far.c:193-207's "bad arguments" */
+#define GRIM_ERR_CUDA 4
+#define GRIM_ERR_NOMEM 5
+#define GRIM_ERR_SINGULAR 6
+#define GRIM_ERR_NOT_CONVERGED 7
+#define GRIM_ERR_NONFINITE 8
+
+#define GRIM_POL_TM 0            /* HH, Dirichlet, EFIE */
+#define GRIM_POL_TE 1            /* VV, Neumann, MFIE   */
+
+#define GRIM_PREC_FP64 0         /* plain FP64 drop-in                               */
+#define GRIM_PREC_MIXED 1        /* FP32 factor, FP64 residual / update refinement   */
+
+typedef struct grim_context *grim_handle_t;
+
+/* Per-solve telemetry (reference: twod/solver.py:226-288 dense-backend events). */
+typedef struct grim_solve_info {
+    double backward_error;       /* max normwise backward error over columns        */
+    double initial_backward_error;
+    int refinement_steps;
+    int pivoted_panels;          /* panels that needed row interchanges (0 = diagonal pivots certified) */
+    int precision_mode;
+    int info;                    /* LAPACK-style: >0 = U(info,info) exactly zero      */
+    double ms_factor;            /* device time of the factorization                 */
+    double ms_solve;             /* device time of the triangular solves + refinement */
+} grim_solve_info;
+
+/* ---- context ------------------------------------------------------------------ */
+int grim_create(int device, grim_handle_t *out);
+int grim_destroy(grim_handle_t h);
+/* Use a caller stream (cudaStream_t passed as void*); NULL restores the handle's own stream. */
+int grim_set_stream(grim_handle_t h, void *stream);
+void *grim_get_stream(grim_handle_t h);
+int grim_synchronize(grim_handle_t h);
+const char *grim_last_error(void);
+int grim_device_name(grim_handle_t h, char *buf, int len);
+int grim_version(void);
+/* Number of kernel launches this handle has issued (for launch accounting). */
+int64_t grim_launch_count(grim_handle_t h);
+/* Release the handle's cached device workspace. */
+int grim_release_workspace(grim_handle_t h);
+
+/* ---- 2-D pulse-basis fill, excitation, far field --------------------------------
+ * geom: 7*n doubles, panel-major: (cx, cy, tx, ty, h, nx, ny) per panel -- midpoint,
+ *       unit tangent, half-length, outward unit normal.
+ * diag_extra: NULL or n doubles added to the TE diagonal 1/2 (curvature correction).
+ * Z is written in full (n x n, leading dimension ldz); out_complex64 selects the
+ * complex64 fill (FP32 arithmetic for kR >= 12, FP64 for small kR, self terms and
+ * phases) instead of complex128.
+ */
+int grim_fill2d(grim_handle_t h, int pol, int n, const double *geom, const double *diag_extra,
+                double k, void *Z, int64_t ldz, int out_complex64);
+/* B[:, a] = TM: -exp(jk d_a.c), TE: -jk (d_a.n) exp(jk d_a.c); d_a = (cos, sin)(angle_deg[a]). */
+int grim_rhs2d(grim_handle_t h, int pol, int n, const double *geom, int nang, const double *angles_deg,
+               double k, void *B, int64_t ldb, int out_complex64);
+/* amp[a] = sum_n X[n, a] * 2h_n exp(jk d_a.c_n) sinc(k (d_a.t_n) h_n)  (complex128 out). */
+int grim_farfield2d(grim_handle_t h, int n, const double *geom, int nang, const double *angles_deg,
+                    double k, const void *X, int64_t ldx, int x_complex64, void *amp);
+
+/* ---- dense LU / solve ------------------------------------------------------------
+ * grim_zgetrf / grim_cgetrf: LAPACK getrf semantics (partial pivoting by |re|+|im|,
+ * 1-based ipiv, info > 0 for an exactly singular U).  The factorization first
+ * eliminates without interchanges and certifies, panel by panel, that partial
+ * pivoting would have chosen every diagonal pivot; a panel that fails the
+ * certificate is refactored with row interchanges.
+ */
+int grim_zgetrf(grim_handle_t h, int n, void *A, int64_t lda, int *ipiv, int *info);
+int grim_zgetrs(grim_handle_t h, int n, int nrhs, const void *LU, int64_t lda, const int *ipiv,
+                void *B, int64_t ldb);
+int grim_cgetrf(grim_handle_t h, int n, void *A, int64_t lda, int *ipiv, int *info);
+int grim_cgetrs(grim_handle_t h, int n, int nrhs, const void *LU, int64_t lda, const int *ipiv,
+                void *B, int64_t ldb);
+
+/* Normwise backward error per column (reference twod/solver.py:695-720):
+ * berr[j] = max_i |A x_j - b_j|_i / (||A||_inf max|x_j| + max|b_j|), A complex128 or complex64. */
+int grim_backward_error(grim_handle_t h, int n, int nrhs, const void *A, int64_t lda, int a_complex64,
+                        const void *X, int64_t ldx, const void *B, int64_t ldb, double *berr_dev);
+
+/* Device-resident solve of A X = B, X overwrites B (complex128).
+ * precision_mode GRIM_PREC_FP64: zgetrf + zgetrs.  GRIM_PREC_MIXED: complex64 LU of A
+ * (or of A32 when given), FP64 residual against A (complex128, or the exact promotion
+ * of A32 when A is NULL) and FP64 update, at most max_iter steps until the backward
+ * error is <= tol or stalls (ratio > 0.98); reference linalg/refined_lu.py:25-61.
+ * A is preserved.  info: LAPACK-style.  stats may be NULL. */
+int grim_zgesv_mixed(grim_handle_t h, int n, int nrhs, const void *A, int64_t lda, const void *A32,
+                     int64_t lda32, void *B, int64_t ldb, int precision_mode, double tol, int max_iter,
+                     int *info, grim_solve_info *stats);
+
+/* B1 drop-in (host buffers): solve A X = B for all nrhs columns, X overwrites B.
+ * A: n x n complex128 column-major (lda >= n), B: n x nrhs complex128 (ldb >= n).
+ * Copies host -> device, solves, copies device -> host; synchronous. */
+int grim_zgesv_batched(grim_handle_t h, int n, int nrhs, const double *A, int lda, double *B, int ldb,
+                       int precision_mode, int *info);
+int grim_last_solve_info(grim_handle_t h, grim_solve_info *out);
+
+/* Free / total device memory in bytes (admission control). */
+int grim_mem_info(grim_handle_t h, size_t *free_bytes, size_t *total_bytes);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GRIMGPU_H */

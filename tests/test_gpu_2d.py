@@ -1,0 +1,121 @@
+"""GPU 2-D fill / excitation / far field / end-to-end solve against the FP64 oracle."""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import mie, pulse2d as P
+from grim_20261007_b200 import synthetic as S
+from tests.conftest import GOLDEN
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip('torch')
+
+
+@pytest.fixture(scope='module')
+def ctx():
+    if not torch.cuda.is_available():
+        pytest.skip('no CUDA device')
+    from grim_20261007_b200.device import context
+    return context()
+
+
+def _body(v, pol):
+    from grim_20261007_b200.twod import geometry as geo, operators as ops
+    g = geo.panel_geometry([v])
+    return ops.DeviceBody(g, geo.te_curvature_correction([v]) if pol == 'TE' else None), g
+
+
+CASES = [
+    ('circle200', lambda: (S.circle(1.0, 200), 10.0)),
+    ('naca256', lambda: (S.naca_symmetric(0.12, 256), 2 * np.pi / (S.polygon_perimeter(S.naca_symmetric(0.12, 256)) * 10 / 256))),
+    ('superellipse150', lambda: (S.superellipse(0.7, 0.3, 3.5, 150), 25.0)),
+]
+
+
+@pytest.mark.parametrize('case', CASES, ids=[c[0] for c in CASES])
+@pytest.mark.parametrize('pol', ['TM', 'TE'])
+def test_fill_fp64_matches_oracle(ctx, case, pol):
+    from grim_20261007_b200.twod import operators as ops
+    from grim_20261007_b200.device import to_host_matrix
+    v, k = case[1]()
+    body, g = _body(v, pol)
+    z = to_host_matrix(ops.fill(body, k, pol))
+    c, t, h, n = P.panel_arrays([v])
+    zr = P.fill(k, c, t, h, n, pol, te_diag=P.te_curvature_correction([v]) if pol == 'TE' else None)
+    scale = np.max(np.abs(zr), axis=0)
+    assert np.max(np.abs(z - zr) / scale[None, :]) <= 1e-12
+
+
+@pytest.mark.parametrize('case', CASES, ids=[c[0] for c in CASES])
+@pytest.mark.parametrize('pol', ['TM', 'TE'])
+def test_fill_complex64_matches_oracle(ctx, case, pol):
+    from grim_20261007_b200.twod import operators as ops
+    from grim_20261007_b200.device import to_host_matrix
+    v, k = case[1]()
+    body, g = _body(v, pol)
+    z = to_host_matrix(ops.fill(body, k, pol, complex64=True)).astype(np.complex128)
+    c, t, h, n = P.panel_arrays([v])
+    zr = P.fill(k, c, t, h, n, pol, te_diag=P.te_curvature_correction([v]) if pol == 'TE' else None)
+    scale = np.max(np.abs(zr), axis=0)
+    # FP32 entries: a few units of FP32 rounding relative to the column scale
+    assert np.max(np.abs(z - zr) / scale[None, :]) <= 2e-6
+
+
+@pytest.mark.parametrize('pol', ['TM', 'TE'])
+def test_rhs_and_farfield_match_oracle(ctx, pol):
+    from grim_20261007_b200.twod import operators as ops
+    from grim_20261007_b200.device import to_host_matrix, to_device_colmajor
+    v = S.naca_symmetric(0.1, 300)
+    k = 120.0
+    body, g = _body(v, pol)
+    ang = np.arange(0.0, 360.0, 7.5)
+    ad = torch.as_tensor(ang, device='cuda')
+    b = to_host_matrix(ops.rhs(body, k, pol, ad))
+    c, t, h, n = P.panel_arrays([v])
+    br = P.rhs(k, c, n, ang, pol)
+    assert np.max(np.abs(b - br)) <= 1e-11 * np.max(np.abs(br))
+    rng = np.random.default_rng(0)
+    x = rng.standard_normal(br.shape) + 1j * rng.standard_normal(br.shape)
+    amp = ops.farfield(body, k, ad, to_device_colmajor(x)).cpu().numpy()
+    ampr = P.monostatic_amplitude(P.farfield_weights(k, c, t, h, ang), x)
+    assert np.max(np.abs(amp - ampr)) <= 1e-12 * np.max(np.abs(ampr))
+
+
+def test_end_to_end_c1_cylinder_fp64(ctx):
+    """Config 1: PEC cylinder a=1 m, ka=10, 200 panels, 360 angles, TM, FP64."""
+    from grim_20261007_b200.twod.solver import solve_monostatic_rcs_2d_single_polarization
+    g = np.load(os.path.join(GOLDEN, 'ref_cylinder_c1.npz'))
+    snap = S.snapshot_from_polygons([S.circle(1.0, 200)])
+    res = solve_monostatic_rcs_2d_single_polarization(snap, [float(g['frequency_ghz'])], list(g['angles']), 'TM',
+                                                      geometry_units='meters', strict_quality_gate=True)
+    amp = np.array([complex(s['rcs_amp_real'], s['rcs_amp_imag']) for s in res['samples']])
+    sig = np.array([s['rcs_linear'] for s in res['samples']])
+    o = P.solve(float(g['k']), [S.circle(1.0, 200)], g['angles'], 'TM')
+    assert np.max(np.abs(amp - o['amplitude']) / np.abs(o['amplitude'])) <= 1e-10
+    assert np.max(np.abs(10 * np.log10(sig / g['sigma_TM']))) <= 1e-3          # reference solver
+    assert abs(10 * np.log10(sig[0] / mie.cylinder_sigma(1.0, float(g['k']), 'TM'))) <= 1e-3  # Mie
+    assert max(s['linear_residual'] for s in res['samples']) <= 1e-12
+    assert res['metadata']['device']
+
+
+def test_end_to_end_co_polarized_and_mixed(ctx):
+    from grim_20261007_b200.execution import linear_precision
+    from grim_20261007_b200.twod.solver import solve_monostatic_rcs_2d
+    v, k, f, _ = S.airfoil_case(1, 512)
+    snap = S.snapshot_from_polygons([v])
+    ang = list(np.arange(0.0, 360.0, 2.0))
+    r64 = solve_monostatic_rcs_2d(snap, [f / 1e9], ang, geometry_units='meters')
+    with linear_precision('mixed'):
+        r32 = solve_monostatic_rcs_2d(snap, [f / 1e9], ang, geometry_units='meters')
+    assert [s['polarization'] for s in r64['samples']][:1] == ['VV']
+    for pol in ('TE', 'TM'):
+        o = P.solve(k, [v], ang, pol)
+        exp = 'VV' if pol == 'TE' else 'HH'
+        a64 = np.array([complex(s['rcs_amp_real'], s['rcs_amp_imag']) for s in r64['samples'] if s['polarization'] == exp])
+        s64 = np.array([s['rcs_linear'] for s in r64['samples'] if s['polarization'] == exp])
+        s32 = np.array([s['rcs_linear'] for s in r32['samples'] if s['polarization'] == exp])
+        assert np.max(np.abs(a64 - o['amplitude'])) <= 1e-9 * np.max(np.abs(o['amplitude']))
+        db64 = 10 * np.log10(s64)
+        mask = db64 > db64.max() - 40
+        assert np.max(np.abs(10 * np.log10(s32 / s64))[mask]) <= 0.05

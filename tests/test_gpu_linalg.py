@@ -1,0 +1,158 @@
+"""GPU dense LU / solve parity through the C ABI (LAPACK getrf/getrs via scipy as the oracle)."""
+import ctypes
+import os
+
+import numpy as np
+import pytest
+import scipy.linalg as sla
+
+from tests.conftest import GOLDEN
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip('torch')
+
+
+@pytest.fixture(scope='module')
+def ctx():
+    if not torch.cuda.is_available():
+        pytest.skip('no CUDA device')
+    from grim_20261007_b200.device import context
+    return context()
+
+
+def _dev(a, dtype=None):
+    from grim_20261007_b200.device import to_device_colmajor
+    return to_device_colmajor(a, dtype=dtype or torch.complex128)
+
+
+def _host(t):
+    from grim_20261007_b200.device import to_host_matrix
+    return to_host_matrix(t)
+
+
+def _rand(n, m, seed, dominant=False):
+    rng = np.random.default_rng(seed)
+    a = rng.standard_normal((n, m)) + 1j * rng.standard_normal((n, m))
+    if dominant:
+        a += np.diag(np.full(n, 4.0 * n))
+    return a
+
+
+def _getrf(ctx, a, complex64=False):
+    from grim_20261007_b200 import _lib
+    from grim_20261007_b200.device import ptr
+    n = a.shape[0]
+    t = _dev(a, torch.complex64 if complex64 else torch.complex128)
+    ipiv = torch.zeros(n, dtype=torch.int32, device='cuda')
+    info = ctypes.c_int(-1)
+    fn = ctx.lib.grim_cgetrf if complex64 else ctx.lib.grim_zgetrf
+    _lib.check(fn(ctx.h, n, ptr(t), n, ptr(ipiv), ctypes.byref(info)))
+    return t, ipiv, info.value
+
+
+@pytest.mark.parametrize('n', [1, 7, 64, 97, 200, 333])
+def test_zgetrf_matches_lapack_with_pivoting(ctx, n):
+    a = _rand(n, n, n)
+    t, ipiv, info = _getrf(ctx, a)
+    lu_ref, piv_ref = sla.lu_factor(a)
+    assert info == 0
+    np.testing.assert_array_equal(ipiv.cpu().numpy(), piv_ref + 1)
+    lu = _host(t)
+    assert np.max(np.abs(lu - lu_ref)) <= 1e-11 * max(1.0, np.max(np.abs(lu_ref)))
+
+
+@pytest.mark.parametrize('n', [64, 130, 256])
+def test_zgetrf_diagonal_certificate_path(ctx, n):
+    a = _rand(n, n, 100 + n, dominant=True)
+    t, ipiv, info = _getrf(ctx, a)
+    lu_ref, piv_ref = sla.lu_factor(a)
+    assert np.all(piv_ref == np.arange(n))
+    np.testing.assert_array_equal(ipiv.cpu().numpy(), np.arange(1, n + 1))
+    assert ctx.lib.grim_launch_count(ctx.h) > 0
+    from grim_20261007_b200 import _lib
+    st = _lib.GrimSolveInfo()
+    ctx.lib.grim_last_solve_info(ctx.h, ctypes.byref(st))
+    assert st.pivoted_panels == 0
+    assert np.max(np.abs(_host(t) - lu_ref)) <= 1e-12 * np.max(np.abs(lu_ref))
+
+
+def test_zgetrf_reports_exact_singularity(ctx):
+    a = _rand(70, 70, 3)
+    a[:, 5] = 0.0
+    _t, _ipiv, info = _getrf(ctx, a)
+    lu_ref, piv_ref, info_ref = sla.lapack.zgetrf(a)
+    assert info == info_ref == 6
+
+
+@pytest.mark.parametrize('n,nrhs', [(97, 1), (200, 33), (256, 720)])
+def test_zgetrs_multi_rhs(ctx, n, nrhs):
+    from grim_20261007_b200 import _lib
+    from grim_20261007_b200.device import ptr
+    a = _rand(n, n, 7 * n)
+    b = _rand(n, nrhs, 11 * n)
+    t, ipiv, info = _getrf(ctx, a)
+    bt = _dev(b)
+    _lib.check(ctx.lib.grim_zgetrs(ctx.h, n, nrhs, ptr(t), n, ptr(ipiv), ptr(bt), n))
+    x = _host(bt)
+    x_ref = sla.lu_solve(sla.lu_factor(a), b)
+    assert np.max(np.abs(x - x_ref)) <= 1e-10 * np.max(np.abs(x_ref))
+
+
+def test_cgetrf_matches_lapack_complex64(ctx):
+    n = 160
+    a = _rand(n, n, 5).astype(np.complex64)
+    t, ipiv, info = _getrf(ctx, a, complex64=True)
+    lu_ref, piv_ref = sla.lu_factor(a)
+    np.testing.assert_array_equal(ipiv.cpu().numpy(), piv_ref + 1)
+    assert np.max(np.abs(_host(t) - lu_ref)) <= 2e-4 * np.max(np.abs(lu_ref))
+
+
+def test_reference_dense_systems_at_the_gpu_hook(ctx):
+    """B1 parity: the reference's own assembled systems, solved through grim_zgesv_batched."""
+    from grim_20261007_b200.twod.solver import _solve_dense_gpu, _solve_dense_system
+    d = np.load(os.path.join(GOLDEN, 'ref_dense_system.npz'))
+    names = sorted({k[:-2] for k in d.files if k.endswith('_a')})
+    assert len(names) >= 7
+    for name in names:
+        a, b, x_ref = d[name + '_a'], d[name + '_b'], d[name + '_x']
+        x, dev = _solve_dense_gpu(a, b)
+        assert isinstance(dev, str) and dev
+        assert np.max(np.abs(x - x_ref)) <= 1e-10 * np.max(np.abs(x_ref)), name
+        r = a @ x - b
+        berr = np.max(np.abs(r), axis=0) / (np.max(np.sum(np.abs(a), axis=1)) * np.max(np.abs(x), axis=0)
+                                            + np.max(np.abs(b), axis=0))
+        assert np.max(berr) <= 1e-12, name
+        x2 = _solve_dense_system(a, b, None, name)
+        assert np.max(np.abs(x2 - x_ref)) <= 1e-10 * np.max(np.abs(x_ref))
+    # the 2x2 system of the reference's own hook test: rtol 2e-14
+    x, _ = _solve_dense_gpu(d['tiny_a'], d['tiny_b'][:, 0])
+    np.testing.assert_allclose(d['tiny_a'] @ x, d['tiny_b'][:, 0], rtol=2e-14, atol=2e-14)
+
+
+def test_mixed_solve_refines_to_fp64(ctx):
+    from grim_20261007_b200.execution import linear_precision
+    from grim_20261007_b200.twod.solver import _solve_dense_gpu
+    d = np.load(os.path.join(GOLDEN, 'ref_dense_system.npz'))
+    a, b, x_ref = d['cyl96_ka5_TM_a'], d['cyl96_ka5_TM_b'], d['cyl96_ka5_TM_x']
+    with linear_precision('mixed'):
+        x, _ = _solve_dense_gpu(a, b)
+    assert np.max(np.abs(x - x_ref)) <= 1e-9 * np.max(np.abs(x_ref))
+    rel = np.max(np.abs(a @ x - b), axis=0) / np.max(np.abs(b), axis=0)
+    assert np.max(rel) <= 2e-12
+
+
+def test_backward_error_kernel_matches_host(ctx):
+    from grim_20261007_b200 import _lib
+    from grim_20261007_b200.device import ptr
+    n, m = 150, 9
+    a = _rand(n, n, 1)
+    x = _rand(n, m, 2)
+    b = a @ x + 1e-9 * _rand(n, m, 3)
+    at, xt, bt = _dev(a), _dev(x), _dev(b)
+    berr = torch.empty(m, dtype=torch.float64, device='cuda')
+    _lib.check(ctx.lib.grim_backward_error(ctx.h, n, m, ptr(at), n, 0, ptr(xt), n, ptr(bt), n, ptr(berr)))
+    r = a @ x - b
+    ref = np.max(np.abs(r), axis=0) / (np.max(np.sum(np.abs(a), axis=1)) * np.max(np.abs(x), axis=0)
+                                       + np.max(np.abs(b), axis=0))
+    np.testing.assert_allclose(berr.cpu().numpy(), ref, rtol=1e-6)

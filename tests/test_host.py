@@ -1,0 +1,106 @@
+"""Host-side logic and the C ABI library, without a GPU."""
+import ctypes
+import math
+
+import numpy as np
+import pytest
+
+from grim_20261007_b200 import _lib, synthetic as S
+from grim_20261007_b200.twod import geometry as geo
+from oracle import pulse2d as P
+
+
+def test_library_loads_and_exports_every_declared_symbol():
+    lib = _lib.load()
+    declared = _lib.header_symbols()
+    assert len(declared) >= 20
+    for name in declared:
+        assert hasattr(lib, name), name
+    bound = {s[0] for s in _lib.SIGNATURES}
+    assert set(declared) <= bound | {'grim_noalloc_zgesv'} or set(declared) <= bound
+    assert lib.grim_version() >= 1
+
+
+def test_library_reports_errors_without_device():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip('a GPU is present')
+    lib = _lib.load()
+    h = ctypes.c_void_p()
+    status = lib.grim_create(0, ctypes.byref(h))
+    assert status != _lib.GRIM_OK
+    assert _lib.last_error()
+    assert lib.grim_fill2d(None, 0, 10, None, None, 1.0, None, 10, 0) == _lib.GRIM_ERR_ARGUMENT
+
+
+def test_snapshot_panel_rules():
+    v = S.circle(1.0, 12)
+    snap = S.snapshot_from_polygons([v])
+    polys = geo.contours_from_snapshot(snap, 'meters')
+    assert len(polys) == 1 and polys[0].shape == (12, 2)
+    np.testing.assert_allclose(polys[0], v, atol=1e-15)
+    # N = 3 panels per primitive
+    for seg in snap['segments']:
+        seg['properties'][1] = '3'
+    assert geo.contours_from_snapshot(snap, 'meters')[0].shape == (36, 2)
+    # N < 0: |N| panels per wavelength
+    for seg in snap['segments']:
+        seg['properties'][1] = '-10'
+    side = 2 * math.sin(math.pi / 12)
+    got = geo.contours_from_snapshot(snap, 'meters', wavelength=0.1)[0].shape[0]
+    assert got == 12 * math.ceil(side * 10 / 0.1)
+    # inches
+    for seg in snap['segments']:
+        seg['properties'][1] = '1'
+    np.testing.assert_allclose(geo.contours_from_snapshot(snap, 'inches')[0], v * 0.0254)
+
+
+def test_snapshot_rejects_out_of_scope_boundaries():
+    snap = S.snapshot_from_polygons([S.circle(1.0, 8)])
+    snap['segments'][0]['seg_type'] = 3
+    with pytest.raises(NotImplementedError):
+        geo.contours_from_snapshot(snap, 'meters')
+    snap = S.snapshot_from_polygons([S.circle(1.0, 8)])
+    snap['dielectrics'] = [['1', '4', '0', '1', '0']]
+    with pytest.raises(NotImplementedError):
+        geo.contours_from_snapshot(snap, 'meters')
+
+
+def test_panel_geometry_matches_oracle_and_normals_point_outward():
+    v = S.naca_symmetric(0.12, 64)
+    g = geo.panel_geometry([v])
+    c, t, h, n = P.panel_arrays([v])
+    np.testing.assert_array_equal(g[:, 0:2], c)
+    np.testing.assert_array_equal(g[:, 2:4], t)
+    np.testing.assert_array_equal(g[:, 4], h)
+    np.testing.assert_array_equal(g[:, 5:7], n)
+    # outward: centroid-to-midpoint has positive projection on the normal for a convex-ish body
+    cen = v.mean(axis=0)
+    assert np.mean(np.sum((c - cen) * n, axis=1) > 0) > 0.95
+    # counter-clockwise input gives the same outward normals
+    g2 = geo.panel_geometry([v[::-1]])
+    assert np.allclose(np.sort(g2[:, 5]), np.sort(g[:, 5]))
+    np.testing.assert_array_equal(geo.te_curvature_correction([v]), P.te_curvature_correction([v]))
+
+
+def test_te_curvature_correction_on_circle():
+    n = 50
+    corr = geo.te_curvature_correction([S.circle(2.0, n)])
+    side = 2 * 2.0 * math.sin(math.pi / n)
+    kappa = (2 * math.pi / n) / side
+    np.testing.assert_allclose(corr, kappa * side / (4 * math.pi), rtol=1e-12)
+
+
+def test_synthetic_workloads_are_seeded_and_clockwise():
+    v1, k1, f1, t1 = S.airfoil_case(7, 2048)
+    v2, k2, f2, t2 = S.airfoil_case(7, 2048)
+    np.testing.assert_array_equal(v1, v2)
+    assert 0.08 <= t1 <= 0.15 and v1.shape == (2048, 2)
+    b = np.roll(v1, -1, axis=0)
+    area = 0.5 * np.sum(v1[:, 0] * b[:, 1] - b[:, 0] * v1[:, 1])
+    assert area < 0
+    lam = 2 * math.pi / k1
+    assert abs(geo.perimeter([v1]) / 2048 - lam / 10) < 1e-12
+    gen, length, half = S.ogive_case(3)
+    assert gen[0, 0] == 0 and gen[-1, 0] == 0 and gen[0, 1] > gen[-1, 1]
+    assert 2 <= length <= 4 and 15 <= half <= 30
