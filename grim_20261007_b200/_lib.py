@@ -76,6 +76,8 @@ SIGNATURES = [
     ('grim_zgesv_batched', c_int, [c_void_p, c_int, c_int, c_void_p, c_int, c_void_p, c_int, c_int, P_int]),
     ('grim_last_solve_info', c_int, [c_void_p, ctypes.POINTER(GrimSolveInfo)]),
     ('grim_mem_info', c_int, [c_void_p, ctypes.POINTER(c_size_t), ctypes.POINTER(c_size_t)]),
+    ('grim_profile_enable', c_int, [c_void_p, c_int]),
+    ('grim_profile_report', c_int, [c_void_p, c_char_p, c_int]),
 ]
 
 _lib = None

@@ -54,6 +54,15 @@ template <typename C> __host__ __device__ __forceinline__ C cdiv(C a, C b) {
         return mk((ar * r + ai) / d, (ai * r - ar) / d);
     }
 }
+// 1 / b with the components scaled by max(|re|, |im|) first (no over/underflow of |b|^2)
+template <typename C> __host__ __device__ __forceinline__ C crecip(C b) {
+    using R = typename real_of<C>::type;
+    const R s = fmax(fabs(b.x), fabs(b.y));
+    const R rs = (R)1 / s;
+    const R br = b.x * rs, bi = b.y * rs;
+    const R d = (R)1 / (br * br + bi * bi);
+    return mk(br * d * rs, -bi * d * rs);
+}
 template <typename C> __host__ __device__ __forceinline__ typename real_of<C>::type cabs1(C a) {
     return fabs(a.x) + fabs(a.y);
 }
@@ -78,12 +87,16 @@ int grim_cuda_check(cudaError_t e, const char *what);
         if (_e != cudaSuccess) return grim_cuda_check(_e, #call);                 \
     } while (0)
 
-#define GRIM_CHECK_LAUNCH(h, what)                                                \
+// After every kernel launch: count it, check the launch, and (profiling on) record an
+// end event so that consecutive events on the stream bracket each kernel.
+#define GRIM_CHECK_LAUNCH_W(h, what, flops, bytes)                                \
     do {                                                                          \
         (h)->launches++;                                                          \
         cudaError_t _e = cudaGetLastError();                                      \
         if (_e != cudaSuccess) return grim_cuda_check(_e, what);                  \
+        if ((h)->profiling) grim_prof_mark((h), (what), (double)(flops), (double)(bytes)); \
     } while (0)
+#define GRIM_CHECK_LAUNCH(h, what) GRIM_CHECK_LAUNCH_W(h, what, 0.0, 0.0)
 
 #define GRIM_TRY(call)                                                            \
     do {                                                                          \
@@ -101,7 +114,18 @@ struct grim_context {
     std::unordered_map<std::string, std::pair<void *, size_t>> ws;
     grim_solve_info last{};
     int sm_count = 148;
+    // profiling: one event per launch (plus a start event), aggregated by kernel name
+    int profiling = 0;
+    cudaEvent_t prof_start = nullptr;
+    struct ProfMark {
+        std::string name;
+        cudaEvent_t ev;
+        double flops, bytes;
+    };
+    std::vector<ProfMark> marks;
 };
+
+void grim_prof_mark(grim_context *h, const char *name, double flops, double bytes);
 
 // Ensure a named workspace of at least `bytes` exists; returns its pointer in *out.
 int grim_workspace(grim_context *h, const char *name, size_t bytes, void **out);

@@ -14,6 +14,7 @@
 #include "fill2d.cuh"
 #include "hankel.cuh"
 #include "linalg.cuh"
+#include "lu.cuh"
 
 // ============================================================== errors
 static thread_local std::string g_last_error;
@@ -169,7 +170,8 @@ extern "C" int grim_destroy(grim_handle_t h) {
 
 extern "C" int grim_set_stream(grim_handle_t h, void *stream) {
     if (!h) return grim_fail(GRIM_ERR_ARGUMENT, "null handle");
-    h->stream = stream ? (cudaStream_t)stream : h->own_stream;
+    // NULL is CUDA's default (legacy) stream, which is where PyTorch runs by default.
+    h->stream = (cudaStream_t)stream;
     return GRIM_OK;
 }
 extern "C" void *grim_get_stream(grim_handle_t h) { return h ? (void *)h->stream : nullptr; }
@@ -258,9 +260,10 @@ template <typename ACC, typename TA, typename TB, typename TC, bool NEG, bool BE
 static int gemm(grim_context *h, int M, int N, int K, const TA *A, int64_t lda, const TB *B, int64_t ldb, TC *C,
                 int64_t ldc) {
     if (M <= 0 || N <= 0) return GRIM_OK;
-    dim3 grid(ceil_div(M, GEMM_BM), ceil_div(N, GEMM_BN));
-    k_gemm<ACC, TA, TB, TC, NEG, BETA><<<grid, GEMM_THREADS, 0, h->stream>>>(M, N, K, A, lda, B, ldb, C, ldc);
-    GRIM_CHECK_LAUNCH(h, "k_gemm");
+    dim3 grid(ceil_div(M, RT_BM), ceil_div(N, RT_BN));
+    k_gemm_rt<ACC, TA, TB, TC, NEG, BETA><<<grid, RT_THREADS, 0, h->stream>>>(M, N, K, A, lda, B, ldb, C, ldc);
+    GRIM_CHECK_LAUNCH_W(h, sizeof(ACC) == 16 ? "k_gemm_rt<f64>" : "k_gemm_rt<f32>", 8.0 * M * N * K,
+                        (double)sizeof(TA) * M * K + (double)sizeof(TB) * K * N + (BETA ? 2.0 : 1.0) * sizeof(TC) * M * N);
     return GRIM_OK;
 }
 
@@ -269,59 +272,60 @@ template <typename C>
 static int smem_opt_in() {
     static bool done = false;
     if (done) return GRIM_OK;
-    const int big = 3 * LU_NB * LU_NB * (int)sizeof(C);
-    GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_diag_lu<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_panel_fix<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_invert_blocks<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    const int strip = LU_NB * 32 * (int)sizeof(C);
-    GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_panel_l21<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, strip));
-    GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_row_update<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, strip));
-    GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_tri_apply<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, strip));
+    const int tri = (NB * NBP + NB) * (int)sizeof(C);
+    GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_panel_apply<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, tri));
+    GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_diag_lu<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, tri));
+    GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_trsm_diag<C, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, tri));
+    GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_trsm_diag<C, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, tri));
     done = true;
     return GRIM_OK;
 }
 
-// Device counters for one factorization: [0] info, [1] pivoted panels, [2..2+npan) cert, then swapped.
+static const char *kname(const char *base, size_t csize) {
+    // kernel names for profiling, distinguished by precision
+    static thread_local std::string s;
+    s = std::string(base) + (csize == 16 ? "<c128>" : "<c64>");
+    return s.c_str();
+}
+
+// Device flag layout for one factorization: [0] info, [1] pivoted panels, then per panel
+// cert[npan], swapped[npan], counter[npan].
 template <typename C>
 static int getrf_impl(grim_context *h, int n, C *A, int64_t lda, int *ipiv, int *info_host) {
     if (!h || n <= 0 || !A || lda < n || !ipiv) return grim_fail(GRIM_ERR_ARGUMENT, "getrf: bad arguments");
     DeviceGuard g(h->device);
     GRIM_TRY(smem_opt_in<C>());
-    const int nb = LU_NB;
-    const int npan = ceil_div(n, nb);
-    void *p_inv = nullptr, *p_backup = nullptr, *p_flags = nullptr;
-    GRIM_TRY(grim_workspace(h, "lu_inv", 2 * (size_t)LU_NB * LU_NB * sizeof(C), &p_inv));
-    GRIM_TRY(grim_workspace(h, "lu_backup", (size_t)n * nb * sizeof(C), &p_backup));
-    GRIM_TRY(grim_workspace(h, "lu_flags", (size_t)(2 + 2 * npan) * sizeof(int), &p_flags));
-    C *linv = (C *)p_inv, *uinv = linv + LU_NB * LU_NB, *backup = (C *)p_backup;
+    const int npan = ceil_div(n, NB);
+    void *p_bc = nullptr, *p_br = nullptr, *p_flags = nullptr;
+    GRIM_TRY(grim_workspace(h, "lu_backup_col", (size_t)n * NB * sizeof(C), &p_bc));
+    GRIM_TRY(grim_workspace(h, "lu_backup_row", (size_t)n * NB * sizeof(C), &p_br));
+    GRIM_TRY(grim_workspace(h, "lu_flags", (size_t)(2 + 3 * npan) * sizeof(int), &p_flags));
+    C *bcol = (C *)p_bc, *brow = (C *)p_br;
     int *flags = (int *)p_flags;
-    int *d_info = flags, *d_pivoted = flags + 1, *cert = flags + 2, *swapped = flags + 2 + npan;
-    GRIM_CHECK_CUDA(cudaMemsetAsync(flags, 0, (size_t)(2 + 2 * npan) * sizeof(int), h->stream));
-    const size_t big = 3 * (size_t)LU_NB * LU_NB * sizeof(C);
-    const size_t strip = (size_t)LU_NB * 32 * sizeof(C);
+    int *d_info = flags, *d_pivoted = flags + 1, *cert = flags + 2, *swapped = cert + npan, *counter = swapped + npan;
+    GRIM_CHECK_CUDA(cudaMemsetAsync(flags, 0, (size_t)(2 + 3 * npan) * sizeof(int), h->stream));
+    const size_t tri = (size_t)(NB * NBP + NB) * sizeof(C);
     for (int p = 0; p < npan; ++p) {
-        const int j = p * nb, nbj = std::min(nb, n - j);
-        k_diag_lu<C><<<1, 256, big, h->stream>>>(n, A, lda, j, nbj, linv, uinv, backup, cert + p, ipiv);
-        GRIM_CHECK_LAUNCH(h, "k_diag_lu");
-        const int below = n - j - nbj;
-        if (below > 0) {
-            k_panel_l21<C><<<ceil_div(below, 32), 256, strip, h->stream>>>(n, A, lda, j, nbj, uinv, backup, cert + p);
-            GRIM_CHECK_LAUNCH(h, "k_panel_l21");
-        }
-        k_panel_fix<C><<<1, 1024, big, h->stream>>>(n, A, lda, j, nbj, linv, uinv, backup, cert + p, swapped + p, ipiv,
-                                                   d_info, d_pivoted);
-        GRIM_CHECK_LAUNCH(h, "k_panel_fix");
-        const int right = n - j - nbj;
-        if (right > 0) {
-            k_row_update<C><<<ceil_div(right, 32), 256, strip, h->stream>>>(n, A, lda, j, nbj, linv, swapped + p, ipiv);
-            GRIM_CHECK_LAUNCH(h, "k_row_update");
-            GRIM_TRY((gemm<C, C, C, C, true, true>(h, below, right, nbj, A + (int64_t)j * lda + j + nbj, lda,
+        const int j = p * NB, nbj = std::min(NB, n - j);
+        k_diag_lu<C><<<1, 256, (size_t)NB * NBP * sizeof(C), h->stream>>>(n, A, lda, j, nbj, bcol, cert + p, ipiv);
+        GRIM_CHECK_LAUNCH_W(h, kname("k_diag_lu", sizeof(C)), 8.0 * nbj * nbj * nbj / 3.0, 0);
+        const int rest = n - j - nbj;
+        if (rest > 0) {
+            const int nL = ceil_div(rest, NB), nU = nL;
+            k_panel_apply<C><<<nL + nU, 256, tri, h->stream>>>(n, A, lda, j, nbj, nL, bcol, brow, cert + p,
+                                                               counter + p, swapped + p, ipiv, d_info, d_pivoted);
+            GRIM_CHECK_LAUNCH_W(h, kname("k_panel_apply", sizeof(C)), 8.0 * 2 * rest * nbj * nbj, 0);
+            GRIM_TRY((gemm<C, C, C, C, true, true>(h, rest, rest, nbj, A + (int64_t)j * lda + j + nbj, lda,
                                                   A + (int64_t)(j + nbj) * lda + j, lda,
                                                   A + (int64_t)(j + nbj) * lda + j + nbj, lda)));
+        } else {
+            k_panel_last<C><<<1, 256, 0, h->stream>>>(n, A, lda, j, nbj, bcol, cert + p, swapped + p, ipiv, d_info,
+                                                      d_pivoted);
+            GRIM_CHECK_LAUNCH(h, kname("k_panel_last", sizeof(C)));
         }
     }
-    k_laswp_left<C><<<ceil_div(n, 128), 128, 0, h->stream>>>(n, A, lda, nb, swapped, ipiv);
-    GRIM_CHECK_LAUNCH(h, "k_laswp_left");
+    k_laswp_left<C><<<ceil_div(n, 128), 128, 0, h->stream>>>(n, A, lda, NB, swapped, ipiv);
+    GRIM_CHECK_LAUNCH(h, kname("k_laswp_left", sizeof(C)));
     int hostf[2] = {0, 0};
     GRIM_CHECK_CUDA(cudaMemcpyAsync(hostf, flags, 2 * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
     GRIM_CHECK_CUDA(cudaStreamSynchronize(h->stream));
@@ -331,40 +335,56 @@ static int getrf_impl(grim_context *h, int n, C *A, int64_t lda, int *ipiv, int 
     return GRIM_OK;
 }
 
+// getrs: interchanges (skipped when ipiv is the identity), then per 64-row block an
+// in-place diagonal triangular solve and a GEMM update of the remaining rows.
 template <typename C>
-static int getrs_impl(grim_context *h, int n, int nrhs, const C *LU, int64_t lda, const int *ipiv, C *B, int64_t ldb) {
-    if (!h || n <= 0 || nrhs <= 0 || !LU || !ipiv || !B || lda < n || ldb < n)
-        return grim_fail(GRIM_ERR_ARGUMENT, "getrs: bad arguments");
-    DeviceGuard g(h->device);
-    GRIM_TRY(smem_opt_in<C>());
-    const int nb = LU_NB, npan = ceil_div(n, nb);
-    void *p_inv = nullptr;
-    GRIM_TRY(grim_workspace(h, sizeof(C) == 16 ? "rs_inv64" : "rs_inv32", 2 * (size_t)npan * LU_NB * LU_NB * sizeof(C), &p_inv));
-    C *linv = (C *)p_inv, *uinv = linv + (size_t)npan * LU_NB * LU_NB;
-    const size_t big = 3 * (size_t)LU_NB * LU_NB * sizeof(C);
-    const size_t strip = (size_t)LU_NB * 32 * sizeof(C);
-    k_invert_blocks<C><<<npan, 256, big, h->stream>>>(n, LU, lda, nb, linv, uinv);
-    GRIM_CHECK_LAUNCH(h, "k_invert_blocks");
-    k_laswp_rhs<C><<<ceil_div(nrhs, 128), 128, 0, h->stream>>>(n, nrhs, B, ldb, ipiv);
-    GRIM_CHECK_LAUNCH(h, "k_laswp_rhs");
-    const int ctiles = ceil_div(nrhs, 32);
+static int getrs_prepare(grim_context *h, int n, const int *ipiv, int **ident_out) {
+    void *p_id = nullptr;
+    GRIM_TRY(grim_workspace(h, sizeof(C) == 16 ? "rs_ident64" : "rs_ident32", sizeof(int), &p_id));
+    int *ident = (int *)p_id;
+    GRIM_CHECK_CUDA(cudaMemsetAsync(ident, 0xff, sizeof(int), h->stream));
+    k_ipiv_identity<<<ceil_div(n, 256), 256, 0, h->stream>>>(n, ipiv, ident);
+    GRIM_CHECK_LAUNCH(h, "k_ipiv_identity");
+    *ident_out = ident;
+    return GRIM_OK;
+}
+
+template <typename C>
+static int getrs_apply(grim_context *h, int n, int nrhs, const C *LU, int64_t lda, const int *ipiv, const int *ident,
+                       C *B, int64_t ldb) {
+    const int npan = ceil_div(n, NB);
+    const size_t tri = (size_t)(NB * NBP + NB) * sizeof(C);
+    k_laswp_rhs<C><<<ceil_div(nrhs, 128), 128, 0, h->stream>>>(n, nrhs, B, ldb, ipiv, ident);
+    GRIM_CHECK_LAUNCH(h, kname("k_laswp_rhs", sizeof(C)));
+    const int ctiles = ceil_div(nrhs, TRSM_COLS);
     for (int p = 0; p < npan; ++p) {
-        const int j = p * nb, nbj = std::min(nb, n - j);
-        k_tri_apply<C><<<ctiles, 256, strip, h->stream>>>(nrhs, B, ldb, j, nbj, linv + (size_t)p * LU_NB * LU_NB);
-        GRIM_CHECK_LAUNCH(h, "k_tri_apply");
+        const int j = p * NB, nbj = std::min(NB, n - j);
+        k_trsm_diag<C, false><<<ctiles, 4 * TRSM_COLS, tri, h->stream>>>(nrhs, LU, lda, B, ldb, j, nbj);
+        GRIM_CHECK_LAUNCH_W(h, kname("k_trsm_diag", sizeof(C)), 4.0 * nbj * nbj * nrhs, 0);
         const int below = n - j - nbj;
         if (below > 0)
             GRIM_TRY((gemm<C, C, C, C, true, true>(h, below, nrhs, nbj, LU + (int64_t)j * lda + j + nbj, lda, B + j, ldb,
                                                   B + j + nbj, ldb)));
     }
     for (int p = npan - 1; p >= 0; --p) {
-        const int j = p * nb, nbj = std::min(nb, n - j);
-        k_tri_apply<C><<<ctiles, 256, strip, h->stream>>>(nrhs, B, ldb, j, nbj, uinv + (size_t)p * LU_NB * LU_NB);
-        GRIM_CHECK_LAUNCH(h, "k_tri_apply");
+        const int j = p * NB, nbj = std::min(NB, n - j);
+        k_trsm_diag<C, true><<<ctiles, 4 * TRSM_COLS, tri, h->stream>>>(nrhs, LU, lda, B, ldb, j, nbj);
+        GRIM_CHECK_LAUNCH_W(h, kname("k_trsm_diag", sizeof(C)), 4.0 * nbj * nbj * nrhs, 0);
         if (j > 0)
             GRIM_TRY((gemm<C, C, C, C, true, true>(h, j, nrhs, nbj, LU + (int64_t)j * lda, lda, B + j, ldb, B, ldb)));
     }
     return GRIM_OK;
+}
+
+template <typename C>
+static int getrs_impl(grim_context *h, int n, int nrhs, const C *LU, int64_t lda, const int *ipiv, C *B, int64_t ldb) {
+    if (!h || n <= 0 || nrhs <= 0 || !LU || !ipiv || !B || lda < n || ldb < n)
+        return grim_fail(GRIM_ERR_ARGUMENT, "getrs: bad arguments");
+    DeviceGuard g(h->device);
+    GRIM_TRY(smem_opt_in<C>());
+    int *ident;
+    GRIM_TRY(getrs_prepare<C>(h, n, ipiv, &ident));
+    return getrs_apply<C>(h, n, nrhs, LU, lda, ipiv, ident, B, ldb);
 }
 
 extern "C" int grim_zgetrf(grim_handle_t h, int n, void *A, int64_t lda, int *ipiv, int *info) {
@@ -403,10 +423,14 @@ static int residual_and_berr(grim_context *h, int n, int nrhs, const TA *A, int6
 
 template <typename TA>
 static int inf_norm(grim_context *h, int n, const TA *A, int64_t lda, double *anorm_dev) {
-    void *p = nullptr;
+    void *p = nullptr, *pp = nullptr;
     GRIM_TRY(grim_workspace(h, "rowsum", (size_t)n * sizeof(double), &p));
-    k_row_abs_sum<TA><<<ceil_div(n, 128), 128, 0, h->stream>>>(n, A, lda, (double *)p);
-    GRIM_CHECK_LAUNCH(h, "k_row_abs_sum");
+    GRIM_TRY(grim_workspace(h, "rowsum_partial", (size_t)n * ROWSUM_CHUNKS * sizeof(double), &pp));
+    dim3 g(ceil_div(n, 128), ROWSUM_CHUNKS);
+    k_row_abs_partial<TA><<<g, 128, 0, h->stream>>>(n, A, lda, (double *)pp);
+    GRIM_CHECK_LAUNCH(h, "k_row_abs_partial");
+    k_row_abs_finish<<<ceil_div(n, 128), 128, 0, h->stream>>>(n, (const double *)pp, (double *)p);
+    GRIM_CHECK_LAUNCH(h, "k_row_abs_finish");
     k_max_reduce<<<1, 1024, 0, h->stream>>>(n, (const double *)p, anorm_dev);
     GRIM_CHECK_LAUNCH(h, "k_max_reduce");
     return GRIM_OK;
@@ -451,10 +475,13 @@ static int mixed_refine(grim_context *h, int n, int nrhs, const TA *Ares, int64_
                                       cudaMemcpyDeviceToDevice, h->stream));
     GRIM_TRY(inf_norm(h, n, Ares, ldres, sc));
     dim3 eg(ceil_div(n, 256), nrhs);
-    // x0 = solve32(b)
+    // x0 = solve32(b); the diagonal-block inverses are formed once for every solve
+    int *ident;
+    GRIM_TRY(smem_opt_in<float2>());
+    GRIM_TRY(getrs_prepare<float2>(h, n, ipiv, &ident));
     k_convert<float2, double2><<<eg, 256, 0, h->stream>>>(n, nrhs, B0, n, R32, n);
     GRIM_CHECK_LAUNCH(h, "k_convert");
-    GRIM_TRY(getrs_impl<float2>(h, n, nrhs, lu32, n, ipiv, R32, n));
+    GRIM_TRY(getrs_apply<float2>(h, n, nrhs, lu32, n, ipiv, ident, R32, n));
     k_convert<double2, float2><<<eg, 256, 0, h->stream>>>(n, nrhs, R32, n, X, n);
     GRIM_CHECK_LAUNCH(h, "k_convert");
     double prev = INFINITY;
@@ -481,7 +508,7 @@ static int mixed_refine(grim_context *h, int n, int nrhs, const TA *Ares, int64_
         prev = relres;
         k_convert<float2, double2><<<eg, 256, 0, h->stream>>>(n, nrhs, R, n, R32, n);
         GRIM_CHECK_LAUNCH(h, "k_convert");
-        GRIM_TRY(getrs_impl<float2>(h, n, nrhs, lu32, n, ipiv, R32, n));
+        GRIM_TRY(getrs_apply<float2>(h, n, nrhs, lu32, n, ipiv, ident, R32, n));
         k_add_update<float2><<<eg, 256, 0, h->stream>>>(n, nrhs, X, n, R32, n);
         GRIM_CHECK_LAUNCH(h, "k_add_update");
         ++steps;
@@ -587,5 +614,68 @@ extern "C" int grim_zgesv_batched(grim_handle_t h, int n, int nrhs, const double
     GRIM_CHECK_CUDA(cudaMemcpy2DAsync(B, (size_t)ldb * sizeof(double2), pb, n * sizeof(double2), n * sizeof(double2),
                                       nrhs, cudaMemcpyDeviceToHost, h->stream));
     GRIM_CHECK_CUDA(cudaStreamSynchronize(h->stream));
+    return GRIM_OK;
+}
+
+// ============================================================== profiling
+void grim_prof_mark(grim_context *h, const char *name, double flops, double bytes) {
+    cudaEvent_t e;
+    if (cudaEventCreate(&e) != cudaSuccess) return;
+    cudaEventRecord(e, h->stream);
+    h->marks.push_back({std::string(name), e, flops, bytes});
+}
+
+static void prof_clear(grim_context *h) {
+    for (auto &m : h->marks) cudaEventDestroy(m.ev);
+    h->marks.clear();
+    if (h->prof_start) {
+        cudaEventDestroy(h->prof_start);
+        h->prof_start = nullptr;
+    }
+}
+
+extern "C" int grim_profile_enable(grim_handle_t h, int enable) {
+    if (!h) return grim_fail(GRIM_ERR_ARGUMENT, "null handle");
+    DeviceGuard g(h->device);
+    prof_clear(h);
+    h->profiling = enable ? 1 : 0;
+    if (enable) {
+        GRIM_CHECK_CUDA(cudaEventCreate(&h->prof_start));
+        GRIM_CHECK_CUDA(cudaEventRecord(h->prof_start, h->stream));
+    }
+    return GRIM_OK;
+}
+
+// JSON object {"kernel": {"launches": n, "ms": total, "flops": f, "bytes": b}, ...}; each
+// kernel's time is the span from the previous event on the stream to its end event.
+extern "C" int grim_profile_report(grim_handle_t h, char *buf, int len) {
+    if (!h || !buf || len <= 0) return grim_fail(GRIM_ERR_ARGUMENT, "grim_profile_report: bad arguments");
+    DeviceGuard g(h->device);
+    GRIM_CHECK_CUDA(cudaStreamSynchronize(h->stream));
+    struct Agg { int n = 0; double ms = 0, flops = 0, bytes = 0; };
+    std::vector<std::pair<std::string, Agg>> agg;
+    cudaEvent_t prev = h->prof_start;
+    for (auto &m : h->marks) {
+        float ms = 0.f;
+        if (prev) cudaEventElapsedTime(&ms, prev, m.ev);
+        prev = m.ev;
+        auto it = std::find_if(agg.begin(), agg.end(), [&](const std::pair<std::string, Agg> &p) { return p.first == m.name; });
+        if (it == agg.end()) { agg.push_back({m.name, Agg()}); it = agg.end() - 1; }
+        it->second.n++;
+        it->second.ms += ms;
+        it->second.flops += m.flops;
+        it->second.bytes += m.bytes;
+    }
+    std::string out = "{";
+    for (size_t i = 0; i < agg.size(); ++i) {
+        char tmp[256];
+        std::snprintf(tmp, sizeof(tmp), "%s\"%s\": {\"launches\": %d, \"ms\": %.6f, \"flops\": %.6e, \"bytes\": %.6e}",
+                      i ? ", " : "", agg[i].first.c_str(), agg[i].second.n, agg[i].second.ms, agg[i].second.flops,
+                      agg[i].second.bytes);
+        out += tmp;
+    }
+    out += "}";
+    if ((int)out.size() + 1 > len) return grim_fail(GRIM_ERR_ARGUMENT, "grim_profile_report: buffer too small");
+    std::memcpy(buf, out.c_str(), out.size() + 1);
     return GRIM_OK;
 }

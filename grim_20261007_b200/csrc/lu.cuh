@@ -1,0 +1,596 @@
+// Dense complex LU (getrf) and multi-RHS triangular solves (getrs) on column-major
+// complex128 / complex64 matrices, SIMT kernels.
+//
+// Factorization (right-looking, block width NB = 64), three launches per panel j:
+//   k_diag_lu     one CTA: unpivoted LU of the NB x NB diagonal block in shared memory,
+//                 the diagonal-pivot certificate inside it, and inv(L11), inv(U11) by a
+//                 blocked recursive inversion (8 x 8 leaves per warp, then 16, 32, 64);
+//   k_panel_apply one CTA per 64-row strip of A21 (L21 = A21 inv(U11), certificate
+//                 |l_ic u_cc|_1 <= |u_cc|_1) and per 64-column strip of A12
+//                 (U12 = inv(L11) A12), both with backups; the last CTA to finish
+//                 refactors the panel with partial pivoting if any certificate failed;
+//   k_gemm_rt     A22 -= L21 U12.
+// Partial pivoting picks the diagonal at step c exactly when |a_ic^(c)|_1 <= |a_cc^(c)|_1
+// for every i > c (LAPACK izamax: |re|+|im|, first index on ties), and a_ic^(c) = l_ic u_cc,
+// so a passing certificate proves the unpivoted factors equal getrf's
+// (reference linalg/dense.py:114-155 via scipy.linalg.lu_factor).
+#pragma once
+#include "common.cuh"
+
+#define NB 64
+#define RT_BM 64
+#define RT_BN 128
+#define RT_BK 8
+#define RT_THREADS 256
+
+// ------------------------------------------------------------------ register-tiled GEMM
+// C[MxN] = (BETA ? C : 0) + (NEG ? -1 : 1) * A[MxK] * B[KxN], column-major, ACC arithmetic.
+// 64 x 128 CTA tile, 256 threads each owning 4 x 8 outputs, two shared-memory stages
+// filled through registers.
+template <typename ACC, typename TA, typename TB, typename TC, bool NEG, bool BETA>
+__global__ void __launch_bounds__(RT_THREADS)
+k_gemm_rt(int M, int N, int K, const TA *__restrict__ A, int64_t lda, const TB *__restrict__ B, int64_t ldb,
+          TC *__restrict__ C, int64_t ldc) {
+    using R = typename real_of<ACC>::type;
+    __shared__ ACC As[2][RT_BK][RT_BM];
+    __shared__ ACC Bs[2][RT_BK][RT_BN];
+    const int t = threadIdx.x;
+    const int tx = t & 15, ty = t >> 4;
+    const int m0 = blockIdx.x * RT_BM, n0 = blockIdx.y * RT_BN;
+    ACC acc[4][8];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[i][j] = czero<ACC>();
+    ACC ra[2], rb[4];
+    auto load = [&](int k0) {
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+            const int e = t + RT_THREADS * i;
+            const int r = e & 63, c = e >> 6;
+            const int gm = m0 + r, gk = k0 + c;
+            ACC v = czero<ACC>();
+            if (gm < M && gk < K) {
+                const TA x = A[(int64_t)gk * lda + gm];
+                v = mk((R)x.x, (R)x.y);
+            }
+            ra[i] = v;
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int e = t + RT_THREADS * i;
+            const int r = e & 7, c = e >> 3;
+            const int gk = k0 + r, gn = n0 + c;
+            ACC v = czero<ACC>();
+            if (gk < K && gn < N) {
+                const TB x = B[(int64_t)gn * ldb + gk];
+                v = mk((R)x.x, (R)x.y);
+            }
+            rb[i] = v;
+        }
+    };
+    auto store = [&](int s) {
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+            const int e = t + RT_THREADS * i;
+            As[s][e >> 6][e & 63] = ra[i];
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int e = t + RT_THREADS * i;
+            Bs[s][e & 7][e >> 3] = rb[i];
+        }
+    };
+    const int nk = (K + RT_BK - 1) / RT_BK;
+    load(0);
+    store(0);
+    __syncthreads();
+    for (int kt = 0; kt < nk; ++kt) {
+        const int cur = kt & 1;
+        if (kt + 1 < nk) load((kt + 1) * RT_BK);
+#pragma unroll
+        for (int kk = 0; kk < RT_BK; ++kk) {
+            ACC a[4], b[8];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) a[i] = As[cur][kk][tx + 16 * i];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) b[j] = Bs[cur][kk][ty + 16 * j];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 8; ++j) cfma(acc[i][j], a[i], b[j]);
+        }
+        if (kt + 1 < nk) store(cur ^ 1);
+        __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int gm = m0 + tx + 16 * i;
+        if (gm >= M) continue;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const int gn = n0 + ty + 16 * j;
+            if (gn >= N) continue;
+            TC *p = C + (int64_t)gn * ldc + gm;
+            ACC v = acc[i][j];
+            if (NEG) v = mk(-v.x, -v.y);
+            if (BETA) {
+                const TC o = *p;
+                v.x += (R)o.x;
+                v.y += (R)o.y;
+            }
+            TC w;
+            w.x = (decltype(w.x))v.x;
+            w.y = (decltype(w.y))v.y;
+            *p = w;
+        }
+    }
+}
+
+// ------------------------------------------------------------------ small-block helpers
+template <typename C>
+__device__ __forceinline__ C one_c() {
+    return mk((typename real_of<C>::type)1, (typename real_of<C>::type)0);
+}
+
+// Padded leading dimension of 64 x 64 triangular blocks in shared memory: row r, column c
+// at [c * NBP + r]; the odd padding keeps the four sub-lanes of a substitution on
+// distinct banks.
+#define NBP 65
+
+template <typename C>
+__device__ __forceinline__ C shfl_xor_c(C v, int m) {
+    v.x = __shfl_xor_sync(0xffffffffu, v.x, m);
+    v.y = __shfl_xor_sync(0xffffffffu, v.y, m);
+    return v;
+}
+template <typename C>
+__device__ __forceinline__ C shfl_c(C v, int src) {
+    v.x = __shfl_sync(0xffffffffu, v.x, src);
+    v.y = __shfl_sync(0xffffffffu, v.y, src);
+    return v;
+}
+template <typename C>
+__device__ __forceinline__ C reduce4(C v) {
+    C o = shfl_xor_c(v, 1);
+    v.x += o.x;
+    v.y += o.y;
+    o = shfl_xor_c(v, 2);
+    v.x += o.x;
+    v.y += o.y;
+    return v;
+}
+
+// Substitutions on one 64-long vector, shared by 4 consecutive lanes (sub-lane s owns
+// the entries p = 4 i + s, i < 16, in registers v[i]).  T is a 64 x 64 block in smem
+// (leading dim NBP), rd[c] = 1 / T(c, c).  Fully unrolled so v[] stays in registers.
+//
+// row_upper:   x T = a  (x a row vector, T upper)      x_c = (a_c - sum_{p<c} x_p T_pc) rd_c
+// col_lower1:  T x = a  (T unit lower)                 x_r = a_r - sum_{p<r} T_rp x_p
+// col_upper:   T x = a  (T upper)                      x_r = (a_r - sum_{p>r} T_rp x_p) rd_r
+template <typename C>
+__device__ __forceinline__ void subst_row_upper(C (&v)[16], const C *T, const C *rd, int nbj, int s) {
+#pragma unroll
+    for (int c = 0; c < NB; ++c) {
+        if (c < nbj) {
+            C part = czero<C>();
+#pragma unroll
+            for (int i = 0; i < 16; ++i)
+                if (4 * i + s < c) cfma(part, v[i], T[c * NBP + 4 * i + s]);
+            part = reduce4(part);
+            if (s == (c & 3)) v[c >> 2] = cmul(csub(v[c >> 2], part), rd[c]);
+        }
+    }
+}
+template <typename C>
+__device__ __forceinline__ void subst_col_lower1(C (&v)[16], const C *T, int nbj, int s) {
+#pragma unroll
+    for (int r = 0; r < NB; ++r) {
+        if (r < nbj) {
+            C part = czero<C>();
+#pragma unroll
+            for (int i = 0; i < 16; ++i)
+                if (4 * i + s < r) cfma(part, T[(4 * i + s) * NBP + r], v[i]);
+            part = reduce4(part);
+            if (s == (r & 3)) v[r >> 2] = csub(v[r >> 2], part);
+        }
+    }
+}
+template <typename C>
+__device__ __forceinline__ void subst_col_upper(C (&v)[16], const C *T, const C *rd, int nbj, int s) {
+#pragma unroll
+    for (int r = NB - 1; r >= 0; --r) {
+        if (r < nbj) {
+            C part = czero<C>();
+#pragma unroll
+            for (int i = 0; i < 16; ++i)
+                if (4 * i + s > r && 4 * i + s < nbj) cfma(part, T[(4 * i + s) * NBP + r], v[i]);
+            part = reduce4(part);
+            if (s == (r & 3)) v[r >> 2] = cmul(csub(v[r >> 2], part), rd[r]);
+        }
+    }
+}
+
+// Stage the nbj x nbj diagonal block at (j, j) into smem T (padded, zero outside) and
+// the reciprocals of its diagonal into rd (1 outside).
+template <typename C>
+__device__ __forceinline__ void stage_diag(const C *A, int64_t lda, int j, int nbj, C *T, C *rd) {
+    for (int e = threadIdx.x; e < NB * NB; e += blockDim.x) {
+        const int r = e & 63, c = e >> 6;
+        T[c * NBP + r] = (r < nbj && c < nbj) ? A[(int64_t)(j + c) * lda + j + r] : czero<C>();
+    }
+    __syncthreads();
+    for (int r = threadIdx.x; r < NB; r += blockDim.x) rd[r] = r < nbj ? crecip(T[r * NBP + r]) : one_c<C>();
+    __syncthreads();
+}
+
+// ------------------------------------------------------------------ diagonal block
+// Warp-synchronous unpivoted LU of a 32 x 32 block held one row per lane (lane r owns
+// row r in v[0..31]): per column the pivot and then each pivot-row entry are broadcast
+// with shuffles.  Certificate: |a_rk^(k)|_1 <= |a_kk^(k)|_1 for rows r > k < m.
+template <typename C>
+__device__ __forceinline__ void warp_lu32(C (&v)[32], int m, int &bad) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int kk = 0; kk < 32; ++kk) {
+        if (kk < m) {
+            const C piv = shfl_c(v[kk], kk);
+            const auto pa = cabs1(piv);
+            const bool below = lane > kk && lane < m;
+            if (below && !(cabs1(v[kk]) <= pa)) bad = 1;
+            if (pa == 0) bad = 1;
+            const C rp = pa != 0 ? crecip(piv) : czero<C>();
+            if (below) v[kk] = cmul(v[kk], rp);
+#pragma unroll
+            for (int c = kk + 1; c < 32; ++c) {
+                const C u = shfl_c(v[c], kk);
+                if (below) cfms(v[c], v[kk], u);
+            }
+        }
+    }
+}
+
+// One CTA of 256 threads: unpivoted LU of the nbj x nbj diagonal block (nbj <= 64) as
+// LU(A11) [warp 0] -> U12 = inv(L11) A12 and L21 = A21 inv(U11) [warps 0-1, one lane per
+// column / row] -> A22 -= L21 U12 [all threads] -> LU(A22) [warp 0]; certificate over
+// the whole block, backup of the block, identity ipiv entries.
+template <typename C>
+__global__ void __launch_bounds__(256)
+k_diag_lu(int n, C *A, int64_t lda, int j, int nbj, C *backup_col, int *cert, int *ipiv) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C *S = reinterpret_cast<C *>(smem_raw);  // NB x NB block, leading dim NBP (dynamic smem)
+    __shared__ int s_bad;
+    const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+    if (t == 0) s_bad = 0;
+    for (int e = t; e < NB * NB; e += 256) {
+        const int r = e & 63, c = e >> 6;
+        C x = czero<C>();
+        if (r < nbj && c < nbj) {
+            x = A[(int64_t)(j + c) * lda + j + r];
+            backup_col[(int64_t)c * n + r] = x;
+        }
+        S[c * NBP + r] = x;
+    }
+    for (int r = t; r < nbj; r += 256) ipiv[j + r] = j + r + 1;
+    __syncthreads();
+    const int m1 = min(32, nbj), m2 = nbj - m1;
+    int bad = 0;
+    C v[32];
+    // LU(A11)
+    if (warp == 0) {
+#pragma unroll
+        for (int c = 0; c < 32; ++c) v[c] = S[c * NBP + lane];
+        warp_lu32(v, m1, bad);
+#pragma unroll
+        for (int c = 0; c < 32; ++c) S[c * NBP + lane] = v[c];
+    }
+    __syncthreads();
+    if (m2 > 0) {
+        // warp 0: column lane of A12 -> U12 (unit lower L11);  warp 1: row lane of A21 -> L21
+        if (warp == 0) {
+            const int col = 32 + lane;
+#pragma unroll
+            for (int r = 0; r < 32; ++r) v[r] = S[col * NBP + r];
+#pragma unroll
+            for (int r = 0; r < 32; ++r)
+#pragma unroll
+                for (int p = 0; p < r; ++p) cfms(v[r], S[p * NBP + r], v[p]);
+#pragma unroll
+            for (int r = 0; r < 32; ++r) S[col * NBP + r] = v[r];
+        } else if (warp == 1) {
+            const int row = 32 + lane;
+#pragma unroll
+            for (int c = 0; c < 32; ++c) v[c] = S[c * NBP + row];
+#pragma unroll
+            for (int c = 0; c < 32; ++c) {
+#pragma unroll
+                for (int p = 0; p < c; ++p) cfms(v[c], v[p], S[c * NBP + p]);
+                const C ucc = S[c * NBP + c];
+                v[c] = cmul(v[c], crecip(ucc));
+                if (row < nbj && !(cabs1(cmul(v[c], ucc)) <= cabs1(ucc))) bad = 1;
+            }
+#pragma unroll
+            for (int c = 0; c < 32; ++c) S[c * NBP + row] = v[c];
+        }
+        __syncthreads();
+        // A22 -= L21 U12: thread owns 4 entries (row 32 + (t & 31), columns 32 + (t >> 5) + 8 q)
+        {
+            const int r = 32 + (t & 31);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int c = 32 + (t >> 5) + 8 * q;
+                C acc = S[c * NBP + r];
+#pragma unroll 8
+                for (int p = 0; p < 32; ++p) cfms(acc, S[p * NBP + r], S[c * NBP + p]);
+                S[c * NBP + r] = acc;
+            }
+        }
+        __syncthreads();
+        // LU(A22)
+        if (warp == 0) {
+#pragma unroll
+            for (int c = 0; c < 32; ++c) v[c] = S[(32 + c) * NBP + 32 + lane];
+            warp_lu32(v, m2, bad);
+#pragma unroll
+            for (int c = 0; c < 32; ++c) S[(32 + c) * NBP + 32 + lane] = v[c];
+        }
+    }
+    if (bad) s_bad = 1;
+    __syncthreads();
+    for (int e = t; e < NB * NB; e += 256) {
+        const int r = e & 63, c = e >> 6;
+        if (r < nbj && c < nbj) A[(int64_t)(j + c) * lda + j + r] = S[c * NBP + r];
+    }
+    if (t == 0 && s_bad) atomicOr(cert, 1);
+}
+
+// ------------------------------------------------------------------ pivoted panel (fallback)
+// Executed by one CTA (256 threads) after restoring the panel: LAPACK getf2 on the
+// (n - j) x nbj panel in global memory, then row interchanges and U12 = inv(L11) A12
+// (forward substitution) on every trailing column.
+template <typename C>
+__device__ void pivoted_panel(int n, C *A, int64_t lda, int j, int nbj, int *ipiv, int *info, int *swapped) {
+    using R = typename real_of<C>::type;
+    __shared__ R wv[8];
+    __shared__ int wi[8];
+    __shared__ int s_piv, s_any;
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    if (t == 0) s_any = 0;
+    __syncthreads();
+    for (int kk = 0; kk < nbj; ++kk) {
+        const int col = j + kk;
+        R best = (R)-1;
+        int bi = 0x7fffffff;
+        for (int r = col + t; r < n; r += 256) {
+            const R v = cabs1(A[(int64_t)col * lda + r]);
+            if (v > best || (v == best && r < bi)) { best = v; bi = r; }
+        }
+        for (int off = 16; off > 0; off >>= 1) {
+            const R ov = __shfl_down_sync(0xffffffffu, best, off);
+            const int oi = __shfl_down_sync(0xffffffffu, bi, off);
+            if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
+        }
+        if (lane == 0) { wv[warp] = best; wi[warp] = bi; }
+        __syncthreads();
+        if (t == 0) {
+            best = wv[0];
+            bi = wi[0];
+            for (int w = 1; w < 8; ++w)
+                if (wv[w] > best || (wv[w] == best && wi[w] < bi)) { best = wv[w]; bi = wi[w]; }
+            s_piv = bi;
+            ipiv[col] = bi + 1;
+            if (bi != col) s_any = 1;
+        }
+        __syncthreads();
+        const int p = s_piv;
+        const C pv = A[(int64_t)col * lda + p];
+        const bool zero = (pv.x == 0 && pv.y == 0);
+        if (zero) {
+            if (t == 0 && *info == 0) *info = col + 1;
+        } else if (p != col) {
+            for (int c = t; c < n; c += 256) {  // whole rows from column j on
+                if (c < j) continue;
+                C *a = A + (int64_t)c * lda;
+                const C x = a[col];
+                a[col] = a[p];
+                a[p] = x;
+            }
+        }
+        __syncthreads();
+        if (!zero) {
+            const C d = A[(int64_t)col * lda + col];
+            for (int r = col + 1 + t; r < n; r += 256) A[(int64_t)col * lda + r] = cdiv(A[(int64_t)col * lda + r], d);
+        }
+        __syncthreads();
+        for (int r = col + 1 + t; r < n; r += 256) {
+            const C l = A[(int64_t)col * lda + r];
+            for (int c = kk + 1; c < nbj; ++c) cfms(A[(int64_t)(j + c) * lda + r], l, A[(int64_t)(j + c) * lda + col]);
+        }
+        __syncthreads();
+    }
+    // U12 = inv(L11) A12 by forward substitution, one thread per trailing column
+    for (int c = j + nbj + t; c < n; c += 256) {
+        C *a = A + (int64_t)c * lda;
+        for (int i = 1; i < nbj; ++i) {
+            C acc = a[j + i];
+            for (int p = 0; p < i; ++p) cfms(acc, A[(int64_t)(j + p) * lda + j + i], a[j + p]);
+            a[j + i] = acc;
+        }
+    }
+    if (t == 0) *swapped = s_any;
+}
+
+
+// ------------------------------------------------------------------ panel apply
+// grid.x = nL + nU CTAs of 256 threads.  CTA b < nL: 64 rows of A21 (4 lanes per row),
+// L21 = A21 inv(U11) by row substitution, certificate |l_ic u_cc|_1 <= |u_cc|_1.
+// CTA b >= nL: 64 columns of A12, U12 = inv(L11) A12 by column substitution.
+// Both back up what they overwrite; the last CTA to finish runs the pivoted
+// refactorization when any certificate failed.  Dynamic smem: NB * NBP + NB elements.
+template <typename C>
+__global__ void __launch_bounds__(256)
+k_panel_apply(int n, C *A, int64_t lda, int j, int nbj, int nL, C *backup_col, C *backup_row, int *cert,
+              int *counter, int *swapped, int *ipiv, int *info, int *pivoted) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C *T = reinterpret_cast<C *>(smem_raw);
+    C *rd = T + NB * NBP;
+    const int t = threadIdx.x, s = t & 3, lane_vec = t >> 2;
+    const int b = blockIdx.x;
+    const bool is_l = b < nL;
+    stage_diag(A, lda, j, nbj, T, rd);
+    C v[16];
+    int bad = 0;
+    if (is_l) {
+        const int row = j + nbj + NB * b + lane_vec;
+        const bool ok = row < n;
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+            const int c = 4 * i + s;
+            C x = czero<C>();
+            if (ok && c < nbj) {
+                x = A[(int64_t)(j + c) * lda + row];
+                backup_col[(int64_t)c * n + (row - j)] = x;
+            }
+            v[i] = x;
+        }
+        subst_row_upper(v, T, rd, nbj, s);
+        if (ok) {
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+                const int c = 4 * i + s;
+                if (c < nbj) {
+                    const C ucc = T[c * NBP + c];
+                    if (!(cabs1(cmul(v[i], ucc)) <= cabs1(ucc))) bad = 1;
+                    A[(int64_t)(j + c) * lda + row] = v[i];
+                }
+            }
+        }
+    } else {
+        const int col = j + nbj + NB * (b - nL) + lane_vec;
+        const bool ok = col < n;
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+            const int r = 4 * i + s;
+            C x = czero<C>();
+            if (ok && r < nbj) {
+                x = A[(int64_t)col * lda + j + r];
+                backup_row[(int64_t)(col - j - nbj) * NB + r] = x;
+            }
+            v[i] = x;
+        }
+        subst_col_lower1(v, T, nbj, s);
+        if (ok) {
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+                const int r = 4 * i + s;
+                if (r < nbj) A[(int64_t)col * lda + j + r] = v[i];
+            }
+        }
+    }
+    if (__syncthreads_or(bad) && t == 0) atomicOr(cert, 1);
+    // last CTA: pivoted fallback if any certificate failed
+    __shared__ int s_last;
+    __threadfence();
+    __syncthreads();
+    if (t == 0) s_last = (atomicAdd(counter, 1) == (int)gridDim.x - 1);
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    if (atomicAdd(cert, 0) == 0) return;
+    for (int c = 0; c < nbj; ++c)
+        for (int r = t; r < n - j; r += 256) A[(int64_t)(j + c) * lda + j + r] = backup_col[(int64_t)c * n + r];
+    for (int c = j + nbj; c < n; ++c)
+        for (int r = t; r < nbj; r += 256) A[(int64_t)c * lda + j + r] = backup_row[(int64_t)(c - j - nbj) * NB + r];
+    __syncthreads();
+    pivoted_panel(n, A, lda, j, nbj, ipiv, info, swapped);
+    if (t == 0) atomicAdd(pivoted, 1);
+}
+
+// Single-CTA fallback driver when there is no trailing strip (last panel).
+template <typename C>
+__global__ void __launch_bounds__(256)
+k_panel_last(int n, C *A, int64_t lda, int j, int nbj, C *backup_col, int *cert, int *swapped, int *ipiv, int *info,
+             int *pivoted) {
+    if (*cert == 0) return;
+    for (int c = 0; c < nbj; ++c)
+        for (int r = threadIdx.x; r < n - j; r += 256) A[(int64_t)(j + c) * lda + j + r] = backup_col[(int64_t)c * n + r];
+    __syncthreads();
+    pivoted_panel(n, A, lda, j, nbj, ipiv, info, swapped);
+    if (threadIdx.x == 0) atomicAdd(pivoted, 1);
+}
+
+// Apply interchanges of later panels to the columns left of them.
+template <typename C>
+__global__ void k_laswp_left(int n, C *A, int64_t lda, int nb, const int *swapped, const int *ipiv) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    const int npan = (n + nb - 1) / nb;
+    C *a = A + (int64_t)c * lda;
+    for (int pnl = 0; pnl < npan; ++pnl) {
+        const int j = pnl * nb;
+        if (!swapped[pnl] || c >= j) continue;
+        const int nbj = min(nb, n - j);
+        for (int kk = 0; kk < nbj; ++kk) {
+            const int p = ipiv[j + kk] - 1;
+            if (p != j + kk) {
+                const C x = a[j + kk];
+                a[j + kk] = a[p];
+                a[p] = x;
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------------ getrs
+// ident[0] = 1 when ipiv is the identity permutation (cleared by any entry that is not).
+__global__ void k_ipiv_identity(int n, const int *ipiv, int *ident) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n && ipiv[i] != i + 1) atomicAnd(ident, 0);
+}
+
+template <typename C>
+__global__ void k_laswp_rhs(int n, int nrhs, C *B, int64_t ldb, const int *ipiv, const int *ident) {
+    if (*ident) return;
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nrhs) return;
+    C *b = B + (int64_t)c * ldb;
+    for (int i = 0; i < n; ++i) {
+        const int p = ipiv[i] - 1;
+        if (p != i) {
+            const C x = b[i];
+            b[i] = b[p];
+            b[p] = x;
+        }
+    }
+}
+
+// In-place triangular solve of the nbj-row strip of B at row j with the diagonal block of
+// LU at (j, j): UPPER = false -> unit lower L, true -> upper U.  4 lanes per column,
+// TRSM_COLS columns per CTA.  Dynamic smem: NB * NBP + NB elements.
+#define TRSM_COLS 16
+template <typename C, bool UPPER>
+__global__ void __launch_bounds__(4 * TRSM_COLS)
+k_trsm_diag(int nrhs, const C *__restrict__ LU, int64_t lda, C *B, int64_t ldb, int j, int nbj) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C *T = reinterpret_cast<C *>(smem_raw);
+    C *rd = T + NB * NBP;
+    const int t = threadIdx.x, s = t & 3;
+    stage_diag(LU, lda, j, nbj, T, rd);
+    const int col = blockIdx.x * TRSM_COLS + (t >> 2);
+    const bool ok = col < nrhs;
+    C v[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+        const int r = 4 * i + s;
+        v[i] = (ok && r < nbj) ? B[(int64_t)col * ldb + j + r] : czero<C>();
+    }
+    if (UPPER) subst_col_upper(v, T, rd, nbj, s);
+    else subst_col_lower1(v, T, nbj, s);
+    if (ok) {
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+            const int r = 4 * i + s;
+            if (r < nbj) B[(int64_t)col * ldb + j + r] = v[i];
+        }
+    }
+}

@@ -66,7 +66,8 @@ typedef struct grim_solve_info {
 /* ---- context ------------------------------------------------------------------ */
 int grim_create(int device, grim_handle_t *out);
 int grim_destroy(grim_handle_t h);
-/* Use a caller stream (cudaStream_t passed as void*); NULL restores the handle's own stream. */
+/* Run on a caller stream (cudaStream_t passed as void*; NULL = the CUDA default stream).
+ * A new handle runs on its own non-blocking stream until this is called. */
 int grim_set_stream(grim_handle_t h, void *stream);
 void *grim_get_stream(grim_handle_t h);
 int grim_synchronize(grim_handle_t h);
@@ -130,6 +131,12 @@ int grim_zgesv_mixed(grim_handle_t h, int n, int nrhs, const void *A, int64_t ld
 int grim_zgesv_batched(grim_handle_t h, int n, int nrhs, const double *A, int lda, double *B, int ldb,
                        int precision_mode, int *info);
 int grim_last_solve_info(grim_handle_t h, grim_solve_info *out);
+
+/* Per-kernel profiling: while enabled, every launch records a CUDA event on the handle
+ * stream; the report is JSON {"kernel": {"launches", "ms", "flops", "bytes"}} where a
+ * kernel's time is the span from the previous event to its own (gaps included). */
+int grim_profile_enable(grim_handle_t h, int enable);
+int grim_profile_report(grim_handle_t h, char *buf, int len);
 
 /* Free / total device memory in bytes (admission control). */
 int grim_mem_info(grim_handle_t h, size_t *free_bytes, size_t *total_bytes);
