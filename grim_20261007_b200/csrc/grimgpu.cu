@@ -15,6 +15,7 @@
 #include "hankel.cuh"
 #include "linalg.cuh"
 #include "lu.cuh"
+#include "bor.cuh"
 
 // ============================================================== errors
 static thread_local std::string g_last_error;
@@ -677,5 +678,65 @@ extern "C" int grim_profile_report(grim_handle_t h, char *buf, int len) {
     out += "}";
     if ((int)out.size() + 1 > len) return grim_fail(GRIM_ERR_ARGUMENT, "grim_profile_report: buffer too small");
     std::memcpy(buf, out.c_str(), out.size() + 1);
+    return GRIM_OK;
+}
+
+// ============================================================== body of revolution
+extern "C" int64_t grim_bor_moments_size(int ne, int mmax) {
+    return (int64_t)ne * ne * (mmax + 2) * BOR_SLOTS * (int64_t)sizeof(double2);
+}
+
+static size_t bor_smem(int nxi_max) { return (size_t)nxi_max * (sizeof(double2) + sizeof(double)) + BOR_MAX_MODES * sizeof(double2); }
+
+extern "C" int grim_bor_moments(grim_handle_t h, int ne, const double *nodes, double k, int mmax, int nxi_max,
+                                void *mom) {
+    if (!h || ne < 2 || !nodes || !mom || !(k > 0) || mmax < 0 || mmax + 2 > BOR_MAX_MODES || nxi_max < 32 ||
+        nxi_max > BOR_MAX_NXI || ne > 65535)
+        return grim_fail(GRIM_ERR_ARGUMENT, "grim_bor_moments: bad arguments");
+    DeviceGuard g(h->device);
+    const size_t smem = bor_smem(std::max(nxi_max, BOR_NEAR_XI));
+    GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_bor_moments, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    // the kernel clamps per-pair sample counts to BOR_MAX_NXI; the caller's nxi_max bounds them here
+    dim3 grid(ne, ne);
+    k_bor_moments<<<grid, 128, smem, h->stream>>>(ne, nodes, k, mmax, std::max(nxi_max, BOR_NEAR_XI), (double2 *)mom);
+    GRIM_CHECK_LAUNCH(h, "k_bor_moments");
+    return GRIM_OK;
+}
+
+extern "C" int grim_bor_assemble(grim_handle_t h, int ne, const double *nodes, double k, int mmax, int m,
+                                 const void *mom, int nred, const int *red_full, const void *red_w, void *Z,
+                                 int64_t ldz) {
+    if (!h || ne < 2 || !nodes || !mom || !red_full || !red_w || !Z || nred <= 0 || ldz < nred || abs(m) > mmax)
+        return grim_fail(GRIM_ERR_ARGUMENT, "grim_bor_assemble: bad arguments");
+    DeviceGuard g(h->device);
+    dim3 grid(ceil_div(nred, 16), ceil_div(nred, 16)), block(16, 16);
+    k_bor_assemble<<<grid, block, 0, h->stream>>>(ne, mmax, m, k, (const double2 *)mom, nred, red_full,
+                                                  (const double2 *)red_w, nodes, (double2 *)Z, ldz);
+    GRIM_CHECK_LAUNCH(h, "k_bor_assemble");
+    return GRIM_OK;
+}
+
+extern "C" int grim_bor_excitation(grim_handle_t h, int ne, const double *nodes, double k, int m, int nth,
+                                   const double *thetas_deg, int far, int nred, const int *red_full, const void *red_w,
+                                   void *V, int64_t ldv) {
+    if (!h || ne < 2 || !nodes || !thetas_deg || !red_full || !red_w || !V || nth <= 0 || 2 * nth > 65535 ||
+        nred <= 0 || ldv < nred)
+        return grim_fail(GRIM_ERR_ARGUMENT, "grim_bor_excitation: bad arguments");
+    DeviceGuard g(h->device);
+    dim3 grid(ceil_div(nred, 128), 2 * nth);
+    k_bor_excitation<<<grid, 128, 0, h->stream>>>(ne, nodes, k, m, nth, thetas_deg, far, nred, red_full,
+                                                  (const double2 *)red_w, (double2 *)V, ldv);
+    GRIM_CHECK_LAUNCH(h, "k_bor_excitation");
+    return GRIM_OK;
+}
+
+extern "C" int grim_bor_farfield_accumulate(grim_handle_t h, int nred, int ncol, const void *W, int64_t ldw,
+                                            const void *X, int64_t ldx, void *amp) {
+    if (!h || nred <= 0 || ncol <= 0 || !W || !X || !amp || ldw < nred || ldx < nred)
+        return grim_fail(GRIM_ERR_ARGUMENT, "grim_bor_farfield_accumulate: bad arguments");
+    DeviceGuard g(h->device);
+    k_bor_farfield_accumulate<<<ncol, 256, 0, h->stream>>>(nred, ncol, (const double2 *)W, ldw, (const double2 *)X,
+                                                           ldx, (double2 *)amp);
+    GRIM_CHECK_LAUNCH(h, "k_bor_farfield_accumulate");
     return GRIM_OK;
 }

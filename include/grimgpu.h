@@ -132,6 +132,30 @@ int grim_zgesv_batched(grim_handle_t h, int n, int nrhs, const double *A, int ld
                        int precision_mode, int *info);
 int grim_last_solve_info(grim_handle_t h, grim_solve_info *out);
 
+/* ---- body of revolution (PEC EFIE per azimuthal mode) -----------------------------
+ * nodes: 2*(ne+1) doubles (rho, z) of the generatrix, +z pole to -z pole.
+ * grim_bor_moments: mode-independent element-pair moments of the modal Green's function
+ *   for n = 0..mmax+1 (reference bor/kernels.py:632 banded_modal_kernels and
+ *   bor/bor_stream_kernel.c:332-418 samplers); mom holds grim_bor_moments_size(ne, mmax)
+ *   bytes; nxi_max bounds the per-pair azimuthal sample count (<= 8192).
+ * grim_bor_assemble: reduced mode-m EFIE matrix (reference bor/solver.py:1769 assemble_mode
+ *   with the pole reduction of :2428 reduce_pole_operator); red_full[2*nred] lists the
+ *   full components (t: node, phi: (ne+1)+node; -1 unused) of each reduced function and
+ *   red_w[2*nred] (complex128) their weights.
+ * grim_bor_excitation: reduced right-hand sides (far = 0) or far-field weights (far = 1),
+ *   columns [VV theta..., HH theta...] (reference bor/solver.py:2558 rhs_vv_hh_batch,
+ *   :2608 farfield_vv_hh_batch).
+ * grim_bor_farfield_accumulate: amp[c] += sum_r W[r, c] X[r, c]. */
+int64_t grim_bor_moments_size(int ne, int mmax);
+int grim_bor_moments(grim_handle_t h, int ne, const double *nodes, double k, int mmax, int nxi_max, void *mom);
+int grim_bor_assemble(grim_handle_t h, int ne, const double *nodes, double k, int mmax, int m, const void *mom,
+                      int nred, const int *red_full, const void *red_w, void *Z, int64_t ldz);
+int grim_bor_excitation(grim_handle_t h, int ne, const double *nodes, double k, int m, int nth,
+                        const double *thetas_deg, int far, int nred, const int *red_full, const void *red_w,
+                        void *V, int64_t ldv);
+int grim_bor_farfield_accumulate(grim_handle_t h, int nred, int ncol, const void *W, int64_t ldw, const void *X,
+                                 int64_t ldx, void *amp);
+
 /* Per-kernel profiling: while enabled, every launch records a CUDA event on the handle
  * stream; the report is JSON {"kernel": {"launches", "ms", "flops", "bytes"}} where a
  * kernel's time is the span from the previous event to its own (gaps included). */

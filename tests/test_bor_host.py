@@ -1,0 +1,49 @@
+"""BoR host logic (no GPU): pole reduction map, mode limits, sample counts."""
+import numpy as np
+
+from grim_20261007_b200 import synthetic as S
+from grim_20261007_b200.bor import solver as B
+from oracle import bor as OB
+
+
+def _q_from_map(rf, rw, nred, nn):
+    Q = np.zeros((2 * nn, nred), dtype=complex)
+    for r in range(nred):
+        for i in range(2):
+            f = rf[2 * r + i]
+            if f >= 0:
+                Q[f, r] = rw[2 * r + i]
+    return Q
+
+
+def test_pole_map_matches_oracle_transform():
+    pts = S.sphere_generatrix(1.0, 12)
+    body = OB.Body(pts)
+    for m in (-3, -1, 0, 1, 2):
+        rf, rw, nred = B.pole_map(pts, m)
+        Q = _q_from_map(rf, rw, nred, len(pts))
+        np.testing.assert_array_equal(Q, OB.pole_transform(body, m))
+
+
+def test_mode_limits_follow_reference_rule():
+    cap, bw = B.mode_limits(25.0, 1.0, [0, 90], None)
+    assert bw == 25 and cap == 25 + max(12, int(np.ceil(4.05 * 25 ** (1 / 3) + 2)))
+    assert B.mode_limits(25.0, 1.0, [0.0, 180.0], None) == (1, 1)
+    assert B.mode_limits(3.0, 1.0, [30.0], 10) == (10, 2)
+
+
+def test_nxi_bound_matches_oracle_rule():
+    pts = S.sphere_generatrix(1.0, 20)
+    k, mmax = 3.0, 8
+    got = B.nxi_max(pts, k, mmax)
+    body = OB.Body(pts)
+    asm_pts = B.far_points(pts)
+    best = 0
+    ne = len(pts) - 1
+    el = np.repeat(np.arange(ne), 3)
+    for i in range(len(asm_pts)):
+        for j in range(len(asm_pts)):
+            if abs(el[i] - el[j]) >= 2:
+                r0 = np.hypot(*(asm_pts[i] - asm_pts[j]))
+                best = max(best, int(OB.n_xi(k, asm_pts[i, 0], asm_pts[j, 0], r0, mmax)))
+    assert got == best

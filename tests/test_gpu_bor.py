@@ -1,0 +1,78 @@
+"""GPU body-of-revolution path against the FP64 oracle, the reference solver and Mie."""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import bor as OB, mie
+from grim_20261007_b200 import synthetic as S
+from tests.conftest import GOLDEN
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip('torch')
+
+
+@pytest.fixture(scope='module')
+def ctx():
+    if not torch.cuda.is_available():
+        pytest.skip('no CUDA device')
+    from grim_20261007_b200.device import context
+    return context()
+
+
+@pytest.mark.parametrize('m', [0, 1, -1, 2, -3])
+def test_mode_matrix_matches_oracle(ctx, m):
+    from grim_20261007_b200.bor import solver as B
+    pts = S.sphere_generatrix(1.0, 14)
+    k, mmax = 2.5, 4
+    dev = B.BorDevice(pts, k, mmax)
+    Zg = dev.matrix(m).cpu().numpy().T
+    body = OB.Body(pts)
+    asm = OB.Assembler(body, k, mmax)
+    Q = OB.pole_transform(body, m)
+    Zr = Q.conj().T @ asm.matrix(m) @ Q
+    assert np.max(np.abs(Zg - Zr)) <= 1e-11 * np.max(np.abs(Zr))
+
+
+def test_excitation_matches_oracle(ctx):
+    from grim_20261007_b200.bor import solver as B
+    pts = S.ogive_generatrix(3.0, 22.0, 16)
+    k = 4.0
+    dev = B.BorDevice(pts, k, 3)
+    th = torch.as_tensor(np.array([5.0, 47.0, 90.0, 133.0]), device='cuda')
+    body = OB.Body(pts)
+    for m in (-2, -1, 0, 1, 3):
+        Q = OB.pole_transform(body, m)
+        for far in (False, True):
+            got = dev.excitation(m, th, far).cpu().numpy().T
+            full = OB.excitation(body, k, th.cpu().numpy(), m, far=far)
+            ref = (Q.T if far else Q.conj().T) @ full
+            assert np.max(np.abs(got - ref)) <= 1e-12 * max(1e-30, np.max(np.abs(ref)))
+
+
+def test_solve_matches_oracle_and_mie(ctx):
+    from grim_20261007_b200.bor.solver import solve_bor
+    pts = S.sphere_generatrix(1.0, 24)
+    k = 2.0
+    th = [0.0, 35.0, 90.0, 160.0]
+    res = solve_bor(pts, k * S.C0 / (2 * np.pi), th, formulation='efie', n_modes=6)
+    o = OB.solve(pts, k, th, 6)
+    for key in ('amp_vv', 'amp_hh'):
+        got = np.asarray(res[key])
+        assert np.max(np.abs(got - o[key])) <= 1e-9 * np.max(np.abs(o[key]))
+    db = 10 * np.log10(np.asarray(res['sigma_vv']) / mie.sphere_sigma(1.0, k))
+    assert np.max(np.abs(db)) < 0.1  # 24 elements: second-order discretisation error ~0.07 dB
+
+
+def test_reference_sphere_golden(ctx):
+    """Reference solve_bor (EFIE) on the 45-element sphere at ka = 3 (tests/golden/ref_bor_sphere.npz)."""
+    from grim_20261007_b200.bor.solver import solve_bor
+    g = np.load(os.path.join(GOLDEN, 'ref_bor_sphere.npz'))
+    res = solve_bor(g['points'], float(g['freq_hz']), g['thetas'], formulation='efie', n_modes=int(g['modes_used']))
+    for pol in ('vv', 'hh'):
+        got = np.asarray(res['sigma_' + pol])
+        assert np.max(np.abs(10 * np.log10(got / g['sigma_%s_efie' % pol]))) < 0.01
+        amp = np.asarray(res['amp_' + pol])
+        assert np.max(np.abs(amp - g['amp_%s_efie' % pol]) / np.abs(g['amp_%s_efie' % pol])) < 2e-3
+    assert np.max(np.abs(10 * np.log10(np.asarray(res['sigma_vv']) / float(g['mie_sigma'])))) < 0.02
+    assert res['n_unknowns'] == int(g['n_unknowns'])
