@@ -740,3 +740,6 @@ extern "C" int grim_bor_farfield_accumulate(grim_handle_t h, int nred, int ncol,
     GRIM_CHECK_LAUNCH(h, "k_bor_farfield_accumulate");
     return GRIM_OK;
 }
+
+// ============================================================== allocation-free backward error
+#include "noalloc.cu"

@@ -115,6 +115,19 @@ int grim_cgetrs(grim_handle_t h, int n, int nrhs, const void *LU, int64_t lda, c
 int grim_backward_error(grim_handle_t h, int n, int nrhs, const void *A, int64_t lda, int a_complex64,
                         const void *X, int64_t ldx, const void *B, int64_t ldb, double *berr_dev);
 
+/* Allocation-free grim_backward_error (no counterpart in the reference).  For callers
+ * that cannot allocate device memory when they call it (memory owned by another
+ * framework's allocator, allocation-free serving loops, FFI callers without a device
+ * allocator): same arguments and result as grim_backward_error, but its scratch is one
+ * fixed array compiled into the library (about 2.6 MB on every device that loads it,
+ * kept until the process exits) instead of handle workspace.  Limits: n <= 1024,
+ * nrhs <= 128; larger sizes return GRIM_ERR_ARGUMENT.  The first call on a device looks
+ * up the array's device address; make that first call before any stream capture on
+ * that device.  All calls on a device share the array: calls whose GPU work overlaps
+ * race and must be serialized by the caller. */
+int grim_backward_error_noalloc(grim_handle_t h, int n, int nrhs, const void *A, int64_t lda, int a_complex64,
+                                const void *X, int64_t ldx, const void *B, int64_t ldb, double *berr_dev);
+
 /* Device-resident solve of A X = B, X overwrites B (complex128).
  * precision_mode GRIM_PREC_FP64: zgetrf + zgetrs.  GRIM_PREC_MIXED: complex64 LU of A
  * (or of A32 when given), FP64 residual against A (complex128, or the exact promotion

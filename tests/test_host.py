@@ -17,7 +17,7 @@ def test_library_loads_and_exports_every_declared_symbol():
     for name in declared:
         assert hasattr(lib, name), name
     bound = {s[0] for s in _lib.SIGNATURES}
-    assert set(declared) <= bound | {'grim_noalloc_zgesv'} or set(declared) <= bound
+    assert set(declared) <= bound
     assert lib.grim_version() >= 1
 
 
