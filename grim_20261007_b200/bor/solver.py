@@ -131,8 +131,8 @@ def nxi_max(nodes, k, mmax):
 class BorDevice:
     """Device-resident generatrix, moments and per-mode maps of one (body, k)."""
 
-    def __init__(self, points, k, mmax):
-        self.ctx = context()
+    def __init__(self, points, k, mmax, ctx=None):
+        self.ctx = ctx or context()
         self.nodes = validate_generatrix(points)
         self.k = float(k)
         self.mmax = int(mmax)
@@ -170,9 +170,9 @@ class BorDevice:
         return V
 
 
-def solve_bor_device(points, k, thetas_deg, mmax, precision='double', tol=None):
+def solve_bor_device(points, k, thetas_deg, mmax, precision='double', tol=None, ctx=None):
     """Device path: returns (F[2 nth] complex128 on the host, telemetry)."""
-    dev = BorDevice(points, k, mmax)
+    dev = BorDevice(points, k, mmax, ctx=ctx)
     th = torch.as_tensor(np.asarray(thetas_deg, dtype=np.float64), device='cuda')
     nth = int(th.numel())
     amp = torch.zeros(2 * nth, dtype=torch.complex128, device='cuda')
@@ -181,7 +181,7 @@ def solve_bor_device(points, k, thetas_deg, mmax, precision='double', tol=None):
         Z = dev.matrix(m)
         V = dev.excitation(m, th, far=False)
         W = dev.excitation(m, th, far=True)
-        st = ops2d.solve_inplace(Z, V, precision, tol=tol)
+        st = ops2d.solve_inplace(Z, V, precision, tol=tol, ctx=dev.ctx)
         tele['refinement_steps'] = max(tele['refinement_steps'], int(st.get('refinement_steps', 0)))
         nred = int(Z.shape[0])
         _lib.check(dev.ctx.lib.grim_bor_farfield_accumulate(dev.ctx.h, nred, 2 * nth, ptr(W), nred, ptr(V), nred,

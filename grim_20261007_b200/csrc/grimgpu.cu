@@ -597,6 +597,32 @@ extern "C" int grim_zgesv_mixed(grim_handle_t h, int n, int nrhs, const void *A,
     return GRIM_OK;
 }
 
+// Mixed-precision solve that reuses an existing complex64 factorization (LU32, ipiv from
+// grim_cgetrf with leading dimension n): FP64 refinement against A (complex128) or the
+// exact promotion of A32.  Used by the serving engine's resident factor cache.
+extern "C" int grim_zgesv_mixed_factored(grim_handle_t h, int n, int nrhs, const void *A, int64_t lda,
+                                         const void *A32, int64_t lda32, void *LU32, const int *ipiv, void *B,
+                                         int64_t ldb, double tol, int max_iter, grim_solve_info *stats) {
+    if (!h || n <= 0 || nrhs <= 0 || !B || ldb < n || (!A && !A32) || (A && lda < n) || (A32 && lda32 < n) || !LU32 ||
+        !ipiv)
+        return grim_fail(GRIM_ERR_ARGUMENT, "grim_zgesv_mixed_factored: bad arguments");
+    DeviceGuard g(h->device);
+    grim_solve_info st{};
+    st.precision_mode = GRIM_PREC_MIXED;
+    StreamTimer ts(h->stream);
+    int s;
+    if (A)
+        s = mixed_refine<double2>(h, n, nrhs, (const double2 *)A, lda, (float2 *)LU32, ipiv, (double2 *)B, ldb, tol,
+                                  max_iter, &st);
+    else
+        s = mixed_refine<float2>(h, n, nrhs, (const float2 *)A32, lda32, (float2 *)LU32, ipiv, (double2 *)B, ldb, tol,
+                                 max_iter, &st);
+    st.ms_solve = ts.stop_ms();
+    h->last = st;
+    if (stats) *stats = st;
+    return s;
+}
+
 // B1 drop-in with host buffers.
 extern "C" int grim_zgesv_batched(grim_handle_t h, int n, int nrhs, const double *A, int lda, double *B, int ldb,
                                   int precision_mode, int *info) {

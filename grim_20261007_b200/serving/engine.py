@@ -1,0 +1,309 @@
+"""Continuous-batching RCS request engine on one GPU.
+
+* Requests (2-D closed PEC contours or bodies of revolution) arrive at any time
+  (``submit``); each returns a ``concurrent.futures.Future``.
+* ``slots`` worker threads each own a libgrimgpu handle and a CUDA stream; a request is
+  admitted into a free slot only when its estimated device memory fits in the HBM budget
+  next to the requests already running (the reference admits solves by RAM the same way:
+  ``twod/solver.py:1474`` ``_estimate_memory_gb``, ``:2382-2398``).  Requests that arrive
+  while others run are admitted as soon as a slot and memory free up, so their kernels
+  overlap on the device.
+* A resident factor cache keeps the system matrix and its LU factors of recent 2-D
+  geometries on the device, keyed by (geometry hash, k, polarization, precision); a
+  repeat geometry skips the fill and the factorization and only solves its angles.
+* ``stats()`` reports completed solves, solves/s and p50/p99 latency (arrival to result).
+
+Results do not depend on what else runs: every kernel's reductions have a fixed order
+per problem size, so a request gives the same answer alone and in the mix.
+"""
+from __future__ import annotations
+
+import collections
+import concurrent.futures as cf
+import ctypes
+import hashlib
+import threading
+import time
+
+import numpy as np
+import torch
+
+from .. import _lib
+from ..device import Context, ptr, require_cuda
+from ..twod import geometry as geo, operators as ops
+
+
+class Request:
+    """One RCS solve: kind '2d' (vertices, polarization) or 'bor' (generatrix, both pols)."""
+
+    _ids = 0
+
+    def __init__(self, kind, geometry, k, angles_deg, polarization='TM', precision='mixed', n_modes=None):
+        if kind not in ('2d', 'bor'):
+            raise ValueError("request kind must be '2d' or 'bor'")
+        Request._ids += 1
+        self.id = Request._ids
+        self.kind = kind
+        self.geometry = np.ascontiguousarray(np.asarray(geometry, dtype=np.float64))
+        self.k = float(k)
+        self.angles = np.ascontiguousarray(np.asarray(angles_deg, dtype=np.float64).reshape(-1))
+        self.pol = ops.canonical_pol(polarization) if kind == '2d' else 'VV+HH'
+        self.precision = precision
+        self.n_modes = n_modes
+        self.arrival = None
+        self.started = None
+        self.finished = None
+        self.cache_hit = False
+
+    @property
+    def n(self):
+        return len(self.geometry) if self.kind == '2d' else 2 * len(self.geometry)
+
+    def cache_key(self):
+        h = hashlib.sha256(self.geometry.tobytes()).hexdigest()[:24]
+        return (self.kind, h, round(self.k, 12), self.pol, self.precision)
+
+    def estimate_bytes(self, cached=False):
+        """Device memory while running (matrix, factors, right-hand sides, workspace)."""
+        r = max(1, len(self.angles))
+        if self.kind == '2d':
+            esz = 8 if self.precision == 'mixed' else 16
+            fixed = 0 if cached else 2 * self.n * self.n * esz + 2 * self.n * 64 * esz
+            return fixed + 8 * self.n * r * 16 + (1 << 20)
+        ne = len(self.geometry) - 1
+        mm = (self.n_modes or 40) + 2
+        return ne * ne * mm * 20 * 16 + 4 * (2 * ne + 2) ** 2 * 16 + 8 * (2 * ne + 2) * 2 * r * 16 + (1 << 20)
+
+
+class FactorCache:
+    """LRU cache of resident 2-D system matrices and factors, bounded in bytes."""
+
+    def __init__(self, capacity_bytes):
+        self.capacity = int(capacity_bytes)
+        self.used = 0
+        self.items = collections.OrderedDict()
+        self.lock = threading.Lock()
+        self.hits = 0
+        self.misses = 0
+
+    def contains(self, key):
+        with self.lock:
+            return key in self.items
+
+    def get(self, key):
+        with self.lock:
+            e = self.items.get(key)
+            if e is None:
+                self.misses += 1
+                return None
+            self.items.move_to_end(key)
+            self.hits += 1
+            return e
+
+    def put(self, key, entry, nbytes):
+        with self.lock:
+            if nbytes > self.capacity:
+                return
+            while self.used + nbytes > self.capacity and self.items:
+                _k, old = self.items.popitem(last=False)
+                self.used -= old['bytes']
+            entry['bytes'] = nbytes
+            self.items[key] = entry
+            self.used += nbytes
+
+
+class _Slot:
+    def __init__(self, device):
+        self.ctx = Context(device)
+        self.stream = torch.cuda.Stream(device)
+
+
+class ServingEngine:
+    def __init__(self, slots=4, hbm_budget_bytes=None, cache_bytes=None, device=0, tol=None):
+        require_cuda()
+        self.device = int(device)
+        torch.cuda.set_device(self.device)
+        free, _total = torch.cuda.mem_get_info(self.device)
+        self.budget = int(hbm_budget_bytes or 0.8 * free)
+        self.cache = FactorCache(cache_bytes if cache_bytes is not None else self.budget // 4)
+        self.tol = ops.MIXED_RCS_TOL if tol is None else float(tol)
+        self.slots = [_Slot(self.device) for _ in range(int(slots))]
+        self.pending = collections.deque()
+        self.cv = threading.Condition()
+        self.in_use = 0
+        self.running = 0
+        self.max_running = 0
+        self.closed = False
+        self.done = []
+        self.t0 = None
+        self.threads = [threading.Thread(target=self._worker, args=(s,), daemon=True) for s in self.slots]
+        for t in self.threads:
+            t.start()
+
+    # ------------------------------------------------------------------ API
+    def submit(self, req):
+        fut = cf.Future()
+        req.arrival = time.perf_counter()
+        with self.cv:
+            if self.closed:
+                raise RuntimeError('engine is closed')
+            if self.t0 is None:
+                self.t0 = req.arrival
+            est = req.estimate_bytes(cached=self.cache.contains(req.cache_key()))
+            if est > self.budget:
+                fut.set_exception(MemoryError(f'request {req.id} needs ~{est / 2**30:.2f} GiB, above the '
+                                              f'{self.budget / 2**30:.2f} GiB device budget'))
+                return fut
+            self.pending.append((req, fut, est))
+            self.cv.notify_all()
+        return fut
+
+    def close(self):
+        with self.cv:
+            self.closed = True
+            self.cv.notify_all()
+        for t in self.threads:
+            t.join()
+
+    def stats(self):
+        with self.cv:
+            lat = np.array([r.finished - r.arrival for r in self.done])
+            span = (max(r.finished for r in self.done) - self.t0) if self.done else 0.0
+        out = {'completed': int(len(lat)), 'max_concurrent': int(self.max_running),
+               'cache_hits': self.cache.hits, 'cache_misses': self.cache.misses}
+        if len(lat):
+            out.update(p50_ms=float(np.percentile(lat, 50) * 1e3), p99_ms=float(np.percentile(lat, 99) * 1e3),
+                       mean_ms=float(lat.mean() * 1e3), solves_per_s=float(len(lat) / span) if span > 0 else None)
+        return out
+
+    # ------------------------------------------------------------------ scheduling
+    def _take(self):
+        """Admit the oldest pending request that fits next to the running ones."""
+        for i, (req, fut, est) in enumerate(self.pending):
+            if self.in_use + est <= self.budget or self.running == 0:
+                del self.pending[i]
+                return req, fut, est
+        return None
+
+    def _worker(self, slot):
+        torch.cuda.set_device(self.device)
+        while True:
+            with self.cv:
+                item = None
+                while item is None:
+                    if self.closed and not self.pending:
+                        return
+                    item = self._take()
+                    if item is None:
+                        self.cv.wait(timeout=0.05)
+                req, fut, est = item
+                self.in_use += est
+                self.running += 1
+                self.max_running = max(self.max_running, self.running)
+            try:
+                req.started = time.perf_counter()
+                result = self._run(slot, req)
+                req.finished = time.perf_counter()
+                fut.set_result(result)
+            except BaseException as exc:  # surfaced to the caller through the future
+                req.finished = time.perf_counter()
+                fut.set_exception(exc)
+            finally:
+                with self.cv:
+                    self.in_use -= est
+                    self.running -= 1
+                    if fut.exception() is None:
+                        self.done.append(req)
+                    self.cv.notify_all()
+
+    # ------------------------------------------------------------------ execution
+    def _run(self, slot, req):
+        with torch.cuda.stream(slot.stream):
+            slot.ctx.bind_stream(slot.stream)
+            if req.kind == '2d':
+                amp, tele = self._run_2d(slot, req)
+                return {'id': req.id, 'amplitude': amp, 'telemetry': tele}
+            from ..bor.solver import solve_bor_device, mode_limits
+            mcap, _ = mode_limits(req.k, float(np.max(req.geometry[:, 0])), req.angles, req.n_modes)
+            F, tele = solve_bor_device(req.geometry, req.k, req.angles, mcap,
+                                       precision=req.precision, tol=self.tol, ctx=slot.ctx)
+            nth = len(req.angles)
+            return {'id': req.id, 'amp_vv': F[:nth], 'amp_hh': F[nth:], 'telemetry': tele}
+
+    def _run_2d(self, slot, req):
+        ctx, s = slot.ctx, slot.stream
+        v = req.geometry
+        body = ops.DeviceBody(geo.panel_geometry([v]), geo.te_curvature_correction([v]) if req.pol == 'TE' else None)
+        ang = torch.as_tensor(req.angles, device='cuda')
+        n = body.n
+        key = req.cache_key()
+        entry = self.cache.get(key)
+        req.cache_hit = entry is not None
+        mixed = req.precision == 'mixed'
+        if entry is None:
+            z = ops.fill(body, req.k, req.pol, complex64=mixed, ctx=ctx)
+            lu = z.clone()
+            ipiv = torch.empty(n, dtype=torch.int32, device='cuda')
+            info = ctypes.c_int(0)
+            fn = ctx.lib.grim_cgetrf if mixed else ctx.lib.grim_zgetrf
+            _lib.check(fn(ctx.h, n, ptr(lu), n, ptr(ipiv), ctypes.byref(info)), 'getrf')
+            if info.value:
+                raise _lib.GrimError(_lib.GRIM_ERR_SINGULAR, f'request {req.id}: singular system (info={info.value})')
+            entry = {'z': z, 'lu': lu, 'ipiv': ipiv}
+            self.cache.put(key, entry, 2 * z.numel() * z.element_size())
+        else:
+            for t in (entry['z'], entry['lu'], entry['ipiv']):
+                t.record_stream(s)
+        b = ops.rhs(body, req.k, req.pol, ang, ctx=ctx)
+        tele = {'cache_hit': req.cache_hit, 'n': n}
+        st = _lib.GrimSolveInfo()
+        if mixed:
+            status = ctx.lib.grim_zgesv_mixed_factored(ctx.h, n, int(b.shape[0]), None, 0, ptr(entry['z']), n,
+                                                       ptr(entry['lu']), ptr(entry['ipiv']), ptr(b), n, self.tol, 10,
+                                                       ctypes.byref(st))
+            _lib.check(status, 'grim_zgesv_mixed_factored')
+            x = b
+            tele.update(st.as_dict())
+        else:
+            x = b.clone()
+            _lib.check(ctx.lib.grim_zgetrs(ctx.h, n, int(b.shape[0]), ptr(entry['lu']), n, ptr(entry['ipiv']), ptr(x),
+                                           n), 'grim_zgetrs')
+            berr = ops.backward_error(entry['z'], x, b, ctx=ctx)
+            tele['backward_error'] = float(berr.max().item())
+        amp = ops.farfield(body, req.k, ang, x, ctx=ctx)
+        return amp.cpu().numpy(), tele
+
+
+def synthetic_stream(seed, count, nmax=8192, angle_max=720, repeat_fraction=0.3, bor_fraction=0.2,
+                     bor_elements=120, precision='mixed'):
+    """Seeded mixed request list (2-D superellipses/airfoils and BoR ogives)."""
+    from .. import synthetic as S
+    rng = np.random.default_rng(seed)
+    reqs = []
+    made = []
+    for _ in range(count):
+        nang = int(rng.integers(1, angle_max + 1))
+        ang = np.sort(rng.uniform(0.0, 360.0, nang))
+        if made and rng.random() < repeat_fraction:
+            geom, k, pol = made[int(rng.integers(0, len(made)))]
+            reqs.append(Request('2d', geom, k, ang, pol, precision))
+            continue
+        if rng.random() < bor_fraction:
+            gen, length, half = S.ogive_case(int(rng.integers(0, 1 << 30)), n=bor_elements)
+            k = float(rng.uniform(2.0, 12.0))
+            mm = int(rng.integers(8, 41))
+            th = np.sort(rng.uniform(0.0, 180.0, min(nang, 181)))
+            reqs.append(Request('bor', gen, k, th, precision=precision, n_modes=mm))
+            continue
+        n = int(rng.integers(32, nmax // 2 + 1)) * 2
+        if rng.random() < 0.5:
+            v = S.superellipse(float(rng.uniform(0.3, 1.0)), float(rng.uniform(0.2, 0.8)), float(rng.uniform(1.5, 4.0)), n)
+        else:
+            v = S.naca_symmetric(float(rng.uniform(0.08, 0.15)), n)
+        lam = S.polygon_perimeter(v) * 10.0 / n
+        k = 2 * np.pi / lam
+        pol = 'TM' if rng.random() < 0.5 else 'TE'
+        made.append((v, k, pol))
+        reqs.append(Request('2d', v, k, ang, pol, precision))
+    gaps = rng.exponential(1.0, count)
+    return reqs, gaps

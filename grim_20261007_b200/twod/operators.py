@@ -47,8 +47,8 @@ class DeviceBody:
         self.h2d_bytes = g.nbytes + (0 if te_diag is None else np.asarray(te_diag).nbytes)
 
 
-def fill(body, k, pol, complex64=False, out=None):
-    ctx = context()
+def fill(body, k, pol, complex64=False, out=None, ctx=None):
+    ctx = ctx or context()
     n = body.n
     dt = torch.complex64 if complex64 else torch.complex128
     z = out if out is not None else torch.empty((n, n), dtype=dt, device=body.geom.device)
@@ -58,8 +58,8 @@ def fill(body, k, pol, complex64=False, out=None):
     return z
 
 
-def rhs(body, k, pol, angles_dev, complex64=False, out=None):
-    ctx = context()
+def rhs(body, k, pol, angles_dev, complex64=False, out=None, ctx=None):
+    ctx = ctx or context()
     n, nang = body.n, int(angles_dev.numel())
     dt = torch.complex64 if complex64 else torch.complex128
     b = out if out is not None else torch.empty((nang, n), dtype=dt, device=body.geom.device)
@@ -68,8 +68,8 @@ def rhs(body, k, pol, angles_dev, complex64=False, out=None):
     return b
 
 
-def farfield(body, k, angles_dev, x, out=None):
-    ctx = context()
+def farfield(body, k, angles_dev, x, out=None, ctx=None):
+    ctx = ctx or context()
     nang = int(angles_dev.numel())
     amp = out if out is not None else torch.empty(nang, dtype=torch.complex128, device=body.geom.device)
     _lib.check(ctx.lib.grim_farfield2d(ctx.h, body.n, ptr(body.geom), nang, ptr(angles_dev), float(k), ptr(x),
@@ -77,7 +77,7 @@ def farfield(body, k, angles_dev, x, out=None):
     return amp
 
 
-def solve_inplace(z, b, precision='double', tol=None, max_iter=10, z32=None):
+def solve_inplace(z, b, precision='double', tol=None, max_iter=10, z32=None, ctx=None):
     """Solve Z X = B on the device; X overwrites ``b`` (complex128, shape (nrhs, n)).
 
     precision 'double': FP64 LU + triangular solves.  'mixed': complex64 LU of ``z32``
@@ -85,7 +85,7 @@ def solve_inplace(z, b, precision='double', tol=None, max_iter=10, z32=None):
     when ``z`` is None, against the exact promotion of ``z32``.
     Returns the solve telemetry dict.
     """
-    ctx = context()
+    ctx = ctx or context()
     n = int(b.shape[1])
     nrhs = int(b.shape[0])
     info = ctypes.c_int(0)
@@ -98,9 +98,9 @@ def solve_inplace(z, b, precision='double', tol=None, max_iter=10, z32=None):
     return st.as_dict()
 
 
-def backward_error(z, x, b):
+def backward_error(z, x, b, ctx=None):
     """Per-column normwise backward error on the device (reference twod/solver.py:695-720)."""
-    ctx = context()
+    ctx = ctx or context()
     n, nrhs = int(b.shape[1]), int(b.shape[0])
     berr = torch.empty(nrhs, dtype=torch.float64, device=b.device)
     _lib.check(ctx.lib.grim_backward_error(ctx.h, n, nrhs, ptr(z), n, int(z.dtype == torch.complex64), ptr(x), n,

@@ -138,6 +138,13 @@ int grim_zgesv_mixed(grim_handle_t h, int n, int nrhs, const void *A, int64_t ld
                      int64_t lda32, void *B, int64_t ldb, int precision_mode, double tol, int max_iter,
                      int *info, grim_solve_info *stats);
 
+/* Mixed solve reusing a complex64 factorization (LU32 and ipiv from grim_cgetrf, leading
+ * dimension n) with FP64 refinement against A or the promotion of A32; for resident
+ * factor caches (reference linalg/refined_lu.py:41-61 RefinedLU.solve on a kept factor). */
+int grim_zgesv_mixed_factored(grim_handle_t h, int n, int nrhs, const void *A, int64_t lda, const void *A32,
+                              int64_t lda32, void *LU32, const int *ipiv, void *B, int64_t ldb, double tol,
+                              int max_iter, grim_solve_info *stats);
+
 /* B1 drop-in (host buffers): solve A X = B for all nrhs columns, X overwrites B.
  * A: n x n complex128 column-major (lda >= n), B: n x nrhs complex128 (ldb >= n).
  * Copies host -> device, solves, copies device -> host; synchronous. */
