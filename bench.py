@@ -110,6 +110,65 @@ def profile_step(ctx, fn):
     return json.loads(buf.value.decode())
 
 
+def run_serving(args):
+    """Seeded Poisson stream of mixed requests at ~80% of the measured service rate."""
+    from grim_20261007_b200.serving import ServingEngine, synthetic_stream
+    reqs, gaps = synthetic_stream(args.seed + 17, args.serving_requests, nmax=8192, angle_max=720)
+    probe, _ = synthetic_stream(args.seed + 17, args.serving_requests, nmax=8192, angle_max=720)
+    eng = ServingEngine(slots=1)
+    t0 = time.perf_counter()
+    for r in probe[: max(4, len(probe) // 4)]:
+        eng.submit(r).result()
+    service = (time.perf_counter() - t0) / max(4, len(probe) // 4)
+    eng.close()
+    rate = 0.8 / service  # requests per second at ~80% load of one slot's service rate
+    eng = ServingEngine(slots=4)
+    futs = []
+    t0 = time.perf_counter()
+    due = 0.0
+    for r, g in zip(reqs, gaps):
+        due += g / rate
+        delay = t0 + due - time.perf_counter()
+        if delay > 0:
+            time.sleep(delay)
+        futs.append(eng.submit(r))
+    for f in futs:
+        f.result()
+    st = eng.stats()
+    eng.close()
+    st.update(requests=len(reqs), arrival_rate_per_s=rate, mean_service_s_single_slot=service,
+              mix='2-D superellipse/airfoil N~U[64,8192] (TM/TE), BoR ogives |m|<=U{8..40}, 1-720 angles, '
+                  '30% repeat geometries, mixed precision')
+    return st
+
+
+def run_bor(args):
+    """Body-of-revolution ogive: 400 generatrix segments, |m| <= 40, 361 aspects, VV/HH."""
+    import torch
+    from grim_20261007_b200 import synthetic as S
+    from grim_20261007_b200.bor.solver import solve_bor_device
+    gen, length, half = S.ogive_case(args.seed, n=400)
+    k = 25.0 / max(1e-9, float(np.max(gen[:, 0])))  # k rho_max = 25 (the reference's |m| <= 40 converges)
+    th = np.arange(361) * 0.5
+    out = {'length_m': length, 'half_angle_deg': half, 'k': k, 'segments': 400, 'modes': 81, 'aspects': 361}
+    res = {}
+    for prec in ('double', 'mixed'):
+        solve_bor_device(gen, k, th[:8], 4, precision=prec)  # warm-up
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        F, tele = solve_bor_device(gen, k, th, 40, precision=prec)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        res[prec] = F
+        out[prec] = {'seconds': dt, 'solves_per_s': 1.0 / dt, 'refinement_steps': tele['refinement_steps']}
+    s64 = 4 * np.pi * np.abs(res['double']) ** 2
+    s32 = 4 * np.pi * np.abs(res['mixed']) ** 2
+    db = 10 * np.log10(np.maximum(s64, 1e-30))
+    mask = db > db.max() - 40
+    out['max_db_error_mixed_vs_fp64'] = float(np.max(np.abs(10 * np.log10(s32[mask] / s64[mask]))))
+    return out
+
+
 def workload(seed, n, nang):
     from grim_20261007_b200 import synthetic as S
     v, k, f, t = S.airfoil_case(seed, n)
@@ -177,6 +236,9 @@ def main():
     ap.add_argument('--angles', type=int, default=720)
     ap.add_argument('--seed', type=int, default=0)
     ap.add_argument('--cpu-sample', type=int, default=1, help='oracle solves timed for cpu_baseline (0 = skip)')
+    ap.add_argument('--serving', type=int, default=1, help='run the mixed request stream (p50/p99 latency)')
+    ap.add_argument('--serving-requests', type=int, default=32)
+    ap.add_argument('--bor', type=int, default=1, help='time the body-of-revolution ogive workload')
     args = ap.parse_args()
 
     world = int(os.environ.get('WORLD_SIZE', '1'))
@@ -289,6 +351,9 @@ def main():
     h2d = 2 * (geom.nbytes + len(ang) * 8) + geom.shape[0] * 8
     d2h = 2 * len(ang) * 16
 
+    serving = run_serving(args) if (args.serving and rank == 0 and world == 1) else None
+    bor = run_bor(args) if (args.bor and rank == 0 and world == 1) else None
+
     # per-kernel profile of one mixed step (CUDA events after every launch, separate from the timed loop)
     n = args.n
     prof = profile_step(ctx, lambda: step('mixed'))
@@ -336,6 +401,8 @@ def main():
                     'path': 'solve_monostatic_rcs_2d (public API), linear_precision("mixed")'},
             'gpu_launches': int(launches32),
             'roofline': roofline,
+            'serving': serving,
+            'bor_ogive': bor,
             'kernel_profile_mixed': prof,
             'kernel_profile_fp64': prof64,
             'cpu_baseline': cpu_baseline,

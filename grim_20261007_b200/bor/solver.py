@@ -181,7 +181,17 @@ def solve_bor_device(points, k, thetas_deg, mmax, precision='double', tol=None, 
         Z = dev.matrix(m)
         V = dev.excitation(m, th, far=False)
         W = dev.excitation(m, th, far=True)
-        st = ops2d.solve_inplace(Z, V, precision, tol=tol, ctx=dev.ctx)
+        if precision == 'mixed':
+            V0 = V.clone()
+            try:
+                st = ops2d.solve_inplace(Z, V, 'mixed', tol=tol, ctx=dev.ctx)
+            except _lib.GrimNotConverged:
+                # ill-conditioned mode: the reference's ladder falls back to the double LU
+                tele['fp64_fallback_modes'] = tele.get('fp64_fallback_modes', 0) + 1
+                V = V0
+                st = ops2d.solve_inplace(Z, V, 'double', ctx=dev.ctx)
+        else:
+            st = ops2d.solve_inplace(Z, V, precision, tol=tol, ctx=dev.ctx)
         tele['refinement_steps'] = max(tele['refinement_steps'], int(st.get('refinement_steps', 0)))
         nred = int(Z.shape[0])
         _lib.check(dev.ctx.lib.grim_bor_farfield_accumulate(dev.ctx.h, nred, 2 * nth, ptr(W), nred, ptr(V), nred,

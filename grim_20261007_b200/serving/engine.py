@@ -258,11 +258,19 @@ class ServingEngine:
         tele = {'cache_hit': req.cache_hit, 'n': n}
         st = _lib.GrimSolveInfo()
         if mixed:
+            b0 = b.clone()
             status = ctx.lib.grim_zgesv_mixed_factored(ctx.h, n, int(b.shape[0]), None, 0, ptr(entry['z']), n,
                                                        ptr(entry['lu']), ptr(entry['ipiv']), ptr(b), n, self.tol, 10,
                                                        ctypes.byref(st))
-            _lib.check(status, 'grim_zgesv_mixed_factored')
-            x = b
+            if status == _lib.GRIM_ERR_NOT_CONVERGED:
+                # stalled refinement: solve this request in FP64 (reference mixed -> double ladder)
+                z64 = ops.fill(body, req.k, req.pol, ctx=ctx)
+                x = b0
+                ops.solve_inplace(z64, x, 'double', ctx=ctx)
+                tele['fp64_fallback'] = True
+            else:
+                _lib.check(status, 'grim_zgesv_mixed_factored')
+                x = b
             tele.update(st.as_dict())
         else:
             x = b.clone()

@@ -126,10 +126,19 @@ def monostatic_solve(body, k, angles_deg, pol, precision='double', tol=None, che
     if precision == 'mixed':
         z32 = fill(body, k, pol, complex64=True)
         b = rhs(body, k, pol, angles_dev)
-        st = solve_inplace(None, b, 'mixed', tol=MIXED_RCS_TOL if tol is None else tol, z32=z32)
+        b0 = b.clone()
+        try:
+            st = solve_inplace(None, b, 'mixed', tol=MIXED_RCS_TOL if tol is None else tol, z32=z32)
+            x = b
+            z = z32
+        except _lib.GrimNotConverged:
+            # refinement stalled (ill-conditioned system): fall back to the FP64 path, as the
+            # reference's mixed -> double ladder does (linalg/dense.py:74-98)
+            z = fill(body, k, pol)
+            x = b0
+            st = solve_inplace(z, x, 'double')
+            st['fp64_fallback'] = True
         tele.update(st)
-        x = b
-        z = z32
     else:
         z = fill(body, k, pol)
         b = rhs(body, k, pol, angles_dev)

@@ -119,6 +119,12 @@ def _solve_dense_gpu(a_eval, rhs_eval):
         torch.cuda.current_stream().synchronize()
         status = ctx.lib.grim_zgesv_batched(ctx.h, n, nrhs, a_f.ctypes.data_as(_lib.c_void_p), n,
                                             x.ctypes.data_as(_lib.c_void_p), n, mode, _lib.ctypes.byref(info))
+        if status == _lib.GRIM_ERR_NOT_CONVERGED and mode == _lib.PREC_MIXED:
+            # mixed -> double ladder (reference linalg/dense.py:74-98)
+            x[...] = b2
+            status = ctx.lib.grim_zgesv_batched(ctx.h, n, nrhs, a_f.ctypes.data_as(_lib.c_void_p), n,
+                                                x.ctypes.data_as(_lib.c_void_p), n, _lib.PREC_FP64,
+                                                _lib.ctypes.byref(info))
         _lib.check(status, 'grim_zgesv_batched')
     except _lib.GrimMemoryError as exc:
         raise MemoryError(str(exc)) from exc

@@ -156,3 +156,21 @@ def test_backward_error_kernel_matches_host(ctx):
     ref = np.max(np.abs(r), axis=0) / (np.max(np.sum(np.abs(a), axis=1)) * np.max(np.abs(x), axis=0)
                                        + np.max(np.abs(b), axis=0))
     np.testing.assert_allclose(berr.cpu().numpy(), ref, rtol=1e-6)
+
+
+def test_mixed_falls_back_to_fp64_when_refinement_stalls(ctx):
+    """complex64 LU of a kappa ~ 1e10 system cannot refine to 2e-12: the ladder solves it in FP64."""
+    from grim_20261007_b200.execution import linear_precision
+    from grim_20261007_b200.twod.solver import _solve_dense_gpu
+    rng = np.random.default_rng(4)
+    n = 96
+    u, _ = np.linalg.qr(rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n)))
+    v, _ = np.linalg.qr(rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n)))
+    a = (u * np.logspace(0, -10, n)) @ v.conj().T
+    b = rng.standard_normal((n, 3)) + 1j * rng.standard_normal((n, 3))
+    with linear_precision('mixed'):
+        x, _ = _solve_dense_gpu(a, b)
+    r = a @ x - b
+    berr = np.max(np.abs(r), axis=0) / (np.max(np.sum(np.abs(a), axis=1)) * np.max(np.abs(x), axis=0)
+                                        + np.max(np.abs(b), axis=0))
+    assert np.max(berr) < 1e-14
