@@ -71,6 +71,8 @@ SIGNATURES = [
     ('grim_cgetrs', c_int, [c_void_p, c_int, c_int, c_void_p, c_int64, c_void_p, c_void_p, c_int64]),
     ('grim_backward_error', c_int, [c_void_p, c_int, c_int, c_void_p, c_int64, c_int, c_void_p, c_int64, c_void_p,
                                     c_int64, c_void_p]),
+    ('grim_cgemm_sub', c_int, [c_void_p, c_int, c_int, c_int, c_void_p, c_int64, c_void_p, c_int64, c_void_p,
+                               c_int64, c_int]),
     ('grim_backward_error_noalloc', c_int, [c_void_p, c_int, c_int, c_void_p, c_int64, c_int, c_void_p, c_int64,
                                             c_void_p, c_int64, c_void_p]),
     ('grim_zgesv_mixed', c_int, [c_void_p, c_int, c_int, c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_int64,

@@ -6,6 +6,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <cstdlib>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -16,6 +17,7 @@
 #include "linalg.cuh"
 #include "lu.cuh"
 #include "bor.cuh"
+#include "tc_gemm.cuh"
 
 // ============================================================== errors
 static thread_local std::string g_last_error;
@@ -268,6 +270,75 @@ static int gemm(grim_context *h, int M, int N, int K, const TA *A, int64_t lda, 
     return GRIM_OK;
 }
 
+// ============================================================== tensor-core complex64 update
+static int tc_enabled() {
+    static int v = -1;
+    if (v < 0) {
+        const char *e = std::getenv("GRIM_TENSOR_CORES");
+        v = (e && e[0] == '0') ? 0 : 1;
+    }
+    return v;
+}
+
+// C[MxN] -= A[MxK] B[KxN] (complex64, column-major) on tcgen05 (split TF32).
+static int tc_cgemm_sub(grim_context *h, int M, int N, int K, const float2 *A, int64_t lda, const float2 *B,
+                        int64_t ldb, float2 *C, int64_t ldc) {
+    if (M <= 0 || N <= 0 || K <= 0) return GRIM_OK;
+    static bool attr = false;
+    if (!attr) {
+        GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_tc_gemm_sub, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM_BYTES));
+        attr = true;
+    }
+    const int Mp = ceil_div(2 * M, TC_BM) * TC_BM, Np = ceil_div(N, TC_BN) * TC_BN, Kp = ceil_div(2 * K, TC_BK) * TC_BK;
+    void *pa = nullptr, *pb = nullptr, *pe = nullptr;
+    GRIM_TRY(grim_workspace(h, "tc_a", 2 * (size_t)Mp * Kp * sizeof(float), &pa));
+    GRIM_TRY(grim_workspace(h, "tc_b", 2 * (size_t)Np * Kp * sizeof(float), &pb));
+    GRIM_TRY(grim_workspace(h, "tc_err", sizeof(int), &pe));
+    GRIM_CHECK_CUDA(cudaMemsetAsync(pe, 0, sizeof(int), h->stream));
+    float *ahi = (float *)pa, *alo = ahi + (size_t)Mp * Kp, *bhi = (float *)pb, *blo = bhi + (size_t)Np * Kp;
+    const int64_t na = (int64_t)Mp * Kp, nb = (int64_t)Np * Kp;
+    k_tc_pack_a<<<ceil_div(na, 256), 256, 0, h->stream>>>(M, K, A, lda, ahi, alo, Mp, Kp);
+    GRIM_CHECK_LAUNCH(h, "k_tc_pack_a");
+    k_tc_pack_b<<<ceil_div(nb, 256), 256, 0, h->stream>>>(K, N, B, ldb, bhi, blo, Np, Kp);
+    GRIM_CHECK_LAUNCH(h, "k_tc_pack_b");
+    dim3 grid(Mp / TC_BM, Np / TC_BN);
+    k_tc_gemm_sub<<<grid, TC_THREADS, TC_SMEM_BYTES, h->stream>>>(Kp, ahi, alo, bhi, blo, (float *)C, 2 * ldc, 2 * M, N,
+                                                                  (int *)pe);
+    GRIM_CHECK_LAUNCH_W(h, "k_tc_gemm_sub", 8.0 * M * N * K,
+                        4.0 * 2 * ((double)Mp * Kp + (double)Np * Kp) + 2.0 * 8 * M * N);
+    return GRIM_OK;
+}
+
+// Trailing / solve updates C -= A B: tensor cores for complex64 (unless disabled), SIMT otherwise.
+template <typename C>
+static int gemm_sub(grim_context *h, int M, int N, int K, const C *A, int64_t lda, const C *B, int64_t ldb, C *Cm,
+                    int64_t ldc) {
+    if constexpr (sizeof(C) == sizeof(float2)) {
+        if (tc_enabled()) return tc_cgemm_sub(h, M, N, K, (const float2 *)A, lda, (const float2 *)B, ldb, (float2 *)Cm, ldc);
+    }
+    return gemm<C, C, C, C, true, true>(h, M, N, K, A, lda, B, ldb, Cm, ldc);
+}
+
+// Test entry: C -= A B for complex64 (use_tensor_cores 1: tcgen05 path, 0: SIMT path).
+extern "C" int grim_cgemm_sub(grim_handle_t h, int M, int N, int K, const void *A, int64_t lda, const void *B,
+                              int64_t ldb, void *Cm, int64_t ldc, int use_tensor_cores) {
+    if (!h || M <= 0 || N <= 0 || K <= 0 || !A || !B || !Cm || lda < M || ldb < K || ldc < M)
+        return grim_fail(GRIM_ERR_ARGUMENT, "grim_cgemm_sub: bad arguments");
+    DeviceGuard g(h->device);
+    if (use_tensor_cores) {
+        GRIM_TRY(tc_cgemm_sub(h, M, N, K, (const float2 *)A, lda, (const float2 *)B, ldb, (float2 *)Cm, ldc));
+        void *pe = nullptr;
+        GRIM_TRY(grim_workspace(h, "tc_err", sizeof(int), &pe));
+        int err = 0;
+        GRIM_CHECK_CUDA(cudaMemcpyAsync(&err, pe, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+        GRIM_CHECK_CUDA(cudaStreamSynchronize(h->stream));
+        if (err) return grim_fail(GRIM_ERR_CUDA, "grim_cgemm_sub: tensor-core pipeline wait timed out");
+        return GRIM_OK;
+    }
+    return gemm<float2, float2, float2, float2, true, true>(h, M, N, K, (const float2 *)A, lda, (const float2 *)B, ldb,
+                                                          (float2 *)Cm, ldc);
+}
+
 // ============================================================== getrf / getrs
 template <typename C>
 static int smem_opt_in() {
@@ -316,7 +387,7 @@ static int getrf_impl(grim_context *h, int n, C *A, int64_t lda, int *ipiv, int 
             k_panel_apply<C><<<nL + nU, 256, tri, h->stream>>>(n, A, lda, j, nbj, nL, bcol, brow, cert + p,
                                                                counter + p, swapped + p, ipiv, d_info, d_pivoted);
             GRIM_CHECK_LAUNCH_W(h, kname("k_panel_apply", sizeof(C)), 8.0 * 2 * rest * nbj * nbj, 0);
-            GRIM_TRY((gemm<C, C, C, C, true, true>(h, rest, rest, nbj, A + (int64_t)j * lda + j + nbj, lda,
+            GRIM_TRY((gemm_sub<C>(h, rest, rest, nbj, A + (int64_t)j * lda + j + nbj, lda,
                                                   A + (int64_t)(j + nbj) * lda + j, lda,
                                                   A + (int64_t)(j + nbj) * lda + j + nbj, lda)));
         } else {
@@ -364,7 +435,7 @@ static int getrs_apply(grim_context *h, int n, int nrhs, const C *LU, int64_t ld
         GRIM_CHECK_LAUNCH_W(h, kname("k_trsm_diag", sizeof(C)), 4.0 * nbj * nbj * nrhs, 0);
         const int below = n - j - nbj;
         if (below > 0)
-            GRIM_TRY((gemm<C, C, C, C, true, true>(h, below, nrhs, nbj, LU + (int64_t)j * lda + j + nbj, lda, B + j, ldb,
+            GRIM_TRY((gemm_sub<C>(h, below, nrhs, nbj, LU + (int64_t)j * lda + j + nbj, lda, B + j, ldb,
                                                   B + j + nbj, ldb)));
     }
     for (int p = npan - 1; p >= 0; --p) {
@@ -372,7 +443,7 @@ static int getrs_apply(grim_context *h, int n, int nrhs, const C *LU, int64_t ld
         k_trsm_diag<C, true><<<ctiles, 4 * TRSM_COLS, tri, h->stream>>>(nrhs, LU, lda, B, ldb, j, nbj);
         GRIM_CHECK_LAUNCH_W(h, kname("k_trsm_diag", sizeof(C)), 4.0 * nbj * nbj * nrhs, 0);
         if (j > 0)
-            GRIM_TRY((gemm<C, C, C, C, true, true>(h, j, nrhs, nbj, LU + (int64_t)j * lda, lda, B + j, ldb, B, ldb)));
+            GRIM_TRY((gemm_sub<C>(h, j, nrhs, nbj, LU + (int64_t)j * lda, lda, B + j, ldb, B, ldb)));
     }
     return GRIM_OK;
 }

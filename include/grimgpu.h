@@ -110,6 +110,12 @@ int grim_cgetrf(grim_handle_t h, int n, void *A, int64_t lda, int *ipiv, int *in
 int grim_cgetrs(grim_handle_t h, int n, int nrhs, const void *LU, int64_t lda, const int *ipiv,
                 void *B, int64_t ldb);
 
+/* C[MxN] -= A[MxK] B[KxN], complex64 column-major: use_tensor_cores = 1 runs the tcgen05
+ * split-TF32 kernel used by grim_cgetrf / grim_cgetrs for their updates, 0 the SIMT kernel
+ * (reference: the BLAS zgemm calls inside LAPACK getrf/getrs, linalg/dense.py:139-155). */
+int grim_cgemm_sub(grim_handle_t h, int M, int N, int K, const void *A, int64_t lda, const void *B, int64_t ldb,
+                   void *C, int64_t ldc, int use_tensor_cores);
+
 /* Normwise backward error per column (reference twod/solver.py:695-720):
  * berr[j] = max_i |A x_j - b_j|_i / (||A||_inf max|x_j| + max|b_j|), A complex128 or complex64. */
 int grim_backward_error(grim_handle_t h, int n, int nrhs, const void *A, int64_t lda, int a_complex64,
