@@ -114,6 +114,8 @@ struct grim_context {
     std::unordered_map<std::string, std::pair<void *, size_t>> ws;
     grim_solve_info last{};
     int sm_count = 148;
+    // error flag of the tensor-core kernels (device int, zeroed at first use)
+    int *tc_err = nullptr;
     // profiling: one event per launch (plus a start event), aggregated by kernel name
     int profiling = 0;
     cudaEvent_t prof_start = nullptr;

@@ -18,6 +18,7 @@
 #include "lu.cuh"
 #include "bor.cuh"
 #include "tc_gemm.cuh"
+#include "ozaki.cuh"
 
 // ============================================================== errors
 static thread_local std::string g_last_error;
@@ -166,6 +167,10 @@ extern "C" int grim_destroy(grim_handle_t h) {
     if (!h) return GRIM_OK;
     DeviceGuard g(h->device);
     grim_release_workspace(h);
+    if (h->tc_err) {
+        cudaStreamSynchronize(h->stream);
+        cudaFree(h->tc_err);
+    }
     if (h->own_stream) cudaStreamDestroy(h->own_stream);
     delete h;
     return GRIM_OK;
@@ -280,33 +285,110 @@ static int tc_enabled() {
     return v;
 }
 
-// C[MxN] -= A[MxK] B[KxN] (complex64, column-major) on tcgen05 (split TF32).
+// Device error flag of the tensor-core kernels: zeroed once per context; a set flag is
+// reported (and cleared) by the next tc_err_check.
+static int tc_err_flag(grim_context *h, int **out) {
+    if (!h->tc_err) {
+        void *p = nullptr;
+        GRIM_CHECK_CUDA(cudaMalloc(&p, sizeof(int)));
+        GRIM_CHECK_CUDA(cudaMemsetAsync(p, 0, sizeof(int), h->stream));
+        h->tc_err = (int *)p;
+    }
+    *out = h->tc_err;
+    return GRIM_OK;
+}
+
+// Host read of the flag (synchronises the stream; called where the host waits anyway).
+static int tc_err_check(grim_context *h, const char *what) {
+    if (!h->tc_err) return GRIM_OK;
+    int v = 0;
+    GRIM_CHECK_CUDA(cudaMemcpyAsync(&v, h->tc_err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    GRIM_CHECK_CUDA(cudaStreamSynchronize(h->stream));
+    if (v) {
+        GRIM_CHECK_CUDA(cudaMemsetAsync(h->tc_err, 0, sizeof(int), h->stream));
+        return grim_fail(GRIM_ERR_CUDA, std::string(what) + ": tensor-core pipeline wait timed out");
+    }
+    return GRIM_OK;
+}
+
+// A packed tensor-core operand (tile layout of tc_gemm.cuh): hi and lo arrays of
+// rows_p x kp floats.
+struct TcPacked {
+    float *hi = nullptr, *lo = nullptr;
+    int rows_p = 0, kp = 0;
+};
+
+static int tc_ws(grim_context *h, const char *name, int rows_p, int kp, TcPacked *out) {
+    void *p = nullptr;
+    GRIM_TRY(grim_workspace(h, name, 2 * (size_t)rows_p * kp * sizeof(float), &p));
+    out->hi = (float *)p;
+    out->lo = out->hi + (size_t)rows_p * kp;
+    out->rows_p = rows_p;
+    out->kp = kp;
+    return GRIM_OK;
+}
+
+static inline int tc_rows_a(int M) { return ceil_div(2 * M, TC_BM) * TC_BM; }
+static inline int tc_kp(int K) { return ceil_div(2 * K, TC_BK) * TC_BK; }
+// Output-tile width: 128 columns for wide right-hand sides, 64 otherwise.
+static inline int tc_bn(int N) { return N > 192 ? 128 : 64; }
+
+static int tc_pack_a(grim_context *h, int M, int K, const float2 *A, int64_t lda, float sign, const TcPacked &P) {
+    const int64_t chunks = (int64_t)P.rows_p * (P.kp / 4);
+    k_tc_pack_a<<<ceil_div(chunks, 256), 256, 0, h->stream>>>(M, K, A, lda, P.hi, P.lo, P.rows_p, P.kp, sign);
+    GRIM_CHECK_LAUNCH_W(h, "k_tc_pack_a", 0.0, 8.0 * M * K + 32.0 * chunks);
+    return GRIM_OK;
+}
+
+static int tc_pack_b(grim_context *h, int K, int N, const float2 *B, int64_t ldb, const TcPacked &P) {
+    const int64_t chunks = (int64_t)P.rows_p * (P.kp / 4);
+    k_tc_pack_b<<<ceil_div(chunks, 256), 256, 0, h->stream>>>(K, N, B, ldb, P.hi, P.lo, P.rows_p, P.kp);
+    GRIM_CHECK_LAUNCH_W(h, "k_tc_pack_b", 0.0, 8.0 * K * N + 32.0 * chunks);
+    return GRIM_OK;
+}
+
+template <int BN, int STAGES>
+static int tc_launch(grim_context *h, const TcPacked &A, const TcPacked &B, float2 *C, int64_t ldc, int M, int N,
+                     int Kc, float alpha, int ow_lo, int ow_hi, int *err) {
+    static bool attr = false;
+    if (!attr) {
+        GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_tc_gemm<BN, STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             TcCfg<BN, STAGES>::SMEM_BYTES));
+        attr = true;
+    }
+    dim3 grid(A.rows_p / TC_BM, B.rows_p / BN);
+    k_tc_gemm<BN, STAGES><<<grid, TC_THREADS, TcCfg<BN, STAGES>::SMEM_BYTES, h->stream>>>(
+        A.kp / TC_BK, A.hi, A.lo, A.rows_p, B.hi, B.lo, B.rows_p, (float *)C, 2 * ldc, 2 * M, N, alpha, 2 * ow_lo,
+        2 * ow_hi, err);
+    GRIM_CHECK_LAUNCH_W(h, BN == 128 ? "k_tc_gemm<128>" : "k_tc_gemm<64>", 8.0 * M * N * Kc,
+                        8.0 * ((double)A.rows_p * A.kp * (B.rows_p / BN) + (double)B.rows_p * B.kp) + 16.0 * M * N);
+    return GRIM_OK;
+}
+
+// C[M x N] = (complex rows in [ow_lo, ow_hi) ? 0 : C) + alpha * A B with packed A (2M real
+// rows) and B (rows padded to bn); Kc is the complex inner dimension (for the flop count).
+static int tc_gemm_packed(grim_context *h, int bn, const TcPacked &A, const TcPacked &B, float2 *C, int64_t ldc,
+                          int M, int N, int Kc, float alpha, int ow_lo, int ow_hi) {
+    if (M <= 0 || N <= 0) return GRIM_OK;
+    if (A.kp != B.kp || B.rows_p % bn || A.rows_p % TC_BM || A.rows_p < 2 * M || B.rows_p < N)
+        return grim_fail(GRIM_ERR_ARGUMENT, "tensor-core GEMM: packed operand shapes disagree");
+    int *err;
+    GRIM_TRY(tc_err_flag(h, &err));
+    if (bn == 128) return tc_launch<128, 3>(h, A, B, C, ldc, M, N, Kc, alpha, ow_lo, ow_hi, err);
+    return tc_launch<64, 4>(h, A, B, C, ldc, M, N, Kc, alpha, ow_lo, ow_hi, err);
+}
+
+// C[MxN] -= A B[KxN] (complex64, column-major) on tcgen05 (split TF32), packing both operands.
 static int tc_cgemm_sub(grim_context *h, int M, int N, int K, const float2 *A, int64_t lda, const float2 *B,
                         int64_t ldb, float2 *C, int64_t ldc) {
     if (M <= 0 || N <= 0 || K <= 0) return GRIM_OK;
-    static bool attr = false;
-    if (!attr) {
-        GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_tc_gemm_sub, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM_BYTES));
-        attr = true;
-    }
-    const int Mp = ceil_div(2 * M, TC_BM) * TC_BM, Np = ceil_div(N, TC_BN) * TC_BN, Kp = ceil_div(2 * K, TC_BK) * TC_BK;
-    void *pa = nullptr, *pb = nullptr, *pe = nullptr;
-    GRIM_TRY(grim_workspace(h, "tc_a", 2 * (size_t)Mp * Kp * sizeof(float), &pa));
-    GRIM_TRY(grim_workspace(h, "tc_b", 2 * (size_t)Np * Kp * sizeof(float), &pb));
-    GRIM_TRY(grim_workspace(h, "tc_err", sizeof(int), &pe));
-    GRIM_CHECK_CUDA(cudaMemsetAsync(pe, 0, sizeof(int), h->stream));
-    float *ahi = (float *)pa, *alo = ahi + (size_t)Mp * Kp, *bhi = (float *)pb, *blo = bhi + (size_t)Np * Kp;
-    const int64_t na = (int64_t)Mp * Kp, nb = (int64_t)Np * Kp;
-    k_tc_pack_a<<<ceil_div(na, 256), 256, 0, h->stream>>>(M, K, A, lda, ahi, alo, Mp, Kp);
-    GRIM_CHECK_LAUNCH(h, "k_tc_pack_a");
-    k_tc_pack_b<<<ceil_div(nb, 256), 256, 0, h->stream>>>(K, N, B, ldb, bhi, blo, Np, Kp);
-    GRIM_CHECK_LAUNCH(h, "k_tc_pack_b");
-    dim3 grid(Mp / TC_BM, Np / TC_BN);
-    k_tc_gemm_sub<<<grid, TC_THREADS, TC_SMEM_BYTES, h->stream>>>(Kp, ahi, alo, bhi, blo, (float *)C, 2 * ldc, 2 * M, N,
-                                                                  (int *)pe);
-    GRIM_CHECK_LAUNCH_W(h, "k_tc_gemm_sub", 8.0 * M * N * K,
-                        4.0 * 2 * ((double)Mp * Kp + (double)Np * Kp) + 2.0 * 8 * M * N);
-    return GRIM_OK;
+    const int bn = tc_bn(N), Kp = tc_kp(K);
+    TcPacked pa, pb;
+    GRIM_TRY(tc_ws(h, "tc_a", tc_rows_a(M), Kp, &pa));
+    GRIM_TRY(tc_ws(h, "tc_b", ceil_div(N, bn) * bn, Kp, &pb));
+    GRIM_TRY(tc_pack_a(h, M, K, A, lda, 1.f, pa));
+    GRIM_TRY(tc_pack_b(h, K, N, B, ldb, pb));
+    return tc_gemm_packed(h, bn, pa, pb, C, ldc, M, N, K, -1.f, 0, 0);
 }
 
 // Trailing / solve updates C -= A B: tensor cores for complex64 (unless disabled), SIMT otherwise.
@@ -327,13 +409,7 @@ extern "C" int grim_cgemm_sub(grim_handle_t h, int M, int N, int K, const void *
     DeviceGuard g(h->device);
     if (use_tensor_cores) {
         GRIM_TRY(tc_cgemm_sub(h, M, N, K, (const float2 *)A, lda, (const float2 *)B, ldb, (float2 *)Cm, ldc));
-        void *pe = nullptr;
-        GRIM_TRY(grim_workspace(h, "tc_err", sizeof(int), &pe));
-        int err = 0;
-        GRIM_CHECK_CUDA(cudaMemcpyAsync(&err, pe, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
-        GRIM_CHECK_CUDA(cudaStreamSynchronize(h->stream));
-        if (err) return grim_fail(GRIM_ERR_CUDA, "grim_cgemm_sub: tensor-core pipeline wait timed out");
-        return GRIM_OK;
+        return tc_err_check(h, "grim_cgemm_sub");
     }
     return gemm<float2, float2, float2, float2, true, true>(h, M, N, K, (const float2 *)A, lda, (const float2 *)B, ldb,
                                                           (float2 *)Cm, ldc);
@@ -401,6 +477,7 @@ static int getrf_impl(grim_context *h, int n, C *A, int64_t lda, int *ipiv, int 
     int hostf[2] = {0, 0};
     GRIM_CHECK_CUDA(cudaMemcpyAsync(hostf, flags, 2 * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
     GRIM_CHECK_CUDA(cudaStreamSynchronize(h->stream));
+    if (sizeof(C) == sizeof(float2)) GRIM_TRY(tc_err_check(h, "getrf"));
     if (info_host) *info_host = hostf[0];
     h->last.pivoted_panels = hostf[1];
     h->last.info = hostf[0];
@@ -459,6 +536,115 @@ static int getrs_impl(grim_context *h, int n, int nrhs, const C *LU, int64_t lda
     return getrs_apply<C>(h, n, nrhs, LU, lda, ipiv, ident, B, ldb);
 }
 
+// ------------------------------------------------ complex64 getrs on packed block panels
+// For many right-hand sides the two triangular solves run in GS_NB-row blocks, each block
+// one tensor-core GEMM with a panel formed once per factorization:
+//   forward  (L unit lower), block i at rows J..J+nb:  PL_i = [Linv_ii; -L_below,i Linv_ii]
+//            B[J:n] = [0; B[J+nb:n]] + PL_i B[J:J+nb]
+//   backward (U upper),      block i:                  PU_i = [-U_above,i Uinv_ii; Uinv_ii]
+//            B[0:J+nb] = [B[0:J]; 0] + PU_i B[J:J+nb]
+// PL_i is the forward substitution of the 64-row diagonal steps inside block i applied to
+// [I; 0], PU_i the backward one applied to [0; I]; both are packed (split TF32, tile
+// layout) and kept for every solve of a refinement loop.  The block solve multiplies by
+// the inverse of a triangular diagonal block instead of substituting; its rounding is
+// that of an FP32 GEMM, and the FP64 refinement that consumes these solves removes it.
+#define GS_NB 256
+
+struct GsPanels {
+    int n = 0, nblk = 0;
+    std::vector<TcPacked> L, U;
+};
+
+static int gs_build(grim_context *h, int n, const float2 *LU, int64_t lda, GsPanels *P) {
+    const int nblk = ceil_div(n, GS_NB);
+    size_t floats_l = 0, floats_u = 0;
+    for (int i = 0; i < nblk; ++i) {
+        const int J = i * GS_NB, nbj = std::min(GS_NB, n - J);
+        floats_l += 2 * (size_t)tc_rows_a(n - J) * tc_kp(nbj);
+        floats_u += 2 * (size_t)tc_rows_a(J + nbj) * tc_kp(nbj);
+    }
+    void *pl = nullptr, *pu = nullptr, *pe = nullptr;
+    GRIM_TRY(grim_workspace(h, "gs_l", floats_l * sizeof(float), &pl));
+    GRIM_TRY(grim_workspace(h, "gs_u", floats_u * sizeof(float), &pu));
+    GRIM_TRY(grim_workspace(h, "gs_e", (size_t)n * GS_NB * sizeof(float2), &pe));
+    float2 *E = (float2 *)pe;
+    P->n = n;
+    P->nblk = nblk;
+    P->L.assign(nblk, TcPacked{});
+    P->U.assign(nblk, TcPacked{});
+    const size_t tri = (size_t)(NB * NBP + NB) * sizeof(float2);
+    float *fl = (float *)pl, *fu = (float *)pu;
+    for (int i = 0; i < nblk; ++i) {
+        const int J = i * GS_NB, nbj = std::min(GS_NB, n - J), kp = tc_kp(nbj);
+        const int ctiles = ceil_div(nbj, TRSM_COLS);
+        // forward panel: rows J..n of [I; 0] through the diagonal steps of block i
+        const int rl = n - J;
+        k_set_unit<float2><<<dim3(ceil_div(rl, 256), nbj), 256, 0, h->stream>>>(rl, nbj, E, rl, 0);
+        GRIM_CHECK_LAUNCH(h, "k_set_unit");
+        for (int j = J; j < J + nbj; j += NB) {
+            const int nb = std::min(NB, J + nbj - j);
+            k_trsm_diag<float2, false><<<ctiles, 4 * TRSM_COLS, tri, h->stream>>>(nbj, LU + (int64_t)J * lda + J, lda,
+                                                                                  E, rl, j - J, nb);
+            GRIM_CHECK_LAUNCH_W(h, "k_trsm_diag<c64>", 4.0 * nb * nb * nbj, 0);
+            const int below = n - j - nb;
+            if (below > 0)
+                GRIM_TRY((gemm_sub<float2>(h, below, nbj, nb, LU + (int64_t)j * lda + j + nb, lda, E + (j - J), rl,
+                                           E + (j - J) + nb, rl)));
+        }
+        TcPacked &pli = P->L[i];
+        pli.hi = fl;
+        pli.rows_p = tc_rows_a(rl);
+        pli.kp = kp;
+        pli.lo = fl + (size_t)pli.rows_p * kp;
+        fl += 2 * (size_t)pli.rows_p * kp;
+        GRIM_TRY(tc_pack_a(h, rl, nbj, E, rl, 1.f, pli));
+        // backward panel: rows 0..J+nbj of [0; I] through the diagonal steps of block i
+        const int ru = J + nbj;
+        k_set_unit<float2><<<dim3(ceil_div(ru, 256), nbj), 256, 0, h->stream>>>(ru, nbj, E, ru, J);
+        GRIM_CHECK_LAUNCH(h, "k_set_unit");
+        for (int j = J + ((nbj - 1) / NB) * NB; j >= J; j -= NB) {
+            const int nb = std::min(NB, J + nbj - j);
+            k_trsm_diag<float2, true><<<ctiles, 4 * TRSM_COLS, tri, h->stream>>>(nbj, LU, lda, E, ru, j, nb);
+            GRIM_CHECK_LAUNCH_W(h, "k_trsm_diag<c64>", 4.0 * nb * nb * nbj, 0);
+            if (j > 0) GRIM_TRY((gemm_sub<float2>(h, j, nbj, nb, LU + (int64_t)j * lda, lda, E + j, ru, E, ru)));
+        }
+        TcPacked &pui = P->U[i];
+        pui.hi = fu;
+        pui.rows_p = tc_rows_a(ru);
+        pui.kp = kp;
+        pui.lo = fu + (size_t)pui.rows_p * kp;
+        fu += 2 * (size_t)pui.rows_p * kp;
+        GRIM_TRY(tc_pack_a(h, ru, nbj, E, ru, 1.f, pui));
+    }
+    return GRIM_OK;
+}
+
+static int gs_apply(grim_context *h, const GsPanels &P, int nrhs, const int *ipiv, const int *ident, float2 *B,
+                    int64_t ldb) {
+    const int n = P.n;
+    k_laswp_rhs<float2><<<ceil_div(nrhs, 128), 128, 0, h->stream>>>(n, nrhs, B, ldb, ipiv, ident);
+    GRIM_CHECK_LAUNCH(h, "k_laswp_rhs<c64>");
+    const int bn = tc_bn(nrhs), np = ceil_div(nrhs, bn) * bn;
+    TcPacked pb;
+    GRIM_TRY(tc_ws(h, "gs_b", np, tc_kp(GS_NB), &pb));
+    for (int i = 0; i < P.nblk; ++i) {
+        const int J = i * GS_NB, nbj = std::min(GS_NB, n - J);
+        pb.kp = P.L[i].kp;
+        GRIM_TRY(tc_pack_b(h, nbj, nrhs, B + J, ldb, pb));
+        GRIM_TRY(tc_gemm_packed(h, bn, P.L[i], pb, B + J, ldb, n - J, nrhs, nbj, 1.f, 0, nbj));
+    }
+    for (int i = P.nblk - 1; i >= 0; --i) {
+        const int J = i * GS_NB, nbj = std::min(GS_NB, n - J);
+        pb.kp = P.U[i].kp;
+        GRIM_TRY(tc_pack_b(h, nbj, nrhs, B + J, ldb, pb));
+        GRIM_TRY(tc_gemm_packed(h, bn, P.U[i], pb, B, ldb, J + nbj, nrhs, nbj, 1.f, J, J + nbj));
+    }
+    return GRIM_OK;
+}
+
+// The packed-panel solve pays for itself with wide right-hand sides on tensor cores.
+static bool gs_wanted(int n, int nrhs) { return tc_enabled() && n >= 2 * GS_NB && nrhs >= 128; }
+
 extern "C" int grim_zgetrf(grim_handle_t h, int n, void *A, int64_t lda, int *ipiv, int *info) {
     return getrf_impl<double2>(h, n, (double2 *)A, lda, ipiv, info);
 }
@@ -477,6 +663,19 @@ extern "C" int grim_cgetrs(grim_handle_t h, int n, int nrhs, const void *LU, int
 // ============================================================== residual / backward error
 // R = B - A X (FP64 arithmetic; A complex128 or complex64), then per-column maxima and the
 // normwise backward error.  maxes_dev[0] = max berr, [1] = max relative residual.
+// Backward error and relative residual per column from an existing residual R.
+static int berr_from_residual(grim_context *h, int n, int nrhs, const double2 *R, int64_t ldr, const double2 *X,
+                              int64_t ldx, const double2 *B, int64_t ldb, const double *anorm, double *berr,
+                              double *relres, double *maxes) {
+    void *p = nullptr;
+    GRIM_TRY(grim_workspace(h, "berr_absmax", (size_t)3 * nrhs * sizeof(double), &p));
+    k_col_absmax3<double2><<<nrhs, 256, 0, h->stream>>>(n, R, ldr, X, ldx, B, ldb, (double *)p);
+    GRIM_CHECK_LAUNCH(h, "k_col_absmax3");
+    k_berr_finish<<<1, 1024, 0, h->stream>>>(nrhs, (const double *)p, anorm, berr, relres, maxes);
+    GRIM_CHECK_LAUNCH(h, "k_berr_finish");
+    return GRIM_OK;
+}
+
 template <typename TA>
 static int residual_and_berr(grim_context *h, int n, int nrhs, const TA *A, int64_t lda, const double2 *X, int64_t ldx,
                              const double2 *B, int64_t ldb, double2 *R, int64_t ldr, const double *anorm, double *berr,
@@ -484,12 +683,77 @@ static int residual_and_berr(grim_context *h, int n, int nrhs, const TA *A, int6
     GRIM_CHECK_CUDA(cudaMemcpy2DAsync(R, ldr * sizeof(double2), B, ldb * sizeof(double2), n * sizeof(double2), nrhs,
                                       cudaMemcpyDeviceToDevice, h->stream));
     GRIM_TRY((gemm<double2, TA, double2, double2, true, true>(h, n, nrhs, n, A, lda, X, ldx, R, ldr)));
-    void *p = nullptr;
-    GRIM_TRY(grim_workspace(h, "berr_absmax", (size_t)3 * nrhs * sizeof(double), &p));
-    k_col_absmax3<double2><<<nrhs, 256, 0, h->stream>>>(n, R, ldr, X, ldx, B, ldb, (double *)p);
-    GRIM_CHECK_LAUNCH(h, "k_col_absmax3");
-    k_berr_finish<<<1, 1024, 0, h->stream>>>(nrhs, (const double *)p, anorm, berr, relres, maxes);
-    GRIM_CHECK_LAUNCH(h, "k_berr_finish");
+    return berr_from_residual(h, n, nrhs, R, ldr, X, ldx, B, ldb, anorm, berr, relres, maxes);
+}
+
+// ------------------------------------------------ residual on the integer tensor cores
+// A~ cut once into OZ_SLICES int8 slices (ozaki.cuh); every residual then slices X and
+// runs one k_oz_gemm (BN 64, 8 accumulators = all 512 tensor-memory columns).
+#define OZ_SLICES 8
+#define OZ_BN 64
+
+struct OzA {
+    int n = 0, S = 0, Rp = 0;
+    int8_t *Q = nullptr;
+    int *row_exp = nullptr;
+};
+
+// int32 accumulators hold S products of 2n terms of at most 64^2.
+static bool oz_fits(int n, int S) { return (double)S * 2.0 * n * 64.0 * 64.0 < 2147483647.0; }
+
+template <typename TA>
+static int oz_prepare_a(grim_context *h, int n, const TA *A, int64_t lda, int S, OzA *out) {
+    if (S != OZ_SLICES) return grim_fail(GRIM_ERR_ARGUMENT, "integer-slice residual: unsupported slice count");
+    const int Rp = ceil_div(2 * n, 128) * 128;
+    void *pq = nullptr, *pm = nullptr, *pe = nullptr;
+    GRIM_TRY(grim_workspace(h, "oz_q", (size_t)S * Rp * Rp, &pq));
+    GRIM_TRY(grim_workspace(h, "oz_rowmax", (size_t)n * sizeof(unsigned long long), &pm));
+    GRIM_TRY(grim_workspace(h, "oz_rowexp", (size_t)n * sizeof(int), &pe));
+    GRIM_CHECK_CUDA(cudaMemsetAsync(pm, 0, (size_t)n * sizeof(unsigned long long), h->stream));
+    k_oz_rowmax<TA><<<dim3(ceil_div(n, 256), 32), 256, 0, h->stream>>>(n, A, lda, (unsigned long long *)pm);
+    GRIM_CHECK_LAUNCH(h, "k_oz_rowmax");
+    const int64_t threads = (int64_t)(Rp / 2) * (Rp / 16);
+    k_oz_slice_a<TA, OZ_SLICES><<<ceil_div(threads, 256), 256, 0, h->stream>>>(
+        n, A, lda, (const unsigned long long *)pm, (int8_t *)pq, Rp, Rp, (int *)pe);
+    GRIM_CHECK_LAUNCH_W(h, "k_oz_slice_a", 0.0, (double)sizeof(TA) * n * n + (double)S * Rp * Rp);
+    out->n = n;
+    out->S = S;
+    out->Rp = Rp;
+    out->Q = (int8_t *)pq;
+    out->row_exp = (int *)pe;
+    return GRIM_OK;
+}
+
+// R = B - A X with A prepared by oz_prepare_a (R and B distinct).
+static int oz_residual(grim_context *h, const OzA &qa, int nrhs, const double2 *X, int64_t ldx, const double2 *B,
+                       int64_t ldb, double2 *R, int64_t ldr) {
+    using Cfg = OzCfg<OZ_SLICES, OZ_BN>;
+    const int n = qa.n, S = qa.S, Np = ceil_div(nrhs, OZ_BN) * OZ_BN, Kp = qa.Rp;
+    void *pp = nullptr, *pc = nullptr, *pe = nullptr;
+    GRIM_TRY(grim_workspace(h, "oz_p", (size_t)S * Np * Kp, &pp));
+    GRIM_TRY(grim_workspace(h, "oz_colmax", (size_t)nrhs * sizeof(double), &pc));
+    GRIM_TRY(grim_workspace(h, "oz_colexp", (size_t)nrhs * sizeof(int), &pe));
+    k_oz_colmax<<<nrhs, 256, 0, h->stream>>>(n, X, ldx, (double *)pc);
+    GRIM_CHECK_LAUNCH(h, "k_oz_colmax");
+    const int64_t threads = (int64_t)Np * (Kp / 16);
+    k_oz_slice_x<OZ_SLICES><<<ceil_div(threads, 256), 256, 0, h->stream>>>(n, nrhs, X, ldx, (const double *)pc,
+                                                                            (int8_t *)pp, Np, Kp, (int *)pe);
+    GRIM_CHECK_LAUNCH_W(h, "k_oz_slice_x", 0.0, 16.0 * n * nrhs + (double)S * Np * Kp);
+    int *err;
+    GRIM_TRY(tc_err_flag(h, &err));
+    static bool attr = false;
+    if (!attr) {
+        GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_oz_gemm<OZ_SLICES, OZ_BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             Cfg::SMEM_BYTES));
+        attr = true;
+    }
+    dim3 grid(qa.Rp / TC_BM, Np / OZ_BN);
+    k_oz_gemm<OZ_SLICES, OZ_BN><<<grid, TC_THREADS, Cfg::SMEM_BYTES, h->stream>>>(
+        qa.Rp / OZ_KT, qa.Q, qa.Rp, (const int8_t *)pp, Np, Kp, qa.row_exp, (const int *)pe, (const double *)B,
+        2 * ldb, (double *)R, 2 * ldr, 2 * n, nrhs, err);
+    GRIM_CHECK_LAUNCH_W(h, "k_oz_gemm", 8.0 * n * n * nrhs,
+                        (double)S * qa.Rp * qa.Rp * (Np / OZ_BN) + (double)S * Np * Kp * (qa.Rp / TC_BM) +
+                            32.0 * n * nrhs);
     return GRIM_OK;
 }
 
@@ -529,6 +793,32 @@ extern "C" int grim_backward_error(grim_handle_t h, int n, int nrhs, const void 
     return GRIM_OK;
 }
 
+// Test / diagnostic entry: R = B - A X with the FP64 SIMT GEMM (slices 0) or on the integer
+// tensor cores with 8 int8 slices per operand.
+extern "C" int grim_residual(grim_handle_t h, int n, int nrhs, const void *A, int64_t lda, int a_complex64,
+                             const void *X, int64_t ldx, const void *B, int64_t ldb, void *R, int64_t ldr, int slices) {
+    if (!h || n <= 0 || nrhs <= 0 || !A || !X || !B || !R || lda < n || ldx < n || ldb < n || ldr < n ||
+        (slices != 0 && slices != OZ_SLICES) || (slices && !oz_fits(n, slices)))
+        return grim_fail(GRIM_ERR_ARGUMENT, "grim_residual: bad arguments");
+    DeviceGuard g(h->device);
+    const double2 *Xd = (const double2 *)X, *Bd = (const double2 *)B;
+    double2 *Rd = (double2 *)R;
+    if (slices == 0) {
+        GRIM_CHECK_CUDA(cudaMemcpy2DAsync(Rd, ldr * sizeof(double2), Bd, ldb * sizeof(double2), n * sizeof(double2),
+                                          nrhs, cudaMemcpyDeviceToDevice, h->stream));
+        if (a_complex64)
+            return gemm<double2, float2, double2, double2, true, true>(h, n, nrhs, n, (const float2 *)A, lda, Xd, ldx,
+                                                                       Rd, ldr);
+        return gemm<double2, double2, double2, double2, true, true>(h, n, nrhs, n, (const double2 *)A, lda, Xd, ldx, Rd,
+                                                                    ldr);
+    }
+    OzA qa;
+    if (a_complex64) GRIM_TRY(oz_prepare_a(h, n, (const float2 *)A, lda, slices, &qa));
+    else GRIM_TRY(oz_prepare_a(h, n, (const double2 *)A, lda, slices, &qa));
+    GRIM_TRY(oz_residual(h, qa, nrhs, Xd, ldx, Bd, ldb, Rd, ldr));
+    return tc_err_check(h, "grim_residual");
+}
+
 // ============================================================== solve (FP64 or mixed)
 template <typename TA>
 static int mixed_refine(grim_context *h, int n, int nrhs, const TA *Ares, int64_t ldres, float2 *lu32, const int *ipiv,
@@ -551,20 +841,37 @@ static int mixed_refine(grim_context *h, int n, int nrhs, const TA *Ares, int64_
     int *ident;
     GRIM_TRY(smem_opt_in<float2>());
     GRIM_TRY(getrs_prepare<float2>(h, n, ipiv, &ident));
+    GsPanels panels;
+    const bool use_gs = gs_wanted(n, nrhs);
+    if (use_gs) GRIM_TRY(gs_build(h, n, lu32, n, &panels));
+    auto solve32 = [&](float2 *X32) -> int {
+        if (use_gs) return gs_apply(h, panels, nrhs, ipiv, ident, X32, n);
+        return getrs_apply<float2>(h, n, nrhs, lu32, n, ipiv, ident, X32, n);
+    };
     k_convert<float2, double2><<<eg, 256, 0, h->stream>>>(n, nrhs, B0, n, R32, n);
     GRIM_CHECK_LAUNCH(h, "k_convert");
-    GRIM_TRY(getrs_apply<float2>(h, n, nrhs, lu32, n, ipiv, ident, R32, n));
+    GRIM_TRY(solve32(R32));
     k_convert<double2, float2><<<eg, 256, 0, h->stream>>>(n, nrhs, R32, n, X, n);
     GRIM_CHECK_LAUNCH(h, "k_convert");
     double prev = INFINITY;
     int steps = 0;
     double berr = INFINITY, relres = INFINITY, first = -1.0;
     int status = GRIM_OK;
+    // residuals on the integer tensor cores when the slice accumulators fit
+    OzA qa;
+    const bool use_oz = tc_enabled() && n >= 256 && nrhs >= 16 && oz_fits(n, OZ_SLICES);
+    if (use_oz) GRIM_TRY(oz_prepare_a(h, n, Ares, ldres, OZ_SLICES, &qa));
     for (int it = 0; it <= max_iter; ++it) {
-        GRIM_TRY(residual_and_berr(h, n, nrhs, Ares, ldres, X, n, B0, n, R, n, sc, nullptr, nullptr, sc + 1));
+        if (use_oz) {
+            GRIM_TRY(oz_residual(h, qa, nrhs, X, n, B0, n, R, n));
+            GRIM_TRY(berr_from_residual(h, n, nrhs, R, n, X, n, B0, n, sc, nullptr, nullptr, sc + 1));
+        } else {
+            GRIM_TRY(residual_and_berr(h, n, nrhs, Ares, ldres, X, n, B0, n, R, n, sc, nullptr, nullptr, sc + 1));
+        }
         double hv[2];
         GRIM_CHECK_CUDA(cudaMemcpyAsync(hv, sc + 1, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
         GRIM_CHECK_CUDA(cudaStreamSynchronize(h->stream));
+        GRIM_TRY(tc_err_check(h, "mixed-precision solve"));
         berr = hv[0];
         relres = hv[1];
         if (first < 0) first = berr;
@@ -580,7 +887,7 @@ static int mixed_refine(grim_context *h, int n, int nrhs, const TA *Ares, int64_
         prev = relres;
         k_convert<float2, double2><<<eg, 256, 0, h->stream>>>(n, nrhs, R, n, R32, n);
         GRIM_CHECK_LAUNCH(h, "k_convert");
-        GRIM_TRY(getrs_apply<float2>(h, n, nrhs, lu32, n, ipiv, ident, R32, n));
+        GRIM_TRY(solve32(R32));
         k_add_update<float2><<<eg, 256, 0, h->stream>>>(n, nrhs, X, n, R32, n);
         GRIM_CHECK_LAUNCH(h, "k_add_update");
         ++steps;

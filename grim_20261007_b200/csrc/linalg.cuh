@@ -139,3 +139,13 @@ __global__ void k_berr_finish(int ncol, const double *absmax3, const double *ano
         if (lane == 0) { maxes[0] = mb; maxes[1] = mr; }
     }
 }
+
+// E[rows x cols] = 0 except E[row_off + c, c] = 1 (a shifted identity block).
+template <typename C>
+__global__ void k_set_unit(int rows, int cols, C *__restrict__ E, int64_t lde, int row_off) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x, c = blockIdx.y;
+    if (r >= rows || c >= cols) return;
+    C v = czero<C>();
+    if (r == row_off + c) v.x = 1;
+    E[(int64_t)c * lde + r] = v;
+}

@@ -1,33 +1,50 @@
-// Complex64 GEMM update C -= A B on the 5th-generation tensor cores (tcgen05, kind::tf32),
-// with FP32-level accuracy from a split-TF32 product: x = hi + lo (hi = tf32(x),
-// lo = tf32(x - hi)) and A B ~ A_hi B_hi + A_hi B_lo + A_lo B_hi, all accumulated in FP32
-// in tensor memory.
+// Complex64 GEMM on the 5th-generation tensor cores (tcgen05, kind::tf32) with FP32-level
+// accuracy from a split-TF32 product: x = hi + lo (hi = tf32(x), lo = tf32(x - hi)) and
+// A B ~ A_hi B_hi + A_hi B_lo + A_lo B_hi, all accumulated in FP32 in tensor memory.
 //
 // Complex -> real: with C and B viewed as interleaved real column-major matrices
 // (C^ is 2M x N, B^ is 2K x N), C^ = A~ B^ where A~ (2M x 2K) expands every complex a into
-// the 2 x 2 block [re -im; im re].  The operands are packed once into K-major row-major
-// float arrays (k_tc_pack_a: A~ rows of length 2K; k_tc_pack_b: B^ columns of length 2K),
-// split into hi and lo, zero padded to the tile grid.
+// the 2 x 2 block [re -im; im re].  No flop is wasted: 2M x N x 2K x 2 = 8 M N K.
 //
-// Tile: 128 real rows (64 complex rows) x 64 columns, K in stages of 32 floats (one
-// 128-byte row).  Shared-memory tiles use the canonical K-major 128-byte-swizzle layout
-// (8-row atoms of 1024 B, 16-byte chunk c of row r at chunk c ^ (r & 7)), filled with
-// cp.async by all 128 threads, two stages.  Thread 0 issues the tcgen05.mma
-// instructions (4 K-steps x 3 products per stage) into a 64-column FP32 accumulator in
-// tensor memory and commits them to the stage's mbarrier; all four warps then read the
-// accumulator with tcgen05.ld (warp w owns lanes 32w..32w+31 = rows) and apply C -= D.
-// Every mbarrier wait is bounded (about one second of clock); on timeout the kernel
-// records an error flag, stops issuing, frees its tensor memory and returns.
+// Packed operand layout ("tile layout"): a real operand of Rp rows x Kp columns (Rp a
+// multiple of the tile height, Kp a multiple of 32) is stored K-tile by K-tile; inside a
+// K-tile the Rp rows of 32 floats (128 bytes) follow each other, each row's 16-byte chunk
+// c stored at chunk c ^ (r & 7) -- the canonical K-major 128-byte-swizzle order of 8-row,
+// 1024-byte atoms.  Rows [r0, r0 + 128) of K-tile kt are therefore one contiguous, already
+// swizzled 16 KB block: a single cp.async.bulk moves it into shared memory, where the UMMA
+// descriptors read it directly.  Operands are packed once (hi and lo in separate arrays)
+// and can be reused by many GEMMs: the blocked triangular solves keep their packed panels
+// for every right-hand side of a refinement loop.
+//
+// Kernel (one 128 x BN output tile per CTA, STAGES-deep pipeline, 128 threads):
+//   warp 0, lane 0  producer: waits for a free stage, posts the expected byte count on the
+//                   stage's "full" mbarrier and issues 4 bulk copies (A hi/lo, B hi/lo);
+//   warp 1, lane 0  MMA issuer: waits for a full stage, issues 3 products x 4 K-steps of
+//                   tcgen05.mma (M 128, N BN, K 8) into a BN-column FP32 accumulator in
+//                   tensor memory, and commits to the stage's "empty" mbarrier, which frees
+//                   the stage for the producer once those MMAs have read it;
+//   warps 2-3       meanwhile prefetch this CTA's slice of C into L2;
+//   all 4 warps     epilogue after the final commit: tcgen05.ld of the accumulator (warp w
+//                   owns TMEM lanes 32w..32w+31 = output rows), then
+//                   C = (row in [ow_lo, ow_hi) ? 0 : C) + alpha * D, coalesced along rows.
+// Every mbarrier wait is bounded (about one second of clock).  On a timeout the kernel
+// records an error flag, stops issuing, waits (bounded) for the copies and MMAs it has in
+// flight, frees its tensor memory and returns.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
 
 #define TC_BM 128
-#define TC_BN 64
 #define TC_BK 32
 #define TC_THREADS 128
-#define TC_STAGE_BYTES (2 * TC_BM * TC_BK * 4 + 2 * TC_BN * TC_BK * 4)  // Ahi, Alo, Bhi, Blo
-#define TC_SMEM_BYTES (2 * TC_STAGE_BYTES + 1024)
+
+template <int BN, int STAGES>
+struct TcCfg {
+    static constexpr int A_BYTES = TC_BM * TC_BK * 4;              // one hi or lo A tile
+    static constexpr int B_BYTES = BN * TC_BK * 4;                 // one hi or lo B tile
+    static constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;  // Ahi, Alo, Bhi, Blo
+    static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024;
+};
 
 __device__ __forceinline__ float tf32_rna(float x) {
     uint32_t r;
@@ -35,38 +52,63 @@ __device__ __forceinline__ float tf32_rna(float x) {
     return __uint_as_float(r);
 }
 
-// A~ packing: hi/lo[r * Kp + c] for r < Mp (real rows), c < Kp (real K), zero padded.
-__global__ void k_tc_pack_a(int M, int K, const float2 *__restrict__ A, int64_t lda, float *__restrict__ hi,
-                            float *__restrict__ lo, int Mp, int Kp) {
-    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= (int64_t)Mp * Kp) return;
-    const int r = (int)(idx / Kp), c = (int)(idx % Kp);
-    const int m = r >> 1, t = r & 1, k = c >> 1, s = c & 1;
-    float v = 0.f;
-    if (m < M && k < K) {
-        const float2 a = A[(int64_t)k * lda + m];
-        v = t == 0 ? (s == 0 ? a.x : -a.y) : (s == 0 ? a.y : a.x);
-    }
-    const float h = tf32_rna(v);
-    hi[idx] = h;
-    lo[idx] = tf32_rna(v - h);
+// Float offset of element (r, k) in the tile layout of an operand with Rp rows.
+__host__ __device__ __forceinline__ int64_t tc_tile_offset(int r, int k, int Rp) {
+    return (int64_t)(k >> 5) * Rp * 32 + (int64_t)r * 32 + ((((k & 31) >> 2) ^ (r & 7)) << 2) + (k & 3);
 }
 
-// B^ packing: hi/lo[n * Kp + c] = (re, im) of B[c >> 1, n], n < Np, zero padded.
+__device__ __forceinline__ void tc_store_chunk(float *hi, float *lo, int64_t off, float v0, float v1, float v2,
+                                               float v3) {
+    const float h0 = tf32_rna(v0), h1 = tf32_rna(v1), h2 = tf32_rna(v2), h3 = tf32_rna(v3);
+    *reinterpret_cast<float4 *>(hi + off) = make_float4(h0, h1, h2, h3);
+    *reinterpret_cast<float4 *>(lo + off) =
+        make_float4(tf32_rna(v0 - h0), tf32_rna(v1 - h1), tf32_rna(v2 - h2), tf32_rna(v3 - h3));
+}
+
+// A~ (2M x 2K real, from complex M x K column-major A) into the tile layout, zero padded
+// to Mp x Kp and scaled by sign (+1 or -1).  One thread per 16-byte chunk; consecutive
+// threads take consecutive rows so that the complex reads are coalesced.
+__global__ void k_tc_pack_a(int M, int K, const float2 *__restrict__ A, int64_t lda, float *__restrict__ hi,
+                            float *__restrict__ lo, int Mp, int Kp, float sign) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (int64_t)Mp * (Kp >> 2)) return;
+    const int r = (int)(idx % Mp), k0 = (int)(idx / Mp) * 4;
+    const int m = r >> 1, t = r & 1, kc = k0 >> 1;
+    float v[4] = {0.f, 0.f, 0.f, 0.f};
+    if (m < M) {
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            if (kc + q < K) {
+                const float2 a = A[(int64_t)(kc + q) * lda + m];
+                v[2 * q] = sign * (t == 0 ? a.x : a.y);
+                v[2 * q + 1] = sign * (t == 0 ? -a.y : a.x);
+            }
+        }
+    }
+    tc_store_chunk(hi, lo, tc_tile_offset(r, k0, Mp), v[0], v[1], v[2], v[3]);
+}
+
+// B^ (rows n < Np, real columns 2k+s = (re, im) of B[k, n]) into the tile layout, zero
+// padded.  One thread per 16-byte chunk, consecutive threads along k (coalesced reads and
+// writes of a column).
 __global__ void k_tc_pack_b(int K, int N, const float2 *__restrict__ B, int64_t ldb, float *__restrict__ hi,
                             float *__restrict__ lo, int Np, int Kp) {
     const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= (int64_t)Np * Kp) return;
-    const int n = (int)(idx / Kp), c = (int)(idx % Kp);
-    const int k = c >> 1, s = c & 1;
-    float v = 0.f;
-    if (n < N && k < K) {
-        const float2 b = B[(int64_t)n * ldb + k];
-        v = s == 0 ? b.x : b.y;
+    const int kq = Kp >> 2;
+    if (idx >= (int64_t)Np * kq) return;
+    const int n = (int)(idx / kq), k0 = (int)(idx % kq) * 4, kc = k0 >> 1;
+    float v[4] = {0.f, 0.f, 0.f, 0.f};
+    if (n < N) {
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            if (kc + q < K) {
+                const float2 b = B[(int64_t)n * ldb + kc + q];
+                v[2 * q] = b.x;
+                v[2 * q + 1] = b.y;
+            }
+        }
     }
-    const float h = tf32_rna(v);
-    hi[idx] = h;
-    lo[idx] = tf32_rna(v - h);
+    tc_store_chunk(hi, lo, tc_tile_offset(n, k0, Np), v[0], v[1], v[2], v[3]);
 }
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -99,43 +141,70 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
     }
 }
 
-__device__ __forceinline__ void cp_async16(uint32_t dst, const void *src) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
 }
 
-// Load one stage: rows [row0, row0 + rows) of a packed array (row length Kp floats),
-// columns [k0, k0 + 32), into a swizzled tile at smem address tile.
-__device__ __forceinline__ void tc_load_tile(uint32_t tile, const float *__restrict__ src, int row0, int rows,
-                                             int Kp, int k0) {
-    for (int e = threadIdx.x; e < rows * 8; e += TC_THREADS) {
-        const int r = e >> 3, c = e & 7;
-        const uint32_t dst = tile + (uint32_t)((r >> 3) * 1024 + (r & 7) * 128 + ((c ^ (r & 7)) << 4));
-        cp_async16(dst, src + (int64_t)(row0 + r) * Kp + k0 + 4 * c);
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+// Plain (non-multicast) bulk copy global -> this CTA's shared memory, completing on bar.
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
+}
+
+__device__ __forceinline__ void umma_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+// D[tmem] (+)= A[sA] * B[sB]^T for one 32-float K-tile: 4 MMAs of K 8.
+__device__ __forceinline__ void umma_ktile_tf32(uint32_t tmem, uint32_t sA, uint32_t sB, uint32_t idesc, bool first) {
+#pragma unroll
+    for (int kk = 0; kk < TC_BK / 8; ++kk) {
+        const uint64_t da = umma_desc_sw128(sA + kk * 32);
+        const uint64_t db = umma_desc_sw128(sB + kk * 32);
+        const uint32_t acc = (first && kk == 0) ? 0u : 1u;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n\t}"
+            :
+            : "r"(tmem), "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0u)
+            : "memory");
     }
 }
 
-// C (interleaved complex64 viewed as real, column stride ldc_real floats) -= D.
-// grid = (Mp / 128, Np / 64).  Mvalid real rows and N columns are written.
+// C (interleaved complex64 viewed as real, column stride ldc_real floats):
+// C[m, n] = (m in [ow_lo, ow_hi) ? 0 : C[m, n]) + alpha * (A~ B^)[m, n]
+// for m < Mvalid, n < Nvalid.  grid = (Mp / 128, Np / BN); A and B in the tile layout.
+template <int BN, int STAGES>
 __global__ void __launch_bounds__(TC_THREADS)
-k_tc_gemm_sub(int Kp, const float *__restrict__ Ahi, const float *__restrict__ Alo, const float *__restrict__ Bhi,
-              const float *__restrict__ Blo, float *__restrict__ C, int64_t ldc_real, int Mvalid, int N, int *err) {
+k_tc_gemm(int nk, const float *__restrict__ Ahi, const float *__restrict__ Alo, int Mp, const float *__restrict__ Bhi,
+          const float *__restrict__ Blo, int Np, float *__restrict__ C, int64_t ldc_real, int Mvalid, int Nvalid,
+          float alpha, int ow_lo, int ow_hi, int *err) {
+    using Cfg = TcCfg<BN, STAGES>;
     extern __shared__ __align__(1024) unsigned char smem_dyn[];
-    __shared__ __align__(8) uint64_t bar[2];
+    __shared__ __align__(8) uint64_t full[STAGES], empty[STAGES], done;
     __shared__ uint32_t tmem_slot;
     __shared__ int s_fail;
-    // 1024-aligned stage bases inside the dynamic allocation
     const uint32_t base = (smem_addr(smem_dyn) + 1023u) & ~1023u;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int m0 = blockIdx.x * TC_BM, n0 = blockIdx.y * TC_BN;
+    const int m0 = blockIdx.x * TC_BM, n0 = blockIdx.y * BN;
     if (threadIdx.x == 0) {
         s_fail = 0;
-        for (int s = 0; s < 2; ++s)
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&bar[s])) : "memory");
+        for (int s = 0; s < STAGES; ++s) {
+            mbar_init(smem_addr(&full[s]), 1);
+            mbar_init(smem_addr(&empty[s]), 1);
+        }
+        mbar_init(smem_addr(&done), 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&tmem_slot)),
-                     "r"(TC_BN)
+                     "r"(BN)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
@@ -143,82 +212,101 @@ k_tc_gemm_sub(int Kp, const float *__restrict__ Ahi, const float *__restrict__ A
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = tmem_slot;
-    const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(TC_BN >> 3) << 17) |
-                           ((uint32_t)(TC_BM >> 4) << 24);
-    const int nk = Kp / TC_BK;
-    uint32_t uses[2] = {0u, 0u};
-    bool ok = true;
-    for (int kt = 0; kt < nk && ok; ++kt) {
-        const int st = kt & 1;
-        if (kt >= 2) {
-            if (!mbar_wait(smem_addr(&bar[st]), (uses[st] - 1) & 1)) ok = false;
-        }
-        if (__syncthreads_or(!ok)) {
-            ok = false;
-            break;
-        }
-        const uint32_t sA = base + st * TC_STAGE_BYTES;
-        const uint32_t sAl = sA + TC_BM * TC_BK * 4;
-        const uint32_t sB = sAl + TC_BM * TC_BK * 4;
-        const uint32_t sBl = sB + TC_BN * TC_BK * 4;
-        tc_load_tile(sA, Ahi, m0, TC_BM, Kp, kt * TC_BK);
-        tc_load_tile(sAl, Alo, m0, TC_BM, Kp, kt * TC_BK);
-        tc_load_tile(sB, Bhi, n0, TC_BN, Kp, kt * TC_BK);
-        tc_load_tile(sBl, Blo, n0, TC_BN, Kp, kt * TC_BK);
-        asm volatile("cp.async.commit_group;" ::: "memory");
-        asm volatile("cp.async.wait_group 0;" ::: "memory");
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const uint32_t pa[3] = {sA, sA, sAl}, pb[3] = {sB, sBl, sB};
-#pragma unroll
-            for (int pr = 0; pr < 3; ++pr) {
-#pragma unroll
-                for (int kk = 0; kk < TC_BK / 8; ++kk) {
-                    const uint64_t da = umma_desc_sw128(pa[pr] + kk * 32);
-                    const uint64_t db = umma_desc_sw128(pb[pr] + kk * 32);
-                    const uint32_t acc = (kt > 0 || pr > 0 || kk > 0) ? 1u : 0u;
-                    asm volatile(
-                        "{\n\t.reg .pred p;\n\t"
-                        "setp.ne.b32 p, %4, 0;\n\t"
-                        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n\t}"
-                        :
-                        : "r"(tmem), "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0u)
-                        : "memory");
+    volatile int *vfail = &s_fail;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            // producer
+            int issued = 0;
+            for (int kt = 0; kt < nk; ++kt) {
+                const int s = kt % STAGES;
+                if (kt >= STAGES && !mbar_wait(smem_addr(&empty[s]), ((kt / STAGES) + 1) & 1)) {
+                    *vfail = 1;
+                    break;
                 }
+                if (*vfail) break;
+                const uint32_t sA = base + s * Cfg::STAGE_BYTES, sAl = sA + Cfg::A_BYTES, sB = sAl + Cfg::A_BYTES,
+                               sBl = sB + Cfg::B_BYTES;
+                const uint32_t fb = smem_addr(&full[s]);
+                mbar_expect_tx(fb, Cfg::STAGE_BYTES);
+                const int64_t aoff = (int64_t)kt * Mp * 32 + (int64_t)m0 * 32;
+                const int64_t boff = (int64_t)kt * Np * 32 + (int64_t)n0 * 32;
+                bulk_g2s(sA, Ahi + aoff, Cfg::A_BYTES, fb);
+                bulk_g2s(sAl, Alo + aoff, Cfg::A_BYTES, fb);
+                bulk_g2s(sB, Bhi + boff, Cfg::B_BYTES, fb);
+                bulk_g2s(sBl, Blo + boff, Cfg::B_BYTES, fb);
+                issued = kt + 1;
             }
-            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                             smem_addr(&bar[st]))
-                         : "memory");
+            // on the failure path, copies issued but not yet consumed must land before exit
+            if (*vfail) {
+                for (int kt = (issued > STAGES ? issued - STAGES : 0); kt < issued; ++kt)
+                    mbar_wait(smem_addr(&full[kt % STAGES]), (kt / STAGES) & 1);
+            }
         }
-        uses[st]++;
+        __syncwarp();
+    } else if (warp == 1) {
+        if (lane == 0) {
+            // MMA issuer
+            const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(BN >> 3) << 17) |
+                                   ((uint32_t)(TC_BM >> 4) << 24);
+            for (int kt = 0; kt < nk; ++kt) {
+                const int s = kt % STAGES;
+                if (!mbar_wait(smem_addr(&full[s]), (kt / STAGES) & 1)) {
+                    *vfail = 1;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t sA = base + s * Cfg::STAGE_BYTES, sAl = sA + Cfg::A_BYTES, sB = sAl + Cfg::A_BYTES,
+                               sBl = sB + Cfg::B_BYTES;
+                umma_ktile_tf32(tmem, sA, sB, idesc, kt == 0);
+                umma_ktile_tf32(tmem, sA, sBl, idesc, false);
+                umma_ktile_tf32(tmem, sAl, sB, idesc, false);
+                umma_commit(smem_addr(&empty[s]));
+            }
+            umma_commit(smem_addr(&done));  // arrives once every MMA issued above has completed
+        }
+        __syncwarp();
+    } else {
+        // warps 2-3: pull this CTA's slice of C into L2 while the main loop runs
+        // (one 128-byte line per prefetch; rows of the overwrite window are not read)
+        const int lines_per_col = TC_BM / 32;
+        for (int e = threadIdx.x - 64; e < BN * lines_per_col; e += 64) {
+            const int n = n0 + e / lines_per_col, r = m0 + (e % lines_per_col) * 32;
+            if (n < Nvalid && r < Mvalid && !(r >= ow_lo && r + 32 <= ow_hi))
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(C + (int64_t)n * ldc_real + r));
+        }
     }
-    // wait for the last commit (it tracks every MMA issued before it)
-    if (ok && nk > 0) {
-        const int st = (nk - 1) & 1;
-        if (!mbar_wait(smem_addr(&bar[st]), (uses[st] - 1) & 1)) ok = false;
-    }
-    if (!ok) s_fail = 1;
+    // everyone: wait for the accumulator (bounded)
+    if (!mbar_wait(smem_addr(&done), 0)) *vfail = 1;
     __syncthreads();
-    if (s_fail) {
+    if (*vfail) {
         if (threadIdx.x == 0) atomicOr(err, 1);
     } else {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const int m = m0 + warp * 32 + lane;
-#pragma unroll
-        for (int c = 0; c < TC_BN; c += 8) {
-            uint32_t v[8];
+        const bool row_ok = m < Mvalid, ow = m >= ow_lo && m < ow_hi;
+#pragma unroll 1
+        for (int c = 0; c < BN; c += 16) {
+            uint32_t v[16];
             asm volatile(
-                "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+                "%14, %15}, [%16];"
+                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                  "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
                 : "r"(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c));
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-            if (m < Mvalid) {
+            if (row_ok) {
+                // all 16 loads first, then the stores (no load waits behind a store)
+                float cv[16];
 #pragma unroll
-                for (int j = 0; j < 8; ++j) {
+                for (int j = 0; j < 16; ++j) {
                     const int n = n0 + c + j;
-                    if (n < N) C[(int64_t)n * ldc_real + m] -= __uint_as_float(v[j]);
+                    cv[j] = (!ow && n < Nvalid) ? C[(int64_t)n * ldc_real + m] : 0.f;
+                }
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    const int n = n0 + c + j;
+                    if (n < Nvalid) C[(int64_t)n * ldc_real + m] = cv[j] + alpha * __uint_as_float(v[j]);
                 }
             }
         }
@@ -226,6 +314,6 @@ k_tc_gemm_sub(int Kp, const float *__restrict__ Ahi, const float *__restrict__ A
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     if (warp == 0) {
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_BN) : "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BN) : "memory");
     }
 }

@@ -116,6 +116,15 @@ int grim_cgetrs(grim_handle_t h, int n, int nrhs, const void *LU, int64_t lda, c
 int grim_cgemm_sub(grim_handle_t h, int M, int N, int K, const void *A, int64_t lda, const void *B, int64_t ldb,
                    void *C, int64_t ldc, int use_tensor_cores);
 
+/* R = B - A X (complex128 X, B, R; A complex64 if a_complex64 else complex128), the
+ * residual of the FP64 refinement (reference linalg/refined_lu.py:50-53, the numpy
+ * residual of RefinedLU).  slices = 0: FP64 SIMT GEMM; 8: int8 slicing of both
+ * operands on the tcgen05 integer tensor cores (error per product term below
+ * 2^-56 of max|A row| max|X column|, the accuracy of an FP64 GEMM), as used inside
+ * grim_zgesv_mixed.  R must not overlap B.  slices = 8 needs n < 32768. */
+int grim_residual(grim_handle_t h, int n, int nrhs, const void *A, int64_t lda, int a_complex64, const void *X,
+                  int64_t ldx, const void *B, int64_t ldb, void *R, int64_t ldr, int slices);
+
 /* Normwise backward error per column (reference twod/solver.py:695-720):
  * berr[j] = max_i |A x_j - b_j|_i / (||A||_inf max|x_j| + max|b_j|), A complex128 or complex64. */
 int grim_backward_error(grim_handle_t h, int n, int nrhs, const void *A, int64_t lda, int a_complex64,

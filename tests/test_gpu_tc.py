@@ -27,3 +27,76 @@ def test_tensor_core_cgemm_matches_reference(m, n, k):
         scale = np.sqrt(k) * 4.0
         err = np.max(np.abs(got - ref)) / scale
         assert err < (1e-5 if tc else 2e-6), (tc, err)  # split TF32 accumulates in tensor-core FP32
+
+
+@pytest.mark.parametrize('n,nrhs', [(700, 150), (1024, 300)])
+def test_mixed_solve_on_packed_block_panels(n, nrhs):
+    """Wide right-hand sides take the packed-panel complex64 solve; refinement still reaches FP64."""
+    import ctypes
+    if not torch.cuda.is_available():
+        pytest.skip('no CUDA device')
+    from grim_20261007_b200 import _lib
+    from grim_20261007_b200.device import context, ptr, to_device_colmajor, to_host_matrix
+    ctx = context()
+    rng = np.random.default_rng(n)
+    a = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    b = rng.standard_normal((n, nrhs)) + 1j * rng.standard_normal((n, nrhs))
+    at = to_device_colmajor(a, torch.complex128)
+    bt = to_device_colmajor(b, torch.complex128)
+    info, st = ctypes.c_int(-1), _lib.GrimSolveInfo()
+    _lib.check(ctx.lib.grim_zgesv_mixed(ctx.h, n, nrhs, ptr(at), n, None, 0, ptr(bt), n, _lib.PREC_MIXED, 1e-12, 10,
+                                        ctypes.byref(info), ctypes.byref(st)))
+    x = to_host_matrix(bt)
+    ref = np.linalg.solve(a, b)
+    assert info.value == 0
+    assert np.max(np.abs(x - ref)) <= 1e-10 * np.max(np.abs(ref)), st.as_dict()
+    assert st.initial_backward_error < 1e-5 and st.refinement_steps >= 1, st.as_dict()
+
+
+@pytest.mark.parametrize('n,nrhs,complex64', [(300, 37, True), (300, 37, False), (1024, 130, True)])
+def test_integer_slice_residual_matches_fp64(n, nrhs, complex64):
+    """R = B - A X on the int8 tensor cores (8 slices) agrees with an FP64 residual to FP64 accuracy."""
+    if not torch.cuda.is_available():
+        pytest.skip('no CUDA device')
+    from grim_20261007_b200 import _lib
+    from grim_20261007_b200.device import context, ptr, to_device_colmajor, to_host_matrix
+    ctx = context()
+    rng = np.random.default_rng(n + nrhs)
+    a = (rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))) * np.exp(2 * rng.standard_normal((n, 1)))
+    if complex64:
+        a = a.astype(np.complex64).astype(np.complex128)
+    x = (rng.standard_normal((n, nrhs)) + 1j * rng.standard_normal((n, nrhs))) * np.exp(rng.standard_normal(nrhs))
+    x[:, 5] = 0.0
+    b = a @ x + 1e-9 * (rng.standard_normal((n, nrhs)) + 1j * rng.standard_normal((n, nrhs)))
+    at = to_device_colmajor(a, torch.complex64 if complex64 else torch.complex128)
+    xt, bt = to_device_colmajor(x, torch.complex128), to_device_colmajor(b, torch.complex128)
+    out = {}
+    for slices in (8, 0):
+        rt = to_device_colmajor(np.zeros((n, nrhs)), torch.complex128)
+        _lib.check(ctx.lib.grim_residual(ctx.h, n, nrhs, ptr(at), n, int(complex64), ptr(xt), n, ptr(bt), n, ptr(rt), n,
+                                         slices))
+        out[slices] = to_host_matrix(rt)
+    ref = b - a @ x
+    bound = 2e-14 * (np.abs(a) @ np.abs(x)).max()
+    assert np.max(np.abs(out[8] - ref)) <= bound
+    assert np.max(np.abs(out[0] - ref)) <= bound
+
+
+def test_integer_slice_residual_propagates_nonfinite():
+    if not torch.cuda.is_available():
+        pytest.skip('no CUDA device')
+    from grim_20261007_b200 import _lib
+    from grim_20261007_b200.device import context, ptr, to_device_colmajor, to_host_matrix
+    ctx = context()
+    rng = np.random.default_rng(9)
+    n, nrhs = 256, 20
+    a = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    x = rng.standard_normal((n, nrhs)) + 1j * rng.standard_normal((n, nrhs))
+    x[17, 3] = np.nan
+    b = np.ones((n, nrhs), complex)
+    at, xt, bt = (to_device_colmajor(v, torch.complex128) for v in (a, x, b))
+    rt = to_device_colmajor(np.zeros((n, nrhs)), torch.complex128)
+    _lib.check(ctx.lib.grim_residual(ctx.h, n, nrhs, ptr(at), n, 0, ptr(xt), n, ptr(bt), n, ptr(rt), n, 8))
+    r = to_host_matrix(rt)
+    assert np.all(np.isnan(r[:, 3]))
+    assert np.all(np.isfinite(np.delete(r, 3, axis=1)))
