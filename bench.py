@@ -97,17 +97,26 @@ class ClockSampler:
         return out
 
 
-def profile_step(ctx, fn):
-    """Run fn once with libgrimgpu's per-launch event profiling; returns {kernel: stats}."""
+def profile_step(ctxs, fn):
+    """Run fn once with libgrimgpu's per-launch event profiling on every context in ctxs;
+    returns {kernel: stats} summed over them."""
     import ctypes
     import torch
     torch.cuda.synchronize()
-    ctx.lib.grim_profile_enable(ctx.h, 1)
+    for c in ctxs:
+        c.lib.grim_profile_enable(c.h, 1)
     fn()
-    buf = ctypes.create_string_buffer(1 << 16)
-    ctx.lib.grim_profile_report(ctx.h, buf, len(buf))
-    ctx.lib.grim_profile_enable(ctx.h, 0)
-    return json.loads(buf.value.decode())
+    torch.cuda.synchronize()
+    merged = {}
+    for c in ctxs:
+        buf = ctypes.create_string_buffer(1 << 16)
+        c.lib.grim_profile_report(c.h, buf, len(buf))
+        c.lib.grim_profile_enable(c.h, 0)
+        for name, v in json.loads(buf.value.decode()).items():
+            m = merged.setdefault(name, {'launches': 0, 'ms': 0.0, 'flops': 0.0, 'bytes': 0.0})
+            for key in m:
+                m[key] += v[key]
+    return merged
 
 
 def run_serving(args):
@@ -256,7 +265,7 @@ def main():
         import datetime
         dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=120))
 
-    from grim_20261007_b200.device import context
+    from grim_20261007_b200.device import all_contexts, context, run_concurrent
     from grim_20261007_b200.execution import linear_precision
     from grim_20261007_b200.twod import geometry as geo, operators as ops
     from grim_20261007_b200.twod.solver import solve_monostatic_rcs_2d
@@ -270,10 +279,21 @@ def main():
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device='cuda')
 
     def step(precision):
-        out = {}
-        for pol in ('TM', 'TE'):
-            out[pol] = ops.monostatic_solve(bodies[pol], k, ang, pol, precision=precision, angles_dev=ang_dev)
-        return out
+        # the two polarisations are independent solves: run them on two device workers at once
+        pols = ('TM', 'TE')
+        res = run_concurrent([
+            (lambda p=p: ops.monostatic_solve(bodies[p], k, ang, p, precision=precision, angles_dev=ang_dev))
+            for p in pols])
+        return dict(zip(pols, res))
+
+    def step_serial(precision):
+        # one polarisation after the other on the default context: per-kernel event times
+        # are then those of a kernel alone on the GPU (used for the kernel profile only)
+        return {p: ops.monostatic_solve(bodies[p], k, ang, p, precision=precision, angles_dev=ang_dev)
+                for p in ('TM', 'TE')}
+
+    def launch_count():
+        return sum(c.launches for c in all_contexts())
 
     def barrier():
         if world > 1:
@@ -286,7 +306,7 @@ def main():
         barrier()
         torch.cuda.synchronize()
         times = []
-        launches0 = ctx.launches
+        launches0 = launch_count()
         last = None
         for _ in range(steps):
             flush.fill_(1.0)  # L2 flush (256 MiB write) outside the event window
@@ -299,7 +319,7 @@ def main():
         torch.cuda.synchronize()
         barrier()
         torch.cuda.synchronize()
-        launches = ctx.launches - launches0
+        launches = launch_count() - launches0
         ms = [a.elapsed_time(b) for a, b in times]
         return ms, launches, last
 
@@ -354,10 +374,13 @@ def main():
     serving = run_serving(args) if (args.serving and rank == 0 and world == 1) else None
     bor = run_bor(args) if (args.bor and rank == 0 and world == 1) else None
 
-    # per-kernel profile of one mixed step (CUDA events after every launch, separate from the timed loop)
+    # per-kernel profile of one mixed step, polarisations in turn (CUDA events after every
+    # launch on the launching stream, separate from the timed loop)
     n = args.n
-    prof = profile_step(ctx, lambda: step('mixed'))
-    prof64 = profile_step(ctx, lambda: step('double'))
+    step_serial('mixed')  # the default context's workspaces exist before its profile starts
+    step_serial('double')
+    prof = profile_step([ctx], lambda: step_serial('mixed'))
+    prof64 = profile_step([ctx], lambda: step_serial('double'))
     hbm, bf16, src = _peaks()
     dom_name, dom = max(prof.items(), key=lambda kv: kv[1]['ms'])
     step_ms = sum(v['ms'] for v in prof.values())

@@ -3,11 +3,19 @@
 PyTorch provides device memory (its caching allocator), pinned host buffers and the
 stream; all arithmetic runs in libgrimgpu's kernels.  Matrices live in torch tensors
 of shape (ncols, ld): row c of the tensor is column c of the column-major matrix.
+
+Independent solves (the two co-polarised channels of a 2-D solve, the systems of a
+sweep) overlap on the GPU through ``run_concurrent``: each runs in its own host thread
+on a worker -- its own libgrimgpu handle (workspaces, error flag) and CUDA stream --
+so one solve's latency-bound panel chain runs beside another's tensor-core updates.
 """
 from __future__ import annotations
 
+import contextlib
+import contextvars
 import ctypes
 import threading
+from concurrent.futures import ThreadPoolExecutor
 
 import numpy as np
 import torch
@@ -16,6 +24,8 @@ from . import _lib
 
 _contexts = {}
 _ctx_lock = threading.Lock()
+_workers = {}  # (device, index) -> (Context, torch.cuda.Stream)
+_tls = threading.local()  # per-thread override of context() inside a worker
 
 
 def require_cuda():
@@ -67,6 +77,10 @@ class Context:
 def context(device=None):
     require_cuda()
     dev = torch.cuda.current_device() if device is None else int(device)
+    over = getattr(_tls, 'ctx', None)
+    if over is not None and over.device == dev:
+        over.bind_stream()
+        return over
     with _ctx_lock:
         ctx = _contexts.get(dev)
         if ctx is None:
@@ -74,6 +88,90 @@ def context(device=None):
             _contexts[dev] = ctx
     ctx.bind_stream()
     return ctx
+
+
+def _worker(dev, index):
+    with _ctx_lock:
+        w = _workers.get((dev, index))
+        if w is None:
+            with torch.cuda.device(dev):
+                w = (Context(dev), torch.cuda.Stream(dev))
+            _workers[(dev, index)] = w
+    return w
+
+
+def all_contexts(device=None):
+    """The default context and every worker context created so far on ``device``."""
+    dev = torch.cuda.current_device() if device is None else int(device)
+    out = [context(dev)]
+    with _ctx_lock:
+        out += [w[0] for (d, _), w in sorted(_workers.items()) if d == dev]
+    return out
+
+
+@contextlib.contextmanager
+def worker(index, device=None):
+    """Route this thread's library calls (``context()``) and torch work to worker ``index``."""
+    dev = torch.cuda.current_device() if device is None else int(device)
+    ctx, stream = _worker(dev, index)
+    prev = getattr(_tls, 'ctx', None)
+    _tls.ctx = ctx
+    try:
+        with torch.cuda.device(dev), torch.cuda.stream(stream):
+            ctx.bind_stream(stream)
+            yield ctx, stream
+    finally:
+        _tls.ctx = prev
+
+
+def _record_on(obj, stream):
+    """Mark every CUDA tensor in a (nested) result as used by ``stream`` (caching-allocator safety)."""
+    if isinstance(obj, torch.Tensor):
+        if obj.is_cuda:
+            obj.record_stream(stream)
+    elif isinstance(obj, dict):
+        for v in obj.values():
+            _record_on(v, stream)
+    elif isinstance(obj, (list, tuple)):
+        for v in obj:
+            _record_on(v, stream)
+
+
+def run_concurrent(fns, device=None):
+    """Run the callables ``fns`` at once, fns[i] in its own thread on worker i.
+
+    Each worker stream first waits for the work already queued on the caller's current
+    stream; the caller's stream then waits for every worker, so results (device tensors
+    included) can be used on it directly.  Every callable runs in a copy of the caller's
+    context variables (``linear_precision`` and other scoped options apply inside it).
+    Exceptions propagate (the first one raised).
+    """
+    fns = list(fns)
+    if len(fns) <= 1:
+        return [f() for f in fns]
+    dev = torch.cuda.current_device() if device is None else int(device)
+    caller = torch.cuda.current_stream(dev)
+    ready = torch.cuda.Event()
+    ready.record(caller)
+
+    scopes = [contextvars.copy_context() for _ in fns]
+
+    def run(i):
+        with worker(i, dev) as (_ctx, stream):
+            stream.wait_event(ready)
+            result = scopes[i].run(fns[i])
+            done = torch.cuda.Event()
+            done.record(stream)
+            return result, done
+
+    with ThreadPoolExecutor(max_workers=len(fns)) as ex:
+        outs = list(ex.map(run, range(len(fns))))
+    results = []
+    for result, done in outs:
+        caller.wait_event(done)
+        _record_on(result, caller)
+        results.append(result)
+    return results
 
 
 def ptr(t):

@@ -109,7 +109,7 @@ def backward_error(z, x, b, ctx=None):
 
 
 def monostatic_solve(body, k, angles_deg, pol, precision='double', tol=None, check_backward_error=True,
-                     angles_dev=None, keep=False):
+                     angles_dev=None, keep=False, ctx=None):
     """One (geometry, frequency, polarization) solve with all its angles, on the device.
 
     Returns dict(amplitude=<device complex128 (nang,)>, telemetry).  With precision
@@ -124,31 +124,31 @@ def monostatic_solve(body, k, angles_deg, pol, precision='double', tol=None, che
         angles_dev = torch.as_tensor(np.asarray(angles_deg, dtype=np.float64), device=dev)
     tele = {}
     if precision == 'mixed':
-        z32 = fill(body, k, pol, complex64=True)
-        b = rhs(body, k, pol, angles_dev)
+        z32 = fill(body, k, pol, complex64=True, ctx=ctx)
+        b = rhs(body, k, pol, angles_dev, ctx=ctx)
         b0 = b.clone()
         try:
-            st = solve_inplace(None, b, 'mixed', tol=MIXED_RCS_TOL if tol is None else tol, z32=z32)
+            st = solve_inplace(None, b, 'mixed', tol=MIXED_RCS_TOL if tol is None else tol, z32=z32, ctx=ctx)
             x = b
             z = z32
         except _lib.GrimNotConverged:
             # refinement stalled (ill-conditioned system): fall back to the FP64 path, as the
             # reference's mixed -> double ladder does (linalg/dense.py:74-98)
-            z = fill(body, k, pol)
+            z = fill(body, k, pol, ctx=ctx)
             x = b0
-            st = solve_inplace(z, x, 'double')
+            st = solve_inplace(z, x, 'double', ctx=ctx)
             st['fp64_fallback'] = True
         tele.update(st)
     else:
-        z = fill(body, k, pol)
-        b = rhs(body, k, pol, angles_dev)
+        z = fill(body, k, pol, ctx=ctx)
+        b = rhs(body, k, pol, angles_dev, ctx=ctx)
         x = b.clone() if check_backward_error else b
-        st = solve_inplace(z, x, 'double')
+        st = solve_inplace(z, x, 'double', ctx=ctx)
         tele.update(st)
         if check_backward_error:
-            berr = backward_error(z, x, b)
+            berr = backward_error(z, x, b, ctx=ctx)
             tele['backward_error_dev'] = berr
-    amp = farfield(body, k, angles_dev, x)
+    amp = farfield(body, k, angles_dev, x, ctx=ctx)
     out = dict(amplitude=amp, telemetry=tele)
     if keep:
         out.update(matrix=z, solution=x)

@@ -29,7 +29,7 @@ import numpy as np
 import torch
 
 from .. import _lib
-from ..device import context, ptr, require_cuda
+from ..device import context, ptr, require_cuda, run_concurrent
 from ..execution import requested_dense_backend, requested_precision
 from . import geometry as geo
 from . import operators as ops
@@ -355,16 +355,32 @@ def solve_monostatic_rcs_2d(geometry_snapshot, frequencies_ghz, elevations_deg, 
                             strict_quality_gate=True, compute_condition_number=False, max_panels=MAX_PANELS_DEFAULT,
                             mesh_reference_ghz=None, rcs_normalization_mode="physical", abort_event=None,
                             solver_method="auto"):
-    """Both physical co-polarised channels (reference ``twod/solver.py:3193``): VV (TE) then HH (TM)."""
-    channels = {}
-    for export, pol in _CO_POLARIZED_2D_CHANNELS:
-        channels[export] = solve_monostatic_rcs_2d_single_polarization(
+    """Both physical co-polarised channels (reference ``twod/solver.py:3193``): VV (TE) then HH (TM).
+
+    The two channels are independent systems; they are solved at the same time on two
+    device workers (own handle, stream and host thread), so that one channel's
+    latency-bound factorization steps overlap the other's tensor-core updates.  Samples
+    and metadata are those of the two single-polarisation solves, VV first.
+    """
+    progress_lock = threading.Lock()
+
+    def progress(*a):
+        if progress_callback is not None:
+            with progress_lock:
+                progress_callback(*a)
+
+    def channel(pol):
+        return lambda: solve_monostatic_rcs_2d_single_polarization(
             geometry_snapshot, frequencies_ghz, elevations_deg, pol, geometry_units=geometry_units,
-            material_base_dir=material_base_dir, progress_callback=progress_callback,
+            material_base_dir=material_base_dir, progress_callback=progress if progress_callback else None,
             quality_thresholds=quality_thresholds, strict_quality_gate=strict_quality_gate,
             compute_condition_number=compute_condition_number, max_panels=max_panels,
             mesh_reference_ghz=mesh_reference_ghz, rcs_normalization_mode=rcs_normalization_mode,
             abort_event=abort_event, solver_method=solver_method)
+
+    require_cuda()
+    results = run_concurrent([channel(pol) for _export, pol in _CO_POLARIZED_2D_CHANNELS])
+    channels = {export: res for (export, _pol), res in zip(_CO_POLARIZED_2D_CHANNELS, results)}
     samples = []
     for export, _pol in _CO_POLARIZED_2D_CHANNELS:
         for s in channels[export]['samples']:

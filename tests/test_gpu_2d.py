@@ -119,3 +119,24 @@ def test_end_to_end_co_polarized_and_mixed(ctx):
         db64 = 10 * np.log10(s64)
         mask = db64 > db64.max() - 40
         assert np.max(np.abs(10 * np.log10(s32 / s64))[mask]) <= 0.05
+
+
+def test_concurrent_channels_match_single_channel_solves(ctx):
+    """The co-polarised solve runs VV and HH on two device workers at once; each channel's
+    result equals the same channel solved alone (the kernels are deterministic)."""
+    from grim_20261007_b200.execution import linear_precision
+    from grim_20261007_b200.twod.solver import (solve_monostatic_rcs_2d,
+                                                solve_monostatic_rcs_2d_single_polarization)
+    v, k, f, _ = S.airfoil_case(3, 640)
+    snap = S.snapshot_from_polygons([v])
+    ang = list(np.arange(0.0, 360.0, 1.5))
+    for prec in ('double', 'mixed'):
+        with linear_precision(prec):
+            both = solve_monostatic_rcs_2d(snap, [f / 1e9], ang, geometry_units='meters', strict_quality_gate=False)
+            for pol, exp in (('TE', 'VV'), ('TM', 'HH')):
+                alone = solve_monostatic_rcs_2d_single_polarization(snap, [f / 1e9], ang, pol, geometry_units='meters',
+                                                                    strict_quality_gate=False)
+                a1 = np.array([complex(s['rcs_amp_real'], s['rcs_amp_imag']) for s in alone['samples']])
+                a2 = np.array([complex(s['rcs_amp_real'], s['rcs_amp_imag']) for s in both['samples']
+                               if s['polarization'] == exp])
+                np.testing.assert_allclose(a2, a1, rtol=1e-13, atol=1e-13 * np.max(np.abs(a1)))
