@@ -76,23 +76,28 @@ def contours_from_snapshot(snapshot, geometry_units='inches', wavelength=None, m
         if seg_type != 2 or ibc != 0 or pos != 0 or neg != 0:
             raise NotImplementedError(
                 f"Segment {seg.get('name', '?')!r}: only closed PEC contours (TYPE 2, IBC 0) are solved on the GPU path.")
-        pts = []
-        pts_last = None
-        for pair in seg.get('point_pairs', []) or []:
-            a = np.array([float(pair['x1']), float(pair['y1'])]) * scale
-            b = np.array([float(pair['x2']), float(pair['y2'])]) * scale
-            length = float(np.hypot(*(b - a)))
-            cnt = panel_count(n_prop, length, wavelength)
-            t = np.linspace(0.0, 1.0, cnt + 1)
-            seg_pts = a[None, :] + t[:, None] * (b - a)[None, :]
-            seg_pts[-1] = b
-            if pts_last is not None and np.hypot(*(pts_last - a)) > max(WELD_TOL, 1e-9 * max(1.0, length)):
-                raise ValueError(f"Segment {seg.get('name', '?')!r}: primitives do not form a head-to-tail chain.")
-            pts.extend(seg_pts[:-1])
-            pts_last = b
-        if not pts:
+        pairs = seg.get('point_pairs', []) or []
+        if not pairs:
             continue
-        poly = np.asarray(pts, dtype=np.float64)
+        xy = np.array([(float(p['x1']), float(p['y1']), float(p['x2']), float(p['y2'])) for p in pairs],
+                      dtype=np.float64) * scale
+        a, b = xy[:, :2], xy[:, 2:]
+        lengths = np.hypot(b[:, 0] - a[:, 0], b[:, 1] - a[:, 1])
+        if n_prop > 0:
+            cnt = np.full(len(pairs), int(n_prop), dtype=np.int64)
+        else:
+            cnt = np.array([panel_count(n_prop, float(L), wavelength) for L in lengths], dtype=np.int64)
+        gaps = np.hypot(*(b[:-1] - a[1:]).T)
+        tol = np.maximum(WELD_TOL, 1e-9 * np.maximum(1.0, lengths[1:]))
+        if np.any(gaps > tol):
+            raise ValueError(f"Segment {seg.get('name', '?')!r}: primitives do not form a head-to-tail chain.")
+        # panel vertices a + i (b - a) / cnt, i < cnt, of every primitive (linspace's i * (1 / cnt))
+        owner = np.repeat(np.arange(len(pairs)), cnt)
+        first = np.cumsum(cnt) - cnt
+        step = 1.0 / cnt.astype(np.float64)
+        t = (np.arange(int(cnt.sum())) - first[owner]) * step[owner]
+        poly = a[owner] + t[:, None] * (b - a)[owner]
+        pts_last = b[-1]
         if np.hypot(*(pts_last - poly[0])) > max(WELD_TOL, 1e-9):
             raise ValueError(f"Segment {seg.get('name', '?')!r} is not closed; open contours are outside this path.")
         total += len(poly)
