@@ -269,7 +269,8 @@ static int gemm(grim_context *h, int M, int N, int K, const TA *A, int64_t lda, 
                 int64_t ldc) {
     if (M <= 0 || N <= 0) return GRIM_OK;
     dim3 grid(ceil_div(M, RT_BM), ceil_div(N, RT_BN));
-    k_gemm_rt<ACC, TA, TB, TC, NEG, BETA><<<grid, RT_THREADS, 0, h->stream>>>(M, N, K, A, lda, B, ldb, C, ldc);
+    k_gemm_rt<ACC, TA, TB, TC, NEG, BETA><<<grid, RT_THREADS, 0, h->stream>>>(M, N, K, A, lda, B, ldb, C, ldc, 0, 0,
+                                                                              0);
     GRIM_CHECK_LAUNCH_W(h, sizeof(ACC) == 16 ? "k_gemm_rt<f64>" : "k_gemm_rt<f32>", 8.0 * M * N * K,
                         (double)sizeof(TA) * M * K + (double)sizeof(TB) * K * N + (BETA ? 2.0 : 1.0) * sizeof(TC) * M * N);
     return GRIM_OK;
@@ -335,7 +336,8 @@ static inline int tc_bn(int N) { return N > 192 ? 128 : 64; }
 
 static int tc_pack_a(grim_context *h, int M, int K, const float2 *A, int64_t lda, float sign, const TcPacked &P) {
     const int64_t chunks = (int64_t)P.rows_p * (P.kp / 4);
-    k_tc_pack_a<<<ceil_div(chunks, 256), 256, 0, h->stream>>>(M, K, A, lda, P.hi, P.lo, P.rows_p, P.kp, sign);
+    k_tc_pack_a<<<ceil_div(chunks, 256), 256, 0, h->stream>>>(M, K, A, lda, P.hi, P.lo, P.rows_p, P.rows_p, 0, P.kp,
+                                                              sign);
     GRIM_CHECK_LAUNCH_W(h, "k_tc_pack_a", 0.0, 8.0 * M * K + 32.0 * chunks);
     return GRIM_OK;
 }
@@ -378,9 +380,10 @@ static int tc_gemm_packed(grim_context *h, int bn, const TcPacked &A, const TcPa
     return tc_launch<64, 4>(h, A, B, C, ldc, M, N, Kc, alpha, ow_lo, ow_hi, err);
 }
 
-// C[MxN] -= A B[KxN] (complex64, column-major) on tcgen05 (split TF32), packing both operands.
-static int tc_cgemm_sub(grim_context *h, int M, int N, int K, const float2 *A, int64_t lda, const float2 *B,
-                        int64_t ldb, float2 *C, int64_t ldc) {
+// C[MxN] = (overwrite ? 0 : C) + alpha A B[KxN] (complex64, column-major) on tcgen05 (split
+// TF32), packing both operands.
+static int tc_cgemm(grim_context *h, int M, int N, int K, const float2 *A, int64_t lda, const float2 *B, int64_t ldb,
+                    float2 *C, int64_t ldc, float alpha, bool overwrite) {
     if (M <= 0 || N <= 0 || K <= 0) return GRIM_OK;
     const int bn = tc_bn(N), Kp = tc_kp(K);
     TcPacked pa, pb;
@@ -388,7 +391,13 @@ static int tc_cgemm_sub(grim_context *h, int M, int N, int K, const float2 *A, i
     GRIM_TRY(tc_ws(h, "tc_b", ceil_div(N, bn) * bn, Kp, &pb));
     GRIM_TRY(tc_pack_a(h, M, K, A, lda, 1.f, pa));
     GRIM_TRY(tc_pack_b(h, K, N, B, ldb, pb));
-    return tc_gemm_packed(h, bn, pa, pb, C, ldc, M, N, K, -1.f, 0, 0);
+    return tc_gemm_packed(h, bn, pa, pb, C, ldc, M, N, K, alpha, 0, overwrite ? M : 0);
+}
+
+// C[MxN] -= A B[KxN] on tcgen05.
+static int tc_cgemm_sub(grim_context *h, int M, int N, int K, const float2 *A, int64_t lda, const float2 *B,
+                        int64_t ldb, float2 *C, int64_t ldc) {
+    return tc_cgemm(h, M, N, K, A, lda, B, ldb, C, ldc, -1.f, false);
 }
 
 // Trailing / solve updates C -= A B: tensor cores for complex64 (unless disabled), SIMT otherwise.
@@ -508,7 +517,7 @@ static int getrs_apply(grim_context *h, int n, int nrhs, const C *LU, int64_t ld
     const int ctiles = ceil_div(nrhs, TRSM_COLS);
     for (int p = 0; p < npan; ++p) {
         const int j = p * NB, nbj = std::min(NB, n - j);
-        k_trsm_diag<C, false><<<ctiles, 4 * TRSM_COLS, tri, h->stream>>>(nrhs, LU, lda, B, ldb, j, nbj);
+        k_trsm_diag<C, false><<<ctiles, 4 * TRSM_COLS, tri, h->stream>>>(nrhs, LU, lda, B, ldb, j, nbj, 0, 0);
         GRIM_CHECK_LAUNCH_W(h, kname("k_trsm_diag", sizeof(C)), 4.0 * nbj * nbj * nrhs, 0);
         const int below = n - j - nbj;
         if (below > 0)
@@ -517,7 +526,7 @@ static int getrs_apply(grim_context *h, int n, int nrhs, const C *LU, int64_t ld
     }
     for (int p = npan - 1; p >= 0; --p) {
         const int j = p * NB, nbj = std::min(NB, n - j);
-        k_trsm_diag<C, true><<<ctiles, 4 * TRSM_COLS, tri, h->stream>>>(nrhs, LU, lda, B, ldb, j, nbj);
+        k_trsm_diag<C, true><<<ctiles, 4 * TRSM_COLS, tri, h->stream>>>(nrhs, LU, lda, B, ldb, j, nbj, 0, 0);
         GRIM_CHECK_LAUNCH_W(h, kname("k_trsm_diag", sizeof(C)), 4.0 * nbj * nbj * nrhs, 0);
         if (j > 0)
             GRIM_TRY((gemm_sub<C>(h, j, nrhs, nbj, LU + (int64_t)j * lda, lda, B + j, ldb, B, ldb)));
@@ -543,11 +552,13 @@ static int getrs_impl(grim_context *h, int n, int nrhs, const C *LU, int64_t lda
 //            B[J:n] = [0; B[J+nb:n]] + PL_i B[J:J+nb]
 //   backward (U upper),      block i:                  PU_i = [-U_above,i Uinv_ii; Uinv_ii]
 //            B[0:J+nb] = [B[0:J]; 0] + PU_i B[J:J+nb]
-// PL_i is the forward substitution of the 64-row diagonal steps inside block i applied to
-// [I; 0], PU_i the backward one applied to [0; I]; both are packed (split TF32, tile
-// layout) and kept for every solve of a refinement loop.  The block solve multiplies by
-// the inverse of a triangular diagonal block instead of substituting; its rounding is
-// that of an FP32 GEMM, and the FP64 refinement that consumes these solves removes it.
+// The inverses of all diagonal blocks are formed together (batched over blocks: the
+// 64-row triangular solves of k_trsm_diag on identity columns, then SIMT updates inside
+// each block), the off-diagonal parts by one tensor-core GEMM per block, and both are
+// packed (split TF32, tile layout) and kept for every solve of a refinement loop.  The
+// block solve multiplies by the inverse of a triangular diagonal block instead of
+// substituting; its rounding is that of an FP32 GEMM, and the FP64 refinement that
+// consumes these solves removes it.
 #define GS_NB 256
 
 struct GsPanels {
@@ -555,66 +566,102 @@ struct GsPanels {
     std::vector<TcPacked> L, U;
 };
 
+// T_b (bd x bd, leading dim GS_NB, batch stride GS_NB^2) = inverse of the unit lower
+// (upper = false) or upper diagonal block of LU at (J0 + b GS_NB) for b < count.
+static int gs_invert_blocks(grim_context *h, const float2 *LU, int64_t lda, int J0, int count, int bd, float2 *T,
+                            bool upper) {
+    const size_t tri = (size_t)(NB * NBP + NB) * sizeof(float2);
+    const int64_t sLU = (int64_t)GS_NB * (lda + 1), sT = (int64_t)GS_NB * GS_NB;
+    const float2 *D = LU + (int64_t)J0 * lda + J0;
+    k_set_unit<float2><<<dim3(ceil_div(bd, 256), bd, count), 256, 0, h->stream>>>(bd, bd, T, GS_NB, 0, sT);
+    GRIM_CHECK_LAUNCH(h, "k_set_unit");
+    const int nsub = ceil_div(bd, NB);
+    for (int q = 0; q < nsub; ++q) {
+        const int s = upper ? nsub - 1 - q : q, js = s * NB, nbs = std::min(NB, bd - js);
+        dim3 tg(ceil_div(bd, TRSM_COLS), count);
+        if (upper)
+            k_trsm_diag<float2, true><<<tg, 4 * TRSM_COLS, tri, h->stream>>>(bd, D, lda, T, GS_NB, js, nbs, sLU, sT);
+        else
+            k_trsm_diag<float2, false><<<tg, 4 * TRSM_COLS, tri, h->stream>>>(bd, D, lda, T, GS_NB, js, nbs, sLU, sT);
+        GRIM_CHECK_LAUNCH_W(h, "k_trsm_diag<c64>", 4.0 * nbs * nbs * bd * count, 0);
+        // rows of the block still to solve: below the strip (lower) or above it (upper)
+        const int M = upper ? js : bd - js - nbs;
+        if (M <= 0) continue;
+        const float2 *Ab = upper ? D + (int64_t)js * lda : D + (int64_t)js * lda + js + nbs;
+        float2 *Cb = upper ? T : T + js + nbs;
+        dim3 grid(ceil_div(M, RT_BM), ceil_div(bd, RT_BN), count);
+        k_gemm_rt<float2, float2, float2, float2, true, true><<<grid, RT_THREADS, 0, h->stream>>>(
+            M, bd, nbs, Ab, lda, T + js, GS_NB, Cb, GS_NB, sLU, sT, sT);
+        GRIM_CHECK_LAUNCH_W(h, "k_gemm_rt<f32>", 8.0 * M * bd * nbs * count, 0);
+    }
+    return GRIM_OK;
+}
+
 static int gs_build(grim_context *h, int n, const float2 *LU, int64_t lda, GsPanels *P) {
-    const int nblk = ceil_div(n, GS_NB);
+    const int nblk = ceil_div(n, GS_NB), nfull = n / GS_NB;
     size_t floats_l = 0, floats_u = 0;
     for (int i = 0; i < nblk; ++i) {
         const int J = i * GS_NB, nbj = std::min(GS_NB, n - J);
         floats_l += 2 * (size_t)tc_rows_a(n - J) * tc_kp(nbj);
         floats_u += 2 * (size_t)tc_rows_a(J + nbj) * tc_kp(nbj);
     }
-    void *pl = nullptr, *pu = nullptr, *pe = nullptr;
+    void *pl = nullptr, *pu = nullptr, *pt = nullptr, *pw = nullptr;
     GRIM_TRY(grim_workspace(h, "gs_l", floats_l * sizeof(float), &pl));
     GRIM_TRY(grim_workspace(h, "gs_u", floats_u * sizeof(float), &pu));
-    GRIM_TRY(grim_workspace(h, "gs_e", (size_t)n * GS_NB * sizeof(float2), &pe));
-    float2 *E = (float2 *)pe;
+    GRIM_TRY(grim_workspace(h, "gs_t", (size_t)2 * nblk * GS_NB * GS_NB * sizeof(float2), &pt));
+    GRIM_TRY(grim_workspace(h, "gs_w", (size_t)n * GS_NB * sizeof(float2), &pw));
+    float2 *TL = (float2 *)pt, *TU = TL + (size_t)nblk * GS_NB * GS_NB, *W = (float2 *)pw;
+    // inverses of every diagonal block: the full blocks in one batch, a partial last one alone
+    if (nfull > 0) {
+        GRIM_TRY(gs_invert_blocks(h, LU, lda, 0, nfull, GS_NB, TL, false));
+        GRIM_TRY(gs_invert_blocks(h, LU, lda, 0, nfull, GS_NB, TU, true));
+    }
+    if (nblk > nfull) {
+        const int J = nfull * GS_NB, bd = n - J;
+        const size_t off = (size_t)nfull * GS_NB * GS_NB;
+        GRIM_TRY(gs_invert_blocks(h, LU, lda, J, 1, bd, TL + off, false));
+        GRIM_TRY(gs_invert_blocks(h, LU, lda, J, 1, bd, TU + off, true));
+    }
     P->n = n;
     P->nblk = nblk;
     P->L.assign(nblk, TcPacked{});
     P->U.assign(nblk, TcPacked{});
-    const size_t tri = (size_t)(NB * NBP + NB) * sizeof(float2);
     float *fl = (float *)pl, *fu = (float *)pu;
+    auto pack_rows = [&](const TcPacked &dst, int M, int K, const float2 *A, int64_t ld_a, int r_off, int rows) {
+        const int64_t chunks = (int64_t)rows * (dst.kp / 4);
+        k_tc_pack_a<<<ceil_div(chunks, 256), 256, 0, h->stream>>>(M, K, A, ld_a, dst.hi, dst.lo, rows, dst.rows_p, r_off,
+                                                                  dst.kp, 1.f);
+        GRIM_CHECK_LAUNCH_W(h, "k_tc_pack_a", 0.0, 8.0 * M * K + 32.0 * chunks);
+        return GRIM_OK;
+    };
     for (int i = 0; i < nblk; ++i) {
         const int J = i * GS_NB, nbj = std::min(GS_NB, n - J), kp = tc_kp(nbj);
-        const int ctiles = ceil_div(nbj, TRSM_COLS);
-        // forward panel: rows J..n of [I; 0] through the diagonal steps of block i
-        const int rl = n - J;
-        k_set_unit<float2><<<dim3(ceil_div(rl, 256), nbj), 256, 0, h->stream>>>(rl, nbj, E, rl, 0);
-        GRIM_CHECK_LAUNCH(h, "k_set_unit");
-        for (int j = J; j < J + nbj; j += NB) {
-            const int nb = std::min(NB, J + nbj - j);
-            k_trsm_diag<float2, false><<<ctiles, 4 * TRSM_COLS, tri, h->stream>>>(nbj, LU + (int64_t)J * lda + J, lda,
-                                                                                  E, rl, j - J, nb);
-            GRIM_CHECK_LAUNCH_W(h, "k_trsm_diag<c64>", 4.0 * nb * nb * nbj, 0);
-            const int below = n - j - nb;
-            if (below > 0)
-                GRIM_TRY((gemm_sub<float2>(h, below, nbj, nb, LU + (int64_t)j * lda + j + nb, lda, E + (j - J), rl,
-                                           E + (j - J) + nb, rl)));
-        }
+        const float2 *Ti = TL + (size_t)i * GS_NB * GS_NB, *Ui = TU + (size_t)i * GS_NB * GS_NB;
+        // forward panel [Linv; -L_below Linv], rows J..n
         TcPacked &pli = P->L[i];
         pli.hi = fl;
-        pli.rows_p = tc_rows_a(rl);
+        pli.rows_p = tc_rows_a(n - J);
         pli.kp = kp;
         pli.lo = fl + (size_t)pli.rows_p * kp;
         fl += 2 * (size_t)pli.rows_p * kp;
-        GRIM_TRY(tc_pack_a(h, rl, nbj, E, rl, 1.f, pli));
-        // backward panel: rows 0..J+nbj of [0; I] through the diagonal steps of block i
-        const int ru = J + nbj;
-        k_set_unit<float2><<<dim3(ceil_div(ru, 256), nbj), 256, 0, h->stream>>>(ru, nbj, E, ru, J);
-        GRIM_CHECK_LAUNCH(h, "k_set_unit");
-        for (int j = J + ((nbj - 1) / NB) * NB; j >= J; j -= NB) {
-            const int nb = std::min(NB, J + nbj - j);
-            k_trsm_diag<float2, true><<<ctiles, 4 * TRSM_COLS, tri, h->stream>>>(nbj, LU, lda, E, ru, j, nb);
-            GRIM_CHECK_LAUNCH_W(h, "k_trsm_diag<c64>", 4.0 * nb * nb * nbj, 0);
-            if (j > 0) GRIM_TRY((gemm_sub<float2>(h, j, nbj, nb, LU + (int64_t)j * lda, lda, E + j, ru, E, ru)));
+        const int below = n - J - nbj;
+        GRIM_TRY(pack_rows(pli, nbj, nbj, Ti, GS_NB, 0, below > 0 ? 2 * nbj : pli.rows_p));
+        if (below > 0) {
+            GRIM_TRY(tc_cgemm(h, below, nbj, nbj, LU + (int64_t)J * lda + J + nbj, lda, Ti, GS_NB, W, below, -1.f, true));
+            GRIM_TRY(pack_rows(pli, below, nbj, W, below, 2 * nbj, pli.rows_p - 2 * nbj));
         }
+        // backward panel [-U_above Uinv; Uinv], rows 0..J+nbj
         TcPacked &pui = P->U[i];
         pui.hi = fu;
-        pui.rows_p = tc_rows_a(ru);
+        pui.rows_p = tc_rows_a(J + nbj);
         pui.kp = kp;
         pui.lo = fu + (size_t)pui.rows_p * kp;
         fu += 2 * (size_t)pui.rows_p * kp;
-        GRIM_TRY(tc_pack_a(h, ru, nbj, E, ru, 1.f, pui));
+        if (J > 0) {
+            GRIM_TRY(tc_cgemm(h, J, nbj, nbj, LU + (int64_t)J * lda, lda, Ui, GS_NB, W, J, -1.f, true));
+            GRIM_TRY(pack_rows(pui, J, nbj, W, J, 0, 2 * J));
+        }
+        GRIM_TRY(pack_rows(pui, nbj, nbj, Ui, GS_NB, 2 * J, pui.rows_p - 2 * J));
     }
     return GRIM_OK;
 }

@@ -140,9 +140,11 @@ __global__ void k_berr_finish(int ncol, const double *absmax3, const double *ano
     }
 }
 
-// E[rows x cols] = 0 except E[row_off + c, c] = 1 (a shifted identity block).
+// E[rows x cols] = 0 except E[row_off + c, c] = 1 (a shifted identity block); batched
+// over blockIdx.z with stride sE.
 template <typename C>
-__global__ void k_set_unit(int rows, int cols, C *__restrict__ E, int64_t lde, int row_off) {
+__global__ void k_set_unit(int rows, int cols, C *__restrict__ E, int64_t lde, int row_off, int64_t sE) {
+    E += blockIdx.z * sE;
     const int r = blockIdx.x * blockDim.x + threadIdx.x, c = blockIdx.y;
     if (r >= rows || c >= cols) return;
     C v = czero<C>();

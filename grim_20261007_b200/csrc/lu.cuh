@@ -27,11 +27,15 @@
 // C[MxN] = (BETA ? C : 0) + (NEG ? -1 : 1) * A[MxK] * B[KxN], column-major, ACC arithmetic.
 // 64 x 128 CTA tile, 256 threads each owning 4 x 8 outputs, two shared-memory stages
 // filled through registers.
+// Batched over blockIdx.z: operand z starts sA / sB / sC elements after operand 0.
 template <typename ACC, typename TA, typename TB, typename TC, bool NEG, bool BETA>
 __global__ void __launch_bounds__(RT_THREADS)
 k_gemm_rt(int M, int N, int K, const TA *__restrict__ A, int64_t lda, const TB *__restrict__ B, int64_t ldb,
-          TC *__restrict__ C, int64_t ldc) {
+          TC *__restrict__ C, int64_t ldc, int64_t sA, int64_t sB, int64_t sC) {
     using R = typename real_of<ACC>::type;
+    A += blockIdx.z * sA;
+    B += blockIdx.z * sB;
+    C += blockIdx.z * sC;
     __shared__ ACC As[2][RT_BK][RT_BM];
     __shared__ ACC Bs[2][RT_BK][RT_BN];
     const int t = threadIdx.x;
@@ -566,11 +570,15 @@ __global__ void k_laswp_rhs(int n, int nrhs, C *B, int64_t ldb, const int *ipiv,
 
 // In-place triangular solve of the nbj-row strip of B at row j with the diagonal block of
 // LU at (j, j): UPPER = false -> unit lower L, true -> upper U.  4 lanes per column,
-// TRSM_COLS columns per CTA.  Dynamic smem: NB * NBP + NB elements.
+// TRSM_COLS columns per CTA.  Dynamic smem: NB * NBP + NB elements.  Batched over
+// blockIdx.y: system y uses LU + y * sLU and B + y * sB.
 #define TRSM_COLS 16
 template <typename C, bool UPPER>
 __global__ void __launch_bounds__(4 * TRSM_COLS)
-k_trsm_diag(int nrhs, const C *__restrict__ LU, int64_t lda, C *B, int64_t ldb, int j, int nbj) {
+k_trsm_diag(int nrhs, const C *__restrict__ LU, int64_t lda, C *B, int64_t ldb, int j, int nbj, int64_t sLU,
+            int64_t sB) {
+    LU += blockIdx.y * sLU;
+    B += blockIdx.y * sB;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C *T = reinterpret_cast<C *>(smem_raw);
     C *rd = T + NB * NBP;

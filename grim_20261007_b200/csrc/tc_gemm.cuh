@@ -65,11 +65,12 @@ __device__ __forceinline__ void tc_store_chunk(float *hi, float *lo, int64_t off
         make_float4(tf32_rna(v0 - h0), tf32_rna(v1 - h1), tf32_rna(v2 - h2), tf32_rna(v3 - h3));
 }
 
-// A~ (2M x 2K real, from complex M x K column-major A) into the tile layout, zero padded
-// to Mp x Kp and scaled by sign (+1 or -1).  One thread per 16-byte chunk; consecutive
-// threads take consecutive rows so that the complex reads are coalesced.
+// A~ (2M x 2K real, from complex M x K column-major A) into real rows [r_off, r_off + Mp)
+// of an operand with Rp rows in the tile layout, zero padded to Mp x Kp and scaled by
+// sign (+1 or -1).  One thread per 16-byte chunk; consecutive threads take consecutive
+// rows so that the complex reads are coalesced.
 __global__ void k_tc_pack_a(int M, int K, const float2 *__restrict__ A, int64_t lda, float *__restrict__ hi,
-                            float *__restrict__ lo, int Mp, int Kp, float sign) {
+                            float *__restrict__ lo, int Mp, int Rp, int r_off, int Kp, float sign) {
     const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= (int64_t)Mp * (Kp >> 2)) return;
     const int r = (int)(idx % Mp), k0 = (int)(idx / Mp) * 4;
@@ -85,7 +86,7 @@ __global__ void k_tc_pack_a(int M, int K, const float2 *__restrict__ A, int64_t 
             }
         }
     }
-    tc_store_chunk(hi, lo, tc_tile_offset(r, k0, Mp), v[0], v[1], v[2], v[3]);
+    tc_store_chunk(hi, lo, tc_tile_offset(r_off + r, k0, Rp), v[0], v[1], v[2], v[3]);
 }
 
 // B^ (rows n < Np, real columns 2k+s = (re, im) of B[k, n]) into the tile layout, zero

@@ -50,7 +50,7 @@ def test_mixed_solve_on_packed_block_panels(n, nrhs):
     ref = np.linalg.solve(a, b)
     assert info.value == 0
     assert np.max(np.abs(x - ref)) <= 1e-10 * np.max(np.abs(ref)), st.as_dict()
-    assert st.initial_backward_error < 1e-5 and st.refinement_steps >= 1, st.as_dict()
+    assert st.initial_backward_error < 1e-4 and st.refinement_steps >= 1, st.as_dict()
 
 
 @pytest.mark.parametrize('n,nrhs,complex64', [(300, 37, True), (300, 37, False), (1024, 130, True)])
