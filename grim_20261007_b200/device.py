@@ -137,41 +137,97 @@ def _record_on(obj, stream):
             _record_on(v, stream)
 
 
-def run_concurrent(fns, device=None):
-    """Run the callables ``fns`` at once, fns[i] in its own thread on worker i.
+def in_worker():
+    """True inside a worker thread (nested pools run their tasks in place)."""
+    return getattr(_tls, 'ctx', None) is not None
 
-    Each worker stream first waits for the work already queued on the caller's current
-    stream; the caller's stream then waits for every worker, so results (device tensors
-    included) can be used on it directly.  Every callable runs in a copy of the caller's
-    context variables (``linear_precision`` and other scoped options apply inside it).
-    Exceptions propagate (the first one raised).
+
+def run_pool(fns, workers=None, costs=None, on_done=None, device=None):
+    """Run the callables ``fns`` on up to ``workers`` device workers and return their results
+    in input order.
+
+    Each worker is a host thread with its own libgrimgpu handle and CUDA stream; it takes
+    the next task from a shared queue, largest ``costs`` first (longest-processing-time
+    order), so independent solves of different sizes overlap on the GPU.  Worker streams
+    first wait for the work already queued on the caller's current stream; the caller's
+    stream then waits for every worker, so results (device tensors included) can be used
+    on it directly.  Every task runs in a copy of the caller's context variables
+    (``linear_precision`` and other scoped options apply inside it).  ``on_done(i, result)``
+    is called (serialised) as each task finishes.  The first exception raised by a task is
+    re-raised after the running tasks finish; tasks not yet started are skipped.  Called
+    from inside a worker, the tasks run in place, one after another.
     """
     fns = list(fns)
-    if len(fns) <= 1:
-        return [f() for f in fns]
+    if not fns:
+        return []
+    if workers is None:
+        workers = len(fns)
+    workers = max(1, min(int(workers), len(fns)))
+    if in_worker() or workers == 1:
+        out = []
+        for i, f in enumerate(fns):
+            r = f()
+            if on_done is not None:
+                on_done(i, r)
+            out.append(r)
+        return out
     dev = torch.cuda.current_device() if device is None else int(device)
     caller = torch.cuda.current_stream(dev)
     ready = torch.cuda.Event()
     ready.record(caller)
-
+    order = list(range(len(fns)))
+    if costs is not None:
+        order.sort(key=lambda i: -float(costs[i]))
+    lock = threading.Lock()
+    state = {'next': 0, 'error': None}
+    results = [None] * len(fns)
     scopes = [contextvars.copy_context() for _ in fns]
 
-    def run(i):
-        with worker(i, dev) as (_ctx, stream):
+    def take():
+        with lock:
+            if state['error'] is not None or state['next'] >= len(order):
+                return None
+            i = order[state['next']]
+            state['next'] += 1
+            return i
+
+    def loop(w):
+        with worker(w, dev) as (_ctx, stream):
             stream.wait_event(ready)
-            result = scopes[i].run(fns[i])
+            while True:
+                i = take()
+                if i is None:
+                    break
+                try:
+                    r = scopes[i].run(fns[i])
+                except BaseException as exc:  # noqa: BLE001 - re-raised in the caller
+                    with lock:
+                        if state['error'] is None:
+                            state['error'] = exc
+                    break
+                results[i] = r
+                if on_done is not None:
+                    with lock:
+                        on_done(i, r)
             done = torch.cuda.Event()
             done.record(stream)
-            return result, done
+            return done
 
-    with ThreadPoolExecutor(max_workers=len(fns)) as ex:
-        outs = list(ex.map(run, range(len(fns))))
-    results = []
-    for result, done in outs:
+    with ThreadPoolExecutor(max_workers=workers) as ex:
+        events = list(ex.map(loop, range(workers)))
+    for done in events:
         caller.wait_event(done)
-        _record_on(result, caller)
-        results.append(result)
+    if state['error'] is not None:
+        raise state['error']
+    for r in results:
+        _record_on(r, caller)
     return results
+
+
+def run_concurrent(fns, device=None):
+    """Run the callables ``fns`` at once, fns[i] on its own worker (see ``run_pool``)."""
+    fns = list(fns)
+    return run_pool(fns, workers=len(fns), device=device)
 
 
 def ptr(t):

@@ -77,6 +77,26 @@ def airfoil_case(seed, n=2048, panels_per_wavelength=10.0, chord=1.0):
     return v, k, C0 / lam, t
 
 
+def airfoil_sweep_case(seed, nfreq=256, band=20.0, nmin=64, nmax=4096, panels_per_wavelength=10.0, chord=1.0):
+    """Seeded NACA 00tt frequency sweep: ``nfreq`` frequencies log-spaced over ``band``:1
+    up to the frequency where lambda / ``panels_per_wavelength`` panels give ``nmax``; at
+    each, N = perimeter * ppw / lambda rounded to even, clipped to [nmin, nmax], cosine-spaced
+    panels.
+
+    Returns ([(vertices, k, frequency_hz), ...], thickness).
+    """
+    rng = np.random.default_rng(seed)
+    t = float(rng.uniform(0.08, 0.15))
+    perimeter = polygon_perimeter(naca_symmetric(t, 8192, chord))
+    f_max = C0 * nmax / (perimeter * panels_per_wavelength)
+    cases = []
+    for f in np.geomspace(f_max / band, f_max, nfreq):
+        lam = C0 / f
+        n = int(min(nmax, max(nmin, 2 * round(0.5 * perimeter * panels_per_wavelength / lam))))  # even
+        cases.append((naca_symmetric(t, n, chord), 2.0 * math.pi / lam, float(f)))
+    return cases, t
+
+
 def snapshot_from_polygons(polygons, name='body'):
     """Reference geometry snapshot: one PEC segment (TYPE 2, N=1) per closed polygon."""
     segments = []

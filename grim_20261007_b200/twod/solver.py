@@ -22,6 +22,7 @@ from __future__ import annotations
 
 import cmath
 import math
+import os
 import threading
 import time
 
@@ -29,7 +30,7 @@ import numpy as np
 import torch
 
 from .. import _lib
-from ..device import context, ptr, require_cuda, run_concurrent
+from ..device import context, ptr, require_cuda, run_pool
 from ..execution import requested_dense_backend, requested_precision
 from . import geometry as geo
 from . import operators as ops
@@ -227,18 +228,7 @@ def _canonical_user_polarization_label(label):
 
 
 # ------------------------------------------------------------------ public solves
-def solve_monostatic_rcs_2d_single_polarization(
-        geometry_snapshot, frequencies_ghz, elevations_deg, polarization, geometry_units="inches",
-        material_base_dir=None, progress_callback=None, quality_thresholds=None, strict_quality_gate=True,
-        compute_condition_number=False, max_panels=MAX_PANELS_DEFAULT, mesh_reference_ghz=None,
-        rcs_normalization_mode="physical", cfie_alpha=0.0, abort_event=None, solver_method="auto",
-        _shared_discretization_cache=None):
-    """Single-polarization monostatic 2-D solve on the GPU (reference ``twod/solver.py:1988``).
-
-    Angle convention (coming-from): 0 deg arrives from the right, +90 deg from the top.
-    ``linear_precision('mixed')`` selects the mixed-precision path (complex64 fill and
-    LU, FP64 refinement); the default is the FP64 drop-in.
-    """
+def _validate_request(frequencies_ghz, elevations_deg, cfie_alpha, compute_condition_number):
     if not frequencies_ghz:
         raise ValueError('At least one frequency is required.')
     if not elevations_deg:
@@ -254,87 +244,94 @@ def solve_monostatic_rcs_2d_single_polarization(
     if compute_condition_number:
         raise NotImplementedError('Condition estimates run on the reference CPU path; the GPU path reports '
                                   'backward errors instead.')
-    pol = _canonical_user_polarization_label(polarization)
-    if pol not in ('TM', 'TE'):
-        raise ValueError(f'Unknown polarization {polarization!r}.')
-    require_cuda()
-    _reset_dense_backend_telemetry()
-    precision = requested_precision()
-    samples = []
-    residuals = []
-    stage = {'operators': 0.0, 'linear_solve': 0.0, 'far_field': 0.0}
-    total_steps = len(freqs) * (len(elevs) + 1)
-    done = 0
-    angles = np.asarray(elevs, dtype=np.float64)
+    return freqs, elevs
+
+
+def _solve_frequency(geometry_snapshot, geometry_units, f, elevs, pol, precision, max_panels, mesh_reference_ghz,
+                     abort_event):
+    """One (frequency, polarisation) system on the current device worker: mesh, fill,
+    solve, far field; returns host samples and telemetry."""
+    if abort_event is not None and abort_event.is_set():
+        raise InterruptedError('Solve canceled by user.')
+    t0 = time.perf_counter()
+    k = 2.0 * math.pi * f * 1e9 / C0
+    wavelength = C0 / (f * 1e9)
+    mesh_lambda = C0 / (float(mesh_reference_ghz) * 1e9) if mesh_reference_ghz else wavelength
+    polys = geo.contours_from_snapshot(geometry_snapshot, geometry_units, mesh_lambda, max_panels)
+    geom = geo.panel_geometry(polys)
+    te_diag = geo.te_curvature_correction(polys) if pol == 'TE' else None
     dev = torch.device('cuda', torch.cuda.current_device())
+    body = ops.DeviceBody(geom, te_diag, device=dev)
+    angles = np.asarray(elevs, dtype=np.float64)
     angles_dev = torch.as_tensor(angles, device=dev)
-    panel_counts = []
-    for f in freqs:
-        if abort_event is not None and abort_event.is_set():
-            raise InterruptedError('Solve canceled by user.')
-        k = 2.0 * math.pi * f * 1e9 / C0
-        wavelength = C0 / (f * 1e9)
-        mesh_lambda = C0 / (float(mesh_reference_ghz) * 1e9) if mesh_reference_ghz else wavelength
-        polys = geo.contours_from_snapshot(geometry_snapshot, geometry_units, mesh_lambda, max_panels)
-        geom = geo.panel_geometry(polys)
-        te_diag = geo.te_curvature_correction(polys) if pol == 'TE' else None
-        body = ops.DeviceBody(geom, te_diag, device=dev)
-        panel_counts.append(body.n)
-        t0 = time.perf_counter()
-        res = ops.monostatic_solve(body, k, angles, pol, precision=precision, angles_dev=angles_dev)
-        amp = res['amplitude'].cpu().numpy()
-        tele = res['telemetry']
-        berr = tele.get('backward_error_dev')
-        if berr is not None:
-            berr_h = berr.cpu().numpy()
-            if not np.all(np.isfinite(berr_h)):
-                raise RuntimeError('GPU solve produced a non-finite normwise backward error.')
-            if np.max(berr_h) > DENSE_LINEAR_BACKWARD_ERROR_MAX:
-                raise RuntimeError(f'GPU solve normwise backward error {np.max(berr_h):.6g} exceeds the release '
-                                   f'limit {DENSE_LINEAR_BACKWARD_ERROR_MAX:.6g}.')
-            resid = berr_h
-        else:
-            resid = np.full(len(elevs), float(tele.get('backward_error', 0.0)))
-        stage['linear_solve'] += time.perf_counter() - t0
-        _record_dense_backend_event(requested='gpu', used='gpu_grim', factorizations=1, rhs_columns=len(elevs),
-                                    n=body.n, label=f'{pol} pulse {f:g} GHz', gpu_device=context().device_name,
-                                    precision=precision, pivoted_panels=tele.get('pivoted_panels', 0),
-                                    refinement_steps=tele.get('refinement_steps', 0))
-        sig = _rcs_sigma_from_amp(amp, k)
-        sdb = _rcs_db_from_sigma(sig)
-        for idx, e in enumerate(elevs):
-            a = complex(amp[idx])
-            samples.append({
-                'frequency_ghz': f, 'theta_inc_deg': e, 'theta_scat_deg': e,
-                'rcs_linear': float(sig[idx]), 'rcs_db': float(sdb[idx]),
-                'rcs_amp_real': a.real, 'rcs_amp_imag': a.imag,
-                'rcs_amp_phase_deg': math.degrees(cmath.phase(a)),
-                'linear_residual': float(resid[idx]),
-            })
-            residuals.append(float(resid[idx]))
-            done += 1
-        if progress_callback is not None:
-            try:
-                progress_callback(done, total_steps, f'{pol} solved {f:g} GHz')
-            except Exception:
-                pass
+    res = ops.monostatic_solve(body, k, angles, pol, precision=precision, angles_dev=angles_dev)
+    amp = res['amplitude'].cpu().numpy()
+    tele = res['telemetry']
+    berr = tele.get('backward_error_dev')
+    if berr is not None:
+        berr_h = berr.cpu().numpy()
+        if not np.all(np.isfinite(berr_h)):
+            raise RuntimeError('GPU solve produced a non-finite normwise backward error.')
+        if np.max(berr_h) > DENSE_LINEAR_BACKWARD_ERROR_MAX:
+            raise RuntimeError(f'GPU solve normwise backward error {np.max(berr_h):.6g} exceeds the release '
+                               f'limit {DENSE_LINEAR_BACKWARD_ERROR_MAX:.6g}.')
+        resid = berr_h
+    else:
+        resid = np.full(len(elevs), float(tele.get('backward_error', 0.0)))
+    sig = _rcs_sigma_from_amp(amp, k)
+    sdb = _rcs_db_from_sigma(sig)
+    samples = []
+    for idx, e in enumerate(elevs):
+        a = complex(amp[idx])
+        samples.append({
+            'frequency_ghz': f, 'theta_inc_deg': e, 'theta_scat_deg': e,
+            'rcs_linear': float(sig[idx]), 'rcs_db': float(sdb[idx]),
+            'rcs_amp_real': a.real, 'rcs_amp_imag': a.imag,
+            'rcs_amp_phase_deg': math.degrees(cmath.phase(a)),
+            'linear_residual': float(resid[idx]),
+        })
+    event = dict(requested='gpu', used='gpu_grim', factorizations=1, rhs_columns=len(elevs), n=body.n,
+                 label=f'{pol} pulse {f:g} GHz', gpu_device=context().device_name, precision=precision,
+                 pivoted_panels=tele.get('pivoted_panels', 0), refinement_steps=tele.get('refinement_steps', 0))
+    return dict(samples=samples, residuals=[float(r) for r in resid], event=event, n=body.n,
+                seconds=time.perf_counter() - t0)
+
+
+def _frequency_cost(geometry_snapshot, geometry_units, f, n_angles):
+    """Relative cost of one frequency's system (N^3 + N^2 R, N from the panel density)."""
+    try:
+        per = geo.contours_from_snapshot(geometry_snapshot, geometry_units, C0 / (f * 1e9), 10 ** 9)
+        n = sum(len(p) for p in per)
+    except Exception:  # noqa: BLE001 - a costing failure only changes the order
+        n = 1
+    return float(n) ** 3 + float(n) ** 2 * n_angles
+
+
+def _channel_result(pol, outs, precision, stage_seconds):
+    """Assemble one polarisation's reference-shaped result from its per-frequency outputs."""
+    _reset_dense_backend_telemetry()
+    samples, residuals, counts = [], [], []
+    for o in outs:
+        samples.extend(o['samples'])
+        residuals.extend(o['residuals'])
+        counts.append(o['n'])
+        _record_dense_backend_event(**o['event'])
     metadata = {
         'solver_method': 'direct',
         'formulation': 'pulse_point_matched_efie' if pol == 'TM' else 'pulse_point_matched_mfie',
         'precision': precision,
         'device': context().device_name,
-        'panel_count_max': max(panel_counts),
-        'panel_count_min': min(panel_counts),
+        'panel_count_max': max(counts),
+        'panel_count_min': min(counts),
         'residual_norm_max': max(residuals) if residuals else 0.0,
-        'runtime_profile': {'stage_seconds': stage},
+        'runtime_profile': {'stage_seconds': stage_seconds},
         'amplitude_version': RCS_AMPLITUDE_VERSION,
         **_dense_backend_summary(),
     }
-    metadata['quality_gate'] = {'passed': bool(max(residuals) <= (DENSE_LINEAR_BACKWARD_ERROR_MAX if precision == 'double'
+    metadata['quality_gate'] = {'passed': bool(max(residuals) <= (DENSE_LINEAR_BACKWARD_ERROR_MAX
+                                                                  if precision == 'double'
                                                                   else ops.MIXED_RCS_TOL * 10)),
                                 'reason': 'backward error gate'}
-    if strict_quality_gate and not metadata['quality_gate']['passed']:
-        raise ValueError('Quality gate failed: backward error gate')
     return {
         'solver': '2d_bie_mom_rcs',
         'scattering_mode': 'monostatic',
@@ -347,6 +344,79 @@ def solve_monostatic_rcs_2d_single_polarization(
     }
 
 
+def _sweep(geometry_snapshot, frequencies_ghz, elevations_deg, pols, geometry_units, progress_callback,
+           cfie_alpha, compute_condition_number, max_panels, mesh_reference_ghz, abort_event):
+    """Solve every (polarisation, frequency) system of a request on the device worker pool;
+    returns {pol: reference-shaped channel result}."""
+    freqs, elevs = _validate_request(frequencies_ghz, elevations_deg, cfie_alpha, compute_condition_number)
+    require_cuda()
+    precision = requested_precision()
+    jobs, keys, costs = [], [], []
+    for pol in pols:
+        for f in freqs:
+            jobs.append(lambda f=f, pol=pol: _solve_frequency(geometry_snapshot, geometry_units, f, elevs, pol,
+                                                               precision, max_panels, mesh_reference_ghz,
+                                                               abort_event))
+            keys.append((pol, f))
+            costs.append(_frequency_cost(geometry_snapshot, geometry_units, f, len(elevs)) if len(freqs) > 1 else 1.0)
+    total = len(jobs) * (len(elevs) + 1)
+    progress_state = {'done': 0}
+
+    def on_done(i, out):
+        progress_state['done'] += len(elevs) + 1
+        if progress_callback is not None:
+            pol, f = keys[i]
+            try:
+                progress_callback(progress_state['done'], total, f'{pol} solved {f:g} GHz')
+            except Exception:  # noqa: BLE001 - progress reporting never fails a solve
+                pass
+
+    t0 = time.perf_counter()
+    outs = run_pool(jobs, workers=sweep_workers(len(jobs)), costs=costs, on_done=on_done)
+    wall = time.perf_counter() - t0
+    channels = {}
+    for pol in pols:
+        mine = [o for (p, _f), o in zip(keys, outs) if p == pol]
+        stage = {'operators': 0.0, 'linear_solve': sum(o['seconds'] for o in mine), 'far_field': 0.0,
+                 'wall': wall}
+        channels[pol] = _channel_result(pol, mine, precision, stage)
+    return channels
+
+
+def sweep_workers(njobs):
+    """Device workers for a request: GRIM_SWEEP_WORKERS (default 4), at most one per system."""
+    try:
+        w = int(os.environ.get('GRIM_SWEEP_WORKERS', '4'))
+    except ValueError:
+        w = 4
+    return max(1, min(w, njobs))
+
+
+def solve_monostatic_rcs_2d_single_polarization(
+        geometry_snapshot, frequencies_ghz, elevations_deg, polarization, geometry_units="inches",
+        material_base_dir=None, progress_callback=None, quality_thresholds=None, strict_quality_gate=True,
+        compute_condition_number=False, max_panels=MAX_PANELS_DEFAULT, mesh_reference_ghz=None,
+        rcs_normalization_mode="physical", cfie_alpha=0.0, abort_event=None, solver_method="auto",
+        _shared_discretization_cache=None):
+    """Single-polarization monostatic 2-D solve on the GPU (reference ``twod/solver.py:1988``).
+
+    Angle convention (coming-from): 0 deg arrives from the right, +90 deg from the top.
+    ``linear_precision('mixed')`` selects the mixed-precision path (complex64 fill and
+    LU, FP64 refinement); the default is the FP64 drop-in.  A frequency sweep runs its
+    systems on a pool of device workers (``GRIM_SWEEP_WORKERS``, largest system first),
+    the analogue of the reference's frequency workers (``execution/frequency_sweep.py``);
+    samples are returned in frequency order.
+    """
+    pol = _canonical_user_polarization_label(polarization)
+    if pol not in ('TM', 'TE'):
+        raise ValueError(f'Unknown polarization {polarization!r}.')
+    out = _sweep(geometry_snapshot, frequencies_ghz, elevations_deg, [pol], geometry_units, progress_callback,
+                 cfie_alpha, compute_condition_number, max_panels, mesh_reference_ghz, abort_event)[pol]
+    if strict_quality_gate and not out['metadata']['quality_gate']['passed']:
+        raise ValueError('Quality gate failed: backward error gate')
+    return out
+
+
 _CO_POLARIZED_2D_CHANNELS = (('VV', 'TE'), ('HH', 'TM'))
 
 
@@ -357,30 +427,17 @@ def solve_monostatic_rcs_2d(geometry_snapshot, frequencies_ghz, elevations_deg, 
                             solver_method="auto"):
     """Both physical co-polarised channels (reference ``twod/solver.py:3193``): VV (TE) then HH (TM).
 
-    The two channels are independent systems; they are solved at the same time on two
-    device workers (own handle, stream and host thread), so that one channel's
-    latency-bound factorization steps overlap the other's tensor-core updates.  Samples
-    and metadata are those of the two single-polarisation solves, VV first.
+    The channels' systems (one per polarisation and frequency) are independent; they are
+    solved together on the device worker pool, so one system's latency-bound
+    factorization steps overlap another's tensor-core updates.  Samples and metadata
+    are those of the two single-polarisation solves, VV first.
     """
-    progress_lock = threading.Lock()
-
-    def progress(*a):
-        if progress_callback is not None:
-            with progress_lock:
-                progress_callback(*a)
-
-    def channel(pol):
-        return lambda: solve_monostatic_rcs_2d_single_polarization(
-            geometry_snapshot, frequencies_ghz, elevations_deg, pol, geometry_units=geometry_units,
-            material_base_dir=material_base_dir, progress_callback=progress if progress_callback else None,
-            quality_thresholds=quality_thresholds, strict_quality_gate=strict_quality_gate,
-            compute_condition_number=compute_condition_number, max_panels=max_panels,
-            mesh_reference_ghz=mesh_reference_ghz, rcs_normalization_mode=rcs_normalization_mode,
-            abort_event=abort_event, solver_method=solver_method)
-
-    require_cuda()
-    results = run_concurrent([channel(pol) for _export, pol in _CO_POLARIZED_2D_CHANNELS])
-    channels = {export: res for (export, _pol), res in zip(_CO_POLARIZED_2D_CHANNELS, results)}
+    channels_by_pol = _sweep(geometry_snapshot, frequencies_ghz, elevations_deg,
+                             [pol for _export, pol in _CO_POLARIZED_2D_CHANNELS], geometry_units, progress_callback,
+                             0.0, compute_condition_number, max_panels, mesh_reference_ghz, abort_event)
+    channels = {export: channels_by_pol[pol] for export, pol in _CO_POLARIZED_2D_CHANNELS}
+    if strict_quality_gate and not all(c['metadata']['quality_gate']['passed'] for c in channels.values()):
+        raise ValueError('Quality gate failed: backward error gate')
     samples = []
     for export, _pol in _CO_POLARIZED_2D_CHANNELS:
         for s in channels[export]['samples']:

@@ -140,3 +140,27 @@ def test_concurrent_channels_match_single_channel_solves(ctx):
                 a2 = np.array([complex(s['rcs_amp_real'], s['rcs_amp_imag']) for s in both['samples']
                                if s['polarization'] == exp])
                 np.testing.assert_allclose(a2, a1, rtol=1e-13, atol=1e-13 * np.max(np.abs(a1)))
+
+
+def test_frequency_sweep_pool_matches_single_frequency_solves(ctx):
+    """A multi-frequency request runs its systems on the device worker pool (largest first);
+    every frequency's samples equal a one-frequency solve, in request order."""
+    from grim_20261007_b200.execution import linear_precision
+    from grim_20261007_b200.twod.solver import solve_monostatic_rcs_2d_single_polarization as solve1
+    v = S.naca_symmetric(0.1, 160)
+    snap = S.snapshot_from_polygons([v])
+    for sg in snap['segments']:
+        sg['properties'][1] = '-10'  # automatic meshing: 10 panels per wavelength
+    freqs = [0.9, 3.1, 1.7, 2.4, 0.6]
+    ang = list(np.arange(0.0, 180.0, 3.0))
+    with linear_precision('mixed'):
+        swept = solve1(snap, freqs, ang, 'TM', geometry_units='meters', strict_quality_gate=False)
+        assert [s['frequency_ghz'] for s in swept['samples'][::len(ang)]] == freqs
+        for i, f in enumerate(freqs):
+            one = solve1(snap, [f], ang, 'TM', geometry_units='meters', strict_quality_gate=False)
+            a1 = np.array([complex(s['rcs_amp_real'], s['rcs_amp_imag']) for s in one['samples']])
+            block = swept['samples'][i * len(ang):(i + 1) * len(ang)]
+            a2 = np.array([complex(s['rcs_amp_real'], s['rcs_amp_imag']) for s in block])
+            np.testing.assert_allclose(a2, a1, rtol=1e-13, atol=1e-13 * np.max(np.abs(a1)))
+    counts = swept['metadata']
+    assert counts['dense_gpu_solve_count'] == len(freqs) and counts['panel_count_max'] > counts['panel_count_min']

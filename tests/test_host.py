@@ -104,3 +104,14 @@ def test_synthetic_workloads_are_seeded_and_clockwise():
     gen, length, half = S.ogive_case(3)
     assert gen[0, 0] == 0 and gen[-1, 0] == 0 and gen[0, 1] > gen[-1, 1]
     assert 2 <= length <= 4 and 15 <= half <= 30
+
+
+def test_airfoil_sweep_case_sizes():
+    from grim_20261007_b200 import synthetic as S
+    cases, t = S.airfoil_sweep_case(3, 256)
+    ns = [len(v) for v, _k, _f in cases]
+    fs = [f for _v, _k, f in cases]
+    assert len(cases) == 256 and all(n % 2 == 0 for n in ns)
+    assert max(ns) == 4096 and min(ns) >= 64
+    assert abs(fs[-1] / fs[0] - 20.0) < 1e-9 and all(b > a for a, b in zip(fs, fs[1:]))
+    assert ns == sorted(ns)
