@@ -22,7 +22,7 @@ import numpy as np
 import torch
 
 from .. import _lib
-from ..device import context, ptr, require_cuda
+from ..device import context, ptr, require_cuda, run_pool
 from ..execution import requested_precision
 from ..twod import operators as ops2d
 
@@ -152,50 +152,82 @@ class BorDevice:
             self._maps[key] = (torch.from_numpy(rf).to('cuda'), torch.from_numpy(rw).to('cuda'), nred)
         return self._maps[key]
 
-    def matrix(self, m):
+    def matrix(self, m, ctx=None):
+        ctx = ctx or self.ctx
         rf, rw, nred = self.mode_map(m)
         Z = torch.empty((nred, nred), dtype=torch.complex128, device='cuda')
-        _lib.check(self.ctx.lib.grim_bor_assemble(self.ctx.h, self.ne, ptr(self.nodes_dev), self.k, self.mmax, m,
-                                                  ptr(self.mom), nred, ptr(rf), ptr(rw), ptr(Z), nred),
+        _lib.check(ctx.lib.grim_bor_assemble(ctx.h, self.ne, ptr(self.nodes_dev), self.k, self.mmax, m,
+                                             ptr(self.mom), nred, ptr(rf), ptr(rw), ptr(Z), nred),
                    'grim_bor_assemble')
         return Z
 
-    def excitation(self, m, th_dev, far):
+    def excitation(self, m, th_dev, far, ctx=None):
+        ctx = ctx or self.ctx
         rf, rw, nred = self.mode_map(m)
         nth = int(th_dev.numel())
         V = torch.empty((2 * nth, nred), dtype=torch.complex128, device='cuda')
-        _lib.check(self.ctx.lib.grim_bor_excitation(self.ctx.h, self.ne, ptr(self.nodes_dev), self.k, m, nth,
-                                                    ptr(th_dev), int(far), nred, ptr(rf), ptr(rw), ptr(V), nred),
+        _lib.check(ctx.lib.grim_bor_excitation(ctx.h, self.ne, ptr(self.nodes_dev), self.k, m, nth,
+                                               ptr(th_dev), int(far), nred, ptr(rf), ptr(rw), ptr(V), nred),
                    'grim_bor_excitation')
         return V
 
 
-def solve_bor_device(points, k, thetas_deg, mmax, precision='double', tol=None, ctx=None):
-    """Device path: returns (F[2 nth] complex128 on the host, telemetry)."""
-    dev = BorDevice(points, k, mmax, ctx=ctx)
-    th = torch.as_tensor(np.asarray(thetas_deg, dtype=np.float64), device='cuda')
+def _solve_mode(dev, m, th, precision, tol, ctx=None):
+    """One Fourier mode on ``ctx`` (default: the current device worker): assemble, excite,
+    solve and project; returns (this mode's far-field contribution [2 nth], telemetry)."""
+    ctx = ctx or context()
+    Z = dev.matrix(m, ctx=ctx)
+    V = dev.excitation(m, th, far=False, ctx=ctx)
+    W = dev.excitation(m, th, far=True, ctx=ctx)
+    tele = {'fp64_fallback': False}
+    if precision == 'mixed':
+        V0 = V.clone()
+        try:
+            st = ops2d.solve_inplace(Z, V, 'mixed', tol=tol, ctx=ctx)
+        except _lib.GrimNotConverged:
+            # ill-conditioned mode: the reference's ladder falls back to the double LU
+            tele['fp64_fallback'] = True
+            V = V0
+            st = ops2d.solve_inplace(Z, V, 'double', ctx=ctx)
+    else:
+        st = ops2d.solve_inplace(Z, V, precision, tol=tol, ctx=ctx)
+    tele['refinement_steps'] = int(st.get('refinement_steps', 0))
     nth = int(th.numel())
-    amp = torch.zeros(2 * nth, dtype=torch.complex128, device='cuda')
-    tele = {'modes': 2 * mmax + 1, 'refinement_steps': 0, 'max_backward_error': 0.0, 'nxi_max': dev.nxi}
-    for m in range(-mmax, mmax + 1):
-        Z = dev.matrix(m)
-        V = dev.excitation(m, th, far=False)
-        W = dev.excitation(m, th, far=True)
-        if precision == 'mixed':
-            V0 = V.clone()
-            try:
-                st = ops2d.solve_inplace(Z, V, 'mixed', tol=tol, ctx=dev.ctx)
-            except _lib.GrimNotConverged:
-                # ill-conditioned mode: the reference's ladder falls back to the double LU
-                tele['fp64_fallback_modes'] = tele.get('fp64_fallback_modes', 0) + 1
-                V = V0
-                st = ops2d.solve_inplace(Z, V, 'double', ctx=dev.ctx)
-        else:
-            st = ops2d.solve_inplace(Z, V, precision, tol=tol, ctx=dev.ctx)
-        tele['refinement_steps'] = max(tele['refinement_steps'], int(st.get('refinement_steps', 0)))
-        nred = int(Z.shape[0])
-        _lib.check(dev.ctx.lib.grim_bor_farfield_accumulate(dev.ctx.h, nred, 2 * nth, ptr(W), nred, ptr(V), nred,
-                                                            ptr(amp)), 'grim_bor_farfield_accumulate')
+    part = torch.zeros(2 * nth, dtype=torch.complex128, device='cuda')
+    nred = int(Z.shape[0])
+    _lib.check(ctx.lib.grim_bor_farfield_accumulate(ctx.h, nred, 2 * nth, ptr(W), nred, ptr(V), nred, ptr(part)),
+               'grim_bor_farfield_accumulate')
+    return part, tele
+
+
+def solve_bor_device(points, k, thetas_deg, mmax, precision='double', tol=None, ctx=None, workers=None):
+    """Device path: returns (F[2 nth] complex128 on the host, telemetry).
+
+    The modal moments are built once; the 2 mmax + 1 per-mode systems are independent and
+    run on the device worker pool (``GRIM_SWEEP_WORKERS`` workers), each contributing its
+    own far-field vector; the contributions are summed in mode order, so the result does
+    not depend on the scheduling.  With an explicit ``ctx`` (a serving slot) the modes run
+    in turn on that handle.
+    """
+    from ..twod.solver import sweep_workers
+    dev = BorDevice(points, k, mmax, ctx=ctx)
+    for m in (0, 1, -1, 2):
+        dev.mode_map(m)  # build the shared pole maps before the workers read them
+    th = torch.as_tensor(np.asarray(thetas_deg, dtype=np.float64), device='cuda')
+    modes = list(range(-mmax, mmax + 1))
+    if ctx is not None:
+        outs = [_solve_mode(dev, m, th, precision, tol, ctx=ctx) for m in modes]
+    else:
+        jobs = [(lambda m=m: _solve_mode(dev, m, th, precision, tol)) for m in modes]
+        outs = run_pool(jobs, workers=sweep_workers(len(jobs)) if workers is None else workers)
+    amp = torch.zeros(2 * int(th.numel()), dtype=torch.complex128, device='cuda')
+    for part, _t in outs:
+        amp += part
+    tele = {'modes': 2 * mmax + 1, 'max_backward_error': 0.0, 'nxi_max': dev.nxi,
+            'refinement_steps': max(t['refinement_steps'] for _p, t in outs)}
+    fallbacks = sum(1 for _p, t in outs if t['fp64_fallback'])
+    if fallbacks:
+        tele['fp64_fallback_modes'] = fallbacks
     F = amp.cpu().numpy() * (-1j * k * ETA0 / (4.0 * np.pi))
     tele['n_unknowns'] = 2 * (dev.ne + 1)
     return F, tele

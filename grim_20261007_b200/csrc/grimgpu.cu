@@ -431,7 +431,6 @@ static int smem_opt_in() {
     if (done) return GRIM_OK;
     const int tri = (NB * NBP + NB) * (int)sizeof(C);
     GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_panel_apply<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, tri));
-    GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_diag_lu<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, tri));
     GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_trsm_diag<C, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, tri));
     GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_trsm_diag<C, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, tri));
     done = true;
@@ -464,7 +463,7 @@ static int getrf_impl(grim_context *h, int n, C *A, int64_t lda, int *ipiv, int 
     const size_t tri = (size_t)(NB * NBP + NB) * sizeof(C);
     for (int p = 0; p < npan; ++p) {
         const int j = p * NB, nbj = std::min(NB, n - j);
-        k_diag_lu<C><<<1, 256, (size_t)NB * NBP * sizeof(C), h->stream>>>(n, A, lda, j, nbj, bcol, cert + p, ipiv);
+        k_diag_lu<C><<<1, 256, 0, h->stream>>>(n, A, lda, j, nbj, bcol, cert + p, ipiv);
         GRIM_CHECK_LAUNCH_W(h, kname("k_diag_lu", sizeof(C)), 8.0 * nbj * nbj * nbj / 3.0, 0);
         const int rest = n - j - nbj;
         if (rest > 0) {

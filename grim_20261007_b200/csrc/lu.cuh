@@ -229,123 +229,90 @@ __device__ __forceinline__ void stage_diag(const C *A, int64_t lda, int j, int n
 }
 
 // ------------------------------------------------------------------ diagonal block
-// Warp-synchronous unpivoted LU of a 32 x 32 block held one row per lane (lane r owns
-// row r in v[0..31]): per column the pivot and then each pivot-row entry are broadcast
-// with shuffles.  Certificate: |a_rk^(k)|_1 <= |a_kk^(k)|_1 for rows r > k < m.
-template <typename C>
-__device__ __forceinline__ void warp_lu32(C (&v)[32], int m, int &bad) {
-    const int lane = threadIdx.x & 31;
+// Runtime-indexed read / write of a small register array through a static select chain
+// (keeps the array in registers).
+template <typename C, int L>
+__device__ __forceinline__ C vget(const C (&v)[L], int idx) {
+    C x = czero<C>();
 #pragma unroll
-    for (int kk = 0; kk < 32; ++kk) {
-        if (kk < m) {
-            const C piv = shfl_c(v[kk], kk);
-            const auto pa = cabs1(piv);
-            const bool below = lane > kk && lane < m;
-            if (below && !(cabs1(v[kk]) <= pa)) bad = 1;
-            if (pa == 0) bad = 1;
-            const C rp = pa != 0 ? crecip(piv) : czero<C>();
-            if (below) v[kk] = cmul(v[kk], rp);
+    for (int i = 0; i < L; ++i)
+        if (i == idx) x = v[i];
+    return x;
+}
+template <typename C, int L>
+__device__ __forceinline__ void vset(C (&v)[L], int idx, C x) {
 #pragma unroll
-            for (int c = kk + 1; c < 32; ++c) {
-                const C u = shfl_c(v[c], kk);
-                if (below) cfms(v[c], v[kk], u);
-            }
-        }
-    }
+    for (int i = 0; i < L; ++i)
+        if (i == idx) v[i] = x;
 }
 
-// One CTA of 256 threads: unpivoted LU of the nbj x nbj diagonal block (nbj <= 64) as
-// LU(A11) [warp 0] -> U12 = inv(L11) A12 and L21 = A21 inv(U11) [warps 0-1, one lane per
-// column / row] -> A22 -= L21 U12 [all threads] -> LU(A22) [warp 0]; certificate over
-// the whole block, backup of the block, identity ipiv entries.
+// One CTA of 256 threads: unpivoted right-looking LU of the nbj x nbj diagonal block
+// (nbj <= 64), the diagonal-pivot certificate, a backup of the block and identity ipiv
+// entries.  Warp w owns rows 32 (w / 4) + lane and columns 16 (w % 4) .. + 15 in
+// registers, so that a warp whose rows or columns are all factored is idle as a whole.
+// Step k (three phases, two barriers; shared buffers double-buffered by step parity):
+//   the owners of row k publish it, the owner of a_kk its reciprocal;
+//   the warps holding column k form l_rk = a_rk / a_kk for their rows r > k;
+//   every warp with rows and columns beyond k applies a_rc -= l_rk a_kc.
+// Certificate: |a_rk^(k)|_1 <= |a_kk^(k)|_1 for r > k, and a_kk != 0.
 template <typename C>
 __global__ void __launch_bounds__(256)
 k_diag_lu(int n, C *A, int64_t lda, int j, int nbj, C *backup_col, int *cert, int *ipiv) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    C *S = reinterpret_cast<C *>(smem_raw);  // NB x NB block, leading dim NBP (dynamic smem)
-    __shared__ int s_bad;
+    __shared__ C rowbuf[2][NB];
+    __shared__ C lbuf[2][NB];
+    __shared__ C rpiv[2];
     const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
-    if (t == 0) s_bad = 0;
-    for (int e = t; e < NB * NB; e += 256) {
-        const int r = e & 63, c = e >> 6;
+    const int h = warp >> 2, g = warp & 3, r = 32 * h + lane, c0 = 16 * g;
+    C v[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+        const int c = c0 + i;
         C x = czero<C>();
         if (r < nbj && c < nbj) {
             x = A[(int64_t)(j + c) * lda + j + r];
             backup_col[(int64_t)c * n + r] = x;
         }
-        S[c * NBP + r] = x;
+        v[i] = x;
     }
-    for (int r = t; r < nbj; r += 256) ipiv[j + r] = j + r + 1;
-    __syncthreads();
-    const int m1 = min(32, nbj), m2 = nbj - m1;
+    if (t < nbj) ipiv[j + t] = j + t + 1;
     int bad = 0;
-    C v[32];
-    // LU(A11)
-    if (warp == 0) {
+#pragma unroll 1
+    for (int k = 0; k < nbj; ++k) {
+        const int buf = k & 1, gk = k >> 4, ik = k & 15;
+        if (r == k) {
 #pragma unroll
-        for (int c = 0; c < 32; ++c) v[c] = S[c * NBP + lane];
-        warp_lu32(v, m1, bad);
-#pragma unroll
-        for (int c = 0; c < 32; ++c) S[c * NBP + lane] = v[c];
-    }
-    __syncthreads();
-    if (m2 > 0) {
-        // warp 0: column lane of A12 -> U12 (unit lower L11);  warp 1: row lane of A21 -> L21
-        if (warp == 0) {
-            const int col = 32 + lane;
-#pragma unroll
-            for (int r = 0; r < 32; ++r) v[r] = S[col * NBP + r];
-#pragma unroll
-            for (int r = 0; r < 32; ++r)
-#pragma unroll
-                for (int p = 0; p < r; ++p) cfms(v[r], S[p * NBP + r], v[p]);
-#pragma unroll
-            for (int r = 0; r < 32; ++r) S[col * NBP + r] = v[r];
-        } else if (warp == 1) {
-            const int row = 32 + lane;
-#pragma unroll
-            for (int c = 0; c < 32; ++c) v[c] = S[c * NBP + row];
-#pragma unroll
-            for (int c = 0; c < 32; ++c) {
-#pragma unroll
-                for (int p = 0; p < c; ++p) cfms(v[c], v[p], S[c * NBP + p]);
-                const C ucc = S[c * NBP + c];
-                v[c] = cmul(v[c], crecip(ucc));
-                if (row < nbj && !(cabs1(cmul(v[c], ucc)) <= cabs1(ucc))) bad = 1;
-            }
-#pragma unroll
-            for (int c = 0; c < 32; ++c) S[c * NBP + row] = v[c];
-        }
-        __syncthreads();
-        // A22 -= L21 U12: thread owns 4 entries (row 32 + (t & 31), columns 32 + (t >> 5) + 8 q)
-        {
-            const int r = 32 + (t & 31);
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const int c = 32 + (t >> 5) + 8 * q;
-                C acc = S[c * NBP + r];
-#pragma unroll 8
-                for (int p = 0; p < 32; ++p) cfms(acc, S[p * NBP + r], S[c * NBP + p]);
-                S[c * NBP + r] = acc;
+            for (int i = 0; i < 16; ++i) rowbuf[buf][c0 + i] = v[i];
+            if (g == gk) {
+                const C piv = vget(v, ik);
+                if (cabs1(piv) == 0) bad = 1;
+                rpiv[buf] = crecip(piv);
             }
         }
         __syncthreads();
-        // LU(A22)
-        if (warp == 0) {
+        if (g == gk && 32 * h + 31 > k) {
+            if (r > k && r < nbj) {
+                const C a = vget(v, ik);
+                if (!(cabs1(a) <= cabs1(rowbuf[buf][k]))) bad = 1;
+                const C l = cmul(a, rpiv[buf]);
+                vset(v, ik, l);
+                lbuf[buf][r] = l;
+            }
+        }
+        __syncthreads();
+        if (c0 + 15 > k && 32 * h + 31 > k && r > k && r < nbj) {
+            const C l = lbuf[buf][r];
+            const C *u = rowbuf[buf] + c0;
 #pragma unroll
-            for (int c = 0; c < 32; ++c) v[c] = S[(32 + c) * NBP + 32 + lane];
-            warp_lu32(v, m2, bad);
-#pragma unroll
-            for (int c = 0; c < 32; ++c) S[(32 + c) * NBP + 32 + lane] = v[c];
+            for (int i = 0; i < 16; ++i)
+                if (c0 + i > k) cfms(v[i], l, u[i]);
         }
     }
-    if (bad) s_bad = 1;
-    __syncthreads();
-    for (int e = t; e < NB * NB; e += 256) {
-        const int r = e & 63, c = e >> 6;
-        if (r < nbj && c < nbj) A[(int64_t)(j + c) * lda + j + r] = S[c * NBP + r];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+        const int c = c0 + i;
+        if (r < nbj && c < nbj) A[(int64_t)(j + c) * lda + j + r] = v[i];
     }
-    if (t == 0 && s_bad) atomicOr(cert, 1);
+    if (__syncthreads_or(bad) && t == 0) atomicOr(cert, 1);
 }
 
 // ------------------------------------------------------------------ pivoted panel (fallback)

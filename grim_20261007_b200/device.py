@@ -90,6 +90,9 @@ def context(device=None):
     return ctx
 
 
+_busy = set()  # (device, index) of workers held by a running pool
+
+
 def _worker(dev, index):
     with _ctx_lock:
         w = _workers.get((dev, index))
@@ -98,6 +101,25 @@ def _worker(dev, index):
                 w = (Context(dev), torch.cuda.Stream(dev))
             _workers[(dev, index)] = w
     return w
+
+
+def _acquire(dev, count):
+    """Indices of ``count`` workers no other pool holds (new ones are created on demand), so
+    that pools started from different host threads never share a handle or a stream."""
+    with _ctx_lock:
+        got, i = [], 0
+        while len(got) < count:
+            if (dev, i) not in _busy:
+                _busy.add((dev, i))
+                got.append(i)
+            i += 1
+    return got
+
+
+def _release(dev, indices):
+    with _ctx_lock:
+        for i in indices:
+            _busy.discard((dev, i))
 
 
 def all_contexts(device=None):
@@ -191,8 +213,10 @@ def run_pool(fns, workers=None, costs=None, on_done=None, device=None):
             state['next'] += 1
             return i
 
+    held = _acquire(dev, workers)
+
     def loop(w):
-        with worker(w, dev) as (_ctx, stream):
+        with worker(held[w], dev) as (_ctx, stream):
             stream.wait_event(ready)
             while True:
                 i = take()
@@ -213,8 +237,11 @@ def run_pool(fns, workers=None, costs=None, on_done=None, device=None):
             done.record(stream)
             return done
 
-    with ThreadPoolExecutor(max_workers=workers) as ex:
-        events = list(ex.map(loop, range(workers)))
+    try:
+        with ThreadPoolExecutor(max_workers=workers) as ex:
+            events = list(ex.map(loop, range(workers)))
+    finally:
+        _release(dev, held)
     for done in events:
         caller.wait_event(done)
     if state['error'] is not None:
