@@ -33,6 +33,15 @@ METRIC = 'RCS solves/s at N=2048 (mixed vs FP64 GPU, <=0.05 dB); p50/p99 serve l
 UNIT = 'solves/s'
 
 
+# DRAM bytes (read + write) of one captured launch of the tensor-core kernels, from ncu
+# (profiles/k_tc_gemm_airfoil_n2048.md, profiles/k_oz_gemm_airfoil_n2048.md), with that
+# launch's algorithmic flops; a launch's traffic is scaled from it by its flops.
+NCU_TRAFFIC = {
+    'k_tc_gemm<128>': (8.833024e6, 8.0 * 512 * 720 * 256),
+    'k_oz_gemm': (454.434816e6 + 23.171584e6, 8.0 * 2048 * 2048 * 720),
+}
+
+
 def _peaks():
     try:
         with open(os.path.join(ROOT, 'MEASURED_PEAKS.json')) as f:
@@ -439,7 +448,13 @@ def main():
                     'traffic': None, 'kernel': dom_name, 'launches': dom['launches'],
                     'avg_launch_ms': dom['ms'] / dom['launches'], 'flops_per_launch': dom['flops'] / dom['launches'],
                     'share_of_step': dom['ms'] / step_ms, 'peak_source': src,
-                    'peak_note': 'dense bf16 tensor peak (measured); the kernel runs complex FP32 on CUDA cores'}
+                    'peak_note': 'measured dense bf16 tensor peak; the kernel computes complex64 as split TF32 '
+                                 '(3 tcgen05 TF32 products, 8 M N K algorithmic flops counted once) and the dense '
+                                 'TF32 rate is half the bf16 rate'}
+        if dom_name in NCU_TRAFFIC:
+            nbytes, nflops = NCU_TRAFFIC[dom_name]
+            roofline['traffic'] = nbytes * (dom['flops'] / dom['launches']) / nflops
+            roofline['traffic_note'] = 'bytes per launch: one ncu capture scaled by the launch flops'
     else:
         achieved = dom['bytes'] / (dom['ms'] * 1e-3) / 1e9
         roofline = {'bound': 'hbm', 'achieved': achieved, 'peak': hbm, 'unit': 'GB/s', 'frac': achieved / hbm,
