@@ -54,13 +54,40 @@ template <typename C> __host__ __device__ __forceinline__ C cdiv(C a, C b) {
         return mk((ar * r + ai) / d, (ai * r - ar) / d);
     }
 }
+// Reciprocal 1/x: on the device the hardware approximation refined by Newton-Raphson
+// (y <- y + y (1 - x y), one step for FP32, two for FP64, from the ~2^-20 seed of the
+// FP64 approximation), within an ulp or so of the rounded quotient; plain division on
+// the host.  Used on the pivot chain of the LU, where a full IEEE division sits on the
+// critical path of every column step.
+__host__ __device__ __forceinline__ float rcp_nr(float x) {
+#ifdef __CUDA_ARCH__
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    const float e = fmaf(-x, y, 1.0f);
+    return fmaf(y, e, y);
+#else
+    return 1.0f / x;
+#endif
+}
+__host__ __device__ __forceinline__ double rcp_nr(double x) {
+#ifdef __CUDA_ARCH__
+    double y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+    double e = fma(-x, y, 1.0);
+    y = fma(y, e, y);
+    e = fma(-x, y, 1.0);
+    return fma(y, e, y);
+#else
+    return 1.0 / x;
+#endif
+}
 // 1 / b with the components scaled by max(|re|, |im|) first (no over/underflow of |b|^2)
 template <typename C> __host__ __device__ __forceinline__ C crecip(C b) {
     using R = typename real_of<C>::type;
     const R s = fmax(fabs(b.x), fabs(b.y));
-    const R rs = (R)1 / s;
+    const R rs = rcp_nr(s);
     const R br = b.x * rs, bi = b.y * rs;
-    const R d = (R)1 / (br * br + bi * bi);
+    const R d = rcp_nr(br * br + bi * bi);
     return mk(br * d * rs, -bi * d * rs);
 }
 template <typename C> __host__ __device__ __forceinline__ typename real_of<C>::type cabs1(C a) {

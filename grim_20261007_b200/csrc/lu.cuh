@@ -249,9 +249,11 @@ __device__ __forceinline__ void vset(C (&v)[L], int idx, C x) {
 // One CTA of 256 threads: unpivoted right-looking LU of the nbj x nbj diagonal block
 // (nbj <= 64), the diagonal-pivot certificate, a backup of the block and identity ipiv
 // entries.  Warp w owns rows 32 (w / 4) + lane and columns 16 (w % 4) .. + 15 in
-// registers, so that a warp whose rows or columns are all factored is idle as a whole.
-// Step k (three phases, two barriers; shared buffers double-buffered by step parity):
-//   the owners of row k publish it, the owner of a_kk its reciprocal;
+// registers, so that a warp whose rows or columns are all factored skips a step as a
+// whole.  The column loop is split into 4 groups of 16 with the inner 16 unrolled, so
+// every register index is a compile-time constant.  Step k (two barriers; shared buffers
+// double-buffered by step parity):
+//   the owners of row k publish it;
 //   the warps holding column k form l_rk = a_rk / a_kk for their rows r > k;
 //   every warp with rows and columns beyond k applies a_rc -= l_rk a_kc.
 // Certificate: |a_rk^(k)|_1 <= |a_kk^(k)|_1 for r > k, and a_kk != 0.
@@ -260,7 +262,6 @@ __global__ void __launch_bounds__(256)
 k_diag_lu(int n, C *A, int64_t lda, int j, int nbj, C *backup_col, int *cert, int *ipiv) {
     __shared__ C rowbuf[2][NB];
     __shared__ C lbuf[2][NB];
-    __shared__ C rpiv[2];
     const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
     const int h = warp >> 2, g = warp & 3, r = 32 * h + lane, c0 = 16 * g;
     C v[16];
@@ -276,35 +277,45 @@ k_diag_lu(int n, C *A, int64_t lda, int j, int nbj, C *backup_col, int *cert, in
     }
     if (t < nbj) ipiv[j + t] = j + t + 1;
     int bad = 0;
+    const int nkg = (nbj + 15) >> 4;
 #pragma unroll 1
-    for (int k = 0; k < nbj; ++k) {
-        const int buf = k & 1, gk = k >> 4, ik = k & 15;
-        if (r == k) {
+    for (int kg = 0; kg < nkg; ++kg) {
 #pragma unroll
-            for (int i = 0; i < 16; ++i) rowbuf[buf][c0 + i] = v[i];
-            if (g == gk) {
-                const C piv = vget(v, ik);
-                if (cabs1(piv) == 0) bad = 1;
-                rpiv[buf] = crecip(piv);
-            }
-        }
-        __syncthreads();
-        if (g == gk && 32 * h + 31 > k) {
-            if (r > k && r < nbj) {
-                const C a = vget(v, ik);
-                if (!(cabs1(a) <= cabs1(rowbuf[buf][k]))) bad = 1;
-                const C l = cmul(a, rpiv[buf]);
-                vset(v, ik, l);
-                lbuf[buf][r] = l;
-            }
-        }
-        __syncthreads();
-        if (c0 + 15 > k && 32 * h + 31 > k && r > k && r < nbj) {
-            const C l = lbuf[buf][r];
-            const C *u = rowbuf[buf] + c0;
+        for (int ik = 0; ik < 16; ++ik) {
+            const int k = 16 * kg + ik;
+            if (k >= nbj) break;
+            const int buf = k & 1;
+            if (r == k) {
 #pragma unroll
-            for (int i = 0; i < 16; ++i)
-                if (c0 + i > k) cfms(v[i], l, u[i]);
+                for (int i = 0; i < 16; ++i) rowbuf[buf][c0 + i] = v[i];
+            }
+            __syncthreads();
+            const bool rows_left = 32 * h + 31 > k;
+            const bool below = r > k && r < nbj;
+            if (g == kg && rows_left) {
+                const C piv = rowbuf[buf][k];
+                if (r == k && cabs1(piv) == 0) bad = 1;
+                if (below) {
+                    const C a = v[ik];
+                    if (!(cabs1(a) <= cabs1(piv))) bad = 1;
+                    v[ik] = cmul(a, crecip(piv));
+                    lbuf[buf][r] = v[ik];
+                }
+            }
+            __syncthreads();
+            if (rows_left && below) {
+                if (g > kg) {
+                    const C l = lbuf[buf][r];
+                    const C *u = rowbuf[buf] + c0;
+#pragma unroll
+                    for (int i = 0; i < 16; ++i) cfms(v[i], l, u[i]);
+                } else if (g == kg) {
+                    const C l = v[ik];
+                    const C *u = rowbuf[buf] + c0;
+#pragma unroll
+                    for (int i = ik + 1; i < 16; ++i) cfms(v[i], l, u[i]);
+                }
+            }
         }
     }
 #pragma unroll
