@@ -180,6 +180,8 @@ def _solve_mode(dev, m, th, precision, tol, ctx=None):
     V = dev.excitation(m, th, far=False, ctx=ctx)
     W = dev.excitation(m, th, far=True, ctx=ctx)
     tele = {'fp64_fallback': False}
+    if tol is None:
+        tol = ops2d.MIXED_RCS_TOL  # an RCS solve: the same refinement target as the 2-D RCS path
     if precision == 'mixed':
         V0 = V.clone()
         try:

@@ -545,7 +545,7 @@ static int getrs_impl(grim_context *h, int n, int nrhs, const C *LU, int64_t lda
 }
 
 // ------------------------------------------------ complex64 getrs on packed block panels
-// For many right-hand sides the two triangular solves run in GS_NB-row blocks, each block
+// For many right-hand sides the two triangular solves run in nb-row blocks, each block
 // one tensor-core GEMM with a panel formed once per factorization:
 //   forward  (L unit lower), block i at rows J..J+nb:  PL_i = [Linv_ii; -L_below,i Linv_ii]
 //            B[J:n] = [0; B[J+nb:n]] + PL_i B[J:J+nb]
@@ -558,30 +558,33 @@ static int getrs_impl(grim_context *h, int n, int nrhs, const C *LU, int64_t lda
 // block solve multiplies by the inverse of a triangular diagonal block instead of
 // substituting; its rounding is that of an FP32 GEMM, and the FP64 refinement that
 // consumes these solves removes it.
-#define GS_NB 256
+// Block height: 512 rows for large, wide solves (fewer, longer GEMMs), 256 otherwise (a
+// cheaper panel build when it is amortised over fewer right-hand sides).
+#define GS_NB_MAX 512
+static inline int gs_block(int n, int nrhs) { return (n >= 2048 && nrhs >= 512) ? 512 : 256; }
 
 struct GsPanels {
-    int n = 0, nblk = 0;
+    int n = 0, nblk = 0, nb = 256;
     std::vector<TcPacked> L, U;
 };
 
-// T_b (bd x bd, leading dim GS_NB, batch stride GS_NB^2) = inverse of the unit lower
-// (upper = false) or upper diagonal block of LU at (J0 + b GS_NB) for b < count.
+// T_b (bd x bd, leading dim nb, batch stride nb^2) = inverse of the unit lower
+// (upper = false) or upper diagonal block of LU at (J0 + b nb) for b < count.
 static int gs_invert_blocks(grim_context *h, const float2 *LU, int64_t lda, int J0, int count, int bd, float2 *T,
-                            bool upper) {
+                            bool upper, int nb) {
     const size_t tri = (size_t)(NB * NBP + NB) * sizeof(float2);
-    const int64_t sLU = (int64_t)GS_NB * (lda + 1), sT = (int64_t)GS_NB * GS_NB;
+    const int64_t sLU = (int64_t)nb * (lda + 1), sT = (int64_t)nb * nb;
     const float2 *D = LU + (int64_t)J0 * lda + J0;
-    k_set_unit<float2><<<dim3(ceil_div(bd, 256), bd, count), 256, 0, h->stream>>>(bd, bd, T, GS_NB, 0, sT);
+    k_set_unit<float2><<<dim3(ceil_div(bd, 256), bd, count), 256, 0, h->stream>>>(bd, bd, T, nb, 0, sT);
     GRIM_CHECK_LAUNCH(h, "k_set_unit");
     const int nsub = ceil_div(bd, NB);
     for (int q = 0; q < nsub; ++q) {
         const int s = upper ? nsub - 1 - q : q, js = s * NB, nbs = std::min(NB, bd - js);
         dim3 tg(ceil_div(bd, TRSM_COLS), count);
         if (upper)
-            k_trsm_diag<float2, true><<<tg, 4 * TRSM_COLS, tri, h->stream>>>(bd, D, lda, T, GS_NB, js, nbs, sLU, sT);
+            k_trsm_diag<float2, true><<<tg, 4 * TRSM_COLS, tri, h->stream>>>(bd, D, lda, T, nb, js, nbs, sLU, sT);
         else
-            k_trsm_diag<float2, false><<<tg, 4 * TRSM_COLS, tri, h->stream>>>(bd, D, lda, T, GS_NB, js, nbs, sLU, sT);
+            k_trsm_diag<float2, false><<<tg, 4 * TRSM_COLS, tri, h->stream>>>(bd, D, lda, T, nb, js, nbs, sLU, sT);
         GRIM_CHECK_LAUNCH_W(h, "k_trsm_diag<c64>", 4.0 * nbs * nbs * bd * count, 0);
         // rows of the block still to solve: below the strip (lower) or above it (upper)
         const int M = upper ? js : bd - js - nbs;
@@ -590,39 +593,40 @@ static int gs_invert_blocks(grim_context *h, const float2 *LU, int64_t lda, int 
         float2 *Cb = upper ? T : T + js + nbs;
         dim3 grid(ceil_div(M, RT_BM), ceil_div(bd, RT_BN), count);
         k_gemm_rt<float2, float2, float2, float2, true, true><<<grid, RT_THREADS, 0, h->stream>>>(
-            M, bd, nbs, Ab, lda, T + js, GS_NB, Cb, GS_NB, sLU, sT, sT);
+            M, bd, nbs, Ab, lda, T + js, nb, Cb, nb, sLU, sT, sT);
         GRIM_CHECK_LAUNCH_W(h, "k_gemm_rt<f32>", 8.0 * M * bd * nbs * count, 0);
     }
     return GRIM_OK;
 }
 
-static int gs_build(grim_context *h, int n, const float2 *LU, int64_t lda, GsPanels *P) {
-    const int nblk = ceil_div(n, GS_NB), nfull = n / GS_NB;
+static int gs_build(grim_context *h, int n, const float2 *LU, int64_t lda, int nb, GsPanels *P) {
+    const int nblk = ceil_div(n, nb), nfull = n / nb;
     size_t floats_l = 0, floats_u = 0;
     for (int i = 0; i < nblk; ++i) {
-        const int J = i * GS_NB, nbj = std::min(GS_NB, n - J);
+        const int J = i * nb, nbj = std::min(nb, n - J);
         floats_l += 2 * (size_t)tc_rows_a(n - J) * tc_kp(nbj);
         floats_u += 2 * (size_t)tc_rows_a(J + nbj) * tc_kp(nbj);
     }
     void *pl = nullptr, *pu = nullptr, *pt = nullptr, *pw = nullptr;
     GRIM_TRY(grim_workspace(h, "gs_l", floats_l * sizeof(float), &pl));
     GRIM_TRY(grim_workspace(h, "gs_u", floats_u * sizeof(float), &pu));
-    GRIM_TRY(grim_workspace(h, "gs_t", (size_t)2 * nblk * GS_NB * GS_NB * sizeof(float2), &pt));
-    GRIM_TRY(grim_workspace(h, "gs_w", (size_t)n * GS_NB * sizeof(float2), &pw));
-    float2 *TL = (float2 *)pt, *TU = TL + (size_t)nblk * GS_NB * GS_NB, *W = (float2 *)pw;
+    GRIM_TRY(grim_workspace(h, "gs_t", (size_t)2 * nblk * nb * nb * sizeof(float2), &pt));
+    GRIM_TRY(grim_workspace(h, "gs_w", (size_t)n * nb * sizeof(float2), &pw));
+    float2 *TL = (float2 *)pt, *TU = TL + (size_t)nblk * nb * nb, *W = (float2 *)pw;
     // inverses of every diagonal block: the full blocks in one batch, a partial last one alone
     if (nfull > 0) {
-        GRIM_TRY(gs_invert_blocks(h, LU, lda, 0, nfull, GS_NB, TL, false));
-        GRIM_TRY(gs_invert_blocks(h, LU, lda, 0, nfull, GS_NB, TU, true));
+        GRIM_TRY(gs_invert_blocks(h, LU, lda, 0, nfull, nb, TL, false, nb));
+        GRIM_TRY(gs_invert_blocks(h, LU, lda, 0, nfull, nb, TU, true, nb));
     }
     if (nblk > nfull) {
-        const int J = nfull * GS_NB, bd = n - J;
-        const size_t off = (size_t)nfull * GS_NB * GS_NB;
-        GRIM_TRY(gs_invert_blocks(h, LU, lda, J, 1, bd, TL + off, false));
-        GRIM_TRY(gs_invert_blocks(h, LU, lda, J, 1, bd, TU + off, true));
+        const int J = nfull * nb, bd = n - J;
+        const size_t off = (size_t)nfull * nb * nb;
+        GRIM_TRY(gs_invert_blocks(h, LU, lda, J, 1, bd, TL + off, false, nb));
+        GRIM_TRY(gs_invert_blocks(h, LU, lda, J, 1, bd, TU + off, true, nb));
     }
     P->n = n;
     P->nblk = nblk;
+    P->nb = nb;
     P->L.assign(nblk, TcPacked{});
     P->U.assign(nblk, TcPacked{});
     float *fl = (float *)pl, *fu = (float *)pu;
@@ -634,8 +638,8 @@ static int gs_build(grim_context *h, int n, const float2 *LU, int64_t lda, GsPan
         return GRIM_OK;
     };
     for (int i = 0; i < nblk; ++i) {
-        const int J = i * GS_NB, nbj = std::min(GS_NB, n - J), kp = tc_kp(nbj);
-        const float2 *Ti = TL + (size_t)i * GS_NB * GS_NB, *Ui = TU + (size_t)i * GS_NB * GS_NB;
+        const int J = i * nb, nbj = std::min(nb, n - J), kp = tc_kp(nbj);
+        const float2 *Ti = TL + (size_t)i * nb * nb, *Ui = TU + (size_t)i * nb * nb;
         // forward panel [Linv; -L_below Linv], rows J..n
         TcPacked &pli = P->L[i];
         pli.hi = fl;
@@ -644,9 +648,9 @@ static int gs_build(grim_context *h, int n, const float2 *LU, int64_t lda, GsPan
         pli.lo = fl + (size_t)pli.rows_p * kp;
         fl += 2 * (size_t)pli.rows_p * kp;
         const int below = n - J - nbj;
-        GRIM_TRY(pack_rows(pli, nbj, nbj, Ti, GS_NB, 0, below > 0 ? 2 * nbj : pli.rows_p));
+        GRIM_TRY(pack_rows(pli, nbj, nbj, Ti, nb, 0, below > 0 ? 2 * nbj : pli.rows_p));
         if (below > 0) {
-            GRIM_TRY(tc_cgemm(h, below, nbj, nbj, LU + (int64_t)J * lda + J + nbj, lda, Ti, GS_NB, W, below, -1.f, true));
+            GRIM_TRY(tc_cgemm(h, below, nbj, nbj, LU + (int64_t)J * lda + J + nbj, lda, Ti, nb, W, below, -1.f, true));
             GRIM_TRY(pack_rows(pli, below, nbj, W, below, 2 * nbj, pli.rows_p - 2 * nbj));
         }
         // backward panel [-U_above Uinv; Uinv], rows 0..J+nbj
@@ -657,30 +661,30 @@ static int gs_build(grim_context *h, int n, const float2 *LU, int64_t lda, GsPan
         pui.lo = fu + (size_t)pui.rows_p * kp;
         fu += 2 * (size_t)pui.rows_p * kp;
         if (J > 0) {
-            GRIM_TRY(tc_cgemm(h, J, nbj, nbj, LU + (int64_t)J * lda, lda, Ui, GS_NB, W, J, -1.f, true));
+            GRIM_TRY(tc_cgemm(h, J, nbj, nbj, LU + (int64_t)J * lda, lda, Ui, nb, W, J, -1.f, true));
             GRIM_TRY(pack_rows(pui, J, nbj, W, J, 0, 2 * J));
         }
-        GRIM_TRY(pack_rows(pui, nbj, nbj, Ui, GS_NB, 2 * J, pui.rows_p - 2 * J));
+        GRIM_TRY(pack_rows(pui, nbj, nbj, Ui, nb, 2 * J, pui.rows_p - 2 * J));
     }
     return GRIM_OK;
 }
 
 static int gs_apply(grim_context *h, const GsPanels &P, int nrhs, const int *ipiv, const int *ident, float2 *B,
                     int64_t ldb) {
-    const int n = P.n;
+    const int n = P.n, nb = P.nb;
     k_laswp_rhs<float2><<<ceil_div(nrhs, 128), 128, 0, h->stream>>>(n, nrhs, B, ldb, ipiv, ident);
     GRIM_CHECK_LAUNCH(h, "k_laswp_rhs<c64>");
     const int bn = tc_bn(nrhs), np = ceil_div(nrhs, bn) * bn;
     TcPacked pb;
-    GRIM_TRY(tc_ws(h, "gs_b", np, tc_kp(GS_NB), &pb));
+    GRIM_TRY(tc_ws(h, "gs_b", np, tc_kp(GS_NB_MAX), &pb));
     for (int i = 0; i < P.nblk; ++i) {
-        const int J = i * GS_NB, nbj = std::min(GS_NB, n - J);
+        const int J = i * nb, nbj = std::min(nb, n - J);
         pb.kp = P.L[i].kp;
         GRIM_TRY(tc_pack_b(h, nbj, nrhs, B + J, ldb, pb));
         GRIM_TRY(tc_gemm_packed(h, bn, P.L[i], pb, B + J, ldb, n - J, nrhs, nbj, 1.f, 0, nbj));
     }
     for (int i = P.nblk - 1; i >= 0; --i) {
-        const int J = i * GS_NB, nbj = std::min(GS_NB, n - J);
+        const int J = i * nb, nbj = std::min(nb, n - J);
         pb.kp = P.U[i].kp;
         GRIM_TRY(tc_pack_b(h, nbj, nrhs, B + J, ldb, pb));
         GRIM_TRY(tc_gemm_packed(h, bn, P.U[i], pb, B, ldb, J + nbj, nrhs, nbj, 1.f, J, J + nbj));
@@ -689,7 +693,7 @@ static int gs_apply(grim_context *h, const GsPanels &P, int nrhs, const int *ipi
 }
 
 // The packed-panel solve pays for itself with wide right-hand sides on tensor cores.
-static bool gs_wanted(int n, int nrhs) { return tc_enabled() && n >= 2 * GS_NB && nrhs >= 128; }
+static bool gs_wanted(int n, int nrhs) { return tc_enabled() && n >= 512 && nrhs >= 128; }
 
 extern "C" int grim_zgetrf(grim_handle_t h, int n, void *A, int64_t lda, int *ipiv, int *info) {
     return getrf_impl<double2>(h, n, (double2 *)A, lda, ipiv, info);
@@ -793,7 +797,7 @@ static int oz_residual(grim_context *h, const OzA &qa, int nrhs, const double2 *
                                              Cfg::SMEM_BYTES));
         attr = true;
     }
-    dim3 grid(qa.Rp / TC_BM, Np / OZ_BN);
+    dim3 grid(Np / OZ_BN, qa.Rp / TC_BM);
     k_oz_gemm<OZ_SLICES, OZ_BN><<<grid, TC_THREADS, Cfg::SMEM_BYTES, h->stream>>>(
         qa.Rp / OZ_KT, qa.Q, qa.Rp, (const int8_t *)pp, Np, Kp, qa.row_exp, (const int *)pe, (const double *)B,
         2 * ldb, (double *)R, 2 * ldr, 2 * n, nrhs, err);
@@ -889,7 +893,7 @@ static int mixed_refine(grim_context *h, int n, int nrhs, const TA *Ares, int64_
     GRIM_TRY(getrs_prepare<float2>(h, n, ipiv, &ident));
     GsPanels panels;
     const bool use_gs = gs_wanted(n, nrhs);
-    if (use_gs) GRIM_TRY(gs_build(h, n, lu32, n, &panels));
+    if (use_gs) GRIM_TRY(gs_build(h, n, lu32, n, gs_block(n, nrhs), &panels));
     auto solve32 = [&](float2 *X32) -> int {
         if (use_gs) return gs_apply(h, panels, nrhs, ipiv, ident, X32, n);
         return getrs_apply<float2>(h, n, nrhs, lu32, n, ipiv, ident, X32, n);

@@ -214,7 +214,7 @@ __device__ __forceinline__ void oz_mma_slice(uint32_t tmem, uint32_t sA, uint32_
 }
 
 // R[r, j] = B[r, j] - 2^(e_m + f_j) sum_d 2^-7(d+2) D_d[r, j] on interleaved complex128
-// (real row r = 2m + t).  grid = (Rp / 128, Np / BN).
+// (real row r = 2m + t).  grid = (Np / BN, Rp / 128).
 template <int S, int BN>
 __global__ void __launch_bounds__(TC_THREADS)
 k_oz_gemm(int nk, const int8_t *__restrict__ Q, int Rp, const int8_t *__restrict__ P, int Np, int Kp,
@@ -228,7 +228,8 @@ k_oz_gemm(int nk, const int8_t *__restrict__ Q, int Rp, const int8_t *__restrict
     const uint32_t base = (smem_addr(smem_dyn) + 1023u) & ~1023u;
     const uint32_t xbase = base, abase = base + 2 * Cfg::XBUF_BYTES;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int m0 = blockIdx.x * TC_BM, n0 = blockIdx.y * BN;
+    // blockIdx.x runs over the N tiles, so the CTAs resident together share A slice tiles in L2
+    const int m0 = blockIdx.y * TC_BM, n0 = blockIdx.x * BN;
     if (threadIdx.x == 0) {
         s_fail = 0;
         for (int i = 0; i < 2; ++i) {

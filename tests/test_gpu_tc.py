@@ -29,7 +29,7 @@ def test_tensor_core_cgemm_matches_reference(m, n, k):
         assert err < (1e-5 if tc else 2e-6), (tc, err)  # split TF32 accumulates in tensor-core FP32
 
 
-@pytest.mark.parametrize('n,nrhs', [(700, 150), (1024, 300)])
+@pytest.mark.parametrize('n,nrhs', [(700, 150), (1024, 300), (1300, 200)])
 def test_mixed_solve_on_packed_block_panels(n, nrhs):
     """Wide right-hand sides take the packed-panel complex64 solve; refinement still reaches FP64."""
     import ctypes
