@@ -568,23 +568,24 @@ struct GsPanels {
     std::vector<TcPacked> L, U;
 };
 
-// T_b (bd x bd, leading dim nb, batch stride nb^2) = inverse of the unit lower
-// (upper = false) or upper diagonal block of LU at (J0 + b nb) for b < count.
+// T_b (bd x bd, leading dim ldt, batch stride sT) = inverse of the unit lower (upper =
+// false) or upper diagonal block of LU at (J0 + b nb) for b < count, by 64-row
+// substitution steps (used for a partial last block).
 static int gs_invert_blocks(grim_context *h, const float2 *LU, int64_t lda, int J0, int count, int bd, float2 *T,
-                            bool upper, int nb) {
+                            int64_t ldt, int64_t sT, bool upper, int nb) {
     const size_t tri = (size_t)(NB * NBP + NB) * sizeof(float2);
-    const int64_t sLU = (int64_t)nb * (lda + 1), sT = (int64_t)nb * nb;
+    const int64_t sLU = (int64_t)nb * (lda + 1);
     const float2 *D = LU + (int64_t)J0 * lda + J0;
-    k_set_unit<float2><<<dim3(ceil_div(bd, 256), bd, count), 256, 0, h->stream>>>(bd, bd, T, nb, 0, sT);
+    k_set_unit<float2><<<dim3(ceil_div(bd, 256), bd, count), 256, 0, h->stream>>>(bd, bd, T, ldt, 0, sT);
     GRIM_CHECK_LAUNCH(h, "k_set_unit");
     const int nsub = ceil_div(bd, NB);
     for (int q = 0; q < nsub; ++q) {
         const int s = upper ? nsub - 1 - q : q, js = s * NB, nbs = std::min(NB, bd - js);
         dim3 tg(ceil_div(bd, TRSM_COLS), count);
         if (upper)
-            k_trsm_diag<float2, true><<<tg, 4 * TRSM_COLS, tri, h->stream>>>(bd, D, lda, T, nb, js, nbs, sLU, sT);
+            k_trsm_diag<float2, true><<<tg, 4 * TRSM_COLS, tri, h->stream>>>(bd, D, lda, T, ldt, js, nbs, sLU, sT);
         else
-            k_trsm_diag<float2, false><<<tg, 4 * TRSM_COLS, tri, h->stream>>>(bd, D, lda, T, nb, js, nbs, sLU, sT);
+            k_trsm_diag<float2, false><<<tg, 4 * TRSM_COLS, tri, h->stream>>>(bd, D, lda, T, ldt, js, nbs, sLU, sT);
         GRIM_CHECK_LAUNCH_W(h, "k_trsm_diag<c64>", 4.0 * nbs * nbs * bd * count, 0);
         // rows of the block still to solve: below the strip (lower) or above it (upper)
         const int M = upper ? js : bd - js - nbs;
@@ -593,8 +594,56 @@ static int gs_invert_blocks(grim_context *h, const float2 *LU, int64_t lda, int 
         float2 *Cb = upper ? T : T + js + nbs;
         dim3 grid(ceil_div(M, RT_BM), ceil_div(bd, RT_BN), count);
         k_gemm_rt<float2, float2, float2, float2, true, true><<<grid, RT_THREADS, 0, h->stream>>>(
-            M, bd, nbs, Ab, lda, T + js, nb, Cb, nb, sLU, sT, sT);
+            M, bd, nbs, Ab, lda, T + js, ldt, Cb, ldt, sLU, sT, sT);
         GRIM_CHECK_LAUNCH_W(h, "k_gemm_rt<f32>", 8.0 * M * bd * nbs * count, 0);
+    }
+    return GRIM_OK;
+}
+
+// Inverses of the diagonal nb-blocks of the first `rows` rows (a multiple of nb) of the
+// unit lower (upper = false) or upper factor, into the same positions of T (leading dim
+// ldt; T zeroed outside the blocks), by recursive doubling: the 64 x 64 diagonal blocks
+// are inverted by one batched substitution launch, then, for s = 64, 128, ..., nb / 2,
+// every 2s-block [A 0; C D] (lower) gets its off-diagonal part -D^-1 (C A^-1), or
+// [A B; 0 D] (upper) gets -A^-1 (B D^-1), by two batched GEMMs over all 2s-blocks.
+static int gs_invert_recursive(grim_context *h, const float2 *LU, int64_t lda, int rows, int nb, float2 *T,
+                               int64_t ldt, float2 *TW, bool upper) {
+    const size_t tri = (size_t)(NB * NBP + NB) * sizeof(float2);
+    const int nq = rows / NB;
+    GRIM_CHECK_CUDA(cudaMemset2DAsync(T, ldt * sizeof(float2), 0, rows * sizeof(float2), rows, h->stream));
+    k_set_unit<float2><<<dim3(1, NB, nq), NB, 0, h->stream>>>(NB, NB, T, ldt, 0, (int64_t)NB * (ldt + 1));
+    GRIM_CHECK_LAUNCH(h, "k_set_unit");
+    dim3 tg(NB / TRSM_COLS, nq);
+    if (upper)
+        k_trsm_diag<float2, true><<<tg, 4 * TRSM_COLS, tri, h->stream>>>(NB, LU, lda, T, ldt, 0, NB,
+                                                                         (int64_t)NB * (lda + 1),
+                                                                         (int64_t)NB * (ldt + 1));
+    else
+        k_trsm_diag<float2, false><<<tg, 4 * TRSM_COLS, tri, h->stream>>>(NB, LU, lda, T, ldt, 0, NB,
+                                                                          (int64_t)NB * (lda + 1),
+                                                                          (int64_t)NB * (ldt + 1));
+    GRIM_CHECK_LAUNCH_W(h, "k_trsm_diag<c64>", 4.0 * NB * NB * NB * nq, 0);
+    for (int s = NB; s < nb; s *= 2) {
+        const int count = rows / (2 * s);
+        const int64_t sLU = (int64_t)2 * s * (lda + 1), sT = (int64_t)2 * s * (ldt + 1), sW = (int64_t)s * s;
+        dim3 grid(ceil_div(s, RT_BM), ceil_div(s, RT_BN), count);
+        if (!upper) {
+            // W = C A^-1;  X = -D^-1 W  (C = L[o+s:o+2s, o:o+s], X at T[o+s:, o:])
+            k_gemm_rt<float2, float2, float2, float2, false, false><<<grid, RT_THREADS, 0, h->stream>>>(
+                s, s, s, LU + s, lda, T, ldt, TW, s, sLU, sT, sW);
+            GRIM_CHECK_LAUNCH_W(h, "k_gemm_rt<f32>", 8.0 * s * s * s * count, 0);
+            k_gemm_rt<float2, float2, float2, float2, true, false><<<grid, RT_THREADS, 0, h->stream>>>(
+                s, s, s, T + (int64_t)s * (ldt + 1), ldt, TW, s, T + s, ldt, sT, sW, sT);
+            GRIM_CHECK_LAUNCH_W(h, "k_gemm_rt<f32>", 8.0 * s * s * s * count, 0);
+        } else {
+            // W = B D^-1;  X = -A^-1 W  (B = U[o:o+s, o+s:o+2s], X at T[o:, o+s:])
+            k_gemm_rt<float2, float2, float2, float2, false, false><<<grid, RT_THREADS, 0, h->stream>>>(
+                s, s, s, LU + (int64_t)s * lda, lda, T + (int64_t)s * (ldt + 1), ldt, TW, s, sLU, sT, sW);
+            GRIM_CHECK_LAUNCH_W(h, "k_gemm_rt<f32>", 8.0 * s * s * s * count, 0);
+            k_gemm_rt<float2, float2, float2, float2, true, false><<<grid, RT_THREADS, 0, h->stream>>>(
+                s, s, s, T, ldt, TW, s, T + (int64_t)s * ldt, ldt, sT, sW, sT);
+            GRIM_CHECK_LAUNCH_W(h, "k_gemm_rt<f32>", 8.0 * s * s * s * count, 0);
+        }
     }
     return GRIM_OK;
 }
@@ -607,22 +656,26 @@ static int gs_build(grim_context *h, int n, const float2 *LU, int64_t lda, int n
         floats_l += 2 * (size_t)tc_rows_a(n - J) * tc_kp(nbj);
         floats_u += 2 * (size_t)tc_rows_a(J + nbj) * tc_kp(nbj);
     }
-    void *pl = nullptr, *pu = nullptr, *pt = nullptr, *pw = nullptr;
+    void *pl = nullptr, *pu = nullptr, *pt = nullptr, *pw = nullptr, *ptw = nullptr;
     GRIM_TRY(grim_workspace(h, "gs_l", floats_l * sizeof(float), &pl));
     GRIM_TRY(grim_workspace(h, "gs_u", floats_u * sizeof(float), &pu));
-    GRIM_TRY(grim_workspace(h, "gs_t", (size_t)2 * nblk * nb * nb * sizeof(float2), &pt));
+    // diagonal-block inverses live at their own positions of two n x n matrices
+    GRIM_TRY(grim_workspace(h, "gs_t", (size_t)2 * n * n * sizeof(float2), &pt));
     GRIM_TRY(grim_workspace(h, "gs_w", (size_t)n * nb * sizeof(float2), &pw));
-    float2 *TL = (float2 *)pt, *TU = TL + (size_t)nblk * nb * nb, *W = (float2 *)pw;
-    // inverses of every diagonal block: the full blocks in one batch, a partial last one alone
+    GRIM_TRY(grim_workspace(h, "gs_tw", (size_t)n * nb / 2 * sizeof(float2), &ptw));
+    float2 *TL = (float2 *)pt, *TU = TL + (size_t)n * n, *W = (float2 *)pw;
+    const int64_t ldt = n;
+    // full blocks: recursive doubling over all of them at once; a partial last block by
+    // 64-row substitution steps
     if (nfull > 0) {
-        GRIM_TRY(gs_invert_blocks(h, LU, lda, 0, nfull, nb, TL, false, nb));
-        GRIM_TRY(gs_invert_blocks(h, LU, lda, 0, nfull, nb, TU, true, nb));
+        GRIM_TRY(gs_invert_recursive(h, LU, lda, nfull * nb, nb, TL, ldt, (float2 *)ptw, false));
+        GRIM_TRY(gs_invert_recursive(h, LU, lda, nfull * nb, nb, TU, ldt, (float2 *)ptw, true));
     }
     if (nblk > nfull) {
         const int J = nfull * nb, bd = n - J;
-        const size_t off = (size_t)nfull * nb * nb;
-        GRIM_TRY(gs_invert_blocks(h, LU, lda, J, 1, bd, TL + off, false, nb));
-        GRIM_TRY(gs_invert_blocks(h, LU, lda, J, 1, bd, TU + off, true, nb));
+        const int64_t off = (int64_t)J * (ldt + 1);
+        GRIM_TRY(gs_invert_blocks(h, LU, lda, J, 1, bd, TL + off, ldt, 0, false, nb));
+        GRIM_TRY(gs_invert_blocks(h, LU, lda, J, 1, bd, TU + off, ldt, 0, true, nb));
     }
     P->n = n;
     P->nblk = nblk;
@@ -639,7 +692,7 @@ static int gs_build(grim_context *h, int n, const float2 *LU, int64_t lda, int n
     };
     for (int i = 0; i < nblk; ++i) {
         const int J = i * nb, nbj = std::min(nb, n - J), kp = tc_kp(nbj);
-        const float2 *Ti = TL + (size_t)i * nb * nb, *Ui = TU + (size_t)i * nb * nb;
+        const float2 *Ti = TL + (int64_t)J * (ldt + 1), *Ui = TU + (int64_t)J * (ldt + 1);
         // forward panel [Linv; -L_below Linv], rows J..n
         TcPacked &pli = P->L[i];
         pli.hi = fl;
@@ -648,9 +701,9 @@ static int gs_build(grim_context *h, int n, const float2 *LU, int64_t lda, int n
         pli.lo = fl + (size_t)pli.rows_p * kp;
         fl += 2 * (size_t)pli.rows_p * kp;
         const int below = n - J - nbj;
-        GRIM_TRY(pack_rows(pli, nbj, nbj, Ti, nb, 0, below > 0 ? 2 * nbj : pli.rows_p));
+        GRIM_TRY(pack_rows(pli, nbj, nbj, Ti, ldt, 0, below > 0 ? 2 * nbj : pli.rows_p));
         if (below > 0) {
-            GRIM_TRY(tc_cgemm(h, below, nbj, nbj, LU + (int64_t)J * lda + J + nbj, lda, Ti, nb, W, below, -1.f, true));
+            GRIM_TRY(tc_cgemm(h, below, nbj, nbj, LU + (int64_t)J * lda + J + nbj, lda, Ti, ldt, W, below, -1.f, true));
             GRIM_TRY(pack_rows(pli, below, nbj, W, below, 2 * nbj, pli.rows_p - 2 * nbj));
         }
         // backward panel [-U_above Uinv; Uinv], rows 0..J+nbj
@@ -661,10 +714,10 @@ static int gs_build(grim_context *h, int n, const float2 *LU, int64_t lda, int n
         pui.lo = fu + (size_t)pui.rows_p * kp;
         fu += 2 * (size_t)pui.rows_p * kp;
         if (J > 0) {
-            GRIM_TRY(tc_cgemm(h, J, nbj, nbj, LU + (int64_t)J * lda, lda, Ui, nb, W, J, -1.f, true));
+            GRIM_TRY(tc_cgemm(h, J, nbj, nbj, LU + (int64_t)J * lda, lda, Ui, ldt, W, J, -1.f, true));
             GRIM_TRY(pack_rows(pui, J, nbj, W, J, 0, 2 * J));
         }
-        GRIM_TRY(pack_rows(pui, nbj, nbj, Ui, nb, 2 * J, pui.rows_p - 2 * J));
+        GRIM_TRY(pack_rows(pui, nbj, nbj, Ui, ldt, 2 * J, pui.rows_p - 2 * J));
     }
     return GRIM_OK;
 }
