@@ -147,14 +147,17 @@ def worker(index, device=None):
 
 
 def _record_on(obj, stream):
-    """Mark every CUDA tensor in a (nested) result as used by ``stream`` (caching-allocator safety)."""
+    """Mark every CUDA tensor in a result (a tensor, or dicts and tuples nesting them) as used by
+    ``stream`` (caching-allocator safety).  Lists are host data (sample records) and are not
+    searched."""
     if isinstance(obj, torch.Tensor):
         if obj.is_cuda:
             obj.record_stream(stream)
     elif isinstance(obj, dict):
         for v in obj.values():
-            _record_on(v, stream)
-    elif isinstance(obj, (list, tuple)):
+            if isinstance(v, (torch.Tensor, dict, tuple)):
+                _record_on(v, stream)
+    elif isinstance(obj, tuple):
         for v in obj:
             _record_on(v, stream)
 
