@@ -20,7 +20,7 @@ GRIM_ERR_SINGULAR = 6
 GRIM_ERR_NOT_CONVERGED = 7
 GRIM_ERR_NONFINITE = 8
 POL_TM, POL_TE = 0, 1
-PREC_FP64, PREC_MIXED = 0, 1
+PREC_FP64, PREC_MIXED, PREC_MIXED_BERR = 0, 1, 2
 
 c_int, c_int64, c_double, c_void_p, c_char_p = ctypes.c_int, ctypes.c_int64, ctypes.c_double, ctypes.c_void_p, ctypes.c_char_p
 c_size_t = ctypes.c_size_t

@@ -185,7 +185,7 @@ def _solve_mode(dev, m, th, precision, tol, ctx=None):
     if precision == 'mixed':
         V0 = V.clone()
         try:
-            st = ops2d.solve_inplace(Z, V, 'mixed', tol=tol, ctx=ctx)
+            st = ops2d.solve_inplace(Z, V, 'mixed', tol=tol, ctx=ctx, stop='berr')
         except _lib.GrimNotConverged:
             # ill-conditioned mode: the reference's ladder falls back to the double LU
             tele['fp64_fallback'] = True

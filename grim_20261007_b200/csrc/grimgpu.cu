@@ -925,7 +925,8 @@ extern "C" int grim_residual(grim_handle_t h, int n, int nrhs, const void *A, in
 // ============================================================== solve (FP64 or mixed)
 template <typename TA>
 static int mixed_refine(grim_context *h, int n, int nrhs, const TA *Ares, int64_t ldres, float2 *lu32, const int *ipiv,
-                        double2 *Bio, int64_t ldb, double tol, int max_iter, grim_solve_info *st) {
+                        double2 *Bio, int64_t ldb, double tol, int max_iter, grim_solve_info *st,
+                        bool berr_test = false) {
     // Bio holds B on entry and X on exit.
     void *pB = nullptr, *pX = nullptr, *pR = nullptr, *pR32 = nullptr, *pS = nullptr;
     GRIM_TRY(grim_workspace(h, "mx_B", (size_t)n * nrhs * sizeof(double2), &pB));
@@ -978,8 +979,9 @@ static int mixed_refine(grim_context *h, int n, int nrhs, const TA *Ares, int64_
         berr = hv[0];
         relres = hv[1];
         if (first < 0) first = berr;
-        if (std::isfinite(relres) && relres <= tol) break;
-        if (!std::isfinite(relres) || relres >= prev * 0.98) {
+        const double measure = berr_test ? berr : relres;
+        if (std::isfinite(measure) && measure <= tol) break;
+        if (!std::isfinite(measure) || measure >= prev * 0.98) {
             status = grim_fail(GRIM_ERR_NOT_CONVERGED, "mixed-precision refinement stalled; double LU required");
             break;
         }
@@ -987,7 +989,7 @@ static int mixed_refine(grim_context *h, int n, int nrhs, const TA *Ares, int64_
             status = grim_fail(GRIM_ERR_NOT_CONVERGED, "mixed-precision refinement exceeded its correction limit");
             break;
         }
-        prev = relres;
+        prev = measure;
         k_convert<float2, double2><<<eg, 256, 0, h->stream>>>(n, nrhs, R, n, R32, n);
         GRIM_CHECK_LAUNCH(h, "k_convert");
         GRIM_TRY(solve32(R32));
@@ -1007,7 +1009,8 @@ extern "C" int grim_zgesv_mixed(grim_handle_t h, int n, int nrhs, const void *A,
                                 int64_t lda32, void *B, int64_t ldb, int precision_mode, double tol, int max_iter,
                                 int *info, grim_solve_info *stats) {
     if (!h || n <= 0 || nrhs <= 0 || !B || ldb < n || (!A && !A32) || (A && lda < n) || (A32 && lda32 < n) ||
-        (precision_mode != GRIM_PREC_FP64 && precision_mode != GRIM_PREC_MIXED))
+        (precision_mode != GRIM_PREC_FP64 && precision_mode != GRIM_PREC_MIXED &&
+         precision_mode != GRIM_PREC_MIXED_BERR))
         return grim_fail(GRIM_ERR_ARGUMENT, "grim_zgesv_mixed: bad arguments");
     if (precision_mode == GRIM_PREC_FP64 && !A)
         return grim_fail(GRIM_ERR_ARGUMENT, "grim_zgesv_mixed: FP64 mode needs the complex128 matrix");
@@ -1062,10 +1065,13 @@ extern "C" int grim_zgesv_mixed(grim_handle_t h, int n, int nrhs, const void *A,
         }
         StreamTimer ts(h->stream);
         int s;
+        const bool berr_test = precision_mode == GRIM_PREC_MIXED_BERR;
         if (A)
-            s = mixed_refine<double2>(h, n, nrhs, (const double2 *)A, lda, lu, ipiv, (double2 *)B, ldb, tol, max_iter, &st);
+            s = mixed_refine<double2>(h, n, nrhs, (const double2 *)A, lda, lu, ipiv, (double2 *)B, ldb, tol, max_iter, &st,
+                                      berr_test);
         else
-            s = mixed_refine<float2>(h, n, nrhs, (const float2 *)A32, lda32, lu, ipiv, (double2 *)B, ldb, tol, max_iter, &st);
+            s = mixed_refine<float2>(h, n, nrhs, (const float2 *)A32, lda32, lu, ipiv, (double2 *)B, ldb, tol, max_iter,
+                                     &st, berr_test);
         st.ms_solve = ts.stop_ms();
         h->last = st;
         if (stats) *stats = st;

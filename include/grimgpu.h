@@ -48,6 +48,7 @@ extern "C" {
 
 #define GRIM_PREC_FP64 0         /* plain FP64 drop-in                               */
 #define GRIM_PREC_MIXED 1        /* FP32 factor, FP64 residual / update refinement   */
+#define GRIM_PREC_MIXED_BERR 2   /* as MIXED, stopping on the normwise backward error */
 
 typedef struct grim_context *grim_handle_t;
 
@@ -146,9 +147,13 @@ int grim_backward_error_noalloc(grim_handle_t h, int n, int nrhs, const void *A,
 /* Device-resident solve of A X = B, X overwrites B (complex128).
  * precision_mode GRIM_PREC_FP64: zgetrf + zgetrs.  GRIM_PREC_MIXED: complex64 LU of A
  * (or of A32 when given), FP64 residual against A (complex128, or the exact promotion
- * of A32 when A is NULL) and FP64 update, at most max_iter steps until the backward
- * error is <= tol or stalls (ratio > 0.98); reference linalg/refined_lu.py:25-61.
- * A is preserved.  info: LAPACK-style.  stats may be NULL. */
+ * of A32 when A is NULL) and FP64 update, at most max_iter steps until the relative
+ * residual max|r| / max|b| of every column is <= tol or stalls (ratio > 0.98);
+ * reference linalg/refined_lu.py:25-61.  GRIM_PREC_MIXED_BERR: the same refinement
+ * stopping when the normwise backward error |r| / (|A| |x| + |b|) of every column is
+ * <= tol (the form of test LAPACK's zcgesv uses), for callers whose accuracy target
+ * is a backward error (the RCS solves).  A is preserved.  info: LAPACK-style.  stats
+ * may be NULL. */
 int grim_zgesv_mixed(grim_handle_t h, int n, int nrhs, const void *A, int64_t lda, const void *A32,
                      int64_t lda32, void *B, int64_t ldb, int precision_mode, double tol, int max_iter,
                      int *info, grim_solve_info *stats);

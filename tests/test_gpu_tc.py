@@ -100,3 +100,32 @@ def test_integer_slice_residual_propagates_nonfinite():
     r = to_host_matrix(rt)
     assert np.all(np.isnan(r[:, 3]))
     assert np.all(np.isfinite(np.delete(r, 3, axis=1)))
+
+
+def test_backward_error_stopping_mode():
+    """GRIM_PREC_MIXED_BERR stops on the normwise backward error; GRIM_PREC_MIXED on the relative residual."""
+    import ctypes
+    if not torch.cuda.is_available():
+        pytest.skip('no CUDA device')
+    from grim_20261007_b200 import _lib
+    from grim_20261007_b200.device import context, ptr, to_device_colmajor, to_host_matrix
+    ctx = context()
+    rng = np.random.default_rng(5)
+    n, nrhs = 600, 64
+    a = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n)) + 8 * np.sqrt(n) * np.eye(n)
+    b = rng.standard_normal((n, nrhs)) + 1j * rng.standard_normal((n, nrhs))
+    at = to_device_colmajor(a, torch.complex128)
+    for mode in (_lib.PREC_MIXED, _lib.PREC_MIXED_BERR):
+        bt = to_device_colmajor(b, torch.complex128)
+        info, st = ctypes.c_int(-1), _lib.GrimSolveInfo()
+        _lib.check(ctx.lib.grim_zgesv_mixed(ctx.h, n, nrhs, ptr(at), n, None, 0, ptr(bt), n, mode, 1e-10, 10,
+                                            ctypes.byref(info), ctypes.byref(st)))
+        x = to_host_matrix(bt)
+        r = a @ x - b
+        berr = np.max(np.abs(r), axis=0) / (np.max(np.sum(np.abs(a), axis=1)) * np.max(np.abs(x), axis=0)
+                                            + np.max(np.abs(b), axis=0))
+        relres = np.max(np.abs(r), axis=0) / np.max(np.abs(b), axis=0)
+        if mode == _lib.PREC_MIXED_BERR:
+            assert np.max(berr) <= 1e-10 * 1.01 and st.backward_error <= 1e-10, st.as_dict()
+        else:
+            assert np.max(relres) <= 1e-10 * 1.01, st.as_dict()
