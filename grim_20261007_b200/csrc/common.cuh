@@ -143,6 +143,10 @@ struct grim_context {
     int sm_count = 148;
     // error flag of the tensor-core kernels (device int, zeroed at first use)
     int *tc_err = nullptr;
+    // factorization look-ahead: a high-priority stream for the panel chain, a low-priority
+    // one for the wide trailing updates, and the events that order them (created lazily)
+    cudaStream_t chain = nullptr, bulk = nullptr;
+    std::vector<cudaEvent_t> events;
     // profiling: one event per launch (plus a start event), aggregated by kernel name
     int profiling = 0;
     cudaEvent_t prof_start = nullptr;

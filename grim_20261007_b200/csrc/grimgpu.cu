@@ -105,6 +105,16 @@ int grim_upload_gauss(void) {
     return upload_tables(dev);
 }
 
+// Status-returning form of GRIM_CHECK_LAUNCH_W, for code that must clean up on failure.
+int grim_launch_status(grim_context *h, const char *what, double flops, double bytes) {
+    h->launches++;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return grim_cuda_check(e, what);
+    if (h->profiling) grim_prof_mark(h, what, flops, bytes);
+    return GRIM_OK;
+}
+int grim_cuda_status(cudaError_t e, const char *what) { return e == cudaSuccess ? GRIM_OK : grim_cuda_check(e, what); }
+
 // ============================================================== workspace
 int grim_workspace(grim_context *h, const char *name, size_t bytes, void **out) {
     auto it = h->ws.find(name);
@@ -171,6 +181,11 @@ extern "C" int grim_destroy(grim_handle_t h) {
         cudaStreamSynchronize(h->stream);
         cudaFree(h->tc_err);
     }
+    if (h->chain) cudaStreamSynchronize(h->chain);
+    if (h->bulk) cudaStreamSynchronize(h->bulk);
+    for (cudaEvent_t e : h->events) cudaEventDestroy(e);
+    if (h->chain) cudaStreamDestroy(h->chain);
+    if (h->bulk) cudaStreamDestroy(h->bulk);
     if (h->own_stream) cudaStreamDestroy(h->own_stream);
     delete h;
     return GRIM_OK;
@@ -358,7 +373,7 @@ static int tc_launch(grim_context *h, const TcPacked &A, const TcPacked &B, floa
                                              TcCfg<BN, STAGES>::SMEM_BYTES));
         attr = true;
     }
-    dim3 grid(A.rows_p / TC_BM, B.rows_p / BN);
+    dim3 grid(A.rows_p / TC_BM, ceil_div(N, BN));  // B.rows_p is the row stride of the packed B
     k_tc_gemm<BN, STAGES><<<grid, TC_THREADS, TcCfg<BN, STAGES>::SMEM_BYTES, h->stream>>>(
         A.kp / TC_BK, A.hi, A.lo, A.rows_p, B.hi, B.lo, B.rows_p, (float *)C, 2 * ldc, 2 * M, N, alpha, 2 * ow_lo,
         2 * ow_hi, err);
@@ -444,8 +459,79 @@ static const char *kname(const char *base, size_t csize) {
     return s.c_str();
 }
 
+// Streams and events of the look-ahead (created once per handle).
+static int lookahead_streams(grim_context *h, int nevents) {
+    if (!h->chain) {
+        int least = 0, greatest = 0;
+        GRIM_CHECK_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        GRIM_CHECK_CUDA(cudaStreamCreateWithPriority(&h->chain, cudaStreamNonBlocking, greatest));
+        GRIM_CHECK_CUDA(cudaStreamCreateWithPriority(&h->bulk, cudaStreamNonBlocking, least));
+    }
+    while ((int)h->events.size() < nevents) {
+        cudaEvent_t e;
+        GRIM_CHECK_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        h->events.push_back(e);
+    }
+    return GRIM_OK;
+}
+
+// Trailing update A22 -= L21 U12 split into the next panel's 64 columns ("narrow", on the
+// current stream) and the rest ("wide", on `wide_stream`).  For complex64 both operands
+// are packed once, into the buffer pair `slot`, and shared by the two tensor-core GEMMs.
+template <typename C>
+static int trailing_update(grim_context *h, int rest, int nbj, const C *L21, const C *U12, C *A22, int64_t lda,
+                           cudaStream_t wide_stream, cudaEvent_t packed, int slot) {
+    const int nn = std::min(NB, rest), nw = rest - nn;
+    if constexpr (sizeof(C) == sizeof(float2)) {
+        if (tc_enabled()) {
+            const int Kp = tc_kp(nbj);
+            TcPacked pa, pb;
+            // B rows padded so that a 128-wide tile starting at row 64 stays inside the buffer
+            GRIM_TRY(tc_ws(h, slot ? "lu_pa1" : "lu_pa0", tc_rows_a(rest), Kp, &pa));
+            GRIM_TRY(tc_ws(h, slot ? "lu_pb1" : "lu_pb0", ceil_div(rest + NB, 128) * 128, Kp, &pb));
+            GRIM_TRY(tc_pack_a(h, rest, nbj, (const float2 *)L21, lda, 1.f, pa));
+            GRIM_TRY(tc_pack_b(h, nbj, rest, (const float2 *)U12, lda, pb));
+            GRIM_TRY(tc_gemm_packed(h, 64, pa, pb, (float2 *)A22, lda, rest, nn, nbj, -1.f, 0, 0));
+            if (nw > 0) {
+                GRIM_CHECK_CUDA(cudaEventRecord(packed, h->stream));
+                GRIM_CHECK_CUDA(cudaStreamWaitEvent(wide_stream, packed, 0));
+                const cudaStream_t keep = h->stream;
+                h->stream = wide_stream;
+                TcPacked pw = pb;
+                pw.hi += (size_t)NB * 32;
+                pw.lo += (size_t)NB * 32;
+                const int bn = tc_bn(nw);
+                int s = tc_gemm_packed(h, bn, pa, pw, (float2 *)(A22 + (int64_t)nn * lda), lda, rest, nw, nbj, -1.f, 0,
+                                       0);
+                h->stream = keep;
+                GRIM_TRY(s);
+            }
+            return GRIM_OK;
+        }
+    }
+    GRIM_TRY((gemm<C, C, C, C, true, true>(h, rest, nn, nbj, L21, lda, U12, lda, A22, lda)));
+    if (nw > 0) {
+        GRIM_CHECK_CUDA(cudaEventRecord(packed, h->stream));
+        GRIM_CHECK_CUDA(cudaStreamWaitEvent(wide_stream, packed, 0));
+        const cudaStream_t keep = h->stream;
+        h->stream = wide_stream;
+        int s = gemm<C, C, C, C, true, true>(h, rest, nw, nbj, L21, lda, U12 + (int64_t)nn * lda, lda,
+                                             A22 + (int64_t)nn * lda, lda);
+        h->stream = keep;
+        GRIM_TRY(s);
+    }
+    return GRIM_OK;
+}
+
 // Device flag layout for one factorization: [0] info, [1] pivoted panels, then per panel
 // cert[npan], swapped[npan], counter[npan].
+//
+// Look-ahead: the panel chain (diagonal block, panel solve, the next panel's 64-column
+// update) runs on a high-priority stream, the rest of each trailing update on a
+// low-priority one, so that the diagonal block of panel p+1 is factored while the wide
+// update of panel p is still running; panel p+1's solve waits for that update (its U12
+// reads the updated columns).  With per-launch profiling on, everything runs on the
+// handle's stream in order.
 template <typename C>
 static int getrf_impl(grim_context *h, int n, C *A, int64_t lda, int *ipiv, int *info_host) {
     if (!h || n <= 0 || !A || lda < n || !ipiv) return grim_fail(GRIM_ERR_ARGUMENT, "getrf: bad arguments");
@@ -461,27 +547,64 @@ static int getrf_impl(grim_context *h, int n, C *A, int64_t lda, int *ipiv, int 
     int *d_info = flags, *d_pivoted = flags + 1, *cert = flags + 2, *swapped = cert + npan, *counter = swapped + npan;
     GRIM_CHECK_CUDA(cudaMemsetAsync(flags, 0, (size_t)(2 + 3 * npan) * sizeof(int), h->stream));
     const size_t tri = (size_t)(NB * NBP + NB) * sizeof(C);
-    for (int p = 0; p < npan; ++p) {
+    const bool split = !h->profiling;
+    const cudaStream_t caller = h->stream;
+    cudaStream_t wide = caller;
+    // events: [0] start, [1] end, then per panel "packed" (2 + p) and "wide done" (2 + npan + p)
+    if (split) {
+        GRIM_TRY(lookahead_streams(h, 2 + 2 * npan));
+        GRIM_CHECK_CUDA(cudaEventRecord(h->events[0], caller));
+        GRIM_CHECK_CUDA(cudaStreamWaitEvent(h->chain, h->events[0], 0));
+        GRIM_CHECK_CUDA(cudaStreamWaitEvent(h->bulk, h->events[0], 0));
+        h->stream = h->chain;
+        wide = h->bulk;
+    } else {
+        GRIM_TRY(lookahead_streams(h, 2 + 2 * npan));
+    }
+    int status = GRIM_OK;
+    bool wide_pending = false;
+    for (int p = 0; p < npan && status == GRIM_OK; ++p) {
         const int j = p * NB, nbj = std::min(NB, n - j);
         k_diag_lu<C><<<1, 256, 0, h->stream>>>(n, A, lda, j, nbj, bcol, cert + p, ipiv);
-        GRIM_CHECK_LAUNCH_W(h, kname("k_diag_lu", sizeof(C)), 8.0 * nbj * nbj * nbj / 3.0, 0);
+        status = grim_launch_status(h, kname("k_diag_lu", sizeof(C)), 8.0 * nbj * nbj * nbj / 3.0, 0);
+        if (status != GRIM_OK) break;
+        if (wide_pending) {
+            GRIM_CHECK_CUDA(cudaStreamWaitEvent(h->stream, h->events[2 + npan + p - 1], 0));
+            wide_pending = false;
+        }
         const int rest = n - j - nbj;
         if (rest > 0) {
             const int nL = ceil_div(rest, NB), nU = nL;
             k_panel_apply<C><<<nL + nU, 256, tri, h->stream>>>(n, A, lda, j, nbj, nL, bcol, brow, cert + p,
                                                                counter + p, swapped + p, ipiv, d_info, d_pivoted);
-            GRIM_CHECK_LAUNCH_W(h, kname("k_panel_apply", sizeof(C)), 8.0 * 2 * rest * nbj * nbj, 0);
-            GRIM_TRY((gemm_sub<C>(h, rest, rest, nbj, A + (int64_t)j * lda + j + nbj, lda,
-                                                  A + (int64_t)(j + nbj) * lda + j, lda,
-                                                  A + (int64_t)(j + nbj) * lda + j + nbj, lda)));
+            status = grim_launch_status(h, kname("k_panel_apply", sizeof(C)), 8.0 * 2 * rest * nbj * nbj, 0);
+            if (status != GRIM_OK) break;
+            status = trailing_update<C>(h, rest, nbj, A + (int64_t)j * lda + j + nbj, A + (int64_t)(j + nbj) * lda + j,
+                                        A + (int64_t)(j + nbj) * lda + j + nbj, lda, wide, h->events[2 + p], p & 1);
+            if (status != GRIM_OK) break;
+            if (rest > NB && split) {
+                status = grim_cuda_status(cudaEventRecord(h->events[2 + npan + p], wide), "cudaEventRecord");
+                wide_pending = status == GRIM_OK;
+            }
         } else {
             k_panel_last<C><<<1, 256, 0, h->stream>>>(n, A, lda, j, nbj, bcol, cert + p, swapped + p, ipiv, d_info,
                                                       d_pivoted);
-            GRIM_CHECK_LAUNCH(h, kname("k_panel_last", sizeof(C)));
+            status = grim_launch_status(h, kname("k_panel_last", sizeof(C)), 0, 0);
         }
     }
-    k_laswp_left<C><<<ceil_div(n, 128), 128, 0, h->stream>>>(n, A, lda, NB, swapped, ipiv);
-    GRIM_CHECK_LAUNCH(h, kname("k_laswp_left", sizeof(C)));
+    if (status == GRIM_OK) {
+        k_laswp_left<C><<<ceil_div(n, 128), 128, 0, h->stream>>>(n, A, lda, NB, swapped, ipiv);
+        status = grim_launch_status(h, kname("k_laswp_left", sizeof(C)), 0, 0);
+    }
+    if (split) {
+        // the caller's stream waits for both streams, whatever happened above
+        cudaEventRecord(h->events[1], h->bulk);
+        cudaStreamWaitEvent(h->chain, h->events[1], 0);
+        cudaEventRecord(h->events[1], h->chain);
+        cudaStreamWaitEvent(caller, h->events[1], 0);
+        h->stream = caller;
+    }
+    GRIM_TRY(status);
     int hostf[2] = {0, 0};
     GRIM_CHECK_CUDA(cudaMemcpyAsync(hostf, flags, 2 * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
     GRIM_CHECK_CUDA(cudaStreamSynchronize(h->stream));
