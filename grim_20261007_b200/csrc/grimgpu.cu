@@ -913,9 +913,10 @@ static int residual_and_berr(grim_context *h, int n, int nrhs, const TA *A, int6
 }
 
 // ------------------------------------------------ residual on the integer tensor cores
-// A~ cut once into OZ_SLICES int8 slices (ozaki.cuh); every residual then slices X and
-// runs one k_oz_gemm (BN 64, 8 accumulators = all 512 tensor-memory columns).
-#define OZ_SLICES 8
+// A~ cut once into S int8 slices (ozaki.cuh); every residual then slices X and runs one
+// k_oz_gemm (BN 64, S accumulators of 64 tensor-memory columns).  S = 8 gives an FP64
+// GEMM's accuracy (4e-17 of max |A||X|), S = 7 gives 6e-15 with 28 slice pairs instead of
+// 36 (see oz_slices_for).
 #define OZ_BN 64
 
 struct OzA {
@@ -924,12 +925,18 @@ struct OzA {
     int *row_exp = nullptr;
 };
 
+static inline bool oz_supported(int S) { return S == 7 || S == 8; }
+// 7 slices leave an error of about 6e-15 of |A||X| in the residual: enough for a backward-
+// error target of 1e-13 or looser.  A relative-residual target (|r| / |b|) is scaled by
+// |b| instead, which for an ill-conditioned system is far below |A||X|: 8 slices.
+static inline int oz_slices_for(bool berr_test, double tol) { return (berr_test && tol >= 1e-13) ? 7 : 8; }
+
 // int32 accumulators hold S products of 2n terms of at most 64^2.
 static bool oz_fits(int n, int S) { return (double)S * 2.0 * n * 64.0 * 64.0 < 2147483647.0; }
 
 template <typename TA>
 static int oz_prepare_a(grim_context *h, int n, const TA *A, int64_t lda, int S, OzA *out) {
-    if (S != OZ_SLICES) return grim_fail(GRIM_ERR_ARGUMENT, "integer-slice residual: unsupported slice count");
+    if (!oz_supported(S)) return grim_fail(GRIM_ERR_ARGUMENT, "integer-slice residual: unsupported slice count");
     const int Rp = ceil_div(2 * n, 128) * 128;
     void *pq = nullptr, *pm = nullptr, *pe = nullptr;
     GRIM_TRY(grim_workspace(h, "oz_q", (size_t)S * Rp * Rp, &pq));
@@ -939,8 +946,12 @@ static int oz_prepare_a(grim_context *h, int n, const TA *A, int64_t lda, int S,
     k_oz_rowmax<TA><<<dim3(ceil_div(n, 256), 32), 256, 0, h->stream>>>(n, A, lda, (unsigned long long *)pm);
     GRIM_CHECK_LAUNCH(h, "k_oz_rowmax");
     const int64_t threads = (int64_t)(Rp / 2) * (Rp / 16);
-    k_oz_slice_a<TA, OZ_SLICES><<<ceil_div(threads, 256), 256, 0, h->stream>>>(
-        n, A, lda, (const unsigned long long *)pm, (int8_t *)pq, Rp, Rp, (int *)pe);
+    if (S == 7)
+        k_oz_slice_a<TA, 7><<<ceil_div(threads, 256), 256, 0, h->stream>>>(n, A, lda, (const unsigned long long *)pm,
+                                                                           (int8_t *)pq, Rp, Rp, (int *)pe);
+    else
+        k_oz_slice_a<TA, 8><<<ceil_div(threads, 256), 256, 0, h->stream>>>(n, A, lda, (const unsigned long long *)pm,
+                                                                           (int8_t *)pq, Rp, Rp, (int *)pe);
     GRIM_CHECK_LAUNCH_W(h, "k_oz_slice_a", 0.0, (double)sizeof(TA) * n * n + (double)S * Rp * Rp);
     out->n = n;
     out->S = S;
@@ -950,10 +961,29 @@ static int oz_prepare_a(grim_context *h, int n, const TA *A, int64_t lda, int S,
     return GRIM_OK;
 }
 
+template <int S>
+static int oz_launch(grim_context *h, const OzA &qa, const int8_t *P, int Np, const int *col_exp, const double2 *B,
+                     int64_t ldb, double2 *R, int64_t ldr, int nrhs, int *err) {
+    using Cfg = OzCfg<S, OZ_BN>;
+    static bool attr = false;
+    if (!attr) {
+        GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_oz_gemm<S, OZ_BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             Cfg::SMEM_BYTES));
+        attr = true;
+    }
+    dim3 grid(Np / OZ_BN, qa.Rp / TC_BM);
+    k_oz_gemm<S, OZ_BN><<<grid, TC_THREADS, Cfg::SMEM_BYTES, h->stream>>>(
+        qa.Rp / OZ_KT, qa.Q, qa.Rp, P, Np, qa.Rp, qa.row_exp, col_exp, (const double *)B, 2 * ldb, (double *)R,
+        2 * ldr, 2 * qa.n, nrhs, err);
+    GRIM_CHECK_LAUNCH_W(h, "k_oz_gemm", 8.0 * qa.n * qa.n * nrhs,
+                        (double)S * qa.Rp * qa.Rp * (Np / OZ_BN) + (double)S * Np * qa.Rp * (qa.Rp / TC_BM) +
+                            32.0 * qa.n * nrhs);
+    return GRIM_OK;
+}
+
 // R = B - A X with A prepared by oz_prepare_a (R and B distinct).
 static int oz_residual(grim_context *h, const OzA &qa, int nrhs, const double2 *X, int64_t ldx, const double2 *B,
                        int64_t ldb, double2 *R, int64_t ldr) {
-    using Cfg = OzCfg<OZ_SLICES, OZ_BN>;
     const int n = qa.n, S = qa.S, Np = ceil_div(nrhs, OZ_BN) * OZ_BN, Kp = qa.Rp;
     void *pp = nullptr, *pc = nullptr, *pe = nullptr;
     GRIM_TRY(grim_workspace(h, "oz_p", (size_t)S * Np * Kp, &pp));
@@ -962,25 +992,17 @@ static int oz_residual(grim_context *h, const OzA &qa, int nrhs, const double2 *
     k_oz_colmax<<<nrhs, 256, 0, h->stream>>>(n, X, ldx, (double *)pc);
     GRIM_CHECK_LAUNCH(h, "k_oz_colmax");
     const int64_t threads = (int64_t)Np * (Kp / 16);
-    k_oz_slice_x<OZ_SLICES><<<ceil_div(threads, 256), 256, 0, h->stream>>>(n, nrhs, X, ldx, (const double *)pc,
-                                                                            (int8_t *)pp, Np, Kp, (int *)pe);
+    if (S == 7)
+        k_oz_slice_x<7><<<ceil_div(threads, 256), 256, 0, h->stream>>>(n, nrhs, X, ldx, (const double *)pc,
+                                                                        (int8_t *)pp, Np, Kp, (int *)pe);
+    else
+        k_oz_slice_x<8><<<ceil_div(threads, 256), 256, 0, h->stream>>>(n, nrhs, X, ldx, (const double *)pc,
+                                                                        (int8_t *)pp, Np, Kp, (int *)pe);
     GRIM_CHECK_LAUNCH_W(h, "k_oz_slice_x", 0.0, 16.0 * n * nrhs + (double)S * Np * Kp);
     int *err;
     GRIM_TRY(tc_err_flag(h, &err));
-    static bool attr = false;
-    if (!attr) {
-        GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_oz_gemm<OZ_SLICES, OZ_BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             Cfg::SMEM_BYTES));
-        attr = true;
-    }
-    dim3 grid(Np / OZ_BN, qa.Rp / TC_BM);
-    k_oz_gemm<OZ_SLICES, OZ_BN><<<grid, TC_THREADS, Cfg::SMEM_BYTES, h->stream>>>(
-        qa.Rp / OZ_KT, qa.Q, qa.Rp, (const int8_t *)pp, Np, Kp, qa.row_exp, (const int *)pe, (const double *)B,
-        2 * ldb, (double *)R, 2 * ldr, 2 * n, nrhs, err);
-    GRIM_CHECK_LAUNCH_W(h, "k_oz_gemm", 8.0 * n * n * nrhs,
-                        (double)S * qa.Rp * qa.Rp * (Np / OZ_BN) + (double)S * Np * Kp * (qa.Rp / TC_BM) +
-                            32.0 * n * nrhs);
-    return GRIM_OK;
+    if (S == 7) return oz_launch<7>(h, qa, (const int8_t *)pp, Np, (const int *)pe, B, ldb, R, ldr, nrhs, err);
+    return oz_launch<8>(h, qa, (const int8_t *)pp, Np, (const int *)pe, B, ldb, R, ldr, nrhs, err);
 }
 
 template <typename TA>
@@ -1020,11 +1042,11 @@ extern "C" int grim_backward_error(grim_handle_t h, int n, int nrhs, const void 
 }
 
 // Test / diagnostic entry: R = B - A X with the FP64 SIMT GEMM (slices 0) or on the integer
-// tensor cores with 8 int8 slices per operand.
+// tensor cores with 7 or 8 int8 slices per operand.
 extern "C" int grim_residual(grim_handle_t h, int n, int nrhs, const void *A, int64_t lda, int a_complex64,
                              const void *X, int64_t ldx, const void *B, int64_t ldb, void *R, int64_t ldr, int slices) {
     if (!h || n <= 0 || nrhs <= 0 || !A || !X || !B || !R || lda < n || ldx < n || ldb < n || ldr < n ||
-        (slices != 0 && slices != OZ_SLICES) || (slices && !oz_fits(n, slices)))
+        (slices != 0 && !oz_supported(slices)) || (slices && !oz_fits(n, slices)))
         return grim_fail(GRIM_ERR_ARGUMENT, "grim_residual: bad arguments");
     DeviceGuard g(h->device);
     const double2 *Xd = (const double2 *)X, *Bd = (const double2 *)B;
@@ -1086,8 +1108,9 @@ static int mixed_refine(grim_context *h, int n, int nrhs, const TA *Ares, int64_
     int status = GRIM_OK;
     // residuals on the integer tensor cores when the slice accumulators fit
     OzA qa;
-    const bool use_oz = tc_enabled() && n >= 256 && nrhs >= 16 && oz_fits(n, OZ_SLICES);
-    if (use_oz) GRIM_TRY(oz_prepare_a(h, n, Ares, ldres, OZ_SLICES, &qa));
+    const int oz_s = oz_slices_for(berr_test, tol);
+    const bool use_oz = tc_enabled() && n >= 256 && nrhs >= 16 && oz_fits(n, oz_s);
+    if (use_oz) GRIM_TRY(oz_prepare_a(h, n, Ares, ldres, oz_s, &qa));
     for (int it = 0; it <= max_iter; ++it) {
         if (use_oz) {
             GRIM_TRY(oz_residual(h, qa, nrhs, X, n, B0, n, R, n));
