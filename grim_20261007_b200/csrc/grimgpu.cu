@@ -19,6 +19,7 @@
 #include "bor.cuh"
 #include "tc_gemm.cuh"
 #include "ozaki.cuh"
+#include "dmma.cuh"
 
 // ============================================================== errors
 static thread_local std::string g_last_error;
@@ -279,10 +280,34 @@ extern "C" int grim_farfield2d(grim_handle_t h, int n, const double *geom, int n
 }
 
 // ============================================================== GEMM launcher
+static int tc_enabled();
+
+template <bool NEG, bool BETA>
+static int dmma_gemm(grim_context *h, int M, int N, int K, const double2 *A, int64_t lda, const double2 *B,
+                     int64_t ldb, double2 *C, int64_t ldc) {
+    static bool attr = false;
+    if (!attr) {
+        GRIM_CHECK_CUDA(
+            cudaFuncSetAttribute(k_gemm_dmma<NEG, BETA>, cudaFuncAttributeMaxDynamicSharedMemorySize, DM_SMEM_BYTES));
+        attr = true;
+    }
+    dim3 grid(ceil_div(M, DM_BM), ceil_div(N, DM_BN));
+    k_gemm_dmma<NEG, BETA><<<grid, DM_THREADS, DM_SMEM_BYTES, h->stream>>>(M, N, K, A, lda, B, ldb, C, ldc);
+    GRIM_CHECK_LAUNCH_W(h, "k_gemm_dmma", 8.0 * M * N * K, 16.0 * ((double)M * K + (double)K * N + 2.0 * M * N));
+    return GRIM_OK;
+}
+
+// C = (BETA ? C : 0) + (NEG ? -1 : 1) A B.  Complex128 throughout: FP64 tensor cores
+// (k_gemm_dmma) unless disabled; other type mixes: the SIMT register-tiled kernel.
 template <typename ACC, typename TA, typename TB, typename TC, bool NEG, bool BETA>
 static int gemm(grim_context *h, int M, int N, int K, const TA *A, int64_t lda, const TB *B, int64_t ldb, TC *C,
                 int64_t ldc) {
     if (M <= 0 || N <= 0) return GRIM_OK;
+    if constexpr (sizeof(ACC) == 16 && sizeof(TA) == 16 && sizeof(TB) == 16 && sizeof(TC) == 16) {
+        if (tc_enabled() && K > 0)
+            return dmma_gemm<NEG, BETA>(h, M, N, K, (const double2 *)A, lda, (const double2 *)B, ldb, (double2 *)C,
+                                        ldc);
+    }
     dim3 grid(ceil_div(M, RT_BM), ceil_div(N, RT_BN));
     k_gemm_rt<ACC, TA, TB, TC, NEG, BETA><<<grid, RT_THREADS, 0, h->stream>>>(M, N, K, A, lda, B, ldb, C, ldc, 0, 0,
                                                                               0);
