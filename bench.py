@@ -187,49 +187,59 @@ def run_bor(args):
     return out
 
 
-def run_sweep(args):
+def run_sweep(args, rank=0, world=1):
     """Frequency sweep on the seeded airfoil: 256 frequencies log-spaced over 20:1, N = 10 panels
     per wavelength (uneven sizes), 181 angles, TM, mixed precision, every system on the
-    device worker pool (largest first); a spread sample of 8 frequencies is re-solved in FP64."""
+    device worker pool (largest first); a spread sample of 8 frequencies is re-solved in FP64.
+    With several ranks the frequencies are split by the LPT rule (no data-path collective)
+    and the sweep time is the maximum over ranks."""
     import torch
     from grim_20261007_b200 import synthetic as S
     from grim_20261007_b200.device import run_pool
+    from grim_20261007_b200.sharding import max_over_ranks, my_units
     from grim_20261007_b200.twod import geometry as geo, operators as ops
     from grim_20261007_b200.twod.solver import sweep_workers
     cases, thick = S.airfoil_sweep_case(args.seed + 3, args.sweep)
     ang = np.arange(181) * 1.0
     ang_dev = torch.as_tensor(ang, device='cuda')
-    bodies = [ops.DeviceBody(geo.panel_geometry([v]), None) for v, _k, _f in cases]
-    ns = [b.n for b in bodies]
+    all_n = [len(v) for v, _k, _f in cases]
+    costs_all = [float(n) ** 3 + 181.0 * n * n for n in all_n]
+    mine = my_units(costs_all, rank, world)
+    bodies = {i: ops.DeviceBody(geo.panel_geometry([cases[i][0]]), None) for i in mine}
+    ns = [bodies[i].n for i in mine]
 
     def jobs(prec, idx):
         return [(lambda i=i: ops.monostatic_solve(bodies[i], cases[i][1], ang, 'TM', precision=prec,
                                                   angles_dev=ang_dev)) for i in idx]
 
-    idx = list(range(len(cases)))
-    costs = [float(n) ** 3 + 181.0 * n * n for n in ns]
+    idx = mine
+    costs = [costs_all[i] for i in idx]
     workers = sweep_workers(len(idx))
-    big = sorted(idx, key=lambda i: -costs[i])[: 2 * workers]
+    big = sorted(idx, key=lambda i: -costs_all[i])[: 2 * workers]
     run_pool(jobs('mixed', big), workers=workers)  # warm-up: every worker's workspaces at their largest size
     torch.cuda.synchronize()
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
     outs = run_pool(jobs('mixed', idx), workers=workers, costs=costs)
     e1.record()
     torch.cuda.synchronize()
-    sec = e0.elapsed_time(e1) / 1e3
-    sample = [int(round(x)) for x in np.linspace(0, len(idx) - 1, 8)]
+    sec = max_over_ranks(e0.elapsed_time(e1) / 1e3, device='cuda')
+    pos = {i: p for p, i in enumerate(idx)}
+    sample = [idx[int(round(x))] for x in np.linspace(0, len(idx) - 1, min(8, len(idx)))]
     ref = run_pool(jobs('double', sample), workers=workers)
     err = 0.0
     for i, r in zip(sample, ref):
         s64 = ops.sigma_2d(r['amplitude'].cpu().numpy(), cases[i][1])
-        s32 = ops.sigma_2d(outs[i]['amplitude'].cpu().numpy(), cases[i][1])
+        s32 = ops.sigma_2d(outs[pos[i]]['amplitude'].cpu().numpy(), cases[i][1])
         db = ops.sigma_db(s64)
         mask = db > db.max() - 40
         err = max(err, float(np.max(np.abs(10 * np.log10(s32[mask] / s64[mask])))))
-    return {'systems': len(idx), 'band': '20:1', 'frequency_ghz': [cases[0][2] / 1e9, cases[-1][2] / 1e9],
-            'n_min': min(ns), 'n_max': max(ns), 'angles': 181, 'polarization': 'TM', 'thickness': thick,
-            'workers': workers, 'seconds': sec, 'solves_per_s': len(idx) / sec,
+    return {'systems': len(cases), 'band': '20:1', 'frequency_ghz': [cases[0][2] / 1e9, cases[-1][2] / 1e9],
+            'n_min': min(all_n), 'n_max': max(all_n), 'angles': 181, 'polarization': 'TM', 'thickness': thick,
+            'ranks': world, 'workers_per_rank': workers, 'seconds': sec, 'solves_per_s': len(cases) / sec,
             'fp64_fallbacks': sum(1 for o in outs if o['telemetry'].get('fp64_fallback')),
             'max_db_error_vs_fp64_sampled': err, 'sampled_frequencies': len(sample)}
 
@@ -430,7 +440,7 @@ def main():
 
     serving = run_serving(args) if (args.serving and rank == 0 and world == 1) else None
     bor = run_bor(args) if (args.bor and rank == 0 and world == 1) else None
-    sweep = run_sweep(args) if (args.sweep and rank == 0 and world == 1) else None
+    sweep = run_sweep(args, rank, world) if args.sweep else None
 
     # per-kernel profile of one mixed step, polarisations in turn (CUDA events after every
     # launch on the launching stream, separate from the timed loop)
