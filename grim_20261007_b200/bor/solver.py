@@ -202,30 +202,38 @@ def _solve_mode(dev, m, th, precision, tol, ctx=None):
     return part, tele
 
 
-def solve_bor_device(points, k, thetas_deg, mmax, precision='double', tol=None, ctx=None, workers=None):
+def solve_bor_device(points, k, thetas_deg, mmax, precision='double', tol=None, ctx=None, workers=None,
+                     signed_mode_symmetry=True):
     """Device path: returns (F[2 nth] complex128 on the host, telemetry).
 
-    The modal moments are built once; the 2 mmax + 1 per-mode systems are independent and
-    run on the device worker pool (``GRIM_SWEEP_WORKERS`` workers), each contributing its
-    own far-field vector; the contributions are summed in mode order, so the result does
-    not depend on the scheduling.  With an explicit ``ctx`` (a serving slot) the modes run
-    in turn on that handle.
+    The modal moments are built once; the per-mode systems are independent and run on the
+    device worker pool (``GRIM_SWEEP_WORKERS`` workers), each contributing its own
+    far-field vector; the contributions are summed in mode order, so the result does not
+    depend on the scheduling.  With ``signed_mode_symmetry`` (the reference's setting in
+    every solve_bor path, ``bor/solver.py:2972,3061``) only m = 0..mmax are solved and
+    m > 0 counts twice: for the co-polarised monostatic far field the +m and -m
+    contributions are identical (equal to the last bit in the oracle, for the sphere and
+    the ogive).  With an explicit ``ctx`` (a serving slot) the modes run in turn on that
+    handle.
     """
     from ..twod.solver import sweep_workers
     dev = BorDevice(points, k, mmax, ctx=ctx)
     for m in (0, 1, -1, 2):
         dev.mode_map(m)  # build the shared pole maps before the workers read them
     th = torch.as_tensor(np.asarray(thetas_deg, dtype=np.float64), device='cuda')
-    modes = list(range(-mmax, mmax + 1))
+    modes = list(range(0, mmax + 1)) if signed_mode_symmetry else list(range(-mmax, mmax + 1))
     if ctx is not None:
         outs = [_solve_mode(dev, m, th, precision, tol, ctx=ctx) for m in modes]
     else:
         jobs = [(lambda m=m: _solve_mode(dev, m, th, precision, tol)) for m in modes]
         outs = run_pool(jobs, workers=sweep_workers(len(jobs)) if workers is None else workers)
     amp = torch.zeros(2 * int(th.numel()), dtype=torch.complex128, device='cuda')
-    for part, _t in outs:
-        amp += part
-    tele = {'modes': 2 * mmax + 1, 'max_backward_error': 0.0, 'nxi_max': dev.nxi,
+    for m, (part, _t) in zip(modes, outs):
+        if signed_mode_symmetry and m > 0:
+            amp += 2.0 * part
+        else:
+            amp += part
+    tele = {'modes': 2 * mmax + 1, 'mode_systems_solved': len(modes), 'max_backward_error': 0.0, 'nxi_max': dev.nxi,
             'refinement_steps': max(t['refinement_steps'] for _p, t in outs)}
     fallbacks = sum(1 for _p, t in outs if t['fp64_fallback'])
     if fallbacks:

@@ -76,3 +76,17 @@ def test_reference_sphere_golden(ctx):
         assert np.max(np.abs(amp - g['amp_%s_efie' % pol]) / np.abs(g['amp_%s_efie' % pol])) < 2e-3
     assert np.max(np.abs(10 * np.log10(np.asarray(res['sigma_vv']) / float(g['mie_sigma'])))) < 0.02
     assert res['n_unknowns'] == int(g['n_unknowns'])
+
+
+def test_signed_mode_symmetry_matches_all_modes():
+    """Solving m = 0..M with m > 0 counted twice equals summing every signed mode."""
+    if not torch.cuda.is_available():
+        pytest.skip('no CUDA device')
+    from grim_20261007_b200.bor.solver import solve_bor_device
+    gen, _length, _half = S.ogive_case(6, n=40)
+    k = 8.0 / float(np.max(gen[:, 0]))
+    th = np.arange(0.0, 180.5, 7.5)
+    f_half, t_half = solve_bor_device(gen, k, th, 9)
+    f_all, t_all = solve_bor_device(gen, k, th, 9, signed_mode_symmetry=False)
+    assert t_half['mode_systems_solved'] == 10 and t_all['mode_systems_solved'] == 19
+    np.testing.assert_allclose(f_half, f_all, rtol=1e-11, atol=1e-11 * np.max(np.abs(f_all)))
