@@ -20,7 +20,6 @@ analytic Mie series for the circular cylinder.
 """
 from __future__ import annotations
 
-import cmath
 import math
 import os
 import threading
@@ -247,18 +246,36 @@ def _validate_request(frequencies_ghz, elevations_deg, cfie_alpha, compute_condi
     return freqs, elevs
 
 
-def _solve_frequency(geometry_snapshot, geometry_units, f, elevs, pol, precision, max_panels, mesh_reference_ghz,
-                     abort_event):
+class _MeshCache:
+    """Meshes of one request, shared by the systems that use the same frequency (both
+    polarisations of a co-polarised solve mesh the contour once)."""
+
+    def __init__(self, geometry_snapshot, geometry_units, max_panels, mesh_reference_ghz):
+        self.args = (geometry_snapshot, geometry_units, max_panels, mesh_reference_ghz)
+        self.lock = threading.Lock()
+        self.locks = {}
+        self.meshes = {}
+
+    def get(self, f):
+        with self.lock:
+            lk = self.locks.setdefault(f, threading.Lock())
+        with lk:
+            if f not in self.meshes:
+                snapshot, units, max_panels, ref_ghz = self.args
+                mesh_lambda = C0 / (float(ref_ghz) * 1e9) if ref_ghz else C0 / (f * 1e9)
+                polys = geo.contours_from_snapshot(snapshot, units, mesh_lambda, max_panels)
+                self.meshes[f] = (polys, geo.panel_geometry(polys))
+            return self.meshes[f]
+
+
+def _solve_frequency(meshes, f, elevs, pol, precision, abort_event):
     """One (frequency, polarisation) system on the current device worker: mesh, fill,
     solve, far field; returns host samples and telemetry."""
     if abort_event is not None and abort_event.is_set():
         raise InterruptedError('Solve canceled by user.')
     t0 = time.perf_counter()
     k = 2.0 * math.pi * f * 1e9 / C0
-    wavelength = C0 / (f * 1e9)
-    mesh_lambda = C0 / (float(mesh_reference_ghz) * 1e9) if mesh_reference_ghz else wavelength
-    polys = geo.contours_from_snapshot(geometry_snapshot, geometry_units, mesh_lambda, max_panels)
-    geom = geo.panel_geometry(polys)
+    polys, geom = meshes.get(f)
     te_diag = geo.te_curvature_correction(polys) if pol == 'TE' else None
     dev = torch.device('cuda', torch.cuda.current_device())
     body = ops.DeviceBody(geom, te_diag, device=dev)
@@ -280,16 +297,14 @@ def _solve_frequency(geometry_snapshot, geometry_units, f, elevs, pol, precision
         resid = np.full(len(elevs), float(tele.get('backward_error', 0.0)))
     sig = _rcs_sigma_from_amp(amp, k)
     sdb = _rcs_db_from_sigma(sig)
-    samples = []
-    for idx, e in enumerate(elevs):
-        a = complex(amp[idx])
-        samples.append({
-            'frequency_ghz': f, 'theta_inc_deg': e, 'theta_scat_deg': e,
-            'rcs_linear': float(sig[idx]), 'rcs_db': float(sdb[idx]),
-            'rcs_amp_real': a.real, 'rcs_amp_imag': a.imag,
-            'rcs_amp_phase_deg': math.degrees(cmath.phase(a)),
-            'linear_residual': float(resid[idx]),
-        })
+    phase = np.degrees(np.angle(amp))
+    samples = [{
+        'frequency_ghz': f, 'theta_inc_deg': e, 'theta_scat_deg': e,
+        'rcs_linear': sl, 'rcs_db': sd, 'rcs_amp_real': ar, 'rcs_amp_imag': ai,
+        'rcs_amp_phase_deg': ph, 'linear_residual': rr,
+    } for e, sl, sd, ar, ai, ph, rr in zip(elevs, np.asarray(sig, dtype=float).tolist(),
+                                           np.asarray(sdb, dtype=float).tolist(), amp.real.tolist(),
+                                           amp.imag.tolist(), phase.tolist(), np.asarray(resid, float).tolist())]
     event = dict(requested='gpu', used='gpu_grim', factorizations=1, rhs_columns=len(elevs), n=body.n,
                  label=f'{pol} pulse {f:g} GHz', gpu_device=context().device_name, precision=precision,
                  pivoted_panels=tele.get('pivoted_panels', 0), refinement_steps=tele.get('refinement_steps', 0))
@@ -351,12 +366,11 @@ def _sweep(geometry_snapshot, frequencies_ghz, elevations_deg, pols, geometry_un
     freqs, elevs = _validate_request(frequencies_ghz, elevations_deg, cfie_alpha, compute_condition_number)
     require_cuda()
     precision = requested_precision()
+    meshes = _MeshCache(geometry_snapshot, geometry_units, max_panels, mesh_reference_ghz)
     jobs, keys, costs = [], [], []
     for pol in pols:
         for f in freqs:
-            jobs.append(lambda f=f, pol=pol: _solve_frequency(geometry_snapshot, geometry_units, f, elevs, pol,
-                                                               precision, max_panels, mesh_reference_ghz,
-                                                               abort_event))
+            jobs.append(lambda f=f, pol=pol: _solve_frequency(meshes, f, elevs, pol, precision, abort_event))
             keys.append((pol, f))
             costs.append(_frequency_cost(geometry_snapshot, geometry_units, f, len(elevs)) if len(freqs) > 1 else 1.0)
     total = len(jobs) * (len(elevs) + 1)
