@@ -315,6 +315,7 @@ def main():
     ap.add_argument('--serving-requests', type=int, default=32)
     ap.add_argument('--bor', type=int, default=1, help='time the body-of-revolution ogive workload')
     ap.add_argument('--sweep', type=int, default=256, help='frequencies of the airfoil sweep leg (0 = skip)')
+    ap.add_argument('--autotune', type=int, default=1, help='tune the solve tile shapes for the workload first')
     args = ap.parse_args()
 
     world = int(os.environ.get('WORLD_SIZE', '1'))
@@ -389,6 +390,13 @@ def main():
         launches = launch_count() - launches0
         ms = [a.elapsed_time(b) for a, b in times]
         return ms, launches, last
+
+    # tile shapes of the mixed solve for this (N, angles): timed candidates, fastest kept (every
+    # handle picks it up from the tuner's cache before its solves)
+    autotune = None
+    if args.autotune:
+        from grim_20261007_b200 import tuning
+        autotune = tuning.tune_dense(args.n, args.angles, ctx=ctx)
 
     # FP64 drop-in arm (ratio and accuracy reference)
     ms64, _l64, out64 = timed('double', max(2, args.steps // 2), 1)
@@ -501,6 +509,7 @@ def main():
             'serving': serving,
             'bor_ogive': bor,
             'frequency_sweep': sweep,
+            'autotune': autotune,
             'kernel_profile_mixed': prof,
             'kernel_profile_fp64': prof64,
             'cpu_baseline': cpu_baseline,

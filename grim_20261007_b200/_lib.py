@@ -21,6 +21,7 @@ GRIM_ERR_NOT_CONVERGED = 7
 GRIM_ERR_NONFINITE = 8
 POL_TM, POL_TE = 0, 1
 PREC_FP64, PREC_MIXED, PREC_MIXED_BERR = 0, 1, 2
+TUNE_SOLVE_BN, TUNE_GS_BLOCK = 1, 2
 
 c_int, c_int64, c_double, c_void_p, c_char_p = ctypes.c_int, ctypes.c_int64, ctypes.c_double, ctypes.c_void_p, ctypes.c_char_p
 c_size_t = ctypes.c_size_t
@@ -84,6 +85,7 @@ SIGNATURES = [
     ('grim_zgesv_batched', c_int, [c_void_p, c_int, c_int, c_void_p, c_int, c_void_p, c_int, c_int, P_int]),
     ('grim_last_solve_info', c_int, [c_void_p, ctypes.POINTER(GrimSolveInfo)]),
     ('grim_mem_info', c_int, [c_void_p, ctypes.POINTER(c_size_t), ctypes.POINTER(c_size_t)]),
+    ('grim_set_tuning', c_int, [c_void_p, c_int, c_int]),
     ('grim_bor_moments_size', c_int64, [c_int, c_int]),
     ('grim_bor_moments', c_int, [c_void_p, c_int, c_void_p, c_double, c_int, c_int, c_void_p]),
     ('grim_bor_assemble', c_int, [c_void_p, c_int, c_void_p, c_double, c_int, c_int, c_void_p, c_int, c_void_p,

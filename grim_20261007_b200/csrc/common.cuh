@@ -147,6 +147,9 @@ struct grim_context {
     // one for the wide trailing updates, and the events that order them (created lazily)
     cudaStream_t chain = nullptr, bulk = nullptr;
     std::vector<cudaEvent_t> events;
+    // tile-shape overrides set by the autotuner (0 = built-in rule)
+    int tune_solve_bn = 0;  // output-tile width of the right-hand-side GEMMs (64 or 128)
+    int tune_gs_block = 0;  // row block of the packed-panel solve (256 or 512)
     // profiling: one event per launch (plus a start event), aggregated by kernel name
     int profiling = 0;
     cudaEvent_t prof_start = nullptr;

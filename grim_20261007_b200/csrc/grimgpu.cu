@@ -219,6 +219,19 @@ extern "C" int grim_mem_info(grim_handle_t h, size_t *free_bytes, size_t *total_
     GRIM_CHECK_CUDA(cudaMemGetInfo(free_bytes, total_bytes));
     return GRIM_OK;
 }
+extern "C" int grim_set_tuning(grim_handle_t h, int key, int value) {
+    if (!h) return grim_fail(GRIM_ERR_ARGUMENT, "null handle");
+    if (key == GRIM_TUNE_SOLVE_BN && (value == 0 || value == 64 || value == 128)) {
+        h->tune_solve_bn = value;
+        return GRIM_OK;
+    }
+    if (key == GRIM_TUNE_GS_BLOCK && (value == 0 || value == 256 || value == 512)) {
+        h->tune_gs_block = value;
+        return GRIM_OK;
+    }
+    return grim_fail(GRIM_ERR_ARGUMENT, "grim_set_tuning: unknown key or value out of range");
+}
+
 extern "C" int grim_last_solve_info(grim_handle_t h, grim_solve_info *out) {
     if (!h || !out) return grim_fail(GRIM_ERR_ARGUMENT, "grim_last_solve_info: bad arguments");
     *out = h->last;
@@ -875,7 +888,7 @@ static int gs_apply(grim_context *h, const GsPanels &P, int nrhs, const int *ipi
     const int n = P.n, nb = P.nb;
     k_laswp_rhs<float2><<<ceil_div(nrhs, 128), 128, 0, h->stream>>>(n, nrhs, B, ldb, ipiv, ident);
     GRIM_CHECK_LAUNCH(h, "k_laswp_rhs<c64>");
-    const int bn = tc_bn(nrhs), np = ceil_div(nrhs, bn) * bn;
+    const int bn = h->tune_solve_bn ? h->tune_solve_bn : tc_bn(nrhs), np = ceil_div(nrhs, bn) * bn;
     TcPacked pb;
     GRIM_TRY(tc_ws(h, "gs_b", np, tc_kp(GS_NB_MAX), &pb));
     for (int i = 0; i < P.nblk; ++i) {
@@ -1117,7 +1130,7 @@ static int mixed_refine(grim_context *h, int n, int nrhs, const TA *Ares, int64_
     GRIM_TRY(getrs_prepare<float2>(h, n, ipiv, &ident));
     GsPanels panels;
     const bool use_gs = gs_wanted(n, nrhs);
-    if (use_gs) GRIM_TRY(gs_build(h, n, lu32, n, gs_block(n, nrhs), &panels));
+    if (use_gs) GRIM_TRY(gs_build(h, n, lu32, n, h->tune_gs_block ? h->tune_gs_block : gs_block(n, nrhs), &panels));
     auto solve32 = [&](float2 *X32) -> int {
         if (use_gs) return gs_apply(h, panels, nrhs, ipiv, ident, X32, n);
         return getrs_apply<float2>(h, n, nrhs, lu32, n, ipiv, ident, X32, n);

@@ -78,14 +78,15 @@ def farfield(body, k, angles_dev, x, out=None, ctx=None):
     return amp
 
 
-def solve_inplace(z, b, precision='double', tol=None, max_iter=10, z32=None, ctx=None, stop='relres'):
+def solve_inplace(z, b, precision='double', tol=None, max_iter=10, z32=None, ctx=None, stop='relres', tuned=True):
     """Solve Z X = B on the device; X overwrites ``b`` (complex128, shape (nrhs, n)).
 
     precision 'double': FP64 LU + triangular solves.  'mixed': complex64 LU of ``z32``
     (or of ``z`` rounded) with FP64 residual and update against ``z`` (complex128) or,
     when ``z`` is None, against the exact promotion of ``z32``; the refinement stops when
     every column's relative residual (``stop='relres'``, the reference RefinedLU test) or
-    normwise backward error (``stop='berr'``) is <= ``tol``.
+    normwise backward error (``stop='berr'``) is <= ``tol``.  With ``tuned`` the handle's
+    tile shapes come from the autotuner's cache (``tuning.apply``).
     Returns the solve telemetry dict.
     """
     ctx = ctx or context()
@@ -95,6 +96,9 @@ def solve_inplace(z, b, precision='double', tol=None, max_iter=10, z32=None, ctx
     st = _lib.GrimSolveInfo()
     if precision == 'mixed':
         mode = _lib.PREC_MIXED_BERR if stop == 'berr' else _lib.PREC_MIXED
+        if tuned:
+            from .. import tuning
+            tuning.apply(ctx, n, nrhs)
     else:
         mode = _lib.PREC_FP64
     tol = MIXED_DROPIN_TOL if tol is None else float(tol)

@@ -206,6 +206,15 @@ int grim_profile_report(grim_handle_t h, char *buf, int len);
 /* Free / total device memory in bytes (admission control). */
 int grim_mem_info(grim_handle_t h, size_t *free_bytes, size_t *total_bytes);
 
+/* Tile-shape overrides chosen by the autotuner (grim_20261007_b200.tuning), per handle;
+ * value 0 restores the built-in rule.  GRIM_TUNE_SOLVE_BN: output-tile width (64 or 128)
+ * of the tensor-core GEMMs of the packed-panel solve; GRIM_TUNE_GS_BLOCK: row block (256
+ * or 512) of the packed-panel solve.  No counterpart in the reference (its BLAS picks its
+ * own blocking). */
+#define GRIM_TUNE_SOLVE_BN 1
+#define GRIM_TUNE_GS_BLOCK 2
+int grim_set_tuning(grim_handle_t h, int key, int value);
+
 #ifdef __cplusplus
 }
 #endif

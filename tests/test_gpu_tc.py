@@ -130,3 +130,31 @@ def test_backward_error_stopping_mode():
             assert np.max(berr) <= 1e-10 * 1.01 and st.backward_error <= 1e-10, st.as_dict()
         else:
             assert np.max(relres) <= 1e-10 * 1.01, st.as_dict()
+
+
+def test_autotuner_times_every_candidate_and_keeps_results(tmp_path, monkeypatch):
+    """The tuner times each tile-shape pair on a seeded system and the chosen shapes give the same solution."""
+    if not torch.cuda.is_available():
+        pytest.skip('no CUDA device')
+    from grim_20261007_b200 import synthetic as S, tuning
+    from grim_20261007_b200.device import context
+    from grim_20261007_b200.twod import geometry as geo, operators as ops
+    monkeypatch.setenv('GRIM_TUNING_CACHE', str(tmp_path / 'tuning.json'))
+    monkeypatch.setattr(tuning, '_table', None)
+    ctx = context()
+    entry = tuning.tune_dense(640, 200, ctx=ctx, reps=1)
+    assert len(entry['timings_ms']) == 4 and entry['choice']['solve_bn'] in (64, 128)
+    assert tuning.lookup(ctx.device_name, 640, 200)['choice'] == entry['choice']
+    v, k, _f, _t = S.airfoil_case(0, 640)
+    body = ops.DeviceBody(geo.panel_geometry([v]), None)
+    ang = torch.as_tensor(np.arange(200) * 1.8, device='cuda')
+    z32 = ops.fill(body, k, 'TM', complex64=True)
+    b0 = ops.rhs(body, k, 'TM', ang)
+    xs = []
+    for shapes in ((64, 256), (128, 512)):
+        tuning.set_handle(ctx, *shapes)
+        b = b0.clone()
+        ops.solve_inplace(None, b, 'mixed', tol=1e-10, z32=z32, stop='berr', tuned=False)
+        xs.append(b.cpu().numpy())
+    tuning.set_handle(ctx, 0, 0)
+    np.testing.assert_allclose(xs[0], xs[1], rtol=1e-8, atol=1e-8 * np.max(np.abs(xs[1])))

@@ -115,3 +115,16 @@ def test_airfoil_sweep_case_sizes():
     assert max(ns) == 4096 and min(ns) >= 64
     assert abs(fs[-1] / fs[0] - 20.0) < 1e-9 and all(b > a for a, b in zip(fs, fs[1:]))
     assert ns == sorted(ns)
+
+
+def test_tuning_buckets_and_cache_roundtrip(tmp_path, monkeypatch):
+    from grim_20261007_b200 import tuning
+    assert tuning.bucket(2048, 720) == (2048, 1024)
+    assert tuning.bucket(100, 1) == (512, 16)
+    assert tuning.bucket(2049, 1024) == (2560, 1024)
+    monkeypatch.setenv('GRIM_TUNING_CACHE', str(tmp_path / 'tuning.json'))
+    monkeypatch.setattr(tuning, '_table', None)
+    assert tuning.lookup('dev', 2048, 720) is None
+    tuning._store(tuning._key('dev', 2048, 720), {'choice': {'solve_bn': 64, 'gs_block': 512}})
+    monkeypatch.setattr(tuning, '_table', None)  # a fresh process reads the file
+    assert tuning.lookup('dev', 2000, 600)['choice'] == {'solve_bn': 64, 'gs_block': 512}
