@@ -952,22 +952,36 @@ static int residual_and_berr(grim_context *h, int n, int nrhs, const TA *A, int6
 
 // ------------------------------------------------ residual on the integer tensor cores
 // A~ cut once into S int8 slices (ozaki.cuh); every residual then slices X and runs one
-// k_oz_gemm (BN 64, S accumulators of 64 tensor-memory columns).  S = 8 gives an FP64
-// GEMM's accuracy (4e-17 of max |A||X|), S = 7 gives 6e-15 with 28 slice pairs instead of
-// 36 (see oz_slices_for).
-#define OZ_BN 64
-
+// k_oz_gemm (S accumulators of BN tensor-memory columns).  S = 8 gives an FP64 GEMM's
+// accuracy (4e-17 of max |A||X|), S = 7 about 6e-15 with 28 slice pairs instead of 36,
+// S = 6 about 1e-12 with 21 pairs (see oz_slices_for).  BN is 64, or 80 for S = 6 when
+// that needs fewer waves of CTAs (6 x 80 accumulator columns still fit the 512 of TMEM).
 struct OzA {
     int n = 0, S = 0, Rp = 0;
     int8_t *Q = nullptr;
     int *row_exp = nullptr;
 };
 
-static inline bool oz_supported(int S) { return S == 7 || S == 8; }
-// 7 slices leave an error of about 6e-15 of |A||X| in the residual: enough for a backward-
-// error target of 1e-13 or looser.  A relative-residual target (|r| / |b|) is scaled by
-// |b| instead, which for an ill-conditioned system is far below |A||X|: 8 slices.
-static inline int oz_slices_for(bool berr_test, double tol) { return (berr_test && tol >= 1e-13) ? 7 : 8; }
+static inline bool oz_supported(int S) { return S >= 6 && S <= 8; }
+// 7 slices leave an error of about 6e-15 of |A||X| in the residual, 6 slices about 1e-12:
+// enough for a backward-error target of 1e-13 (7) or 1e-11 (6) and looser, with two
+// orders of magnitude to spare.  A relative-residual target (|r| / |b|) is scaled by |b|
+// instead, which for an ill-conditioned system is far below |A||X|: 8 slices.
+static inline int oz_slices_for(bool berr_test, double tol) {
+    if (!berr_test) return 8;
+    return tol >= 1e-11 ? 6 : (tol >= 1e-13 ? 7 : 8);
+}
+
+// Output-tile width of the slice GEMM: 64, or 80 when S = 6 and the wider tile needs
+// fewer waves of CTAs in total time (waves x width, one CTA per SM).
+static int oz_bn(int S, int nrhs, int Rp, int sms) {
+    if (S != 6) return 64;
+    auto cost = [&](int bn) {
+        const int64_t tiles = (int64_t)ceil_div(nrhs, bn) * (Rp / 128);
+        return (int64_t)ceil_div(tiles, (int64_t)sms) * bn;
+    };
+    return cost(80) < cost(64) ? 80 : 64;
+}
 
 // int32 accumulators hold S products of 2n terms of at most 64^2.
 static bool oz_fits(int n, int S) { return (double)S * 2.0 * n * 64.0 * 64.0 < 2147483647.0; }
@@ -984,12 +998,13 @@ static int oz_prepare_a(grim_context *h, int n, const TA *A, int64_t lda, int S,
     k_oz_rowmax<TA><<<dim3(ceil_div(n, 256), 32), 256, 0, h->stream>>>(n, A, lda, (unsigned long long *)pm);
     GRIM_CHECK_LAUNCH(h, "k_oz_rowmax");
     const int64_t threads = (int64_t)(Rp / 2) * (Rp / 16);
-    if (S == 7)
-        k_oz_slice_a<TA, 7><<<ceil_div(threads, 256), 256, 0, h->stream>>>(n, A, lda, (const unsigned long long *)pm,
-                                                                           (int8_t *)pq, Rp, Rp, (int *)pe);
+    const unsigned long long *rm = (const unsigned long long *)pm;
+    if (S == 6)
+        k_oz_slice_a<TA, 6><<<ceil_div(threads, 256), 256, 0, h->stream>>>(n, A, lda, rm, (int8_t *)pq, Rp, Rp, (int *)pe);
+    else if (S == 7)
+        k_oz_slice_a<TA, 7><<<ceil_div(threads, 256), 256, 0, h->stream>>>(n, A, lda, rm, (int8_t *)pq, Rp, Rp, (int *)pe);
     else
-        k_oz_slice_a<TA, 8><<<ceil_div(threads, 256), 256, 0, h->stream>>>(n, A, lda, (const unsigned long long *)pm,
-                                                                           (int8_t *)pq, Rp, Rp, (int *)pe);
+        k_oz_slice_a<TA, 8><<<ceil_div(threads, 256), 256, 0, h->stream>>>(n, A, lda, rm, (int8_t *)pq, Rp, Rp, (int *)pe);
     GRIM_CHECK_LAUNCH_W(h, "k_oz_slice_a", 0.0, (double)sizeof(TA) * n * n + (double)S * Rp * Rp);
     out->n = n;
     out->S = S;
@@ -999,22 +1014,22 @@ static int oz_prepare_a(grim_context *h, int n, const TA *A, int64_t lda, int S,
     return GRIM_OK;
 }
 
-template <int S>
+template <int S, int BN>
 static int oz_launch(grim_context *h, const OzA &qa, const int8_t *P, int Np, const int *col_exp, const double2 *B,
                      int64_t ldb, double2 *R, int64_t ldr, int nrhs, int *err) {
-    using Cfg = OzCfg<S, OZ_BN>;
+    using Cfg = OzCfg<S, BN>;
     static bool attr = false;
     if (!attr) {
-        GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_oz_gemm<S, OZ_BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_oz_gemm<S, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              Cfg::SMEM_BYTES));
         attr = true;
     }
-    dim3 grid(Np / OZ_BN, qa.Rp / TC_BM);
-    k_oz_gemm<S, OZ_BN><<<grid, TC_THREADS, Cfg::SMEM_BYTES, h->stream>>>(
+    dim3 grid(Np / BN, qa.Rp / TC_BM);
+    k_oz_gemm<S, BN><<<grid, TC_THREADS, Cfg::SMEM_BYTES, h->stream>>>(
         qa.Rp / OZ_KT, qa.Q, qa.Rp, P, Np, qa.Rp, qa.row_exp, col_exp, (const double *)B, 2 * ldb, (double *)R,
         2 * ldr, 2 * qa.n, nrhs, err);
     GRIM_CHECK_LAUNCH_W(h, "k_oz_gemm", 8.0 * qa.n * qa.n * nrhs,
-                        (double)S * qa.Rp * qa.Rp * (Np / OZ_BN) + (double)S * Np * qa.Rp * (qa.Rp / TC_BM) +
+                        (double)S * qa.Rp * qa.Rp * (Np / BN) + (double)S * Np * qa.Rp * (qa.Rp / TC_BM) +
                             32.0 * qa.n * nrhs);
     return GRIM_OK;
 }
@@ -1022,7 +1037,8 @@ static int oz_launch(grim_context *h, const OzA &qa, const int8_t *P, int Np, co
 // R = B - A X with A prepared by oz_prepare_a (R and B distinct).
 static int oz_residual(grim_context *h, const OzA &qa, int nrhs, const double2 *X, int64_t ldx, const double2 *B,
                        int64_t ldb, double2 *R, int64_t ldr) {
-    const int n = qa.n, S = qa.S, Np = ceil_div(nrhs, OZ_BN) * OZ_BN, Kp = qa.Rp;
+    const int n = qa.n, S = qa.S, Kp = qa.Rp;
+    const int bn = oz_bn(S, nrhs, qa.Rp, h->sm_count), Np = ceil_div(nrhs, bn) * bn;
     void *pp = nullptr, *pc = nullptr, *pe = nullptr;
     GRIM_TRY(grim_workspace(h, "oz_p", (size_t)S * Np * Kp, &pp));
     GRIM_TRY(grim_workspace(h, "oz_colmax", (size_t)nrhs * sizeof(double), &pc));
@@ -1030,17 +1046,24 @@ static int oz_residual(grim_context *h, const OzA &qa, int nrhs, const double2 *
     k_oz_colmax<<<nrhs, 256, 0, h->stream>>>(n, X, ldx, (double *)pc);
     GRIM_CHECK_LAUNCH(h, "k_oz_colmax");
     const int64_t threads = (int64_t)Np * (Kp / 16);
-    if (S == 7)
-        k_oz_slice_x<7><<<ceil_div(threads, 256), 256, 0, h->stream>>>(n, nrhs, X, ldx, (const double *)pc,
-                                                                        (int8_t *)pp, Np, Kp, (int *)pe);
+    const double *cm = (const double *)pc;
+    int8_t *Pq = (int8_t *)pp;
+    int *ce = (int *)pe;
+    if (S == 6)
+        k_oz_slice_x<6><<<ceil_div(threads, 256), 256, 0, h->stream>>>(n, nrhs, X, ldx, cm, Pq, Np, Kp, ce);
+    else if (S == 7)
+        k_oz_slice_x<7><<<ceil_div(threads, 256), 256, 0, h->stream>>>(n, nrhs, X, ldx, cm, Pq, Np, Kp, ce);
     else
-        k_oz_slice_x<8><<<ceil_div(threads, 256), 256, 0, h->stream>>>(n, nrhs, X, ldx, (const double *)pc,
-                                                                        (int8_t *)pp, Np, Kp, (int *)pe);
+        k_oz_slice_x<8><<<ceil_div(threads, 256), 256, 0, h->stream>>>(n, nrhs, X, ldx, cm, Pq, Np, Kp, ce);
     GRIM_CHECK_LAUNCH_W(h, "k_oz_slice_x", 0.0, 16.0 * n * nrhs + (double)S * Np * Kp);
     int *err;
     GRIM_TRY(tc_err_flag(h, &err));
-    if (S == 7) return oz_launch<7>(h, qa, (const int8_t *)pp, Np, (const int *)pe, B, ldb, R, ldr, nrhs, err);
-    return oz_launch<8>(h, qa, (const int8_t *)pp, Np, (const int *)pe, B, ldb, R, ldr, nrhs, err);
+    if (S == 6) {
+        if (bn == 80) return oz_launch<6, 80>(h, qa, Pq, Np, ce, B, ldb, R, ldr, nrhs, err);
+        return oz_launch<6, 64>(h, qa, Pq, Np, ce, B, ldb, R, ldr, nrhs, err);
+    }
+    if (S == 7) return oz_launch<7, 64>(h, qa, Pq, Np, ce, B, ldb, R, ldr, nrhs, err);
+    return oz_launch<8, 64>(h, qa, Pq, Np, ce, B, ldb, R, ldr, nrhs, err);
 }
 
 template <typename TA>
@@ -1080,7 +1103,7 @@ extern "C" int grim_backward_error(grim_handle_t h, int n, int nrhs, const void 
 }
 
 // Test / diagnostic entry: R = B - A X with the FP64 SIMT GEMM (slices 0) or on the integer
-// tensor cores with 7 or 8 int8 slices per operand.
+// tensor cores with 6, 7 or 8 int8 slices per operand.
 extern "C" int grim_residual(grim_handle_t h, int n, int nrhs, const void *A, int64_t lda, int a_complex64,
                              const void *X, int64_t ldx, const void *B, int64_t ldb, void *R, int64_t ldr, int slices) {
     if (!h || n <= 0 || nrhs <= 0 || !A || !X || !B || !R || lda < n || ldx < n || ldb < n || ldr < n ||

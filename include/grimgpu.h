@@ -119,10 +119,11 @@ int grim_cgemm_sub(grim_handle_t h, int M, int N, int K, const void *A, int64_t 
 
 /* R = B - A X (complex128 X, B, R; A complex64 if a_complex64 else complex128), the
  * residual of the FP64 refinement (reference linalg/refined_lu.py:50-53, the numpy
- * residual of RefinedLU).  slices = 0: FP64 SIMT GEMM; 7 or 8: int8 slicing of both
+ * residual of RefinedLU).  slices = 0: FP64 SIMT GEMM; 6, 7 or 8: int8 slicing of both
  * operands on the tcgen05 integer tensor cores (error per product term below
  * 2^-7s of max|A row| max|X column|; 8 slices match an FP64 GEMM), as used inside
- * grim_zgesv_mixed (7 slices for backward-error targets of 1e-13 and looser).  R must not
+ * grim_zgesv_mixed (backward-error targets: 6 slices for 1e-11 and looser, 7 for 1e-13
+ * and looser; relative-residual targets: 8).  R must not
  * overlap B.  Needs n < 2^31 / (2 slices 64^2). */
 int grim_residual(grim_handle_t h, int n, int nrhs, const void *A, int64_t lda, int a_complex64, const void *X,
                   int64_t ldx, const void *B, int64_t ldb, void *R, int64_t ldr, int slices);
