@@ -189,8 +189,10 @@ def run_bor(args):
 
 def run_sweep(args, rank=0, world=1):
     """Frequency sweep on the seeded airfoil: 256 frequencies log-spaced over 20:1, N = 10 panels
-    per wavelength (uneven sizes), 181 angles, TM, mixed precision, every system on the
-    device worker pool (largest first); a spread sample of 8 frequencies is re-solved in FP64.
+    per wavelength (uneven sizes), 181 angles, TM, mixed precision.  Timed twice: every system
+    on the device worker pool with its own factorization (largest first), and the grouped
+    path (one grouped LU of all systems, replayed as a CUDA graph, then solves on the pool),
+    which is the reported sweep time; a spread sample of 8 frequencies is re-solved in FP64.
     With several ranks the frequencies are split by the LPT rule (no data-path collective)
     and the sweep time is the maximum over ranks."""
     import torch
@@ -218,15 +220,27 @@ def run_sweep(args, rank=0, world=1):
     big = sorted(idx, key=lambda i: -costs_all[i])[: 2 * workers]
     run_pool(jobs('mixed', big), workers=workers)  # warm-up: every worker's workspaces at their largest size
     torch.cuda.synchronize()
-    if world > 1:
-        import torch.distributed as dist
-        dist.barrier()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    outs = run_pool(jobs('mixed', idx), workers=workers, costs=costs)
-    e1.record()
+
+    def timed(fn):
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        out = fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return out, max_over_ranks(e0.elapsed_time(e1) / 1e3, device='cuda')
+
+    # per system on the worker pool (each system's own factorization chain)
+    outs_pool, sec_pool = timed(lambda: run_pool(jobs('mixed', idx), workers=workers, costs=costs))
+    # grouped: one captured launch sequence factors every system, then solves on the pool
+    # (the first call captures the graph; the timed one replays it)
+    grouped = lambda: ops.monostatic_solves_grouped([bodies[i] for i in idx], [cases[i][1] for i in idx], ang, 'TM',
+                                                    precision='mixed', angles_dev=ang_dev, workers=workers)
+    grouped()
     torch.cuda.synchronize()
-    sec = max_over_ranks(e0.elapsed_time(e1) / 1e3, device='cuda')
+    outs, sec = timed(grouped)
     pos = {i: p for p, i in enumerate(idx)}
     sample = [idx[int(round(x))] for x in np.linspace(0, len(idx) - 1, min(8, len(idx)))]
     ref = run_pool(jobs('double', sample), workers=workers)
@@ -239,7 +253,9 @@ def run_sweep(args, rank=0, world=1):
         err = max(err, float(np.max(np.abs(10 * np.log10(s32[mask] / s64[mask])))))
     return {'systems': len(cases), 'band': '20:1', 'frequency_ghz': [cases[0][2] / 1e9, cases[-1][2] / 1e9],
             'n_min': min(all_n), 'n_max': max(all_n), 'angles': 181, 'polarization': 'TM', 'thickness': thick,
-            'ranks': world, 'workers_per_rank': workers, 'seconds': sec, 'solves_per_s': len(cases) / sec,
+            'ranks': world, 'workers_per_rank': workers, 'path': 'grouped LU (one CUDA graph) + pooled solves',
+            'seconds': sec, 'solves_per_s': len(cases) / sec,
+            'per_system_pool': {'seconds': sec_pool, 'solves_per_s': len(cases) / sec_pool},
             'fp64_fallbacks': sum(1 for o in outs if o['telemetry'].get('fp64_fallback')),
             'max_db_error_vs_fp64_sampled': err, 'sampled_frequencies': len(sample)}
 

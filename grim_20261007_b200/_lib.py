@@ -82,6 +82,11 @@ SIGNATURES = [
                                  c_int, c_double, c_int, P_int, ctypes.POINTER(GrimSolveInfo)]),
     ('grim_zgesv_mixed_factored', c_int, [c_void_p, c_int, c_int, c_void_p, c_int64, c_void_p, c_int64, c_void_p,
                                           c_void_p, c_void_p, c_int64, c_double, c_int, ctypes.POINTER(GrimSolveInfo)]),
+    ('grim_zgesv_refine_factored', c_int, [c_void_p, c_int, c_int, c_void_p, c_int64, c_void_p, c_int64, c_void_p,
+                                           c_void_p, c_void_p, c_int64, c_int, c_double, c_int,
+                                           ctypes.POINTER(GrimSolveInfo)]),
+    ('grim_getrf_grouped', c_int, [c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int, P_int,
+                                   P_int]),
     ('grim_zgesv_batched', c_int, [c_void_p, c_int, c_int, c_void_p, c_int, c_void_p, c_int, c_int, P_int]),
     ('grim_last_solve_info', c_int, [c_void_p, ctypes.POINTER(GrimSolveInfo)]),
     ('grim_mem_info', c_int, [c_void_p, ctypes.POINTER(c_size_t), ctypes.POINTER(c_size_t)]),

@@ -150,6 +150,11 @@ struct grim_context {
     // tile-shape overrides set by the autotuner (0 = built-in rule)
     int tune_solve_bn = 0;  // output-tile width of the right-hand-side GEMMs (64 or 128)
     int tune_gs_block = 0;  // row block of the packed-panel solve (256 or 512)
+    // grouped factorization: the instantiated CUDA graph of the last plan, the key it was
+    // captured for (element size, orders, device buffers it reads) and its launch count
+    cudaGraphExec_t grp_exec = nullptr;
+    std::vector<int64_t> grp_key;
+    int64_t grp_graph_launches = 0;
     // profiling: one event per launch (plus a start event), aggregated by kernel name
     int profiling = 0;
     cudaEvent_t prof_start = nullptr;

@@ -36,16 +36,15 @@ __device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b)
 }
 
 template <bool NEG, bool BETA>
-__global__ void __launch_bounds__(DM_THREADS)
-k_gemm_dmma(int M, int N, int K, const double2 *__restrict__ A, int64_t lda, const double2 *__restrict__ B,
-            int64_t ldb, double2 *__restrict__ C, int64_t ldc) {
+__device__ __forceinline__ void gemm_dmma_cta(int M, int N, int K, const double2 *__restrict__ A, int64_t lda,
+                                              const double2 *__restrict__ B, int64_t ldb, double2 *__restrict__ C,
+                                              int64_t ldc, int m0, int n0) {
     extern __shared__ __align__(16) unsigned char dm_smem[];
     double2 *As = reinterpret_cast<double2 *>(dm_smem);               // [stage][k][DM_LDA]
     double2 *Bs = As + DM_STAGES * DM_BK * DM_LDA;                     // [stage][k][DM_LDB] (k-major rows of n)
     const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
     const int g = lane >> 2, q = lane & 3;
     const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
-    const int m0 = blockIdx.x * DM_BM, n0 = blockIdx.y * DM_BN;
     const int nk = (K + DM_BK - 1) / DM_BK;
 
     auto load_stage = [&](int stage, int kt) {
@@ -143,4 +142,12 @@ k_gemm_dmma(int M, int N, int K, const double2 *__restrict__ A, int64_t lda, con
             }
         }
     }
+}
+
+// grid = (ceil(M / 64), ceil(N / 64)).
+template <bool NEG, bool BETA>
+__global__ void __launch_bounds__(DM_THREADS)
+k_gemm_dmma(int M, int N, int K, const double2 *__restrict__ A, int64_t lda, const double2 *__restrict__ B,
+            int64_t ldb, double2 *__restrict__ C, int64_t ldc) {
+    gemm_dmma_cta<NEG, BETA>(M, N, K, A, lda, B, ldb, C, ldc, blockIdx.x * DM_BM, blockIdx.y * DM_BN);
 }

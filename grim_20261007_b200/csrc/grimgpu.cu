@@ -20,6 +20,7 @@
 #include "tc_gemm.cuh"
 #include "ozaki.cuh"
 #include "dmma.cuh"
+#include "grouped.cuh"
 
 // ============================================================== errors
 static thread_local std::string g_last_error;
@@ -171,6 +172,11 @@ extern "C" int grim_release_workspace(grim_handle_t h) {
     for (auto &kv : h->ws) cudaFreeAsync(kv.second.first, h->stream);
     h->ws.clear();
     GRIM_CHECK_CUDA(cudaStreamSynchronize(h->stream));
+    if (h->grp_exec) {  // the captured grouped factorization read the freed buffers
+        cudaGraphExecDestroy(h->grp_exec);
+        h->grp_exec = nullptr;
+        h->grp_key.clear();
+    }
     return GRIM_OK;
 }
 
@@ -187,6 +193,7 @@ extern "C" int grim_destroy(grim_handle_t h) {
     for (cudaEvent_t e : h->events) cudaEventDestroy(e);
     if (h->chain) cudaStreamDestroy(h->chain);
     if (h->bulk) cudaStreamDestroy(h->bulk);
+    if (h->grp_exec) cudaGraphExecDestroy(h->grp_exec);
     if (h->own_stream) cudaStreamDestroy(h->own_stream);
     delete h;
     return GRIM_OK;
@@ -1311,6 +1318,273 @@ extern "C" int grim_zgesv_mixed_factored(grim_handle_t h, int n, int nrhs, const
     else
         s = mixed_refine<float2>(h, n, nrhs, (const float2 *)A32, lda32, (float2 *)LU32, ipiv, (double2 *)B, ldb, tol,
                                  max_iter, &st);
+    st.ms_solve = ts.stop_ms();
+    h->last = st;
+    if (stats) *stats = st;
+    return s;
+}
+
+// ============================================================== grouped factorization
+// Schedule of one grouped factorization (grouped.cuh): systems sorted by decreasing order;
+// per 64-column step p the number of active systems, of systems with a trailing matrix,
+// and, for the latter, prefix sums of the CTA counts of the panel solve, the operand
+// packing and the trailing update (offsets into one int array).
+struct GrpPlan {
+    std::vector<int> order;                 // sorted position -> caller's index
+    std::vector<int> active, upd;           // per step
+    std::vector<int> off, tot;              // 3 per step: apply, pack, update
+    std::vector<double> fl_diag, fl_apply, fl_upd;
+    std::vector<int> sched;
+    int nmax = 0;
+};
+
+template <typename C>
+static int grp_plan(int count, const int *n, GrpPlan *P) {
+    P->order.resize(count);
+    for (int i = 0; i < count; ++i) P->order[i] = i;
+    std::stable_sort(P->order.begin(), P->order.end(), [&](int a, int b) { return n[a] > n[b]; });
+    P->nmax = n[P->order[0]];
+    const int steps = ceil_div(P->nmax, NB);
+    P->active.assign(steps, 0);
+    for (int i = 0; i < count; ++i)
+        for (int p = 0; p < ceil_div(n[i], NB); ++p) P->active[p]++;
+    P->upd.assign(steps, 0);
+    for (int p = 0; p + 1 < steps; ++p) P->upd[p] = P->active[p + 1];
+    P->off.assign(3 * steps, 0);
+    P->tot.assign(3 * steps, 0);
+    P->fl_diag.assign(steps, 0.0);
+    P->fl_apply.assign(steps, 0.0);
+    P->fl_upd.assign(steps, 0.0);
+    P->sched.clear();
+    for (int p = 0; p < steps; ++p) {
+        for (int i = 0; i < P->active[p]; ++i) {
+            const int nbj = std::min(NB, n[P->order[i]] - NB * p);
+            P->fl_diag[p] += 8.0 * nbj * nbj * nbj / 3.0;
+        }
+        const int u = P->upd[p];
+        for (int k = 0; k < 3; ++k) {
+            P->off[3 * p + k] = (int)P->sched.size();
+            int64_t acc = 0;
+            P->sched.push_back(0);
+            for (int i = 0; i < u; ++i) {
+                const int rest = n[P->order[i]] - NB * p - NB;
+                int64_t c;
+                if (k == 0) {
+                    c = 2 * ceil_div(rest, NB);
+                    P->fl_apply[p] += 8.0 * 2.0 * rest * NB * NB;
+                } else if (k == 1) {
+                    c = sizeof(C) == sizeof(float2) ? (grp_rows_a(rest) + grp_rows_b(rest)) / 8 : 0;
+                } else {
+                    c = sizeof(C) == sizeof(float2) ? (int64_t)(grp_rows_a(rest) / TC_BM) * (grp_rows_b(rest) / GRP_BN)
+                                                    : (int64_t)ceil_div(rest, DM_BM) * ceil_div(rest, DM_BN);
+                    P->fl_upd[p] += 8.0 * (double)rest * rest * NB;
+                }
+                acc += c;
+                if (acc > 2000000000LL) return grim_fail(GRIM_ERR_ARGUMENT, "grouped factorization: too much work per step");
+                P->sched.push_back((int)acc);
+            }
+            P->tot[3 * p + k] = (int)acc;
+        }
+    }
+    return GRIM_OK;
+}
+
+// The launches of one grouped factorization, on h->stream (captured into a graph or not).
+template <typename C>
+static int grp_sequence(grim_context *h, const GrpPlan &P, const GrpSys *dsys, const int *dsched, int count,
+                        int *dout, int *err) {
+    const int steps = (int)P.active.size();
+    const size_t tri = (size_t)(NB * NBP + NB) * sizeof(C);
+    for (int p = 0; p < steps; ++p) {
+        const int a = P.active[p], u = P.upd[p];
+        k_grp_diag<C><<<a, 256, 0, h->stream>>>(dsys, p);
+        GRIM_CHECK_LAUNCH_W(h, kname("k_grp_diag", sizeof(C)), P.fl_diag[p], 0);
+        if (u > 0) {
+            k_grp_apply<C><<<P.tot[3 * p], 256, tri, h->stream>>>(dsys, p, dsched + P.off[3 * p], u);
+            GRIM_CHECK_LAUNCH_W(h, kname("k_grp_apply", sizeof(C)), P.fl_apply[p], 0);
+        }
+        if (a > u) {
+            k_grp_last<C><<<a - u, 256, 0, h->stream>>>(dsys, p, u);
+            GRIM_CHECK_LAUNCH(h, kname("k_grp_last", sizeof(C)));
+        }
+        if (u == 0) continue;
+        if constexpr (sizeof(C) == sizeof(float2)) {
+            k_grp_pack<<<P.tot[3 * p + 1], 256, 0, h->stream>>>(dsys, p, dsched + P.off[3 * p + 1], u);
+            GRIM_CHECK_LAUNCH(h, "k_grp_pack");
+            k_grp_tc_update<GRP_BN, GRP_STAGES><<<P.tot[3 * p + 2], TC_THREADS, TcCfg<GRP_BN, GRP_STAGES>::SMEM_BYTES,
+                                                 h->stream>>>(dsys, p, dsched + P.off[3 * p + 2], u, err);
+            GRIM_CHECK_LAUNCH_W(h, "k_grp_tc_update", P.fl_upd[p], 0);
+        } else {
+            k_grp_dmma_update<<<P.tot[3 * p + 2], DM_THREADS, DM_SMEM_BYTES, h->stream>>>(dsys, p,
+                                                                                           dsched + P.off[3 * p + 2], u);
+            GRIM_CHECK_LAUNCH_W(h, "k_grp_dmma_update", P.fl_upd[p], 0);
+        }
+    }
+    k_grp_laswp<C><<<dim3(ceil_div(P.nmax, 128), count), 128, 0, h->stream>>>(dsys);
+    GRIM_CHECK_LAUNCH(h, kname("k_grp_laswp", sizeof(C)));
+    k_grp_flags<<<ceil_div(count, 128), 128, 0, h->stream>>>(dsys, count, dout);
+    GRIM_CHECK_LAUNCH(h, "k_grp_flags");
+    return GRIM_OK;
+}
+
+template <typename C>
+static int grp_getrf(grim_context *h, int count, const int *n, void *const *A, const int64_t *lda, int *const *ipiv,
+                     bool use_graph, int *info, int *pivoted) {
+    GrpPlan P;
+    GRIM_TRY(grp_plan<C>(count, n, &P));
+    static bool attr = false;
+    if (!attr) {
+        const int tri = (NB * NBP + NB) * (int)sizeof(C);
+        GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_grp_apply<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, tri));
+        if constexpr (sizeof(C) == sizeof(float2))
+            GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_grp_tc_update<GRP_BN, GRP_STAGES>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 TcCfg<GRP_BN, GRP_STAGES>::SMEM_BYTES));
+        else
+            GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_grp_dmma_update, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 DM_SMEM_BYTES));
+        attr = true;
+    }
+    // per-system device buffers, carved from one workspace at 256-byte boundaries
+    auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    size_t ws_bytes = 0, flag_ints = 0;
+    for (int i = 0; i < count; ++i) {
+        const int m = n[P.order[i]];
+        ws_bytes += 2 * al((size_t)m * NB * sizeof(C));
+        if (sizeof(C) == sizeof(float2) && m > NB)
+            ws_bytes += 2 * al((size_t)grp_rows_a(m - NB) * GRP_KP * sizeof(float)) +
+                        2 * al((size_t)grp_rows_b(m - NB) * GRP_KP * sizeof(float));
+        flag_ints += 2 + 3 * (size_t)ceil_div(m, NB);
+    }
+    void *pws = nullptr, *pflags = nullptr, *ptab = nullptr, *psched = nullptr, *pout = nullptr;
+    GRIM_TRY(grim_workspace(h, "grp_ws", ws_bytes, &pws));
+    GRIM_TRY(grim_workspace(h, "grp_flags", flag_ints * sizeof(int), &pflags));
+    GRIM_TRY(grim_workspace(h, "grp_table", (size_t)count * sizeof(GrpSys), &ptab));
+    GRIM_TRY(grim_workspace(h, "grp_sched", P.sched.size() * sizeof(int), &psched));
+    GRIM_TRY(grim_workspace(h, "grp_out", 2 * (size_t)count * sizeof(int), &pout));
+    int *err = nullptr;
+    if (sizeof(C) == sizeof(float2)) GRIM_TRY(tc_err_flag(h, &err));
+    std::vector<GrpSys> tab(count);
+    char *w = (char *)pws;
+    int *f = (int *)pflags;
+    for (int i = 0; i < count; ++i) {
+        const int src = P.order[i], m = n[src];
+        GrpSys &S = tab[i];
+        S.A = A[src];
+        S.lda = lda[src];
+        S.n = m;
+        S.npan = ceil_div(m, NB);
+        S.ipiv = ipiv[src];
+        S.bcol = w;
+        w += al((size_t)m * NB * sizeof(C));
+        S.brow = w;
+        w += al((size_t)m * NB * sizeof(C));
+        S.flags = f;
+        f += 2 + 3 * S.npan;
+        S.pa_hi = S.pa_lo = S.pb_hi = S.pb_lo = nullptr;
+        if (sizeof(C) == sizeof(float2) && m > NB) {
+            const size_t ra = (size_t)grp_rows_a(m - NB) * GRP_KP, rb = (size_t)grp_rows_b(m - NB) * GRP_KP;
+            S.pa_hi = (float *)w;
+            w += al(ra * sizeof(float));
+            S.pa_lo = (float *)w;
+            w += al(ra * sizeof(float));
+            S.pb_hi = (float *)w;
+            w += al(rb * sizeof(float));
+            S.pb_lo = (float *)w;
+            w += al(rb * sizeof(float));
+        }
+    }
+    GRIM_CHECK_CUDA(cudaMemcpyAsync(ptab, tab.data(), (size_t)count * sizeof(GrpSys), cudaMemcpyHostToDevice, h->stream));
+    GRIM_CHECK_CUDA(cudaMemcpyAsync(psched, P.sched.data(), P.sched.size() * sizeof(int), cudaMemcpyHostToDevice,
+                                    h->stream));
+    GRIM_CHECK_CUDA(cudaMemsetAsync(pflags, 0, flag_ints * sizeof(int), h->stream));
+    const GrpSys *dsys = (const GrpSys *)ptab;
+    const int *dsched = (const int *)psched;
+    int *dout = (int *)pout;
+    if (use_graph && !h->profiling) {
+        std::vector<int64_t> key = {(int64_t)sizeof(C), (int64_t)count, (int64_t)(intptr_t)pws,
+                                    (int64_t)(intptr_t)pflags, (int64_t)(intptr_t)ptab, (int64_t)(intptr_t)psched,
+                                    (int64_t)(intptr_t)pout, (int64_t)(intptr_t)err};
+        for (int i = 0; i < count; ++i) key.push_back(n[P.order[i]]);
+        if (!h->grp_exec || key != h->grp_key) {
+            if (h->grp_exec) {
+                cudaGraphExecDestroy(h->grp_exec);
+                h->grp_exec = nullptr;
+                h->grp_key.clear();
+            }
+            // captured on the handle's private stream (the caller's may be the legacy
+            // default stream, which cannot be captured), launched on the caller's
+            GRIM_TRY(lookahead_streams(h, 2));
+            const cudaStream_t caller = h->stream;
+            GRIM_CHECK_CUDA(cudaStreamBeginCapture(h->chain, cudaStreamCaptureModeThreadLocal));
+            const int64_t l0 = h->launches;
+            h->stream = h->chain;
+            const int st = grp_sequence<C>(h, P, dsys, dsched, count, dout, err);
+            h->stream = caller;
+            cudaGraph_t graph = nullptr;
+            const cudaError_t ce = cudaStreamEndCapture(h->chain, &graph);
+            if (st != GRIM_OK) {
+                if (graph) cudaGraphDestroy(graph);
+                return st;
+            }
+            GRIM_CHECK_CUDA(ce);
+            const cudaError_t ie = cudaGraphInstantiate(&h->grp_exec, graph, 0);
+            cudaGraphDestroy(graph);
+            GRIM_CHECK_CUDA(ie);
+            h->grp_key = key;
+            h->grp_graph_launches = h->launches - l0;
+            h->launches = l0;
+        }
+        GRIM_CHECK_CUDA(cudaGraphLaunch(h->grp_exec, h->stream));
+        h->launches += h->grp_graph_launches;
+    } else {
+        GRIM_TRY(grp_sequence<C>(h, P, dsys, dsched, count, dout, err));
+    }
+    std::vector<int> out(2 * (size_t)count);
+    GRIM_CHECK_CUDA(cudaMemcpyAsync(out.data(), dout, out.size() * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    GRIM_CHECK_CUDA(cudaStreamSynchronize(h->stream));
+    if (sizeof(C) == sizeof(float2)) GRIM_TRY(tc_err_check(h, "grouped factorization"));
+    for (int i = 0; i < count; ++i) {
+        if (info) info[P.order[i]] = out[2 * i];
+        if (pivoted) pivoted[P.order[i]] = out[2 * i + 1];
+    }
+    return GRIM_OK;
+}
+
+extern "C" int grim_getrf_grouped(grim_handle_t h, int count, const int *n, void *const *A, const int64_t *lda,
+                                  int *const *ipiv, int complex64, int use_graph, int *info, int *pivoted) {
+    if (!h || count <= 0 || count > 65535 || !n || !A || !lda || !ipiv || !info)
+        return grim_fail(GRIM_ERR_ARGUMENT, "grim_getrf_grouped: bad arguments");
+    for (int i = 0; i < count; ++i)
+        if (n[i] <= 0 || !A[i] || !ipiv[i] || lda[i] < n[i])
+            return grim_fail(GRIM_ERR_ARGUMENT, "grim_getrf_grouped: bad system " + std::to_string(i));
+    DeviceGuard g(h->device);
+    if (complex64) return grp_getrf<float2>(h, count, n, A, lda, ipiv, use_graph != 0, info, pivoted);
+    return grp_getrf<double2>(h, count, n, A, lda, ipiv, use_graph != 0, info, pivoted);
+}
+
+// Refinement against an existing complex64 factorization with the stopping test chosen
+// by precision_mode (GRIM_PREC_MIXED: relative residual, GRIM_PREC_MIXED_BERR: backward
+// error).
+extern "C" int grim_zgesv_refine_factored(grim_handle_t h, int n, int nrhs, const void *A, int64_t lda,
+                                          const void *A32, int64_t lda32, void *LU32, const int *ipiv, void *B,
+                                          int64_t ldb, int precision_mode, double tol, int max_iter,
+                                          grim_solve_info *stats) {
+    if (!h || n <= 0 || nrhs <= 0 || !B || ldb < n || (!A && !A32) || (A && lda < n) || (A32 && lda32 < n) || !LU32 ||
+        !ipiv || (precision_mode != GRIM_PREC_MIXED && precision_mode != GRIM_PREC_MIXED_BERR))
+        return grim_fail(GRIM_ERR_ARGUMENT, "grim_zgesv_refine_factored: bad arguments");
+    DeviceGuard g(h->device);
+    grim_solve_info st{};
+    st.precision_mode = precision_mode;
+    const bool berr_test = precision_mode == GRIM_PREC_MIXED_BERR;
+    StreamTimer ts(h->stream);
+    int s;
+    if (A)
+        s = mixed_refine<double2>(h, n, nrhs, (const double2 *)A, lda, (float2 *)LU32, ipiv, (double2 *)B, ldb, tol,
+                                  max_iter, &st, berr_test);
+    else
+        s = mixed_refine<float2>(h, n, nrhs, (const float2 *)A32, lda32, (float2 *)LU32, ipiv, (double2 *)B, ldb, tol,
+                                 max_iter, &st, berr_test);
     st.ms_solve = ts.stop_ms();
     h->last = st;
     if (stats) *stats = st;

@@ -258,8 +258,8 @@ __device__ __forceinline__ void vset(C (&v)[L], int idx, C x) {
 //   every warp with rows and columns beyond k applies a_rc -= l_rk a_kc.
 // Certificate: |a_rk^(k)|_1 <= |a_kk^(k)|_1 for r > k, and a_kk != 0.
 template <typename C>
-__global__ void __launch_bounds__(256)
-k_diag_lu(int n, C *A, int64_t lda, int j, int nbj, C *backup_col, int *cert, int *ipiv) {
+__device__ __forceinline__ void diag_lu_cta(int n, C *A, int64_t lda, int j, int nbj, C *backup_col, int *cert,
+                                            int *ipiv) {
     __shared__ C rowbuf[2][NB];
     __shared__ C lbuf[2][NB];
     const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
@@ -324,6 +324,12 @@ k_diag_lu(int n, C *A, int64_t lda, int j, int nbj, C *backup_col, int *cert, in
         if (r < nbj && c < nbj) A[(int64_t)(j + c) * lda + j + r] = v[i];
     }
     if (__syncthreads_or(bad) && t == 0) atomicOr(cert, 1);
+}
+
+template <typename C>
+__global__ void __launch_bounds__(256)
+k_diag_lu(int n, C *A, int64_t lda, int j, int nbj, C *backup_col, int *cert, int *ipiv) {
+    diag_lu_cta<C>(n, A, lda, j, nbj, backup_col, cert, ipiv);
 }
 
 // ------------------------------------------------------------------ pivoted panel (fallback)
@@ -404,20 +410,20 @@ __device__ void pivoted_panel(int n, C *A, int64_t lda, int j, int nbj, int *ipi
 
 
 // ------------------------------------------------------------------ panel apply
-// grid.x = nL + nU CTAs of 256 threads.  CTA b < nL: 64 rows of A21 (4 lanes per row),
-// L21 = A21 inv(U11) by row substitution, certificate |l_ic u_cc|_1 <= |u_cc|_1.
-// CTA b >= nL: 64 columns of A12, U12 = inv(L11) A12 by column substitution.
-// Both back up what they overwrite; the last CTA to finish runs the pivoted
-// refactorization when any certificate failed.  Dynamic smem: NB * NBP + NB elements.
+// nblocks = nL + nU CTAs of 256 threads; this is CTA b.  CTA b < nL: 64 rows of A21 (4
+// lanes per row), L21 = A21 inv(U11) by row substitution, certificate
+// |l_ic u_cc|_1 <= |u_cc|_1.  CTA b >= nL: 64 columns of A12, U12 = inv(L11) A12 by column
+// substitution.  Both back up what they overwrite; the last CTA to finish runs the
+// pivoted refactorization when any certificate failed.  Dynamic smem: NB * NBP + NB
+// elements.
 template <typename C>
-__global__ void __launch_bounds__(256)
-k_panel_apply(int n, C *A, int64_t lda, int j, int nbj, int nL, C *backup_col, C *backup_row, int *cert,
-              int *counter, int *swapped, int *ipiv, int *info, int *pivoted) {
+__device__ __forceinline__ void panel_apply_cta(int n, C *A, int64_t lda, int j, int nbj, int nL, int b, int nblocks,
+                                                C *backup_col, C *backup_row, int *cert, int *counter, int *swapped,
+                                                int *ipiv, int *info, int *pivoted) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C *T = reinterpret_cast<C *>(smem_raw);
     C *rd = T + NB * NBP;
     const int t = threadIdx.x, s = t & 3, lane_vec = t >> 2;
-    const int b = blockIdx.x;
     const bool is_l = b < nL;
     stage_diag(A, lda, j, nbj, T, rd);
     C v[16];
@@ -474,7 +480,7 @@ k_panel_apply(int n, C *A, int64_t lda, int j, int nbj, int nL, C *backup_col, C
     __shared__ int s_last;
     __threadfence();
     __syncthreads();
-    if (t == 0) s_last = (atomicAdd(counter, 1) == (int)gridDim.x - 1);
+    if (t == 0) s_last = (atomicAdd(counter, 1) == nblocks - 1);
     __syncthreads();
     if (!s_last) return;
     __threadfence();
@@ -488,11 +494,18 @@ k_panel_apply(int n, C *A, int64_t lda, int j, int nbj, int nL, C *backup_col, C
     if (t == 0) atomicAdd(pivoted, 1);
 }
 
-// Single-CTA fallback driver when there is no trailing strip (last panel).
 template <typename C>
 __global__ void __launch_bounds__(256)
-k_panel_last(int n, C *A, int64_t lda, int j, int nbj, C *backup_col, int *cert, int *swapped, int *ipiv, int *info,
-             int *pivoted) {
+k_panel_apply(int n, C *A, int64_t lda, int j, int nbj, int nL, C *backup_col, C *backup_row, int *cert,
+              int *counter, int *swapped, int *ipiv, int *info, int *pivoted) {
+    panel_apply_cta<C>(n, A, lda, j, nbj, nL, blockIdx.x, gridDim.x, backup_col, backup_row, cert, counter, swapped,
+                       ipiv, info, pivoted);
+}
+
+// Single-CTA fallback driver when there is no trailing strip (last panel).
+template <typename C>
+__device__ __forceinline__ void panel_last_cta(int n, C *A, int64_t lda, int j, int nbj, C *backup_col, int *cert,
+                                               int *swapped, int *ipiv, int *info, int *pivoted) {
     if (*cert == 0) return;
     for (int c = 0; c < nbj; ++c)
         for (int r = threadIdx.x; r < n - j; r += 256) A[(int64_t)(j + c) * lda + j + r] = backup_col[(int64_t)c * n + r];
@@ -501,10 +514,17 @@ k_panel_last(int n, C *A, int64_t lda, int j, int nbj, C *backup_col, int *cert,
     if (threadIdx.x == 0) atomicAdd(pivoted, 1);
 }
 
+template <typename C>
+__global__ void __launch_bounds__(256)
+k_panel_last(int n, C *A, int64_t lda, int j, int nbj, C *backup_col, int *cert, int *swapped, int *ipiv, int *info,
+             int *pivoted) {
+    panel_last_cta<C>(n, A, lda, j, nbj, backup_col, cert, swapped, ipiv, info, pivoted);
+}
+
 // Apply interchanges of later panels to the columns left of them.
 template <typename C>
-__global__ void k_laswp_left(int n, C *A, int64_t lda, int nb, const int *swapped, const int *ipiv) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void laswp_left_col(int c, int n, C *A, int64_t lda, int nb, const int *swapped,
+                                               const int *ipiv) {
     if (c >= n) return;
     const int npan = (n + nb - 1) / nb;
     C *a = A + (int64_t)c * lda;
@@ -521,6 +541,11 @@ __global__ void k_laswp_left(int n, C *A, int64_t lda, int nb, const int *swappe
             }
         }
     }
+}
+
+template <typename C>
+__global__ void k_laswp_left(int n, C *A, int64_t lda, int nb, const int *swapped, const int *ipiv) {
+    laswp_left_col<C>(blockIdx.x * blockDim.x + threadIdx.x, n, A, lda, nb, swapped, ipiv);
 }
 
 // ------------------------------------------------------------------ getrs

@@ -69,9 +69,9 @@ __device__ __forceinline__ void tc_store_chunk(float *hi, float *lo, int64_t off
 // of an operand with Rp rows in the tile layout, zero padded to Mp x Kp and scaled by
 // sign (+1 or -1).  One thread per 16-byte chunk; consecutive threads take consecutive
 // rows so that the complex reads are coalesced.
-__global__ void k_tc_pack_a(int M, int K, const float2 *__restrict__ A, int64_t lda, float *__restrict__ hi,
-                            float *__restrict__ lo, int Mp, int Rp, int r_off, int Kp, float sign) {
-    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void tc_pack_a_chunk(int64_t idx, int M, int K, const float2 *__restrict__ A, int64_t lda,
+                                                float *__restrict__ hi, float *__restrict__ lo, int Mp, int Rp,
+                                                int r_off, int Kp, float sign) {
     if (idx >= (int64_t)Mp * (Kp >> 2)) return;
     const int r = (int)(idx % Mp), k0 = (int)(idx / Mp) * 4;
     const int m = r >> 1, t = r & 1, kc = k0 >> 1;
@@ -89,12 +89,16 @@ __global__ void k_tc_pack_a(int M, int K, const float2 *__restrict__ A, int64_t 
     tc_store_chunk(hi, lo, tc_tile_offset(r_off + r, k0, Rp), v[0], v[1], v[2], v[3]);
 }
 
+__global__ void k_tc_pack_a(int M, int K, const float2 *__restrict__ A, int64_t lda, float *__restrict__ hi,
+                            float *__restrict__ lo, int Mp, int Rp, int r_off, int Kp, float sign) {
+    tc_pack_a_chunk((int64_t)blockIdx.x * blockDim.x + threadIdx.x, M, K, A, lda, hi, lo, Mp, Rp, r_off, Kp, sign);
+}
+
 // B^ (rows n < Np, real columns 2k+s = (re, im) of B[k, n]) into the tile layout, zero
 // padded.  One thread per 16-byte chunk, consecutive threads along k (coalesced reads and
 // writes of a column).
-__global__ void k_tc_pack_b(int K, int N, const float2 *__restrict__ B, int64_t ldb, float *__restrict__ hi,
-                            float *__restrict__ lo, int Np, int Kp) {
-    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void tc_pack_b_chunk(int64_t idx, int K, int N, const float2 *__restrict__ B, int64_t ldb,
+                                                float *__restrict__ hi, float *__restrict__ lo, int Np, int Kp) {
     const int kq = Kp >> 2;
     if (idx >= (int64_t)Np * kq) return;
     const int n = (int)(idx / kq), k0 = (int)(idx % kq) * 4, kc = k0 >> 1;
@@ -110,6 +114,11 @@ __global__ void k_tc_pack_b(int K, int N, const float2 *__restrict__ B, int64_t 
         }
     }
     tc_store_chunk(hi, lo, tc_tile_offset(n, k0, Np), v[0], v[1], v[2], v[3]);
+}
+
+__global__ void k_tc_pack_b(int K, int N, const float2 *__restrict__ B, int64_t ldb, float *__restrict__ hi,
+                            float *__restrict__ lo, int Np, int Kp) {
+    tc_pack_b_chunk((int64_t)blockIdx.x * blockDim.x + threadIdx.x, K, N, B, ldb, hi, lo, Np, Kp);
 }
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -180,12 +189,13 @@ __device__ __forceinline__ void umma_ktile_tf32(uint32_t tmem, uint32_t sA, uint
 
 // C (interleaved complex64 viewed as real, column stride ldc_real floats):
 // C[m, n] = (m in [ow_lo, ow_hi) ? 0 : C[m, n]) + alpha * (A~ B^)[m, n]
-// for m < Mvalid, n < Nvalid.  grid = (Mp / 128, Np / BN); A and B in the tile layout.
+// for m < Mvalid, n < Nvalid; this CTA computes the tile at rows m0, columns n0.  A and B
+// in the tile layout.
 template <int BN, int STAGES>
-__global__ void __launch_bounds__(TC_THREADS)
-k_tc_gemm(int nk, const float *__restrict__ Ahi, const float *__restrict__ Alo, int Mp, const float *__restrict__ Bhi,
-          const float *__restrict__ Blo, int Np, float *__restrict__ C, int64_t ldc_real, int Mvalid, int Nvalid,
-          float alpha, int ow_lo, int ow_hi, int *err) {
+__device__ __forceinline__ void tc_gemm_cta(int nk, const float *__restrict__ Ahi, const float *__restrict__ Alo,
+                                            int Mp, const float *__restrict__ Bhi, const float *__restrict__ Blo,
+                                            int Np, float *__restrict__ C, int64_t ldc_real, int Mvalid, int Nvalid,
+                                            float alpha, int ow_lo, int ow_hi, int *err, int m0, int n0) {
     using Cfg = TcCfg<BN, STAGES>;
     extern __shared__ __align__(1024) unsigned char smem_dyn[];
     __shared__ __align__(8) uint64_t full[STAGES], empty[STAGES], done;
@@ -193,7 +203,6 @@ k_tc_gemm(int nk, const float *__restrict__ Ahi, const float *__restrict__ Alo, 
     __shared__ int s_fail;
     const uint32_t base = (smem_addr(smem_dyn) + 1023u) & ~1023u;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int m0 = blockIdx.x * TC_BM, n0 = blockIdx.y * BN;
     if (threadIdx.x == 0) {
         s_fail = 0;
         for (int s = 0; s < STAGES; ++s) {
@@ -317,4 +326,14 @@ k_tc_gemm(int nk, const float *__restrict__ Ahi, const float *__restrict__ Alo, 
     if (warp == 0) {
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BN) : "memory");
     }
+}
+
+// grid = (Mp / 128, Np / BN).
+template <int BN, int STAGES>
+__global__ void __launch_bounds__(TC_THREADS)
+k_tc_gemm(int nk, const float *__restrict__ Ahi, const float *__restrict__ Alo, int Mp, const float *__restrict__ Bhi,
+          const float *__restrict__ Blo, int Np, float *__restrict__ C, int64_t ldc_real, int Mvalid, int Nvalid,
+          float alpha, int ow_lo, int ow_hi, int *err) {
+    tc_gemm_cta<BN, STAGES>(nk, Ahi, Alo, Mp, Bhi, Blo, Np, C, ldc_real, Mvalid, Nvalid, alpha, ow_lo, ow_hi, err,
+                            blockIdx.x * TC_BM, blockIdx.y * BN);
 }

@@ -166,6 +166,81 @@ def monostatic_solve(body, k, angles_deg, pol, precision='double', tol=None, che
     return out
 
 
+def monostatic_solves_grouped(bodies, ks, angles_deg, pol, precision='mixed', tol=None, angles_dev=None,
+                              use_graph=True, workers=4):
+    """Many (geometry, frequency) systems of one polarization and one angle set -- the
+    systems of a frequency sweep -- solved together: fills and excitations on the device
+    worker pool, ONE grouped LU of all matrices (``grouped.getrf_grouped``, a captured CUDA
+    graph), then per system the triangular solves, the FP64 refinement (mixed) or backward
+    error (double) and the far field on the pool.  Same numerics per system as
+    ``monostatic_solve`` (the grouped factors equal the single-system ones), including the
+    mixed -> double fallback of a stalled refinement.  Returns [dict(amplitude, telemetry)]
+    in input order.
+    """
+    from ..device import run_pool
+    from ..grouped import getrf_grouped, refine_factored
+    from .. import tuning
+    pol = canonical_pol(pol)
+    if not bodies:
+        return []
+    dev = bodies[0].geom.device
+    if angles_dev is None:
+        angles_dev = torch.as_tensor(np.asarray(angles_deg, dtype=np.float64), device=dev)
+    nang = int(angles_dev.numel())
+    mixed = precision == 'mixed'
+    tol = MIXED_RCS_TOL if tol is None else float(tol)
+    costs = [float(b.n) ** 3 + nang * float(b.n) ** 2 for b in bodies]
+
+    def prep(i):
+        def run():
+            c = context()
+            z = fill(bodies[i], ks[i], pol, complex64=mixed, ctx=c)
+            b = rhs(bodies[i], ks[i], pol, angles_dev, ctx=c)
+            return {'z': z, 'lu': z.clone(), 'b': b}
+        return run
+
+    parts = run_pool([prep(i) for i in range(len(bodies))], workers=workers, costs=costs)
+    ipivs, infos, piv = getrf_grouped([p['lu'] for p in parts], use_graph=use_graph)
+    for i, inf in enumerate(infos):
+        if inf:
+            raise _lib.GrimError(_lib.GRIM_ERR_SINGULAR, f'system {i} (n={bodies[i].n}) is exactly singular '
+                                                         f'(info={inf})')
+
+    def finish(i):
+        def run():
+            c = context()
+            p = parts[i]
+            tele = {'grouped': True, 'pivoted_panels': piv[i]}
+            if mixed:
+                tuning.apply(c, bodies[i].n, nang)
+                b0 = p['b'].clone()
+                try:
+                    st = refine_factored(p['z'], p['lu'], ipivs[i], p['b'], tol, stop='berr', ctx=c)
+                    x = p['b']
+                except _lib.GrimNotConverged:
+                    z64 = fill(bodies[i], ks[i], pol, ctx=c)
+                    x = b0
+                    st = solve_inplace(z64, x, 'double', ctx=c)
+                    st['fp64_fallback'] = True
+            else:
+                x = p['b'].clone()
+                n = bodies[i].n
+                _lib.check(c.lib.grim_zgetrs(c.h, n, nang, ptr(p['lu']), n, ptr(ipivs[i]), ptr(x), n), 'grim_zgetrs')
+                st = {'precision_mode': _lib.PREC_FP64, 'backward_error_dev': backward_error(p['z'], x, p['b'], ctx=c)}
+            tele.update(st)
+            amp = farfield(bodies[i], ks[i], angles_dev, x, ctx=c)
+            # release this system's matrices as soon as its work is queued: they were
+            # allocated on another worker's stream, so the allocator must wait for this one
+            cur = torch.cuda.current_stream()
+            for t in p.values():
+                t.record_stream(cur)
+            p.clear()
+            return dict(amplitude=amp, telemetry=tele)
+        return run
+
+    return run_pool([finish(i) for i in range(len(bodies))], workers=workers, costs=costs)
+
+
 def sigma_2d(amp, k):
     return 0.25 / float(k) * np.abs(amp) ** 2
 

@@ -167,6 +167,31 @@ int grim_zgesv_mixed_factored(grim_handle_t h, int n, int nrhs, const void *A, i
                               int64_t lda32, void *LU32, const int *ipiv, void *B, int64_t ldb, double tol,
                               int max_iter, grim_solve_info *stats);
 
+/* grim_zgesv_mixed_factored with the stopping test of grim_zgesv_mixed: precision_mode
+ * GRIM_PREC_MIXED (relative residual) or GRIM_PREC_MIXED_BERR (backward error).  Used
+ * after grim_getrf_grouped for the systems of a sweep. */
+int grim_zgesv_refine_factored(grim_handle_t h, int n, int nrhs, const void *A, int64_t lda, const void *A32,
+                               int64_t lda32, void *LU32, const int *ipiv, void *B, int64_t ldb, int precision_mode,
+                               double tol, int max_iter, grim_solve_info *stats);
+
+/* Grouped LU of `count` (<= 65535) independent systems of different orders in one
+ * sequence of launches: the systems of a frequency sweep or the Fourier modes of a body
+ * of revolution, which the reference factors one per worker process
+ * (execution/frequency_sweep.py:140-188 _plan / _compute; bor/solver.py:2827-3250
+ * _mode_sweep_impl with bor/factor.py:120 ModalFactor per mode).  Each step of 64
+ * columns is one launch per stage over all systems (diagonal blocks, panel solves,
+ * trailing updates: split-TF32 tcgen05 for complex64, FP64 tensor cores for
+ * complex128).  Per system: n[i], device matrix A[i] (lda[i] >= n[i], complex64 if
+ * complex64 else complex128, overwritten by L\U with the same certified diagonal-pivot
+ * / partial-pivot fallback as grim_cgetrf / grim_zgetrf, identical factors), device
+ * pivots ipiv[i] (n[i] ints, 1-based).  use_graph: capture the launch sequence in a
+ * CUDA graph, kept on the handle and replayed while the orders (and the handle's
+ * buffers) stay the same.  info[i] (host): 0, or k+1 when U(k,k) is exactly zero;
+ * pivoted[i] (host, may be NULL): panels that fell back to partial pivoting.  Blocks
+ * until done. */
+int grim_getrf_grouped(grim_handle_t h, int count, const int *n, void *const *A, const int64_t *lda,
+                       int *const *ipiv, int complex64, int use_graph, int *info, int *pivoted);
+
 /* B1 drop-in (host buffers): solve A X = B for all nrhs columns, X overwrites B.
  * A: n x n complex128 column-major (lda >= n), B: n x nrhs complex128 (ldb >= n).
  * Copies host -> device, solves, copies device -> host; synchronous. */
