@@ -202,8 +202,47 @@ def _solve_mode(dev, m, th, precision, tol, ctx=None):
     return part, tele
 
 
+def _solve_modes_grouped(dev, modes, th, precision, tol, workers):
+    """All mode systems through one grouped LU (``grouped.solve_grouped``): assembly and
+    excitations on the worker pool, one grouped factorization of every mode matrix, then
+    the per-mode solves / refinement on the pool and the far-field projections here.  A
+    mode whose refinement stalls is re-solved in FP64 (the reference's ladder)."""
+    from ..grouped import solve_grouped
+
+    def prep(m):
+        def run():
+            c = context()
+            return dev.matrix(m, ctx=c), dev.excitation(m, th, far=False, ctx=c), dev.excitation(m, th, far=True, ctx=c)
+        return run
+
+    parts = run_pool([prep(m) for m in modes], workers=workers)
+    Zs = [p[0] for p in parts]
+    Vs = [p[1] for p in parts]
+    V0s = [v.clone() for v in Vs] if precision == 'mixed' else None
+    if tol is None:
+        tol = ops2d.MIXED_RCS_TOL
+    sts = solve_grouped(Zs, Vs, precision=precision, tol=tol, stop='berr', workers=workers)
+    ctx = context()
+    nth = int(th.numel())
+    outs = []
+    for i, st in enumerate(sts):
+        tele = {'fp64_fallback': False, 'grouped': True}
+        V = Vs[i]
+        if st.get('not_converged'):
+            tele['fp64_fallback'] = True
+            V = V0s[i]
+            st = ops2d.solve_inplace(Zs[i], V, 'double', ctx=ctx)
+        tele['refinement_steps'] = int(st.get('refinement_steps', 0))
+        part = torch.zeros(2 * nth, dtype=torch.complex128, device='cuda')
+        nred = int(Zs[i].shape[0])
+        _lib.check(ctx.lib.grim_bor_farfield_accumulate(ctx.h, nred, 2 * nth, ptr(parts[i][2]), nred, ptr(V), nred,
+                                                        ptr(part)), 'grim_bor_farfield_accumulate')
+        outs.append((part, tele))
+    return outs
+
+
 def solve_bor_device(points, k, thetas_deg, mmax, precision='double', tol=None, ctx=None, workers=None,
-                     signed_mode_symmetry=True):
+                     signed_mode_symmetry=True, grouped=True):
     """Device path: returns (F[2 nth] complex128 on the host, telemetry).
 
     The modal moments are built once; the per-mode systems are independent and run on the
@@ -214,7 +253,8 @@ def solve_bor_device(points, k, thetas_deg, mmax, precision='double', tol=None, 
     m > 0 counts twice: for the co-polarised monostatic far field the +m and -m
     contributions are identical (equal to the last bit in the oracle, for the sphere and
     the ogive).  With an explicit ``ctx`` (a serving slot) the modes run in turn on that
-    handle.
+    handle.  With ``grouped`` (default) the mode systems are factored together by one
+    grouped LU (``grouped.py``); otherwise each mode is factored on its own worker.
     """
     from ..twod.solver import sweep_workers
     dev = BorDevice(points, k, mmax, ctx=ctx)
@@ -224,6 +264,9 @@ def solve_bor_device(points, k, thetas_deg, mmax, precision='double', tol=None, 
     modes = list(range(0, mmax + 1)) if signed_mode_symmetry else list(range(-mmax, mmax + 1))
     if ctx is not None:
         outs = [_solve_mode(dev, m, th, precision, tol, ctx=ctx) for m in modes]
+    elif grouped:
+        outs = _solve_modes_grouped(dev, modes, th, precision, tol,
+                                    sweep_workers(len(modes)) if workers is None else workers)
     else:
         jobs = [(lambda m=m: _solve_mode(dev, m, th, precision, tol)) for m in modes]
         outs = run_pool(jobs, workers=sweep_workers(len(jobs)) if workers is None else workers)

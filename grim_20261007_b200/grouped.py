@@ -52,16 +52,18 @@ def getrf_grouped(mats, use_graph=True, ctx=None):
     return ipivs, list(info), list(piv)
 
 
-def refine_factored(z32, lu32, ipiv, b, tol, stop='berr', max_iter=10, ctx=None):
-    """FP64 refinement of the complex64 factorization ``lu32`` / ``ipiv`` of ``z32`` for the
-    right-hand sides ``b`` (complex128, (nrhs, n)); X overwrites ``b``.  Raises
-    GrimNotConverged when the refinement stalls.  Returns the solve telemetry dict."""
+def refine_factored(z, lu32, ipiv, b, tol, stop='berr', max_iter=10, ctx=None):
+    """FP64 refinement of the complex64 factorization ``lu32`` / ``ipiv`` of ``z`` (complex128,
+    or complex64 whose exact promotion is the system) for the right-hand sides ``b``
+    (complex128, (nrhs, n)); X overwrites ``b``.  Raises GrimNotConverged when the
+    refinement stalls.  Returns the solve telemetry dict."""
     ctx = ctx or context()
     n, nrhs = int(b.shape[1]), int(b.shape[0])
     mode = _lib.PREC_MIXED_BERR if stop == 'berr' else _lib.PREC_MIXED
     st = _lib.GrimSolveInfo()
-    status = ctx.lib.grim_zgesv_refine_factored(ctx.h, n, nrhs, None, 0, ptr(z32), n, ptr(lu32), ptr(ipiv), ptr(b), n,
-                                                mode, float(tol), int(max_iter), ctypes.byref(st))
+    z64, z32 = (z, None) if z.dtype == torch.complex128 else (None, z)
+    status = ctx.lib.grim_zgesv_refine_factored(ctx.h, n, nrhs, ptr(z64), n, ptr(z32), n, ptr(lu32), ptr(ipiv), ptr(b),
+                                                n, mode, float(tol), int(max_iter), ctypes.byref(st))
     _lib.check(status, 'grim_zgesv_refine_factored')
     return st.as_dict()
 
@@ -70,13 +72,14 @@ def solve_grouped(zs, bs, precision='mixed', tol=None, stop='berr', use_graph=Tr
     """Solve Z_i X_i = B_i for every system: one grouped LU of all matrices, then the
     triangular solves (and, mixed, the FP64 refinement) per system on the worker pool.
 
-    ``zs``: complex64 (mixed) or complex128 (double) column-major device matrices, kept;
+    ``zs``: column-major device matrices, kept (complex128, or for mixed complex64 whose exact
+    promotion is the system); the LU runs in complex64 (mixed) or complex128 (double);
     ``bs``: complex128 (nrhs_i, n_i) right-hand sides, overwritten by the solutions.
     Returns per-system telemetry dicts; a mixed system whose refinement stalls carries
     ``not_converged=True`` and its ``bs`` entry is left as the partial solution.
     """
     from .twod.operators import MIXED_RCS_TOL
-    lus = [z.clone() for z in zs]
+    lus = [z.to(torch.complex64, copy=True) if precision == 'mixed' else z.clone() for z in zs]
     ipivs, infos, piv = getrf_grouped(lus, use_graph=use_graph)
     for i, inf in enumerate(infos):
         if inf:

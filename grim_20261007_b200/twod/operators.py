@@ -168,8 +168,9 @@ def monostatic_solve(body, k, angles_deg, pol, precision='double', tol=None, che
 
 def monostatic_solves_grouped(bodies, ks, angles_deg, pol, precision='mixed', tol=None, angles_dev=None,
                               use_graph=True, workers=4):
-    """Many (geometry, frequency) systems of one polarization and one angle set -- the
-    systems of a frequency sweep -- solved together: fills and excitations on the device
+    """Many (geometry, frequency, polarization) systems with one angle set -- the systems
+    of a frequency sweep; ``pol`` is one polarization or one per system -- solved
+    together: fills and excitations on the device
     worker pool, ONE grouped LU of all matrices (``grouped.getrf_grouped``, a captured CUDA
     graph), then per system the triangular solves, the FP64 refinement (mixed) or backward
     error (double) and the far field on the pool.  Same numerics per system as
@@ -180,9 +181,9 @@ def monostatic_solves_grouped(bodies, ks, angles_deg, pol, precision='mixed', to
     from ..device import run_pool
     from ..grouped import getrf_grouped, refine_factored
     from .. import tuning
-    pol = canonical_pol(pol)
     if not bodies:
         return []
+    pols = [canonical_pol(pol)] * len(bodies) if isinstance(pol, str) else [canonical_pol(p) for p in pol]
     dev = bodies[0].geom.device
     if angles_dev is None:
         angles_dev = torch.as_tensor(np.asarray(angles_deg, dtype=np.float64), device=dev)
@@ -194,8 +195,8 @@ def monostatic_solves_grouped(bodies, ks, angles_deg, pol, precision='mixed', to
     def prep(i):
         def run():
             c = context()
-            z = fill(bodies[i], ks[i], pol, complex64=mixed, ctx=c)
-            b = rhs(bodies[i], ks[i], pol, angles_dev, ctx=c)
+            z = fill(bodies[i], ks[i], pols[i], complex64=mixed, ctx=c)
+            b = rhs(bodies[i], ks[i], pols[i], angles_dev, ctx=c)
             return {'z': z, 'lu': z.clone(), 'b': b}
         return run
 
@@ -218,7 +219,7 @@ def monostatic_solves_grouped(bodies, ks, angles_deg, pol, precision='mixed', to
                     st = refine_factored(p['z'], p['lu'], ipivs[i], p['b'], tol, stop='berr', ctx=c)
                     x = p['b']
                 except _lib.GrimNotConverged:
-                    z64 = fill(bodies[i], ks[i], pol, ctx=c)
+                    z64 = fill(bodies[i], ks[i], pols[i], ctx=c)
                     x = b0
                     st = solve_inplace(z64, x, 'double', ctx=c)
                     st['fp64_fallback'] = True

@@ -77,6 +77,7 @@ def _dense_backend_summary():
         'dense_rhs_column_count': sum(int(e.get('rhs_columns', 0)) for e in events),
         'dense_max_rhs_columns': max([int(e.get('rhs_columns', 0)) for e in events] or [0]),
         'dense_mixed_precision_solve_count': sum(1 for e in events if e.get('precision') == 'mixed'),
+        'dense_grouped_factorization_count': sum(1 for e in events if e.get('grouped_factorization')),
         'dense_fallback_reasons': [],
         'dense_gpu_fallback_reasons': [],
         'dense_gpu_devices': devices,
@@ -268,20 +269,19 @@ class _MeshCache:
             return self.meshes[f]
 
 
-def _solve_frequency(meshes, f, elevs, pol, precision, abort_event):
-    """One (frequency, polarisation) system on the current device worker: mesh, fill,
-    solve, far field; returns host samples and telemetry."""
+def _frequency_body(meshes, f, pol, abort_event):
+    """(wavenumber, device body) of one (frequency, polarisation) system."""
     if abort_event is not None and abort_event.is_set():
         raise InterruptedError('Solve canceled by user.')
-    t0 = time.perf_counter()
     k = 2.0 * math.pi * f * 1e9 / C0
     polys, geom = meshes.get(f)
     te_diag = geo.te_curvature_correction(polys) if pol == 'TE' else None
     dev = torch.device('cuda', torch.cuda.current_device())
-    body = ops.DeviceBody(geom, te_diag, device=dev)
-    angles = np.asarray(elevs, dtype=np.float64)
-    angles_dev = torch.as_tensor(angles, device=dev)
-    res = ops.monostatic_solve(body, k, angles, pol, precision=precision, angles_dev=angles_dev)
+    return k, ops.DeviceBody(geom, te_diag, device=dev)
+
+
+def _frequency_record(f, elevs, pol, precision, k, body, res, t0):
+    """Host samples and telemetry of one solved (frequency, polarisation) system."""
     amp = res['amplitude'].cpu().numpy()
     tele = res['telemetry']
     berr = tele.get('backward_error_dev')
@@ -307,9 +307,39 @@ def _solve_frequency(meshes, f, elevs, pol, precision, abort_event):
                                            amp.imag.tolist(), phase.tolist(), np.asarray(resid, float).tolist())]
     event = dict(requested='gpu', used='gpu_grim', factorizations=1, rhs_columns=len(elevs), n=body.n,
                  label=f'{pol} pulse {f:g} GHz', gpu_device=context().device_name, precision=precision,
-                 pivoted_panels=tele.get('pivoted_panels', 0), refinement_steps=tele.get('refinement_steps', 0))
+                 pivoted_panels=tele.get('pivoted_panels', 0), refinement_steps=tele.get('refinement_steps', 0),
+                 grouped_factorization=bool(tele.get('grouped', False)))
     return dict(samples=samples, residuals=[float(r) for r in resid], event=event, n=body.n,
                 seconds=time.perf_counter() - t0)
+
+
+def _solve_frequency(meshes, f, elevs, pol, precision, abort_event):
+    """One (frequency, polarisation) system on the current device worker: mesh, fill,
+    solve, far field; returns host samples and telemetry."""
+    t0 = time.perf_counter()
+    k, body = _frequency_body(meshes, f, pol, abort_event)
+    angles = np.asarray(elevs, dtype=np.float64)
+    angles_dev = torch.as_tensor(angles, device=body.geom.device)
+    res = ops.monostatic_solve(body, k, angles, pol, precision=precision, angles_dev=angles_dev)
+    return _frequency_record(f, elevs, pol, precision, k, body, res, t0)
+
+
+def _solve_frequencies_grouped(meshes, keys, elevs, precision, abort_event, workers):
+    """Every (polarisation, frequency) system of a sweep through one grouped factorization
+    (``operators.monostatic_solves_grouped``); returns the per-system outputs of
+    ``_solve_frequency`` in ``keys`` order."""
+    t0 = time.perf_counter()
+    built = run_pool([(lambda f=f, pol=pol: _frequency_body(meshes, f, pol, abort_event)) for pol, f in keys],
+                     workers=workers)
+    angles = np.asarray(elevs, dtype=np.float64)
+    angles_dev = torch.as_tensor(angles, device=built[0][1].geom.device)
+    res = ops.monostatic_solves_grouped([b for _k, b in built], [k for k, _b in built], angles,
+                                        [pol for pol, _f in keys], precision=precision, angles_dev=angles_dev,
+                                        workers=workers)
+    if abort_event is not None and abort_event.is_set():
+        raise InterruptedError('Solve canceled by user.')
+    return [_frequency_record(f, elevs, pol, precision, k, body, r, t0)
+            for (pol, f), (k, body), r in zip(keys, built, res)]
 
 
 def _frequency_cost(geometry_snapshot, geometry_units, f, n_angles):
@@ -386,7 +416,13 @@ def _sweep(geometry_snapshot, frequencies_ghz, elevations_deg, pols, geometry_un
                 pass
 
     t0 = time.perf_counter()
-    outs = run_pool(jobs, workers=sweep_workers(len(jobs)), costs=costs, on_done=on_done)
+    if len(freqs) > 1 and _grouped_sweeps():
+        # a sweep: every system through one grouped factorization (one CUDA graph)
+        outs = _solve_frequencies_grouped(meshes, keys, elevs, precision, abort_event, sweep_workers(len(jobs)))
+        for i, o in enumerate(outs):
+            on_done(i, o)
+    else:
+        outs = run_pool(jobs, workers=sweep_workers(len(jobs)), costs=costs, on_done=on_done)
     wall = time.perf_counter() - t0
     channels = {}
     for pol in pols:
@@ -395,6 +431,11 @@ def _sweep(geometry_snapshot, frequencies_ghz, elevations_deg, pols, geometry_un
                  'wall': wall}
         channels[pol] = _channel_result(pol, mine, precision, stage)
     return channels
+
+
+def _grouped_sweeps():
+    """Multi-frequency requests use the grouped factorization unless GRIM_GROUPED_SWEEP=0."""
+    return os.environ.get('GRIM_GROUPED_SWEEP', '1') != '0'
 
 
 def sweep_workers(njobs):

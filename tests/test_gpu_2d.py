@@ -142,9 +142,12 @@ def test_concurrent_channels_match_single_channel_solves(ctx):
                 np.testing.assert_allclose(a2, a1, rtol=1e-13, atol=1e-13 * np.max(np.abs(a1)))
 
 
-def test_frequency_sweep_pool_matches_single_frequency_solves(ctx):
-    """A multi-frequency request runs its systems on the device worker pool (largest first);
-    every frequency's samples equal a one-frequency solve, in request order."""
+@pytest.mark.parametrize('grouped', ['1', '0'])
+def test_frequency_sweep_pool_matches_single_frequency_solves(ctx, grouped, monkeypatch):
+    """A multi-frequency request factors its systems with one grouped LU (GRIM_GROUPED_SWEEP=1,
+    the default) or each on the device worker pool (0); either way every frequency's samples
+    equal a one-frequency solve, in request order."""
+    monkeypatch.setenv('GRIM_GROUPED_SWEEP', grouped)
     from grim_20261007_b200.execution import linear_precision
     from grim_20261007_b200.twod.solver import solve_monostatic_rcs_2d_single_polarization as solve1
     v = S.naca_symmetric(0.1, 160)
@@ -164,3 +167,4 @@ def test_frequency_sweep_pool_matches_single_frequency_solves(ctx):
             np.testing.assert_allclose(a2, a1, rtol=1e-13, atol=1e-13 * np.max(np.abs(a1)))
     counts = swept['metadata']
     assert counts['dense_gpu_solve_count'] == len(freqs) and counts['panel_count_max'] > counts['panel_count_min']
+    assert counts['dense_grouped_factorization_count'] == (len(freqs) if grouped == '1' else 0)

@@ -90,3 +90,21 @@ def test_signed_mode_symmetry_matches_all_modes():
     f_all, t_all = solve_bor_device(gen, k, th, 9, signed_mode_symmetry=False)
     assert t_half['mode_systems_solved'] == 10 and t_all['mode_systems_solved'] == 19
     np.testing.assert_allclose(f_half, f_all, rtol=1e-11, atol=1e-11 * np.max(np.abs(f_all)))
+
+
+@pytest.mark.parametrize('precision', ['double', 'mixed'])
+def test_grouped_modes_match_per_mode_solves(precision):
+    """The mode systems factored by one grouped LU give the same far field as each mode
+    factored on its own (identical factors; the mixed refinement stops at the same
+    backward-error target)."""
+    if not torch.cuda.is_available():
+        pytest.skip('no CUDA device')
+    from grim_20261007_b200.bor.solver import solve_bor_device
+    gen, _length, _half = S.ogive_case(8, n=60)
+    k = 10.0 / float(np.max(gen[:, 0]))
+    th = np.arange(0.0, 180.5, 5.0)
+    f_g, t_g = solve_bor_device(gen, k, th, 12, precision=precision)
+    f_1, t_1 = solve_bor_device(gen, k, th, 12, precision=precision, grouped=False)
+    assert t_g['mode_systems_solved'] == t_1['mode_systems_solved'] == 13
+    rtol = 1e-12 if precision == 'double' else 1e-8
+    np.testing.assert_allclose(f_g, f_1, rtol=rtol, atol=rtol * np.max(np.abs(f_1)))
