@@ -409,23 +409,29 @@ static int tc_pack_b(grim_context *h, int K, int N, const float2 *B, int64_t ldb
     return GRIM_OK;
 }
 
-template <int BN, int STAGES>
+template <int BN, int STAGES, bool STAGE_C>
 static int tc_launch(grim_context *h, const TcPacked &A, const TcPacked &B, float2 *C, int64_t ldc, int M, int N,
                      int Kc, float alpha, int ow_lo, int ow_hi, int *err) {
+    using Cfg = TcCfg<BN, STAGES, STAGE_C>;
     static bool attr = false;
     if (!attr) {
-        GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_tc_gemm<BN, STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             TcCfg<BN, STAGES>::SMEM_BYTES));
+        GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_tc_gemm<BN, STAGES, STAGE_C>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM_BYTES));
         attr = true;
     }
     dim3 grid(A.rows_p / TC_BM, ceil_div(N, BN));  // B.rows_p is the row stride of the packed B
-    k_tc_gemm<BN, STAGES><<<grid, TC_THREADS, TcCfg<BN, STAGES>::SMEM_BYTES, h->stream>>>(
+    k_tc_gemm<BN, STAGES, STAGE_C><<<grid, TC_THREADS, Cfg::SMEM_BYTES, h->stream>>>(
         A.kp / TC_BK, A.hi, A.lo, A.rows_p, B.hi, B.lo, B.rows_p, (float *)C, 2 * ldc, 2 * M, N, alpha, 2 * ow_lo,
         2 * ow_hi, err);
     GRIM_CHECK_LAUNCH_W(h, BN == 128 ? "k_tc_gemm<128>" : "k_tc_gemm<64>", 8.0 * M * N * Kc,
                         8.0 * ((double)A.rows_p * A.kp * (B.rows_p / BN) + (double)B.rows_p * B.kp) + 16.0 * M * N);
     return GRIM_OK;
 }
+
+// Short inner dimensions (at most 8 K-tiles of 32 floats: the rank-64 factorization updates)
+// spend most of a CTA's time in the epilogue: those launches stage C in shared memory during
+// the main loop (two or three pipeline stages are enough for so few K-tiles).
+#define TC_STAGE_C_MAX_KT 8
 
 // C[M x N] = (complex rows in [ow_lo, ow_hi) ? 0 : C) + alpha * A B with packed A (2M real
 // rows) and B (rows padded to bn); Kc is the complex inner dimension (for the flop count).
@@ -436,8 +442,13 @@ static int tc_gemm_packed(grim_context *h, int bn, const TcPacked &A, const TcPa
         return grim_fail(GRIM_ERR_ARGUMENT, "tensor-core GEMM: packed operand shapes disagree");
     int *err;
     GRIM_TRY(tc_err_flag(h, &err));
-    if (bn == 128) return tc_launch<128, 3>(h, A, B, C, ldc, M, N, Kc, alpha, ow_lo, ow_hi, err);
-    return tc_launch<64, 4>(h, A, B, C, ldc, M, N, Kc, alpha, ow_lo, ow_hi, err);
+    const bool stage_c = A.kp / TC_BK <= TC_STAGE_C_MAX_KT;
+    if (bn == 128) {
+        if (stage_c) return tc_launch<128, 2, true>(h, A, B, C, ldc, M, N, Kc, alpha, ow_lo, ow_hi, err);
+        return tc_launch<128, 3, false>(h, A, B, C, ldc, M, N, Kc, alpha, ow_lo, ow_hi, err);
+    }
+    if (stage_c) return tc_launch<64, 3, true>(h, A, B, C, ldc, M, N, Kc, alpha, ow_lo, ow_hi, err);
+    return tc_launch<64, 4, false>(h, A, B, C, ldc, M, N, Kc, alpha, ow_lo, ow_hi, err);
 }
 
 // C[MxN] = (overwrite ? 0 : C) + alpha A B[KxN] (complex64, column-major) on tcgen05 (split
@@ -1361,10 +1372,23 @@ struct GrpPlan {
     std::vector<double> fl_diag, fl_apply, fl_upd;
     std::vector<int> sched;
     int nmax = 0;
+    int bn = 128;  // output-tile width of the complex64 trailing update
 };
 
+// Output-tile width of the grouped complex64 trailing update: 128 (one CTA per SM, three
+// stages) or 64 (two stages, two CTAs per SM so that one CTA's epilogue overlaps the other's
+// loads).  GRIM_GROUPED_BN selects it; the packed operands are padded for either.
+static int grp_bn() {
+    static int bn = [] {
+        const char *e = getenv("GRIM_GROUPED_BN");
+        return (e && atoi(e) == 64) ? 64 : 128;
+    }();
+    return bn;
+}
+
 template <typename C>
-static int grp_plan(int count, const int *n, GrpPlan *P) {
+static int grp_plan(int count, const int *n, int bn, GrpPlan *P) {
+    P->bn = bn;
     P->order.resize(count);
     for (int i = 0; i < count; ++i) P->order[i] = i;
     std::stable_sort(P->order.begin(), P->order.end(), [&](int a, int b) { return n[a] > n[b]; });
@@ -1400,7 +1424,7 @@ static int grp_plan(int count, const int *n, GrpPlan *P) {
                 } else if (k == 1) {
                     c = sizeof(C) == sizeof(float2) ? (grp_rows_a(rest) + grp_rows_b(rest)) / 8 : 0;
                 } else {
-                    c = sizeof(C) == sizeof(float2) ? (int64_t)(grp_rows_a(rest) / TC_BM) * (grp_rows_b(rest) / GRP_BN)
+                    c = sizeof(C) == sizeof(float2) ? (int64_t)(grp_rows_a(rest) / TC_BM) * (grp_rows_b(rest) / bn)
                                                     : (int64_t)ceil_div(rest, DM_BM) * ceil_div(rest, DM_BN);
                     P->fl_upd[p] += 8.0 * (double)rest * rest * NB;
                 }
@@ -1436,8 +1460,13 @@ static int grp_sequence(grim_context *h, const GrpPlan &P, const GrpSys *dsys, c
         if constexpr (sizeof(C) == sizeof(float2)) {
             k_grp_pack<<<P.tot[3 * p + 1], 256, 0, h->stream>>>(dsys, p, dsched + P.off[3 * p + 1], u);
             GRIM_CHECK_LAUNCH(h, "k_grp_pack");
-            k_grp_tc_update<GRP_BN, GRP_STAGES><<<P.tot[3 * p + 2], TC_THREADS, TcCfg<GRP_BN, GRP_STAGES>::SMEM_BYTES,
-                                                 h->stream>>>(dsys, p, dsched + P.off[3 * p + 2], u, err);
+            if (P.bn == 64)
+                k_grp_tc_update<64, 3><<<P.tot[3 * p + 2], TC_THREADS, TcCfg<64, 3, true>::SMEM_BYTES, h->stream>>>(
+                    dsys, p, dsched + P.off[3 * p + 2], u, err);
+            else
+                k_grp_tc_update<GRP_BN, GRP_STAGES><<<P.tot[3 * p + 2], TC_THREADS,
+                                                     TcCfg<GRP_BN, GRP_STAGES, true>::SMEM_BYTES, h->stream>>>(
+                    dsys, p, dsched + P.off[3 * p + 2], u, err);
             GRIM_CHECK_LAUNCH_W(h, "k_grp_tc_update", P.fl_upd[p], 0);
         } else {
             k_grp_dmma_update<<<P.tot[3 * p + 2], DM_THREADS, DM_SMEM_BYTES, h->stream>>>(dsys, p,
@@ -1456,15 +1485,19 @@ template <typename C>
 static int grp_getrf(grim_context *h, int count, const int *n, void *const *A, const int64_t *lda, int *const *ipiv,
                      bool use_graph, int *info, int *pivoted) {
     GrpPlan P;
-    GRIM_TRY(grp_plan<C>(count, n, &P));
+    GRIM_TRY(grp_plan<C>(count, n, grp_bn(), &P));
     static bool attr = false;
     if (!attr) {
         const int tri = (NB * NBP + NB) * (int)sizeof(C);
         GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_grp_apply<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, tri));
         if constexpr (sizeof(C) == sizeof(float2))
+        {
             GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_grp_tc_update<GRP_BN, GRP_STAGES>,
                                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 TcCfg<GRP_BN, GRP_STAGES>::SMEM_BYTES));
+                                                 TcCfg<GRP_BN, GRP_STAGES, true>::SMEM_BYTES));
+            GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_grp_tc_update<64, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 TcCfg<64, 3, true>::SMEM_BYTES));
+        }
         else
             GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_grp_dmma_update, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                  DM_SMEM_BYTES));
@@ -1527,7 +1560,7 @@ static int grp_getrf(grim_context *h, int count, const int *n, void *const *A, c
     const int *dsched = (const int *)psched;
     int *dout = (int *)pout;
     if (use_graph && !h->profiling) {
-        std::vector<int64_t> key = {(int64_t)sizeof(C), (int64_t)count, (int64_t)(intptr_t)pws,
+        std::vector<int64_t> key = {(int64_t)sizeof(C), (int64_t)P.bn, (int64_t)count, (int64_t)(intptr_t)pws,
                                     (int64_t)(intptr_t)pflags, (int64_t)(intptr_t)ptab, (int64_t)(intptr_t)psched,
                                     (int64_t)(intptr_t)pout, (int64_t)(intptr_t)err};
         for (int i = 0; i < count; ++i) key.push_back(n[P.order[i]]);

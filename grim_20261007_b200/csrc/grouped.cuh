@@ -11,7 +11,8 @@
 //   k_grp_last      one CTA per system whose last panel this is (panel_last_cta);
 //   trailing update A22 -= L21 U12 of every system: complex64 as split-TF32 on tcgen05
 //                   (k_grp_pack packs both operands of all systems, k_grp_tc_update runs
-//                   every 128 x 128 output tile of every system), complex128 on the FP64
+//                   every 128 x 128 output tile of every system, its C tile staged in
+//                   shared memory during the main loop), complex128 on the FP64
 //                   tensor cores (k_grp_dmma_update, every 64 x 64 tile).
 // Systems are ordered by decreasing order, so the systems active at step p are a prefix
 // of the list.  A CTA finds its system by binary search in a per-step prefix sum of the
@@ -24,7 +25,7 @@
 #include "tc_gemm.cuh"
 
 #define GRP_BN 128              // output-tile width of the tensor-core trailing update
-#define GRP_STAGES 3
+#define GRP_STAGES 2              // pipeline stages (4 K-tiles per update; the C tile is staged too)
 #define GRP_KP (2 * NB)         // real inner dimension of a complex64 update (K = 64 complex)
 
 struct GrpSys {
@@ -109,8 +110,8 @@ k_grp_tc_update(const GrpSys *__restrict__ sys, int p, const int *prefix, int co
     const int Mp = grp_rows_a(rest), Np = grp_rows_b(rest), mt = Mp / TC_BM;
     const int t = blockIdx.x - __ldg(prefix + s);
     float2 *A22 = (float2 *)S.A + (int64_t)(j + NB) * S.lda + j + NB;
-    tc_gemm_cta<BN, STAGES>(GRP_KP / TC_BK, S.pa_hi, S.pa_lo, Mp, S.pb_hi, S.pb_lo, Np, (float *)A22, 2 * S.lda,
-                            2 * rest, rest, -1.f, 0, 0, err, (t % mt) * TC_BM, (t / mt) * BN);
+    tc_gemm_cta<BN, STAGES, true>(GRP_KP / TC_BK, S.pa_hi, S.pa_lo, Mp, S.pb_hi, S.pb_lo, Np, (float *)A22,
+                                  2 * S.lda, 2 * rest, rest, -1.f, 0, 0, err, (t % mt) * TC_BM, (t / mt) * BN);
 }
 
 // A22 -= L21 U12 for every updating complex128 system: ceil(rest / 64)^2 tiles each.

@@ -38,13 +38,20 @@
 #define TC_BK 32
 #define TC_THREADS 128
 
-template <int BN, int STAGES>
+template <int BN, int STAGES, bool STAGE_C = false>
 struct TcCfg {
     static constexpr int A_BYTES = TC_BM * TC_BK * 4;              // one hi or lo A tile
     static constexpr int B_BYTES = BN * TC_BK * 4;                 // one hi or lo B tile
     static constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;  // Ahi, Alo, Bhi, Blo
-    static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024;
+    static constexpr int C_BYTES = STAGE_C ? TC_BM * BN * 4 : 0;   // the C tile, staged during the main loop
+    static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + C_BYTES + 1024;
+    static_assert(SMEM_BYTES <= 227 * 1024, "shared memory per CTA");
 };
+
+// 8-byte asynchronous global -> shared copy (zero-filled when !valid; src then unused).
+__device__ __forceinline__ void cp_async8(uint32_t dst, const void *src, bool valid) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(dst), "l"(src), "r"(valid ? 8 : 0) : "memory");
+}
 
 __device__ __forceinline__ float tf32_rna(float x) {
     uint32_t r;
@@ -191,12 +198,16 @@ __device__ __forceinline__ void umma_ktile_tf32(uint32_t tmem, uint32_t sA, uint
 // C[m, n] = (m in [ow_lo, ow_hi) ? 0 : C[m, n]) + alpha * (A~ B^)[m, n]
 // for m < Mvalid, n < Nvalid; this CTA computes the tile at rows m0, columns n0.  A and B
 // in the tile layout.
-template <int BN, int STAGES>
+//
+// STAGE_C: warps 2-3 copy this CTA's C tile into shared memory (8-byte cp.async, one complex
+// element per copy) while the main loop runs, and the epilogue reads it from there, so no
+// global load waits in the epilogue; without it they only prefetch the tile into L2.
+template <int BN, int STAGES, bool STAGE_C = false>
 __device__ __forceinline__ void tc_gemm_cta(int nk, const float *__restrict__ Ahi, const float *__restrict__ Alo,
                                             int Mp, const float *__restrict__ Bhi, const float *__restrict__ Blo,
                                             int Np, float *__restrict__ C, int64_t ldc_real, int Mvalid, int Nvalid,
                                             float alpha, int ow_lo, int ow_hi, int *err, int m0, int n0) {
-    using Cfg = TcCfg<BN, STAGES>;
+    using Cfg = TcCfg<BN, STAGES, STAGE_C>;
     extern __shared__ __align__(1024) unsigned char smem_dyn[];
     __shared__ __align__(8) uint64_t full[STAGES], empty[STAGES], done;
     __shared__ uint32_t tmem_slot;
@@ -276,6 +287,19 @@ __device__ __forceinline__ void tc_gemm_cta(int nk, const float *__restrict__ Ah
             umma_commit(smem_addr(&done));  // arrives once every MMA issued above has completed
         }
         __syncwarp();
+    } else if (STAGE_C) {
+        // warps 2-3: C tile -> shared memory, [column][128 rows] floats; thread t copies the
+        // complex element (real rows 2t, 2t+1) of every column (zero outside the matrix and
+        // in the overwrite window)
+        const int t = threadIdx.x - 64, r = m0 + 2 * t;
+        const bool row_ok = r < Mvalid && !(r >= ow_lo && r < ow_hi);
+        const uint32_t sC = base + STAGES * Cfg::STAGE_BYTES + 8 * t;
+        for (int c = 0; c < BN; ++c) {
+            const bool ok = row_ok && n0 + c < Nvalid;
+            cp_async8(sC + c * (TC_BM * 4), ok ? (const void *)(C + (int64_t)(n0 + c) * ldc_real + r) : (const void *)C,
+                      ok);
+        }
+        asm volatile("cp.async.commit_group;\n\tcp.async.wait_all;" ::: "memory");
     } else {
         // warps 2-3: pull this CTA's slice of C into L2 while the main loop runs
         // (one 128-byte line per prefetch; rows of the overwrite window are not read)
@@ -308,10 +332,17 @@ __device__ __forceinline__ void tc_gemm_cta(int nk, const float *__restrict__ Ah
             if (row_ok) {
                 // all 16 loads first, then the stores (no load waits behind a store)
                 float cv[16];
+                if (STAGE_C) {
+                    const float *sCf = reinterpret_cast<const float *>(smem_dyn + (base - smem_addr(smem_dyn)) +
+                                                                       STAGES * Cfg::STAGE_BYTES);
 #pragma unroll
-                for (int j = 0; j < 16; ++j) {
-                    const int n = n0 + c + j;
-                    cv[j] = (!ow && n < Nvalid) ? C[(int64_t)n * ldc_real + m] : 0.f;
+                    for (int j = 0; j < 16; ++j) cv[j] = sCf[(c + j) * TC_BM + (m - m0)];
+                } else {
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) {
+                        const int n = n0 + c + j;
+                        cv[j] = (!ow && n < Nvalid) ? C[(int64_t)n * ldc_real + m] : 0.f;
+                    }
                 }
 #pragma unroll
                 for (int j = 0; j < 16; ++j) {
@@ -329,11 +360,11 @@ __device__ __forceinline__ void tc_gemm_cta(int nk, const float *__restrict__ Ah
 }
 
 // grid = (Mp / 128, Np / BN).
-template <int BN, int STAGES>
+template <int BN, int STAGES, bool STAGE_C = false>
 __global__ void __launch_bounds__(TC_THREADS)
 k_tc_gemm(int nk, const float *__restrict__ Ahi, const float *__restrict__ Alo, int Mp, const float *__restrict__ Bhi,
           const float *__restrict__ Blo, int Np, float *__restrict__ C, int64_t ldc_real, int Mvalid, int Nvalid,
           float alpha, int ow_lo, int ow_hi, int *err) {
-    tc_gemm_cta<BN, STAGES>(nk, Ahi, Alo, Mp, Bhi, Blo, Np, C, ldc_real, Mvalid, Nvalid, alpha, ow_lo, ow_hi, err,
-                            blockIdx.x * TC_BM, blockIdx.y * BN);
+    tc_gemm_cta<BN, STAGES, STAGE_C>(nk, Ahi, Alo, Mp, Bhi, Blo, Np, C, ldc_real, Mvalid, Nvalid, alpha, ow_lo, ow_hi,
+                                     err, blockIdx.x * TC_BM, blockIdx.y * BN);
 }
