@@ -187,6 +187,92 @@ def run_bor(args):
     return out
 
 
+def run_far_block(args):
+    """Galerkin far-field element-pair blocks (boundary B2, the reference's dominant fill
+    pass): a 1024 x 1024 tile of linear elements on the seeded airfoil (every pair farther
+    than 3 element lengths, 6 x 6 Gauss points, S, K and mirrored K), on the GPU
+    (device-resident inputs: CUDA events; host buffers through ghost_far_block: wall
+    clock) and, where it was built, the reference's own far.c on one host core over a
+    bounded sample of rows."""
+    import ctypes
+    import torch
+    from grim_20261007_b200 import synthetic as S
+    from grim_20261007_b200.device import context
+    from grim_20261007_b200.twod.farblock import KernelTable, far_block
+    v, _k, _f, _t = S.airfoil_case(args.seed, 1024)
+    a, b = v, np.roll(v, -1, axis=0)
+    x, w = np.polynomial.legendre.leggauss(6)
+    sfrac = (x + 1) / 2
+    pts = np.ascontiguousarray(a[:, None, :] * (1 - sfrac)[None, :, None] + b[:, None, :] * sfrac[None, :, None])
+    tan = b - a
+    length = np.linalg.norm(tan, axis=1)
+    normal = np.ascontiguousarray(np.stack([tan[:, 1], -tan[:, 0]], -1) / length[:, None])
+    qw = np.ascontiguousarray(w * 0.5)
+    phi = np.ascontiguousarray(np.stack([(1 - x) / 2, (1 + x) / 2], -1))
+    cent = (a + b) / 2
+    far = np.ascontiguousarray((np.linalg.norm(cent[:, None] - cent[None], axis=-1) > 3 * length.max())
+                               .astype(np.uint8))
+    k = 2 * np.pi / (10 * np.median(length))  # 10 elements per wavelength
+    table = KernelTable(k, 1.2)  # chord 1 m: every distance lies inside the table
+    mb = nb = len(v)
+    pairs = int(far.sum())
+    ctx = context()
+    dev = {key: torch.as_tensor(val, device='cuda') for key, val in
+           dict(o=pts, s=pts, qw=qw, phi=phi, on=normal, sn=normal, far=far).items()}
+    db = torch.as_tensor(table.bounds, device='cuda')
+    dc = torch.as_tensor(table.normalized_power.view(np.float64).ravel(), device='cuda')
+    accs = [torch.zeros((4, mb, nb), dtype=torch.complex128, device='cuda') for _ in range(3)]
+    ptrs = [ctypes.c_void_p(dev[key].data_ptr()) for key in ('o', 's', 'qw', 'phi', 'on', 'sn', 'far')]
+
+    def run_dev():
+        for acc in accs:
+            acc.zero_()
+        return ctx.lib.grim_far_block(ctx.h, mb, nb, 6, 2, *ptrs, 1, 1, 1, 1, k, 0.0, len(table.bounds) - 1,
+                                      ctypes.c_void_p(db.data_ptr()), table.normalized_power.shape[1] - 1,
+                                      ctypes.c_void_p(dc.data_ptr()), *(ctypes.c_void_p(t.data_ptr()) for t in accs))
+    assert run_dev() == 0
+    times = []
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        assert run_dev() == 0
+        e1.record()
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1) / 1e3)
+    t_dev = float(np.median(times))
+    far_block(table, k, pts, pts, qw, phi, normal, normal, far, 1, True, True, True)
+    t0 = time.perf_counter()
+    host = far_block(table, k, pts, pts, qw, phi, normal, normal, far, 1, True, True, True)
+    t_host = time.perf_counter() - t0
+    out = {'tile': f'{mb} x {nb} linear elements, 6 x 6 points, S + K + mirrored K', 'far_pairs': pairs,
+           'kernel_table_intervals': len(table.bounds) - 1,
+           'gpu_device_seconds': t_dev, 'gpu_pairs_per_s': pairs / t_dev,
+           'gpu_host_buffers_seconds': t_host, 'gpu_host_buffers_pairs_per_s': pairs / t_host}
+    ref_lib = os.path.join(ROOT, 'oracle', '_ref', 'libghost_far_ref.so')
+    if os.path.exists(ref_lib):
+        lib = ctypes.CDLL(ref_lib)
+        fun = lib.ghost_far_block
+        p = ctypes.c_void_p
+        fun.argtypes = [ctypes.c_int64, ctypes.c_int64, ctypes.c_int, ctypes.c_int] + [p] * 7 + [ctypes.c_int] * 4 + \
+            [ctypes.c_double] * 2 + [ctypes.c_int, p, ctypes.c_int, p, p, p, p]
+        fun.restype = ctypes.c_int
+        rows = 64
+        sub = [np.zeros((4, rows, nb), complex) for _ in range(3)]
+        pw = np.ascontiguousarray(table.normalized_power)
+        t0 = time.perf_counter()
+        st = fun(rows, nb, 6, 2, pts.ctypes.data, pts.ctypes.data, qw.ctypes.data, phi.ctypes.data,
+                 normal.ctypes.data, normal.ctypes.data, far.ctypes.data, 1, 1, 1, 1, k, 0.0, len(table.bounds) - 1,
+                 table.bounds.ctypes.data, pw.shape[1] - 1, pw.ctypes.data, *(a_.ctypes.data for a_ in sub))
+        t_ref = time.perf_counter() - t0
+        sample_pairs = int(far[:rows].sum())
+        same = st == 0 and all(np.array_equal(h_[:, :rows], s_) for h_, s_ in zip(host, sub))
+        out.update(reference_cpu_pairs_per_s=sample_pairs / t_ref, reference_cpu_cores=1,
+                   reference_sample=f'first {rows} observation elements ({sample_pairs} far pairs)',
+                   gpu_vs_reference_cpu=(pairs / t_host) / (sample_pairs / t_ref),
+                   bitwise_equal_to_reference_on_sample=bool(same))
+    return out
+
+
 def run_sweep(args, rank=0, world=1):
     """Frequency sweep on the seeded airfoil: 256 frequencies log-spaced over 20:1, N = 10 panels
     per wavelength (uneven sizes), 181 angles, TM, mixed precision.  Timed twice: every system
@@ -332,6 +418,7 @@ def main():
     ap.add_argument('--bor', type=int, default=1, help='time the body-of-revolution ogive workload')
     ap.add_argument('--sweep', type=int, default=256, help='frequencies of the airfoil sweep leg (0 = skip)')
     ap.add_argument('--autotune', type=int, default=1, help='tune the solve tile shapes for the workload first')
+    ap.add_argument('--far-block', type=int, default=1, help='time the Galerkin far-block pass (boundary B2)')
     args = ap.parse_args()
 
     world = int(os.environ.get('WORLD_SIZE', '1'))
@@ -465,6 +552,7 @@ def main():
     serving = run_serving(args) if (args.serving and rank == 0 and world == 1) else None
     bor = run_bor(args) if (args.bor and rank == 0 and world == 1) else None
     sweep = run_sweep(args, rank, world) if args.sweep else None
+    farblk = run_far_block(args) if (args.far_block and rank == 0 and world == 1) else None
 
     # per-kernel profile of one mixed step, polarisations in turn (CUDA events after every
     # launch on the launching stream, separate from the timed loop)
@@ -525,6 +613,7 @@ def main():
             'serving': serving,
             'bor_ogive': bor,
             'frequency_sweep': sweep,
+            'far_block': farblk,
             'autotune': autotune,
             'kernel_profile_mixed': prof,
             'kernel_profile_fp64': prof64,

@@ -87,6 +87,10 @@ SIGNATURES = [
                                            ctypes.POINTER(GrimSolveInfo)]),
     ('grim_getrf_grouped', c_int, [c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int, P_int,
                                    P_int]),
+    ('ghost_far_block', c_int, [c_int64, c_int64, c_int, c_int] + [c_void_p] * 7 + [c_int] * 4 +
+     [c_double, c_double, c_int, c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p]),
+    ('grim_far_block', c_int, [c_void_p, c_int64, c_int64, c_int, c_int] + [c_void_p] * 7 + [c_int] * 4 +
+     [c_double, c_double, c_int, c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p]),
     ('grim_zgesv_batched', c_int, [c_void_p, c_int, c_int, c_void_p, c_int, c_void_p, c_int, c_int, P_int]),
     ('grim_last_solve_info', c_int, [c_void_p, ctypes.POINTER(GrimSolveInfo)]),
     ('grim_mem_info', c_int, [c_void_p, ctypes.POINTER(c_size_t), ctypes.POINTER(c_size_t)]),

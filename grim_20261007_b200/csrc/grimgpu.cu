@@ -21,6 +21,7 @@
 #include "ozaki.cuh"
 #include "dmma.cuh"
 #include "grouped.cuh"
+#include "farblock.cuh"
 
 // ============================================================== errors
 static thread_local std::string g_last_error;
@@ -1647,6 +1648,124 @@ extern "C" int grim_zgesv_refine_factored(grim_handle_t h, int n, int nrhs, cons
     h->last = st;
     if (stats) *stats = st;
     return s;
+}
+
+// ============================================================== Galerkin far blocks (boundary B2)
+// Argument check of twod/assembly/native/far.c:114-117 (status 3).
+static bool far_args_ok(int64_t mb, int64_t nb, int q, int width, int want_s, int want_k, int mirrored,
+                        int intervals, int degree, const void *acc_s, const void *acc_k, const void *acc_kt) {
+    return !(mb < 0 || nb < 0 || q < 1 || width < 1 || width > FAR_MAX_WIDTH || intervals < 1 || degree < 0 ||
+             degree > 32 || (!want_s && !want_k) || (want_s && !acc_s) || (want_k && !acc_k) ||
+             (want_k && mirrored && !acc_kt));
+}
+
+// Device-pointer form: returns 0, 2 (a far distance below the table: the caller's
+// fallback case, accumulators undefined) or 3 (bad arguments); GRIM_ERR_CUDA on a device
+// error.
+extern "C" int grim_far_block(grim_handle_t h, int64_t mb, int64_t nb, int q, int width, const double *obs_pts,
+                              const double *src_pts, const double *qw, const double *phi, const double *obs_norm,
+                              const double *src_norm, const uint8_t *far, int obs_normal_deriv, int want_s,
+                              int want_k, int mirrored, double k_re, double k_im, int intervals,
+                              const double *bounds, int degree, const double *coeff, double *acc_s, double *acc_k,
+                              double *acc_kt) {
+    if (!h) return grim_fail(GRIM_ERR_ARGUMENT, "grim_far_block: null handle");
+    if (!far_args_ok(mb, nb, q, width, want_s, want_k, mirrored, intervals, degree, acc_s, acc_k, acc_kt)) {
+        grim_set_error("grim_far_block: bad arguments");
+        return 3;
+    }
+    if (mb == 0 || nb == 0) return GRIM_OK;
+    DeviceGuard g(h->device);
+    void *pst = nullptr;
+    GRIM_TRY(grim_workspace(h, "far_status", sizeof(int), &pst));
+    int *status = (int *)pst;
+    GRIM_CHECK_CUDA(cudaMemsetAsync(status, 0, sizeof(int), h->stream));
+    const FarTable t{intervals, degree, bounds, coeff, k_re, k_im};
+    const int64_t pairs = mb * nb;
+    const int threads = 128;
+    const int64_t blocks = (pairs + threads - 1) / threads;
+    if (blocks > 2147483647LL) {
+        grim_set_error("grim_far_block: too many pairs for one launch");
+        return 3;
+    }
+#define FAR_LAUNCH(W)                                                                                            \
+    k_far_block<W><<<(unsigned)blocks, threads, 0, h->stream>>>(mb, nb, q, width, obs_pts, src_pts, qw, phi,     \
+                                                                obs_norm, src_norm, far, obs_normal_deriv,       \
+                                                                want_s, want_k, mirrored, t, acc_s, acc_k,       \
+                                                                acc_kt, status)
+    if (width == 2) FAR_LAUNCH(2);
+    else if (width == 3) FAR_LAUNCH(3);
+    else if (width == 4) FAR_LAUNCH(4);
+    else FAR_LAUNCH(0);
+#undef FAR_LAUNCH
+    GRIM_CHECK_LAUNCH_W(h, "k_far_block", 0.0, 0.0);
+    int hs = 0;
+    GRIM_CHECK_CUDA(cudaMemcpyAsync(&hs, status, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    GRIM_CHECK_CUDA(cudaStreamSynchronize(h->stream));
+    return hs ? 2 : GRIM_OK;
+}
+
+// Host-buffer form with the exact signature and status codes of the reference's
+// ghost_far_block (twod/assembly/native/far.c:193-207, loaded by
+// twod/assembly/native/far.py:184-199): copies in, runs grim_far_block on the calling
+// thread's own handle (current device), copies the accumulators back.  Thread-safe.
+extern "C" int ghost_far_block(int64_t mb, int64_t nb, int q, int width, const double *obs_pts,
+                               const double *src_pts, const double *qw, const double *phi, const double *obs_norm,
+                               const double *src_norm, const uint8_t *far, int obs_normal_deriv, int want_s,
+                               int want_k, int mirrored, double k_re, double k_im, int intervals,
+                               const double *bounds, int degree, const double *coeff, double *acc_s, double *acc_k,
+                               double *acc_kt) {
+    if (!far_args_ok(mb, nb, q, width, want_s, want_k, mirrored, intervals, degree, acc_s, acc_k, acc_kt)) return 3;
+    if (mb == 0 || nb == 0) return 0;
+    static thread_local grim_context *h = nullptr;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return GRIM_ERR_CUDA;
+    if (!h || h->device != dev) {
+        if (h) grim_destroy(h);
+        h = nullptr;
+        GRIM_TRY(grim_create(dev, &h));
+    }
+    DeviceGuard g(h->device);
+    const bool with_kt = want_k && mirrored;
+    const size_t acc_bytes = (size_t)width * width * mb * nb * 2 * sizeof(double);
+    const size_t pts_o = (size_t)mb * q * 2, pts_s = (size_t)nb * q * 2;
+    const size_t tab_c = (size_t)intervals * (degree + 1) * 4;
+    size_t dbl = pts_o + pts_s + q + (size_t)q * width + 2 * (size_t)mb + 2 * (size_t)nb + (intervals + 1) + tab_c;
+    const size_t bytes = dbl * sizeof(double) + (size_t)mb * nb + 3 * acc_bytes + 1024;
+    void *pw = nullptr;
+    GRIM_TRY(grim_workspace(h, "far_io", bytes, &pw));
+    double *d = (double *)pw;
+    double *d_op = d, *d_sp = d_op + pts_o, *d_qw = d_sp + pts_s, *d_phi = d_qw + q, *d_on = d_phi + (size_t)q * width,
+           *d_sn = d_on + 2 * mb, *d_b = d_sn + 2 * nb, *d_c = d_b + (intervals + 1);
+    double *d_as = (double *)(((uintptr_t)(d_c + tab_c) + 255) & ~(uintptr_t)255);
+    double *d_ak = (double *)((char *)d_as + acc_bytes), *d_akt = (double *)((char *)d_ak + acc_bytes);
+    uint8_t *d_far = (uint8_t *)((char *)d_akt + acc_bytes);
+    auto up = [&](void *dst, const void *src, size_t n) {
+        return cudaMemcpyAsync(dst, src, n, cudaMemcpyHostToDevice, h->stream);
+    };
+    GRIM_CHECK_CUDA(up(d_op, obs_pts, pts_o * sizeof(double)));
+    GRIM_CHECK_CUDA(up(d_sp, src_pts, pts_s * sizeof(double)));
+    GRIM_CHECK_CUDA(up(d_qw, qw, q * sizeof(double)));
+    GRIM_CHECK_CUDA(up(d_phi, phi, (size_t)q * width * sizeof(double)));
+    GRIM_CHECK_CUDA(up(d_on, obs_norm, 2 * mb * sizeof(double)));
+    GRIM_CHECK_CUDA(up(d_sn, src_norm, 2 * nb * sizeof(double)));
+    GRIM_CHECK_CUDA(up(d_b, bounds, (intervals + 1) * sizeof(double)));
+    GRIM_CHECK_CUDA(up(d_c, coeff, tab_c * sizeof(double)));
+    GRIM_CHECK_CUDA(up(d_far, far, (size_t)mb * nb));
+    if (want_s) GRIM_CHECK_CUDA(up(d_as, acc_s, acc_bytes));
+    if (want_k) GRIM_CHECK_CUDA(up(d_ak, acc_k, acc_bytes));
+    if (with_kt) GRIM_CHECK_CUDA(up(d_akt, acc_kt, acc_bytes));
+    const int s = grim_far_block(h, mb, nb, q, width, d_op, d_sp, d_qw, d_phi, d_on, d_sn, d_far, obs_normal_deriv,
+                                 want_s, want_k, mirrored, k_re, k_im, intervals, d_b, degree, d_c,
+                                 want_s ? d_as : nullptr, want_k ? d_ak : nullptr, with_kt ? d_akt : nullptr);
+    if (s != GRIM_OK) return s;
+    auto down = [&](void *dst, const void *src, size_t n) {
+        return cudaMemcpyAsync(dst, src, n, cudaMemcpyDeviceToHost, h->stream);
+    };
+    if (want_s) GRIM_CHECK_CUDA(down(acc_s, d_as, acc_bytes));
+    if (want_k) GRIM_CHECK_CUDA(down(acc_k, d_ak, acc_bytes));
+    if (with_kt) GRIM_CHECK_CUDA(down(acc_kt, d_akt, acc_bytes));
+    GRIM_CHECK_CUDA(cudaStreamSynchronize(h->stream));
+    return 0;
 }
 
 // B1 drop-in with host buffers.

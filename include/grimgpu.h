@@ -21,6 +21,8 @@
  *   grim_farfield2d      twod/assembly/kernels.py:163-219  farfield (matched monostatic)
  *   grim_backward_error  twod/solver.py:695-720  backward_metrics (normwise backward error)
  *   grim_bor_*           bor/solver.py:1769-1962,2558-2608  per-mode assembly, excitation, far field
+ *   ghost_far_block      twod/assembly/native/far.c:193-207  ghost_far_block (same signature, GPU)
+ *   grim_far_block       the same on device pointers
  *
  * Status codes: 0 = success; any other value is an error and grim_last_error()
  * returns a message for the calling thread.
@@ -191,6 +193,35 @@ int grim_zgesv_refine_factored(grim_handle_t h, int n, int nrhs, const void *A, 
  * until done. */
 int grim_getrf_grouped(grim_handle_t h, int count, const int *n, void *const *A, const int64_t *lda,
                        int *const *ipiv, int complex64, int use_graph, int *info, int *pivoted);
+
+/* ---- linear-Galerkin far-field element-pair blocks (boundary B2) -------------------
+ * Replaces twod/assembly/native/far.c:100-207 ghost_far_block, the native far pass of
+ * the reference's Galerkin fill (twod/operators.py:2447-2458 _far_tile calls it through
+ * twod/assembly/native/far.py:184-249 far_block).  For every pair (i, j) with far[i*nb+j]
+ * != 0: acc[(width*a + b), i, j] += sum_qi qw[qi] phi[qi,a] sum_qj qw[qj] phi[qj,b] K(r),
+ * K = G (acc_s), the normal derivative (acc_k) and, if mirrored, the transposed-normal
+ * kernel (acc_kt), all interleaved complex128 of shape (width^2, mb, nb); G and dG from
+ * the caller's kernel table (bounds[intervals+1], coeff[intervals][degree+1][2] complex
+ * normalized power coefficients) or, beyond it, the large-argument Hankel expansion.
+ * Same arithmetic and order as the reference (no fused multiply-add): pairs inside the
+ * table get bitwise the reference's sums.  Status: 0; 2 when a distance falls below the
+ * table (the caller's fallback case; accumulators then undefined); 3 on bad arguments
+ * (far.c:114-117); other codes: GRIM_ERR_*.
+ *
+ * ghost_far_block: HOST buffers and the exact signature of the reference's export, so
+ * the reference's far.py can load this library in place of libghost_far.so; each calling
+ * thread gets its own device handle on the current device (kept until process exit). */
+int ghost_far_block(int64_t mb, int64_t nb, int q, int width, const double *obs_pts, const double *src_pts,
+                    const double *qw, const double *phi, const double *obs_norm, const double *src_norm,
+                    const uint8_t *far, int obs_normal_deriv, int want_s, int want_k, int mirrored, double k_re,
+                    double k_im, int intervals, const double *bounds, int degree, const double *coeff, double *acc_s,
+                    double *acc_k, double *acc_kt);
+/* grim_far_block: the same on DEVICE pointers, on the handle's stream (blocks until done). */
+int grim_far_block(grim_handle_t h, int64_t mb, int64_t nb, int q, int width, const double *obs_pts,
+                   const double *src_pts, const double *qw, const double *phi, const double *obs_norm,
+                   const double *src_norm, const uint8_t *far, int obs_normal_deriv, int want_s, int want_k,
+                   int mirrored, double k_re, double k_im, int intervals, const double *bounds, int degree,
+                   const double *coeff, double *acc_s, double *acc_k, double *acc_kt);
 
 /* B1 drop-in (host buffers): solve A X = B for all nrhs columns, X overwrites B.
  * A: n x n complex128 column-major (lda >= n), B: n x nrhs complex128 (ldb >= n).
