@@ -178,7 +178,9 @@ def run_bor(args):
         torch.cuda.synchronize()
         dt = time.perf_counter() - t0
         res[prec] = F
-        out[prec] = {'seconds': dt, 'solves_per_s': 1.0 / dt, 'refinement_steps': tele['refinement_steps']}
+        out[prec] = {'seconds': dt, 'solves_per_s': 1.0 / dt, 'refinement_steps': tele['refinement_steps'],
+                     'fp64_fallback_modes': tele.get('fp64_fallback_modes', 0),
+                     'stage_seconds': tele.get('stage_seconds')}
     s64 = 4 * np.pi * np.abs(res['double']) ** 2
     s32 = 4 * np.pi * np.abs(res['mixed']) ** 2
     db = 10 * np.log10(np.maximum(s64, 1e-30))
@@ -244,9 +246,17 @@ def run_far_block(args):
     t0 = time.perf_counter()
     host = far_block(table, k, pts, pts, qw, phi, normal, normal, far, 1, True, True, True)
     t_host = time.perf_counter() - t0
+    # algorithmic FP64 operations of one pair (width 2, q = 6, inside the table): per point pair
+    # 6 (distance) + 3 (interval coordinate) + 96 (two degree-12 complex Horner chains) + 6 (K
+    # projection) + 18 (S, K partial sums) + 16 (mirrored K), per observation point 52
+    flops_pair = 36 * 145 + 6 * 52
     out = {'tile': f'{mb} x {nb} linear elements, 6 x 6 points, S + K + mirrored K', 'far_pairs': pairs,
            'kernel_table_intervals': len(table.bounds) - 1,
            'gpu_device_seconds': t_dev, 'gpu_pairs_per_s': pairs / t_dev,
+           'roofline': {'bound': 'fp64 pipe (separately rounded multiply and add, no FMA, for bitwise parity)',
+                        'flops_per_pair': flops_pair, 'achieved_tflops': pairs * flops_pair / t_dev / 1e12,
+                        'peak_tflops_nominal_fp64_no_fma': 20.0,
+                        'frac': pairs * flops_pair / t_dev / 1e12 / 20.0},
            'gpu_host_buffers_seconds': t_host, 'gpu_host_buffers_pairs_per_s': pairs / t_host}
     ref_lib = os.path.join(ROOT, 'oracle', '_ref', 'libghost_far_ref.so')
     if os.path.exists(ref_lib):

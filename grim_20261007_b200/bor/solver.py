@@ -215,23 +215,36 @@ def _solve_modes_grouped(dev, modes, th, precision, tol, workers):
             return dev.matrix(m, ctx=c), dev.excitation(m, th, far=False, ctx=c), dev.excitation(m, th, far=True, ctx=c)
         return run
 
+    import time
+    t0 = time.perf_counter()
     parts = run_pool([prep(m) for m in modes], workers=workers)
     Zs = [p[0] for p in parts]
     Vs = [p[1] for p in parts]
     V0s = [v.clone() for v in Vs] if precision == 'mixed' else None
     if tol is None:
         tol = ops2d.MIXED_RCS_TOL
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
     sts = solve_grouped(Zs, Vs, precision=precision, tol=tol, stop='berr', workers=workers)
+    torch.cuda.synchronize()
+    t2 = time.perf_counter()
+    # stalled refinements (ill-conditioned modes): the reference's ladder to the double LU,
+    # here one grouped FP64 factorization of all of them
+    stalled = [i for i, st in enumerate(sts) if st.get('not_converged')]
+    if stalled:
+        redo = solve_grouped([Zs[i] for i in stalled], [V0s[i] for i in stalled], precision='double',
+                             workers=workers)
+        for i, st in zip(stalled, redo):
+            sts[i] = dict(st, fp64_fallback=True)
+            Vs[i] = V0s[i]
+    torch.cuda.synchronize()
+    stage = {'assembly': t1 - t0, 'grouped_factor_and_solves': t2 - t1, 'fp64_fallbacks': time.perf_counter() - t2}
     ctx = context()
     nth = int(th.numel())
     outs = []
     for i, st in enumerate(sts):
-        tele = {'fp64_fallback': False, 'grouped': True}
+        tele = {'fp64_fallback': bool(st.get('fp64_fallback')), 'grouped': True, 'stage_seconds': stage}
         V = Vs[i]
-        if st.get('not_converged'):
-            tele['fp64_fallback'] = True
-            V = V0s[i]
-            st = ops2d.solve_inplace(Zs[i], V, 'double', ctx=ctx)
         tele['refinement_steps'] = int(st.get('refinement_steps', 0))
         part = torch.zeros(2 * nth, dtype=torch.complex128, device='cuda')
         nred = int(Zs[i].shape[0])
@@ -257,9 +270,13 @@ def solve_bor_device(points, k, thetas_deg, mmax, precision='double', tol=None, 
     grouped LU (``grouped.py``); otherwise each mode is factored on its own worker.
     """
     from ..twod.solver import sweep_workers
+    import time
+    tm = time.perf_counter()
     dev = BorDevice(points, k, mmax, ctx=ctx)
     for m in (0, 1, -1, 2):
         dev.mode_map(m)  # build the shared pole maps before the workers read them
+    torch.cuda.synchronize()
+    t_moments = time.perf_counter() - tm
     th = torch.as_tensor(np.asarray(thetas_deg, dtype=np.float64), device='cuda')
     modes = list(range(0, mmax + 1)) if signed_mode_symmetry else list(range(-mmax, mmax + 1))
     if ctx is not None:
@@ -281,6 +298,7 @@ def solve_bor_device(points, k, thetas_deg, mmax, precision='double', tol=None, 
     fallbacks = sum(1 for _p, t in outs if t['fp64_fallback'])
     if fallbacks:
         tele['fp64_fallback_modes'] = fallbacks
+    tele['stage_seconds'] = dict(modal_moments=t_moments, **(outs[0][1].get('stage_seconds') or {}))
     F = amp.cpu().numpy() * (-1j * k * ETA0 / (4.0 * np.pi))
     tele['n_unknowns'] = 2 * (dev.ne + 1)
     return F, tele

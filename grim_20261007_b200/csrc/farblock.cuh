@@ -23,6 +23,8 @@
 
 #define FAR_EPS 1e-12
 #define FAR_MAX_WIDTH 8
+#define FAR_DEGREE 12  // the reference tables' polynomial degree (twod/assembly/kernels.py:338)
+#define FAR_SMEM_BOUNDS 4097  // tables up to 4096 intervals keep their bounds in shared memory
 
 struct FarTable {
     int intervals, degree;
@@ -101,20 +103,39 @@ __device__ void far_asymptotic(const FarTable &t, double r, double *out) {
 // Kernel values at distance r: false below the table (the caller's fallback case).
 __device__ __forceinline__ bool far_kernel(const FarTable &t, double r, double *out) {
     const double *bounds = t.bounds;
-    if (!(r >= __ldg(bounds))) return false;
-    if (r > __ldg(bounds + t.intervals)) {
+    if (!(r >= bounds[0])) return false;
+    if (r > bounds[t.intervals]) {
         far_asymptotic(t, r, out);
         return true;
     }
     int lo = 0, hi = t.intervals;
     while (lo + 1 < hi) {
         const int mid = lo + (hi - lo) / 2;
-        if (r < __ldg(bounds + mid)) hi = mid;
+        if (r < bounds[mid]) hi = mid;
         else lo = mid;
     }
-    const double b0 = __ldg(bounds + lo), b1 = __ldg(bounds + lo + 1);
+    const double b0 = bounds[lo], b1 = bounds[lo + 1];
     const double x = __ddiv_rn(far_sub(r, b0), far_sub(b1, b0));
     const double *base = t.coeff + (int64_t)lo * (t.degree + 1) * 4;
+    if (t.degree == FAR_DEGREE) {
+        // the usual degree: all coefficient loads issued ahead of the two Horner chains
+        double cf[4 * (FAR_DEGREE + 1)];
+#pragma unroll
+        for (int e = 0; e < 4 * (FAR_DEGREE + 1); ++e) cf[e] = __ldg(base + e);
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+            const int off = 2 * c;
+            double re = cf[4 * FAR_DEGREE + off], im = cf[4 * FAR_DEGREE + off + 1];
+#pragma unroll
+            for (int j = FAR_DEGREE - 1; j >= 0; --j) {
+                re = far_add(far_mul(re, x), cf[4 * j + off]);
+                im = far_add(far_mul(im, x), cf[4 * j + off + 1]);
+            }
+            out[2 * c] = re;
+            out[2 * c + 1] = im;
+        }
+        return true;
+    }
     for (int c = 0; c < 2; ++c) {
         const int off = 2 * c;
         double re = __ldg(base + 4 * t.degree + off), im = __ldg(base + 4 * t.degree + off + 1);
@@ -139,8 +160,9 @@ __device__ __forceinline__ void far_first_or_add(double *acc, bool first, double
 }
 
 // W > 0: compile-time width (accumulators in registers); W = 0: runtime width <= 8.
-template <int W>
-__global__ void __launch_bounds__(128)
+// MINB: CTAs per SM the register allocation must allow.
+template <int W, int MINB>
+__global__ void __launch_bounds__(128, MINB)
 k_far_block(int64_t mb, int64_t nb, int q, int width_rt, const double *__restrict__ obs_pts,
             const double *__restrict__ src_pts, const double *__restrict__ qw, const double *__restrict__ phi,
             const double *__restrict__ obs_norm, const double *__restrict__ src_norm, const uint8_t *__restrict__ far,
@@ -150,6 +172,13 @@ k_far_block(int64_t mb, int64_t nb, int q, int width_rt, const double *__restric
     const int width = W > 0 ? W : width_rt;
     const int64_t plane = mb * nb;
     const int64_t pair = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    // the table's interval bounds in shared memory (the binary search reads them most)
+    extern __shared__ double s_bounds[];
+    if (table.intervals + 1 <= FAR_SMEM_BOUNDS) {
+        for (int e = threadIdx.x; e <= table.intervals; e += blockDim.x) s_bounds[e] = table.bounds[e];
+        __syncthreads();
+        table.bounds = s_bounds;
+    }
     if (pair >= plane || !far[pair]) return;
     const int64_t i = pair / nb, j = pair % nb;
     const bool with_kt = want_k && mirrored;

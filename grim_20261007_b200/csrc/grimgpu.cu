@@ -1687,15 +1687,25 @@ extern "C" int grim_far_block(grim_handle_t h, int64_t mb, int64_t nb, int q, in
         grim_set_error("grim_far_block: too many pairs for one launch");
         return 3;
     }
-#define FAR_LAUNCH(W)                                                                                            \
-    k_far_block<W><<<(unsigned)blocks, threads, 0, h->stream>>>(mb, nb, q, width, obs_pts, src_pts, qw, phi,     \
+    const size_t smem = intervals + 1 <= FAR_SMEM_BOUNDS ? (size_t)(intervals + 1) * sizeof(double) : 0;
+    static bool attr = false;
+    if (!attr) {
+        const int mx = FAR_SMEM_BOUNDS * (int)sizeof(double);
+        GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_far_block<0, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+        GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_far_block<2, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+        GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_far_block<3, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+        GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_far_block<4, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+        attr = true;
+    }
+#define FAR_LAUNCH(W, MINB)                                                                                      \
+    k_far_block<W, MINB><<<(unsigned)blocks, threads, smem, h->stream>>>(mb, nb, q, width, obs_pts, src_pts, qw, phi, \
                                                                 obs_norm, src_norm, far, obs_normal_deriv,       \
                                                                 want_s, want_k, mirrored, t, acc_s, acc_k,       \
                                                                 acc_kt, status)
-    if (width == 2) FAR_LAUNCH(2);
-    else if (width == 3) FAR_LAUNCH(3);
-    else if (width == 4) FAR_LAUNCH(4);
-    else FAR_LAUNCH(0);
+    if (width == 2) FAR_LAUNCH(2, 3);
+    else if (width == 3) FAR_LAUNCH(3, 2);
+    else if (width == 4) FAR_LAUNCH(4, 1);
+    else FAR_LAUNCH(0, 1);
 #undef FAR_LAUNCH
     GRIM_CHECK_LAUNCH_W(h, "k_far_block", 0.0, 0.0);
     int hs = 0;
