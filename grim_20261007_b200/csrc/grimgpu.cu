@@ -535,19 +535,28 @@ static int lookahead_streams(grim_context *h, int nevents) {
 // Trailing update A22 -= L21 U12 split into the next panel's 64 columns ("narrow", on the
 // current stream) and the rest ("wide", on `wide_stream`).  For complex64 both operands
 // are packed once, into the buffer pair `slot`, and shared by the two tensor-core GEMMs.
+// Packed operand buffers of one trailing update (double-buffered by panel parity); B rows
+// padded so that a 128-wide tile starting at row 64 stays inside the buffer.
+static int lu_packed(grim_context *h, int rest, int nbj, int slot, TcPacked *pa, TcPacked *pb) {
+    const int Kp = tc_kp(nbj);
+    GRIM_TRY(tc_ws(h, slot ? "lu_pa1" : "lu_pa0", tc_rows_a(rest), Kp, pa));
+    GRIM_TRY(tc_ws(h, slot ? "lu_pb1" : "lu_pb0", ceil_div(rest + NB, 128) * 128, Kp, pb));
+    return GRIM_OK;
+}
+
+// prepacked: the panel solve already wrote both operands into the slot's buffers.
 template <typename C>
 static int trailing_update(grim_context *h, int rest, int nbj, const C *L21, const C *U12, C *A22, int64_t lda,
-                           cudaStream_t wide_stream, cudaEvent_t packed, int slot) {
+                           cudaStream_t wide_stream, cudaEvent_t packed, int slot, bool prepacked = false) {
     const int nn = std::min(NB, rest), nw = rest - nn;
     if constexpr (sizeof(C) == sizeof(float2)) {
         if (tc_enabled()) {
-            const int Kp = tc_kp(nbj);
             TcPacked pa, pb;
-            // B rows padded so that a 128-wide tile starting at row 64 stays inside the buffer
-            GRIM_TRY(tc_ws(h, slot ? "lu_pa1" : "lu_pa0", tc_rows_a(rest), Kp, &pa));
-            GRIM_TRY(tc_ws(h, slot ? "lu_pb1" : "lu_pb0", ceil_div(rest + NB, 128) * 128, Kp, &pb));
-            GRIM_TRY(tc_pack_a(h, rest, nbj, (const float2 *)L21, lda, 1.f, pa));
-            GRIM_TRY(tc_pack_b(h, nbj, rest, (const float2 *)U12, lda, pb));
+            GRIM_TRY(lu_packed(h, rest, nbj, slot, &pa, &pb));
+            if (!prepacked) {
+                GRIM_TRY(tc_pack_a(h, rest, nbj, (const float2 *)L21, lda, 1.f, pa));
+                GRIM_TRY(tc_pack_b(h, nbj, rest, (const float2 *)U12, lda, pb));
+            }
             GRIM_TRY(tc_gemm_packed(h, 64, pa, pb, (float2 *)A22, lda, rest, nn, nbj, -1.f, 0, 0));
             if (nw > 0) {
                 GRIM_CHECK_CUDA(cudaEventRecord(packed, h->stream));
@@ -632,12 +641,27 @@ static int getrf_impl(grim_context *h, int n, C *A, int64_t lda, int *ipiv, int 
         const int rest = n - j - nbj;
         if (rest > 0) {
             const int nL = ceil_div(rest, NB), nU = nL;
+            // complex64 on tensor cores: the panel solve writes the update's packed operands
+            PanelPack pk;
+            const bool prepack = sizeof(C) == sizeof(float2) && tc_enabled() && nbj == NB;
+            if (prepack) {
+                TcPacked pa, pb;
+                status = lu_packed(h, rest, nbj, p & 1, &pa, &pb);
+                if (status != GRIM_OK) break;
+                pk.a_hi = pa.hi;
+                pk.a_lo = pa.lo;
+                pk.a_rows = pa.rows_p;
+                pk.b_hi = pb.hi;
+                pk.b_lo = pb.lo;
+                pk.b_rows = pb.rows_p;
+            }
             k_panel_apply<C><<<nL + nU, 256, tri, h->stream>>>(n, A, lda, j, nbj, nL, bcol, brow, cert + p,
-                                                               counter + p, swapped + p, ipiv, d_info, d_pivoted);
+                                                               counter + p, swapped + p, ipiv, d_info, d_pivoted, pk);
             status = grim_launch_status(h, kname("k_panel_apply", sizeof(C)), 8.0 * 2 * rest * nbj * nbj, 0);
             if (status != GRIM_OK) break;
             status = trailing_update<C>(h, rest, nbj, A + (int64_t)j * lda + j + nbj, A + (int64_t)(j + nbj) * lda + j,
-                                        A + (int64_t)(j + nbj) * lda + j + nbj, lda, wide, h->events[2 + p], p & 1);
+                                        A + (int64_t)(j + nbj) * lda + j + nbj, lda, wide, h->events[2 + p], p & 1,
+                                        prepack);
             if (status != GRIM_OK) break;
             if (rest > NB && split) {
                 status = grim_cuda_status(cudaEventRecord(h->events[2 + npan + p], wide), "cudaEventRecord");
@@ -1459,8 +1483,7 @@ static int grp_sequence(grim_context *h, const GrpPlan &P, const GrpSys *dsys, c
         }
         if (u == 0) continue;
         if constexpr (sizeof(C) == sizeof(float2)) {
-            k_grp_pack<<<P.tot[3 * p + 1], 256, 0, h->stream>>>(dsys, p, dsched + P.off[3 * p + 1], u);
-            GRIM_CHECK_LAUNCH(h, "k_grp_pack");
+            // (the operands were packed by k_grp_apply)
             if (P.bn == 64)
                 k_grp_tc_update<64, 3><<<P.tot[3 * p + 2], TC_THREADS, TcCfg<64, 3, true>::SMEM_BYTES, h->stream>>>(
                     dsys, p, dsched + P.off[3 * p + 2], u, err);

@@ -10,7 +10,7 @@
 //                   that system's pivoted fallback when its certificate failed);
 //   k_grp_last      one CTA per system whose last panel this is (panel_last_cta);
 //   trailing update A22 -= L21 U12 of every system: complex64 as split-TF32 on tcgen05
-//                   (k_grp_pack packs both operands of all systems, k_grp_tc_update runs
+//                   (k_grp_apply writes both operands packed, k_grp_tc_update runs
 //                   every 128 x 128 output tile of every system, its C tile staged in
 //                   shared memory during the main loop), complex128 on the FP64
 //                   tensor cores (k_grp_dmma_update, every 64 x 64 tile).
@@ -63,13 +63,22 @@ __global__ void __launch_bounds__(256, 1) k_grp_diag(const GrpSys *__restrict__ 
 
 // Systems 0..count-1 all have a trailing matrix at step p (rest > 0, so nbj = NB).
 template <typename C>
-__global__ void __launch_bounds__(256) k_grp_apply(const GrpSys *__restrict__ sys, int p, const int *prefix, int count) {
+__global__ void __launch_bounds__(256, sizeof(C) == 8 ? 3 : 2) k_grp_apply(const GrpSys *__restrict__ sys, int p, const int *prefix, int count) {
     const int s = grp_find(prefix, count, blockIdx.x);
     const GrpSys &S = sys[s];
     const int j = NB * p, rest = S.n - j - NB, nL = (rest + NB - 1) / NB;
     int *cert = S.flags + 2, *swapped = cert + S.npan, *counter = swapped + S.npan;
+    PanelPack pk;  // complex64: the panel solve writes the trailing update's packed operands
+    if (sizeof(C) == sizeof(float2)) {
+        pk.a_hi = S.pa_hi;
+        pk.a_lo = S.pa_lo;
+        pk.a_rows = grp_rows_a(rest);
+        pk.b_hi = S.pb_hi;
+        pk.b_lo = S.pb_lo;
+        pk.b_rows = grp_rows_b(rest);
+    }
     panel_apply_cta<C>(S.n, (C *)S.A, S.lda, j, NB, nL, blockIdx.x - __ldg(prefix + s), 2 * nL, (C *)S.bcol,
-                       (C *)S.brow, cert + p, counter + p, swapped + p, S.ipiv, S.flags, S.flags + 1);
+                       (C *)S.brow, cert + p, counter + p, swapped + p, S.ipiv, S.flags, S.flags + 1, pk);
 }
 
 // Systems first..first+gridDim.x-1 end at step p.

@@ -16,6 +16,24 @@
 // (reference linalg/dense.py:114-155 via scipy.linalg.lu_factor).
 #pragma once
 #include "common.cuh"
+#include "tc_gemm.cuh"
+
+// Tensor-core operands of the trailing update written by the complex64 panel solve itself
+// (tile layout of tc_gemm.cuh): L21 as the A operand (real rows 2m, 2m+1 of trailing row
+// m, a_rows rows) and U12 as the B operand (row = trailing column, b_rows rows), both with
+// 2 NB real columns, split into TF32 hi and lo.  a_hi == nullptr: not wanted.
+struct PanelPack {
+    float *a_hi = nullptr, *a_lo = nullptr;
+    int a_rows = 0;
+    float *b_hi = nullptr, *b_lo = nullptr;
+    int b_rows = 0;
+};
+
+__device__ __forceinline__ void pack_pair(float *hi, float *lo, int64_t off, float x0, float x1) {
+    const float h0 = tf32_rna(x0), h1 = tf32_rna(x1);
+    *reinterpret_cast<float2 *>(hi + off) = make_float2(h0, h1);
+    *reinterpret_cast<float2 *>(lo + off) = make_float2(tf32_rna(x0 - h0), tf32_rna(x1 - h1));
+}
 
 #define NB 64
 #define RT_BM 64
@@ -419,7 +437,7 @@ __device__ void pivoted_panel(int n, C *A, int64_t lda, int j, int nbj, int *ipi
 template <typename C>
 __device__ __forceinline__ void panel_apply_cta(int n, C *A, int64_t lda, int j, int nbj, int nL, int b, int nblocks,
                                                 C *backup_col, C *backup_row, int *cert, int *counter, int *swapped,
-                                                int *ipiv, int *info, int *pivoted) {
+                                                int *ipiv, int *info, int *pivoted, PanelPack pk = PanelPack()) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C *T = reinterpret_cast<C *>(smem_raw);
     C *rd = T + NB * NBP;
@@ -453,6 +471,18 @@ __device__ __forceinline__ void panel_apply_cta(int n, C *A, int64_t lda, int j,
                 }
             }
         }
+        if constexpr (sizeof(C) == sizeof(float2)) {
+            if (pk.a_hi) {  // rows past the matrix are written as zero padding
+                const int m = NB * b + lane_vec;
+#pragma unroll
+                for (int i = 0; i < 16; ++i) {
+                    const int c = 4 * i + s;
+                    const float xr = ok ? (float)v[i].x : 0.f, xi = ok ? (float)v[i].y : 0.f;
+                    pack_pair(pk.a_hi, pk.a_lo, tc_tile_offset(2 * m, 2 * c, pk.a_rows), xr, -xi);
+                    pack_pair(pk.a_hi, pk.a_lo, tc_tile_offset(2 * m + 1, 2 * c, pk.a_rows), xi, xr);
+                }
+            }
+        }
     } else {
         const int col = j + nbj + NB * (b - nL) + lane_vec;
         const bool ok = col < n;
@@ -474,6 +504,17 @@ __device__ __forceinline__ void panel_apply_cta(int n, C *A, int64_t lda, int j,
                 if (r < nbj) A[(int64_t)col * lda + j + r] = v[i];
             }
         }
+        if constexpr (sizeof(C) == sizeof(float2)) {
+            if (pk.a_hi) {
+                const int nb_row = NB * (b - nL) + lane_vec;
+#pragma unroll
+                for (int i = 0; i < 16; ++i) {
+                    const int r = 4 * i + s;
+                    pack_pair(pk.b_hi, pk.b_lo, tc_tile_offset(nb_row, 2 * r, pk.b_rows), ok ? (float)v[i].x : 0.f,
+                              ok ? (float)v[i].y : 0.f);
+                }
+            }
+        }
     }
     if (__syncthreads_or(bad) && t == 0) atomicOr(cert, 1);
     // last CTA: pivoted fallback if any certificate failed
@@ -492,14 +533,27 @@ __device__ __forceinline__ void panel_apply_cta(int n, C *A, int64_t lda, int j,
     __syncthreads();
     pivoted_panel(n, A, lda, j, nbj, ipiv, info, swapped);
     if (t == 0) atomicAdd(pivoted, 1);
+    if constexpr (sizeof(C) == sizeof(float2)) {
+        if (pk.a_hi) {  // the refactored panel: pack both operands again (this CTA alone)
+            __syncthreads();
+            const int rest = n - j - nbj;
+            const float2 *Af = reinterpret_cast<const float2 *>(A);
+            for (int64_t e = t; e < (int64_t)pk.a_rows * (2 * NB / 4); e += 256)
+                tc_pack_a_chunk(e, rest, nbj, Af + (int64_t)j * lda + j + nbj, lda, pk.a_hi, pk.a_lo, pk.a_rows,
+                                pk.a_rows, 0, 2 * NB, 1.f);
+            for (int64_t e = t; e < (int64_t)pk.b_rows * (2 * NB / 4); e += 256)
+                tc_pack_b_chunk(e, nbj, rest, Af + (int64_t)(j + nbj) * lda + j, lda, pk.b_hi, pk.b_lo, pk.b_rows,
+                                2 * NB);
+        }
+    }
 }
 
 template <typename C>
 __global__ void __launch_bounds__(256)
 k_panel_apply(int n, C *A, int64_t lda, int j, int nbj, int nL, C *backup_col, C *backup_row, int *cert,
-              int *counter, int *swapped, int *ipiv, int *info, int *pivoted) {
+              int *counter, int *swapped, int *ipiv, int *info, int *pivoted, PanelPack pk) {
     panel_apply_cta<C>(n, A, lda, j, nbj, nL, blockIdx.x, gridDim.x, backup_col, backup_row, cert, counter, swapped,
-                       ipiv, info, pivoted);
+                       ipiv, info, pivoted, pk);
 }
 
 // Single-CTA fallback driver when there is no trailing strip (last panel).
