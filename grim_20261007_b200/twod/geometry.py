@@ -17,7 +17,9 @@ outside this path and are rejected with ``NotImplementedError``.
 """
 from __future__ import annotations
 
+import itertools
 import math
+import operator
 
 import numpy as np
 
@@ -61,6 +63,9 @@ def panel_count(n_prop, length, wavelength):
     return max(1, int(math.ceil(length * per / wavelength)))
 
 
+_PAIR_XY = operator.itemgetter('x1', 'y1', 'x2', 'y2')
+
+
 def contours_from_snapshot(snapshot, geometry_units='inches', wavelength=None, max_panels=20000):
     """Return a list of closed polygons (vertex arrays, metres) ready for ``panel_geometry``."""
     scale = unit_scale(geometry_units)
@@ -79,8 +84,8 @@ def contours_from_snapshot(snapshot, geometry_units='inches', wavelength=None, m
         pairs = seg.get('point_pairs', []) or []
         if not pairs:
             continue
-        xy = np.array([(float(p['x1']), float(p['y1']), float(p['x2']), float(p['y2'])) for p in pairs],
-                      dtype=np.float64) * scale
+        xy = np.fromiter(itertools.chain.from_iterable(map(_PAIR_XY, pairs)), np.float64,
+                         4 * len(pairs)).reshape(-1, 4) * scale
         a, b = xy[:, :2], xy[:, 2:]
         lengths = np.hypot(b[:, 0] - a[:, 0], b[:, 1] - a[:, 1])
         if n_prop > 0:
