@@ -1400,15 +1400,26 @@ struct GrpPlan {
     int bn = 128;  // output-tile width of the complex64 trailing update
 };
 
-// Output-tile width of the grouped complex64 trailing update: 128 (one CTA per SM, three
-// stages) or 64 (two stages, two CTAs per SM so that one CTA's epilogue overlaps the other's
-// loads).  GRIM_GROUPED_BN selects it; the packed operands are padded for either.
+// Output-tile width of the grouped complex64 trailing update (C staged in shared memory in
+// both): 128 (two pipeline stages, one CTA per SM) or 64 (one stage, 81 KB, two CTAs per SM so
+// that one CTA's loads and epilogue overlap the other's).  GRIM_GROUPED_BN selects it; the
+// packed operands are padded for either.
 static int grp_bn() {
     static int bn = [] {
         const char *e = getenv("GRIM_GROUPED_BN");
         return (e && atoi(e) == 64) ? 64 : 128;
     }();
     return bn;
+}
+
+// The complex64 trailing update runs as the persistent kernel (one CTA per SM walking the
+// step's tiles) unless GRIM_GROUPED_PERSIST=0 (one CTA per tile).
+static bool grp_persistent() {
+    static bool on = [] {
+        const char *e = getenv("GRIM_GROUPED_PERSIST");
+        return !(e && atoi(e) == 0);
+    }();
+    return on;
 }
 
 template <typename C>
@@ -1484,8 +1495,12 @@ static int grp_sequence(grim_context *h, const GrpPlan &P, const GrpSys *dsys, c
         if (u == 0) continue;
         if constexpr (sizeof(C) == sizeof(float2)) {
             // (the operands were packed by k_grp_apply)
-            if (P.bn == 64)
-                k_grp_tc_update<64, 3><<<P.tot[3 * p + 2], TC_THREADS, TcCfg<64, 3, true>::SMEM_BYTES, h->stream>>>(
+            if (grp_persistent() && P.bn == GRP_BN) {
+                const int tiles = P.tot[3 * p + 2];
+                k_grp_tc_update_p<GRP_BN><<<std::min(tiles, h->sm_count), GRP_P_THREADS, GrpPCfg<GRP_BN>::SMEM_BYTES,
+                                            h->stream>>>(dsys, p, dsched + P.off[3 * p + 2], u, tiles, err);
+            } else if (P.bn == 64)
+                k_grp_tc_update<64, 1><<<P.tot[3 * p + 2], TC_THREADS, TcCfg<64, 1, true>::SMEM_BYTES, h->stream>>>(
                     dsys, p, dsched + P.off[3 * p + 2], u, err);
             else
                 k_grp_tc_update<GRP_BN, GRP_STAGES><<<P.tot[3 * p + 2], TC_THREADS,
@@ -1519,8 +1534,10 @@ static int grp_getrf(grim_context *h, int count, const int *n, void *const *A, c
             GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_grp_tc_update<GRP_BN, GRP_STAGES>,
                                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                  TcCfg<GRP_BN, GRP_STAGES, true>::SMEM_BYTES));
-            GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_grp_tc_update<64, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 TcCfg<64, 3, true>::SMEM_BYTES));
+            GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_grp_tc_update_p<GRP_BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 GrpPCfg<GRP_BN>::SMEM_BYTES));
+            GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_grp_tc_update<64, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 TcCfg<64, 1, true>::SMEM_BYTES));
         }
         else
             GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_grp_dmma_update, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1584,7 +1601,8 @@ static int grp_getrf(grim_context *h, int count, const int *n, void *const *A, c
     const int *dsched = (const int *)psched;
     int *dout = (int *)pout;
     if (use_graph && !h->profiling) {
-        std::vector<int64_t> key = {(int64_t)sizeof(C), (int64_t)P.bn, (int64_t)count, (int64_t)(intptr_t)pws,
+        std::vector<int64_t> key = {(int64_t)sizeof(C), (int64_t)P.bn, (int64_t)grp_persistent(), (int64_t)count,
+                                    (int64_t)(intptr_t)pws,
                                     (int64_t)(intptr_t)pflags, (int64_t)(intptr_t)ptab, (int64_t)(intptr_t)psched,
                                     (int64_t)(intptr_t)pout, (int64_t)(intptr_t)err};
         for (int i = 0; i < count; ++i) key.push_back(n[P.order[i]]);

@@ -123,6 +123,226 @@ k_grp_tc_update(const GrpSys *__restrict__ sys, int p, const int *prefix, int co
                                   2 * S.lda, 2 * rest, rest, -1.f, 0, 0, err, (t % mt) * TC_BM, (t / mt) * BN);
 }
 
+// Persistent form of k_grp_tc_update: one CTA per SM walks the step's tiles (t = blockIdx.x,
+// blockIdx.x + gridDim.x, ...), so that one tile's epilogue overlaps the next tile's operand
+// loads and MMAs and the set-up (barriers, tensor memory) is paid once per SM.  192 threads:
+//   warp 0 (lane 0)  producer: bulk copies of the packed operands into a 2-stage ring;
+//   warp 1 (lane 0)  MMA issuer: 3 split-TF32 products per K-tile into one of two BN-column
+//                    accumulators (tile i uses accumulator i & 1), commit per stage and per tile;
+//   warps 2-5        epilogue: each thread owns one output row (TMEM lane quadrant = warp % 4),
+//                    copies its row of the C tile into shared memory (4-byte cp.async) while the
+//                    tile's MMAs run, then C = C + alpha D and releases the accumulator.
+// Every wait is bounded; on a timeout the CTA records the error flag, stops, waits (bounded) for
+// its copies and MMAs in flight, frees its tensor memory and returns.
+#define GRP_P_THREADS 192
+#define GRP_P_STAGES 2
+
+template <int BN>
+struct GrpPCfg {
+    static constexpr int A_BYTES = TC_BM * TC_BK * 4;
+    static constexpr int B_BYTES = BN * TC_BK * 4;
+    static constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
+    static constexpr int C_BYTES = TC_BM * BN * 4;
+    static constexpr int SMEM_BYTES = GRP_P_STAGES * STAGE_BYTES + C_BYTES + 1024;
+    static_assert(SMEM_BYTES <= 227 * 1024, "shared memory per CTA");
+};
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ void cp_async4(uint32_t dst, const void *src, bool valid) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(dst), "l"(src), "r"(valid ? 4 : 0) : "memory");
+}
+
+// Tile t of step p: its system and the tile's origin (real rows m0, columns n0).
+struct GrpTile {
+    const GrpSys *S;
+    int rest, Mp, Np, m0, n0;
+};
+
+template <int BN>
+__device__ __forceinline__ GrpTile grp_tile(const GrpSys *__restrict__ sys, int p, const int *prefix, int count,
+                                            int t) {
+    GrpTile g;
+    const int s = grp_find(prefix, count, t);
+    g.S = &sys[s];
+    g.rest = g.S->n - NB * p - NB;
+    g.Mp = grp_rows_a(g.rest);
+    g.Np = grp_rows_b(g.rest);
+    const int mt = g.Mp / TC_BM, local = t - __ldg(prefix + s);
+    g.m0 = (local % mt) * TC_BM;
+    g.n0 = (local / mt) * BN;
+    return g;
+}
+
+template <int BN>
+__global__ void __launch_bounds__(GRP_P_THREADS, 1)
+k_grp_tc_update_p(const GrpSys *__restrict__ sys, int p, const int *prefix, int count, int ntiles, int *err) {
+    using Cfg = GrpPCfg<BN>;
+    constexpr int NK = GRP_KP / TC_BK;
+    extern __shared__ __align__(1024) unsigned char smem_dyn[];
+    __shared__ __align__(8) uint64_t full[GRP_P_STAGES], empty[GRP_P_STAGES], tfull[2], tempty[2], done;
+    __shared__ uint32_t tmem_slot;
+    __shared__ int s_fail;
+    const uint32_t base = (smem_addr(smem_dyn) + 1023u) & ~1023u;
+    const uint32_t sC = base + GRP_P_STAGES * Cfg::STAGE_BYTES;
+    float *sCf = reinterpret_cast<float *>(smem_dyn + (base - smem_addr(smem_dyn)) + GRP_P_STAGES * Cfg::STAGE_BYTES);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        s_fail = 0;
+        for (int i = 0; i < GRP_P_STAGES; ++i) {
+            mbar_init(smem_addr(&full[i]), 1);
+            mbar_init(smem_addr(&empty[i]), 1);
+        }
+        for (int i = 0; i < 2; ++i) {
+            mbar_init(smem_addr(&tfull[i]), 1);
+            mbar_init(smem_addr(&tempty[i]), 4);  // one arrival per epilogue warp
+        }
+        mbar_init(smem_addr(&done), 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&tmem_slot)),
+                     "r"(2 * BN)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tmem_slot;
+    volatile int *vfail = &s_fail;
+    const int j = NB * p;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            int g = 0, issued = 0;
+            for (int t = blockIdx.x; t < ntiles && !*vfail; t += gridDim.x) {
+                const GrpTile tl = grp_tile<BN>(sys, p, prefix, count, t);
+                for (int kt = 0; kt < NK; ++kt, ++g) {
+                    const int st = g % GRP_P_STAGES;
+                    if (g >= GRP_P_STAGES &&
+                        !mbar_wait(smem_addr(&empty[st]), ((g / GRP_P_STAGES) + 1) & 1)) {
+                        *vfail = 1;
+                        break;
+                    }
+                    const uint32_t sA = base + st * Cfg::STAGE_BYTES, sAl = sA + Cfg::A_BYTES,
+                                   sB = sAl + Cfg::A_BYTES, sBl = sB + Cfg::B_BYTES;
+                    const uint32_t fb = smem_addr(&full[st]);
+                    mbar_expect_tx(fb, Cfg::STAGE_BYTES);
+                    const int64_t aoff = (int64_t)kt * tl.Mp * 32 + (int64_t)tl.m0 * 32;
+                    const int64_t boff = (int64_t)kt * tl.Np * 32 + (int64_t)tl.n0 * 32;
+                    bulk_g2s(sA, tl.S->pa_hi + aoff, Cfg::A_BYTES, fb);
+                    bulk_g2s(sAl, tl.S->pa_lo + aoff, Cfg::A_BYTES, fb);
+                    bulk_g2s(sB, tl.S->pb_hi + boff, Cfg::B_BYTES, fb);
+                    bulk_g2s(sBl, tl.S->pb_lo + boff, Cfg::B_BYTES, fb);
+                    issued = g + 1;
+                }
+            }
+            if (*vfail) {  // copies issued but not consumed must land before the CTA exits
+                for (int q = (issued > GRP_P_STAGES ? issued - GRP_P_STAGES : 0); q < issued; ++q)
+                    mbar_wait(smem_addr(&full[q % GRP_P_STAGES]), (q / GRP_P_STAGES) & 1);
+            }
+        }
+        __syncwarp();
+    } else if (warp == 1) {
+        if (lane == 0) {
+            const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(BN >> 3) << 17) |
+                                   ((uint32_t)(TC_BM >> 4) << 24);
+            int g = 0, i = 0;
+            for (int t = blockIdx.x; t < ntiles && !*vfail; t += gridDim.x, ++i) {
+                const int acc = i & 1;
+                if (i >= 2 && !mbar_wait(smem_addr(&tempty[acc]), ((i / 2) + 1) & 1)) {
+                    *vfail = 1;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t d = tmem + (uint32_t)(acc * BN);
+                bool ok = true;
+                for (int kt = 0; kt < NK; ++kt, ++g) {
+                    const int st = g % GRP_P_STAGES;
+                    if (!mbar_wait(smem_addr(&full[st]), (g / GRP_P_STAGES) & 1)) {
+                        ok = false;
+                        break;
+                    }
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    const uint32_t sA = base + st * Cfg::STAGE_BYTES, sAl = sA + Cfg::A_BYTES,
+                                   sB = sAl + Cfg::A_BYTES, sBl = sB + Cfg::B_BYTES;
+                    umma_ktile_tf32(d, sA, sB, idesc, kt == 0);
+                    umma_ktile_tf32(d, sA, sBl, idesc, false);
+                    umma_ktile_tf32(d, sAl, sB, idesc, false);
+                    umma_commit(smem_addr(&empty[st]));
+                }
+                if (!ok) {
+                    *vfail = 1;
+                    break;
+                }
+                umma_commit(smem_addr(&tfull[acc]));
+            }
+            umma_commit(smem_addr(&done));  // arrives once every MMA issued above has completed
+        }
+        __syncwarp();
+    } else {
+        // epilogue warps 2-5: TMEM lane quadrant q = warp % 4 holds output rows 32 q .. 32 q + 31
+        const int q = warp & 3, row = 32 * q + lane;
+        const uint32_t sRow = sC + 4 * row;
+        int i = 0;
+        for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++i) {
+            if (*vfail) break;
+            const GrpTile tl = grp_tile<BN>(sys, p, prefix, count, t);
+            float *C = (float *)tl.S->A + 2 * ((int64_t)(j + NB) * tl.S->lda + j + NB);
+            const int64_t ldc = 2 * tl.S->lda;
+            const int Mvalid = 2 * tl.rest, Nvalid = tl.rest, m = tl.m0 + row;
+            const bool row_ok = m < Mvalid;
+            for (int c = 0; c < BN; ++c) {  // this thread's row of C (only it reads it back)
+                const bool ok = row_ok && tl.n0 + c < Nvalid;
+                cp_async4(sRow + c * (TC_BM * 4), ok ? (const void *)(C + (int64_t)(tl.n0 + c) * ldc + m)
+                                                     : (const void *)C,
+                          ok);
+            }
+            asm volatile("cp.async.commit_group;\n\tcp.async.wait_all;" ::: "memory");
+            const int acc = i & 1;
+            if (!mbar_wait(smem_addr(&tfull[acc]), (i / 2) & 1)) {
+                *vfail = 1;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll 1
+            for (int c = 0; c < BN; c += 16) {
+                uint32_t v[16];
+                asm volatile(
+                    "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
+                    "%13, %14, %15}, [%16];"
+                    : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                      "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
+                      "=r"(v[15])
+                    : "r"(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(acc * BN + c)));
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                if (row_ok) {
+#pragma unroll
+                    for (int jj = 0; jj < 16; ++jj) {
+                        const int n = tl.n0 + c + jj;
+                        if (n < Nvalid)
+                            C[(int64_t)n * ldc + m] = sCf[(c + jj) * TC_BM + row] - __uint_as_float(v[jj]);
+                    }
+                }
+            }
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) mbar_arrive(smem_addr(&tempty[acc]));
+        }
+    }
+    // every MMA has completed before the tensor memory is released (bounded)
+    if (!mbar_wait(smem_addr(&done), 0)) *vfail = 1;
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (*vfail && threadIdx.x == 0) atomicOr(err, 1);
+    if (warp == 0) {
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * BN) : "memory");
+    }
+}
+
 // A22 -= L21 U12 for every updating complex128 system: ceil(rest / 64)^2 tiles each.
 __global__ void __launch_bounds__(DM_THREADS)
 k_grp_dmma_update(const GrpSys *__restrict__ sys, int p, const int *prefix, int count) {
