@@ -559,9 +559,18 @@ def main():
     h2d = 2 * (geom.nbytes + len(ang) * 8) + geom.shape[0] * 8
     d2h = 2 * len(ang) * 16
 
+    def settle():
+        # each leg starts from the same allocator state: cached blocks of the previous leg
+        # (the serving engine's factor cache, N up to 8192) are returned to the device
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+
     serving = run_serving(args) if (args.serving and rank == 0 and world == 1) else None
+    settle()
     bor = run_bor(args) if (args.bor and rank == 0 and world == 1) else None
+    settle()
     sweep = run_sweep(args, rank, world) if args.sweep else None
+    settle()
     farblk = run_far_block(args) if (args.far_block and rank == 0 and world == 1) else None
 
     # per-kernel profile of one mixed step, polarisations in turn (CUDA events after every

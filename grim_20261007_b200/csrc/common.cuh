@@ -200,8 +200,13 @@ struct StreamTimer {
         cudaEventRecord(a, s);
     }
     double stop_ms() {
+        record();
+        return elapsed_ms();
+    }
+    // record the end without waiting; elapsed_ms() reads the interval later
+    void record() { cudaEventRecord(b, s); }
+    double elapsed_ms() {
         float ms = 0.f;
-        cudaEventRecord(b, s);
         cudaEventSynchronize(b);
         cudaEventElapsedTime(&ms, a, b);
         return (double)ms;

@@ -598,8 +598,11 @@ static int trailing_update(grim_context *h, int rest, int nbj, const C *L21, con
 // update of panel p is still running; panel p+1's solve waits for that update (its U12
 // reads the updated columns).  With per-launch profiling on, everything runs on the
 // handle's stream in order.
+// defer: return without reading the info / pivoted-panel flags on the host (no host
+// synchronisation: the caller queues its solves behind the factorization and reads them
+// later with getrf_read_flags); *info_host is then 0.
 template <typename C>
-static int getrf_impl(grim_context *h, int n, C *A, int64_t lda, int *ipiv, int *info_host) {
+static int getrf_impl(grim_context *h, int n, C *A, int64_t lda, int *ipiv, int *info_host, bool defer = false) {
     if (!h || n <= 0 || !A || lda < n || !ipiv) return grim_fail(GRIM_ERR_ARGUMENT, "getrf: bad arguments");
     DeviceGuard g(h->device);
     GRIM_TRY(smem_opt_in<C>());
@@ -686,6 +689,10 @@ static int getrf_impl(grim_context *h, int n, C *A, int64_t lda, int *ipiv, int 
         h->stream = caller;
     }
     GRIM_TRY(status);
+    if (defer) {
+        if (info_host) *info_host = 0;
+        return GRIM_OK;
+    }
     int hostf[2] = {0, 0};
     GRIM_CHECK_CUDA(cudaMemcpyAsync(hostf, flags, 2 * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
     GRIM_CHECK_CUDA(cudaStreamSynchronize(h->stream));
@@ -693,6 +700,18 @@ static int getrf_impl(grim_context *h, int n, C *A, int64_t lda, int *ipiv, int 
     if (info_host) *info_host = hostf[0];
     h->last.pivoted_panels = hostf[1];
     h->last.info = hostf[0];
+    return GRIM_OK;
+}
+
+// The info and pivoted-panel counts of the last deferred getrf_impl on this handle.
+static int getrf_read_flags(grim_context *h, int *info, int *pivoted) {
+    void *p_flags = nullptr;
+    GRIM_TRY(grim_workspace(h, "lu_flags", 2 * sizeof(int), &p_flags));
+    int hostf[2] = {0, 0};
+    GRIM_CHECK_CUDA(cudaMemcpyAsync(hostf, p_flags, 2 * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    GRIM_CHECK_CUDA(cudaStreamSynchronize(h->stream));
+    *info = hostf[0];
+    *pivoted = hostf[1];
     return GRIM_OK;
 }
 
@@ -1328,16 +1347,11 @@ extern "C" int grim_zgesv_mixed(grim_handle_t h, int n, int nrhs, const void *A,
             k_convert<float2, double2><<<eg, 256, 0, h->stream>>>(n, n, (const double2 *)A, lda, lu, n);
             GRIM_CHECK_LAUNCH(h, "k_convert");
         }
+        // the factorization's flags are read after the refinement's first host synchronisation,
+        // so that the solves are queued while the factorization still runs
         StreamTimer tf(h->stream);
-        GRIM_TRY(getrf_impl<float2>(h, n, lu, n, ipiv, &linfo));
-        st.ms_factor = tf.stop_ms();
-        st.pivoted_panels = h->last.pivoted_panels;
-        if (linfo > 0) {
-            st.info = linfo;
-            h->last = st;
-            if (info) *info = linfo;
-            return grim_fail(GRIM_ERR_SINGULAR, "grim_zgesv_mixed: complex64 factor is exactly singular");
-        }
+        GRIM_TRY(getrf_impl<float2>(h, n, lu, n, ipiv, &linfo, true));
+        tf.record();
         StreamTimer ts(h->stream);
         int s;
         const bool berr_test = precision_mode == GRIM_PREC_MIXED_BERR;
@@ -1348,6 +1362,16 @@ extern "C" int grim_zgesv_mixed(grim_handle_t h, int n, int nrhs, const void *A,
             s = mixed_refine<float2>(h, n, nrhs, (const float2 *)A32, lda32, lu, ipiv, (double2 *)B, ldb, tol, max_iter,
                                      &st, berr_test);
         st.ms_solve = ts.stop_ms();
+        st.ms_factor = tf.elapsed_ms();
+        int piv = 0;
+        GRIM_TRY(getrf_read_flags(h, &linfo, &piv));
+        st.pivoted_panels = piv;
+        if (linfo > 0) {
+            st.info = linfo;
+            h->last = st;
+            if (info) *info = linfo;
+            return grim_fail(GRIM_ERR_SINGULAR, "grim_zgesv_mixed: complex64 factor is exactly singular");
+        }
         h->last = st;
         if (stats) *stats = st;
         if (info) *info = 0;
