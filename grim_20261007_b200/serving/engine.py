@@ -159,11 +159,19 @@ class ServingEngine:
         return fut
 
     def close(self):
+        """Stop the slot threads, drop the factor cache and return the slots' device
+        workspaces (the engine's memory goes back to the caller)."""
         with self.cv:
             self.closed = True
             self.cv.notify_all()
         for t in self.threads:
             t.join()
+        with self.cache.lock:
+            self.cache.items.clear()
+            self.cache.used = 0
+        for slot in self.slots:
+            slot.stream.synchronize()
+            slot.ctx.lib.grim_release_workspace(slot.ctx.h)
 
     def stats(self):
         with self.cv:
