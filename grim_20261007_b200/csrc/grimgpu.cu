@@ -1519,10 +1519,13 @@ static int grp_sequence(grim_context *h, const GrpPlan &P, const GrpSys *dsys, c
         if (u == 0) continue;
         if constexpr (sizeof(C) == sizeof(float2)) {
             // (the operands were packed by k_grp_apply)
+            const int tiles = P.tot[3 * p + 2];
             if (grp_persistent() && P.bn == GRP_BN) {
-                const int tiles = P.tot[3 * p + 2];
                 k_grp_tc_update_p<GRP_BN><<<std::min(tiles, h->sm_count), GRP_P_THREADS, GrpPCfg<GRP_BN>::SMEM_BYTES,
                                             h->stream>>>(dsys, p, dsched + P.off[3 * p + 2], u, tiles, err);
+            } else if (grp_persistent()) {
+                k_grp_tc_update_p<64><<<std::min(tiles, h->sm_count), GRP_P_THREADS, GrpPCfg<64>::SMEM_BYTES,
+                                        h->stream>>>(dsys, p, dsched + P.off[3 * p + 2], u, tiles, err);
             } else if (P.bn == 64)
                 k_grp_tc_update<64, 1><<<P.tot[3 * p + 2], TC_THREADS, TcCfg<64, 1, true>::SMEM_BYTES, h->stream>>>(
                     dsys, p, dsched + P.off[3 * p + 2], u, err);
@@ -1560,6 +1563,8 @@ static int grp_getrf(grim_context *h, int count, const int *n, void *const *A, c
                                                  TcCfg<GRP_BN, GRP_STAGES, true>::SMEM_BYTES));
             GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_grp_tc_update_p<GRP_BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                  GrpPCfg<GRP_BN>::SMEM_BYTES));
+            GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_grp_tc_update_p<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 GrpPCfg<64>::SMEM_BYTES));
             GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_grp_tc_update<64, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                  TcCfg<64, 1, true>::SMEM_BYTES));
         }

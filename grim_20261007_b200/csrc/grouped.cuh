@@ -135,15 +135,16 @@ k_grp_tc_update(const GrpSys *__restrict__ sys, int p, const int *prefix, int co
 // Every wait is bounded; on a timeout the CTA records the error flag, stops, waits (bounded) for
 // its copies and MMAs in flight, frees its tensor memory and returns.
 #define GRP_P_THREADS 192
-#define GRP_P_STAGES 2
 
+// BN 128: 2 stages of 64 KB + a 64 KB C tile; BN 64: 4 stages of 48 KB + a 32 KB C tile.
 template <int BN>
 struct GrpPCfg {
+    static constexpr int STAGES = BN == 128 ? 2 : 4;
     static constexpr int A_BYTES = TC_BM * TC_BK * 4;
     static constexpr int B_BYTES = BN * TC_BK * 4;
     static constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
     static constexpr int C_BYTES = TC_BM * BN * 4;
-    static constexpr int SMEM_BYTES = GRP_P_STAGES * STAGE_BYTES + C_BYTES + 1024;
+    static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + C_BYTES + 1024;
     static_assert(SMEM_BYTES <= 227 * 1024, "shared memory per CTA");
 };
 
@@ -182,16 +183,16 @@ k_grp_tc_update_p(const GrpSys *__restrict__ sys, int p, const int *prefix, int 
     using Cfg = GrpPCfg<BN>;
     constexpr int NK = GRP_KP / TC_BK;
     extern __shared__ __align__(1024) unsigned char smem_dyn[];
-    __shared__ __align__(8) uint64_t full[GRP_P_STAGES], empty[GRP_P_STAGES], tfull[2], tempty[2], done;
+    __shared__ __align__(8) uint64_t full[Cfg::STAGES], empty[Cfg::STAGES], tfull[2], tempty[2], done;
     __shared__ uint32_t tmem_slot;
     __shared__ int s_fail;
     const uint32_t base = (smem_addr(smem_dyn) + 1023u) & ~1023u;
-    const uint32_t sC = base + GRP_P_STAGES * Cfg::STAGE_BYTES;
-    float *sCf = reinterpret_cast<float *>(smem_dyn + (base - smem_addr(smem_dyn)) + GRP_P_STAGES * Cfg::STAGE_BYTES);
+    const uint32_t sC = base + Cfg::STAGES * Cfg::STAGE_BYTES;
+    float *sCf = reinterpret_cast<float *>(smem_dyn + (base - smem_addr(smem_dyn)) + Cfg::STAGES * Cfg::STAGE_BYTES);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (threadIdx.x == 0) {
         s_fail = 0;
-        for (int i = 0; i < GRP_P_STAGES; ++i) {
+        for (int i = 0; i < Cfg::STAGES; ++i) {
             mbar_init(smem_addr(&full[i]), 1);
             mbar_init(smem_addr(&empty[i]), 1);
         }
@@ -221,9 +222,9 @@ k_grp_tc_update_p(const GrpSys *__restrict__ sys, int p, const int *prefix, int 
             for (int t = blockIdx.x; t < ntiles && !*vfail; t += gridDim.x) {
                 const GrpTile tl = grp_tile<BN>(sys, p, prefix, count, t);
                 for (int kt = 0; kt < NK; ++kt, ++g) {
-                    const int st = g % GRP_P_STAGES;
-                    if (g >= GRP_P_STAGES &&
-                        !mbar_wait(smem_addr(&empty[st]), ((g / GRP_P_STAGES) + 1) & 1)) {
+                    const int st = g % Cfg::STAGES;
+                    if (g >= Cfg::STAGES &&
+                        !mbar_wait(smem_addr(&empty[st]), ((g / Cfg::STAGES) + 1) & 1)) {
                         *vfail = 1;
                         break;
                     }
@@ -241,8 +242,8 @@ k_grp_tc_update_p(const GrpSys *__restrict__ sys, int p, const int *prefix, int 
                 }
             }
             if (*vfail) {  // copies issued but not consumed must land before the CTA exits
-                for (int q = (issued > GRP_P_STAGES ? issued - GRP_P_STAGES : 0); q < issued; ++q)
-                    mbar_wait(smem_addr(&full[q % GRP_P_STAGES]), (q / GRP_P_STAGES) & 1);
+                for (int q = (issued > Cfg::STAGES ? issued - Cfg::STAGES : 0); q < issued; ++q)
+                    mbar_wait(smem_addr(&full[q % Cfg::STAGES]), (q / Cfg::STAGES) & 1);
             }
         }
         __syncwarp();
@@ -261,8 +262,8 @@ k_grp_tc_update_p(const GrpSys *__restrict__ sys, int p, const int *prefix, int 
                 const uint32_t d = tmem + (uint32_t)(acc * BN);
                 bool ok = true;
                 for (int kt = 0; kt < NK; ++kt, ++g) {
-                    const int st = g % GRP_P_STAGES;
-                    if (!mbar_wait(smem_addr(&full[st]), (g / GRP_P_STAGES) & 1)) {
+                    const int st = g % Cfg::STAGES;
+                    if (!mbar_wait(smem_addr(&full[st]), (g / Cfg::STAGES) & 1)) {
                         ok = false;
                         break;
                     }
