@@ -30,6 +30,7 @@ struct FarTable {
     int intervals, degree;
     const double *bounds, *coeff;
     double k_re, k_im;
+    int coeff16;  // coeff is 16-byte aligned: (re, im) pairs are read as one 16-byte load
 };
 
 __device__ __forceinline__ double far_mul(double a, double b) { return __dmul_rn(a, b); }
@@ -117,23 +118,23 @@ __device__ __forceinline__ bool far_kernel(const FarTable &t, double r, double *
     const double b0 = bounds[lo], b1 = bounds[lo + 1];
     const double x = __ddiv_rn(far_sub(r, b0), far_sub(b1, b0));
     const double *base = t.coeff + (int64_t)lo * (t.degree + 1) * 4;
-    if (t.degree == FAR_DEGREE) {
-        // the usual degree: all coefficient loads issued ahead of the two Horner chains
-        double cf[4 * (FAR_DEGREE + 1)];
+    if (t.degree == FAR_DEGREE && t.coeff16) {
+        // the usual degree: both channels' Horner chains interleaved, (re, im) pairs read
+        // as 16-byte loads that the unrolled loop can issue ahead of their use
+        const double2 *b2 = reinterpret_cast<const double2 *>(base);
+        double2 g = __ldg(b2 + 2 * FAR_DEGREE), d = __ldg(b2 + 2 * FAR_DEGREE + 1);
 #pragma unroll
-        for (int e = 0; e < 4 * (FAR_DEGREE + 1); ++e) cf[e] = __ldg(base + e);
-#pragma unroll
-        for (int c = 0; c < 2; ++c) {
-            const int off = 2 * c;
-            double re = cf[4 * FAR_DEGREE + off], im = cf[4 * FAR_DEGREE + off + 1];
-#pragma unroll
-            for (int j = FAR_DEGREE - 1; j >= 0; --j) {
-                re = far_add(far_mul(re, x), cf[4 * j + off]);
-                im = far_add(far_mul(im, x), cf[4 * j + off + 1]);
-            }
-            out[2 * c] = re;
-            out[2 * c + 1] = im;
+        for (int j = FAR_DEGREE - 1; j >= 0; --j) {
+            const double2 cg = __ldg(b2 + 2 * j), cd = __ldg(b2 + 2 * j + 1);
+            g.x = far_add(far_mul(g.x, x), cg.x);
+            g.y = far_add(far_mul(g.y, x), cg.y);
+            d.x = far_add(far_mul(d.x, x), cd.x);
+            d.y = far_add(far_mul(d.y, x), cd.y);
         }
+        out[0] = g.x;
+        out[1] = g.y;
+        out[2] = d.x;
+        out[3] = d.y;
         return true;
     }
     for (int c = 0; c < 2; ++c) {

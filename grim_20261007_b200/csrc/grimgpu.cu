@@ -1749,7 +1749,7 @@ extern "C" int grim_far_block(grim_handle_t h, int64_t mb, int64_t nb, int q, in
     GRIM_TRY(grim_workspace(h, "far_status", sizeof(int), &pst));
     int *status = (int *)pst;
     GRIM_CHECK_CUDA(cudaMemsetAsync(status, 0, sizeof(int), h->stream));
-    const FarTable t{intervals, degree, bounds, coeff, k_re, k_im};
+    const FarTable t{intervals, degree, bounds, coeff, k_re, k_im, ((uintptr_t)coeff & 15) == 0};
     const int64_t pairs = mb * nb;
     const int threads = 128;
     const int64_t blocks = (pairs + threads - 1) / threads;
@@ -1762,7 +1762,7 @@ extern "C" int grim_far_block(grim_handle_t h, int64_t mb, int64_t nb, int q, in
     if (!attr) {
         const int mx = FAR_SMEM_BOUNDS * (int)sizeof(double);
         GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_far_block<0, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-        GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_far_block<2, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+        GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_far_block<2, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
         GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_far_block<3, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
         GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_far_block<4, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
         attr = true;
@@ -1772,7 +1772,7 @@ extern "C" int grim_far_block(grim_handle_t h, int64_t mb, int64_t nb, int q, in
                                                                 obs_norm, src_norm, far, obs_normal_deriv,       \
                                                                 want_s, want_k, mirrored, t, acc_s, acc_k,       \
                                                                 acc_kt, status)
-    if (width == 2) FAR_LAUNCH(2, 3);
+    if (width == 2) FAR_LAUNCH(2, 4);
     else if (width == 3) FAR_LAUNCH(3, 2);
     else if (width == 4) FAR_LAUNCH(4, 1);
     else FAR_LAUNCH(0, 1);
@@ -1815,7 +1815,8 @@ extern "C" int ghost_far_block(int64_t mb, int64_t nb, int q, int width, const d
     GRIM_TRY(grim_workspace(h, "far_io", bytes, &pw));
     double *d = (double *)pw;
     double *d_op = d, *d_sp = d_op + pts_o, *d_qw = d_sp + pts_s, *d_phi = d_qw + q, *d_on = d_phi + (size_t)q * width,
-           *d_sn = d_on + 2 * mb, *d_b = d_sn + 2 * nb, *d_c = d_b + (intervals + 1);
+           *d_sn = d_on + 2 * mb, *d_b = d_sn + 2 * nb;
+    double *d_c = (double *)(((uintptr_t)(d_b + (intervals + 1)) + 15) & ~(uintptr_t)15);  // 16-byte aligned
     double *d_as = (double *)(((uintptr_t)(d_c + tab_c) + 255) & ~(uintptr_t)255);
     double *d_ak = (double *)((char *)d_as + acc_bytes), *d_akt = (double *)((char *)d_ak + acc_bytes);
     uint8_t *d_far = (uint8_t *)((char *)d_akt + acc_bytes);
