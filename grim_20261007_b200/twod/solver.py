@@ -31,6 +31,7 @@ import torch
 from .. import _lib
 from ..device import context, ptr, require_cuda, run_pool
 from ..execution import requested_dense_backend, requested_precision
+from . import certify
 from . import geometry as geo
 from . import operators as ops
 
@@ -324,12 +325,13 @@ def _solve_frequency(meshes, f, elevs, pol, precision, abort_event):
     return _frequency_record(f, elevs, pol, precision, k, body, res, t0)
 
 
-def _solve_frequencies_grouped(meshes, keys, elevs, precision, abort_event, workers):
-    """Every (polarisation, frequency) system of a sweep through one grouped factorization
-    (``operators.monostatic_solves_grouped``); returns the per-system outputs of
-    ``_solve_frequency`` in ``keys`` order."""
+def _solve_frequencies_grouped(items, elevs, precision, abort_event, workers):
+    """Every (mesh, polarisation, frequency) system of a request through one grouped
+    factorization (``operators.monostatic_solves_grouped``); returns the per-system outputs of
+    ``_solve_frequency`` in ``items`` order."""
     t0 = time.perf_counter()
-    built = run_pool([(lambda f=f, pol=pol: _frequency_body(meshes, f, pol, abort_event)) for pol, f in keys],
+    keys = [(pol, f) for _m, pol, f in items]
+    built = run_pool([(lambda m=m, f=f, pol=pol: _frequency_body(m, f, pol, abort_event)) for m, pol, f in items],
                      workers=workers)
     angles = np.asarray(elevs, dtype=np.float64)
     angles_dev = torch.as_tensor(angles, device=built[0][1].geom.device)
@@ -393,44 +395,66 @@ def _sweep(geometry_snapshot, frequencies_ghz, elevations_deg, pols, geometry_un
            cfie_alpha, compute_condition_number, max_panels, mesh_reference_ghz, abort_event):
     """Solve every (polarisation, frequency) system of a request on the device worker pool;
     returns {pol: reference-shaped channel result}."""
+    channels = _sweep_many([geometry_snapshot], frequencies_ghz, elevations_deg, pols, geometry_units,
+                           progress_callback, cfie_alpha, compute_condition_number, max_panels, mesh_reference_ghz,
+                           abort_event)[0]
+    for ch in channels.values():
+        ch.pop('_outs', None)
+    return channels
+
+
+def _sweep_many(snapshots, frequencies_ghz, elevations_deg, pols, geometry_units, progress_callback, cfie_alpha,
+                compute_condition_number, max_panels, mesh_reference_ghz, abort_event):
+    """Every (snapshot, polarisation, frequency) system of a request: one grouped
+    factorization of all of them when there is more than one frequency or snapshot (a
+    sweep, a certified base/refined pair), else the device worker pool.  Returns, per
+    snapshot, {pol: reference-shaped channel result} (with the per-system outputs under
+    ``'_outs'``)."""
     freqs, elevs = _validate_request(frequencies_ghz, elevations_deg, cfie_alpha, compute_condition_number)
     require_cuda()
     precision = requested_precision()
-    meshes = _MeshCache(geometry_snapshot, geometry_units, max_panels, mesh_reference_ghz)
-    jobs, keys, costs = [], [], []
-    for pol in pols:
-        for f in freqs:
-            jobs.append(lambda f=f, pol=pol: _solve_frequency(meshes, f, elevs, pol, precision, abort_event))
-            keys.append((pol, f))
-            costs.append(_frequency_cost(geometry_snapshot, geometry_units, f, len(elevs)) if len(freqs) > 1 else 1.0)
+    mesh_list = [_MeshCache(snap, geometry_units, max_panels, mesh_reference_ghz) for snap in snapshots]
+    items, jobs, costs = [], [], []
+    for si, meshes in enumerate(mesh_list):
+        for pol in pols:
+            for f in freqs:
+                items.append((si, pol, f))
+                jobs.append(lambda m=meshes, f=f, pol=pol: _solve_frequency(m, f, elevs, pol, precision, abort_event))
+                costs.append(_frequency_cost(snapshots[si], geometry_units, f, len(elevs)) if len(items) > 1 or
+                             len(freqs) > 1 else 1.0)
     total = len(jobs) * (len(elevs) + 1)
     progress_state = {'done': 0}
 
     def on_done(i, out):
         progress_state['done'] += len(elevs) + 1
         if progress_callback is not None:
-            pol, f = keys[i]
+            _si, pol, f = items[i]
             try:
                 progress_callback(progress_state['done'], total, f'{pol} solved {f:g} GHz')
             except Exception:  # noqa: BLE001 - progress reporting never fails a solve
                 pass
 
     t0 = time.perf_counter()
-    if len(freqs) > 1 and _grouped_sweeps():
-        # a sweep: every system through one grouped factorization (one CUDA graph)
-        outs = _solve_frequencies_grouped(meshes, keys, elevs, precision, abort_event, sweep_workers(len(jobs)))
+    if (len(freqs) > 1 or len(snapshots) > 1) and _grouped_sweeps():
+        # every system through one grouped factorization (one CUDA graph)
+        outs = _solve_frequencies_grouped([(mesh_list[si], pol, f) for si, pol, f in items], elevs, precision,
+                                          abort_event, sweep_workers(len(jobs)))
         for i, o in enumerate(outs):
             on_done(i, o)
     else:
         outs = run_pool(jobs, workers=sweep_workers(len(jobs)), costs=costs, on_done=on_done)
     wall = time.perf_counter() - t0
-    channels = {}
-    for pol in pols:
-        mine = [o for (p, _f), o in zip(keys, outs) if p == pol]
-        stage = {'operators': 0.0, 'linear_solve': sum(o['seconds'] for o in mine), 'far_field': 0.0,
-                 'wall': wall}
-        channels[pol] = _channel_result(pol, mine, precision, stage)
-    return channels
+    results = []
+    for si in range(len(snapshots)):
+        channels = {}
+        for pol in pols:
+            mine = [o for (sj, p, _f), o in zip(items, outs) if sj == si and p == pol]
+            stage = {'operators': 0.0, 'linear_solve': sum(o['seconds'] for o in mine), 'far_field': 0.0,
+                     'wall': wall}
+            channels[pol] = _channel_result(pol, mine, precision, stage)
+            channels[pol]['_outs'] = mine
+        results.append(channels)
+    return results
 
 
 def _grouped_sweeps():
@@ -501,6 +525,93 @@ def solve_monostatic_rcs_2d(geometry_snapshot, frequencies_ghz, elevations_deg, 
             samples.append(row)
     metadata = {'channels': {k: v['metadata'] for k, v in channels.items()},
                 'polarizations': [c[0] for c in _CO_POLARIZED_2D_CHANNELS]}
+    return {
+        'solver': '2d_bie_mom_rcs',
+        'scattering_mode': 'monostatic',
+        'amplitude_convention': RCS_AMPLITUDE_CONVENTION,
+        'amplitude_version': RCS_AMPLITUDE_VERSION,
+        'polarization': 'VV+HH',
+        'polarization_export': 'VV+HH',
+        'samples': samples,
+        'metadata': metadata,
+    }
+
+
+# ------------------------------------------------------------------ certified (base + refined mesh)
+def _certified_channels(geometry_snapshot, frequencies_ghz, elevations_deg, pols, geometry_units, progress_callback,
+                        mesh_convergence_policy, max_panels, mesh_reference_ghz, cfie_alpha, abort_event):
+    """Base and refined-mesh solves of every (polarisation, frequency) system in ONE grouped
+    factorization, then per polarisation and frequency the reference's certificate
+    (``twod/solver.py:3663-3880``): the refined result is published only where it agrees
+    with the base one within the policy, else ValueError."""
+    policy = certify.validate_policy(mesh_convergence_policy)
+    fine_snapshot = certify.scale_snapshot_panel_density(geometry_snapshot, policy['fine_factor'])
+    base, fine = _sweep_many([geometry_snapshot, fine_snapshot], frequencies_ghz, elevations_deg, pols,
+                             geometry_units, progress_callback, cfie_alpha, False, max_panels, mesh_reference_ghz,
+                             abort_event)
+    out = {}
+    for pol in pols:
+        b, f = base[pol], fine[pol]
+        b_outs, f_outs = b.pop('_outs'), f.pop('_outs')
+        gates = []
+        for bo, fo in zip(b_outs, f_outs):
+            res = certify.certify({'samples': bo['samples'], 'metadata': b['metadata']},
+                                  {'samples': fo['samples'], 'metadata': f['metadata']}, policy, bo['n'], fo['n'])
+            gates.append(res['metadata']['mesh_convergence'])
+        meta = dict(f['metadata'])
+        qg = dict(meta.get('quality_gate', {}))
+        qg.update(mesh_convergence_certified=True, certification_scope='discrete_linear_system_and_mesh_convergence')
+        meta.update(quality_gate=qg, mesh_convergence=gates[0] if len(gates) == 1 else gates,
+                    mesh_convergence_certified=True, certified_entry_point=True, published_mesh='fine',
+                    mesh_strategy_used='global',
+                    certification_phase_counters={'base': {'dense_factorization_count': len(b_outs)},
+                                                  'fine': {'dense_factorization_count': len(f_outs)}})
+        f['metadata'] = meta
+        out[pol] = f
+    return out
+
+
+def solve_monostatic_rcs_2d_certified_single_polarization(
+        geometry_snapshot, frequencies_ghz, elevations_deg, polarization, geometry_units="inches",
+        material_base_dir=None, progress_callback=None, quality_thresholds=None, mesh_convergence_policy=None,
+        max_panels=MAX_PANELS_DEFAULT, mesh_reference_ghz=None, rcs_normalization_mode="physical", cfie_alpha=0.0,
+        abort_event=None, solver_method="auto", _shared_discretization_caches=None):
+    """Single-polarisation solve with mesh certification (reference ``twod/solver.py:3885``):
+    the base mesh and the mesh refined by the policy's ``fine_factor`` are solved together
+    (one grouped factorization of all their systems) and the refined result is published
+    with its ``mesh_convergence`` report, or ValueError when the two disagree."""
+    pol = _canonical_user_polarization_label(polarization)
+    if pol not in ('TM', 'TE'):
+        raise ValueError(f'Unknown polarization {polarization!r}.')
+    return _certified_channels(geometry_snapshot, frequencies_ghz, elevations_deg, [pol], geometry_units,
+                               progress_callback, mesh_convergence_policy, max_panels, mesh_reference_ghz, cfie_alpha,
+                               abort_event)[pol]
+
+
+def solve_monostatic_rcs_2d_certified(geometry_snapshot, frequencies_ghz, elevations_deg, geometry_units="inches",
+                                      material_base_dir=None, progress_callback=None, quality_thresholds=None,
+                                      mesh_convergence_policy=None, max_panels=MAX_PANELS_DEFAULT,
+                                      mesh_reference_ghz=None, rcs_normalization_mode="physical", abort_event=None,
+                                      solver_method="auto"):
+    """The reference's canonical production monostatic entry (``twod/solver.py:3979``): both
+    co-polarised channels, each certified on a refined mesh; base and refined systems of
+    both channels and every frequency go through one grouped factorization.  Samples VV then
+    HH, as ``solve_monostatic_rcs_2d``."""
+    pols = [pol for _export, pol in _CO_POLARIZED_2D_CHANNELS]
+    by_pol = _certified_channels(geometry_snapshot, frequencies_ghz, elevations_deg, pols, geometry_units,
+                                 progress_callback, mesh_convergence_policy, max_panels, mesh_reference_ghz, 0.0,
+                                 abort_event)
+    channels = {export: by_pol[pol] for export, pol in _CO_POLARIZED_2D_CHANNELS}
+    samples = []
+    for export, _pol in _CO_POLARIZED_2D_CHANNELS:
+        for s_ in channels[export]['samples']:
+            row = dict(s_)
+            row['polarization'] = export
+            samples.append(row)
+    metadata = {'channels': {k: v['metadata'] for k, v in channels.items()},
+                'polarizations': [c[0] for c in _CO_POLARIZED_2D_CHANNELS],
+                'mesh_convergence_certified': True, 'certified_entry_point': True, 'published_mesh': 'fine',
+                'certification_solve_order': ['base_TE', 'base_TM', 'fine_TE', 'fine_TM']}
     return {
         'solver': '2d_bie_mom_rcs',
         'scattering_mode': 'monostatic',

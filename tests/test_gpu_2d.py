@@ -168,3 +168,34 @@ def test_frequency_sweep_pool_matches_single_frequency_solves(ctx, grouped, monk
     counts = swept['metadata']
     assert counts['dense_gpu_solve_count'] == len(freqs) and counts['panel_count_max'] > counts['panel_count_min']
     assert counts['dense_grouped_factorization_count'] == (len(freqs) if grouped == '1' else 0)
+
+
+def test_certified_entry_publishes_the_refined_mesh(ctx):
+    """The certified production entry solves the base and refined meshes of both channels in
+    one grouped factorization and publishes the refined result: equal to a plain solve of the
+    refined snapshot, with the reference-shaped certificate; limits it cannot meet raise."""
+    from grim_20261007_b200.twod import certify
+    from grim_20261007_b200.twod.solver import solve_monostatic_rcs_2d, solve_monostatic_rcs_2d_certified
+    th = -2.0 * np.pi * np.arange(200) / 200.0
+    v = np.stack([np.cos(th), np.sin(th)], -1)  # the 200-vertex circle of radius 1 m (clockwise)
+    snap = S.snapshot_from_polygons([v])
+    for sg in snap['segments']:
+        sg['properties'][1] = '-30'  # 30 panels per wavelength; refined: 45
+    ang = list(np.arange(0.0, 180.0, 4.0))
+    freqs = [0.55, 0.7]  # ka 11.5 and 14.7 (400 -> 600 and 600 -> 800 panels)
+    res = solve_monostatic_rcs_2d_certified(snap, freqs, ang, geometry_units='meters')
+    ref = solve_monostatic_rcs_2d(certify.scale_snapshot_panel_density(snap, 1.5), freqs, ang,
+                                  geometry_units='meters', strict_quality_gate=False)
+    a = np.array([complex(s['rcs_amp_real'], s['rcs_amp_imag']) for s in res['samples']])
+    b = np.array([complex(s['rcs_amp_real'], s['rcs_amp_imag']) for s in ref['samples']])
+    np.testing.assert_allclose(a, b, rtol=1e-12, atol=1e-12 * np.max(np.abs(b)))
+    for export in ('VV', 'HH'):
+        meta = res['metadata']['channels'][export]
+        assert meta['mesh_convergence_certified'] and meta['published_mesh'] == 'fine'
+        gates = meta['mesh_convergence']
+        assert len(gates) == 2 and all(gt['passed'] for gt in gates)
+        assert all(gt['fine_panel_count'] > gt['base_panel_count'] for gt in gates)
+        assert meta['dense_grouped_factorization_count'] == 2
+    with pytest.raises(ValueError, match='mesh convergence failed'):
+        solve_monostatic_rcs_2d_certified(snap, [0.55], ang, geometry_units='meters',
+                                          mesh_convergence_policy={'complex_max_limit': 1e-9})
