@@ -255,7 +255,7 @@ def _solve_modes_grouped(dev, modes, th, precision, tol, workers):
 
 
 def solve_bor_device(points, k, thetas_deg, mmax, precision='double', tol=None, ctx=None, workers=None,
-                     signed_mode_symmetry=True, grouped=True):
+                     signed_mode_symmetry=True, grouped=True, mode_tol=None, tail_start=0):
     """Device path: returns (F[2 nth] complex128 on the host, telemetry).
 
     The modal moments are built once; the per-mode systems are independent and run on the
@@ -267,7 +267,10 @@ def solve_bor_device(points, k, thetas_deg, mmax, precision='double', tol=None, 
     contributions are identical (equal to the last bit in the oracle, for the sphere and
     the ogive).  With an explicit ``ctx`` (a serving slot) the modes run in turn on that
     handle.  With ``grouped`` (default) the mode systems are factored together by one
-    grouped LU (``grouped.py``); otherwise each mode is factored on its own worker.
+    grouped LU (``grouped.py``); otherwise each mode is factored on its own worker.  With
+    ``mode_tol`` the modal sum stops at the reference's adaptive tail (two consecutive
+    modes at or above ``tail_start`` below the tolerance; ``_adaptive_tail``); all modes up
+    to ``mmax`` are solved together first, so the truncation decides only the sum.
     """
     from ..twod.solver import sweep_workers
     import time
@@ -288,7 +291,13 @@ def solve_bor_device(points, k, thetas_deg, mmax, precision='double', tol=None, 
         jobs = [(lambda m=m: _solve_mode(dev, m, th, precision, tol)) for m in modes]
         outs = run_pool(jobs, workers=sweep_workers(len(jobs)) if workers is None else workers)
     amp = torch.zeros(2 * int(th.numel()), dtype=torch.complex128, device='cuda')
+    modes_used, tail = mmax, None
+    if mode_tol is not None and signed_mode_symmetry:
+        modes_used, tail = _adaptive_tail([(2.0 if m > 0 else 1.0) * part for m, (part, _t) in zip(modes, outs)],
+                                          float(mode_tol), int(tail_start))
     for m, (part, _t) in zip(modes, outs):
+        if signed_mode_symmetry and abs(m) > modes_used:
+            continue
         if signed_mode_symmetry and m > 0:
             amp += 2.0 * part
         else:
@@ -301,7 +310,32 @@ def solve_bor_device(points, k, thetas_deg, mmax, precision='double', tol=None, 
     tele['stage_seconds'] = dict(modal_moments=t_moments, **(outs[0][1].get('stage_seconds') or {}))
     F = amp.cpu().numpy() * (-1j * k * ETA0 / (4.0 * np.pi))
     tele['n_unknowns'] = 2 * (dev.ne + 1)
+    tele['modes_used'] = int(modes_used)
+    if tail is not None:
+        tele.update(tail)
     return F, tele
+
+
+def _adaptive_tail(contributions, mode_tol, tail_start):
+    """The reference's modal convergence rule (``bor/solver.py:3130-3190``): accumulate the
+    |m| = 0, 1, ... contributions in order; after each, the worst relative increment over
+    the samples is |dF| / (|F| + mode_tol max|F|); stop once two consecutive modes at or
+    above ``tail_start`` stay below ``mode_tol``.  Returns (last mode used, report)."""
+    F = None
+    quiet, used, rel = 0, 0, 0.0
+    for am, dF in enumerate(contributions):
+        d = dF.cpu().numpy()
+        F = d.copy() if F is None else F + d
+        fa, da = np.abs(F), np.abs(d)
+        scale = max(float(np.max(fa)), 1e-300)
+        eff = fa + mode_tol * scale
+        rel = float(np.max(np.divide(da, eff, out=np.zeros_like(da), where=eff > 0.0)))
+        used = am
+        quiet = quiet + 1 if (am >= tail_start and rel < mode_tol) else 0
+        if quiet >= 2:
+            break
+    return used, {'mode_converged': bool(quiet >= 2), 'mode_selection': 'adaptive_tail',
+                  'mode_tail_start': int(tail_start), 'mode_last_relative_increment': rel}
 
 
 def solve_bor(points, freq_hz, thetas_deg, formulation="auto", cfie_alpha=0.5, zs=None, n_modes=None,
@@ -330,7 +364,8 @@ def solve_bor(points, freq_hz, thetas_deg, formulation="auto", cfie_alpha=0.5, z
     mcap, bandwidth = mode_limits(k, float(np.max(pts[:, 0])), thetas, n_modes)
     if check_abort is not None:
         check_abort()
-    F, tele = solve_bor_device(pts, k, thetas, mcap, precision=requested_precision())
+    F, tele = solve_bor_device(pts, k, thetas, mcap, precision=requested_precision(), mode_tol=mode_tol,
+                               tail_start=bandwidth)
     nth = len(thetas)
     Fv, Fh = F[:nth], F[nth:]
     return {
@@ -339,7 +374,9 @@ def solve_bor(points, freq_hz, thetas_deg, formulation="auto", cfie_alpha=0.5, z
         'sigma_hh': (4.0 * math.pi * np.abs(Fh) ** 2).tolist(),
         'amp_vv': Fv.tolist(),
         'amp_hh': Fh.tolist(),
-        'modes_used': int(mcap),
+        'modes_used': int(tele['modes_used']),
+        'mode_converged': bool(tele.get('mode_converged', False)),
+        'mode_cap': int(mcap),
         'n_unknowns': int(tele['n_unknowns']),
         'formulation': 'efie',
         'formulation_requested': form,

@@ -108,3 +108,16 @@ def test_grouped_modes_match_per_mode_solves(precision):
     assert t_g['mode_systems_solved'] == t_1['mode_systems_solved'] == 13
     rtol = 1e-12 if precision == 'double' else 1e-8
     np.testing.assert_allclose(f_g, f_1, rtol=rtol, atol=rtol * np.max(np.abs(f_1)))
+
+
+def test_adaptive_mode_tail_matches_reference(ctx):
+    """With the default mode cap the modal sum stops where the reference's adaptive tail
+    stopped on the same sphere (tests/golden/ref_bor_sphere.npz: |m| <= 10)."""
+    from grim_20261007_b200.bor.solver import solve_bor
+    g = np.load(os.path.join(GOLDEN, 'ref_bor_sphere.npz'))
+    res = solve_bor(g['points'], float(g['freq_hz']), g['thetas'], formulation='efie')
+    assert res['modes_used'] == int(g['modes_used']) and res['mode_converged']
+    assert res['mode_cap'] > res['modes_used']
+    for pol in ('vv', 'hh'):
+        amp = np.asarray(res['amp_' + pol])
+        assert np.max(np.abs(amp - g['amp_%s_efie' % pol]) / np.abs(g['amp_%s_efie' % pol])) < 2e-3
