@@ -1482,7 +1482,7 @@ static int grp_plan(int count, const int *n, int bn, GrpPlan *P) {
                     c = 2 * ceil_div(rest, NB);
                     P->fl_apply[p] += 8.0 * 2.0 * rest * NB * NB;
                 } else if (k == 1) {
-                    c = sizeof(C) == sizeof(float2) ? (grp_rows_a(rest) + grp_rows_b(rest)) / 8 : 0;
+                    c = 0;  // (operand packing is done by the panel solve)
                 } else {
                     c = sizeof(C) == sizeof(float2) ? (int64_t)(grp_rows_a(rest) / TC_BM) * (grp_rows_b(rest) / bn)
                                                     : (int64_t)ceil_div(rest, DM_BM) * ceil_div(rest, DM_BN);

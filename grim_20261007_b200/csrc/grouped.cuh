@@ -91,24 +91,6 @@ __global__ void __launch_bounds__(256) k_grp_last(const GrpSys *__restrict__ sys
                       S.flags + 1);
 }
 
-// Packing of L21 (A operand, grp_rows_a(rest) rows) and U12 (B operand, grp_rows_b(rest)
-// rows) of every updating system: rows / 8 CTAs of 256 threads per operand (32 chunks per
-// row of GRP_KP floats).
-__global__ void __launch_bounds__(256) k_grp_pack(const GrpSys *__restrict__ sys, int p, const int *prefix, int count) {
-    const int s = grp_find(prefix, count, blockIdx.x);
-    const GrpSys &S = sys[s];
-    const int j = NB * p, rest = S.n - j - NB;
-    const int Mp = grp_rows_a(rest), Np = grp_rows_b(rest);
-    const int b = blockIdx.x - __ldg(prefix + s), ba = Mp / 8;
-    const float2 *A = (const float2 *)S.A;
-    if (b < ba)
-        tc_pack_a_chunk((int64_t)b * 256 + threadIdx.x, rest, NB, A + (int64_t)j * S.lda + j + NB, S.lda, S.pa_hi,
-                        S.pa_lo, Mp, Mp, 0, GRP_KP, 1.f);
-    else
-        tc_pack_b_chunk((int64_t)(b - ba) * 256 + threadIdx.x, NB, rest, A + (int64_t)(j + NB) * S.lda + j, S.lda,
-                        S.pb_hi, S.pb_lo, Np, GRP_KP);
-}
-
 // A22 -= L21 U12 for every updating complex64 system: (Mp / 128) x (Np / BN) tiles each.
 template <int BN, int STAGES>
 __global__ void __launch_bounds__(TC_THREADS)
