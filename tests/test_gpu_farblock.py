@@ -144,3 +144,21 @@ def test_far_block_matches_reference_library_on_a_large_tile():
         assert np.array_equal(acc[:, inside], r[:, inside])
         if outside.any():
             assert np.max(np.abs(acc[:, outside] - r[:, outside])) <= 1e-13 * np.abs(r[:, outside]).max()
+
+
+def test_far_block_width_one_single_point():
+    """Width 1 and one quadrature point (the generic kernel) against the restatement."""
+    if not torch.cuda.is_available():
+        pytest.skip('no CUDA device')
+    g = np.load(GOLDEN)
+    inp, k, bounds, power, upper = case(g, 'w2')
+    inp['obs_pts'] = np.ascontiguousarray(inp['obs_pts'][:, :1])
+    inp['src_pts'] = np.ascontiguousarray(inp['src_pts'][:, :1])
+    inp['qw'] = np.ones(1)
+    inp['phi'] = np.ones((1, 1))
+    inside = F.in_table(inp['obs_pts'], inp['src_pts'], inp['far'], upper)
+    ref = F.far_block(*(inp[key] for key in KEYS), 1, 1, 1, 1, k, bounds, power)
+    status, got = device_far(inp, 1, k, bounds, power)
+    assert status == 0
+    for acc, r in zip(got, ref):
+        assert np.array_equal(acc[:, inside], r[:, inside])

@@ -137,3 +137,22 @@ def test_grouped_sweep_matches_per_system_solves():
             db = 10 * np.log10(s64)
             mask = db > db.max() - 40
             assert np.max(np.abs(10 * np.log10(np.abs(a_g) ** 2 / s64))[mask]) < 0.05
+
+
+@pytest.mark.parametrize('orders', [[1], [300], [1, 2, 3, 64, 65]])
+def test_grouped_edge_orders(ctx, orders):
+    """One system, 1 x 1 systems and orders around one panel: equal to the single-system LU."""
+    from grim_20261007_b200.device import to_device_colmajor, to_host_matrix
+    from grim_20261007_b200.grouped import getrf_grouped
+    rng = np.random.default_rng(len(orders) * 7 + orders[0])
+    mats = [rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n)) + (2.0 * n if i % 2 else 0.0) * np.eye(n)
+            for i, n in enumerate(orders)]
+    for dt in (torch.complex64, torch.complex128):
+        dev = [to_device_colmajor(a, dt) for a in mats]
+        ipivs, infos, _ = getrf_grouped(dev, use_graph=True, ctx=ctx)
+        assert infos == [0] * len(mats)
+        for a, t, ip in zip(mats, dev, ipivs):
+            ts, ips, info = _single(ctx, a, dt)
+            assert info == 0
+            np.testing.assert_array_equal(ip.cpu().numpy(), ips.cpu().numpy())
+            assert np.array_equal(to_host_matrix(t), to_host_matrix(ts))
