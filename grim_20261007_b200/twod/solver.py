@@ -519,10 +519,9 @@ def solve_monostatic_rcs_2d(geometry_snapshot, frequencies_ghz, elevations_deg, 
         raise ValueError('Quality gate failed: backward error gate')
     samples = []
     for export, _pol in _CO_POLARIZED_2D_CHANNELS:
-        for s in channels[export]['samples']:
-            row = dict(s)
+        for row in channels[export]['samples']:  # this call's own records: labelled in place
             row['polarization'] = export
-            samples.append(row)
+        samples.extend(channels[export]['samples'])
     metadata = {'channels': {k: v['metadata'] for k, v in channels.items()},
                 'polarizations': [c[0] for c in _CO_POLARIZED_2D_CHANNELS]}
     return {
@@ -604,10 +603,9 @@ def solve_monostatic_rcs_2d_certified(geometry_snapshot, frequencies_ghz, elevat
     channels = {export: by_pol[pol] for export, pol in _CO_POLARIZED_2D_CHANNELS}
     samples = []
     for export, _pol in _CO_POLARIZED_2D_CHANNELS:
-        for s_ in channels[export]['samples']:
-            row = dict(s_)
+        for row in channels[export]['samples']:
             row['polarization'] = export
-            samples.append(row)
+        samples.extend(channels[export]['samples'])
     metadata = {'channels': {k: v['metadata'] for k, v in channels.items()},
                 'polarizations': [c[0] for c in _CO_POLARIZED_2D_CHANNELS],
                 'mesh_convergence_certified': True, 'certified_entry_point': True, 'published_mesh': 'fine',
