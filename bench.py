@@ -161,20 +161,22 @@ def run_serving(args):
 
 
 def run_bor(args):
-    """Body-of-revolution ogive: 400 generatrix segments, |m| <= 40, 361 aspects, VV/HH."""
+    """Body-of-revolution ogive: 400 generatrix segments, |m| <= 40, 361 aspects, VV/HH, in
+    the reference's default formulation for a closed body (CFIE, alpha = 0.5)."""
     import torch
     from grim_20261007_b200 import synthetic as S
     from grim_20261007_b200.bor.solver import solve_bor_device
     gen, length, half = S.ogive_case(args.seed, n=400)
     k = 25.0 / max(1e-9, float(np.max(gen[:, 0])))  # k rho_max = 25 (the reference's |m| <= 40 converges)
     th = np.arange(361) * 0.5
-    out = {'length_m': length, 'half_angle_deg': half, 'k': k, 'segments': 400, 'modes': 81, 'aspects': 361}
+    out = {'length_m': length, 'half_angle_deg': half, 'k': k, 'segments': 400, 'modes': 81, 'aspects': 361,
+           'formulation': 'cfie'}
     res = {}
     for prec in ('double', 'mixed'):
-        solve_bor_device(gen, k, th[:8], 4, precision=prec)  # warm-up
+        solve_bor_device(gen, k, th[:8], 4, precision=prec, alpha=0.5)  # warm-up
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        F, tele = solve_bor_device(gen, k, th, 40, precision=prec)
+        F, tele = solve_bor_device(gen, k, th, 40, precision=prec, alpha=0.5)
         torch.cuda.synchronize()
         dt = time.perf_counter() - t0
         res[prec] = F

@@ -96,11 +96,13 @@ SIGNATURES = [
     ('grim_mem_info', c_int, [c_void_p, ctypes.POINTER(c_size_t), ctypes.POINTER(c_size_t)]),
     ('grim_set_tuning', c_int, [c_void_p, c_int, c_int]),
     ('grim_bor_moments_size', c_int64, [c_int, c_int]),
-    ('grim_bor_moments', c_int, [c_void_p, c_int, c_void_p, c_double, c_int, c_int, c_void_p]),
-    ('grim_bor_assemble', c_int, [c_void_p, c_int, c_void_p, c_double, c_int, c_int, c_void_p, c_int, c_void_p,
-                                  c_void_p, c_void_p, c_int64]),
-    ('grim_bor_excitation', c_int, [c_void_p, c_int, c_void_p, c_double, c_int, c_int, c_void_p, c_int, c_int,
-                                    c_void_p, c_void_p, c_void_p, c_int64]),
+    ('grim_bor_mfie_moments_size', c_int64, [c_int, c_int]),
+    ('grim_bor_moments', c_int, [c_void_p, c_int, c_void_p, c_double, c_int, c_int, c_void_p, c_int, c_void_p,
+                                 c_void_p, c_void_p, c_void_p]),
+    ('grim_bor_assemble', c_int, [c_void_p, c_int, c_void_p, c_double, c_int, c_int, c_void_p, c_void_p, c_double,
+                                  c_int, c_void_p, c_void_p, c_void_p, c_int64]),
+    ('grim_bor_excitation', c_int, [c_void_p, c_int, c_void_p, c_double, c_int, c_int, c_void_p, c_int, c_double,
+                                    c_int, c_void_p, c_void_p, c_void_p, c_int64]),
     ('grim_bor_farfield_accumulate', c_int, [c_void_p, c_int, c_int, c_void_p, c_int64, c_void_p, c_int64, c_void_p]),
     ('grim_profile_enable', c_int, [c_void_p, c_int]),
     ('grim_profile_report', c_int, [c_void_p, c_char_p, c_int]),

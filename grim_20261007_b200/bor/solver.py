@@ -2,16 +2,16 @@
 
 Pipeline per frequency (all arithmetic in libgrimgpu kernels):
   1. ``grim_bor_moments``: mode-independent element-pair moments of the modal Green's
-     function for n = 0..m_max+1 (one launch over all element pairs);
-  2. per signed mode m = -m_max..m_max: ``grim_bor_assemble`` (reduced EFIE matrix with the
+     function and, for the CFIE / MFIE, of the modal MFIE brackets, for n = 0..m_max+1
+     (far pairs, near work items and their reduction: three launches);
+  2. per signed mode m = -m_max..m_max: ``grim_bor_assemble`` (reduced matrix with the
      axis-pole treatment), ``grim_bor_excitation`` (VV/HH right-hand sides for every aspect
      and the far-field weights), dense solve (``grim_zgesv_mixed``, FP64 or mixed),
      ``grim_bor_farfield_accumulate``;
   3. sigma = 4 pi |F|^2 with F = -(j k eta / 4 pi) sum_m W_m^T x_m.
 
-Only the PEC EFIE is implemented on this path; ``formulation='auto'``/``'cfie'`` run the
-EFIE and say so in the result (``formulation`` key).  Impedance and sheet models are
-rejected.
+The PEC EFIE, MFIE and CFIE are implemented (the reference's default for a closed body is
+the CFIE with alpha = 0.5).  Impedance and sheet models are rejected.
 """
 from __future__ import annotations
 
@@ -25,6 +25,7 @@ from .. import _lib
 from ..device import context, ptr, require_cuda, run_pool
 from ..execution import requested_precision
 from ..twod import operators as ops2d
+from .rules import near_rules, pair_classes
 
 ETA0 = 376.730313668
 C0 = 299_792_458.0
@@ -109,40 +110,67 @@ def far_points(nodes):
     return pts.reshape(-1, 2)
 
 
-def nxi_max(nodes, k, mmax):
-    """Largest per-pair azimuthal sample count over far element pairs (|e - f| >= 2)."""
+def nxi_max(nodes, k, mmax, cls=None):
+    """Largest per-pair azimuthal sample count over far element pairs (class 0)."""
     pts = far_points(nodes)
     ne = len(nodes) - 1
+    if cls is None:
+        cls = pair_classes(nodes)
     el = np.repeat(np.arange(ne), FAR_ORDER)
     best = 32
     for a in range(0, len(pts), 2048):
         pa = pts[a:a + 2048]
         ea = el[a:a + 2048]
-        far = np.abs(ea[:, None] - el[None, :]) >= 2
+        far = cls[ea[:, None], el[None, :]] == 0
         c = np.sqrt(pa[:, None, 0] * pts[None, :, 0])
         r0 = np.hypot(pa[:, None, 0] - pts[None, :, 0], pa[:, None, 1] - pts[None, :, 1])
-        v = 1.5 * (2.0 * k * c + mmax + 2) + 30.0 * c / np.maximum(r0, 1e-300) + 16.0
+        v = 1.5 * (2.0 * k * c + mmax + 2) + 40.0 * c / np.maximum(r0, 1e-300) + 16.0
         n = 32 * np.ceil(v / 32.0)
         if np.any(far):
             best = max(best, int(np.max(n[far])))
     return min(best, MAX_NXI)
 
 
-class BorDevice:
-    """Device-resident generatrix, moments and per-mode maps of one (body, k)."""
+_RULES = None
 
-    def __init__(self, points, k, mmax, ctx=None):
+
+def _near_rules():
+    global _RULES
+    if _RULES is None:
+        _RULES = near_rules()
+    return _RULES
+
+
+class BorDevice:
+    """Device-resident generatrix, moments and per-mode maps of one (body, k).
+
+    ``alpha`` = 1: the EFIE; 0 < alpha < 1: the CFIE alpha EFIE + (1 - alpha) eta0 MFIE
+    (the reference's closed-body default, alpha = 0.5); 0: the MFIE alone."""
+
+    def __init__(self, points, k, mmax, ctx=None, alpha=1.0):
         self.ctx = ctx or context()
         self.nodes = validate_generatrix(points)
         self.k = float(k)
         self.mmax = int(mmax)
+        self.alpha = float(alpha)
+        if not 0.0 <= self.alpha <= 1.0:
+            raise ValueError('alpha must lie in [0, 1]')
         self.ne = len(self.nodes) - 1
         self.nodes_dev = torch.from_numpy(np.ascontiguousarray(self.nodes.reshape(-1))).to('cuda')
         size = int(self.ctx.lib.grim_bor_moments_size(self.ne, self.mmax))
         self.mom = torch.empty(size // 16, dtype=torch.complex128, device='cuda')
-        self.nxi = nxi_max(self.nodes, self.k, self.mmax)
+        self.momk = None
+        if self.alpha < 1.0:
+            size = int(self.ctx.lib.grim_bor_mfie_moments_size(self.ne, self.mmax))
+            self.momk = torch.empty(size // 16, dtype=torch.complex128, device='cuda')
+        self.cls = np.ascontiguousarray(pair_classes(self.nodes))
+        self.nxi = nxi_max(self.nodes, self.k, self.mmax, self.cls)
+        rule, starts = _near_rules()
         _lib.check(self.ctx.lib.grim_bor_moments(self.ctx.h, self.ne, ptr(self.nodes_dev), self.k, self.mmax, self.nxi,
-                                                 ptr(self.mom)), 'grim_bor_moments')
+                                                 self.cls.ctypes.data, len(rule), rule.ctypes.data,
+                                                 starts.ctypes.data, ptr(self.mom),
+                                                 None if self.momk is None else ptr(self.momk)),
+                   'grim_bor_moments')
         self._maps = {}
 
     def mode_map(self, m):
@@ -157,7 +185,8 @@ class BorDevice:
         rf, rw, nred = self.mode_map(m)
         Z = torch.empty((nred, nred), dtype=torch.complex128, device='cuda')
         _lib.check(ctx.lib.grim_bor_assemble(ctx.h, self.ne, ptr(self.nodes_dev), self.k, self.mmax, m,
-                                             ptr(self.mom), nred, ptr(rf), ptr(rw), ptr(Z), nred),
+                                             ptr(self.mom), None if self.momk is None else ptr(self.momk),
+                                             self.alpha, nred, ptr(rf), ptr(rw), ptr(Z), nred),
                    'grim_bor_assemble')
         return Z
 
@@ -167,7 +196,8 @@ class BorDevice:
         nth = int(th_dev.numel())
         V = torch.empty((2 * nth, nred), dtype=torch.complex128, device='cuda')
         _lib.check(ctx.lib.grim_bor_excitation(ctx.h, self.ne, ptr(self.nodes_dev), self.k, m, nth,
-                                               ptr(th_dev), int(far), nred, ptr(rf), ptr(rw), ptr(V), nred),
+                                               ptr(th_dev), int(far), self.alpha, nred, ptr(rf), ptr(rw), ptr(V),
+                                               nred),
                    'grim_bor_excitation')
         return V
 
@@ -255,7 +285,7 @@ def _solve_modes_grouped(dev, modes, th, precision, tol, workers):
 
 
 def solve_bor_device(points, k, thetas_deg, mmax, precision='double', tol=None, ctx=None, workers=None,
-                     signed_mode_symmetry=True, grouped=True, mode_tol=None, tail_start=0):
+                     signed_mode_symmetry=True, grouped=True, mode_tol=None, tail_start=0, alpha=1.0):
     """Device path: returns (F[2 nth] complex128 on the host, telemetry).
 
     The modal moments are built once; the per-mode systems are independent and run on the
@@ -266,7 +296,7 @@ def solve_bor_device(points, k, thetas_deg, mmax, precision='double', tol=None, 
     m > 0 counts twice: for the co-polarised monostatic far field the +m and -m
     contributions are identical (equal to the last bit in the oracle, for the sphere and
     the ogive).  With an explicit ``ctx`` (a serving slot) the modes run in turn on that
-    handle.  With ``grouped`` (default) the mode systems are factored together by one
+    handle.  ``alpha`` selects the formulation (``BorDevice``).  With ``grouped`` (default) the mode systems are factored together by one
     grouped LU (``grouped.py``); otherwise each mode is factored on its own worker.  With
     ``mode_tol`` the modal sum stops at the reference's adaptive tail (two consecutive
     modes at or above ``tail_start`` below the tolerance; ``_adaptive_tail``); all modes up
@@ -275,7 +305,7 @@ def solve_bor_device(points, k, thetas_deg, mmax, precision='double', tol=None, 
     from ..twod.solver import sweep_workers
     import time
     tm = time.perf_counter()
-    dev = BorDevice(points, k, mmax, ctx=ctx)
+    dev = BorDevice(points, k, mmax, ctx=ctx, alpha=alpha)
     for m in (0, 1, -1, 2):
         dev.mode_map(m)  # build the shared pole maps before the workers read them
     torch.cuda.synchronize()
@@ -341,22 +371,38 @@ def _adaptive_tail(contributions, mode_tol, tail_start):
 def solve_bor(points, freq_hz, thetas_deg, formulation="auto", cfie_alpha=0.5, zs=None, n_modes=None,
               gauss_order=FAR_ORDER, mode_tol=1e-6, workers=1, progress=None, check_abort=None,
               table_precision="auto", assembly="auto", stream_budget_gb=8.0, sheet_zs=None):
-    """Monostatic VV/HH RCS of a closed PEC BoR at aspects ``thetas_deg`` (from +z).
+    """Monostatic VV/HH RCS of a PEC BoR at aspects ``thetas_deg`` (from +z).
 
-    Same arguments and result keys as the reference's ``solve_bor``; the GPU path
-    runs the EFIE (see the module docstring).
+    Same arguments and result keys as the reference's ``solve_bor``
+    (``bor/solver.py:4066``).  ``formulation``: 'auto' selects the CFIE for a closed body
+    (both generatrix ends on the axis) and the EFIE otherwise, as the reference does;
+    'cfie' (alpha EFIE + (1 - alpha) eta0 MFIE, ``cfie_alpha`` in (0, 1)) and 'mfie' need a
+    closed body traversed from the +z pole to the -z pole; 'efie' also serves open shells.
     """
     form = str(formulation).strip().lower()
     if form not in {'auto', 'efie', 'cfie', 'mfie'}:
         raise ValueError(f"Unsupported BoR formulation '{formulation}'. Use 'auto', 'efie', 'cfie', or 'mfie'.")
+    if form in {'cfie', 'auto'}:
+        cfie_alpha = float(cfie_alpha)
+        if not np.isfinite(cfie_alpha) or not (0.0 < cfie_alpha < 1.0):
+            raise ValueError('CFIE alpha must be finite and satisfy 0 < alpha < 1.')
     if zs is not None or sheet_zs is not None:
         raise NotImplementedError('Impedance and sheet BoR models are outside the GPU PEC path.')
-    if form == 'mfie':
-        raise NotImplementedError('The MFIE diagnostic formulation is not implemented on the GPU path.')
     if int(gauss_order) != FAR_ORDER:
         raise ValueError(f'The GPU BoR path integrates far pairs with {FAR_ORDER} Gauss points per element.')
     require_cuda()
     pts = validate_generatrix(points)
+    closed = pts[0, 0] == 0.0 and pts[-1, 0] == 0.0
+    if form == 'auto':
+        form = 'cfie' if closed else 'efie'
+    if form in {'cfie', 'mfie'}:
+        if not closed:
+            raise ValueError(f'{form.upper()} requires a closed BoR whose two generatrix endpoints lie on the '
+                             'rotation axis; use EFIE for an intentionally open shell.')
+        if not pts[0, 1] > pts[-1, 1]:
+            raise ValueError('A closed BoR generatrix must be traversed from its +z axis endpoint to its -z axis '
+                             'endpoint so the left-of-travel normal faces the exterior.')
+    alpha = {'efie': 1.0, 'cfie': cfie_alpha, 'mfie': 0.0}[form]
     thetas = np.asarray(thetas_deg, dtype=np.float64).reshape(-1)
     if thetas.size == 0 or not np.all(np.isfinite(thetas)):
         raise ValueError('BoR aspects must be a non-empty list of finite angles.')
@@ -365,7 +411,7 @@ def solve_bor(points, freq_hz, thetas_deg, formulation="auto", cfie_alpha=0.5, z
     if check_abort is not None:
         check_abort()
     F, tele = solve_bor_device(pts, k, thetas, mcap, precision=requested_precision(), mode_tol=mode_tol,
-                               tail_start=bandwidth)
+                               tail_start=bandwidth, alpha=alpha)
     nth = len(thetas)
     Fv, Fh = F[:nth], F[nth:]
     return {
@@ -378,15 +424,13 @@ def solve_bor(points, freq_hz, thetas_deg, formulation="auto", cfie_alpha=0.5, z
         'mode_converged': bool(tele.get('mode_converged', False)),
         'mode_cap': int(mcap),
         'n_unknowns': int(tele['n_unknowns']),
-        'formulation': 'efie',
-        'formulation_requested': form,
+        'formulation': form,
         'boundary_model': 'pec',
         'assembly': 'gpu_moments',
         'table_precision': 'double',
         'device': context().device_name,
         'precision': requested_precision(),
-        'warnings': ([] if form == 'efie' else
-                     [f"formulation '{form}' requested; the GPU path solved the EFIE"]),
+        'warnings': [],
         'mode_bandwidth': int(bandwidth),
         'nxi_max': int(tele['nxi_max']),
     }

@@ -1,33 +1,48 @@
-// Body-of-revolution PEC EFIE, per azimuthal mode.
+// Body-of-revolution PEC EFIE / MFIE / CFIE, per azimuthal mode.
 //
-// Stage 1  k_bor_moments: one CTA per element pair (e, f).  For every point pair it
-//   evaluates the modal Green's function G_n = int_0^{2pi} e^{-jkR}/(4 pi R) cos(n xi) dxi
-//   for n = 0..mmax+1 (uniform trapezoid with a per-pair sample count for far pairs,
-//   sinh-substituted Gauss rule for same/adjacent elements) and accumulates the 20
-//   mode-independent element moments per n:
+// Stage 1  element-pair moments, mode-independent, for n = 0..mmax+1:
+//   EFIE, from the modal Green's function G_n = int_{-pi}^{pi} e^{-jkR}/(4 pi R) cos(n xi) dxi:
 //     A_ac  = sum T_a T_c rho rho' w w' G_n      DD_ac = sum D_a D_c w w' G_n
 //     DT_ac = sum D_a T_c w w' G_n               TD_ac = sum T_a D_c w w' G_n
 //     TT_ac = sum T_a T_c w w' G_n               (a, c in {0, 1}: the element's two tents)
-//   Layout: mom[((e * ne + f) * (mmax + 2) + n) * 20 + slot], complex128.
-// Stage 2  k_bor_assemble: the reduced mode-m matrix from the moments of the <= 4
-//   element pairs touching each node pair, with the pole treatment (inactive pole phi
-//   components, |m| = 1 pole t component tied to phi by j m sign(t_rho)).
-// Stage 3  k_bor_excitation: reduced right-hand sides (VV, HH per aspect) or far-field
-//   weights, with the phi integrals in closed form through J_m (CUDA's jn).
-// Reference: bor/solver.py:1769-1827 (assemble_mode), :2369-2440 (pole reduction),
-// :2558-2608 (rhs_vv_hh_batch / farfield_vv_hh_batch), bor/kernels.py:632 (modal kernels).
+//   MFIE (optional), from the four modal brackets K^n_uv = int F_uv(xi) e^{-j n xi} dxi
+//   (uv = tt, tf, ft, ff; tt/ff even in xi, tf/ft odd):
+//     B_uv,ac = sum T_a T_c rho rho' w w' K^n_uv
+//   Layouts: mom[((e * ne + f) * (mmax + 2) + n) * 20 + slot],
+//            momk[((e * ne + f) * (mmax + 2) + n) * 16 + 4 uv + 2 a + c], complex128.
+//   The element pairs follow the reference's routing (bor/solver.py:1520-1580): far pairs
+//   take 3 x 3 Gauss points and the uniform trapezoid rule in xi (k_bor_far, one CTA per
+//   pair); near pairs take the host's point list -- graded cells for self / adjacent pairs
+//   (bor/solver.py:718-806), a 12 x 12 Gauss rule for the others (:843) -- and a composite
+//   rule on xi in [0, pi] using each integrand's parity (k_bor_near over work items of at
+//   most BOR_NEAR_CHUNK point pairs, then k_bor_near_reduce in a fixed order).
+// Stage 2  k_bor_assemble: the reduced mode-m matrix alpha C EFIE + (1 - alpha) eta0
+//   ((1/2) M - K), C = j k eta 2 pi, from the moments of the <= 4 element pairs touching
+//   each node pair, with the pole treatment (inactive pole phi components, |m| = 1 pole t
+//   component tied to phi by j m sign(t_rho)).
+// Stage 3  k_bor_excitation: reduced right-hand sides alpha <W, E_inc> + (1 - alpha) eta0
+//   <W, n x H_inc> (VV, HH per aspect) or far-field weights, with the phi integrals in
+//   closed form through J_m (CUDA's jn).
+// Reference: bor/solver.py:1769-1827 (assemble_mode), :1962 (assemble_mfie_mode),
+// :2048 (rhs_mfie_mode), :2369-2440 (pole reduction), :2558-2608 (rhs_vv_hh_batch /
+// farfield_vv_hh_batch), :4285-4301 (CFIE), bor/kernels.py:896,996 (MFIE brackets).
 #pragma once
 #include "common.cuh"
 
 #define BOR_FAR_ORDER 3
-#define BOR_NEAR_ORDER 8
-#define BOR_NEAR_XI 32
 #define BOR_MAX_MODES 128
 #define BOR_MAX_NXI 8192
 #define BOR_SLOTS 20
+#define BOR_KSLOTS 16
+#define BOR_ALL_SLOTS (BOR_SLOTS + BOR_KSLOTS)
+#define BOR_THREADS 256
+#define BOR_FAR_CHUNK 256   // far-pair xi samples staged per pass
+#define BOR_NEAR_CHUNK 64   // point pairs per near work item
+#define BOR_XI_CORE 16      // Gauss points of the near rule's sinh core
+#define BOR_XI_PANEL 16     // Gauss points per panel of the near rule
 
 struct BorPt {
-    double rho, z, w, T0, T1, D0, D1;
+    double rho, z, w, T0, T1, D0, D1, tr, tz;
 };
 
 __device__ __forceinline__ BorPt bor_point(const double *nodes, int e, double s, double ws) {
@@ -42,12 +57,15 @@ __device__ __forceinline__ BorPt bor_point(const double *nodes, int e, double s,
     p.T1 = s;
     p.D0 = p.rho * (-1.0 / L) + p.T0 * trho;
     p.D1 = p.rho * (1.0 / L) + p.T1 * trho;
+    p.tr = trho;
+    p.tz = dz / L;
     return p;
 }
 
+// Far-pair xi sample count (multiple of 32, so that sin(x) = cos(x - pi/2) is a table shift).
 __device__ __forceinline__ int bor_nxi(double k, double rp, double rq, double r0, int mmax) {
     const double c = sqrt(rp * rq);
-    const double v = 1.5 * (2.0 * k * c + mmax + 2) + 30.0 * c / fmax(r0, 1e-300) + 16.0;
+    const double v = 1.5 * (2.0 * k * c + mmax + 2) + 40.0 * c / fmax(r0, 1e-300) + 16.0;
     int n = 32 * (int)ceil(v / 32.0);
     return n > BOR_MAX_NXI ? BOR_MAX_NXI : n;
 }
@@ -58,171 +76,399 @@ __device__ __forceinline__ void gl_node(int q, int i, double &x, double &w) {
     w = c_gl_w[q * (q - 1) / 2 + i];
 }
 
-// Source rule for a near pair: point i of the cubically graded rule(s) on [0,1];
-// self pairs split at s_obs (16 points), adjacent pairs cluster at the shared node.
-__device__ __forceinline__ void near_src(int e, int f, double s_obs, int i, double &s, double &ws) {
-    double x, w;
-    if (e == f) {
-        const int half = i / BOR_NEAR_ORDER, ii = i % BOR_NEAR_ORDER;
-        gl_node(BOR_NEAR_ORDER, ii, x, w);
-        const double u = 0.5 * (x + 1.0), wu = 0.5 * w;
-        if (half == 0) {  // [0, s_obs] toward s_obs
-            s = s_obs - s_obs * u * u * u;
-            ws = s_obs * 3.0 * u * u * wu;
-        } else {          // [s_obs, 1] toward s_obs
-            s = s_obs + (1.0 - s_obs) * u * u * u;
-            ws = (1.0 - s_obs) * 3.0 * u * u * wu;
-        }
-    } else {
-        gl_node(BOR_NEAR_ORDER, i, x, w);
-        const double u = 0.5 * (x + 1.0), wu = 0.5 * w;
-        if (f == e + 1) {  // toward 0
-            s = u * u * u;
-        } else {           // toward 1
-            s = 1.0 - u * u * u;
-        }
-        ws = 3.0 * u * u * wu;
+// Geometry of one point pair shared by every xi sample.
+struct BorPair {
+    double k, rp, rq, dr, dz, d2, rr2;     // rr2 = 2 rho rho'
+    double A, N, X, D, trp, tzp, trq, tzq;  // MFIE bracket invariants
+};
+
+__device__ __forceinline__ BorPair bor_pair(double k, const BorPt &p, const BorPt &q) {
+    BorPair s;
+    s.k = k;
+    s.rp = p.rho;
+    s.rq = q.rho;
+    s.dr = p.rho - q.rho;
+    s.dz = p.z - q.z;
+    s.d2 = s.dr * s.dr + s.dz * s.dz;
+    s.rr2 = 2.0 * p.rho * q.rho;
+    s.trp = p.tr;
+    s.tzp = p.tz;
+    s.trq = q.tr;
+    s.tzq = q.tz;
+    s.X = p.tr * q.tz - p.tz * q.tr;
+    s.D = p.tr * q.tr + p.tz * q.tz;
+    s.A = p.tr * s.dr + p.tz * s.dz;
+    s.N = -p.tz * s.dr + p.tr * s.dz;
+    return s;
+}
+
+// One xi sample times weight wt: the Green's function g and (MFIE) the four brackets
+// -p(R) [tt, tf, ft, ff] in the cancellation-free form (h = 1 - cos xi = 2 sin^2(xi/2)).
+template <bool MFIE>
+__device__ __forceinline__ void bor_sample(const BorPair &s, double shalf, double sx, double wt, double2 &g,
+                                           double2 (&F)[4]) {
+    const double h = 2.0 * shalf * shalf;
+    const double R = sqrt(s.d2 + s.rr2 * h);
+    double sk, ck;
+    sincos(s.k * R, &sk, &ck);
+    const double a = wt / (4.0 * GRIM_PI * R);
+    g = make_double2(a * ck, -a * sk);
+    if constexpr (MFIE) {
+        const double kr = s.k * R;
+        const double pre = a / (R * R);
+        // -(1 + j kR) e^{-jkR} / (4 pi R^3) times the weight
+        const double pr = -pre * (ck + kr * sk), pi = -pre * (kr * ck - sk);
+        const double tt = (s.A * s.X - s.D * s.N) +
+                          h * (s.A * s.tzp * s.trq + s.trp * s.rq * s.X + s.D * s.tzp * s.rq + s.trp * s.trq * s.N);
+        const double tf = -sx * s.dz * (s.trp * s.trp + s.tzp * s.tzp);
+        const double ft = sx * (s.rq * s.X + s.trq * s.N);
+        const double ff = -s.tzp * s.rq * h - s.N * (1.0 - h);
+        F[0] = make_double2(pr * tt, pi * tt);
+        F[1] = make_double2(pr * tf, pi * tf);
+        F[2] = make_double2(pr * ft, pi * ft);
+        F[3] = make_double2(pr * ff, pi * ff);
     }
 }
 
-// One point pair: compute G_n (n = 0..nm-1) into sG and accumulate the 20 moments.
-// All threads of the CTA participate; thread n < nm owns mode n's accumulators.
-__device__ __forceinline__ void bor_pair_accumulate(double k, const BorPt &p, const BorPt &q, bool near, int mmax,
-                                                    int nxi_cap, double2 *sg, double *scos, double2 *sG,
-                                                    double2 (&acc)[BOR_SLOTS]) {
-    const int t = threadIdx.x, nt = blockDim.x;
-    const int nm = mmax + 2;
-    const double r0 = sqrt((p.rho - q.rho) * (p.rho - q.rho) + (p.z - q.z) * (p.z - q.z));
-    const double rr4 = 4.0 * p.rho * q.rho;
-    double2 gsum = make_double2(0.0, 0.0);
-    if (!near) {
-        // nxi_cap = the shared-memory capacity the host sized (>= every far pair's count)
-        const int N = min(bor_nxi(k, p.rho, q.rho, r0, mmax), nxi_cap);
-        const double dxi = 2.0 * GRIM_PI / N;
-        for (int i = t; i < N; i += nt) {
-            double sx, cx;
-            sincospi(2.0 * i / (double)N, &sx, &cx);
-            scos[i] = cx;
-            const double s2 = sin(0.5 * i * dxi);
-            const double R = sqrt(r0 * r0 + rr4 * s2 * s2);
-            double sk, ck;
-            sincos(k * R, &sk, &ck);
-            const double f = dxi / (4.0 * GRIM_PI * R);
-            sg[i] = make_double2(ck * f, -sk * f);
-        }
-        __syncthreads();
-        if (t < nm) {
-            int idx = 0;
-            for (int i = 0; i < N; ++i) {
-                const double c = scos[idx];
-                gsum.x += sg[i].x * c;
-                gsum.y += sg[i].y * c;
-                idx += t;
-                if (idx >= N) idx -= N;
-            }
-            sG[t] = gsum;
-        }
-        __syncthreads();
-    } else {
-        const double c = sqrt(p.rho * q.rho);
-        const double umax = asinh(c * GRIM_PI / fmax(r0, 1e-300));
-        const double sc = fmax(r0, 1e-300) / c;
-        for (int i = t; i < BOR_NEAR_XI; i += nt) {
-            double x, w;
-            gl_node(BOR_NEAR_XI, i, x, w);
-            const double u = x * umax;
-            const double xi = sc * sinh(u);
-            const double dx = sc * cosh(u) * w * umax;
-            const double s = sin(0.5 * xi);
-            const double R = sqrt(r0 * r0 + rr4 * s * s);
-            double sk, ck;
-            sincos(k * R, &sk, &ck);
-            const double f = dx / (4.0 * GRIM_PI * R);
-            sg[i] = make_double2(ck * f, -sk * f);
-            scos[i] = xi;
-        }
-        __syncthreads();
-        if (t < nm) {
-            for (int i = 0; i < BOR_NEAR_XI; ++i) {
-                const double c2 = cos(t * scos[i]);
-                gsum.x += sg[i].x * c2;
-                gsum.y += sg[i].y * c2;
-            }
-            sG[t] = gsum;
-        }
-        __syncthreads();
-    }
-    if (t < nm) {
-        const double2 g = sG[t];
-        const double ww = p.w * q.w, rr = p.rho * q.rho * ww;
-        const double Ta[2] = {p.T0, p.T1}, Da[2] = {p.D0, p.D1};
-        const double Tc[2] = {q.T0, q.T1}, Dc[2] = {q.D0, q.D1};
-#pragma unroll
-        for (int a = 0; a < 2; ++a)
-#pragma unroll
-            for (int cc = 0; cc < 2; ++cc) {
-                const int s = 2 * a + cc;
-                const double fa = Ta[a] * Tc[cc] * rr, fdd = Da[a] * Dc[cc] * ww, fdt = Da[a] * Tc[cc] * ww,
-                             ftd = Ta[a] * Dc[cc] * ww, ftt = Ta[a] * Tc[cc] * ww;
-                acc[s].x += fa * g.x;        acc[s].y += fa * g.y;
-                acc[4 + s].x += fdd * g.x;   acc[4 + s].y += fdd * g.y;
-                acc[8 + s].x += fdt * g.x;   acc[8 + s].y += fdt * g.y;
-                acc[12 + s].x += ftd * g.x;  acc[12 + s].y += ftd * g.y;
-                acc[16 + s].x += ftt * g.x;  acc[16 + s].y += ftt * g.y;
-            }
+// The 36 per-point-pair factors multiplying G_n (slots 0..19) or K^n_uv (slots 20..35).
+__device__ __forceinline__ double bor_factor(const BorPt &p, const BorPt &q, int slot) {
+    const int ac = slot & 3, a = ac >> 1, c = ac & 1;
+    const double Ta = a ? p.T1 : p.T0, Tc = c ? q.T1 : q.T0;
+    const double Da = a ? p.D1 : p.D0, Dc = c ? q.D1 : q.D0;
+    const double ww = p.w * q.w;
+    if (slot >= BOR_SLOTS) return Ta * Tc * (p.rho * q.rho * ww);
+    switch (slot >> 2) {
+    case 0: return Ta * Tc * (p.rho * q.rho * ww);
+    case 1: return Da * Dc * ww;
+    case 2: return Da * Tc * ww;
+    case 3: return Ta * Dc * ww;
+    default: return Ta * Tc * ww;
     }
 }
 
-// grid = (ne, ne); dynamic smem: nxi_cap * (16 + 8) bytes + BOR_MAX_MODES * 16.
-__global__ void __launch_bounds__(128)
-k_bor_moments(int ne, const double *__restrict__ nodes, double k, int mmax, int nxi_cap, double2 *__restrict__ mom) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    // layout sized by the host for nxi_cap samples: sg[nxi_cap], scos[nxi_cap], sG[BOR_MAX_MODES]
-    double2 *sg = reinterpret_cast<double2 *>(smem_raw);
-    double *scos = reinterpret_cast<double *>(sg + nxi_cap);
-    double2 *sG = reinterpret_cast<double2 *>(scos + nxi_cap);
+// Shared-memory layout of the moment kernels (sizes from the host: nm modes, nsl slots).
+//   acc[nm * nsl]   running moments of the CTA's element pair / work item
+//   red[S * nm * 5] per-group partial sums of G_n and K^n_uv
+//   fac[nsl]        the current point pair's factors
+//   sum[nm * 5]     G_n, K^n_uv of the current point pair
+template <bool MFIE>
+__device__ __forceinline__ void bor_fold_pair(int nm, int S, double2 *red, double2 *sum, const double *fac,
+                                              double2 *acc) {
+    constexpr int NV = MFIE ? 5 : 1, nsl = MFIE ? BOR_ALL_SLOTS : BOR_SLOTS;
+    const int t = threadIdx.x;
+    // reduce the groups in a fixed order
+    for (int i = t; i < nm * NV; i += blockDim.x) {
+        double2 v = make_double2(0.0, 0.0);
+        for (int gq = 0; gq < S; ++gq) {
+            const double2 r = red[gq * nm * NV + i];
+            v.x += r.x;
+            v.y += r.y;
+        }
+        sum[i] = v;
+    }
+    __syncthreads();
+    for (int i = t; i < nm * nsl; i += blockDim.x) {
+        const int n = i / nsl, slot = i - n * nsl;
+        double2 v;
+        if (slot < BOR_SLOTS) {
+            v = sum[n * NV];
+        } else {
+            const int uv = (slot - BOR_SLOTS) >> 2;
+            const double2 kv = sum[n * NV + 1 + uv];
+            // odd brackets: K = -j sum F sin(n xi)
+            v = (uv == 1 || uv == 2) ? make_double2(kv.y, -kv.x) : kv;
+        }
+        const double f = fac[slot];
+        acc[i].x += f * v.x;
+        acc[i].y += f * v.y;
+    }
+    __syncthreads();
+}
+
+// grid = (ne, ne), BOR_THREADS threads; pairs with cls != 0 return at once.
+// dynamic smem: ctab[nxi_cap] doubles, then chunk samples, red, sum, fac, acc (host-sized).
+template <bool MFIE>
+__global__ void __launch_bounds__(BOR_THREADS)
+k_bor_far(int ne, const double *__restrict__ nodes, const unsigned char *__restrict__ cls, double k, int mmax,
+          int nxi_cap, double2 *__restrict__ mom, double2 *__restrict__ momk) {
+    constexpr int NV = MFIE ? 5 : 1, nsl = MFIE ? BOR_ALL_SLOTS : BOR_SLOTS;
     const int e = blockIdx.x, f = blockIdx.y;
-    const int nm = mmax + 2;
-    const bool near = abs(e - f) <= 1;
-    double2 acc[BOR_SLOTS];
-#pragma unroll
-    for (int s = 0; s < BOR_SLOTS; ++s) acc[s] = make_double2(0.0, 0.0);
+    if (cls[(int64_t)e * ne + f] != 0) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int nm = mmax + 2, S = BOR_THREADS / nm;
+    double *ctab = reinterpret_cast<double *>(smem_raw);
+    double2 *chunk = reinterpret_cast<double2 *>(ctab + nxi_cap);  // [NV][BOR_FAR_CHUNK]
+    double2 *red = chunk + NV * BOR_FAR_CHUNK;
+    double2 *sum = red + S * nm * NV;
+    double2 *acc = sum + nm * NV;
+    double *fac = reinterpret_cast<double *>(acc + nm * nsl);
+    const int t = threadIdx.x, n = t % nm, grp = t / nm;
+    for (int i = t; i < nm * nsl; i += blockDim.x) acc[i] = make_double2(0.0, 0.0);
     for (int ip = 0; ip < BOR_FAR_ORDER; ++ip) {
         double xo, wo;
         gl_node(BOR_FAR_ORDER, ip, xo, wo);
-        const double so = 0.5 * (xo + 1.0);
-        const BorPt p = bor_point(nodes, e, so, 0.5 * wo);
-        if (!near) {
-            for (int iq = 0; iq < BOR_FAR_ORDER; ++iq) {
-                double xs, wsq;
-                gl_node(BOR_FAR_ORDER, iq, xs, wsq);
-                const BorPt q = bor_point(nodes, f, 0.5 * (xs + 1.0), 0.5 * wsq);
-                bor_pair_accumulate(k, p, q, false, mmax, nxi_cap, sg, scos, sG, acc);
+        const BorPt p = bor_point(nodes, e, 0.5 * (xo + 1.0), 0.5 * wo);
+        for (int iq = 0; iq < BOR_FAR_ORDER; ++iq) {
+            double xs, wsq;
+            gl_node(BOR_FAR_ORDER, iq, xs, wsq);
+            const BorPt q = bor_point(nodes, f, 0.5 * (xs + 1.0), 0.5 * wsq);
+            const BorPair pr = bor_pair(k, p, q);
+            const int N = min(bor_nxi(k, p.rho, q.rho, sqrt(pr.d2), mmax), nxi_cap);
+            const double dxi = 2.0 * GRIM_PI / N;
+            for (int i = t; i < N; i += blockDim.x) ctab[i] = cospi(2.0 * i / (double)N);
+            if (t < nsl) fac[t] = bor_factor(p, q, t);
+            double2 sg = make_double2(0.0, 0.0), s1 = sg, s2 = sg, s3 = sg, s4 = sg;
+            for (int i0 = 0; i0 < N; i0 += BOR_FAR_CHUNK) {
+                const int cnt = min(BOR_FAR_CHUNK, N - i0);
+                __syncthreads();
+                for (int j = t; j < cnt; j += blockDim.x) {
+                    const int i = i0 + j;
+                    double2 g, F[4];
+                    bor_sample<MFIE>(pr, sinpi(i / (double)N), sinpi(2.0 * i / (double)N), dxi, g, F);
+                    chunk[j] = g;
+                    if constexpr (MFIE) {
+#pragma unroll
+                        for (int u = 0; u < 4; ++u) chunk[(1 + u) * BOR_FAR_CHUNK + j] = F[u];
+                    }
+                }
+                __syncthreads();
+                if (grp < S) {
+                    // cos(n xi_i) = ctab[n i mod N], sin(n xi_i) = ctab[(n i - N/4) mod N]
+                    int idx = (int)(((int64_t)n * (i0 + grp)) % N);
+                    const int step = (int)(((int64_t)n * S) % N);
+                    for (int j = grp; j < cnt; j += S) {
+                        const double c = ctab[idx];
+                        const double2 v = chunk[j];
+                        sg.x += v.x * c;
+                        sg.y += v.y * c;
+                        if constexpr (MFIE) {
+                            int is = idx - N / 4;
+                            if (is < 0) is += N;
+                            const double sn = ctab[is];
+                            const double2 f0 = chunk[BOR_FAR_CHUNK + j], f1 = chunk[2 * BOR_FAR_CHUNK + j];
+                            const double2 f2 = chunk[3 * BOR_FAR_CHUNK + j], f3 = chunk[4 * BOR_FAR_CHUNK + j];
+                            s1.x += f0.x * c;  s1.y += f0.y * c;
+                            s2.x += f1.x * sn; s2.y += f1.y * sn;
+                            s3.x += f2.x * sn; s3.y += f2.y * sn;
+                            s4.x += f3.x * c;  s4.y += f3.y * c;
+                        }
+                        idx += step;
+                        if (idx >= N) idx -= N;
+                    }
+                }
             }
-        } else {
-            const int nq = (e == f) ? 2 * BOR_NEAR_ORDER : BOR_NEAR_ORDER;
-            for (int iq = 0; iq < nq; ++iq) {
-                double s, ws;
-                near_src(e, f, so, iq, s, ws);
-                const BorPt q = bor_point(nodes, f, s, ws);
-                bor_pair_accumulate(k, p, q, true, mmax, nxi_cap, sg, scos, sG, acc);
+            if (grp < S) {
+                double2 *r = red + (grp * nm + n) * NV;
+                r[0] = sg;
+                if constexpr (MFIE) {
+                    r[1] = s1;
+                    r[2] = s2;
+                    r[3] = s3;
+                    r[4] = s4;
+                }
             }
+            __syncthreads();
+            bor_fold_pair<MFIE>(nm, S, red, sum, fac, acc);
         }
     }
-    if (threadIdx.x < nm) {
-        double2 *o = mom + (((int64_t)e * ne + f) * nm + threadIdx.x) * BOR_SLOTS;
-#pragma unroll
-        for (int s = 0; s < BOR_SLOTS; ++s) o[s] = acc[s];
+    const int64_t base = ((int64_t)e * ne + f) * nm;
+    for (int i = t; i < nm * nsl; i += blockDim.x) {
+        const int nn_ = i / nsl, slot = i - nn_ * nsl;
+        if (slot < BOR_SLOTS) mom[(base + nn_) * BOR_SLOTS + slot] = acc[i];
+        else momk[(base + nn_) * BOR_KSLOTS + slot - BOR_SLOTS] = acc[i];
     }
 }
 
-// grid = ceil(nred / 16) x ceil(nred / 16), block 16 x 16.  rmap[2*nn] gives, for every
-// full component index (t: node, phi: nn + node), the reduced index or -1; tie[2*nn]
-// holds the complex weight of that component inside its reduced function (1 or
-// j m sign(t_rho) for a pole phi folded into the pole t function).  For each reduced
-// pair, the entry is sum over full components mapping to it of conj(w_row) Z_full w_col.
-// full2red: for reduced index r, up to two full components (f0, f1) with weights.
-__global__ void k_bor_assemble(int ne, int mmax, int m, double k, const double2 *__restrict__ mom, int nred,
+// Near-pair xi rule on [0, pi] for delta = R0 / c, span = 2 pi / (nmax + k c + 1):
+// a sinh-mapped Gauss core on [0, a], a = min(4 delta, span, pi), then panels
+// [a 2^g, a 2^(g+1)] while a 2^g < span, then panels of length span up to pi.
+struct BorRule {
+    double delta, span, a, vmax, top;
+    int geo, uni;
+};
+
+__device__ __forceinline__ BorRule bor_rule(double delta, double span) {
+    BorRule r;
+    r.delta = delta;
+    r.span = span;
+    r.a = fmin(fmin(4.0 * delta, span), GRIM_PI);
+    r.vmax = asinh(r.a / delta);
+    r.geo = 0;
+    double top = r.a;
+    while (top < span && top < GRIM_PI && r.geo < 2048) {
+        top *= 2.0;
+        ++r.geo;
+    }
+    r.top = top;
+    int uni = top < GRIM_PI ? (int)ceil((GRIM_PI - top) / span) : 0;
+    if (uni > 0 && top + (uni - 1) * span >= GRIM_PI) --uni;
+    r.uni = uni;
+    return r;
+}
+
+__device__ __forceinline__ int bor_rule_count(const BorRule &r) { return BOR_XI_CORE + BOR_XI_PANEL * (r.geo + r.uni); }
+
+// Node j of the rule: xi and weight (times 2 for the half range).
+__device__ __forceinline__ void bor_rule_node(const BorRule &r, int j, double &xi, double &w) {
+    double x, wg;
+    if (j < BOR_XI_CORE) {
+        gl_node(BOR_XI_CORE, j, x, wg);
+        const double v = 0.5 * (x + 1.0) * r.vmax;
+        xi = r.delta * sinh(v);
+        w = r.delta * cosh(v) * (0.5 * wg) * r.vmax;
+    } else {
+        const int P = (j - BOR_XI_CORE) / BOR_XI_PANEL, q = (j - BOR_XI_CORE) % BOR_XI_PANEL;
+        double lo, hi;
+        if (P < r.geo) {
+            lo = ldexp(r.a, P);
+            hi = fmin(ldexp(r.a, P + 1), GRIM_PI);
+        } else {
+            lo = fmin(r.top + (P - r.geo) * r.span, GRIM_PI);
+            hi = fmin(r.top + (P + 1 - r.geo) * r.span, GRIM_PI);
+        }
+        gl_node(BOR_XI_PANEL, q, x, wg);
+        xi = lo + (hi - lo) * (0.5 * (x + 1.0));
+        w = (hi - lo) * (0.5 * wg);
+    }
+    w *= 2.0;
+}
+
+struct BorItem {
+    int e, f, r0, r1;  // element pair and its point-pair range in the rule table
+};
+
+// grid = number of near work items, BOR_THREADS threads.  rule[3 i .. 3 i + 2] = (s, s', w).
+// Writes the item's moments to part[item][n][slot] (nm x nsl complex).
+// dynamic smem: rot[chn * nm] (e^{j n xi} of the staged samples), samples [NV][chn], xi[chn],
+// then red, sum, fac, acc as in k_bor_far.
+template <bool MFIE>
+__global__ void __launch_bounds__(BOR_THREADS)
+k_bor_near(const BorItem *__restrict__ items, const double *__restrict__ nodes, const double *__restrict__ rule,
+           double k, int mmax, int chn, double2 *__restrict__ part) {
+    constexpr int NV = MFIE ? 5 : 1, nsl = MFIE ? BOR_ALL_SLOTS : BOR_SLOTS;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int nm = mmax + 2, S = BOR_THREADS / nm;
+    double2 *rot = reinterpret_cast<double2 *>(smem_raw);  // [chn][nm]
+    double2 *smp = rot + chn * nm;                         // [NV][chn]
+    double *sxi = reinterpret_cast<double *>(smp + NV * chn);
+    double2 *red = reinterpret_cast<double2 *>(sxi + chn);
+    double2 *sum = red + S * nm * NV;
+    double2 *acc = sum + nm * NV;
+    double *fac = reinterpret_cast<double *>(acc + nm * nsl);
+    const BorItem it = items[blockIdx.x];
+    const int t = threadIdx.x, n = t % nm, grp = t / nm;
+    for (int i = t; i < nm * nsl; i += blockDim.x) acc[i] = make_double2(0.0, 0.0);
+    for (int ipp = it.r0; ipp < it.r1; ++ipp) {
+        const BorPt p = bor_point(nodes, it.e, rule[3 * ipp], rule[3 * ipp + 2]);
+        const BorPt q = bor_point(nodes, it.f, rule[3 * ipp + 1], 1.0);
+        const BorPair pr = bor_pair(k, p, q);
+        const double c = sqrt(p.rho * q.rho);
+        const BorRule rl = bor_rule(sqrt(pr.d2) / c, 2.0 * GRIM_PI / ((mmax + 1) + k * c + 1.0));
+        const int na = bor_rule_count(rl);
+        if (t < nsl) fac[t] = bor_factor(p, q, t);
+        double2 sg = make_double2(0.0, 0.0), s1 = sg, s2 = sg, s3 = sg, s4 = sg;
+        for (int j0 = 0; j0 < na; j0 += chn) {
+            const int cnt = min(chn, na - j0);
+            __syncthreads();
+            for (int j = t; j < cnt; j += blockDim.x) {
+                double xi, w;
+                bor_rule_node(rl, j0 + j, xi, w);
+                double sh, ch, sx, cx;
+                sincos(0.5 * xi, &sh, &ch);
+                sincos(xi, &sx, &cx);
+                double2 g, F[4];
+                bor_sample<MFIE>(pr, sh, sx, w, g, F);
+                smp[j] = g;
+                if constexpr (MFIE) {
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) smp[(1 + u) * chn + j] = F[u];
+                }
+                sxi[j] = xi;
+            }
+            __syncthreads();
+            // e^{j n xi_j}: each of 4 threads per sample starts one quarter of the orders
+            // with sincos and rotates through it
+            {
+                const int q4 = (nm + 3) / 4;
+                for (int task = t; task < 4 * cnt; task += blockDim.x) {
+                    const int j = task % cnt, quarter = task / cnt;
+                    const int n0 = quarter * q4, n1 = min(nm, n0 + q4);
+                    if (n0 >= n1) continue;
+                    const double xi = sxi[j];
+                    double s0, c0, sst, cst;
+                    sincos(n0 * xi, &s0, &c0);
+                    sincos(xi, &sst, &cst);
+                    double2 z = make_double2(c0, s0);
+                    for (int nn_ = n0; nn_ < n1; ++nn_) {
+                        rot[j * nm + nn_] = z;
+                        z = make_double2(z.x * cst - z.y * sst, z.x * sst + z.y * cst);
+                    }
+                }
+            }
+            __syncthreads();
+            if (grp < S) {
+                for (int j = grp; j < cnt; j += S) {
+                    const double2 z = rot[j * nm + n];
+                    const double2 v = smp[j];
+                    sg.x += v.x * z.x;
+                    sg.y += v.y * z.x;
+                    if constexpr (MFIE) {
+                        const double2 f0 = smp[chn + j], f1 = smp[2 * chn + j];
+                        const double2 f2 = smp[3 * chn + j], f3 = smp[4 * chn + j];
+                        s1.x += f0.x * z.x; s1.y += f0.y * z.x;
+                        s2.x += f1.x * z.y; s2.y += f1.y * z.y;
+                        s3.x += f2.x * z.y; s3.y += f2.y * z.y;
+                        s4.x += f3.x * z.x; s4.y += f3.y * z.x;
+                    }
+                }
+            }
+        }
+        if (grp < S) {
+            double2 *r = red + (grp * nm + n) * NV;
+            r[0] = sg;
+            if constexpr (MFIE) {
+                r[1] = s1;
+                r[2] = s2;
+                r[3] = s3;
+                r[4] = s4;
+            }
+        }
+        __syncthreads();
+        bor_fold_pair<MFIE>(nm, S, red, sum, fac, acc);
+    }
+    double2 *out = part + (int64_t)blockIdx.x * nm * nsl;
+    for (int i = t; i < nm * nsl; i += blockDim.x) out[i] = acc[i];
+}
+
+// grid = number of near element pairs; pairs[i] = (e, f, first item, end item).
+template <bool MFIE>
+__global__ void k_bor_near_reduce(int ne, int mmax, const int4 *__restrict__ pairs, const double2 *__restrict__ part,
+                                  double2 *__restrict__ mom, double2 *__restrict__ momk) {
+    constexpr int nsl = MFIE ? BOR_ALL_SLOTS : BOR_SLOTS;
+    const int nm = mmax + 2;
+    const int4 pq = pairs[blockIdx.x];
+    const int64_t base = ((int64_t)pq.x * ne + pq.y) * nm;
+    for (int i = threadIdx.x; i < nm * nsl; i += blockDim.x) {
+        double2 v = make_double2(0.0, 0.0);
+        for (int it = pq.z; it < pq.w; ++it) {
+            const double2 r = part[(int64_t)it * nm * nsl + i];
+            v.x += r.x;
+            v.y += r.y;
+        }
+        const int nn_ = i / nsl, slot = i - nn_ * nsl;
+        if (slot < BOR_SLOTS) mom[(base + nn_) * BOR_SLOTS + slot] = v;
+        else momk[(base + nn_) * BOR_KSLOTS + slot - BOR_SLOTS] = v;
+    }
+}
+
+// grid = ceil(nred / 16) x ceil(nred / 16), block 16 x 16.  red_full[2*nred] lists, for
+// every reduced function, up to two full components (t: node, phi: nn + node; -1 unused)
+// and red_w[2*nred] their complex weights (1, or j m sign(t_rho) for a pole phi folded into
+// the pole t function).  Each entry is sum over the components of conj(w_row) Z_full w_col
+// with Z_full = alpha C EFIE + beta ((1/2) M - K) (beta = (1 - alpha) eta0; momk == nullptr
+// for the EFIE alone, alpha = 1).
+__global__ void k_bor_assemble(int ne, int mmax, int m, double k, const double2 *__restrict__ mom,
+                               const double2 *__restrict__ momk, double alpha, int nred,
                                const int *__restrict__ red_full, const double2 *__restrict__ red_w,
                                const double *__restrict__ nodes, double2 *__restrict__ Z, int64_t ldz) {
     const int r = blockIdx.x * 16 + threadIdx.x;  // row (test)
@@ -232,6 +478,8 @@ __global__ void k_bor_assemble(int ne, int mmax, int m, double k, const double2 
     const int nm = mmax + 2;
     const int am = abs(m), am1 = abs(m - 1), ap1 = abs(m + 1);
     const double km2 = 1.0 / (k * k);
+    const double C = k * 376.730313668 * 2.0 * GRIM_PI;  // C = j k eta 2 pi (times j below)
+    const double beta = momk ? (1.0 - alpha) * 376.730313668 : 0.0;
     double2 total = make_double2(0.0, 0.0);
     for (int ri = 0; ri < 2; ++ri) {
         const int fr = red_full[2 * r + ri];
@@ -243,24 +491,21 @@ __global__ void k_bor_assemble(int ne, int mmax, int m, double k, const double2 
             if (fc < 0) continue;
             const double2 wc = red_w[2 * c + cj];
             const int nj = fc % nn, cc = fc / nn;
-            double2 z = make_double2(0.0, 0.0);
+            double2 z = make_double2(0.0, 0.0), zk = z;
+            double mass = 0.0;
             // element pairs (e, f) with e in {ni-1, ni}, f in {nj-1, nj}
             for (int de = 0; de < 2; ++de) {
                 const int e = ni - 1 + de;
                 if (e < 0 || e >= ne) continue;
                 const int a = 1 - de;  // node ni is node index a of element e (e = ni-1 -> a = 1)
-                const double tre = (nodes[2 * e + 2] - nodes[2 * e]) /
-                                   hypot(nodes[2 * e + 2] - nodes[2 * e], nodes[2 * e + 3] - nodes[2 * e + 1]);
-                const double tze = (nodes[2 * e + 3] - nodes[2 * e + 1]) /
-                                   hypot(nodes[2 * e + 2] - nodes[2 * e], nodes[2 * e + 3] - nodes[2 * e + 1]);
+                const double dre = nodes[2 * e + 2] - nodes[2 * e], dze = nodes[2 * e + 3] - nodes[2 * e + 1];
+                const double Le = hypot(dre, dze), tre = dre / Le, tze = dze / Le;
                 for (int df = 0; df < 2; ++df) {
                     const int f = nj - 1 + df;
                     if (f < 0 || f >= ne) continue;
                     const int b = 1 - df;
-                    const double trf = (nodes[2 * f + 2] - nodes[2 * f]) /
-                                       hypot(nodes[2 * f + 2] - nodes[2 * f], nodes[2 * f + 3] - nodes[2 * f + 1]);
-                    const double tzf = (nodes[2 * f + 3] - nodes[2 * f + 1]) /
-                                       hypot(nodes[2 * f + 2] - nodes[2 * f], nodes[2 * f + 3] - nodes[2 * f + 1]);
+                    const double drf = nodes[2 * f + 2] - nodes[2 * f], dzf = nodes[2 * f + 3] - nodes[2 * f + 1];
+                    const double Lf = hypot(drf, dzf), trf = drf / Lf, tzf = dzf / Lf;
                     const int s = 2 * a + b;
                     const double2 *base = mom + ((int64_t)e * ne + f) * nm * BOR_SLOTS;
                     const double2 A0 = base[am * BOR_SLOTS + s];
@@ -288,17 +533,41 @@ __global__ void k_bor_assemble(int ne, int mmax, int m, double k, const double2 
                     }
                     z.x += v.x;
                     z.y += v.y;
+                    if (momk) {
+                        // K of quadrant uv (tt, tf, ft, ff); odd quadrants change sign with m
+                        const int uv = 2 * ci + cc;
+                        const double sg = (m < 0 && (uv == 1 || uv == 2)) ? -1.0 : 1.0;
+                        const double2 kv =
+                            momk[(((int64_t)e * ne + f) * nm + am) * BOR_KSLOTS + 4 * uv + s];
+                        zk.x += sg * kv.x;
+                        zk.y += sg * kv.y;
+                        if (e == f && ci == cc) {
+                            // mass 2 pi int rho T_a T_b dt on element e (3-point Gauss)
+                            for (int ip = 0; ip < BOR_FAR_ORDER; ++ip) {
+                                double xg, wg;
+                                gl_node(BOR_FAR_ORDER, ip, xg, wg);
+                                const double sq = 0.5 * (xg + 1.0);
+                                const double rho = nodes[2 * e] + sq * dre;
+                                const double Ta = a ? sq : 1.0 - sq, Tb = b ? sq : 1.0 - sq;
+                                mass += 2.0 * GRIM_PI * (0.5 * wg * Le) * rho * Ta * Tb;
+                            }
+                        }
+                    }
                 }
             }
-            // conj(wr) * z * wc
-            const double2 t1 = make_double2(wr.x * z.x + wr.y * z.y, wr.x * z.y - wr.y * z.x);
+            // Z_full = alpha C j z + beta ((1/2) mass - 2 pi zk)
+            double2 v = make_double2(-alpha * C * z.y, alpha * C * z.x);
+            if (momk) {
+                v.x += beta * (0.5 * mass - 2.0 * GRIM_PI * zk.x);
+                v.y += beta * (-2.0 * GRIM_PI * zk.y);
+            }
+            // conj(wr) * v * wc
+            const double2 t1 = make_double2(wr.x * v.x + wr.y * v.y, wr.x * v.y - wr.y * v.x);
             total.x += t1.x * wc.x - t1.y * wc.y;
             total.y += t1.x * wc.y + t1.y * wc.x;
         }
     }
-    // scale j k eta 2 pi
-    const double s = k * 376.730313668 * 2.0 * GRIM_PI;
-    Z[(int64_t)c * ldz + r] = make_double2(-s * total.y, s * total.x);
+    Z[(int64_t)c * ldz + r] = total;
 }
 
 // J_m(x) for any integer m (J_{-m} = (-1)^m J_m), through CUDA's jn.
@@ -312,8 +581,9 @@ __device__ __forceinline__ double jn_signed(int m, double x) {
 // Reduced excitation (far = 0) or far-field weights (far = 1) for mode m.
 // Columns: [VV theta_0..n-1, HH theta_0..n-1].  One thread per (reduced row, column).
 __global__ void k_bor_excitation(int ne, const double *__restrict__ nodes, double k, int m, int nth,
-                                 const double *__restrict__ th_deg, int far, int nred, const int *__restrict__ red_full,
-                                 const double2 *__restrict__ red_w, double2 *__restrict__ V, int64_t ldv) {
+                                 const double *__restrict__ th_deg, int far, double alpha, int nred,
+                                 const int *__restrict__ red_full, const double2 *__restrict__ red_w,
+                                 double2 *__restrict__ V, int64_t ldv) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     const int col = blockIdx.y;
     if (r >= nred || col >= 2 * nth) return;
@@ -361,6 +631,18 @@ __global__ void k_bor_excitation(int ne, const double *__restrict__ nodes, doubl
                 } else {
                     if (comp == 0) ang = make_double2(tr * Is.x, tr * Is.y);
                     else ang = Ic;
+                }
+                if (!far && alpha != 1.0) {
+                    // eta0 <W, n x H_inc> (reference rhs_mfie_mode), weighted 1 - alpha
+                    double2 hm;
+                    if (!hh) {
+                        if (comp == 0) hm = Ic;
+                        else hm = make_double2(-tr * Is.x, -tr * Is.y);
+                    } else {
+                        if (comp == 0) hm = make_double2(ct * Is.x, ct * Is.y);
+                        else hm = make_double2(tr * ct * Ic.x - tz * st * I0.x, tr * ct * Ic.y - tz * st * I0.y);
+                    }
+                    ang = make_double2(alpha * ang.x + (1.0 - alpha) * hm.x, alpha * ang.y + (1.0 - alpha) * hm.y);
                 }
                 double sp, cp;
                 sincos(k * z * ct, &sp, &cp);

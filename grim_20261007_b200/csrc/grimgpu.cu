@@ -1938,45 +1938,121 @@ extern "C" int64_t grim_bor_moments_size(int ne, int mmax) {
     return (int64_t)ne * ne * (mmax + 2) * BOR_SLOTS * (int64_t)sizeof(double2);
 }
 
-static size_t bor_smem(int nxi_max) { return (size_t)nxi_max * (sizeof(double2) + sizeof(double)) + BOR_MAX_MODES * sizeof(double2); }
+extern "C" int64_t grim_bor_mfie_moments_size(int ne, int mmax) {
+    return (int64_t)ne * ne * (mmax + 2) * BOR_KSLOTS * (int64_t)sizeof(double2);
+}
+
+template <bool MFIE>
+static size_t bor_tail_smem(int nm) {
+    const int NV = MFIE ? 5 : 1, nsl = MFIE ? BOR_ALL_SLOTS : BOR_SLOTS, S = BOR_THREADS / nm;
+    return sizeof(double2) * ((size_t)S * nm * NV + (size_t)nm * NV + (size_t)nm * nsl) + sizeof(double) * nsl;
+}
+
+template <bool MFIE>
+static int bor_moments_launch(grim_context *h, int ne, const double *nodes, const unsigned char *d_cls, double k,
+                              int mmax, int nxi_cap, const std::vector<BorItem> &items,
+                              const std::vector<int4> &pairs, const double *d_rule, double2 *mom, double2 *momk) {
+    const int nm = mmax + 2, NV = MFIE ? 5 : 1, nsl = MFIE ? BOR_ALL_SLOTS : BOR_SLOTS;
+    // far pairs
+    const size_t far_smem = (size_t)nxi_cap * sizeof(double) + (size_t)NV * BOR_FAR_CHUNK * sizeof(double2) +
+                            bor_tail_smem<MFIE>(nm);
+    GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_bor_far<MFIE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)far_smem));
+    k_bor_far<MFIE><<<dim3(ne, ne), BOR_THREADS, far_smem, h->stream>>>(ne, nodes, d_cls, k, mmax, nxi_cap, mom,
+                                                                          momk);
+    GRIM_CHECK_LAUNCH(h, MFIE ? "k_bor_far<cfie>" : "k_bor_far<efie>");
+    if (items.empty()) return GRIM_OK;
+    void *p_items = nullptr, *p_pairs = nullptr, *p_part = nullptr;
+    GRIM_TRY(grim_workspace(h, "bor_items", items.size() * sizeof(BorItem), &p_items));
+    GRIM_TRY(grim_workspace(h, "bor_pairs", pairs.size() * sizeof(int4), &p_pairs));
+    GRIM_TRY(grim_workspace(h, "bor_part", items.size() * (size_t)nm * nsl * sizeof(double2), &p_part));
+    GRIM_CHECK_CUDA(cudaMemcpyAsync(p_items, items.data(), items.size() * sizeof(BorItem), cudaMemcpyHostToDevice,
+                                    h->stream));
+    GRIM_CHECK_CUDA(cudaMemcpyAsync(p_pairs, pairs.data(), pairs.size() * sizeof(int4), cudaMemcpyHostToDevice,
+                                    h->stream));
+    const int chn = nm <= 64 ? 64 : 32;
+    const size_t near_smem = (size_t)chn * nm * sizeof(double2) + (size_t)NV * chn * sizeof(double2) +
+                             (size_t)chn * sizeof(double) + bor_tail_smem<MFIE>(nm);
+    GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_bor_near<MFIE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)near_smem));
+    k_bor_near<MFIE><<<(unsigned)items.size(), BOR_THREADS, near_smem, h->stream>>>(
+        (const BorItem *)p_items, nodes, d_rule, k, mmax, chn, (double2 *)p_part);
+    GRIM_CHECK_LAUNCH(h, MFIE ? "k_bor_near<cfie>" : "k_bor_near<efie>");
+    k_bor_near_reduce<MFIE><<<(unsigned)pairs.size(), 256, 0, h->stream>>>(ne, mmax, (const int4 *)p_pairs,
+                                                                           (const double2 *)p_part, mom, momk);
+    GRIM_CHECK_LAUNCH(h, "k_bor_near_reduce");
+    return GRIM_OK;
+}
 
 extern "C" int grim_bor_moments(grim_handle_t h, int ne, const double *nodes, double k, int mmax, int nxi_max,
-                                void *mom) {
+                                const unsigned char *pair_class, int n_rule, const double *rule,
+                                const int *rule_start, void *mom, void *mom_k) {
     if (!h || ne < 2 || !nodes || !mom || !(k > 0) || mmax < 0 || mmax + 2 > BOR_MAX_MODES || nxi_max < 32 ||
-        nxi_max > BOR_MAX_NXI || ne > 65535)
+        nxi_max > BOR_MAX_NXI || ne > 65535 || !pair_class || n_rule <= 0 || !rule || !rule_start)
         return grim_fail(GRIM_ERR_ARGUMENT, "grim_bor_moments: bad arguments");
+    // rule_start[0..4]: point ranges of the self (diagonal), adjacent f = e + 1, adjacent
+    // f = e - 1 and regular near rules in `rule` (s, s', w per point pair)
+    for (int i = 0; i < 4; ++i)
+        if (rule_start[i] < 0 || rule_start[i] >= rule_start[i + 1] || rule_start[i + 1] > n_rule)
+            return grim_fail(GRIM_ERR_ARGUMENT, "grim_bor_moments: bad rule ranges");
+    std::vector<BorItem> items;
+    std::vector<int4> pairs;
+    for (int e = 0; e < ne; ++e)
+        for (int f = 0; f < ne; ++f) {
+            const unsigned char c = pair_class[(size_t)e * ne + f];
+            if (c > 2) return grim_fail(GRIM_ERR_ARGUMENT, "grim_bor_moments: pair class must be 0, 1 or 2");
+            if (c == 1 && std::abs(e - f) > 1)
+                return grim_fail(GRIM_ERR_ARGUMENT, "grim_bor_moments: class 1 is for self and adjacent pairs");
+            if (c == 0) continue;
+            const int kind = c == 2 ? 3 : (e == f ? 0 : (f == e + 1 ? 1 : 2));
+            const int first = (int)items.size();
+            for (int r = rule_start[kind]; r < rule_start[kind + 1]; r += BOR_NEAR_CHUNK)
+                items.push_back(BorItem{e, f, r, std::min(r + BOR_NEAR_CHUNK, rule_start[kind + 1])});
+            pairs.push_back(make_int4(e, f, first, (int)items.size()));
+        }
     DeviceGuard g(h->device);
-    const size_t smem = bor_smem(std::max(nxi_max, BOR_NEAR_XI));
-    GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_bor_moments, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    // the kernel clamps per-pair sample counts to BOR_MAX_NXI; the caller's nxi_max bounds them here
-    dim3 grid(ne, ne);
-    k_bor_moments<<<grid, 128, smem, h->stream>>>(ne, nodes, k, mmax, std::max(nxi_max, BOR_NEAR_XI), (double2 *)mom);
-    GRIM_CHECK_LAUNCH(h, "k_bor_moments");
+    void *p_cls = nullptr, *p_rule = nullptr;
+    GRIM_TRY(grim_workspace(h, "bor_cls", (size_t)ne * ne, &p_cls));
+    GRIM_TRY(grim_workspace(h, "bor_rule", (size_t)3 * n_rule * sizeof(double), &p_rule));
+    GRIM_CHECK_CUDA(cudaMemcpyAsync(p_cls, pair_class, (size_t)ne * ne, cudaMemcpyHostToDevice, h->stream));
+    GRIM_CHECK_CUDA(cudaMemcpyAsync(p_rule, rule, (size_t)3 * n_rule * sizeof(double), cudaMemcpyHostToDevice,
+                                    h->stream));
+    // a multiple of 32 keeps the shared-memory sections after the sample table 16-byte aligned
+    const int cap = std::min(BOR_MAX_NXI, (std::max(32, nxi_max) + 31) / 32 * 32);
+    int s;
+    if (mom_k)
+        s = bor_moments_launch<true>(h, ne, nodes, (const unsigned char *)p_cls, k, mmax, cap, items, pairs,
+                                     (const double *)p_rule, (double2 *)mom, (double2 *)mom_k);
+    else
+        s = bor_moments_launch<false>(h, ne, nodes, (const unsigned char *)p_cls, k, mmax, cap, items, pairs,
+                                      (const double *)p_rule, (double2 *)mom, nullptr);
+    GRIM_TRY(s);
+    // the host vectors above are freed on return: wait for the uploads that read them
+    GRIM_CHECK_CUDA(cudaStreamSynchronize(h->stream));
     return GRIM_OK;
 }
 
 extern "C" int grim_bor_assemble(grim_handle_t h, int ne, const double *nodes, double k, int mmax, int m,
-                                 const void *mom, int nred, const int *red_full, const void *red_w, void *Z,
-                                 int64_t ldz) {
-    if (!h || ne < 2 || !nodes || !mom || !red_full || !red_w || !Z || nred <= 0 || ldz < nred || abs(m) > mmax)
+                                 const void *mom, const void *mom_k, double alpha, int nred, const int *red_full,
+                                 const void *red_w, void *Z, int64_t ldz) {
+    if (!h || ne < 2 || !nodes || !mom || !red_full || !red_w || !Z || nred <= 0 || ldz < nred || abs(m) > mmax ||
+        !(alpha >= 0.0 && alpha <= 1.0) || (!mom_k && alpha != 1.0))
         return grim_fail(GRIM_ERR_ARGUMENT, "grim_bor_assemble: bad arguments");
     DeviceGuard g(h->device);
     dim3 grid(ceil_div(nred, 16), ceil_div(nred, 16)), block(16, 16);
-    k_bor_assemble<<<grid, block, 0, h->stream>>>(ne, mmax, m, k, (const double2 *)mom, nred, red_full,
-                                                  (const double2 *)red_w, nodes, (double2 *)Z, ldz);
+    k_bor_assemble<<<grid, block, 0, h->stream>>>(ne, mmax, m, k, (const double2 *)mom, (const double2 *)mom_k, alpha,
+                                                  nred, red_full, (const double2 *)red_w, nodes, (double2 *)Z, ldz);
     GRIM_CHECK_LAUNCH(h, "k_bor_assemble");
     return GRIM_OK;
 }
 
 extern "C" int grim_bor_excitation(grim_handle_t h, int ne, const double *nodes, double k, int m, int nth,
-                                   const double *thetas_deg, int far, int nred, const int *red_full, const void *red_w,
-                                   void *V, int64_t ldv) {
+                                   const double *thetas_deg, int far, double alpha, int nred, const int *red_full,
+                                   const void *red_w, void *V, int64_t ldv) {
     if (!h || ne < 2 || !nodes || !thetas_deg || !red_full || !red_w || !V || nth <= 0 || 2 * nth > 65535 ||
-        nred <= 0 || ldv < nred)
+        nred <= 0 || ldv < nred || !(alpha >= 0.0 && alpha <= 1.0))
         return grim_fail(GRIM_ERR_ARGUMENT, "grim_bor_excitation: bad arguments");
     DeviceGuard g(h->device);
     dim3 grid(ceil_div(nred, 128), 2 * nth);
-    k_bor_excitation<<<grid, 128, 0, h->stream>>>(ne, nodes, k, m, nth, thetas_deg, far, nred, red_full,
+    k_bor_excitation<<<grid, 128, 0, h->stream>>>(ne, nodes, k, m, nth, thetas_deg, far, alpha, nred, red_full,
                                                   (const double2 *)red_w, (double2 *)V, ldv);
     GRIM_CHECK_LAUNCH(h, "k_bor_excitation");
     return GRIM_OK;

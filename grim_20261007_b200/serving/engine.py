@@ -233,8 +233,10 @@ class ServingEngine:
                 return {'id': req.id, 'amplitude': amp, 'telemetry': tele}
             from ..bor.solver import solve_bor_device, mode_limits
             mcap, _ = mode_limits(req.k, float(np.max(req.geometry[:, 0])), req.angles, req.n_modes)
-            F, tele = solve_bor_device(req.geometry, req.k, req.angles, mcap,
-                                       precision=req.precision, tol=self.tol, ctx=slot.ctx)
+            closed = req.geometry[0, 0] == 0.0 and req.geometry[-1, 0] == 0.0
+            # the reference's default formulation: the CFIE for a closed body, else the EFIE
+            F, tele = solve_bor_device(req.geometry, req.k, req.angles, mcap, precision=req.precision,
+                                       tol=self.tol, ctx=slot.ctx, alpha=0.5 if closed else 1.0)
             nth = len(req.angles)
             return {'id': req.id, 'amp_vv': F[:nth], 'amp_hh': F[nth:], 'telemetry': tele}
 

@@ -230,27 +230,41 @@ int grim_zgesv_batched(grim_handle_t h, int n, int nrhs, const double *A, int ld
                        int precision_mode, int *info);
 int grim_last_solve_info(grim_handle_t h, grim_solve_info *out);
 
-/* ---- body of revolution (PEC EFIE per azimuthal mode) -----------------------------
- * nodes: 2*(ne+1) doubles (rho, z) of the generatrix, +z pole to -z pole.
- * grim_bor_moments: mode-independent element-pair moments of the modal Green's function
- *   for n = 0..mmax+1 (reference bor/kernels.py:632 banded_modal_kernels and
- *   bor/bor_stream_kernel.c:332-418 samplers); mom holds grim_bor_moments_size(ne, mmax)
- *   bytes; nxi_max bounds the per-pair azimuthal sample count (<= 8192).
- * grim_bor_assemble: reduced mode-m EFIE matrix (reference bor/solver.py:1769 assemble_mode
- *   with the pole reduction of :2428 reduce_pole_operator); red_full[2*nred] lists the
- *   full components (t: node, phi: (ne+1)+node; -1 unused) of each reduced function and
- *   red_w[2*nred] (complex128) their weights.
- * grim_bor_excitation: reduced right-hand sides (far = 0) or far-field weights (far = 1),
- *   columns [VV theta..., HH theta...] (reference bor/solver.py:2558 rhs_vv_hh_batch,
+/* ---- body of revolution (PEC EFIE / MFIE / CFIE per azimuthal mode) ----------------
+ * nodes: 2*(ne+1) doubles (rho, z) of the generatrix, +z pole to -z pole (device).
+ * grim_bor_moments: mode-independent element-pair moments for n = 0..mmax+1 of the modal
+ *   Green's function (mom, grim_bor_moments_size bytes) and, when mom_k is not NULL, of
+ *   the four modal MFIE brackets (mom_k, grim_bor_mfie_moments_size bytes)
+ *   (reference bor/kernels.py:632 banded_modal_kernels, :896,996 the MFIE brackets,
+ *   bor/bor_stream_kernel.c:332-418,915-1045 samplers and near rules).
+ *   pair_class (host, ne*ne bytes): 0 far (3 x 3 Gauss points, trapezoid in xi), 1 self or
+ *   adjacent, 2 other near pairs (reference bor/solver.py:1520-1580 near-pair routing);
+ *   near pairs take their point pairs from rule (host, n_rule x (s, s', w)) in the ranges
+ *   rule_start[0..4]: self, adjacent f = e + 1, adjacent f = e - 1, other near
+ *   (reference bor/solver.py:718-806 graded cells, :843 regular cells).
+ *   nxi_max bounds the far pairs' azimuthal sample count (<= 8192).
+ * grim_bor_assemble: reduced mode-m matrix alpha C EFIE + (1 - alpha) eta0 MFIE
+ *   (reference bor/solver.py:1769 assemble_mode, :1962 assemble_mfie_mode, CFIE
+ *   :4285-4301, pole reduction :2428 reduce_pole_operator); 0 <= alpha <= 1 (0: the MFIE
+ *   alone); mom_k = NULL for the EFIE alone, with alpha = 1; red_full[2*nred] lists the full components (t: node, phi:
+ *   (ne+1)+node; -1 unused) of each reduced function and red_w[2*nred] (complex128) their
+ *   weights.
+ * grim_bor_excitation: reduced right-hand sides alpha <W, E_inc> + (1 - alpha) eta0
+ *   <W, n x H_inc> (far = 0) or far-field weights (far = 1), columns [VV theta...,
+ *   HH theta...] (reference bor/solver.py:2558 rhs_vv_hh_batch, :2048 rhs_mfie_mode,
  *   :2608 farfield_vv_hh_batch).
  * grim_bor_farfield_accumulate: amp[c] += sum_r W[r, c] X[r, c]. */
 int64_t grim_bor_moments_size(int ne, int mmax);
-int grim_bor_moments(grim_handle_t h, int ne, const double *nodes, double k, int mmax, int nxi_max, void *mom);
+int64_t grim_bor_mfie_moments_size(int ne, int mmax);
+int grim_bor_moments(grim_handle_t h, int ne, const double *nodes, double k, int mmax, int nxi_max,
+                     const unsigned char *pair_class, int n_rule, const double *rule, const int *rule_start,
+                     void *mom, void *mom_k);
 int grim_bor_assemble(grim_handle_t h, int ne, const double *nodes, double k, int mmax, int m, const void *mom,
-                      int nred, const int *red_full, const void *red_w, void *Z, int64_t ldz);
+                      const void *mom_k, double alpha, int nred, const int *red_full, const void *red_w, void *Z,
+                      int64_t ldz);
 int grim_bor_excitation(grim_handle_t h, int ne, const double *nodes, double k, int m, int nth,
-                        const double *thetas_deg, int far, int nred, const int *red_full, const void *red_w,
-                        void *V, int64_t ldv);
+                        const double *thetas_deg, int far, double alpha, int nred, const int *red_full,
+                        const void *red_w, void *V, int64_t ldv);
 int grim_bor_farfield_accumulate(grim_handle_t h, int nred, int ncol, const void *W, int64_t ldw, const void *X,
                                  int64_t ldx, void *amp);
 

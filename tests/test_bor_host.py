@@ -1,9 +1,12 @@
 """BoR host logic (no GPU): pole reduction map, mode limits, sample counts."""
+import os
+
 import numpy as np
 
 from grim_20261007_b200 import synthetic as S
 from grim_20261007_b200.bor import solver as B
 from oracle import bor as OB
+from tests.conftest import GOLDEN
 
 
 def _q_from_map(rf, rw, nred, nn):
@@ -37,13 +40,28 @@ def test_nxi_bound_matches_oracle_rule():
     k, mmax = 3.0, 8
     got = B.nxi_max(pts, k, mmax)
     body = OB.Body(pts)
+    cls = body.pair_classes()
     asm_pts = B.far_points(pts)
     best = 0
     ne = len(pts) - 1
     el = np.repeat(np.arange(ne), 3)
     for i in range(len(asm_pts)):
         for j in range(len(asm_pts)):
-            if abs(el[i] - el[j]) >= 2:
+            if cls[el[i], el[j]] == 0:
                 r0 = np.hypot(*(asm_pts[i] - asm_pts[j]))
                 best = max(best, int(OB.n_xi(k, asm_pts[i, 0], asm_pts[j, 0], r0, mmax)))
     assert got == best
+
+
+def test_pair_routing_and_point_rules_match_oracle():
+    """The product's near-pair routing and point sets equal the oracle's restatement of the
+    reference's (graded cells for self / adjacent pairs, 12 x 12 Gauss for the others)."""
+    from grim_20261007_b200.bor import rules
+    G = np.load(os.path.join(GOLDEN, 'ref_bor_modes.npz'))
+    for pts in (S.sphere_generatrix(1.0, 20), S.ogive_generatrix(3.0, 22.0, 30), G['graded_points']):
+        np.testing.assert_array_equal(rules.pair_classes(pts), OB.Body(pts).pair_classes())
+    rule, starts = rules.near_rules()
+    parts = [OB.cell_points('diag'), OB.cell_points('corner10'), OB.cell_points('corner01'), OB.regular_points()]
+    for i, (s, sq, w) in enumerate(parts):
+        np.testing.assert_array_equal(rule[starts[i]:starts[i + 1]], np.stack([s, sq, w], axis=1))
+    assert starts[-1] == len(rule)
