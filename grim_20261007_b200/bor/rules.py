@@ -52,15 +52,20 @@ def pair_classes(nodes):
     cls = np.zeros((ne, ne), dtype=np.uint8)
     cls[apart <= NEAR_SPAN] = 2
     cls[apart <= 1] = 1
-    for r0 in range(0, ne, 512):
-        r1 = min(ne, r0 + 512)
-        ar, br = a[r0:r1, None], b[r0:r1, None]
-        dist = np.minimum(np.minimum(_segment_distance(ar, a[None], b[None]), _segment_distance(br, a[None], b[None])),
-                          np.minimum(_segment_distance(a[None], ar, br), _segment_distance(b[None], ar, br)))
-        gap = np.maximum(DIRECT_SCALE * np.maximum(rho_e[r0:r1, None], rho_e[None, :]),
-                         2.0 * np.maximum(lengths[r0:r1, None], lengths[None, :]))
-        block = cls[r0:r1]
-        block[(apart[r0:r1] > NEAR_SPAN) & (dist <= gap)] = 2
+    # candidates by the centre-distance lower bound (the reference's prefilter), then the
+    # exact segment distance
+    mids = 0.5 * (a + b)
+    half = 0.5 * lengths
+    d = np.hypot(mids[:, None, 0] - mids[None, :, 0], mids[:, None, 1] - mids[None, :, 1])
+    gap = np.maximum(DIRECT_SCALE * np.maximum(rho_e[:, None], rho_e[None, :]),
+                     2.0 * np.maximum(lengths[:, None], lengths[None, :]))
+    cand = np.nonzero((apart > NEAR_SPAN) & (d - half[:, None] - half[None, :] <= gap))
+    if len(cand[0]):
+        e, f = cand
+        dist = np.minimum(np.minimum(_segment_distance(a[e], a[f], b[f]), _segment_distance(b[e], a[f], b[f])),
+                          np.minimum(_segment_distance(a[f], a[e], b[e]), _segment_distance(b[f], a[e], b[e])))
+        near = dist <= gap[e, f]
+        cls[e[near], f[near]] = 2
     return cls
 
 

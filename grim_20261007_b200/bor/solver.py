@@ -164,7 +164,8 @@ class BorDevice:
             size = int(self.ctx.lib.grim_bor_mfie_moments_size(self.ne, self.mmax))
             self.momk = torch.empty(size // 16, dtype=torch.complex128, device='cuda')
         self.cls = np.ascontiguousarray(pair_classes(self.nodes))
-        self.nxi = nxi_max(self.nodes, self.k, self.mmax, self.cls)
+        # far pairs size their own sample counts (at most MAX_NXI); no table is staged
+        self.nxi = MAX_NXI
         rule, starts = _near_rules()
         _lib.check(self.ctx.lib.grim_bor_moments(self.ctx.h, self.ne, ptr(self.nodes_dev), self.k, self.mmax, self.nxi,
                                                  self.cls.ctypes.data, len(rule), rule.ctypes.data,
@@ -332,7 +333,7 @@ def solve_bor_device(points, k, thetas_deg, mmax, precision='double', tol=None, 
             amp += 2.0 * part
         else:
             amp += part
-    tele = {'modes': 2 * mmax + 1, 'mode_systems_solved': len(modes), 'max_backward_error': 0.0, 'nxi_max': dev.nxi,
+    tele = {'modes': 2 * mmax + 1, 'mode_systems_solved': len(modes), 'max_backward_error': 0.0,
             'refinement_steps': max(t['refinement_steps'] for _p, t in outs)}
     fallbacks = sum(1 for _p, t in outs if t['fp64_fallback'])
     if fallbacks:
@@ -432,5 +433,4 @@ def solve_bor(points, freq_hz, thetas_deg, formulation="auto", cfie_alpha=0.5, z
         'precision': requested_precision(),
         'warnings': [],
         'mode_bandwidth': int(bandwidth),
-        'nxi_max': int(tele['nxi_max']),
     }

@@ -38,7 +38,7 @@
 #define BOR_THREADS 256
 #define BOR_FAR_CHUNK 256   // far-pair xi samples staged per pass
 #define BOR_NEAR_CHUNK 64   // point pairs per near work item
-#define BOR_XI_CORE 16      // Gauss points of the near rule's sinh core
+#define BOR_XI_CORE 20      // Gauss points of the near rule's sinh core
 #define BOR_XI_PANEL 16     // Gauss points per panel of the near rule
 
 struct BorPt {
@@ -185,101 +185,129 @@ __device__ __forceinline__ void bor_fold_pair(int nm, int S, double2 *red, doubl
     __syncthreads();
 }
 
-// grid = (ne, ne), BOR_THREADS threads; pairs with cls != 0 return at once.
-// dynamic smem: ctab[nxi_cap] doubles, then chunk samples, red, sum, fac, acc (host-sized).
+// grid = (ne, ne), BOR_THREADS threads; pairs with cls != 0 return at once.  Thread
+// (n = t % nm, grp = t / nm) sums mode n over the samples i = grp (mod S) of each point pair,
+// with e^{j n xi_i} carried by rotation and re-anchored exactly every 32 of them; the groups'
+// sums of each of the 9 point pairs are reduced in shared memory, and the 36 slot moments
+// are formed once at the end.
+// dynamic smem: samples [NV][BOR_FAR_CHUNK], red[S][nm][NV], sums[9][nm][NV], fac[9][nsl].
 template <bool MFIE>
-__global__ void __launch_bounds__(BOR_THREADS)
+__global__ void __launch_bounds__(BOR_THREADS, 2)
 k_bor_far(int ne, const double *__restrict__ nodes, const unsigned char *__restrict__ cls, double k, int mmax,
           int nxi_cap, double2 *__restrict__ mom, double2 *__restrict__ momk) {
     constexpr int NV = MFIE ? 5 : 1, nsl = MFIE ? BOR_ALL_SLOTS : BOR_SLOTS;
+    constexpr int NPP = BOR_FAR_ORDER * BOR_FAR_ORDER;
     const int e = blockIdx.x, f = blockIdx.y;
     if (cls[(int64_t)e * ne + f] != 0) return;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int nm = mmax + 2, S = BOR_THREADS / nm;
-    double *ctab = reinterpret_cast<double *>(smem_raw);
-    double2 *chunk = reinterpret_cast<double2 *>(ctab + nxi_cap);  // [NV][BOR_FAR_CHUNK]
-    double2 *red = chunk + NV * BOR_FAR_CHUNK;
-    double2 *sum = red + S * nm * NV;
-    double2 *acc = sum + nm * NV;
-    double *fac = reinterpret_cast<double *>(acc + nm * nsl);
+    double2 *chunk = reinterpret_cast<double2 *>(smem_raw);  // [NV][BOR_FAR_CHUNK]
+    double2 *red = chunk + NV * BOR_FAR_CHUNK;                // [S][nm][NV]
+    double2 *sums = red + S * nm * NV;                         // [NPP][nm][NV]
+    double *fac = reinterpret_cast<double *>(sums + NPP * nm * NV);  // [NPP][nsl]
     const int t = threadIdx.x, n = t % nm, grp = t / nm;
-    for (int i = t; i < nm * nsl; i += blockDim.x) acc[i] = make_double2(0.0, 0.0);
-    for (int ip = 0; ip < BOR_FAR_ORDER; ++ip) {
-        double xo, wo;
+    for (int pp = 0; pp < NPP; ++pp) {
+        const int ip = pp / BOR_FAR_ORDER, iq = pp % BOR_FAR_ORDER;
+        double xo, wo, xs, wsq;
         gl_node(BOR_FAR_ORDER, ip, xo, wo);
+        gl_node(BOR_FAR_ORDER, iq, xs, wsq);
         const BorPt p = bor_point(nodes, e, 0.5 * (xo + 1.0), 0.5 * wo);
-        for (int iq = 0; iq < BOR_FAR_ORDER; ++iq) {
-            double xs, wsq;
-            gl_node(BOR_FAR_ORDER, iq, xs, wsq);
-            const BorPt q = bor_point(nodes, f, 0.5 * (xs + 1.0), 0.5 * wsq);
-            const BorPair pr = bor_pair(k, p, q);
-            const int N = min(bor_nxi(k, p.rho, q.rho, sqrt(pr.d2), mmax), nxi_cap);
-            const double dxi = 2.0 * GRIM_PI / N;
-            for (int i = t; i < N; i += blockDim.x) ctab[i] = cospi(2.0 * i / (double)N);
-            if (t < nsl) fac[t] = bor_factor(p, q, t);
-            double2 sg = make_double2(0.0, 0.0), s1 = sg, s2 = sg, s3 = sg, s4 = sg;
-            for (int i0 = 0; i0 < N; i0 += BOR_FAR_CHUNK) {
-                const int cnt = min(BOR_FAR_CHUNK, N - i0);
-                __syncthreads();
-                for (int j = t; j < cnt; j += blockDim.x) {
-                    const int i = i0 + j;
-                    double2 g, F[4];
-                    bor_sample<MFIE>(pr, sinpi(i / (double)N), sinpi(2.0 * i / (double)N), dxi, g, F);
-                    chunk[j] = g;
-                    if constexpr (MFIE) {
-#pragma unroll
-                        for (int u = 0; u < 4; ++u) chunk[(1 + u) * BOR_FAR_CHUNK + j] = F[u];
-                    }
-                }
-                __syncthreads();
-                if (grp < S) {
-                    // cos(n xi_i) = ctab[n i mod N], sin(n xi_i) = ctab[(n i - N/4) mod N]
-                    int idx = (int)(((int64_t)n * (i0 + grp)) % N);
-                    const int step = (int)(((int64_t)n * S) % N);
-                    for (int j = grp; j < cnt; j += S) {
-                        const double c = ctab[idx];
-                        const double2 v = chunk[j];
-                        sg.x += v.x * c;
-                        sg.y += v.y * c;
-                        if constexpr (MFIE) {
-                            int is = idx - N / 4;
-                            if (is < 0) is += N;
-                            const double sn = ctab[is];
-                            const double2 f0 = chunk[BOR_FAR_CHUNK + j], f1 = chunk[2 * BOR_FAR_CHUNK + j];
-                            const double2 f2 = chunk[3 * BOR_FAR_CHUNK + j], f3 = chunk[4 * BOR_FAR_CHUNK + j];
-                            s1.x += f0.x * c;  s1.y += f0.y * c;
-                            s2.x += f1.x * sn; s2.y += f1.y * sn;
-                            s3.x += f2.x * sn; s3.y += f2.y * sn;
-                            s4.x += f3.x * c;  s4.y += f3.y * c;
-                        }
-                        idx += step;
-                        if (idx >= N) idx -= N;
-                    }
-                }
-            }
-            if (grp < S) {
-                double2 *r = red + (grp * nm + n) * NV;
-                r[0] = sg;
+        const BorPt q = bor_point(nodes, f, 0.5 * (xs + 1.0), 0.5 * wsq);
+        if (t < nsl) fac[pp * nsl + t] = bor_factor(p, q, t);
+        const BorPair pr = bor_pair(k, p, q);
+        const int N = min(bor_nxi(k, p.rho, q.rho, sqrt(pr.d2), mmax), nxi_cap);
+        const double dxi = 2.0 * GRIM_PI / N;
+        double2 sg = make_double2(0.0, 0.0), s1 = sg, s2 = sg, s3 = sg, s4 = sg;
+        // rotation by n S samples (n < 128, N <= 8192: 32-bit phase indices)
+        double rs, rc;
+        sincospi(2.0 * (double)((n * S) % N) / N, &rs, &rc);
+        for (int i0 = 0; i0 < N; i0 += BOR_FAR_CHUNK) {
+            const int cnt = min(BOR_FAR_CHUNK, N - i0);
+            __syncthreads();
+            for (int j = t; j < cnt; j += blockDim.x) {
+                const int i = i0 + j;
+                double sh, ch;
+                sincospi(i / (double)N, &sh, &ch);
+                double2 g, F[4];
+                bor_sample<MFIE>(pr, sh, 2.0 * sh * ch, dxi, g, F);
+                chunk[j] = g;
                 if constexpr (MFIE) {
-                    r[1] = s1;
-                    r[2] = s2;
-                    r[3] = s3;
-                    r[4] = s4;
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) chunk[(1 + u) * BOR_FAR_CHUNK + j] = F[u];
                 }
             }
             __syncthreads();
-            bor_fold_pair<MFIE>(nm, S, red, sum, fac, acc);
+            if (grp < S) {
+                // samples i = grp (mod S); e^{j n xi_i} anchored exactly every 32 of them
+                int j = (grp - i0 % S + S) % S;
+                while (j < cnt) {
+                    double zs, zc;
+                    sincospi(2.0 * (double)((n * (i0 + j)) % N) / N, &zs, &zc);
+                    double2 z = make_double2(zc, zs);
+                    const int jend = min(cnt, j + 32 * S);
+#pragma unroll(MFIE ? 2 : 4)
+                    for (; j < jend; j += S) {
+                        const double2 v = chunk[j];
+                        sg.x += v.x * z.x;
+                        sg.y += v.y * z.x;
+                        if constexpr (MFIE) {
+                            const double2 f0 = chunk[BOR_FAR_CHUNK + j], f1 = chunk[2 * BOR_FAR_CHUNK + j];
+                            const double2 f2 = chunk[3 * BOR_FAR_CHUNK + j], f3 = chunk[4 * BOR_FAR_CHUNK + j];
+                            s1.x += f0.x * z.x; s1.y += f0.y * z.x;
+                            s2.x += f1.x * z.y; s2.y += f1.y * z.y;
+                            s3.x += f2.x * z.y; s3.y += f2.y * z.y;
+                            s4.x += f3.x * z.x; s4.y += f3.y * z.x;
+                        }
+                        z = make_double2(z.x * rc - z.y * rs, z.x * rs + z.y * rc);
+                    }
+                }
+            }
+        }
+        if (grp < S) {
+            double2 *r = red + (grp * nm + n) * NV;
+            r[0] = sg;
+            if constexpr (MFIE) {
+                r[1] = s1;
+                r[2] = s2;
+                r[3] = s3;
+                r[4] = s4;
+            }
+        }
+        __syncthreads();
+        for (int i = t; i < nm * NV; i += blockDim.x) {
+            double2 v = make_double2(0.0, 0.0);
+            for (int gq = 0; gq < S; ++gq) {
+                const double2 r = red[gq * nm * NV + i];
+                v.x += r.x;
+                v.y += r.y;
+            }
+            sums[pp * nm * NV + i] = v;
         }
     }
+    __syncthreads();
     const int64_t base = ((int64_t)e * ne + f) * nm;
     for (int i = t; i < nm * nsl; i += blockDim.x) {
         const int nn_ = i / nsl, slot = i - nn_ * nsl;
-        if (slot < BOR_SLOTS) mom[(base + nn_) * BOR_SLOTS + slot] = acc[i];
-        else momk[(base + nn_) * BOR_KSLOTS + slot - BOR_SLOTS] = acc[i];
+        const int v = slot < BOR_SLOTS ? 0 : 1 + ((slot - BOR_SLOTS) >> 2);
+        double2 a = make_double2(0.0, 0.0);
+        for (int pp = 0; pp < NPP; ++pp) {
+            const double fc = fac[pp * nsl + slot];
+            const double2 sv = sums[(pp * nm + nn_) * NV + v];
+            a.x += fc * sv.x;
+            a.y += fc * sv.y;
+        }
+        if (slot < BOR_SLOTS) {
+            mom[(base + nn_) * BOR_SLOTS + slot] = a;
+        } else {
+            // odd brackets: K = -j (sine sum)
+            if (v == 2 || v == 3) a = make_double2(a.y, -a.x);
+            momk[(base + nn_) * BOR_KSLOTS + slot - BOR_SLOTS] = a;
+        }
     }
 }
 
-// Near-pair xi rule on [0, pi] for delta = R0 / c, span = 2 pi / (nmax + k c + 1):
+// Near-pair xi rule on [0, pi] for delta = R0 / c, span = 4 pi / (nmax + k c + 1) (two
+// periods of the fastest oscillation per panel):
 // a sinh-mapped Gauss core on [0, a], a = min(4 delta, span, pi), then panels
 // [a 2^g, a 2^(g+1)] while a 2^g < span, then panels of length span up to pi.
 struct BorRule {
@@ -337,21 +365,32 @@ struct BorItem {
     int e, f, r0, r1;  // element pair and its point-pair range in the rule table
 };
 
+#define BOR_NEAR_EVAL 256  // near-rule samples evaluated per pass (one per thread)
+
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
 // grid = number of near work items, BOR_THREADS threads.  rule[3 i .. 3 i + 2] = (s, s', w).
-// Writes the item's moments to part[item][n][slot] (nm x nsl complex).
-// dynamic smem: rot[chn * nm] (e^{j n xi} of the staged samples), samples [NV][chn], xi[chn],
-// then red, sum, fac, acc as in k_bor_far.
+// Writes the item's moments to part[item][n][slot] (nm x nsl complex).  Per point pair the
+// rule's samples are evaluated BOR_NEAR_EVAL at a time (one per thread, with e^{j xi} and
+// e^{j Q xi}, Q = ceil(nm / 4)); rows e^{j n xi} of chr samples at a time are then built by
+// rotation (four threads per sample, one quarter of the orders each) and summed by the
+// (mode, group) threads.
+// dynamic smem: smp[NV][BOR_NEAR_EVAL], z1[BOR_NEAR_EVAL], zq[BOR_NEAR_EVAL],
+// rot[chr][P] (P = nm rounded up to odd: conflict-free row writes), then red, sum, acc, fac.
 template <bool MFIE>
-__global__ void __launch_bounds__(BOR_THREADS)
+__global__ void __launch_bounds__(BOR_THREADS, 2)
 k_bor_near(const BorItem *__restrict__ items, const double *__restrict__ nodes, const double *__restrict__ rule,
-           double k, int mmax, int chn, double2 *__restrict__ part) {
+           double k, int mmax, int chr, double2 *__restrict__ part) {
     constexpr int NV = MFIE ? 5 : 1, nsl = MFIE ? BOR_ALL_SLOTS : BOR_SLOTS;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int nm = mmax + 2, S = BOR_THREADS / nm;
-    double2 *rot = reinterpret_cast<double2 *>(smem_raw);  // [chn][nm]
-    double2 *smp = rot + chn * nm;                         // [NV][chn]
-    double *sxi = reinterpret_cast<double *>(smp + NV * chn);
-    double2 *red = reinterpret_cast<double2 *>(sxi + chn);
+    const int nm = mmax + 2, S = BOR_THREADS / nm, P = nm | 1, Q = (nm + 3) / 4;
+    double2 *smp = reinterpret_cast<double2 *>(smem_raw);  // [NV][BOR_NEAR_EVAL]
+    double2 *sz1 = smp + NV * BOR_NEAR_EVAL;
+    double2 *szq = sz1 + BOR_NEAR_EVAL;
+    double2 *rot = szq + BOR_NEAR_EVAL;                     // [chr][P]
+    double2 *red = rot + chr * P;
     double2 *sum = red + S * nm * NV;
     double2 *acc = sum + nm * NV;
     double *fac = reinterpret_cast<double *>(acc + nm * nsl);
@@ -363,62 +402,68 @@ k_bor_near(const BorItem *__restrict__ items, const double *__restrict__ nodes, 
         const BorPt q = bor_point(nodes, it.f, rule[3 * ipp + 1], 1.0);
         const BorPair pr = bor_pair(k, p, q);
         const double c = sqrt(p.rho * q.rho);
-        const BorRule rl = bor_rule(sqrt(pr.d2) / c, 2.0 * GRIM_PI / ((mmax + 1) + k * c + 1.0));
+        const BorRule rl = bor_rule(sqrt(pr.d2) / c, 4.0 * GRIM_PI / ((mmax + 1) + k * c + 1.0));
         const int na = bor_rule_count(rl);
         if (t < nsl) fac[t] = bor_factor(p, q, t);
         double2 sg = make_double2(0.0, 0.0), s1 = sg, s2 = sg, s3 = sg, s4 = sg;
-        for (int j0 = 0; j0 < na; j0 += chn) {
-            const int cnt = min(chn, na - j0);
+        for (int j0 = 0; j0 < na; j0 += BOR_NEAR_EVAL) {
+            const int cnt = min(BOR_NEAR_EVAL, na - j0);
             __syncthreads();
             for (int j = t; j < cnt; j += blockDim.x) {
                 double xi, w;
                 bor_rule_node(rl, j0 + j, xi, w);
-                double sh, ch, sx, cx;
+                double sh, ch;
                 sincos(0.5 * xi, &sh, &ch);
-                sincos(xi, &sx, &cx);
                 double2 g, F[4];
-                bor_sample<MFIE>(pr, sh, sx, w, g, F);
+                bor_sample<MFIE>(pr, sh, 2.0 * sh * ch, w, g, F);
                 smp[j] = g;
                 if constexpr (MFIE) {
 #pragma unroll
-                    for (int u = 0; u < 4; ++u) smp[(1 + u) * chn + j] = F[u];
+                    for (int u = 0; u < 4; ++u) smp[(1 + u) * BOR_NEAR_EVAL + j] = F[u];
                 }
-                sxi[j] = xi;
+                // e^{j xi} and e^{j Q xi} (binary powers)
+                const double2 z1 = make_double2(1.0 - 2.0 * sh * sh, 2.0 * sh * ch);
+                double2 zq = make_double2(1.0, 0.0), b = z1;
+                for (int e2 = Q; e2 > 0; e2 >>= 1) {
+                    if (e2 & 1) zq = cmul(zq, b);
+                    b = cmul(b, b);
+                }
+                sz1[j] = z1;
+                szq[j] = zq;
             }
-            __syncthreads();
-            // e^{j n xi_j}: each of 4 threads per sample starts one quarter of the orders
-            // with sincos and rotates through it
-            {
-                const int q4 = (nm + 3) / 4;
-                for (int task = t; task < 4 * cnt; task += blockDim.x) {
-                    const int j = task % cnt, quarter = task / cnt;
-                    const int n0 = quarter * q4, n1 = min(nm, n0 + q4);
+            for (int s0 = 0; s0 < cnt; s0 += chr) {
+                const int sc = min(chr, cnt - s0);
+                __syncthreads();
+                for (int task = t; task < 4 * sc; task += blockDim.x) {
+                    const int jj = task % sc, quarter = task / sc;
+                    const int n0 = quarter * Q, n1 = min(nm, n0 + Q);
                     if (n0 >= n1) continue;
-                    const double xi = sxi[j];
-                    double s0, c0, sst, cst;
-                    sincos(n0 * xi, &s0, &c0);
-                    sincos(xi, &sst, &cst);
-                    double2 z = make_double2(c0, s0);
+                    const double2 z1 = sz1[s0 + jj], zq = szq[s0 + jj];
+                    double2 z = make_double2(1.0, 0.0);
+                    for (int r = 0; r < quarter; ++r) z = cmul(z, zq);
+                    double2 *row = rot + jj * P;
                     for (int nn_ = n0; nn_ < n1; ++nn_) {
-                        rot[j * nm + nn_] = z;
-                        z = make_double2(z.x * cst - z.y * sst, z.x * sst + z.y * cst);
+                        row[nn_] = z;
+                        z = cmul(z, z1);
                     }
                 }
-            }
-            __syncthreads();
-            if (grp < S) {
-                for (int j = grp; j < cnt; j += S) {
-                    const double2 z = rot[j * nm + n];
-                    const double2 v = smp[j];
-                    sg.x += v.x * z.x;
-                    sg.y += v.y * z.x;
-                    if constexpr (MFIE) {
-                        const double2 f0 = smp[chn + j], f1 = smp[2 * chn + j];
-                        const double2 f2 = smp[3 * chn + j], f3 = smp[4 * chn + j];
-                        s1.x += f0.x * z.x; s1.y += f0.y * z.x;
-                        s2.x += f1.x * z.y; s2.y += f1.y * z.y;
-                        s3.x += f2.x * z.y; s3.y += f2.y * z.y;
-                        s4.x += f3.x * z.x; s4.y += f3.y * z.x;
+                __syncthreads();
+                if (grp < S) {
+#pragma unroll 4
+                    for (int jj = grp; jj < sc; jj += S) {
+                        const double2 z = rot[jj * P + n];
+                        const int j = s0 + jj;
+                        const double2 v = smp[j];
+                        sg.x += v.x * z.x;
+                        sg.y += v.y * z.x;
+                        if constexpr (MFIE) {
+                            const double2 f0 = smp[BOR_NEAR_EVAL + j], f1 = smp[2 * BOR_NEAR_EVAL + j];
+                            const double2 f2 = smp[3 * BOR_NEAR_EVAL + j], f3 = smp[4 * BOR_NEAR_EVAL + j];
+                            s1.x += f0.x * z.x; s1.y += f0.y * z.x;
+                            s2.x += f1.x * z.y; s2.y += f1.y * z.y;
+                            s3.x += f2.x * z.y; s3.y += f2.y * z.y;
+                            s4.x += f3.x * z.x; s4.y += f3.y * z.x;
+                        }
                     }
                 }
             }

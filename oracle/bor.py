@@ -46,10 +46,11 @@ Quadrature, as the reference's:
   12 x 12 Gauss tensor rule (``bor/solver.py:843``);
 * near pairs' xi integrals: this restatement's own rule on [0, pi] (using the parity of
   each integrand), converged far below the reference's 2e-8 agreement test
-  (``bor/kernels.py:18``): a sinh-mapped Gauss core xi = delta sinh(v) on [0, a]
-  (delta = R0 / c, a = min(4 delta, Delta, pi)), then Gauss panels [a 2^g, a 2^(g+1)]
-  while a 2^g < Delta = 2 pi / (n_max + k c + 1), and panels of length Delta from there
-  up to pi (the last one cut at pi).
+  (``bor/kernels.py:18``): a 20-point sinh-mapped Gauss core xi = delta sinh(v) on [0, a]
+  (delta = R0 / c, a = min(4 delta, Delta, pi)), then 16-point Gauss panels
+  [a 2^g, a 2^(g+1)] while a 2^g < Delta = 4 pi / (n_max + k c + 1) (two periods of the
+  fastest oscillation), and panels of length Delta from there up to pi (the last one cut
+  at pi).
 
 Parity pinned against the reference's own per-mode matrices and solves
 (``tests/golden/ref_bor_modes.npz``, ``tests/golden/ref_bor_sphere.npz``).
@@ -69,7 +70,7 @@ CELL_DEPTH = 4
 REGULAR_ORDER = 12
 NEAR_SPAN = 2
 DIRECT_SCALE = 1.001 * 8.0 * 2.0 * math.pi / 8192
-XI_CORE = 16
+XI_CORE = 20
 XI_PANEL = 16
 
 
@@ -211,7 +212,7 @@ def near_xi_rule(delta, nmax, kc):
     per group."""
     delta = np.atleast_1d(np.asarray(delta, dtype=np.float64))
     kc = np.broadcast_to(np.asarray(kc, dtype=np.float64), delta.shape)
-    span = 2.0 * math.pi / (nmax + kc + 1.0)
+    span = 4.0 * math.pi / (nmax + kc + 1.0)
     a = np.minimum(np.minimum(4.0 * delta, span), math.pi)
     # panel ends: a 2^g while below span (lengths doubling), then a 2^G + u span, up to pi
     geo = np.zeros(delta.shape, dtype=np.int64)
