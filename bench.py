@@ -173,7 +173,7 @@ def run_bor(args):
            'formulation': 'cfie'}
     res = {}
     for prec in ('double', 'mixed'):
-        solve_bor_device(gen, k, th[:8], 4, precision=prec, alpha=0.5)  # warm-up
+        solve_bor_device(gen, k, th, 40, precision=prec, alpha=0.5)  # warm-up at the timed size (workspaces)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         F, tele = solve_bor_device(gen, k, th, 40, precision=prec, alpha=0.5)

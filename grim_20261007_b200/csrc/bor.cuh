@@ -623,12 +623,40 @@ __device__ __forceinline__ double jn_signed(int m, double x) {
     return ((-m) & 1) ? -v : v;
 }
 
-// Reduced excitation (far = 0) or far-field weights (far = 1) for mode m.
+// Per (aspect, Gauss point): J_m, J_{m-1}, J_{m+1} at k rho sin(theta) and the axial phase
+// e^{j k z cos(theta)} -- evaluated once and shared by every row that the point touches.
+// tab[((it * ne + e) * BOR_FAR_ORDER + ip) * 5 + {0..4}] = (J_m, J_{m-1}, J_{m+1}, cos, sin).
+__global__ void k_bor_bessel(int ne, const double *__restrict__ nodes, double k, int m, int nth,
+                             const double *__restrict__ th_deg, double *__restrict__ tab) {
+    const int pidx = blockIdx.x * blockDim.x + threadIdx.x;
+    const int it = blockIdx.y;
+    if (pidx >= ne * BOR_FAR_ORDER || it >= nth) return;
+    const int e = pidx / BOR_FAR_ORDER, ip = pidx % BOR_FAR_ORDER;
+    double st, ct;
+    sincospi(th_deg[it] / 180.0, &st, &ct);
+    double xg, wg;
+    gl_node(BOR_FAR_ORDER, ip, xg, wg);
+    const double s = 0.5 * (xg + 1.0);
+    const double r0 = nodes[2 * e], z0 = nodes[2 * e + 1];
+    const double rho = r0 + s * (nodes[2 * e + 2] - r0), z = z0 + s * (nodes[2 * e + 3] - z0);
+    const double x = k * rho * st;
+    double *o = tab + ((int64_t)it * ne * BOR_FAR_ORDER + pidx) * 5;
+    o[0] = jn_signed(m, x);
+    o[1] = jn_signed(m - 1, x);
+    o[2] = jn_signed(m + 1, x);
+    double sp, cp;
+    sincos(k * z * ct, &sp, &cp);
+    o[3] = cp;
+    o[4] = sp;
+}
+
+// Reduced excitation (far = 0) or far-field weights (far = 1) for mode m, from the
+// k_bor_bessel table of the same (m, aspects).
 // Columns: [VV theta_0..n-1, HH theta_0..n-1].  One thread per (reduced row, column).
-__global__ void k_bor_excitation(int ne, const double *__restrict__ nodes, double k, int m, int nth,
-                                 const double *__restrict__ th_deg, int far, double alpha, int nred,
-                                 const int *__restrict__ red_full, const double2 *__restrict__ red_w,
-                                 double2 *__restrict__ V, int64_t ldv) {
+__global__ void k_bor_excitation(int ne, const double *__restrict__ nodes, int m, int nth,
+                                 const double *__restrict__ th_deg, const double *__restrict__ tab, int far,
+                                 double alpha, int nred, const int *__restrict__ red_full,
+                                 const double2 *__restrict__ red_w, double2 *__restrict__ V, int64_t ldv) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     const int col = blockIdx.y;
     if (r >= nred || col >= 2 * nth) return;
@@ -648,16 +676,16 @@ __global__ void k_bor_excitation(int ne, const double *__restrict__ nodes, doubl
             const int e = node - 1 + de;
             if (e < 0 || e >= ne) continue;
             const int a = 1 - de;
-            const double r0 = nodes[2 * e], z0 = nodes[2 * e + 1], dr = nodes[2 * e + 2] - r0, dz = nodes[2 * e + 3] - z0;
+            const double r0 = nodes[2 * e], dr = nodes[2 * e + 2] - r0, dz = nodes[2 * e + 3] - nodes[2 * e + 1];
             const double L = hypot(dr, dz), tr = dr / L, tz = dz / L;
             for (int ip = 0; ip < BOR_FAR_ORDER; ++ip) {
                 double xg, wg;
                 gl_node(BOR_FAR_ORDER, ip, xg, wg);
                 const double s = 0.5 * (xg + 1.0);
-                const double rho = r0 + s * dr, z = z0 + s * dz, w = 0.5 * wg * L;
+                const double rho = r0 + s * dr, w = 0.5 * wg * L;
                 const double T = a == 0 ? 1.0 - s : s;
-                const double x = k * rho * st;
-                const double jm = jn_signed(m, x), jm1 = jn_signed(m - 1, x), jp1 = jn_signed(m + 1, x);
+                const double *tb = tab + (((int64_t)it * ne + e) * BOR_FAR_ORDER + ip) * 5;
+                const double jm = tb[0], jm1 = tb[1], jp1 = tb[2];
                 // j^m, j^(m-1), j^(m+1) as unit complex numbers
                 const int q0 = ((m % 4) + 4) % 4, qm = (((m - 1) % 4) + 4) % 4, qp = (((m + 1) % 4) + 4) % 4;
                 const double2 u0 = make_double2(q0 == 0 ? 1 : (q0 == 2 ? -1 : 0), q0 == 1 ? 1 : (q0 == 3 ? -1 : 0));
@@ -689,8 +717,7 @@ __global__ void k_bor_excitation(int ne, const double *__restrict__ nodes, doubl
                     }
                     ang = make_double2(alpha * ang.x + (1.0 - alpha) * hm.x, alpha * ang.y + (1.0 - alpha) * hm.y);
                 }
-                double sp, cp;
-                sincos(k * z * ct, &sp, &cp);
+                const double cp = tb[3], sp = tb[4];
                 const double f = rho * w * T;
                 const double2 ph = make_double2(cp * f, sp * f);
                 sum.x += ph.x * ang.x - ph.y * ang.y;

@@ -2054,9 +2054,16 @@ extern "C" int grim_bor_excitation(grim_handle_t h, int ne, const double *nodes,
         nred <= 0 || ldv < nred || !(alpha >= 0.0 && alpha <= 1.0))
         return grim_fail(GRIM_ERR_ARGUMENT, "grim_bor_excitation: bad arguments");
     DeviceGuard g(h->device);
+    void *p_tab = nullptr;
+    // sized in steps of 512 aspects so that a handle rarely regrows it between requests
+    GRIM_TRY(grim_workspace(h, "bor_bessel", (size_t)5 * BOR_FAR_ORDER * ne * (size_t)(ceil_div(nth, 512) * 512) *
+                                                 sizeof(double), &p_tab));
+    k_bor_bessel<<<dim3(ceil_div(BOR_FAR_ORDER * ne, 128), nth), 128, 0, h->stream>>>(ne, nodes, k, m, nth, thetas_deg,
+                                                                                      (double *)p_tab);
+    GRIM_CHECK_LAUNCH(h, "k_bor_bessel");
     dim3 grid(ceil_div(nred, 128), 2 * nth);
-    k_bor_excitation<<<grid, 128, 0, h->stream>>>(ne, nodes, k, m, nth, thetas_deg, far, alpha, nred, red_full,
-                                                  (const double2 *)red_w, (double2 *)V, ldv);
+    k_bor_excitation<<<grid, 128, 0, h->stream>>>(ne, nodes, m, nth, thetas_deg, (const double *)p_tab, far, alpha,
+                                                  nred, red_full, (const double2 *)red_w, (double2 *)V, ldv);
     GRIM_CHECK_LAUNCH(h, "k_bor_excitation");
     return GRIM_OK;
 }
