@@ -378,7 +378,8 @@ __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
 // rotation (four threads per sample, one quarter of the orders each) and summed by the
 // (mode, group) threads.
 // dynamic smem: smp[NV][BOR_NEAR_EVAL], z1[BOR_NEAR_EVAL], zq[BOR_NEAR_EVAL],
-// rot[chr][P] (P = nm rounded up to odd: conflict-free row writes), then red, sum, acc, fac.
+// rot[chr][P] (P = nm rounded up to odd: conflict-free row writes; the groups' partial
+// sums red[S][nm][NV] reuse it once a point pair's rows are consumed), then sum, acc, fac.
 template <bool MFIE>
 __global__ void __launch_bounds__(BOR_THREADS, 2)
 k_bor_near(const BorItem *__restrict__ items, const double *__restrict__ nodes, const double *__restrict__ rule,
@@ -390,8 +391,8 @@ k_bor_near(const BorItem *__restrict__ items, const double *__restrict__ nodes, 
     double2 *sz1 = smp + NV * BOR_NEAR_EVAL;
     double2 *szq = sz1 + BOR_NEAR_EVAL;
     double2 *rot = szq + BOR_NEAR_EVAL;                     // [chr][P]
-    double2 *red = rot + chr * P;
-    double2 *sum = red + S * nm * NV;
+    double2 *red = rot;                                     // [S][nm][NV], after the rows
+    double2 *sum = rot + max(chr * P, S * nm * NV);
     double2 *acc = sum + nm * NV;
     double *fac = reinterpret_cast<double *>(acc + nm * nsl);
     const BorItem it = items[blockIdx.x];
@@ -468,6 +469,7 @@ k_bor_near(const BorItem *__restrict__ items, const double *__restrict__ nodes, 
                 }
             }
         }
+        __syncthreads();  // every thread is done with the rows that red overwrites
         if (grp < S) {
             double2 *r = red + (grp * nm + n) * NV;
             r[0] = sg;

@@ -1970,9 +1970,11 @@ static int bor_moments_launch(grim_context *h, int ne, const double *nodes, cons
                                     h->stream));
     GRIM_CHECK_CUDA(cudaMemcpyAsync(p_pairs, pairs.data(), pairs.size() * sizeof(int4), cudaMemcpyHostToDevice,
                                     h->stream));
-    const int chr = nm <= 64 ? 32 : 16;
-    const size_t near_smem = sizeof(double2) * ((size_t)(NV + 2) * BOR_NEAR_EVAL + (size_t)chr * (nm | 1)) +
-                             bor_tail_smem<MFIE>(nm);
+    const int chr = nm <= 64 ? 64 : 32;
+    // rows and the groups' partial sums share one region (red = S nm NV complex)
+    const size_t near_smem = sizeof(double2) * ((size_t)(NV + 2) * BOR_NEAR_EVAL +
+                                                std::max((size_t)chr * (nm | 1), (size_t)S * nm * NV)) +
+                             bor_tail_smem<MFIE>(nm) - sizeof(double2) * (size_t)S * nm * NV;
     GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_bor_near<MFIE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)near_smem));
     k_bor_near<MFIE><<<(unsigned)items.size(), BOR_THREADS, near_smem, h->stream>>>(
         (const BorItem *)p_items, nodes, d_rule, k, mmax, chr, (double2 *)p_part);
