@@ -161,15 +161,15 @@ def run_serving(args):
 
 
 def run_bor(args):
-    """Body-of-revolution ogive: 400 generatrix segments, |m| <= 40, 361 aspects, VV/HH, in
+    """Body-of-revolution ogive: 400 generatrix segments (--bor-segments), |m| <= 40, 361 aspects, VV/HH, in
     the reference's default formulation for a closed body (CFIE, alpha = 0.5)."""
     import torch
     from grim_20261007_b200 import synthetic as S
     from grim_20261007_b200.bor.solver import solve_bor_device
-    gen, length, half = S.ogive_case(args.seed, n=400)
+    gen, length, half = S.ogive_case(args.seed, n=args.bor_segments)
     k = 25.0 / max(1e-9, float(np.max(gen[:, 0])))  # k rho_max = 25 (the reference's |m| <= 40 converges)
     th = np.arange(361) * 0.5
-    out = {'length_m': length, 'half_angle_deg': half, 'k': k, 'segments': 400, 'modes': 81, 'aspects': 361,
+    out = {'length_m': length, 'half_angle_deg': half, 'k': k, 'segments': args.bor_segments, 'modes': 81, 'aspects': 361,
            'formulation': 'cfie'}
     res = {}
     for prec in ('double', 'mixed'):
@@ -428,6 +428,7 @@ def main():
     ap.add_argument('--serving', type=int, default=1, help='run the mixed request stream (p50/p99 latency)')
     ap.add_argument('--serving-requests', type=int, default=32)
     ap.add_argument('--bor', type=int, default=1, help='time the body-of-revolution ogive workload')
+    ap.add_argument('--bor-segments', type=int, default=400, help='generatrix segments of the BoR ogive')
     ap.add_argument('--sweep', type=int, default=256, help='frequencies of the airfoil sweep leg (0 = skip)')
     ap.add_argument('--autotune', type=int, default=1, help='tune the solve tile shapes for the workload first')
     ap.add_argument('--far-block', type=int, default=1, help='time the Galerkin far-block pass (boundary B2)')
