@@ -53,6 +53,31 @@ def test_mixed_solve_on_packed_block_panels(n, nrhs):
     assert st.initial_backward_error < 1e-4 and st.refinement_steps >= 1, st.as_dict()
 
 
+@pytest.mark.parametrize('n,nrhs', [(1100, 200), (2048, 720)])
+def test_mixed_solve_without_row_interchanges(n, nrhs):
+    """A diagonally dominant system factors on the certified path (no row interchanges, a
+    partial last panel block at n = 1100); the packed-panel solve and the refinement still
+    reach FP64."""
+    import ctypes
+    if not torch.cuda.is_available():
+        pytest.skip('no CUDA device')
+    from grim_20261007_b200 import _lib
+    from grim_20261007_b200.device import context, ptr, to_device_colmajor, to_host_matrix
+    ctx = context()
+    rng = np.random.default_rng(n + 1)
+    a = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n)) + 4.0 * np.sqrt(n) * np.eye(n)
+    b = rng.standard_normal((n, nrhs)) + 1j * rng.standard_normal((n, nrhs))
+    at = to_device_colmajor(a, torch.complex128)
+    bt = to_device_colmajor(b, torch.complex128)
+    info, st = ctypes.c_int(-1), _lib.GrimSolveInfo()
+    _lib.check(ctx.lib.grim_zgesv_mixed(ctx.h, n, nrhs, ptr(at), n, None, 0, ptr(bt), n, _lib.PREC_MIXED, 1e-12, 10,
+                                        ctypes.byref(info), ctypes.byref(st)))
+    x = to_host_matrix(bt)
+    ref = np.linalg.solve(a, b)
+    assert info.value == 0 and st.pivoted_panels == 0, st.as_dict()
+    assert np.max(np.abs(x - ref)) <= 1e-10 * np.max(np.abs(ref)), st.as_dict()
+
+
 @pytest.mark.parametrize('n,nrhs,complex64', [(300, 37, True), (300, 37, False), (1024, 130, True)])
 def test_integer_slice_residual_matches_fp64(n, nrhs, complex64):
     """R = B - A X on the int8 tensor cores agrees with an FP64 residual: to FP64 accuracy with 8
