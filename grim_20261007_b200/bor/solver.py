@@ -110,27 +110,6 @@ def far_points(nodes):
     return pts.reshape(-1, 2)
 
 
-def nxi_max(nodes, k, mmax, cls=None):
-    """Largest per-pair azimuthal sample count over far element pairs (class 0)."""
-    pts = far_points(nodes)
-    ne = len(nodes) - 1
-    if cls is None:
-        cls = pair_classes(nodes)
-    el = np.repeat(np.arange(ne), FAR_ORDER)
-    best = 32
-    for a in range(0, len(pts), 2048):
-        pa = pts[a:a + 2048]
-        ea = el[a:a + 2048]
-        far = cls[ea[:, None], el[None, :]] == 0
-        c = np.sqrt(pa[:, None, 0] * pts[None, :, 0])
-        r0 = np.hypot(pa[:, None, 0] - pts[None, :, 0], pa[:, None, 1] - pts[None, :, 1])
-        v = 1.5 * (2.0 * k * c + mmax + 2) + 40.0 * c / np.maximum(r0, 1e-300) + 16.0
-        n = 32 * np.ceil(v / 32.0)
-        if np.any(far):
-            best = max(best, int(np.max(n[far])))
-    return min(best, MAX_NXI)
-
-
 _RULES = None
 
 

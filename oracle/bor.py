@@ -499,9 +499,12 @@ def excitation(body, k, thetas_deg, m, far=False, kind='efie'):
 
 
 def solve(points, k, thetas_deg, mmax, formulation='efie', alpha=0.5):
-    """Monostatic VV/HH far-field amplitudes and sigma (m^2) summing modes -mmax..mmax."""
+    """Monostatic VV/HH far-field amplitudes and sigma (m^2) summing modes -mmax..mmax
+    (formulation 'efie', 'cfie' with weight alpha, or 'mfie' = alpha 0)."""
     body = Body(points)
-    cfie = formulation == 'cfie'
+    if formulation == 'mfie':
+        alpha = 0.0
+    cfie = formulation in ('cfie', 'mfie')
     asm = Assembler(body, k, mmax, mfie=cfie)
     nt = len(thetas_deg)
     F = np.zeros(2 * nt, dtype=np.complex128)

@@ -35,24 +35,6 @@ def test_mode_limits_follow_reference_rule():
     assert B.mode_limits(3.0, 1.0, [30.0], 10) == (10, 2)
 
 
-def test_nxi_bound_matches_oracle_rule():
-    pts = S.sphere_generatrix(1.0, 20)
-    k, mmax = 3.0, 8
-    got = B.nxi_max(pts, k, mmax)
-    body = OB.Body(pts)
-    cls = body.pair_classes()
-    asm_pts = B.far_points(pts)
-    best = 0
-    ne = len(pts) - 1
-    el = np.repeat(np.arange(ne), 3)
-    for i in range(len(asm_pts)):
-        for j in range(len(asm_pts)):
-            if cls[el[i], el[j]] == 0:
-                r0 = np.hypot(*(asm_pts[i] - asm_pts[j]))
-                best = max(best, int(OB.n_xi(k, asm_pts[i, 0], asm_pts[j, 0], r0, mmax)))
-    assert got == best
-
-
 def test_pair_routing_and_point_rules_match_oracle():
     """The product's near-pair routing and point sets equal the oracle's restatement of the
     reference's (graded cells for self / adjacent pairs, 12 x 12 Gauss for the others)."""

@@ -130,6 +130,22 @@ def test_interior_resonance_cfie(ctx):
             assert abs(db) < 0.05
 
 
+@pytest.mark.parametrize('form', ['cfie', 'mfie'])
+def test_cfie_and_mfie_solves_match_oracle(ctx, form):
+    """solve_bor with formulation 'cfie' / 'mfie' against the oracle's solve of the same
+    body (a 20-element ogive, |m| <= 5)."""
+    from grim_20261007_b200.bor.solver import solve_bor
+    pts = S.ogive_generatrix(3.0, 22.0, 20)
+    k = 3.0
+    th = [0.0, 40.0, 90.0, 155.0]
+    res = solve_bor(pts, k * S.C0 / (2 * np.pi), th, formulation=form, n_modes=5)
+    o = OB.solve(pts, k, th, 5, formulation=form)
+    assert res['formulation'] == form
+    for key in ('amp_vv', 'amp_hh'):
+        got = np.asarray(res[key])
+        assert np.max(np.abs(got - o[key])) <= 1e-9 * np.max(np.abs(o[key])), key
+
+
 def test_cfie_rejects_open_shells(ctx):
     from grim_20261007_b200.bor.solver import solve_bor
     pts = S.sphere_generatrix(1.0, 12)[:-2]  # ends off the axis
