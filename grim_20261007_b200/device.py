@@ -14,8 +14,9 @@ from __future__ import annotations
 import contextlib
 import contextvars
 import ctypes
+import queue
 import threading
-from concurrent.futures import ThreadPoolExecutor
+from concurrent.futures import Future
 
 import numpy as np
 import torch
@@ -91,6 +92,31 @@ def context(device=None):
 
 
 _busy = set()  # (device, index) of workers held by a running pool
+_threads = {}  # (device, index) -> task queue of the worker's host thread
+
+
+def _worker_queue(dev, index):
+    """Task queue of worker ``index``'s host thread (started on first use and kept, so a
+    pool call does not start and join threads).  A worker index is held by one pool at a
+    time (``_acquire``), so its thread runs one pool's loop at a time."""
+    with _ctx_lock:
+        q = _threads.get((dev, index))
+        if q is None:
+            q = queue.SimpleQueue()
+
+            def serve(q=q):
+                while True:
+                    fn, fut = q.get()
+                    if not fut.set_running_or_notify_cancel():
+                        continue
+                    try:
+                        fut.set_result(fn())
+                    except BaseException as exc:  # noqa: BLE001 - delivered to the pool's caller
+                        fut.set_exception(exc)
+
+            threading.Thread(target=serve, daemon=True, name=f'grim-worker-{dev}-{index}').start()
+            _threads[(dev, index)] = q
+    return q
 
 
 def _worker(dev, index):
@@ -241,8 +267,12 @@ def run_pool(fns, workers=None, costs=None, on_done=None, device=None):
             return done
 
     try:
-        with ThreadPoolExecutor(max_workers=workers) as ex:
-            events = list(ex.map(loop, range(workers)))
+        futs = []
+        for w in range(workers):
+            fut = Future()
+            _worker_queue(dev, held[w]).put((lambda w=w: loop(w), fut))
+            futs.append(fut)
+        events = [fut.result() for fut in futs]
     finally:
         _release(dev, held)
     for done in events:

@@ -414,14 +414,21 @@ def _sweep_many(snapshots, frequencies_ghz, elevations_deg, pols, geometry_units
     require_cuda()
     precision = requested_precision()
     mesh_list = [_MeshCache(snap, geometry_units, max_panels, mesh_reference_ghz) for snap in snapshots]
-    items, jobs, costs = [], [], []
+    items, jobs = [], []
     for si, meshes in enumerate(mesh_list):
         for pol in pols:
             for f in freqs:
                 items.append((si, pol, f))
                 jobs.append(lambda m=meshes, f=f, pol=pol: _solve_frequency(m, f, elevs, pol, precision, abort_event))
-                costs.append(_frequency_cost(snapshots[si], geometry_units, f, len(elevs)) if len(items) > 1 or
-                             len(freqs) > 1 else 1.0)
+    # longest-processing-time order needs costs only when the systems differ (more than one
+    # frequency or snapshot); each distinct (snapshot, frequency) is costed once
+    costs = None
+    if len(freqs) > 1 or len(snapshots) > 1:
+        per = {}
+        for si, _pol, f in items:
+            if (si, f) not in per:
+                per[(si, f)] = _frequency_cost(snapshots[si], geometry_units, f, len(elevs))
+        costs = [per[(si, f)] for si, _pol, f in items]
     total = len(jobs) * (len(elevs) + 1)
     progress_state = {'done': 0}
 
