@@ -103,6 +103,13 @@ SIGNATURES = [
                                   c_int, c_void_p, c_void_p, c_void_p, c_int64]),
     ('grim_bor_excitation', c_int, [c_void_p, c_int, c_void_p, c_double, c_int, c_int, c_void_p, c_int, c_double,
                                     c_int, c_void_p, c_void_p, c_void_p, c_int64]),
+    ('grim_bor_mirror_halves', c_int, [c_void_p, c_int, c_void_p, c_int64, c_int, c_void_p, c_void_p, c_void_p,
+                                       c_int, c_void_p, c_int, c_void_p, c_void_p, c_void_p]),
+    ('grim_bor_mirror_asymmetry', c_int, [c_void_p, c_int, c_void_p, c_int64, c_void_p, c_void_p, c_void_p]),
+    ('grim_bor_mirror_split', c_int, [c_void_p, c_int, c_void_p, c_int64, c_int, c_void_p, c_void_p, c_void_p, c_int,
+                                      c_void_p, c_int, c_void_p, c_void_p, c_void_p]),
+    ('grim_bor_mirror_join', c_int, [c_void_p, c_int, c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_int,
+                                     c_void_p, c_int, c_void_p, c_void_p, c_int64]),
     ('grim_bor_farfield_accumulate', c_int, [c_void_p, c_int, c_int, c_void_p, c_int64, c_void_p, c_int64, c_void_p]),
     ('grim_profile_enable', c_int, [c_void_p, c_int]),
     ('grim_profile_report', c_int, [c_void_p, c_char_p, c_int]),

@@ -102,6 +102,47 @@ def pole_map(nodes, m):
     return red_full.reshape(-1), red_w.reshape(-1), nred
 
 
+MIRROR_NODE_TOLERANCE = 1e-9
+MIRROR_ASYMMETRY_MAX = 1e-12
+
+
+def mirror_map(nodes, m):
+    """(target, sign) of the reduced unknowns of mode m when the generatrix is symmetric about
+    a plane normal to the axis, else None (reference ``bor/solver.py:3856`` ``mirror_map``):
+    the reflection z -> 2 z0 - z maps node i to node Nn - 1 - i, a reduced unknown to the same
+    component of the mirrored node, J_t with sign -1 (the tangent reverses) and J_phi with +1
+    (an |m| = 1 pole unknown carries its tied phi component along)."""
+    nodes = np.asarray(nodes, dtype=np.float64)
+    nn = len(nodes)
+    size = float(max(np.ptp(nodes[:, 1]), np.max(np.abs(nodes[:, 0])), 1e-300))
+    z0 = 0.5 * (nodes[0, 1] + nodes[-1, 1])
+    reflected = np.column_stack([nodes[::-1, 0], 2.0 * z0 - nodes[::-1, 1]])
+    if nn < 4 or float(np.max(np.abs(reflected - nodes))) > MIRROR_NODE_TOLERANCE * size:
+        return None
+    if (nodes[0, 0] == 0.0) != (nodes[-1, 0] == 0.0):
+        return None
+    rf, _rw, nred = pole_map(nodes, m)
+    prim = rf.reshape(-1, 2)[:, 0]
+    node, comp = prim % nn, prim // nn
+    lookup = np.full(2 * nn, -1, dtype=np.int64)
+    lookup[prim] = np.arange(nred)
+    target = lookup[comp * nn + (nn - 1 - node)]
+    if np.any(target < 0):
+        return None
+    return target.astype(np.int32), np.where(comp == 0, -1.0, 1.0)
+
+
+def mirror_parts(target, sign):
+    """Pairs (p1 < p2 = target[p1], s = sign[p2]) and fixed unknowns (fe: sign +1, fo: -1)."""
+    idx = np.arange(len(target))
+    paired = idx < target
+    p1 = idx[paired].astype(np.int32)
+    p2 = target[paired].astype(np.int32)
+    fixed = idx == target
+    return p1, p2, sign[p2].astype(np.float64), idx[fixed & (sign > 0)].astype(np.int32), \
+        idx[fixed & (sign < 0)].astype(np.int32)
+
+
 def far_points(nodes):
     x, w = np.polynomial.legendre.leggauss(FAR_ORDER)
     s = 0.5 * (x + 1.0)
@@ -160,6 +201,21 @@ class BorDevice:
             self._maps[key] = (torch.from_numpy(rf).to('cuda'), torch.from_numpy(rw).to('cuda'), nred)
         return self._maps[key]
 
+    def mirror(self, m):
+        """Device arrays of mode m's mirror map (``mirror_map``) or None."""
+        key = ('mirror', m if abs(m) == 1 else (0 if m == 0 else 2))
+        if key not in self._maps:
+            mp = mirror_map(self.nodes, m)
+            if mp is None:
+                self._maps[key] = None
+            else:
+                target, sign = mp
+                p1, p2, sg, fe, fo = mirror_parts(target, sign)
+                d = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to('cuda')
+                self._maps[key] = dict(target=d(target), sign=d(sign), p1=d(p1), p2=d(p2), s=d(sg), fe=d(fe),
+                                       fo=d(fo), k=len(p1), nfe=len(fe), nfo=len(fo))
+        return self._maps[key]
+
     def matrix(self, m, ctx=None):
         ctx = ctx or self.ctx
         rf, rw, nred = self.mode_map(m)
@@ -212,6 +268,76 @@ def _solve_mode(dev, m, th, precision, tol, ctx=None):
     return part, tele
 
 
+def _mirror_modes(dev, modes, Zs):
+    """Indices of the modes whose matrices are mirror-symmetric to MIRROR_ASYMMETRY_MAX
+    (relative to their largest entry): max |Z - R Z R| on the device, read in one go."""
+    ctx = context()
+    checks = []
+    for i, (m, Z) in enumerate(zip(modes, Zs)):
+        mp = dev.mirror(m)
+        if mp is None:
+            continue
+        out = torch.empty(2, dtype=torch.float64, device='cuda')
+        n = int(Z.shape[0])
+        _lib.check(ctx.lib.grim_bor_mirror_asymmetry(ctx.h, n, ptr(Z), n, ptr(mp['target']), ptr(mp['sign']),
+                                                     ptr(out)), 'grim_bor_mirror_asymmetry')
+        checks.append((i, out))
+    if not checks:
+        return []
+    vals = torch.stack([o for _i, o in checks]).cpu().numpy()
+    return [i for (i, _o), (d, a) in zip(checks, vals) if np.isfinite(d) and d <= MIRROR_ASYMMETRY_MAX * a]
+
+
+def _solve_mirror_grouped(dev, modes, Zs, Vs, workers):
+    """FP64 solves of mirror-symmetric mode systems through their even and odd halves
+    (reference ``bor/factor.py:37`` ``MirrorSplit``): the halves of every mode in one grouped
+    LU (a quarter of the LU work), then per mode the split right-hand sides, two half
+    solves and the join, on the worker pool.  The modes were checked symmetric to
+    MIRROR_ASYMMETRY_MAX, so the halves are the system itself to rounding and no
+    refinement against the full matrix is needed."""
+    from ..grouped import getrf_grouped
+    ctx = context()
+    halves = []
+    for m, Z in zip(modes, Zs):
+        mp = dev.mirror(m)
+        n = int(Z.shape[0])
+        ke, ko = mp['k'] + mp['nfe'], mp['k'] + mp['nfo']
+        He = torch.empty((ke, ke), dtype=torch.complex128, device='cuda')
+        Ho = torch.empty((ko, ko), dtype=torch.complex128, device='cuda')
+        _lib.check(ctx.lib.grim_bor_mirror_halves(ctx.h, n, ptr(Z), n, mp['k'], ptr(mp['p1']), ptr(mp['p2']),
+                                                  ptr(mp['s']), mp['nfe'], ptr(mp['fe']), mp['nfo'], ptr(mp['fo']),
+                                                  ptr(He), ptr(Ho)), 'grim_bor_mirror_halves')
+        halves += [He, Ho]
+    ipivs, infos, piv = getrf_grouped(halves)
+    for i, inf in enumerate(infos):
+        if inf:
+            raise _lib.GrimError(_lib.GRIM_ERR_SINGULAR, f'mirror half {i % 2} of mode {modes[i // 2]} is exactly '
+                                                         f'singular (info={inf})')
+
+    def job(j):
+        def run():
+            c = context()
+            mp = dev.mirror(modes[j])
+            V = Vs[j]
+            nrhs, n = int(V.shape[0]), int(V.shape[1])
+            ke, ko = mp['k'] + mp['nfe'], mp['k'] + mp['nfo']
+            Be = torch.empty((nrhs, ke), dtype=torch.complex128, device='cuda')
+            Bo = torch.empty((nrhs, ko), dtype=torch.complex128, device='cuda')
+            args = (mp['k'], ptr(mp['p1']), ptr(mp['p2']), ptr(mp['s']), mp['nfe'], ptr(mp['fe']), mp['nfo'],
+                    ptr(mp['fo']))
+            _lib.check(c.lib.grim_bor_mirror_split(c.h, nrhs, ptr(V), n, *args, ptr(Be), ptr(Bo)),
+                       'grim_bor_mirror_split')
+            for H, ipv, B, order in ((halves[2 * j], ipivs[2 * j], Be, ke), (halves[2 * j + 1], ipivs[2 * j + 1], Bo, ko)):
+                _lib.check(c.lib.grim_zgetrs(c.h, order, nrhs, ptr(H), order, ptr(ipv), ptr(B), order), 'grim_zgetrs')
+            _lib.check(c.lib.grim_bor_mirror_join(c.h, nrhs, ptr(Be), ptr(Bo), *args, ptr(V), n),
+                       'grim_bor_mirror_join')
+            return {'precision_mode': _lib.PREC_FP64, 'pivoted_panels': piv[2 * j] + piv[2 * j + 1], 'grouped': True,
+                    'mirror_halves': [ke, ko]}
+        return run
+
+    return run_pool([job(j) for j in range(len(modes))], workers=workers)
+
+
 def _solve_modes_grouped(dev, modes, th, precision, tol, workers):
     """All mode systems through one grouped LU (``grouped.solve_grouped``): assembly and
     excitations on the worker pool, one grouped factorization of every mode matrix, then
@@ -235,7 +361,18 @@ def _solve_modes_grouped(dev, modes, th, precision, tol, workers):
         tol = ops2d.MIXED_RCS_TOL
     torch.cuda.synchronize()
     t1 = time.perf_counter()
-    sts = solve_grouped(Zs, Vs, precision=precision, tol=tol, stop='berr', workers=workers)
+    mirrored = _mirror_modes(dev, modes, Zs) if precision == 'double' else []
+    sts = [None] * len(modes)
+    if mirrored:
+        for i, st in zip(mirrored, _solve_mirror_grouped(dev, [modes[i] for i in mirrored],
+                                                         [Zs[i] for i in mirrored], [Vs[i] for i in mirrored],
+                                                         workers)):
+            sts[i] = st
+    rest = [i for i in range(len(modes)) if sts[i] is None]
+    if rest:
+        for i, st in zip(rest, solve_grouped([Zs[i] for i in rest], [Vs[i] for i in rest], precision=precision,
+                                             tol=tol, stop='berr', workers=workers)):
+            sts[i] = st
     torch.cuda.synchronize()
     t2 = time.perf_counter()
     # stalled refinements (ill-conditioned modes): the reference's ladder to the double LU,

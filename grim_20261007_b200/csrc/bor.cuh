@@ -770,3 +770,109 @@ __global__ void k_bor_farfield_accumulate(int nred, int ncol, const double2 *__r
         }
     }
 }
+
+// ---- mirror-symmetric bodies: even / odd halves of a mode system (reference
+// bor/factor.py:37-116 MirrorSplit).  A body symmetric about a plane normal to the axis
+// maps reduced unknown u to target[u] with sign[u] (J_t changes sign, J_phi does not).
+// Pairs (p1 < p2 = target[p1], s = sign[p2]) and fixed unknowns (fe: sign +1, fo: sign -1)
+// give, with r = 1/sqrt(2), the even half over (r (u_p1 + s u_p2), u_fe) and the odd half
+// over (r (u_p1 - s u_p2), u_fo); when A = R A R they decouple exactly:
+//   H[:k,:k] = (a[p1,p1] + s a[p2,p2] s +- (a[p1,p2] s + s a[p2,p1])) / 2
+//   H[:k,k:] = (a[p1,f] +- s a[p2,f]) r,  H[k:,:k] = (a[f,p1] +- a[f,p2] s) r,  H[k:,k:] = a[f,f].
+struct BorMirror {
+    int k, nfe, nfo;
+    const int *p1, *p2, *fe, *fo;
+    const double *s;
+};
+
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 cscale(double2 a, double f) { return make_double2(a.x * f, a.y * f); }
+
+// grid over the (ke x ke) even and (ko x ko) odd halves; He, Ho column-major (ld ke, ko).
+__global__ void k_bor_mirror_halves(BorMirror mr, const double2 *__restrict__ Z, int64_t ldz, double2 *__restrict__ He,
+                                    double2 *__restrict__ Ho) {
+    const int i = blockIdx.x * 16 + threadIdx.x, j = blockIdx.y * 16 + threadIdx.y;
+    const int k = mr.k, ke = k + mr.nfe, ko = k + mr.nfo;
+    const double r = 0.7071067811865475244;
+    auto a = [&](int row, int col) { return Z[(int64_t)col * ldz + row]; };
+    for (int parity = 0; parity < 2; ++parity) {
+        const int m = parity ? ko : ke;
+        if (i >= m || j >= m) continue;
+        const double sg = parity ? -1.0 : 1.0;
+        const int *fx = parity ? mr.fo : mr.fe;
+        double2 v;
+        if (i < k && j < k) {
+            const int a1 = mr.p1[i], a2 = mr.p2[i], b1 = mr.p1[j], b2 = mr.p2[j];
+            const double si = mr.s[i], sj = mr.s[j];
+            const double2 common = cadd(a(a1, b1), cscale(a(a2, b2), si * sj));
+            const double2 cross = cadd(cscale(a(a1, b2), sj), cscale(a(a2, b1), si));
+            v = cscale(cadd(common, cscale(cross, sg)), 0.5);
+        } else if (i < k) {
+            const int f = fx[j - k];
+            v = cscale(cadd(a(mr.p1[i], f), cscale(a(mr.p2[i], f), sg * mr.s[i])), r);
+        } else if (j < k) {
+            const int f = fx[i - k];
+            v = cscale(cadd(a(f, mr.p1[j]), cscale(a(f, mr.p2[j]), sg * mr.s[j])), r);
+        } else {
+            v = a(fx[i - k], fx[j - k]);
+        }
+        (parity ? Ho : He)[(int64_t)j * m + i] = v;
+    }
+}
+
+// max over entries of |a - (R A R)| and of |a| (two non-negative doubles, as ordered bits).
+__global__ void k_bor_mirror_asym(int n, const double2 *__restrict__ Z, int64_t ldz, const int *__restrict__ target,
+                                  const double *__restrict__ sign, unsigned long long *__restrict__ out) {
+    const int i = blockIdx.x * 16 + threadIdx.x, j = blockIdx.y * 16 + threadIdx.y;
+    double d = 0.0, m = 0.0;
+    if (i < n && j < n) {
+        const double2 a = Z[(int64_t)j * ldz + i];
+        const double2 b = Z[(int64_t)target[j] * ldz + target[i]];
+        const double f = sign[i] * sign[j];
+        d = hypot(a.x - f * b.x, a.y - f * b.y);
+        m = hypot(a.x, a.y);
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+        d = fmax(d, __shfl_down_sync(0xffffffffu, d, off));
+        m = fmax(m, __shfl_down_sync(0xffffffffu, m, off));
+    }
+    if ((threadIdx.x + 16 * threadIdx.y) % 32 == 0) {
+        atomicMax(out, (unsigned long long)__double_as_longlong(d));
+        atomicMax(out + 1, (unsigned long long)__double_as_longlong(m));
+    }
+}
+
+// Right-hand sides (n x nrhs, ld ldb) into the even (ke x nrhs) and odd (ko x nrhs) parts.
+__global__ void k_bor_mirror_split(BorMirror mr, int nrhs, const double2 *__restrict__ B, int64_t ldb,
+                                   double2 *__restrict__ Be, double2 *__restrict__ Bo) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, c = blockIdx.y;
+    const int k = mr.k, ke = k + mr.nfe, ko = k + mr.nfo;
+    if (c >= nrhs) return;
+    const double r = 0.7071067811865475244;
+    const double2 *b = B + (int64_t)c * ldb;
+    if (i < ke) {
+        Be[(int64_t)c * ke + i] = i < k ? cscale(cadd(b[mr.p1[i]], cscale(b[mr.p2[i]], mr.s[i])), r) : b[mr.fe[i - k]];
+    }
+    if (i < ko) {
+        Bo[(int64_t)c * ko + i] = i < k ? cscale(cadd(b[mr.p1[i]], cscale(b[mr.p2[i]], -mr.s[i])), r) : b[mr.fo[i - k]];
+    }
+}
+
+// Solutions of the halves back to the n unknowns.
+__global__ void k_bor_mirror_join(BorMirror mr, int nrhs, const double2 *__restrict__ Ye,
+                                  const double2 *__restrict__ Yo, double2 *__restrict__ X, int64_t ldx) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, c = blockIdx.y;
+    const int k = mr.k, ke = k + mr.nfe, ko = k + mr.nfo;
+    if (c >= nrhs) return;
+    const double r = 0.7071067811865475244;
+    double2 *x = X + (int64_t)c * ldx;
+    const double2 *ye = Ye + (int64_t)c * ke, *yo = Yo + (int64_t)c * ko;
+    if (i < k) {
+        const double2 e = ye[i], o = yo[i];
+        x[mr.p1[i]] = cscale(cadd(e, o), r);
+        x[mr.p2[i]] = cscale(cadd(e, cscale(o, -1.0)), r * mr.s[i]);
+    } else if (i < ke && i - k < mr.nfe) {
+        x[mr.fe[i - k]] = ye[i];
+    }
+    if (i >= k && i < ko) x[mr.fo[i - k]] = yo[i];
+}

@@ -2081,5 +2081,69 @@ extern "C" int grim_bor_farfield_accumulate(grim_handle_t h, int nred, int ncol,
     return GRIM_OK;
 }
 
+// ---- mirror halves (reference bor/factor.py:37 MirrorSplit)
+static bool mirror_args_ok(int k, const int *p1, const int *p2, const double *s, int nfe, const int *fe, int nfo,
+                           const int *fo) {
+    return k >= 0 && nfe >= 0 && nfo >= 0 && k + nfe > 0 && k + nfo > 0 && (k == 0 || (p1 && p2 && s)) &&
+           (nfe == 0 || fe) && (nfo == 0 || fo);
+}
+
+extern "C" int grim_bor_mirror_halves(grim_handle_t h, int n, const void *Z, int64_t ldz, int k, const int *p1,
+                                      const int *p2, const double *s, int nfe, const int *fe, int nfo, const int *fo,
+                                      void *He, void *Ho) {
+    if (!h || n <= 0 || !Z || ldz < n || !He || !Ho || 2 * k + nfe + nfo != n ||
+        !mirror_args_ok(k, p1, p2, s, nfe, fe, nfo, fo))
+        return grim_fail(GRIM_ERR_ARGUMENT, "grim_bor_mirror_halves: bad arguments");
+    DeviceGuard g(h->device);
+    const BorMirror mr{k, nfe, nfo, p1, p2, fe, fo, s};
+    const int m = k + std::max(nfe, nfo);
+    k_bor_mirror_halves<<<dim3(ceil_div(m, 16), ceil_div(m, 16)), dim3(16, 16), 0, h->stream>>>(
+        mr, (const double2 *)Z, ldz, (double2 *)He, (double2 *)Ho);
+    GRIM_CHECK_LAUNCH(h, "k_bor_mirror_halves");
+    return GRIM_OK;
+}
+
+extern "C" int grim_bor_mirror_asymmetry(grim_handle_t h, int n, const void *Z, int64_t ldz, const int *target,
+                                         const double *sign, double *out) {
+    if (!h || n <= 0 || !Z || ldz < n || !target || !sign || !out)
+        return grim_fail(GRIM_ERR_ARGUMENT, "grim_bor_mirror_asymmetry: bad arguments");
+    DeviceGuard g(h->device);
+    GRIM_CHECK_CUDA(cudaMemsetAsync(out, 0, 2 * sizeof(double), h->stream));
+    k_bor_mirror_asym<<<dim3(ceil_div(n, 16), ceil_div(n, 16)), dim3(16, 16), 0, h->stream>>>(
+        n, (const double2 *)Z, ldz, target, sign, (unsigned long long *)out);
+    GRIM_CHECK_LAUNCH(h, "k_bor_mirror_asym");
+    return GRIM_OK;
+}
+
+extern "C" int grim_bor_mirror_split(grim_handle_t h, int nrhs, const void *B, int64_t ldb, int k, const int *p1,
+                                     const int *p2, const double *s, int nfe, const int *fe, int nfo, const int *fo,
+                                     void *Be, void *Bo) {
+    if (!h || nrhs <= 0 || nrhs > 65535 || !B || ldb < 2 * k + nfe + nfo || !Be || !Bo ||
+        !mirror_args_ok(k, p1, p2, s, nfe, fe, nfo, fo))
+        return grim_fail(GRIM_ERR_ARGUMENT, "grim_bor_mirror_split: bad arguments");
+    DeviceGuard g(h->device);
+    const BorMirror mr{k, nfe, nfo, p1, p2, fe, fo, s};
+    const int m = k + std::max(nfe, nfo);
+    k_bor_mirror_split<<<dim3(ceil_div(m, 128), nrhs), 128, 0, h->stream>>>(mr, nrhs, (const double2 *)B, ldb,
+                                                                             (double2 *)Be, (double2 *)Bo);
+    GRIM_CHECK_LAUNCH(h, "k_bor_mirror_split");
+    return GRIM_OK;
+}
+
+extern "C" int grim_bor_mirror_join(grim_handle_t h, int nrhs, const void *Ye, const void *Yo, int k, const int *p1,
+                                    const int *p2, const double *s, int nfe, const int *fe, int nfo, const int *fo,
+                                    void *X, int64_t ldx) {
+    if (!h || nrhs <= 0 || nrhs > 65535 || !Ye || !Yo || !X || ldx < 2 * k + nfe + nfo ||
+        !mirror_args_ok(k, p1, p2, s, nfe, fe, nfo, fo))
+        return grim_fail(GRIM_ERR_ARGUMENT, "grim_bor_mirror_join: bad arguments");
+    DeviceGuard g(h->device);
+    const BorMirror mr{k, nfe, nfo, p1, p2, fe, fo, s};
+    const int m = k + std::max(nfe, nfo);
+    k_bor_mirror_join<<<dim3(ceil_div(m, 128), nrhs), 128, 0, h->stream>>>(mr, nrhs, (const double2 *)Ye,
+                                                                            (const double2 *)Yo, (double2 *)X, ldx);
+    GRIM_CHECK_LAUNCH(h, "k_bor_mirror_join");
+    return GRIM_OK;
+}
+
 // ============================================================== allocation-free backward error
 #include "noalloc.cu"

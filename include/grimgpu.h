@@ -265,6 +265,24 @@ int grim_bor_assemble(grim_handle_t h, int ne, const double *nodes, double k, in
 int grim_bor_excitation(grim_handle_t h, int ne, const double *nodes, double k, int m, int nth,
                         const double *thetas_deg, int far, double alpha, int nred, const int *red_full,
                         const void *red_w, void *V, int64_t ldv);
+/* Mirror-symmetric bodies (reference bor/factor.py:37 MirrorSplit): with the mirror map of
+ * the reduced unknowns as k pairs (p1[i] < p2[i], s[i] = +-1 the sign of p2[i]) and fixed
+ * unknowns fe (sign +1), fo (sign -1), n = 2k + nfe + nfo (device int / double arrays):
+ * grim_bor_mirror_halves: the even (k + nfe) and odd (k + nfo) halves He, Ho (column-major,
+ *   leading dimension = order) of the n x n mode matrix Z, exact when Z = R Z R;
+ * grim_bor_mirror_asymmetry: out (device, 2 doubles) = (max |Z - R Z R|, max |Z|) for the
+ *   full map target[n], sign[n];
+ * grim_bor_mirror_split / grim_bor_mirror_join: right-hand sides into the halves' parts, and
+ *   the halves' solutions back to the n unknowns. */
+int grim_bor_mirror_halves(grim_handle_t h, int n, const void *Z, int64_t ldz, int k, const int *p1, const int *p2,
+                           const double *s, int nfe, const int *fe, int nfo, const int *fo, void *He, void *Ho);
+int grim_bor_mirror_asymmetry(grim_handle_t h, int n, const void *Z, int64_t ldz, const int *target,
+                              const double *sign, double *out);
+int grim_bor_mirror_split(grim_handle_t h, int nrhs, const void *B, int64_t ldb, int k, const int *p1, const int *p2,
+                          const double *s, int nfe, const int *fe, int nfo, const int *fo, void *Be, void *Bo);
+int grim_bor_mirror_join(grim_handle_t h, int nrhs, const void *Ye, const void *Yo, int k, const int *p1,
+                         const int *p2, const double *s, int nfe, const int *fe, int nfo, const int *fo, void *X,
+                         int64_t ldx);
 int grim_bor_farfield_accumulate(grim_handle_t h, int nred, int ncol, const void *W, int64_t ldw, const void *X,
                                  int64_t ldx, void *amp);
 

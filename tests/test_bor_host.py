@@ -47,3 +47,26 @@ def test_pair_routing_and_point_rules_match_oracle():
     for i, (s, sq, w) in enumerate(parts):
         np.testing.assert_array_equal(rule[starts[i]:starts[i + 1]], np.stack([s, sq, w], axis=1))
     assert starts[-1] == len(rule)
+
+
+def test_mirror_map_is_a_signed_involution_matching_the_oracle_matrices():
+    """The mirror map of a symmetric body is an involution with J_t -> -J_t, J_phi -> J_phi,
+    and the oracle's reduced mode matrices satisfy Z = R Z R with it; a body that is not
+    symmetric has no map."""
+    pts = S.ogive_generatrix(3.0, 22.0, 18)
+    body = OB.Body(pts)
+    asm = OB.Assembler(body, 5.0, 3, mfie=True)
+    for m in (0, 1, -1, 2):
+        target, sign = B.mirror_map(pts, m)
+        n = len(target)
+        assert np.array_equal(target[target], np.arange(n)) and np.array_equal(sign[target], sign)
+        R = np.zeros((n, n))
+        R[np.arange(n), target] = sign
+        Q = OB.pole_transform(body, m)
+        Zr = Q.conj().T @ asm.cfie_matrix(m) @ Q
+        assert np.max(np.abs(R @ Zr @ R - Zr)) <= 1e-13 * np.max(np.abs(Zr))
+        p1, p2, s, fe, fo = B.mirror_parts(target, sign)
+        assert 2 * len(p1) + len(fe) + len(fo) == n
+    bent = pts.copy()
+    bent[3, 0] *= 1.01
+    assert B.mirror_map(bent, 0) is None

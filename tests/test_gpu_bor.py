@@ -146,6 +146,31 @@ def test_cfie_and_mfie_solves_match_oracle(ctx, form):
         assert np.max(np.abs(got - o[key])) <= 1e-9 * np.max(np.abs(o[key])), key
 
 
+@pytest.mark.parametrize('m', [0, 1, -2])
+def test_mirror_halves_solve_equals_full_lu(ctx, m):
+    """Even / odd halves of a symmetric body's CFIE mode matrix: split, two half solves and
+    the join equal the LU solve of the full matrix; the asymmetry check reads rounding."""
+    from grim_20261007_b200.bor import solver as B
+    from grim_20261007_b200.device import ptr
+    pts = S.ogive_generatrix(3.0, 22.0, 30)
+    dev = B.BorDevice(pts, 5.0, 4, alpha=0.5)
+    th = torch.as_tensor(np.array([10.0, 60.0, 120.0]), device='cuda')
+    Z = dev.matrix(m)
+    V = dev.excitation(m, th, far=False)
+    mp = dev.mirror(m)
+    assert mp is not None
+    n, nrhs = int(Z.shape[0]), int(V.shape[0])
+    out = torch.empty(2, dtype=torch.float64, device='cuda')
+    ctx.lib.grim_bor_mirror_asymmetry(ctx.h, n, ptr(Z), n, ptr(mp['target']), ptr(mp['sign']), ptr(out))
+    d, a = out.cpu().numpy()
+    assert d <= 1e-13 * a
+    ref = np.linalg.solve(Z.cpu().numpy().T, V.cpu().numpy().T)
+    outs = B._solve_mirror_grouped(dev, [m], [Z.clone()], [V], workers=1)
+    assert outs[0]['mirror_halves'] == [mp['k'] + mp['nfe'], mp['k'] + mp['nfo']]
+    got = V.cpu().numpy().T
+    assert np.max(np.abs(got - ref)) <= 1e-11 * np.max(np.abs(ref))
+
+
 def test_cfie_rejects_open_shells(ctx):
     from grim_20261007_b200.bor.solver import solve_bor
     pts = S.sphere_generatrix(1.0, 12)[:-2]  # ends off the axis
@@ -172,8 +197,8 @@ def test_signed_mode_symmetry_matches_all_modes():
 @pytest.mark.parametrize('precision', ['double', 'mixed'])
 def test_grouped_modes_match_per_mode_solves(precision):
     """The mode systems factored by one grouped LU give the same far field as each mode
-    factored on its own (identical factors; the mixed refinement stops at the same
-    backward-error target)."""
+    factored on its own (identical factors, or for FP64 on this mirror-symmetric ogive the
+    even/odd halves; the mixed refinement stops at the same backward-error target)."""
     if not torch.cuda.is_available():
         pytest.skip('no CUDA device')
     from grim_20261007_b200.bor.solver import solve_bor_device
@@ -183,7 +208,8 @@ def test_grouped_modes_match_per_mode_solves(precision):
     f_g, t_g = solve_bor_device(gen, k, th, 12, precision=precision)
     f_1, t_1 = solve_bor_device(gen, k, th, 12, precision=precision, grouped=False)
     assert t_g['mode_systems_solved'] == t_1['mode_systems_solved'] == 13
-    rtol = 1e-12 if precision == 'double' else 1e-8
+    # double: the grouped path solves the symmetric ogive's modes through their mirror halves
+    rtol = 1e-11 if precision == 'double' else 1e-8
     np.testing.assert_allclose(f_g, f_1, rtol=rtol, atol=rtol * np.max(np.abs(f_1)))
 
 
