@@ -2,6 +2,7 @@
 import os
 
 import numpy as np
+import pytest
 
 from grim_20261007_b200 import synthetic as S
 from grim_20261007_b200.bor import solver as B
@@ -70,3 +71,34 @@ def test_mirror_map_is_a_signed_involution_matching_the_oracle_matrices():
     bent = pts.copy()
     bent[3, 0] *= 1.01
     assert B.mirror_map(bent, 0) is None
+
+
+@pytest.mark.parametrize('kwargs, exc', [
+    (dict(formulation='pmchwt'), ValueError),
+    (dict(formulation='cfie', cfie_alpha=1.0), ValueError),
+    (dict(formulation='auto', cfie_alpha=float('nan')), ValueError),
+    (dict(zs=50.0), NotImplementedError),
+    (dict(sheet_zs=10.0), NotImplementedError),
+    (dict(gauss_order=5), ValueError),
+])
+def test_solve_bor_rejects_arguments_before_any_device_work(kwargs, exc):
+    """solve_bor refuses unsupported formulations, CFIE weights outside (0, 1), impedance and
+    sheet models and other far-pair Gauss orders with the reference's error types, before it
+    needs a device."""
+    with pytest.raises(exc):
+        B.solve_bor(S.sphere_generatrix(1.0, 12), 3e8, [0.0, 90.0], **kwargs)
+
+
+def test_validate_generatrix_rules():
+    pts = S.sphere_generatrix(1.0, 8)
+    out = B.validate_generatrix(pts)
+    assert out[0, 0] == 0.0 and out[-1, 0] == 0.0
+    with pytest.raises(ValueError):
+        B.validate_generatrix(pts[:2])
+    bad = pts.copy()
+    bad[3, 0] = -0.5
+    with pytest.raises(ValueError):
+        B.validate_generatrix(bad)
+    dup = np.vstack([pts[:3], pts[2:]])
+    with pytest.raises(ValueError):
+        B.validate_generatrix(dup)
