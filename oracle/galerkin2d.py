@@ -1,0 +1,194 @@
+"""CPU restatement of the reference's 2-D linear-Galerkin near element blocks (TEST INFRASTRUCTURE).
+
+Only the tests import this module: it is the checker for a GPU port of these blocks, never a
+product path.  It restates, for straight elements with linear (hat) bases and a real
+wavenumber:
+
+* the single-layer self block (``twod/operators.py:1044`` ``_single_layer_block_linear``):
+  on a straight element the kernel depends on u = |t - s| only, so the 2 x 2 block is
+  l^2 (j/4) int_0^1 H0^(2)(k l u) C(u) du with C_diag = (2 - 3u + u^3)/3 and
+  C_off = (1 - u^3)/3; the small-argument series of H0^(2) (J0 times the log term, plus the
+  harmonic-number corrections) turns it into exact moments int u^p = 1/(p+1) and
+  int u^p ln u = -1/(p+1)^2 (``:418`` ``_single_layer_self_block_exact``, up to |k l| = 8);
+  beyond, the element is cut into m sub-intervals with |k| l / m <= 2, each sub-interval's
+  own block by the series, neighbouring sub-intervals by the graded corner rule and
+  separated ones by a 16-point tensor rule, all in the parent element's basis (``:980``
+  ``_single_layer_self_block_composite``);
+* the S and K' blocks of endpoint-touching pairs (``:629``
+  ``_integrate_linear_touching_duffy_sk_vectorized``): the unit square split into two
+  triangles at the shared corner, the radial distance graded as u = t^4 (weight 4 t^7) with
+  a 20-point Gauss rule per direction (``polynomial_quadrature.py:319`` ``_nodes``), the
+  separations formed from the corner so that points next to it keep their accuracy.
+
+G = (j/4) H0^(2)(k r); the normal derivative is (j/4) k H1^(2)(k r) (r . n)/r on the source
+normal (negated for the observation normal); r is floored at 1e-12 and k r at 1e-12.
+J0, Y0, J1, Y1 are SciPy's (the reference's own call sites, ``operators.py:898``).
+
+Pinned against the reference's own blocks in ``tests/golden/galerkin_near.npz`` (made by
+``tests/golden/make_galerkin_near_golden.py``).
+"""
+from __future__ import annotations
+
+import cmath
+import math
+
+import numpy as np
+from scipy import special as sp
+
+EPS = 1e-12
+EULER_GAMMA = 0.5772156649015329
+SERIES_LIMIT = 8.0      # |k l| up to which the self series is used
+SUBINTERVAL_KL = 2.0    # |k| l per sub-interval of the composite self rule
+TOUCH_ORDER = 20        # Gauss points per direction of the graded corner rule
+
+
+def unit_gauss(q):
+    x, w = np.polynomial.legendre.leggauss(int(q))
+    return 0.5 * (x + 1.0), 0.5 * w
+
+
+def hankel2(order, x):
+    """H_order^(2) at real non-negative x (floored at 1e-12)."""
+    xr = np.maximum(np.asarray(x, dtype=float), 1e-12)
+    if order == 0:
+        return sp.j0(xr) - 1j * sp.y0(xr)
+    return sp.j1(xr) - 1j * sp.y1(xr)
+
+
+def green(k, r):
+    """(j/4) H0^(2)(k r), r floored at EPS."""
+    x = float(k) * np.maximum(np.asarray(r, dtype=float), EPS)
+    return 0.25j * hankel2(0, np.where(np.abs(x) <= 1e-12, 1e-12, x))
+
+
+def _moments(p, coeffs):
+    """(int_0^1 u^p c(u) du, int_0^1 u^p ln(u) c(u) du) for c(u) = sum_q coeffs[q] u^q."""
+    plain = sum(c / (p + q + 1) for q, c in enumerate(coeffs))
+    logged = -sum(c / (p + q + 1) ** 2 for q, c in enumerate(coeffs))
+    return plain, logged
+
+
+def self_block_series(length, k, a=0.0, b=1.0):
+    """2 x 2 single-layer block of the sub-interval [a, b] of a straight element (parent
+    basis), by the small-argument series; None where |k l| is outside (1e-30, 8]."""
+    ell = float(length) * (float(b) - float(a))
+    if ell <= 0.0:
+        return np.zeros((2, 2), dtype=np.complex128)
+    z = complex(k) * ell
+    if abs(z) > SERIES_LIMIT or abs(z) <= 1e-30:
+        return None
+    weights = {'diag': (2.0 / 3.0, -1.0, 0.0, 1.0 / 3.0), 'off': (1.0 / 3.0, 0.0, 0.0, -1.0 / 3.0)}
+    c = 2.0 / math.pi
+    shift = cmath.log(z / 2.0) + EULER_GAMMA
+    quarter = (z / 2.0) ** 2
+    total = {'diag': 0j, 'off': 0j}
+    term, harmonic, m = 1.0 + 0j, 0.0, 0
+    while True:
+        factor = term * (1.0 - 1j * c * (shift - harmonic))
+        for key, coeffs in weights.items():
+            plain, logged = _moments(2 * m, coeffs)
+            total[key] += factor * plain - 1j * c * term * logged
+        m += 1
+        term *= -quarter / (m * m)
+        harmonic += 1.0 / m
+        if m > 60:
+            return None
+        if abs(term) < 1e-18 * max(1.0, abs(total['diag'])):
+            break
+    block = (0.25j * ell * ell) * np.array([[total['diag'], total['off']], [total['off'], total['diag']]])
+    if a == 0.0 and b == 1.0:
+        return block
+    t = np.array([[1.0 - a, 1.0 - b], [a, b]], dtype=np.complex128)
+    return t @ block @ t.T
+
+
+def touching_nodes(order=TOUCH_ORDER):
+    """(x, y, w): distances from the shared corner on the unit square by two triangles, the
+    radial coordinate graded as t^4."""
+    n = max(int(order), TOUCH_ORDER)
+    t, w = unit_gauss(n)
+    u = t[:, None] ** 4
+    v = t[None, :]
+    wt = (4.0 * t[:, None] ** 7 * w[:, None] * w[None, :]).ravel()
+    x = np.concatenate((np.broadcast_to(u, (n, n)).ravel(), (u * v).ravel()))
+    y = np.concatenate(((u * v).ravel(), np.broadcast_to(u, (n, n)).ravel()))
+    return x, y, np.tile(wt, 2)
+
+
+def self_block_composite(length, k):
+    """Self block of an electrically long straight element (|k l| > 8)."""
+    ell = float(length)
+    kl = abs(complex(k)) * ell
+    m = max(2, int(math.ceil(kl / SUBINTERVAL_KL)))
+    if m > 256:
+        m = max(256, int(math.ceil(kl / SERIES_LIMIT)))
+    h = 1.0 / m
+    block = np.zeros((2, 2), dtype=np.complex128)
+    for i in range(m):
+        block += self_block_series(length, k, i * h, (i + 1) * h)
+
+    def basis(x):
+        return np.stack((1.0 - x, x), axis=-1)
+
+    # neighbouring sub-intervals, meeting at s = (i + 1) h
+    x, y, w = touching_nodes(TOUCH_ORDER)
+    g = green(k, ell * h * (x + y)) * w
+    joints = (np.arange(m - 1) + 1.0) * h
+    for side in (-1.0, 1.0):
+        xo = joints[:, None] + side * h * x[None, :]
+        xs = joints[:, None] - side * h * y[None, :]
+        block += np.einsum('q,iqa,iqb->ab', g, basis(xo), basis(xs)) * (ell * h) ** 2
+    # separated sub-intervals: the kernel depends on the offset d only
+    t, wt = unit_gauss(16)
+    for d in range(2, m):
+        kern = green(k, ell * h * (d + t[None, :] - t[:, None])) * np.outer(wt, wt)
+        first = np.arange(m - d)[:, None]
+        lower = basis((first + t[None, :]) * h)
+        upper = basis((first + d + t[None, :]) * h)
+        block += (np.einsum('pq,ipa,iqb->ab', kern, lower, upper)
+                  + np.einsum('pq,iqa,ipb->ab', kern, upper, lower)) * (ell * h) ** 2
+    return block
+
+
+def self_block(length, k):
+    """Single-layer self block of a straight element (the series, else the composite)."""
+    out = self_block_series(length, k)
+    if out is not None:
+        return out
+    if abs(complex(k)) * float(length) > SERIES_LIMIT:
+        return self_block_composite(length, k)
+    raise ValueError('self series failed below |k l| = 8')
+
+
+def touching_blocks(obs_ends, src_ends, obs_normal, src_normal, obs_start, src_start, k, obs_normal_deriv,
+                    order=TOUCH_ORDER):
+    """(S, K') 2 x 2 blocks of two elements sharing an end (obs_start: the observation
+    element's shared end is its start p0; likewise src_start)."""
+    po0, po1 = (np.asarray(p, float) for p in obs_ends)
+    ps0, ps1 = (np.asarray(p, float) for p in src_ends)
+    lo, ls = float(np.hypot(*(po1 - po0))), float(np.hypot(*(ps1 - ps0)))
+    x0, y0, w = touching_nodes(order)
+    corner_o = po0 if obs_start else po1
+    corner_s = ps0 if src_start else ps1
+    d_o = (po1 - po0) if obs_start else (po0 - po1)
+    d_s = (ps1 - ps0) if src_start else (ps0 - ps1)
+    origin = corner_o - corner_s
+    tiny = 64.0 * np.finfo(float).eps * max(float(np.hypot(*corner_o)), float(np.hypot(*corner_s)), lo, ls)
+    if float(np.hypot(*origin)) <= tiny:
+        origin = np.zeros(2)
+    diff = origin[None, :] + x0[:, None] * d_o[None, :] - y0[:, None] * d_s[None, :]
+    xo = x0 if obs_start else 1.0 - x0
+    xs = y0 if src_start else 1.0 - y0
+    bo = np.column_stack((1.0 - xo, xo))
+    bs = np.column_stack((1.0 - xs, xs))
+    r = np.hypot(diff[:, 0], diff[:, 1])
+    s_blk = np.einsum('q,q,qa,qb->ab', w, green(k, r), bo, bs)
+    live = r > EPS
+    deriv = np.zeros(len(r), dtype=np.complex128)
+    kr = float(k) * r[live]
+    h1 = hankel2(1, np.where(np.abs(kr) <= 1e-12, 1e-12, kr))
+    n = np.asarray(obs_normal if obs_normal_deriv else src_normal, float)
+    proj = (diff[live] @ n) / r[live]
+    deriv[live] = (0.25j * float(k)) * h1 * proj * (-1.0 if obs_normal_deriv else 1.0)
+    k_blk = np.einsum('q,q,qa,qb->ab', w, deriv, bo, bs)
+    return s_blk * (lo * ls), k_blk * (lo * ls)

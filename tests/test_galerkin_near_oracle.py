@@ -1,0 +1,48 @@
+"""The 2-D linear-Galerkin near-block oracle against the reference's own self and touching
+blocks (tests/golden/galerkin_near.npz, made by tests/golden/make_galerkin_near_golden.py)."""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import galerkin2d as G
+from tests.conftest import GOLDEN
+
+F = np.load(os.path.join(GOLDEN, 'galerkin_near.npz'))
+
+
+@pytest.mark.parametrize('i', range(len(F['self_k'])))
+def test_self_block_matches_reference(i):
+    """Self single-layer blocks: the series up to |k l| = 8, the composite rule beyond."""
+    got = G.self_block(F['self_length'][i], F['self_k'][i])
+    ref = F['self_s'][i]
+    assert np.max(np.abs(got - ref)) <= 1e-13 * np.max(np.abs(ref))
+
+
+def test_self_block_series_on_a_sub_interval_is_the_parent_basis_projection():
+    """A sub-interval's series block in the parent basis equals the full block's series for
+    a sub-interval [0, 1] of a shorter element, mapped by the hat functions."""
+    length, k = 0.2, 15.0
+    sub = G.self_block_series(length, k, 0.25, 0.75)
+    local = G.self_block_series(0.5 * length, k)
+    t = np.array([[0.75, 0.25], [0.25, 0.75]])
+    assert np.allclose(sub, t @ local @ t.T, rtol=1e-14, atol=1e-16)
+
+
+@pytest.mark.parametrize('i', range(len(F['touch_k'])))
+def test_touching_blocks_match_reference(i):
+    ends = F['touch_ends'][i]
+    po, ps = ends[:2], ends[2:]
+
+    def normal(p):
+        t = (p[1] - p[0]) / np.hypot(*(p[1] - p[0]))
+        return np.array([t[1], -t[0]])
+
+    s_blk, k_blk = G.touching_blocks(po, ps, normal(po), normal(ps), bool(F['touch_obs_start'][i]),
+                                     bool(F['touch_src_start'][i]), float(F['touch_k'][i]),
+                                     bool(F['touch_obs_deriv'][i]))
+    s_ref, k_ref = F['touch_s'][i], F['touch_kd'][i]
+    assert np.max(np.abs(s_blk - s_ref)) <= 1e-13 * np.max(np.abs(s_ref))
+    # K' of collinear elements is zero up to rounding: scale the bound by |S| k as well
+    scale = max(np.max(np.abs(k_ref)), np.max(np.abs(s_ref)) * float(F['touch_k'][i]))
+    assert np.max(np.abs(k_blk - k_ref)) <= 1e-13 * scale
