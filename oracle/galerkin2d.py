@@ -18,7 +18,14 @@ wavenumber:
   ``_integrate_linear_touching_duffy_sk_vectorized``): the unit square split into two
   triangles at the shared corner, the radial distance graded as u = t^4 (weight 4 t^7) with
   a 20-point Gauss rule per direction (``polynomial_quadrature.py:319`` ``_nodes``), the
-  separations formed from the corner so that points next to it keep their accuracy.
+  separations formed from the corner so that points next to it keep their accuracy;
+* the routing of separated pairs (``twod/assembly/separation.py:67`` ``requires_adaptive``):
+  the adaptive rule when the centres are closer than 0.75 L, the segments closer than
+  0.25 L, or an end lies within 0.5 L above the other element's interior (L the longer
+  length), else the fixed tensor rule;
+* the fixed-rule S and K' blocks (``twod/operators.py:223``
+  ``_integrate_linear_pairs_box_sk_batched``): 16 Gauss points on each element (the order
+  the reference's ladder settles on for linear elements, ``operators.py:1761-1766``).
 
 G = (j/4) H0^(2)(k r); the normal derivative is (j/4) k H1^(2)(k r) (r . n)/r on the source
 normal (negated for the observation normal); r is floored at 1e-12 and k r at 1e-12.
@@ -192,3 +199,92 @@ def touching_blocks(obs_ends, src_ends, obs_normal, src_normal, obs_start, src_s
     deriv[live] = (0.25j * float(k)) * h1 * proj * (-1.0 if obs_normal_deriv else 1.0)
     k_blk = np.einsum('q,q,qa,qb->ab', w, deriv, bo, bs)
     return s_blk * (lo * ls), k_blk * (lo * ls)
+
+
+# ---- separated near pairs (``twod/assembly/separation.py``, ``twod/operators.py:223``)
+ADAPTIVE_CENTRE = 0.75      # centre distance below this many lengths: adaptive rule
+ADAPTIVE_GAP = 0.25         # segments closer than this many lengths: adaptive rule
+ADAPTIVE_PROJECTION = 0.5   # an end hovering over the other element this close: adaptive rule
+BOX_ORDER = 16              # Gauss points per element of the fixed tensor rule
+
+
+def _point_to_segment_sq(x, a, b):
+    edge = b - a
+    den = float(edge @ edge)
+    t = float((x - a) @ edge) / den if den > 0 else 0.0
+    d = x - a - min(max(t, 0.0), 1.0) * edge
+    return float(d @ d)
+
+
+def segment_distance(p0, p1, q0, q1):
+    """Distance between two closed segments (0 when they cross)."""
+    p0, p1, q0, q1 = (np.asarray(v, float) for v in (p0, p1, q0, q1))
+    sq = min(_point_to_segment_sq(p0, q0, q1), _point_to_segment_sq(p1, q0, q1),
+             _point_to_segment_sq(q0, p0, p1), _point_to_segment_sq(q1, p0, p1))
+    u, v, w = p1 - p0, q1 - q0, q0 - p0
+    cross = lambda a, b: a[0] * b[1] - a[1] * b[0]
+    den = cross(u, v)
+    if den != 0:
+        t, s = cross(w, v) / den, cross(w, u) / den
+        if 0 <= t <= 1 and 0 <= s <= 1:
+            return 0.0
+    return math.sqrt(max(sq, 0.0))
+
+
+def projection_distance(p0, p1, q0, q1):
+    """Smallest distance from an end of one segment to the other's interior (its foot point
+    strictly inside), infinity when no end projects inside."""
+    p0, p1, q0, q1 = (np.asarray(v, float) for v in (p0, p1, q0, q1))
+    best = math.inf
+    for x, a, b in ((p0, q0, q1), (p1, q0, q1), (q0, p0, p1), (q1, p0, p1)):
+        edge = b - a
+        den = float(edge @ edge)
+        t = float((x - a) @ edge) / den if den > 0 else -1.0
+        if 0.0 < t < 1.0:
+            d = x - a - t * edge
+            best = min(best, math.sqrt(float(d @ d)))
+    return best
+
+
+def needs_adaptive(obs_ends, src_ends):
+    """True when a separated pair takes the adaptive rule rather than the 16-point tensor rule:
+    centres closer than 0.75 L, segments closer than 0.25 L, or an end within 0.5 L above the
+    other element's interior (L the longer length)."""
+    p0, p1 = (np.asarray(v, float) for v in obs_ends)
+    q0, q1 = (np.asarray(v, float) for v in src_ends)
+    lo, ls = float(np.hypot(*(p1 - p0))), float(np.hypot(*(q1 - q0)))
+    scale = max(lo, ls)
+    dist = float(np.hypot(*(0.5 * (p0 + p1) - 0.5 * (q0 + q1))))
+    if dist < ADAPTIVE_CENTRE * scale:
+        return True
+    if dist >= 0.5 * (lo + ls) + ADAPTIVE_PROJECTION * scale:
+        return False
+    if dist < 0.5 * (lo + ls) + ADAPTIVE_GAP * scale and segment_distance(p0, p1, q0, q1) < ADAPTIVE_GAP * scale:
+        return True
+    return projection_distance(p0, p1, q0, q1) < ADAPTIVE_PROJECTION * scale
+
+
+def box_blocks(obs_ends, src_ends, obs_normal, src_normal, k, obs_normal_deriv, order=BOX_ORDER):
+    """(S, K') 2 x 2 blocks of a separated pair by the tensor Gauss rule (order points on each
+    element)."""
+    p0, p1 = (np.asarray(v, float) for v in obs_ends)
+    q0, q1 = (np.asarray(v, float) for v in src_ends)
+    t, w = unit_gauss(order)
+    basis = np.column_stack((1.0 - t, t))
+    op = p0[None, :] + t[:, None] * (p1 - p0)[None, :]
+    sp_ = q0[None, :] + t[:, None] * (q1 - q0)[None, :]
+    diff = op[:, None, :] - sp_[None, :, :]
+    r = np.sqrt(np.sum(diff * diff, axis=2))
+    rs = np.maximum(r, EPS)
+    kr = float(k) * rs
+    ww = np.outer(w, w)
+    g = 0.25 * sp.y0(kr) + 0.25j * sp.j0(kr)
+    s_blk = basis.T @ (ww * g) @ basis
+    deriv = 0.25 * float(k) * sp.y1(kr) + 0.25j * float(k) * sp.j1(kr)
+    n = np.asarray(obs_normal if obs_normal_deriv else src_normal, float)
+    proj = np.sum(diff * n[None, None, :], axis=2) / rs
+    dk = (-deriv if obs_normal_deriv else deriv) * proj
+    dk[r <= EPS] = 0.0
+    k_blk = basis.T @ (ww * dk) @ basis
+    scale = float(np.hypot(*(p1 - p0))) * float(np.hypot(*(q1 - q0)))
+    return s_blk * scale, k_blk * scale

@@ -14,7 +14,11 @@ records, for real wavenumbers:
 * ``touch``: S and K' blocks of endpoint-touching element pairs by the graded two-triangle
   corner rule (``:629`` ``_integrate_linear_touching_duffy_sk_vectorized``), for collinear,
   right-angle, sharp and reflex corners, every combination of which end is shared, with the
-  normal derivative on the source or on the observation element.
+  normal derivative on the source or on the observation element;
+* ``ring`` / ``box``: on 60 random elements around a perturbed circle, the reference's
+  adaptive-rule predicate (``twod/assembly/separation.py:67`` ``requires_adaptive``) for every
+  non-adjacent pair closer than 4 element lengths, and the 16-point tensor S and K' blocks
+  (``twod/operators.py:223`` ``_integrate_linear_pairs_box_sk_batched``) of the others.
 """
 from __future__ import annotations
 
@@ -86,8 +90,35 @@ def main(reference_root):
                touch_obs_start=np.array([r[2] for r in rows]), touch_src_start=np.array([r[3] for r in rows]),
                touch_obs_deriv=np.array([r[4] for r in rows]), touch_s=np.array([r[5] for r in rows]),
                touch_kd=np.array([r[6] for r in rows]))
+    # separated-near pairs: random straight elements around a perturbed circle; the
+    # reference's own adaptive / box routing for every pair with centre distance < 4 L, and
+    # its 16-point tensor blocks for the box pairs
+    from ghost_backend.twod.assembly.separation import requires_adaptive
+    n = 60
+    t = np.sort(rng.uniform(0, 2 * math.pi, n))
+    r = 0.5 * (1 + 0.15 * rng.standard_normal(n))
+    pts = np.stack([r * np.cos(t), r * np.sin(t)], axis=1)
+    elems = [element(LE, 'e', pts[i], pts[(i + 1) % n], i) for i in range(n)]
+    pairs, adaptive = [], []
+    for i in range(n):
+        for j in range(n):
+            if abs(i - j) in (0, 1, n - 1):
+                continue
+            a, b = elems[i], elems[j]
+            if np.linalg.norm(a.center - b.center) < 4 * max(a.length, b.length):
+                pairs.append((i, j))
+                adaptive.append(bool(requires_adaptive(a, b)))
+    pairs = np.array(pairs)
+    adaptive = np.array(adaptive)
+    box = pairs[~adaptive]
+    k = 30.0
+    s_box, k_box = O._integrate_linear_pairs_box_sk_batched(elems, box[:, 0], box[:, 1], k, False, 16)
+    _s, k_box_obs = O._integrate_linear_pairs_box_sk_batched(elems, box[:, 0], box[:, 1], k, True, 16)
+    out.update(ring_points=pts, ring_pairs=pairs, ring_adaptive=adaptive, ring_k=np.array(k), box_s=s_box,
+               box_kd_src=k_box, box_kd_obs=k_box_obs)
     np.savez_compressed(os.path.join(HERE, 'galerkin_near.npz'), **out)
-    print('wrote galerkin_near.npz:', len(lengths), 'self blocks,', len(rows), 'touching pairs')
+    print('wrote galerkin_near.npz:', len(lengths), 'self blocks,', len(rows), 'touching pairs,', len(pairs),
+          'near pairs (', int(adaptive.sum()), 'adaptive)')
 
 
 if __name__ == '__main__':

@@ -46,3 +46,35 @@ def test_touching_blocks_match_reference(i):
     # K' of collinear elements is zero up to rounding: scale the bound by |S| k as well
     scale = max(np.max(np.abs(k_ref)), np.max(np.abs(s_ref)) * float(F['touch_k'][i]))
     assert np.max(np.abs(k_blk - k_ref)) <= 1e-13 * scale
+
+
+def _ring():
+    pts = F['ring_points']
+    n = len(pts)
+    ends = [(pts[i], pts[(i + 1) % n]) for i in range(n)]
+
+    def normal(e):
+        t = (e[1] - e[0]) / np.hypot(*(e[1] - e[0]))
+        return np.array([t[1], -t[0]])
+    return ends, [normal(e) for e in ends]
+
+
+def test_adaptive_routing_matches_reference():
+    """The separated-pair predicate (centre, gap and projection clauses) routes every near pair
+    of the ring as the reference does."""
+    ends, _normals = _ring()
+    got = np.array([G.needs_adaptive(ends[i], ends[j]) for i, j in F['ring_pairs']])
+    np.testing.assert_array_equal(got, F['ring_adaptive'])
+    assert got.sum() > 50 and (~got).sum() > 1000
+
+
+def test_box_blocks_match_reference():
+    """16-point tensor S and K' blocks (source and observation normal) of the ring's box pairs."""
+    ends, normals = _ring()
+    box = F['ring_pairs'][~F['ring_adaptive']]
+    k = float(F['ring_k'])
+    for idx, (i, j) in enumerate(box):
+        s_blk, kd_src = G.box_blocks(ends[i], ends[j], normals[i], normals[j], k, False)
+        _s, kd_obs = G.box_blocks(ends[i], ends[j], normals[i], normals[j], k, True)
+        for got, ref in ((s_blk, F['box_s'][idx]), (kd_src, F['box_kd_src'][idx]), (kd_obs, F['box_kd_obs'][idx])):
+            assert np.max(np.abs(got - ref)) <= 1e-13 * max(np.max(np.abs(ref)), np.max(np.abs(F['box_s'][idx])) * k)
