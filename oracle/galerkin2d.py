@@ -25,7 +25,11 @@ wavenumber:
   length), else the fixed tensor rule;
 * the fixed-rule S and K' blocks (``twod/operators.py:223``
   ``_integrate_linear_pairs_box_sk_batched``): 16 Gauss points on each element (the order
-  the reference's ladder settles on for linear elements, ``operators.py:1761-1766``).
+  the reference's ladder settles on for linear elements, ``operators.py:1761-1766``);
+* the close separated pairs (``twod/operators.py:1172`` ``_integrate_linear_pair_adaptive_sk``):
+  each box of sub-intervals compared with its four-way bisection by the same tensor rule,
+  only the unconverged children refined further, to 1e-9 relative to the sum of the
+  children's norms (at most 12 levels).
 
 G = (j/4) H0^(2)(k r); the normal derivative is (j/4) k H1^(2)(k r) (r . n)/r on the source
 normal (negated for the observation normal); r is floored at 1e-12 and k r at 1e-12.
@@ -288,3 +292,79 @@ def box_blocks(obs_ends, src_ends, obs_normal, src_normal, k, obs_normal_deriv, 
     k_blk = basis.T @ (ww * dk) @ basis
     scale = float(np.hypot(*(p1 - p0))) * float(np.hypot(*(q1 - q0)))
     return s_blk * scale, k_blk * scale
+
+
+# ---- close separated pairs: bisection to a relative tolerance (``twod/operators.py:1172``)
+ADAPTIVE_RTOL = 1e-9
+ADAPTIVE_MAX_DEPTH = 12
+
+
+def interval_box(obs_ends, src_ends, obs_normal, src_normal, k, obs_normal_deriv, obs_iv, src_iv, order=BOX_ORDER):
+    """(S, K') of the sub-intervals obs_iv x src_iv (parent parameters in [0, 1]) in the
+    parent elements' hat basis, by the tensor Gauss rule."""
+    p0, p1 = (np.asarray(v, float) for v in obs_ends)
+    q0, q1 = (np.asarray(v, float) for v in src_ends)
+    (oa, ob), (sa, sb) = obs_iv, src_iv
+    ho, hs = max(ob - oa, 0.0), max(sb - sa, 0.0)
+    lo = float(np.hypot(*(p1 - p0))) * ho
+    ls = float(np.hypot(*(q1 - q0))) * hs
+    if lo <= 0.0 or ls <= 0.0:
+        return np.zeros((2, 2), complex), np.zeros((2, 2), complex)
+    t, w = unit_gauss(order)
+    xo, xs = oa + ho * t, sa + hs * t
+    bo, bs = np.column_stack((1.0 - xo, xo)), np.column_stack((1.0 - xs, xs))
+    ro = p0[None, :] + xo[:, None] * (p1 - p0)[None, :]
+    rsrc = q0[None, :] + xs[:, None] * (q1 - q0)[None, :]
+    diff = ro[:, None, :] - rsrc[None, :, :]
+    r = np.sqrt(np.sum(diff * diff, axis=2))
+    rs = np.maximum(r, EPS)
+    kr = float(k) * rs
+    kr = np.where(np.abs(kr) <= 1e-12, 1e-12, kr)
+    ww = np.outer(w, w)
+    g = 0.25j * hankel2(0, kr)
+    n = np.asarray(obs_normal if obs_normal_deriv else src_normal, float)
+    proj = np.sum(diff * n[None, None, :], axis=2) / rs
+    dk = (0.25j * float(k)) * hankel2(1, kr) * proj * (-1.0 if obs_normal_deriv else 1.0)
+    dk[r <= EPS] = 0.0
+    s_blk = np.einsum('ij,ia,jb->ab', ww * g, bo, bs)
+    k_blk = np.einsum('ij,ia,jb->ab', ww * dk, bo, bs)
+    return s_blk * (lo * ls), k_blk * (lo * ls)
+
+
+def adaptive_blocks(obs_ends, src_ends, obs_normal, src_normal, k, obs_normal_deriv, order=BOX_ORDER,
+                    rtol=ADAPTIVE_RTOL, max_depth=ADAPTIVE_MAX_DEPTH):
+    """(S, K') of a close separated pair: each box is compared with its four-way bisection,
+    and only the children whose parent did not meet rtol (relative to the sum of the
+    children's norms) are refined further."""
+    p0, p1 = (np.asarray(v, float) for v in obs_ends)
+    q0, q1 = (np.asarray(v, float) for v in src_ends)
+    floor = np.finfo(float).eps * max(1.0, float(np.hypot(*(p1 - p0))) * float(np.hypot(*(q1 - q0))))
+
+    def box(oi, si):
+        return interval_box(obs_ends, src_ends, obs_normal, src_normal, k, obs_normal_deriv, oi, si, order)
+
+    def err(coarse, kids):
+        fine = sum(kids, np.zeros((2, 2), complex))
+        norms = sum(float(np.linalg.norm(b)) for b in kids)
+        return float(np.linalg.norm(fine - coarse)) / max(norms, floor)
+
+    def refine(oi, si, depth, coarse):
+        om, sm = 0.5 * (oi[0] + oi[1]), 0.5 * (si[0] + si[1])
+        quads = [((oi[0], om), (si[0], sm)), ((oi[0], om), (sm, si[1])),
+                 ((om, oi[1]), (si[0], sm)), ((om, oi[1]), (sm, si[1]))]
+        kids = [box(a, b) for a, b in quads]
+        e = max(err(coarse[0], [c[0] for c in kids]), err(coarse[1], [c[1] for c in kids]))
+        if e <= rtol:
+            return (sum((c[0] for c in kids), np.zeros((2, 2), complex)),
+                    sum((c[1] for c in kids), np.zeros((2, 2), complex)))
+        if depth >= max_depth:
+            raise FloatingPointError('close-pair quadrature did not converge')
+        s_tot, k_tot = np.zeros((2, 2), complex), np.zeros((2, 2), complex)
+        for (a, b), c in zip(quads, kids):
+            cs, ck = refine(a, b, depth + 1, c)
+            s_tot += cs
+            k_tot += ck
+        return s_tot, k_tot
+
+    whole = ((0.0, 1.0), (0.0, 1.0))
+    return refine(whole[0], whole[1], 0, box(*whole))

@@ -18,7 +18,9 @@ records, for real wavenumbers:
 * ``ring`` / ``box``: on 60 random elements around a perturbed circle, the reference's
   adaptive-rule predicate (``twod/assembly/separation.py:67`` ``requires_adaptive``) for every
   non-adjacent pair closer than 4 element lengths, and the 16-point tensor S and K' blocks
-  (``twod/operators.py:223`` ``_integrate_linear_pairs_box_sk_batched``) of the others.
+  (``twod/operators.py:223`` ``_integrate_linear_pairs_box_sk_batched``) of the others, and the
+  adaptive pairs' blocks by the reference's near-pair dispatcher (``:1080``
+  ``_sk_blocks_near_linear``, whose bisection rule is ``:1172``).
 """
 from __future__ import annotations
 
@@ -116,6 +118,11 @@ def main(reference_root):
     _s, k_box_obs = O._integrate_linear_pairs_box_sk_batched(elems, box[:, 0], box[:, 1], k, True, 16)
     out.update(ring_points=pts, ring_pairs=pairs, ring_adaptive=adaptive, ring_k=np.array(k), box_s=s_box,
                box_kd_src=k_box, box_kd_obs=k_box_obs)
+    # the adaptive pairs through the reference's near-pair dispatcher (its bisection rule)
+    close = pairs[adaptive]
+    ad = [[O._sk_blocks_near_linear(elems[i], elems[j], k, deriv) for i, j in close] for deriv in (False, True)]
+    out.update(adaptive_s=np.array([b[0] for b in ad[0]]), adaptive_kd_src=np.array([b[1] for b in ad[0]]),
+               adaptive_kd_obs=np.array([b[1] for b in ad[1]]))
     np.savez_compressed(os.path.join(HERE, 'galerkin_near.npz'), **out)
     print('wrote galerkin_near.npz:', len(lengths), 'self blocks,', len(rows), 'touching pairs,', len(pairs),
           'near pairs (', int(adaptive.sum()), 'adaptive)')

@@ -78,3 +78,18 @@ def test_box_blocks_match_reference():
         _s, kd_obs = G.box_blocks(ends[i], ends[j], normals[i], normals[j], k, True)
         for got, ref in ((s_blk, F['box_s'][idx]), (kd_src, F['box_kd_src'][idx]), (kd_obs, F['box_kd_obs'][idx])):
             assert np.max(np.abs(got - ref)) <= 1e-13 * max(np.max(np.abs(ref)), np.max(np.abs(F['box_s'][idx])) * k)
+
+
+def test_adaptive_blocks_match_reference():
+    """Close separated pairs of the ring (the reference's adaptive routing) by the bisection
+    rule to 1e-9: S and K' (source and observation normal) equal the reference's."""
+    ends, normals = _ring()
+    close = F['ring_pairs'][F['ring_adaptive']]
+    k = float(F['ring_k'])
+    for idx, (i, j) in enumerate(close):
+        s_blk, kd_src = G.adaptive_blocks(ends[i], ends[j], normals[i], normals[j], k, False)
+        _s, kd_obs = G.adaptive_blocks(ends[i], ends[j], normals[i], normals[j], k, True)
+        scale = np.max(np.abs(F['adaptive_s'][idx])) * k
+        for got, ref in ((s_blk, F['adaptive_s'][idx]), (kd_src, F['adaptive_kd_src'][idx]),
+                         (kd_obs, F['adaptive_kd_obs'][idx])):
+            assert np.max(np.abs(got - ref)) <= 1e-13 * max(np.max(np.abs(ref)), scale)
