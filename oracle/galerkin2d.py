@@ -368,3 +368,16 @@ def adaptive_blocks(obs_ends, src_ends, obs_normal, src_normal, k, obs_normal_de
 
     whole = ((0.0, 1.0), (0.0, 1.0))
     return refine(whole[0], whole[1], 0, box(*whole))
+
+
+def maue_block(s_block, k, obs_normal, src_normal, obs_length, src_length):
+    """Hypersingular 2 x 2 block from the single-layer block by the Maue identity
+    (``twod/operators.py:1295,1943``): W = -k^2 (n_o . n_s) S + [[1, -1], [-1, 1]] sum(S) / (L_o L_s),
+    the second term the product of the hat functions' tangential derivatives."""
+    s_block = np.asarray(s_block, dtype=np.complex128)
+    ndn = float(np.dot(np.asarray(obs_normal, float), np.asarray(src_normal, float)))
+    total = (s_block[0, 0] + s_block[0, 1]) + (s_block[1, 0] + s_block[1, 1])
+    denom = max(float(obs_length) * float(src_length), EPS * EPS)
+    quotient = complex(total.real / denom, total.imag / denom)
+    outer = np.array([[1.0, -1.0], [-1.0, 1.0]], dtype=np.complex128)
+    return (-(complex(k) ** 2) * ndn) * s_block + outer * quotient

@@ -20,7 +20,8 @@ records, for real wavenumbers:
   non-adjacent pair closer than 4 element lengths, and the 16-point tensor S and K' blocks
   (``twod/operators.py:223`` ``_integrate_linear_pairs_box_sk_batched``) of the others, and the
   adaptive pairs' blocks by the reference's near-pair dispatcher (``:1080``
-  ``_sk_blocks_near_linear``, whose bisection rule is ``:1172``).
+  ``_sk_blocks_near_linear``, whose bisection rule is ``:1172``), and the hypersingular blocks of
+  the box pairs from their S blocks (``:1943`` ``_maue_blocks``).
 """
 from __future__ import annotations
 
@@ -123,6 +124,11 @@ def main(reference_root):
     ad = [[O._sk_blocks_near_linear(elems[i], elems[j], k, deriv) for i, j in close] for deriv in (False, True)]
     out.update(adaptive_s=np.array([b[0] for b in ad[0]]), adaptive_kd_src=np.array([b[1] for b in ad[0]]),
                adaptive_kd_obs=np.array([b[1] for b in ad[1]]))
+    # hypersingular blocks of the box pairs from their S blocks (the Maue identity)
+    out['box_maue'] = O._maue_blocks(s_box, k, np.array([elems[i].normal for i in box[:, 0]]),
+                                     np.array([elems[j].normal for j in box[:, 1]]),
+                                     np.array([elems[i].length for i in box[:, 0]]),
+                                     np.array([elems[j].length for j in box[:, 1]]))
     np.savez_compressed(os.path.join(HERE, 'galerkin_near.npz'), **out)
     print('wrote galerkin_near.npz:', len(lengths), 'self blocks,', len(rows), 'touching pairs,', len(pairs),
           'near pairs (', int(adaptive.sum()), 'adaptive)')

@@ -93,3 +93,14 @@ def test_adaptive_blocks_match_reference():
         for got, ref in ((s_blk, F['adaptive_s'][idx]), (kd_src, F['adaptive_kd_src'][idx]),
                          (kd_obs, F['adaptive_kd_obs'][idx])):
             assert np.max(np.abs(got - ref)) <= 1e-13 * max(np.max(np.abs(ref)), scale)
+
+
+def test_maue_blocks_match_reference():
+    ends, normals = _ring()
+    box = F['ring_pairs'][~F['ring_adaptive']]
+    k = float(F['ring_k'])
+    for idx, (i, j) in enumerate(box):
+        lo, ls = (float(np.hypot(*(e[1] - e[0]))) for e in (ends[i], ends[j]))
+        got = G.maue_block(F['box_s'][idx], k, normals[i], normals[j], lo, ls)
+        ref = F['box_maue'][idx]
+        assert np.max(np.abs(got - ref)) <= 1e-14 * np.max(np.abs(ref))
