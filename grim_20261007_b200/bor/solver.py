@@ -15,7 +15,6 @@ the CFIE with alpha = 0.5).  Impedance and sheet models are rejected.
 """
 from __future__ import annotations
 
-import ctypes
 import math
 
 import numpy as np

@@ -29,7 +29,7 @@ import numpy as np
 import torch
 
 from .. import _lib
-from ..device import context, ptr, require_cuda, run_pool
+from ..device import context, require_cuda, run_pool
 from ..execution import requested_dense_backend, requested_precision
 from . import certify
 from . import geometry as geo
@@ -145,7 +145,6 @@ def matrix_inf_norm(a):
 
 def _solve_dense_system(a_mat, rhs, condition_diagnostics=None, label='dense system', residual_diagnostics=None):
     """GPU solve + the reference's FP64 backward-error gate (``twod/solver.py:613-773``)."""
-    import scipy.linalg as sla
     a_eval = np.asarray(a_mat, dtype=np.complex128)
     rhs_eval = np.asarray(rhs, dtype=np.complex128)
     if not (np.all(np.isfinite(a_eval)) and np.all(np.isfinite(rhs_eval))):
