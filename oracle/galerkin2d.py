@@ -29,7 +29,12 @@ wavenumber:
 * the close separated pairs (``twod/operators.py:1172`` ``_integrate_linear_pair_adaptive_sk``):
   each box of sub-intervals compared with its four-way bisection by the same tensor rule,
   only the unconverged children refined further, to 1e-9 relative to the sum of the
-  children's norms (at most 12 levels).
+  children's norms (at most 12 levels);
+* the Maue hypersingular blocks from the S blocks (``:1295,1943``);
+* the whole node-based S and observation-normal K' of a contour of at most 192 elements
+  (``:2087`` ``_assemble_multi``, one assembly tile): far pairs (centre distance at least 3 x
+  the longer length, no shared node) by the tensor rule at the tile's calibrated order
+  (``:1443,1474``), near pairs by the routes above, each block added at its nodes.
 
 G = (j/4) H0^(2)(k r); the normal derivative is (j/4) k H1^(2)(k r) (r . n)/r on the source
 normal (negated for the observation normal); r is floored at 1e-12 and k r at 1e-12.
@@ -381,3 +386,66 @@ def maue_block(s_block, k, obs_normal, src_normal, obs_length, src_length):
     quotient = complex(total.real / denom, total.imag / denom)
     outer = np.array([[1.0, -1.0], [-1.0, 1.0]], dtype=np.complex128)
     return (-(complex(k) ** 2) * ndn) * s_block + outer * quotient
+
+
+# ---- whole node-based operators of a closed contour (``twod/operators.py:2087`` ``_assemble_multi``)
+FAR_RATIO = 3.0          # far pairs: centre distance >= 3 x the longer length, no shared node
+FAR_CAP = 8              # the caller's far order, reduced only where the calibrated table allows
+FAR_ORDER_TABLE = (      # (|k| L_max bound, (near, mid, far) orders for linear elements)
+    (0.15, (7, 6, 5)),
+    (0.50, (7, 6, 5)),
+    (1.50, (7, 6, 6)),
+    (3.00, (8, 8, 8)),
+)
+
+
+def far_order(kl_max, ratio_min, cap=FAR_CAP):
+    """Gauss order of a tile whose worst far pair has these parameters
+    (``twod/operators.py:1474`` ``_graded_far_order``, real k, linear elements): near / mid /
+    far columns for the smallest centre-distance ratio below 5, below 10, and beyond."""
+    if not float(ratio_min) >= FAR_RATIO:
+        return int(cap)
+    for bound, (near, mid, far) in FAR_ORDER_TABLE:
+        if kl_max <= bound:
+            order = near if ratio_min < 5.0 else (mid if ratio_min < 10.0 else far)
+            return max(2, min(int(cap), int(order)))
+    return int(cap)
+
+
+def assemble_single_tile(ends, node_ids, normals, k, n_nodes):
+    """Node-based single-layer S and observation-normal K' of straight elements (at most 192,
+    which the reference assembles as one tile with one far order): far pairs by the graded
+    tensor rule, near pairs by the self / touching / adaptive / fixed-rule routes, each 2 x 2
+    block added at its elements' node rows and columns."""
+    ends = [tuple(np.asarray(p, float) for p in e) for e in ends]
+    ne = len(ends)
+    lengths = np.array([float(np.hypot(*(b - a))) for a, b in ends])
+    centres = np.array([0.5 * (a + b) for a, b in ends])
+    S = np.zeros((n_nodes, n_nodes), dtype=np.complex128)
+    K = np.zeros((n_nodes, n_nodes), dtype=np.complex128)
+    dist = np.hypot(centres[:, None, 0] - centres[None, :, 0], centres[:, None, 1] - centres[None, :, 1])
+    ratio = dist / np.maximum(np.maximum(lengths[:, None], lengths[None, :]), EPS)
+    shares = np.array([[bool(set(node_ids[e]) & set(node_ids[f])) for f in range(ne)] for e in range(ne)])
+    far = (ratio >= FAR_RATIO) & ~shares & ~np.eye(ne, dtype=bool)
+    order = far_order(abs(complex(k)) * float(lengths.max()), float(np.min(ratio[far])) if far.any() else np.inf)
+    for e in range(ne):
+        for f in range(ne):
+            if far[e, f]:
+                s_blk, k_blk = box_blocks(ends[e], ends[f], normals[e], normals[f], k, True, order=max(2, order))
+            elif e == f:
+                s_blk, k_blk = self_block(lengths[e], k), np.zeros((2, 2), complex)
+            elif shares[e, f]:
+                obs_start = node_ids[e][0] in node_ids[f]
+                src_start = node_ids[f][0] in node_ids[e]
+                s_blk, k_blk = touching_blocks(ends[e], ends[f], normals[e], normals[f], obs_start, src_start, k,
+                                               True)
+            elif needs_adaptive(ends[e], ends[f]):
+                s_blk, k_blk = adaptive_blocks(ends[e], ends[f], normals[e], normals[f], k, True)
+            else:
+                s_blk, k_blk = box_blocks(ends[e], ends[f], normals[e], normals[f], k, True)
+            rows, cols = node_ids[e], node_ids[f]
+            for a in range(2):
+                for b in range(2):
+                    S[rows[a], cols[b]] += s_blk[a, b]
+                    K[rows[a], cols[b]] += k_blk[a, b]
+    return S, K

@@ -21,7 +21,11 @@ records, for real wavenumbers:
   (``twod/operators.py:223`` ``_integrate_linear_pairs_box_sk_batched``) of the others, and the
   adaptive pairs' blocks by the reference's near-pair dispatcher (``:1080``
   ``_sk_blocks_near_linear``, whose bisection rule is ``:1172``), and the hypersingular blocks of
-  the box pairs from their S blocks (``:1943`` ``_maue_blocks``).
+  the box pairs from their S blocks (``:1943`` ``_maue_blocks``);
+* ``ring_S`` / ``ring_K``: the ring's whole node-based single-layer and observation-normal K'
+  operators by the reference's own assembly (``twod/operators.py:1835``
+  ``_assemble_linear_operator_matrices``: near routes, far pairs in one tile with its graded
+  order, node scatter) at k = 30 and k = 4.
 """
 from __future__ import annotations
 
@@ -101,7 +105,9 @@ def main(reference_root):
     t = np.sort(rng.uniform(0, 2 * math.pi, n))
     r = 0.5 * (1 + 0.15 * rng.standard_normal(n))
     pts = np.stack([r * np.cos(t), r * np.sin(t)], axis=1)
-    elems = [element(LE, 'e', pts[i], pts[(i + 1) % n], i) for i in range(n)]
+    import dataclasses
+    elems = [dataclasses.replace(element(LE, 'e', pts[i], pts[(i + 1) % n], i), node_ids=(i, (i + 1) % n))
+             for i in range(n)]
     pairs, adaptive = [], []
     for i in range(n):
         for j in range(n):
@@ -129,6 +135,14 @@ def main(reference_root):
                                      np.array([elems[j].normal for j in box[:, 1]]),
                                      np.array([elems[i].length for i in box[:, 0]]),
                                      np.array([elems[j].length for j in box[:, 1]]))
+    # the whole single-layer and K' (observation-normal) operators of the ring, node-based,
+    # by the reference's own assembly (one tile: at most 192 elements)
+    from ghost_backend.twod.geometry import LinearMesh, LinearNode
+    mesh = LinearMesh(nodes=[LinearNode(xy=pts[i], key=(i, 0)) for i in range(n)], elements=elems)
+    for kk, tag in ((30.0, 'k30'), (4.0, 'k4')):
+        s_op, k_op = O._assemble_linear_operator_matrices(mesh, kk, True)
+        out[f'ring_S_{tag}'] = np.asarray(s_op)
+        out[f'ring_K_{tag}'] = np.asarray(k_op)
     np.savez_compressed(os.path.join(HERE, 'galerkin_near.npz'), **out)
     print('wrote galerkin_near.npz:', len(lengths), 'self blocks,', len(rows), 'touching pairs,', len(pairs),
           'near pairs (', int(adaptive.sum()), 'adaptive)')

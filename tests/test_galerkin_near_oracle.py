@@ -104,3 +104,15 @@ def test_maue_blocks_match_reference():
         got = G.maue_block(F['box_s'][idx], k, normals[i], normals[j], lo, ls)
         ref = F['box_maue'][idx]
         assert np.max(np.abs(got - ref)) <= 1e-14 * np.max(np.abs(ref))
+
+
+@pytest.mark.parametrize('tag,k', [('k30', 30.0), ('k4', 4.0)])
+def test_whole_ring_operators_match_reference(tag, k):
+    """The ring's node-based S and K' from element blocks (far pairs at the tile's graded
+    order, near pairs by their routes) equal the reference's own assembly."""
+    ends, normals = _ring()
+    n = len(ends)
+    node_ids = [(i, (i + 1) % n) for i in range(n)]
+    S, Kp = G.assemble_single_tile(ends, node_ids, normals, k, n)
+    for got, ref in ((S, F[f'ring_S_{tag}']), (Kp, F[f'ring_K_{tag}'])):
+        assert np.max(np.abs(got - ref)) <= 1e-14 * np.max(np.abs(ref))
