@@ -34,14 +34,20 @@ wavenumber:
 * the whole node-based S and observation-normal K' of a contour of at most 192 elements
   (``:2087`` ``_assemble_multi``, one assembly tile): far pairs (centre distance at least 3 x
   the longer length, no shared node) by the tensor rule at the tile's calibrated order
-  (``:1443,1474``), near pairs by the routes above, each block added at its nodes.
+  (``:1443,1474``), near pairs by the routes above, each block added at its nodes; with the
+  hypersingular W beside them (``:2799``, far S blocks at the W order ``:1512,2433``);
+* the combined PEC system of a closed contour in air as the reference's dense solver receives
+  it (``twod/formulations/regions.py:283-292``, ``twod/formulations/combined_regions.py:21-62,
+  149-204``): S + gamma (D + M/2) for TM, K' - M/2 - gamma W for TE, gamma = 1/(j k), with
+  the consistent mass M and the plane-wave loads, on the solver's reversed node order.
 
 G = (j/4) H0^(2)(k r); the normal derivative is (j/4) k H1^(2)(k r) (r . n)/r on the source
 normal (negated for the observation normal); r is floored at 1e-12 and k r at 1e-12.
 J0, Y0, J1, Y1 are SciPy's (the reference's own call sites, ``operators.py:898``).
 
 Pinned against the reference's own blocks in ``tests/golden/galerkin_near.npz`` (made by
-``tests/golden/make_galerkin_near_golden.py``).
+``tests/golden/make_galerkin_near_golden.py``) and its whole dense systems in
+``tests/golden/ref_dense_system.npz`` (made by ``tests/golden/make_golden.py``).
 """
 from __future__ import annotations
 
@@ -412,22 +418,51 @@ def far_order(kl_max, ratio_min, cap=FAR_CAP):
     return int(cap)
 
 
-def assemble_single_tile(ends, node_ids, normals, k, n_nodes):
+W_FAR_FLOOR = 8          # calibrated W far order for linear elements; 16 outside the calibration
+
+
+def w_far_order(k, lengths, order):
+    """Gauss order of the far tiles that feed W (``twod/operators.py:1512`` ``_graded_w_far_floor``
+    and ``:2433``): the tile's own order raised to the caller's 8 points and to the calibrated W
+    floor, which is 8 for 1e-4 <= |k| L_max <= 3 with no element shorter than 0.001 L_max, else 16."""
+    longest = float(np.max(lengths))
+    calibrated = 1e-4 <= abs(complex(k)) * longest <= 3.0 and float(np.min(lengths)) >= 1e-3 * longest
+    return max(int(order), W_FAR_FLOOR if calibrated else 16, FAR_CAP)
+
+
+def mass_matrix(ends, node_ids, n_nodes):
+    """Consistent linear boundary mass, L [[1/3, 1/6], [1/6, 1/3]] per element at its nodes
+    (``twod/operators.py:3032`` ``_linear_mass_block``, ``twod/assembly/mass.py:6``)."""
+    M = np.zeros((n_nodes, n_nodes), dtype=np.complex128)
+    for (a, b), nd in zip(ends, node_ids):
+        length = float(np.hypot(*(np.asarray(b, float) - np.asarray(a, float))))
+        blk = length * np.array([[1.0 / 3.0, 1.0 / 6.0], [1.0 / 6.0, 1.0 / 3.0]])
+        for i in range(2):
+            for j in range(2):
+                M[nd[i], nd[j]] += blk[i, j]
+    return M
+
+
+def assemble_single_tile(ends, node_ids, normals, k, n_nodes, hypersingular=False):
     """Node-based single-layer S and observation-normal K' of straight elements (at most 192,
     which the reference assembles as one tile with one far order): far pairs by the graded
     tensor rule, near pairs by the self / touching / adaptive / fixed-rule routes, each 2 x 2
-    block added at its elements' node rows and columns."""
+    block added at its elements' node rows and columns.  With ``hypersingular`` the
+    hypersingular W is returned as well: the Maue block of every element pair's S block, the
+    far pairs' S blocks taken at the W far order (``twod/operators.py:2799``)."""
     ends = [tuple(np.asarray(p, float) for p in e) for e in ends]
     ne = len(ends)
     lengths = np.array([float(np.hypot(*(b - a))) for a, b in ends])
     centres = np.array([0.5 * (a + b) for a, b in ends])
     S = np.zeros((n_nodes, n_nodes), dtype=np.complex128)
     K = np.zeros((n_nodes, n_nodes), dtype=np.complex128)
+    W = np.zeros((n_nodes, n_nodes), dtype=np.complex128)
     dist = np.hypot(centres[:, None, 0] - centres[None, :, 0], centres[:, None, 1] - centres[None, :, 1])
     ratio = dist / np.maximum(np.maximum(lengths[:, None], lengths[None, :]), EPS)
     shares = np.array([[bool(set(node_ids[e]) & set(node_ids[f])) for f in range(ne)] for e in range(ne)])
     far = (ratio >= FAR_RATIO) & ~shares & ~np.eye(ne, dtype=bool)
     order = far_order(abs(complex(k)) * float(lengths.max()), float(np.min(ratio[far])) if far.any() else np.inf)
+    w_order = w_far_order(k, lengths, order)
     for e in range(ne):
         for f in range(ne):
             if far[e, f]:
@@ -444,8 +479,79 @@ def assemble_single_tile(ends, node_ids, normals, k, n_nodes):
             else:
                 s_blk, k_blk = box_blocks(ends[e], ends[f], normals[e], normals[f], k, True)
             rows, cols = node_ids[e], node_ids[f]
+            if hypersingular:
+                s_w = (box_blocks(ends[e], ends[f], normals[e], normals[f], k, True, order=w_order)[0]
+                       if far[e, f] else s_blk)
+                w_blk = maue_block(s_w, k, normals[e], normals[f], lengths[e], lengths[f])
             for a in range(2):
                 for b in range(2):
                     S[rows[a], cols[b]] += s_blk[a, b]
                     K[rows[a], cols[b]] += k_blk[a, b]
-    return S, K
+                    if hypersingular:
+                        W[rows[a], cols[b]] += w_blk[a, b]
+    return (S, K, W) if hypersingular else (S, K)
+
+
+# ---- the combined PEC system of a closed contour (``twod/formulations/regions.py:283-292``
+# base rows, ``twod/formulations/combined_regions.py:21-62,149-204`` combined routes)
+def drawn_to_solver_contour(drawn_points):
+    """Nodes of a closed PEC (TYPE 2) contour in the solver's order: the reference reverses
+    every drawn segment (``twod/geometry.py:1009`` ``_apply_user_convention_flip``), so its
+    node j is drawn point -j and its element j runs from node j to node j + 1, the stored
+    normal (-t_y, t_x) (``twod/geometry.py:1935``) pointing into the conductor."""
+    drawn = np.asarray(drawn_points, float)
+    n = len(drawn)
+    return drawn[(-np.arange(n)) % n]
+
+
+def incident_loads(ends, node_ids, normals, n_nodes, k, angles_deg, order=8):
+    """Galerkin loads of the plane wave exp(j k d . r), d = (cos phi, sin phi), and of its
+    normal derivative j k (d . n) exp(j k d . r), at ``order`` Gauss points per element
+    (``twod/operators.py`` ``_linear_element_incident_load_many`` and
+    ``_linear_element_incident_dn_load_many``)."""
+    t, w = unit_gauss(order)
+    phi = np.radians(np.asarray(angles_deg, float))
+    d = np.stack([np.cos(phi), np.sin(phi)], axis=1)
+    load = np.zeros((n_nodes, len(phi)), dtype=np.complex128)
+    dn_load = np.zeros_like(load)
+    for (a, b), nd, nrm in zip(ends, node_ids, normals):
+        a, b = np.asarray(a, float), np.asarray(b, float)
+        length = float(np.hypot(*(b - a)))
+        pts = a[None, :] + t[:, None] * (b - a)[None, :]
+        phase = np.exp(1j * k * (pts @ d.T))                          # (points, angles)
+        dn = phase * (1j * k * (d @ np.asarray(nrm, float)))[None, :]
+        for i, shape in enumerate((1.0 - t, t)):
+            load[nd[i]] += length * ((w * shape) @ phase)
+            dn_load[nd[i]] += length * ((w * shape) @ dn)
+    return load, dn_load
+
+
+def pec_combined_system(nodes, k, angles_deg, polarization, operators=None):
+    """The dense system the reference hands to its dense solver for a closed PEC contour in
+    air (``twod/solver.py:355`` ``_solve_dense_gpu(a_eval, rhs_eval)``), its nodes in the
+    solver's order.  gamma = 1/(j k) (air on the minus side, ``combined_regions.py:39``):
+
+    * TM (Dirichlet trace rows): A = S + gamma (D + M/2), b = -load;
+    * TE (flux rows): A = K' - M/2 - gamma W, b = -(normal-derivative load);
+
+    K' with the observation normal, D the source-normal double layer, which for the
+    symmetric kernel is K' transposed.  ``operators`` = (S, K', W) reuses an assembly."""
+    nodes = np.asarray(nodes, float)
+    n = len(nodes)
+    ends = [(nodes[i], nodes[(i + 1) % n]) for i in range(n)]
+    node_ids = [(i, (i + 1) % n) for i in range(n)]
+    normals = []
+    for a, b in ends:
+        t = (b - a) / np.hypot(*(b - a))
+        normals.append(np.array([-t[1], t[0]]))
+    if operators is None:
+        operators = assemble_single_tile(ends, node_ids, normals, k, n, hypersingular=True)
+    S, Kp, W = operators
+    M = mass_matrix(ends, node_ids, n)
+    gamma = 1.0 / (1j * k)
+    load, dn_load = incident_loads(ends, node_ids, normals, n, k, angles_deg)
+    if polarization == 'TM':
+        return S + gamma * (Kp.T + 0.5 * M), -load
+    if polarization == 'TE':
+        return Kp - 0.5 * M - gamma * W, -dn_load
+    raise ValueError("polarization must be 'TM' or 'TE'")
