@@ -39,7 +39,9 @@ wavenumber:
 * the combined PEC system of a closed contour in air as the reference's dense solver receives
   it (``twod/formulations/regions.py:283-292``, ``twod/formulations/combined_regions.py:21-62,
   149-204``): S + gamma (D + M/2) for TM, K' - M/2 - gamma W for TE, gamma = 1/(j k), with
-  the consistent mass M and the plane-wave loads, on the solver's reversed node order.
+  the consistent mass M and the plane-wave loads, on the solver's reversed node order; and
+  the monostatic scattering width of its solution (single- plus gamma-weighted double-layer
+  far field, sigma = |amp|^2 / (4 k)).
 
 G = (j/4) H0^(2)(k r); the normal derivative is (j/4) k H1^(2)(k r) (r . n)/r on the source
 normal (negated for the observation normal); r is floored at 1e-12 and k r at 1e-12.
@@ -555,3 +557,31 @@ def pec_combined_system(nodes, k, angles_deg, polarization, operators=None):
     if polarization == 'TE':
         return Kp - 0.5 * M - gamma * W, -dn_load
     raise ValueError("polarization must be 'TM' or 'TE'")
+
+
+def pec_combined_sigma(nodes, k, angles_deg, density, order=8):
+    """Monostatic 2-D scattering width of the combined PEC solution ``density`` (one column
+    per angle): amp = sum over elements of L w_q phi_i(q) rho_i exp(j k d . r_q) (single layer)
+    plus the same with rho -> gamma rho and the factor j k (d . n) (double layer), d = (cos phi,
+    sin phi) (``twod/operators.py`` ``_farfield_linear_density_many``, the second potential of
+    ``twod/solver.py:1979`` ``exterior_double_density``); sigma = |amp|^2 / (4 k)
+    (``twod/solver.py:838`` ``_rcs_sigma_from_amp``, ``twod/constants.py:19``)."""
+    nodes = np.asarray(nodes, float)
+    n = len(nodes)
+    rho = np.asarray(density, dtype=np.complex128)
+    t, w = unit_gauss(order)
+    phi = np.radians(np.asarray(angles_deg, float))
+    d = np.stack([np.cos(phi), np.sin(phi)], axis=1)
+    gamma = 1.0 / (1j * k)
+    amp = np.zeros(len(phi), dtype=np.complex128)
+    for i in range(n):
+        a, b = nodes[i], nodes[(i + 1) % n]
+        length = float(np.hypot(*(b - a)))
+        tangent = (b - a) / length
+        normal = np.array([-tangent[1], tangent[0]])
+        pts = a[None, :] + t[:, None] * (b - a)[None, :]
+        phase = np.exp(1j * k * (pts @ d.T))                                  # (points, angles)
+        dens = np.outer(1.0 - t, rho[i]) + np.outer(t, rho[(i + 1) % n])     # (points, angles)
+        factor = 1.0 + gamma * (1j * k * (d @ normal))[None, :]
+        amp += length * np.sum(w[:, None] * dens * phase * factor, axis=0)
+    return 0.25 * np.abs(amp) ** 2 / k
