@@ -33,9 +33,9 @@ METRIC = 'RCS solves/s at N=2048 (mixed vs FP64 GPU, <=0.05 dB); p50/p99 serve l
 UNIT = 'solves/s'
 
 
-# DRAM bytes (read + write) of one captured launch of the tensor-core kernels, from ncu
-# (profiles/k_tc_gemm_airfoil_n2048.md, profiles/k_oz_gemm_airfoil_n2048.md), with that
-# launch's algorithmic flops; a launch's traffic is scaled from it by its flops.
+# DRAM bytes (read + write) of one captured launch of the tensor-core kernels, from one ncu
+# capture of each kernel on the N = 2048 airfoil, with that launch's algorithmic flops; a
+# launch's traffic is scaled from it by its flops.
 NCU_TRAFFIC = {
     'k_tc_gemm<128>': (8.833024e6, 8.0 * 512 * 720 * 256),
     'k_oz_gemm': (454.434816e6 + 23.171584e6, 8.0 * 2048 * 2048 * 720),

@@ -66,6 +66,15 @@ SIGNATURES = [
     ('grim_fill2d', c_int, [c_void_p, c_int, c_int, c_void_p, c_void_p, c_double, c_void_p, c_int64, c_int]),
     ('grim_rhs2d', c_int, [c_void_p, c_int, c_int, c_void_p, c_int, c_void_p, c_double, c_void_p, c_int64, c_int]),
     ('grim_farfield2d', c_int, [c_void_p, c_int, c_void_p, c_int, c_void_p, c_double, c_void_p, c_int64, c_int, c_void_p]),
+    ('grim_gal_near_count', c_int, [c_void_p, c_int, c_void_p, c_void_p, c_void_p, P_int]),
+    ('grim_gal_near_list', c_int, [c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    ('grim_gal_fill', c_int, [c_void_p, c_int, c_int, c_int] + [c_void_p] * 7 + [c_int, c_double, c_int, c_void_p,
+                                                                                  c_int64, c_int]),
+    ('grim_gal_status', c_int, [c_void_p, P_int]),
+    ('grim_gal_rhs', c_int, [c_void_p, c_int, c_int, c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_double,
+                             c_void_p, c_int64, c_int]),
+    ('grim_gal_farfield', c_int, [c_void_p, c_int, c_void_p, c_void_p, c_int, c_void_p, c_double, c_void_p, c_int64,
+                                  c_int, c_void_p]),
     ('grim_zgetrf', c_int, [c_void_p, c_int, c_void_p, c_int64, c_void_p, P_int]),
     ('grim_zgetrs', c_int, [c_void_p, c_int, c_int, c_void_p, c_int64, c_void_p, c_void_p, c_int64]),
     ('grim_cgetrf', c_int, [c_void_p, c_int, c_void_p, c_int64, c_void_p, P_int]),

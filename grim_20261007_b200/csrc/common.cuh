@@ -177,6 +177,23 @@ int grim_workspace(grim_context *h, const char *name, size_t bytes, void **out);
 int grim_upload_gauss(void);
 
 // Scoped device guard
+// A kernel's dynamic shared-memory opt-in (cudaFuncSetAttribute) is a setting of the
+// current device, so each call site remembers it per device, not per process.
+#define GRIM_MAX_DEVICES 64
+struct PerDeviceOnce {
+    bool set[GRIM_MAX_DEVICES] = {};
+    bool needed() const {
+        int dev = -1;
+        cudaGetDevice(&dev);
+        return dev < 0 || dev >= GRIM_MAX_DEVICES || !set[dev];
+    }
+    void mark() {
+        int dev = -1;
+        cudaGetDevice(&dev);
+        if (dev >= 0 && dev < GRIM_MAX_DEVICES) set[dev] = true;
+    }
+};
+
 struct DeviceGuard {
     int prev = -1;
     explicit DeviceGuard(int dev) {

@@ -22,6 +22,7 @@
 #include "dmma.cuh"
 #include "grouped.cuh"
 #include "farblock.cuh"
+#include "galerkin.cuh"
 
 // ============================================================== errors
 static thread_local std::string g_last_error;
@@ -98,6 +99,15 @@ static int upload_tables(int device) {
     }
     GRIM_CHECK_CUDA(cudaMemcpyToSymbol(c_asym_a0, a0, sizeof(a0)));
     GRIM_CHECK_CUDA(cudaMemcpyToSymbol(c_asym_a1, a1, sizeof(a1)));
+    double g0[GAL_ASYM64_TERMS], g1[GAL_ASYM64_TERMS];
+    g0[0] = g1[0] = 1.0;
+    for (int kk = 1; kk < GAL_ASYM64_TERMS; ++kk) {
+        const double odd = (2.0 * kk - 1.0) * (2.0 * kk - 1.0);
+        g0[kk] = g0[kk - 1] * (0.0 - odd) / (8.0 * kk);
+        g1[kk] = g1[kk - 1] * (4.0 - odd) / (8.0 * kk);
+    }
+    GRIM_CHECK_CUDA(cudaMemcpyToSymbol(c_gal_a0, g0, sizeof(g0)));
+    GRIM_CHECK_CUDA(cudaMemcpyToSymbol(c_gal_a1, g1, sizeof(g1)));
     g_tables_ready[device] = 1;
     return GRIM_OK;
 }
@@ -300,17 +310,153 @@ extern "C" int grim_farfield2d(grim_handle_t h, int n, const double *geom, int n
     return GRIM_OK;
 }
 
+// ============================================================== linear-Galerkin fill
+static bool gal_elem_ok(int ne, const double *elem, const int *nodes) { return ne > 0 && elem && nodes; }
+
+extern "C" int grim_gal_near_count(grim_handle_t h, int ne, const double *elem, const int *nodes, int *row_off,
+                                   int *nnz_host) {
+    if (!h || !gal_elem_ok(ne, elem, nodes) || !row_off || !nnz_host)
+        return grim_fail(GRIM_ERR_ARGUMENT, "grim_gal_near_count: bad arguments");
+    DeviceGuard g(h->device);
+    void *pc = nullptr;
+    GRIM_TRY(grim_workspace(h, "gal_count", (size_t)ne * sizeof(int), &pc));
+    const int wpb = 8;
+    k_gal_near_count<<<ceil_div(ne, wpb), 32 * wpb, 0, h->stream>>>(ne, elem, (const int2 *)nodes, (int *)pc);
+    GRIM_CHECK_LAUNCH(h, "k_gal_near_count");
+    k_gal_scan<<<1, 1024, 0, h->stream>>>(ne, (const int *)pc, row_off);
+    GRIM_CHECK_LAUNCH(h, "k_gal_scan");
+    GRIM_CHECK_CUDA(cudaMemcpyAsync(nnz_host, row_off + ne, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    GRIM_CHECK_CUDA(cudaStreamSynchronize(h->stream));
+    return GRIM_OK;
+}
+
+extern "C" int grim_gal_near_list(grim_handle_t h, int ne, const double *elem, const int *nodes, const int *row_off,
+                                  int *col, int *route) {
+    if (!h || !gal_elem_ok(ne, elem, nodes) || !row_off || !col || !route)
+        return grim_fail(GRIM_ERR_ARGUMENT, "grim_gal_near_list: bad arguments");
+    DeviceGuard g(h->device);
+    const int wpb = 8;
+    k_gal_near_list<<<ceil_div(ne, wpb), 32 * wpb, 0, h->stream>>>(ne, elem, (const int2 *)nodes, row_off, col, route);
+    GRIM_CHECK_LAUNCH(h, "k_gal_near_list");
+    return GRIM_OK;
+}
+
+static int gal_err_flag(grim_context *h, int **out) {
+    void *p = nullptr;
+    const bool fresh = h->ws.find("gal_err") == h->ws.end();
+    GRIM_TRY(grim_workspace(h, "gal_err", sizeof(int), &p));
+    if (fresh) GRIM_CHECK_CUDA(cudaMemsetAsync(p, 0, sizeof(int), h->stream));
+    *out = (int *)p;
+    return GRIM_OK;
+}
+
+template <typename C>
+static int gal_fill_impl(grim_context *h, int pol, int ne, int n, const double *elem, const int2 *nodes,
+                         const int *start_of, const int *end_of, const int *row_off, const int *col, const int *route,
+                         int nnz, double k, int far_min_order, C *Z, int64_t ldz) {
+    void *pnb = nullptr, *pe = nullptr;
+    int *err = nullptr;
+    GRIM_TRY(gal_err_flag(h, &err));
+    GRIM_TRY(grim_workspace(h, "gal_nb", (size_t)nnz * 8 * sizeof(double2), &pnb));
+    GRIM_TRY(grim_workspace(h, "gal_e", (size_t)ne * ne * 4 * sizeof(C), &pe));
+    double2 *nbk = (double2 *)pnb;
+    C *E = (C *)pe;
+    k_gal_near<<<ceil_div(nnz, GAL_NEAR_WARPS), GAL_NEAR_WARPS * 32, 0, h->stream>>>(ne, nnz, elem, nodes, row_off,
+                                                                                     col, route, k, nbk, err);
+    GRIM_CHECK_LAUNCH(h, "k_gal_near");
+    const int tiles = ceil_div(ne, GAL_TILE);
+    dim3 fg(tiles, tiles);
+    if (pol == GRIM_POL_TM)
+        k_gal_far<GRIM_POL_TM, C><<<fg, GAL_FAR_THREADS, 0, h->stream>>>(ne, elem, nodes, k, far_min_order, E);
+    else
+        k_gal_far<GRIM_POL_TE, C><<<fg, GAL_FAR_THREADS, 0, h->stream>>>(ne, elem, nodes, k, far_min_order, E);
+    GRIM_CHECK_LAUNCH(h, "k_gal_far");
+    if (pol == GRIM_POL_TM)
+        k_gal_near_route<GRIM_POL_TM, C><<<ceil_div(nnz, 128), 128, 0, h->stream>>>(ne, nnz, elem, row_off, col, nbk, k, E);
+    else
+        k_gal_near_route<GRIM_POL_TE, C><<<ceil_div(nnz, 128), 128, 0, h->stream>>>(ne, nnz, elem, row_off, col, nbk, k, E);
+    GRIM_CHECK_LAUNCH(h, "k_gal_near_route");
+    dim3 gg(ceil_div(n, 128), n);
+    k_gal_gather<C><<<gg, 128, 0, h->stream>>>(ne, n, start_of, end_of, E, Z, ldz);
+    GRIM_CHECK_LAUNCH(h, "k_gal_gather");
+    return GRIM_OK;
+}
+
+extern "C" int grim_gal_fill(grim_handle_t h, int pol, int ne, int n, const double *elem, const int *nodes,
+                             const int *start_of, const int *end_of, const int *row_off, const int *col,
+                             const int *route, int nnz, double k, int far_min_order, void *Z, int64_t ldz,
+                             int out_complex64) {
+    if (!h || !gal_elem_ok(ne, elem, nodes) || n <= 0 || n > 65535 || !start_of || !end_of || !row_off || !col ||
+        !route || nnz < ne || !Z || ldz < n || !(k > 0) || far_min_order < 0 || far_min_order > GAL_MAX_Q ||
+        (pol != GRIM_POL_TM && pol != GRIM_POL_TE))
+        return grim_fail(GRIM_ERR_ARGUMENT, "grim_gal_fill: bad arguments");
+    DeviceGuard g(h->device);
+    if (out_complex64)
+        return gal_fill_impl<float2>(h, pol, ne, n, elem, (const int2 *)nodes, start_of, end_of, row_off, col, route,
+                                     nnz, k, far_min_order, (float2 *)Z, ldz);
+    return gal_fill_impl<double2>(h, pol, ne, n, elem, (const int2 *)nodes, start_of, end_of, row_off, col, route,
+                                  nnz, k, far_min_order, (double2 *)Z, ldz);
+}
+
+extern "C" int grim_gal_status(grim_handle_t h, int *flag_host) {
+    if (!h || !flag_host) return grim_fail(GRIM_ERR_ARGUMENT, "grim_gal_status: bad arguments");
+    DeviceGuard g(h->device);
+    int *err = nullptr;
+    GRIM_TRY(gal_err_flag(h, &err));
+    GRIM_CHECK_CUDA(cudaMemcpyAsync(flag_host, err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    GRIM_CHECK_CUDA(cudaMemsetAsync(err, 0, sizeof(int), h->stream));
+    GRIM_CHECK_CUDA(cudaStreamSynchronize(h->stream));
+    return GRIM_OK;
+}
+
+extern "C" int grim_gal_rhs(grim_handle_t h, int pol, int n, const double *elem, const int *start_of,
+                            const int *end_of, int nang, const double *angles_deg, double k, void *B, int64_t ldb,
+                            int out_complex64) {
+    if (!h || n <= 0 || !elem || !start_of || !end_of || nang <= 0 || nang > 65535 || !angles_deg || !B || ldb < n ||
+        !(k > 0) || (pol != GRIM_POL_TM && pol != GRIM_POL_TE))
+        return grim_fail(GRIM_ERR_ARGUMENT, "grim_gal_rhs: bad arguments");
+    DeviceGuard g(h->device);
+    dim3 grid(ceil_div(n, 128), nang);
+#define GAL_RHS(P, C) k_gal_rhs<P, C><<<grid, 128, 0, h->stream>>>(n, elem, start_of, end_of, nang, angles_deg, k, (C *)B, ldb)
+    if (out_complex64) {
+        if (pol == GRIM_POL_TM) GAL_RHS(GRIM_POL_TM, float2);
+        else GAL_RHS(GRIM_POL_TE, float2);
+    } else {
+        if (pol == GRIM_POL_TM) GAL_RHS(GRIM_POL_TM, double2);
+        else GAL_RHS(GRIM_POL_TE, double2);
+    }
+#undef GAL_RHS
+    GRIM_CHECK_LAUNCH(h, "k_gal_rhs");
+    return GRIM_OK;
+}
+
+extern "C" int grim_gal_farfield(grim_handle_t h, int ne, const double *elem, const int *nodes, int nang,
+                                 const double *angles_deg, double k, const void *X, int64_t ldx, int x_complex64,
+                                 void *amp) {
+    if (!h || !gal_elem_ok(ne, elem, nodes) || nang <= 0 || !angles_deg || !X || !amp || !(k > 0))
+        return grim_fail(GRIM_ERR_ARGUMENT, "grim_gal_farfield: bad arguments");
+    DeviceGuard g(h->device);
+    if (x_complex64)
+        k_gal_farfield<float2><<<nang, 256, 0, h->stream>>>(ne, elem, (const int2 *)nodes, nang, angles_deg, k,
+                                                            (const float2 *)X, ldx, (double2 *)amp);
+    else
+        k_gal_farfield<double2><<<nang, 256, 0, h->stream>>>(ne, elem, (const int2 *)nodes, nang, angles_deg, k,
+                                                             (const double2 *)X, ldx, (double2 *)amp);
+    GRIM_CHECK_LAUNCH(h, "k_gal_farfield");
+    return GRIM_OK;
+}
+
 // ============================================================== GEMM launcher
 static int tc_enabled();
 
 template <bool NEG, bool BETA>
 static int dmma_gemm(grim_context *h, int M, int N, int K, const double2 *A, int64_t lda, const double2 *B,
                      int64_t ldb, double2 *C, int64_t ldc) {
-    static bool attr = false;
-    if (!attr) {
+    static PerDeviceOnce attr;
+    if (attr.needed()) {
         GRIM_CHECK_CUDA(
             cudaFuncSetAttribute(k_gemm_dmma<NEG, BETA>, cudaFuncAttributeMaxDynamicSharedMemorySize, DM_SMEM_BYTES));
-        attr = true;
+        attr.mark();
     }
     dim3 grid(ceil_div(M, DM_BM), ceil_div(N, DM_BN));
     k_gemm_dmma<NEG, BETA><<<grid, DM_THREADS, DM_SMEM_BYTES, h->stream>>>(M, N, K, A, lda, B, ldb, C, ldc);
@@ -414,11 +560,11 @@ template <int BN, int STAGES, bool STAGE_C>
 static int tc_launch(grim_context *h, const TcPacked &A, const TcPacked &B, float2 *C, int64_t ldc, int M, int N,
                      int Kc, float alpha, int ow_lo, int ow_hi, int *err) {
     using Cfg = TcCfg<BN, STAGES, STAGE_C>;
-    static bool attr = false;
-    if (!attr) {
+    static PerDeviceOnce attr;
+    if (attr.needed()) {
         GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_tc_gemm<BN, STAGES, STAGE_C>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM_BYTES));
-        attr = true;
+        attr.mark();
     }
     dim3 grid(A.rows_p / TC_BM, ceil_div(N, BN));  // B.rows_p is the row stride of the packed B
     k_tc_gemm<BN, STAGES, STAGE_C><<<grid, TC_THREADS, Cfg::SMEM_BYTES, h->stream>>>(
@@ -499,13 +645,13 @@ extern "C" int grim_cgemm_sub(grim_handle_t h, int M, int N, int K, const void *
 // ============================================================== getrf / getrs
 template <typename C>
 static int smem_opt_in() {
-    static bool done = false;
-    if (done) return GRIM_OK;
+    static PerDeviceOnce done;
+    if (!done.needed()) return GRIM_OK;
     const int tri = (NB * NBP + NB) * (int)sizeof(C);
     GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_panel_apply<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, tri));
     GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_trsm_diag<C, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, tri));
     GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_trsm_diag<C, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, tri));
-    done = true;
+    done.mark();
     return GRIM_OK;
 }
 
@@ -1080,11 +1226,11 @@ template <int S, int BN>
 static int oz_launch(grim_context *h, const OzA &qa, const int8_t *P, int Np, const int *col_exp, const double2 *B,
                      int64_t ldb, double2 *R, int64_t ldr, int nrhs, int *err) {
     using Cfg = OzCfg<S, BN>;
-    static bool attr = false;
-    if (!attr) {
+    static PerDeviceOnce attr;
+    if (attr.needed()) {
         GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_oz_gemm<S, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              Cfg::SMEM_BYTES));
-        attr = true;
+        attr.mark();
     }
     dim3 grid(Np / BN, qa.Rp / TC_BM);
     k_oz_gemm<S, BN><<<grid, TC_THREADS, Cfg::SMEM_BYTES, h->stream>>>(
@@ -1552,8 +1698,8 @@ static int grp_getrf(grim_context *h, int count, const int *n, void *const *A, c
                      bool use_graph, int *info, int *pivoted) {
     GrpPlan P;
     GRIM_TRY(grp_plan<C>(count, n, grp_bn(), &P));
-    static bool attr = false;
-    if (!attr) {
+    static PerDeviceOnce attr;
+    if (attr.needed()) {
         const int tri = (NB * NBP + NB) * (int)sizeof(C);
         GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_grp_apply<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, tri));
         if constexpr (sizeof(C) == sizeof(float2))
@@ -1571,7 +1717,7 @@ static int grp_getrf(grim_context *h, int count, const int *n, void *const *A, c
         else
             GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_grp_dmma_update, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                  DM_SMEM_BYTES));
-        attr = true;
+        attr.mark();
     }
     // per-system device buffers, carved from one workspace at 256-byte boundaries
     auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
@@ -1758,14 +1904,14 @@ extern "C" int grim_far_block(grim_handle_t h, int64_t mb, int64_t nb, int q, in
         return 3;
     }
     const size_t smem = intervals + 1 <= FAR_SMEM_BOUNDS ? (size_t)(intervals + 1) * sizeof(double) : 0;
-    static bool attr = false;
-    if (!attr) {
+    static PerDeviceOnce attr;
+    if (attr.needed()) {
         const int mx = FAR_SMEM_BOUNDS * (int)sizeof(double);
         GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_far_block<0, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
         GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_far_block<2, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
         GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_far_block<3, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
         GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_far_block<4, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-        attr = true;
+        attr.mark();
     }
 #define FAR_LAUNCH(W, MINB)                                                                                      \
     k_far_block<W, MINB><<<(unsigned)blocks, threads, smem, h->stream>>>(mb, nb, q, width, obs_pts, src_pts, qw, phi, \

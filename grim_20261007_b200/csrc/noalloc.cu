@@ -15,9 +15,12 @@
 // rejected with GRIM_ERR_ARGUMENT and a message, before any GPU work.
 //
 // Set-up: host code cannot pass the array's name to a kernel (in host code the name is
-// only a host-side stand-in, not a device address), so the first call on each device,
-// with that device current, looks the device address up once with cudaGetSymbolAddress
-// and caches it.  Make that first call before any stream capture on that device.
+// only a host-side stand-in, not a device address), so every call, with the handle's
+// device current, looks the device address up with cudaGetSymbolAddress (cheap) and
+// checks the result.  Looking it up per call, not caching it, keeps the address valid
+// if the device's context is torn down and recreated between calls.  The first lookup on
+// a device may load the library's module there, so make the first call on each device
+// before any stream capture on it.
 //
 // Sharing: every call on a device uses the same array and leaves its contents behind.
 // Each call writes every scratch word before reading it (the residual starts as a copy
@@ -25,8 +28,6 @@
 // but two calls whose GPU work overlaps (different streams, threads or handles on the
 // same device) race on the array and must be serialized by the caller.
 #include <cuda_runtime.h>
-
-#include <mutex>
 
 #define GRIM_NOALLOC_MAX_N 1024
 #define GRIM_NOALLOC_MAX_NRHS 128
@@ -43,23 +44,13 @@
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[GRIM_NOALLOC_SCRATCH_BYTES];
 
-#define NOALLOC_MAX_DEVICES 64
-static std::mutex g_noalloc_mutex;
-static void *g_noalloc_ptr[NOALLOC_MAX_DEVICES];
-
-// Device address of the scratch array on h's device (looked up once per device).
+// Device address of the scratch array on h's device, looked up on every call.
 static int noalloc_scratch(grim_context *h, unsigned char **out) {
-    if (h->device < 0 || h->device >= NOALLOC_MAX_DEVICES)
-        return grim_fail(GRIM_ERR_ARGUMENT, "grim_backward_error_noalloc: device index out of range");
-    std::lock_guard<std::mutex> lk(g_noalloc_mutex);
-    if (!g_noalloc_ptr[h->device]) {
-        DeviceGuard g(h->device);
-        void *p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess) return grim_cuda_check(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
-        g_noalloc_ptr[h->device] = p;
-    }
-    *out = (unsigned char *)g_noalloc_ptr[h->device];
+    DeviceGuard g(h->device);
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return grim_cuda_check(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+    *out = (unsigned char *)p;
     return GRIM_OK;
 }
 

@@ -4,8 +4,9 @@ Mirrors the reference's scoped options:
 * ``linear_precision('double'|'mixed')`` -- ``linalg/refined_lu.py:13-22``;
 * ``GHOST_DENSE_BACKEND`` in {cpu, auto, gpu} and ``GHOST_DENSE_GPU_MIN_N`` --
   ``twod/solver.py:291-311``, ``twod/constants.py:25-28``.  This package is the GPU
-  backend, so ``cpu`` is accepted (for configuration compatibility) but still runs
-  on the GPU: there is no CPU fallback in this product.
+  backend and has no CPU solver, so ``cpu`` (a request for the reference's CPU LAPACK
+  path) is refused with ``RuntimeError`` by every solve instead of running on the GPU
+  unasked; ``auto`` and ``gpu`` both run on the GPU.
 """
 from __future__ import annotations
 
@@ -46,3 +47,12 @@ def requested_dense_backend():
     if minimum_n < 1:
         raise ValueError(f'{DENSE_GPU_MIN_N_ENV} must be a positive integer.')
     return backend, minimum_n
+
+
+def require_gpu_dense_backend():
+    """Refuse ``GHOST_DENSE_BACKEND=cpu``: this package has no CPU solver to honour it."""
+    backend, _ = requested_dense_backend()
+    if backend == 'cpu':
+        raise RuntimeError(f'{DENSE_GPU_BACKEND_ENV}=cpu selects the reference CPU solver, which this GPU package '
+                           'does not provide; unset it or use auto/gpu.')
+    return backend

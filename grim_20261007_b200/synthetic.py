@@ -26,28 +26,37 @@ def circle(radius, n):
     return np.stack([radius * np.cos(th), radius * np.sin(th)], axis=1)
 
 
-def naca_symmetric(thickness, n, chord=1.0):
-    """NACA 00tt airfoil with cosine node spacing and a sharp closed trailing edge.
+def naca_symmetric(thickness, n, chord=1.0, closed_te=False):
+    """NACA 00tt airfoil with cosine node spacing, ``n`` elements in total (even), clockwise.
 
-    Half-thickness y_t = 5 t c [0.2969 sqrt(x) - 0.1260 x - 0.3516 x^2 + 0.2843 x^3 - 0.1036 x^4]
-    (the closed-trailing-edge variant of the last coefficient, so y_t(1) = 0).
-    ``n`` panels in total (even); n/2 per surface; clockwise from the trailing edge
-    along the lower surface to the leading edge, then back along the upper surface.
+    Half-thickness y_t = 5 t c [0.2969 sqrt(x) - 0.1260 x - 0.3516 x^2 + 0.2843 x^3 + a4 x^4].
+
+    * default: the standard a4 = -0.1015.  The trailing edge keeps a finite thickness
+      2 y_t(c) = 0.021 t c; its base is closed by two straight elements through (c, 0), and
+      each surface has n/2 - 1 elements.  Vertices start at (c, 0), go down the base, along
+      the lower surface to the leading edge and back along the upper surface.
+    * ``closed_te``: a4 = -0.1036, y_t(c) = 0, a sharp trailing edge and n/2 elements per
+      surface, starting at the trailing edge.  At high element counts the upper and lower
+      vertices next to its tip come closer (7e-7 m at n = 2048, t = 12 %) than the
+      reference's crack tolerance, and the reference refuses the contour.
     """
     if n % 2:
         raise ValueError("NACA panel count must be even")
-    m = n // 2
+    a4 = -0.1036 if closed_te else -0.1015
+    m = n // 2 if closed_te else n // 2 - 1
+    if m < 2:
+        raise ValueError("NACA panel count too small")
     beta = np.pi * np.arange(m + 1) / m
     x = 0.5 * (1.0 + np.cos(beta))  # 1 -> 0
-    xs = x
-    yt = 5.0 * thickness * (0.2969 * np.sqrt(xs) - 0.1260 * xs - 0.3516 * xs ** 2 + 0.2843 * xs ** 3
-                            - 0.1036 * xs ** 4)
-    yt[0] = 0.0
+    yt = 5.0 * thickness * (0.2969 * np.sqrt(x) - 0.1260 * x - 0.3516 * x ** 2 + 0.2843 * x ** 3 + a4 * x ** 4)
     yt[-1] = 0.0
-    lower = np.stack([x * chord, -yt * chord], axis=1)          # TE -> LE along the lower surface
+    if closed_te:
+        yt[0] = 0.0
+    lower = np.stack([x * chord, -yt * chord], axis=1)            # TE -> LE along the lower surface
     upper = np.stack([x[::-1] * chord, yt[::-1] * chord], axis=1)  # LE -> TE along the upper surface
-    verts = np.concatenate([lower[:-1], upper[:-1]], axis=0)
-    return verts
+    if closed_te:
+        return np.concatenate([lower[:-1], upper[:-1]], axis=0)
+    return np.concatenate([[[chord, 0.0]], lower, upper[1:]], axis=0)
 
 
 def superellipse(a, b, p, n):

@@ -2,7 +2,9 @@
 
 Everything here runs in libgrimgpu kernels on the current torch stream; tensors are
 torch CUDA tensors used only as device memory.  Column-major matrices are held in
-tensors of shape (ncols, ld).
+tensors of shape (ncols, ld).  A body is either a pulse-basis ``DeviceBody`` (point-matched
+EFIE / MFIE) or a linear-Galerkin ``galerkin.GalerkinBody`` (the reference's combined
+formulation); ``fill``, ``rhs`` and ``farfield`` dispatch on it, the solve is the same.
 """
 from __future__ import annotations
 
@@ -49,6 +51,8 @@ class DeviceBody:
 
 
 def fill(body, k, pol, complex64=False, out=None, ctx=None):
+    if hasattr(body, 'fill_matrix'):  # linear-Galerkin body (galerkin.GalerkinBody)
+        return body.fill_matrix(k, canonical_pol(pol), complex64=complex64, out=out, ctx=ctx)
     ctx = ctx or context()
     n = body.n
     dt = torch.complex64 if complex64 else torch.complex128
@@ -60,6 +64,8 @@ def fill(body, k, pol, complex64=False, out=None, ctx=None):
 
 
 def rhs(body, k, pol, angles_dev, complex64=False, out=None, ctx=None):
+    if hasattr(body, 'rhs_matrix'):
+        return body.rhs_matrix(k, canonical_pol(pol), angles_dev, complex64=complex64, out=out, ctx=ctx)
     ctx = ctx or context()
     n, nang = body.n, int(angles_dev.numel())
     dt = torch.complex64 if complex64 else torch.complex128
@@ -70,6 +76,8 @@ def rhs(body, k, pol, angles_dev, complex64=False, out=None, ctx=None):
 
 
 def farfield(body, k, angles_dev, x, out=None, ctx=None):
+    if hasattr(body, 'far_amplitude'):
+        return body.far_amplitude(k, angles_dev, x, out=out, ctx=ctx)
     ctx = ctx or context()
     nang = int(angles_dev.numel())
     amp = out if out is not None else torch.empty(nang, dtype=torch.complex128, device=body.geom.device)

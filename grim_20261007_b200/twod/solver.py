@@ -30,7 +30,7 @@ import torch
 
 from .. import _lib
 from ..device import context, require_cuda, run_pool
-from ..execution import requested_dense_backend, requested_precision
+from ..execution import require_gpu_dense_backend, requested_precision
 from . import certify
 from . import geometry as geo
 from . import operators as ops
@@ -149,7 +149,7 @@ def _solve_dense_system(a_mat, rhs, condition_diagnostics=None, label='dense sys
     rhs_eval = np.asarray(rhs, dtype=np.complex128)
     if not (np.all(np.isfinite(a_eval)) and np.all(np.isfinite(rhs_eval))):
         raise FloatingPointError(f'{label} contains non-finite values.')
-    requested, _ = requested_dense_backend()
+    requested = require_gpu_dense_backend()
     solution, device = _solve_dense_gpu(a_eval, rhs_eval)
     matrix_inf = matrix_inf_norm(a_eval)
 
@@ -410,6 +410,7 @@ def _sweep_many(snapshots, frequencies_ghz, elevations_deg, pols, geometry_units
     snapshot, {pol: reference-shaped channel result} (with the per-system outputs under
     ``'_outs'``)."""
     freqs, elevs = _validate_request(frequencies_ghz, elevations_deg, cfie_alpha, compute_condition_number)
+    require_gpu_dense_backend()
     require_cuda()
     precision = requested_precision()
     mesh_list = [_MeshCache(snap, geometry_units, max_panels, mesh_reference_ghz) for snap in snapshots]

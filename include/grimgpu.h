@@ -19,6 +19,9 @@
  *   grim_fill2d          twod/operators.py:2087-2607  _assemble_multi (system-matrix fill)
  *   grim_rhs2d           twod/assembly/kernels.py:223-294  incident_loads
  *   grim_farfield2d      twod/assembly/kernels.py:163-219  farfield (matched monostatic)
+ *   grim_gal_*           twod/operators.py:2087-2607 _assemble_multi, combined_regions.py:149-204,
+ *                        scatter.py:282-368 (linear-Galerkin S + gamma(D + M/2) / K' - M/2 - gamma W fill),
+ *                        twod/assembly/kernels.py:223-294 loads, twod/operators.py:2925-3030 far field
  *   grim_backward_error  twod/solver.py:695-720  backward_metrics (normwise backward error)
  *   grim_bor_*           bor/solver.py:1769-1962,2558-2608  per-mode assembly, excitation, far field
  *   ghost_far_block      twod/assembly/native/far.c:193-207  ghost_far_block (same signature, GPU)
@@ -99,6 +102,45 @@ int grim_rhs2d(grim_handle_t h, int pol, int n, const double *geom, int nang, co
 int grim_farfield2d(grim_handle_t h, int n, const double *geom, int nang, const double *angles_deg,
                     double k, const void *X, int64_t ldx, int x_complex64, void *amp);
 
+/* ---- 2-D linear-Galerkin combined-field fill (the reference's own formulation) ----
+ * Replaces twod/operators.py:2087-2607 _assemble_multi with the combined routing of
+ * twod/formulations/combined_regions.py:21-62,149-204 and the scatter of
+ * twod/assembly/scatter.py:282-368 (closed PEC contours in air, real k).
+ * elem: 8*ne doubles per element (ax, ay, bx, by, nx, ny, L, 0): start and end point, unit
+ *       normal (-t_y, t_x) of the tangent t = (b - a)/L, length.
+ * nodes: 2*ne ints, the element's start and end node.  start_of / end_of: n ints, the
+ *       element that starts / ends at each node (-1 for none).
+ * Near-pair structure (geometry only, reusable for every k and polarisation):
+ *   grim_gal_near_count  row_off (ne + 1 ints, device) = CSR offsets of the pairs that are
+ *                        not far (centre distance < 3 max(L), a shared node, or self);
+ *                        *nnz_host = row_off[ne] (synchronises the stream);
+ *   grim_gal_near_list   col (nnz ints, ascending per row) and route (nnz ints: 0 self,
+ *                        1 touching, 2 16-point tensor rule, 3 adaptive bisection).
+ * grim_gal_fill writes the n x n node matrix: TM (pol 0) S + gamma (D + M/2), TE (pol 1)
+ * K' - M/2 - gamma W, gamma = 1/(j k).  far_min_order: floor on the far Gauss order (the
+ * TE rows' W rule: 8, or 16 outside its calibration; 0 for TM).  Near pairs in FP64;
+ * out_complex64 stores Z as complex64.  An adaptive pair that did not converge or a
+ * failed self series sets a flag that grim_gal_status returns (and clears; synchronises).
+ * grim_gal_rhs: B[:, a] = TM -load, TE -(normal-derivative load) of the plane wave
+ *   exp(jk d_a.x), d_a = (cos, sin)(angle_deg[a]) (twod/assembly/kernels.py:223-294).
+ * grim_gal_farfield: amp[a] = sum_e L_e int (phi_0 x_n0 + phi_1 x_n1) exp(jk d_a.x)
+ *   (1 + d_a.n_e) (twod/operators.py:2925-3030 single + gamma double layer). */
+int grim_gal_near_count(grim_handle_t h, int ne, const double *elem, const int *nodes, int *row_off,
+                        int *nnz_host);
+int grim_gal_near_list(grim_handle_t h, int ne, const double *elem, const int *nodes, const int *row_off,
+                       int *col, int *route);
+int grim_gal_fill(grim_handle_t h, int pol, int ne, int n, const double *elem, const int *nodes,
+                  const int *start_of, const int *end_of, const int *row_off, const int *col,
+                  const int *route, int nnz, double k, int far_min_order, void *Z, int64_t ldz,
+                  int out_complex64);
+int grim_gal_status(grim_handle_t h, int *flag_host);
+int grim_gal_rhs(grim_handle_t h, int pol, int n, const double *elem, const int *start_of,
+                 const int *end_of, int nang, const double *angles_deg, double k, void *B, int64_t ldb,
+                 int out_complex64);
+int grim_gal_farfield(grim_handle_t h, int ne, const double *elem, const int *nodes, int nang,
+                      const double *angles_deg, double k, const void *X, int64_t ldx, int x_complex64,
+                      void *amp);
+
 /* ---- dense LU / solve ------------------------------------------------------------
  * grim_zgetrf / grim_cgetrf: LAPACK getrf semantics (partial pivoting by |re|+|im|,
  * 1-based ipiv, info > 0 for an exactly singular U).  The factorization first
@@ -141,10 +183,11 @@ int grim_backward_error(grim_handle_t h, int n, int nrhs, const void *A, int64_t
  * allocator): same arguments and result as grim_backward_error, but its scratch is one
  * fixed array compiled into the library (about 2.6 MB on every device that loads it,
  * kept until the process exits) instead of handle workspace.  Limits: n <= 1024,
- * nrhs <= 128; larger sizes return GRIM_ERR_ARGUMENT.  The first call on a device looks
- * up the array's device address; make that first call before any stream capture on
- * that device.  All calls on a device share the array: calls whose GPU work overlaps
- * race and must be serialized by the caller. */
+ * nrhs <= 128; larger sizes return GRIM_ERR_ARGUMENT.  Every call looks up the array's
+ * device address on the handle's device (so a recreated device context is picked up);
+ * the first lookup on a device may load the library's module there, so make the first
+ * call on each device before any stream capture on it.  All calls on a device share the
+ * array: calls whose GPU work overlaps race and must be serialized by the caller. */
 int grim_backward_error_noalloc(grim_handle_t h, int n, int nrhs, const void *A, int64_t lda, int a_complex64,
                                 const void *X, int64_t ldx, const void *B, int64_t ldb, double *berr_dev);
 

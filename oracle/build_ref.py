@@ -24,8 +24,11 @@ FAR_LIB = os.path.join(OUT_DIR, 'libghost_far_ref.so')
 REL = os.path.join('tools', 'GHOST', 'ghost_backend', 'twod', 'assembly', 'native', 'far.c')
 
 
-def build(reference_root='/root/reference'):
-    src = os.path.join(reference_root, REL)
+REFERENCE_ROOT = os.environ.get('GRIM_REFERENCE_ROOT', '/root/reference')
+
+
+def build(reference_root=None):
+    src = os.path.join(reference_root or REFERENCE_ROOT, REL)
     if not os.path.exists(src):
         return None
     cc = shutil.which('gcc') or shutil.which('cc')

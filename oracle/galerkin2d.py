@@ -561,11 +561,17 @@ def pec_combined_system(nodes, k, angles_deg, polarization, operators=None):
 
 def pec_combined_sigma(nodes, k, angles_deg, density, order=8):
     """Monostatic 2-D scattering width of the combined PEC solution ``density`` (one column
+    per angle): sigma = |amp|^2 / (4 k) (``twod/solver.py:838`` ``_rcs_sigma_from_amp``,
+    ``twod/constants.py:19``), amp from ``pec_combined_amplitude``."""
+    return 0.25 * np.abs(pec_combined_amplitude(nodes, k, angles_deg, density, order)) ** 2 / k
+
+
+def pec_combined_amplitude(nodes, k, angles_deg, density, order=8):
+    """Monostatic far-field amplitude of the combined PEC solution ``density`` (one column
     per angle): amp = sum over elements of L w_q phi_i(q) rho_i exp(j k d . r_q) (single layer)
     plus the same with rho -> gamma rho and the factor j k (d . n) (double layer), d = (cos phi,
     sin phi) (``twod/operators.py`` ``_farfield_linear_density_many``, the second potential of
-    ``twod/solver.py:1979`` ``exterior_double_density``); sigma = |amp|^2 / (4 k)
-    (``twod/solver.py:838`` ``_rcs_sigma_from_amp``, ``twod/constants.py:19``)."""
+    ``twod/solver.py:1979`` ``exterior_double_density``)."""
     nodes = np.asarray(nodes, float)
     n = len(nodes)
     rho = np.asarray(density, dtype=np.complex128)
@@ -584,4 +590,4 @@ def pec_combined_sigma(nodes, k, angles_deg, density, order=8):
         dens = np.outer(1.0 - t, rho[i]) + np.outer(t, rho[(i + 1) % n])     # (points, angles)
         factor = 1.0 + gamma * (1j * k * (d @ normal))[None, :]
         amp += length * np.sum(w[:, None] * dens * phase * factor, axis=0)
-    return 0.25 * np.abs(amp) ** 2 / k
+    return amp

@@ -128,3 +128,17 @@ def test_tuning_buckets_and_cache_roundtrip(tmp_path, monkeypatch):
     tuning._store(tuning._key('dev', 2048, 720), {'choice': {'solve_bn': 64, 'gs_block': 512}})
     monkeypatch.setattr(tuning, '_table', None)  # a fresh process reads the file
     assert tuning.lookup('dev', 2000, 600)['choice'] == {'solve_bn': 64, 'gs_block': 512}
+
+
+def test_cpu_dense_backend_is_refused_not_run_on_the_gpu(monkeypatch):
+    from grim_20261007_b200 import synthetic as S
+    from grim_20261007_b200.execution import require_gpu_dense_backend
+    from grim_20261007_b200.twod import solver
+    monkeypatch.setenv('GHOST_DENSE_BACKEND', 'cpu')
+    with pytest.raises(RuntimeError, match='CPU solver'):
+        require_gpu_dense_backend()
+    snap = S.snapshot_from_polygons([S.circle(1.0, 32)])
+    with pytest.raises(RuntimeError, match='CPU solver'):
+        solver.solve_monostatic_rcs_2d_single_polarization(snap, [0.3], [0.0], 'TM', geometry_units='meters')
+    monkeypatch.setenv('GHOST_DENSE_BACKEND', 'auto')
+    assert require_gpu_dense_backend() == 'auto'
