@@ -21,7 +21,9 @@ GRIM_ERR_NOT_CONVERGED = 7
 GRIM_ERR_NONFINITE = 8
 POL_TM, POL_TE = 0, 1
 PREC_FP64, PREC_MIXED, PREC_MIXED_BERR = 0, 1, 2
-TUNE_SOLVE_BN, TUNE_GS_BLOCK = 1, 2
+PREC_STATIC_PIVOT, PREC_PARTIAL_PIVOT = 8, 16
+PIVOT_CERTIFIED, PIVOT_STATIC, PIVOT_PARTIAL = 0, 1, 2
+TUNE_SOLVE_BN, TUNE_GS_BLOCK, TUNE_PIVOT = 1, 2, 3
 
 c_int, c_int64, c_double, c_void_p, c_char_p = ctypes.c_int, ctypes.c_int64, ctypes.c_double, ctypes.c_void_p, ctypes.c_char_p
 c_size_t = ctypes.c_size_t
@@ -68,8 +70,8 @@ SIGNATURES = [
     ('grim_farfield2d', c_int, [c_void_p, c_int, c_void_p, c_int, c_void_p, c_double, c_void_p, c_int64, c_int, c_void_p]),
     ('grim_gal_near_count', c_int, [c_void_p, c_int, c_void_p, c_void_p, c_void_p, P_int]),
     ('grim_gal_near_list', c_int, [c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
-    ('grim_gal_fill', c_int, [c_void_p, c_int, c_int, c_int] + [c_void_p] * 7 + [c_int, c_double, c_int, c_void_p,
-                                                                                  c_int64, c_int]),
+    ('grim_gal_fill', c_int, [c_void_p, c_int, c_int, c_int] + [c_void_p] * 7 + [c_int, c_void_p, c_int, c_double,
+                                                                                  c_int, c_void_p, c_int64, c_int]),
     ('grim_gal_status', c_int, [c_void_p, P_int]),
     ('grim_gal_rhs', c_int, [c_void_p, c_int, c_int, c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_double,
                              c_void_p, c_int64, c_int]),
@@ -89,6 +91,8 @@ SIGNATURES = [
                                             c_void_p, c_int64, c_void_p]),
     ('grim_zgesv_mixed', c_int, [c_void_p, c_int, c_int, c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_int64,
                                  c_int, c_double, c_int, P_int, ctypes.POINTER(GrimSolveInfo)]),
+    ('grim_zgesv_guarded', c_int, [c_void_p, c_int, c_int, c_void_p, c_int64, c_void_p, c_int64, c_int, c_double,
+                                   c_int, c_void_p, P_int, ctypes.POINTER(GrimSolveInfo)]),
     ('grim_zgesv_mixed_factored', c_int, [c_void_p, c_int, c_int, c_void_p, c_int64, c_void_p, c_int64, c_void_p,
                                           c_void_p, c_void_p, c_int64, c_double, c_int, ctypes.POINTER(GrimSolveInfo)]),
     ('grim_zgesv_refine_factored', c_int, [c_void_p, c_int, c_int, c_void_p, c_int64, c_void_p, c_int64, c_void_p,

@@ -150,6 +150,10 @@ struct grim_context {
     // tile-shape overrides set by the autotuner (0 = built-in rule)
     int tune_solve_bn = 0;  // output-tile width of the right-hand-side GEMMs (64 or 128)
     int tune_gs_block = 0;  // row block of the packed-panel solve (256 or 512)
+    // pivoting of later factorizations (GRIM_PIVOT_*): certified diagonal pivots with the
+    // partial-pivoting fallback, static diagonal pivots, or partial pivoting throughout;
+    // set per call by the solves that take a pivot mode, and by grim_set_tuning
+    int pivot_mode = 0;
     // grouped factorization: the instantiated CUDA graph of the last plan, the key it was
     // captured for (element size, orders, device buffers it reads) and its launch count
     cudaGraphExec_t grp_exec = nullptr;

@@ -542,80 +542,151 @@ __device__ bool gal_self_composite(double length, double k, GalBlk &out) {
     return ok;
 }
 
-struct GalAdaptEntry {
+// Close separated pairs (the adaptive route), one CTA of GAL_ADAPT_WARPS warps per pair:
+// every box is compared with its four-way bisection (16-point tensor rule on each), and
+// only the children whose parent missed the tolerance are refined further, to at most
+// GAL_ADAPT_DEPTH levels (twod/operators.py:1172 _integrate_linear_pair_adaptive_sk).
+// The reference walks the tree depth first; here the boxes still to refine sit on a stack
+// in global memory (GAL_ADAPT_GCAP per pair) and each round takes up to GAL_ADAPT_BATCH of
+// them from its top, the warps evaluating all their children side by side.  Each box's
+// decision depends only on itself and its children, so both visit the same boxes; only
+// the order of the final sum differs.  A box unconverged at the last level, or a stack
+// overflow, sets err_flag (the reference raises for the first).
+#define GAL_ADAPT_WARPS 16
+#define GAL_ADAPT_BATCH 64
+#define GAL_ADAPT_GCAP 4096
+
+struct GalBox {
     double oa, ob, sa, sb;
     GalBlk cs, ck;
-    int depth;
+    int depth, pad;
 };
 
-// Close separated pair: each box compared with its four-way bisection, the unconverged
-// children refined further (depth-first, an explicit stack in shared memory).
-// Returns false when a box is still unconverged at GAL_ADAPT_DEPTH levels.
-__device__ bool gal_adaptive_warp(const GalElem &o, const GalElem &s, double k, GalAdaptEntry *stack, GalBlk &S,
-                                  GalBlk &K) {
-    const int lane = threadIdx.x & 31;
-    const double floor_ = 2.220446049250313e-16 * fmax(1.0, o.len * s.len);
-    gal_zero(S);
-    gal_zero(K);
-    int top = 0;
-    GalBlk cs, ck;
-    gal_box_warp(o, s, k, 0.0, 1.0, 0.0, 1.0, GAL_BOX_ORDER, cs, ck);
-    if (lane == 0) {
-        stack[0].oa = 0.0; stack[0].ob = 1.0; stack[0].sa = 0.0; stack[0].sb = 1.0;
-        stack[0].cs = cs; stack[0].ck = ck; stack[0].depth = 0;
+__device__ __forceinline__ void gal_child(const GalBox &b, int c, double &oa, double &ob, double &sa, double &sb) {
+    const double om = 0.5 * (b.oa + b.ob), sm = 0.5 * (b.sa + b.sb);
+    oa = c < 2 ? b.oa : om;
+    ob = c < 2 ? om : b.ob;
+    sa = (c & 1) ? sm : b.sa;
+    sb = (c & 1) ? b.sb : sm;
+}
+
+__global__ void __launch_bounds__(GAL_ADAPT_WARPS * 32)
+k_gal_adapt(int ne, int nadapt, const int *__restrict__ adapt_idx, const double *__restrict__ elem,
+            const int *__restrict__ row_off, const int *__restrict__ col, double k, GalBox *__restrict__ stacks,
+            double2 *__restrict__ NBK, int *__restrict__ err_flag) {
+    extern __shared__ __align__(16) unsigned char gal_smem[];
+    GalBox *cur = reinterpret_cast<GalBox *>(gal_smem);                    // this round's boxes
+    GalBlk *kid = reinterpret_cast<GalBlk *>(cur + GAL_ADAPT_BATCH);       // 2 per child: S, K'
+    __shared__ int s_top, s_fail, s_push[GAL_ADAPT_BATCH + 1];
+    __shared__ unsigned char conv[GAL_ADAPT_BATCH];
+    __shared__ double tot[16];
+    if (blockIdx.x >= nadapt) return;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    GalBox *stack = stacks + (size_t)blockIdx.x * GAL_ADAPT_GCAP;
+    const int idx = adapt_idx[blockIdx.x];
+    int lo = 0, hi = ne;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (row_off[mid] <= idx) lo = mid;
+        else hi = mid;
     }
-    top = 1;
-    bool ok = true;
-    __syncwarp();
-    while (top > 0) {
-        const GalAdaptEntry cur = stack[--top];
-        __syncwarp();
-        const double om = 0.5 * (cur.oa + cur.ob), sm = 0.5 * (cur.sa + cur.sb);
-        GalBlk fs, fk;
-        gal_zero(fs);
-        gal_zero(fk);
-        double ns = 0.0, nk = 0.0;
-        // children in the order (lo, lo), (lo, hi), (hi, lo), (hi, hi); each is written to the
-        // slot it takes if this box is refined (child 0 on top, so it is taken first)
-        for (int c = 0; c < 4; ++c) {
-            const double oa = c < 2 ? cur.oa : om, ob = c < 2 ? om : cur.ob;
-            const double sa = (c & 1) ? sm : cur.sa, sb = (c & 1) ? cur.sb : sm;
+    const GalElem o = gal_load(elem, lo), s = gal_load(elem, col[idx]);
+    const double floor_ = 2.220446049250313e-16 * fmax(1.0, o.len * s.len);
+    if (warp == 0) {
+        GalBlk cs, ck;
+        gal_box_warp(o, s, k, 0.0, 1.0, 0.0, 1.0, GAL_BOX_ORDER, cs, ck);
+        if (lane == 0) {
+            GalBox &b = stack[0];
+            b.oa = 0.0; b.ob = 1.0; b.sa = 0.0; b.sb = 1.0;
+            b.cs = cs; b.ck = ck; b.depth = 0;
+            s_top = 1;
+            s_fail = 0;
+        }
+    }
+    if (tid < 16) tot[tid] = 0.0;
+    __syncthreads();
+    while (s_top > 0) {
+        const int top = s_top;
+        const int nb = min(top, GAL_ADAPT_BATCH), base = top - nb;
+        for (int i = tid; i < nb; i += blockDim.x) cur[i] = stack[base + i];
+        __syncthreads();
+        for (int ci = warp; ci < 4 * nb; ci += GAL_ADAPT_WARPS) {
+            double oa, ob, sa, sb;
+            gal_child(cur[ci >> 2], ci & 3, oa, ob, sa, sb);
             GalBlk ks, kk;
             gal_box_warp(o, s, k, oa, ob, sa, sb, GAL_BOX_ORDER, ks, kk);
+            if (lane == 0) {
+                kid[2 * ci] = ks;
+                kid[2 * ci + 1] = kk;
+            }
+        }
+        __syncthreads();
+        for (int i = tid; i < nb; i += blockDim.x) {
+            double ns = 0.0, nk = 0.0;
+            GalBlk ds, dk;
 #pragma unroll
             for (int v = 0; v < 8; ++v) {
-                fs.v[v] += ks.v[v];
-                fk.v[v] += kk.v[v];
+                ds.v[v] = -cur[i].cs.v[v];
+                dk.v[v] = -cur[i].ck.v[v];
             }
-            ns += gal_fro(ks);
-            nk += gal_fro(kk);
-            if (lane == 0 && top + 4 <= GAL_ADAPT_STACK) {
-                GalAdaptEntry &en = stack[top + 3 - c];
-                en.oa = oa; en.ob = ob; en.sa = sa; en.sb = sb;
-                en.cs = ks; en.ck = kk; en.depth = cur.depth + 1;
-            }
-        }
-        GalBlk ds, dk;
+            for (int c = 0; c < 4; ++c) {
+                const GalBlk &a = kid[2 * (4 * i + c)], &b = kid[2 * (4 * i + c) + 1];
 #pragma unroll
-        for (int v = 0; v < 8; ++v) {
-            ds.v[v] = fs.v[v] - cur.cs.v[v];
-            dk.v[v] = fk.v[v] - cur.ck.v[v];
-        }
-        const double err = fmax(gal_fro(ds) / fmax(ns, floor_), gal_fro(dk) / fmax(nk, floor_));
-        if (err <= GAL_ADAPT_RTOL || cur.depth >= GAL_ADAPT_DEPTH || top + 4 > GAL_ADAPT_STACK) {
-            if (!(err <= GAL_ADAPT_RTOL)) ok = false;
-#pragma unroll
-            for (int v = 0; v < 8; ++v) {
-                S.v[v] += fs.v[v];
-                K.v[v] += fk.v[v];
+                for (int v = 0; v < 8; ++v) {
+                    ds.v[v] += a.v[v];
+                    dk.v[v] += b.v[v];
+                }
+                ns += gal_fro(a);
+                nk += gal_fro(b);
             }
-        } else {
-            top += 4;
+            const double err = fmax(gal_fro(ds) / fmax(ns, floor_), gal_fro(dk) / fmax(nk, floor_));
+            conv[i] = err <= GAL_ADAPT_RTOL ? 1 : 0;
         }
-        __syncwarp();
+        __syncthreads();
+        if (tid == 0) {
+            // converged boxes (or boxes at the last level, or with no stack room) add their
+            // children in a fixed order; the others push theirs
+            int pushed = base;
+            for (int i = 0; i < nb; ++i) {
+                s_push[i] = -1;
+                const bool stop = conv[i] || cur[i].depth >= GAL_ADAPT_DEPTH || pushed + 4 > GAL_ADAPT_GCAP;
+                if (stop) {
+                    if (!conv[i]) s_fail = 1;
+                    for (int c = 0; c < 4; ++c)
+#pragma unroll
+                        for (int v = 0; v < 8; ++v) {
+                            tot[v] += kid[2 * (4 * i + c)].v[v];
+                            tot[8 + v] += kid[2 * (4 * i + c) + 1].v[v];
+                        }
+                } else {
+                    s_push[i] = pushed;
+                    pushed += 4;
+                }
+            }
+            s_top = pushed;
+        }
+        __syncthreads();
+        // child 0 ends on top of each pushed group, so it is taken first
+        for (int e = tid; e < 4 * nb; e += blockDim.x) {
+            const int i = e >> 2, c = e & 3;
+            if (s_push[i] < 0) continue;
+            GalBox &d = stack[s_push[i] + 3 - c];
+            gal_child(cur[i], c, d.oa, d.ob, d.sa, d.sb);
+            d.cs = kid[2 * e];
+            d.ck = kid[2 * e + 1];
+            d.depth = cur[i].depth + 1;
+        }
+        __syncthreads();
     }
-    return ok;
+    if (tid == 0 && s_fail) atomicExch(err_flag, 1);
+    if (tid < 8) {
+        double2 *out = NBK + 8 * (size_t)idx;
+        if (tid < 4) out[tid] = make_double2(tot[2 * tid], tot[2 * tid + 1]);
+        else out[tid] = make_double2(tot[8 + 2 * (tid - 4)], tot[8 + 2 * (tid - 4) + 1]);
+    }
 }
+
+#define GAL_ADAPT_SMEM ((size_t)GAL_ADAPT_BATCH * sizeof(GalBox) + (size_t)8 * GAL_ADAPT_BATCH * sizeof(GalBlk))
 
 // S and K' of every near pair: NBK[idx] = 8 double2 (S entries a*2+b, then K').  One warp per
 // pair; err_flag set when an adaptive pair did not converge or a self series failed.
@@ -623,7 +694,6 @@ __global__ void __launch_bounds__(GAL_NEAR_WARPS * 32)
 k_gal_near(int ne, int nnz, const double *__restrict__ elem, const int2 *__restrict__ nodes,
            const int *__restrict__ row_off, const int *__restrict__ col, const int *__restrict__ route, double k,
            double2 *__restrict__ NBK, int *__restrict__ err_flag) {
-    __shared__ GalAdaptEntry stacks[GAL_NEAR_WARPS][GAL_ADAPT_STACK];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int idx = blockIdx.x * GAL_NEAR_WARPS + warp;
     if (idx >= nnz) return;
@@ -648,7 +718,7 @@ k_gal_near(int ne, int nnz, const double *__restrict__ elem, const int2 *__restr
         const bool src_start = ns.x == no.x || ns.x == no.y;
         gal_touch_warp(o, s, obs_start, src_start, k, S, K);
     } else if (rt == GAL_ROUTE_ADAPT) {
-        ok = gal_adaptive_warp(o, s, k, stacks[warp], S, K);
+        return;  // k_gal_adapt
     } else {
         gal_box_warp(o, s, k, 0.0, 1.0, 0.0, 1.0, GAL_BOX_ORDER, S, K);
     }

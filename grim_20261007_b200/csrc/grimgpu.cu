@@ -23,6 +23,7 @@
 #include "grouped.cuh"
 #include "farblock.cuh"
 #include "galerkin.cuh"
+#include "pivot.cuh"
 
 // ============================================================== errors
 static thread_local std::string g_last_error;
@@ -247,6 +248,10 @@ extern "C" int grim_set_tuning(grim_handle_t h, int key, int value) {
         h->tune_gs_block = value;
         return GRIM_OK;
     }
+    if (key == GRIM_TUNE_PIVOT && value >= GRIM_PIVOT_CERTIFIED && value <= GRIM_PIVOT_PARTIAL) {
+        h->pivot_mode = value;
+        return GRIM_OK;
+    }
     return grim_fail(GRIM_ERR_ARGUMENT, "grim_set_tuning: unknown key or value out of range");
 }
 
@@ -353,7 +358,7 @@ static int gal_err_flag(grim_context *h, int **out) {
 template <typename C>
 static int gal_fill_impl(grim_context *h, int pol, int ne, int n, const double *elem, const int2 *nodes,
                          const int *start_of, const int *end_of, const int *row_off, const int *col, const int *route,
-                         int nnz, double k, int far_min_order, C *Z, int64_t ldz) {
+                         int nnz, const int *adapt_idx, int nadapt, double k, int far_min_order, C *Z, int64_t ldz) {
     void *pnb = nullptr, *pe = nullptr;
     int *err = nullptr;
     GRIM_TRY(gal_err_flag(h, &err));
@@ -364,6 +369,19 @@ static int gal_fill_impl(grim_context *h, int pol, int ne, int n, const double *
     k_gal_near<<<ceil_div(nnz, GAL_NEAR_WARPS), GAL_NEAR_WARPS * 32, 0, h->stream>>>(ne, nnz, elem, nodes, row_off,
                                                                                      col, route, k, nbk, err);
     GRIM_CHECK_LAUNCH(h, "k_gal_near");
+    if (nadapt > 0) {
+        static PerDeviceOnce attr;
+        if (attr.needed()) {
+            GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_gal_adapt, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)GAL_ADAPT_SMEM));
+            attr.mark();
+        }
+        void *pst = nullptr;
+        GRIM_TRY(grim_workspace(h, "gal_adapt_stack", (size_t)nadapt * GAL_ADAPT_GCAP * sizeof(GalBox), &pst));
+        k_gal_adapt<<<nadapt, GAL_ADAPT_WARPS * 32, GAL_ADAPT_SMEM, h->stream>>>(ne, nadapt, adapt_idx, elem, row_off,
+                                                                                   col, k, (GalBox *)pst, nbk, err);
+        GRIM_CHECK_LAUNCH(h, "k_gal_adapt");
+    }
     const int tiles = ceil_div(ne, GAL_TILE);
     dim3 fg(tiles, tiles);
     if (pol == GRIM_POL_TM)
@@ -384,18 +402,18 @@ static int gal_fill_impl(grim_context *h, int pol, int ne, int n, const double *
 
 extern "C" int grim_gal_fill(grim_handle_t h, int pol, int ne, int n, const double *elem, const int *nodes,
                              const int *start_of, const int *end_of, const int *row_off, const int *col,
-                             const int *route, int nnz, double k, int far_min_order, void *Z, int64_t ldz,
-                             int out_complex64) {
+                             const int *route, int nnz, const int *adapt_idx, int nadapt, double k,
+                             int far_min_order, void *Z, int64_t ldz, int out_complex64) {
     if (!h || !gal_elem_ok(ne, elem, nodes) || n <= 0 || n > 65535 || !start_of || !end_of || !row_off || !col ||
-        !route || nnz < ne || !Z || ldz < n || !(k > 0) || far_min_order < 0 || far_min_order > GAL_MAX_Q ||
-        (pol != GRIM_POL_TM && pol != GRIM_POL_TE))
+        !route || nnz < ne || nadapt < 0 || (nadapt > 0 && !adapt_idx) || !Z || ldz < n || !(k > 0) ||
+        far_min_order < 0 || far_min_order > GAL_MAX_Q || (pol != GRIM_POL_TM && pol != GRIM_POL_TE))
         return grim_fail(GRIM_ERR_ARGUMENT, "grim_gal_fill: bad arguments");
     DeviceGuard g(h->device);
     if (out_complex64)
         return gal_fill_impl<float2>(h, pol, ne, n, elem, (const int2 *)nodes, start_of, end_of, row_off, col, route,
-                                     nnz, k, far_min_order, (float2 *)Z, ldz);
+                                     nnz, adapt_idx, nadapt, k, far_min_order, (float2 *)Z, ldz);
     return gal_fill_impl<double2>(h, pol, ne, n, elem, (const int2 *)nodes, start_of, end_of, row_off, col, route,
-                                  nnz, k, far_min_order, (double2 *)Z, ldz);
+                                  nnz, adapt_idx, nadapt, k, far_min_order, (double2 *)Z, ldz);
 }
 
 extern "C" int grim_gal_status(grim_handle_t h, int *flag_host) {
@@ -649,6 +667,7 @@ static int smem_opt_in() {
     if (!done.needed()) return GRIM_OK;
     const int tri = (NB * NBP + NB) * (int)sizeof(C);
     GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_panel_apply<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, tri));
+    GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_panel_u_moves<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, tri));
     GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_trsm_diag<C, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, tri));
     GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_trsm_diag<C, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, tri));
     done.mark();
@@ -735,6 +754,62 @@ static int trailing_update(grim_context *h, int rest, int nbj, const C *L21, con
     return GRIM_OK;
 }
 
+// Rows per cluster CTA of the partial-pivoting panel: a panel of m rows takes the smallest
+// power-of-two cluster (at most 16 CTAs) that keeps each CTA's rows within this target
+// (GRIM_GEPP_ROWS overrides), so that short panels pay for few cluster barriers.
+static int gepp_rows_target(size_t csize) {
+    static const int env = [] {
+        const char *e = getenv("GRIM_GEPP_ROWS");
+        return e ? atoi(e) : 0;
+    }();
+    if (env >= 32) return env;
+    return csize == sizeof(double2) ? 128 : 256;
+}
+
+// Partial-pivoting factorization of the panel (j, nbj) of A on one thread-block cluster.
+template <typename C>
+static int gepp_launch(grim_context *h, int n, C *A, int64_t lda, int j, int nbj, int *ipiv, int *d_info,
+                       int *swapped, int *moves, PanelPack pk) {
+    const int m = n - j;
+    const int target = gepp_rows_target(sizeof(C));
+    int cs = 1;
+    while (cs < 16 && ceil_div(m, cs) > target) cs <<= 1;
+    const int rpc = ceil_div(m, cs);
+    const size_t fixed = gepp_fixed_smem<C>();
+    const size_t cap = (size_t)227 * 1024 - 1024 - fixed;
+    const int rows_smem = std::min(rpc, (int)(cap / (GEPP_LDR * sizeof(C))));
+    const size_t smem = fixed + (size_t)rows_smem * GEPP_LDR * sizeof(C);
+    C *gs = nullptr;
+    if (rpc > rows_smem) {
+        void *p = nullptr;
+        GRIM_TRY(grim_workspace(h, sizeof(C) == 16 ? "gepp_scratch64" : "gepp_scratch32",
+                                (size_t)cs * (rpc - rows_smem) * NB * sizeof(C), &p));
+        gs = (C *)p;
+    }
+    static PerDeviceOnce attr;
+    if (attr.needed()) {
+        GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_panel_gepp<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             227 * 1024 - 1024));
+        GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_panel_gepp<C>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+        attr.mark();
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(cs);
+    cfg.blockDim = dim3(GEPP_THREADS);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = h->stream;
+    cudaLaunchAttribute la[1];
+    la[0].id = cudaLaunchAttributeClusterDimension;
+    la[0].val.clusterDim.x = cs;
+    la[0].val.clusterDim.y = 1;
+    la[0].val.clusterDim.z = 1;
+    cfg.attrs = la;
+    cfg.numAttrs = 1;
+    GRIM_CHECK_CUDA(cudaLaunchKernelEx(&cfg, k_panel_gepp<C>, n, A, lda, j, nbj, rpc, rows_smem, gs, ipiv, d_info,
+                                       swapped, moves, pk));
+    return grim_launch_status(h, kname("k_panel_gepp", sizeof(C)), 8.0 * m * nbj * nbj / 2.0, 0);
+}
+
 // Device flag layout for one factorization: [0] info, [1] pivoted panels, then per panel
 // cert[npan], swapped[npan], counter[npan].
 //
@@ -778,7 +853,51 @@ static int getrf_impl(grim_context *h, int n, C *A, int64_t lda, int *ipiv, int 
     }
     int status = GRIM_OK;
     bool wide_pending = false;
-    for (int p = 0; p < npan && status == GRIM_OK; ++p) {
+    int *moves = nullptr;
+    if (h->pivot_mode == GRIM_PIVOT_PARTIAL) {
+        void *pm = nullptr;
+        GRIM_TRY(grim_workspace(h, "gepp_moves", (1 + 2 * GEPP_MAX_MOVES) * sizeof(int), &pm));
+        moves = (int *)pm;
+    }
+    for (int p = 0; p < npan && status == GRIM_OK && moves; ++p) {
+        // partial pivoting: the panel on a cluster, then the trailing columns' row moves and
+        // U12, then the trailing update (the same look-ahead as below)
+        const int j = p * NB, nbj = std::min(NB, n - j);
+        const int rest = n - j - nbj;
+        PanelPack pk;
+        const bool prepack = sizeof(C) == sizeof(float2) && tc_enabled() && nbj == NB && rest > 0;
+        if (prepack) {
+            TcPacked pa, pb;
+            status = lu_packed(h, rest, nbj, p & 1, &pa, &pb);
+            if (status != GRIM_OK) break;
+            pk.a_hi = pa.hi;
+            pk.a_lo = pa.lo;
+            pk.a_rows = pa.rows_p;
+            pk.b_hi = pb.hi;
+            pk.b_lo = pb.lo;
+            pk.b_rows = pb.rows_p;
+        }
+        status = gepp_launch<C>(h, n, A, lda, j, nbj, ipiv, d_info, swapped + p, moves, pk);
+        if (status != GRIM_OK) break;
+        if (wide_pending) {
+            GRIM_CHECK_CUDA(cudaStreamWaitEvent(h->stream, h->events[2 + npan + p - 1], 0));
+            wide_pending = false;
+        }
+        if (rest > 0) {
+            k_panel_u_moves<C><<<ceil_div(rest, NB), 256, tri, h->stream>>>(n, A, lda, j, nbj, moves, pk);
+            status = grim_launch_status(h, kname("k_panel_u_moves", sizeof(C)), 8.0 * rest * nbj * nbj / 2.0, 0);
+            if (status != GRIM_OK) break;
+            status = trailing_update<C>(h, rest, nbj, A + (int64_t)j * lda + j + nbj, A + (int64_t)(j + nbj) * lda + j,
+                                        A + (int64_t)(j + nbj) * lda + j + nbj, lda, wide, h->events[2 + p], p & 1,
+                                        prepack);
+            if (status != GRIM_OK) break;
+            if (rest > NB && split) {
+                status = grim_cuda_status(cudaEventRecord(h->events[2 + npan + p], wide), "cudaEventRecord");
+                wide_pending = status == GRIM_OK;
+            }
+        }
+    }
+    for (int p = 0; p < npan && status == GRIM_OK && !moves; ++p) {
         const int j = p * NB, nbj = std::min(NB, n - j);
         k_diag_lu<C><<<1, 256, 0, h->stream>>>(n, A, lda, j, nbj, bcol, cert + p, ipiv);
         status = grim_launch_status(h, kname("k_diag_lu", sizeof(C)), 8.0 * nbj * nbj * nbj / 3.0, 0);
@@ -805,7 +924,8 @@ static int getrf_impl(grim_context *h, int n, C *A, int64_t lda, int *ipiv, int 
                 pk.b_rows = pb.rows_p;
             }
             k_panel_apply<C><<<nL + nU, 256, tri, h->stream>>>(n, A, lda, j, nbj, nL, bcol, brow, cert + p,
-                                                               counter + p, swapped + p, ipiv, d_info, d_pivoted, pk);
+                                                               counter + p, swapped + p, ipiv, d_info, d_pivoted, pk,
+                                                               h->pivot_mode == GRIM_PIVOT_STATIC);
             status = grim_launch_status(h, kname("k_panel_apply", sizeof(C)), 8.0 * 2 * rest * nbj * nbj, 0);
             if (status != GRIM_OK) break;
             status = trailing_update<C>(h, rest, nbj, A + (int64_t)j * lda + j + nbj, A + (int64_t)(j + nbj) * lda + j,
@@ -818,7 +938,7 @@ static int getrf_impl(grim_context *h, int n, C *A, int64_t lda, int *ipiv, int 
             }
         } else {
             k_panel_last<C><<<1, 256, 0, h->stream>>>(n, A, lda, j, nbj, bcol, cert + p, swapped + p, ipiv, d_info,
-                                                      d_pivoted);
+                                                      d_pivoted, h->pivot_mode == GRIM_PIVOT_STATIC);
             status = grim_launch_status(h, kname("k_panel_last", sizeof(C)), 0, 0);
         }
     }
@@ -1448,10 +1568,19 @@ static int mixed_refine(grim_context *h, int n, int nrhs, const TA *Ares, int64_
 extern "C" int grim_zgesv_mixed(grim_handle_t h, int n, int nrhs, const void *A, int64_t lda, const void *A32,
                                 int64_t lda32, void *B, int64_t ldb, int precision_mode, double tol, int max_iter,
                                 int *info, grim_solve_info *stats) {
+    const int pivot_req = (precision_mode & GRIM_PREC_PARTIAL_PIVOT) ? GRIM_PIVOT_PARTIAL
+                          : (precision_mode & GRIM_PREC_STATIC_PIVOT) ? GRIM_PIVOT_STATIC : -1;
+    precision_mode &= ~(GRIM_PREC_STATIC_PIVOT | GRIM_PREC_PARTIAL_PIVOT);
     if (!h || n <= 0 || nrhs <= 0 || !B || ldb < n || (!A && !A32) || (A && lda < n) || (A32 && lda32 < n) ||
         (precision_mode != GRIM_PREC_FP64 && precision_mode != GRIM_PREC_MIXED &&
          precision_mode != GRIM_PREC_MIXED_BERR))
         return grim_fail(GRIM_ERR_ARGUMENT, "grim_zgesv_mixed: bad arguments");
+    struct PivotScope {  // a pivot bit applies to this call's factorization only
+        grim_context *h;
+        int keep;
+        PivotScope(grim_context *hh, int mode) : h(hh), keep(hh->pivot_mode) { if (mode >= 0) h->pivot_mode = mode; }
+        ~PivotScope() { h->pivot_mode = keep; }
+    } scope(h, pivot_req);
     if (precision_mode == GRIM_PREC_FP64 && !A)
         return grim_fail(GRIM_ERR_ARGUMENT, "grim_zgesv_mixed: FP64 mode needs the complex128 matrix");
     DeviceGuard g(h->device);
@@ -1526,6 +1655,107 @@ extern "C" int grim_zgesv_mixed(grim_handle_t h, int n, int nrhs, const void *A,
     h->last = st;
     if (stats) *stats = st;
     if (info) *info = linfo;
+    return GRIM_OK;
+}
+
+// FP64 solve of the RCS path with the reference's dense gate: LU in the requested pivot
+// mode, the solution's per-column normwise backward error |r| / (|A| |x| + |b|), at most
+// max_refine FP64 refinement steps with the same factors while the largest exceeds tol
+// (each kept only if it lowers it), and, when the gate still fails or the factors are not
+// finite, a certified factorization (LAPACK getrf's pivots) and solve.
+extern "C" int grim_zgesv_guarded(grim_handle_t h, int n, int nrhs, const void *A, int64_t lda, void *B, int64_t ldb,
+                                  int pivot, double tol, int max_refine, double *berr_dev, int *info,
+                                  grim_solve_info *stats) {
+    if (!h || n <= 0 || nrhs <= 0 || !A || lda < n || !B || ldb < n || !(tol > 0) || max_refine < 0 ||
+        pivot < GRIM_PIVOT_CERTIFIED || pivot > GRIM_PIVOT_PARTIAL)
+        return grim_fail(GRIM_ERR_ARGUMENT, "grim_zgesv_guarded: bad arguments");
+    DeviceGuard g(h->device);
+    grim_solve_info st{};
+    st.precision_mode = GRIM_PREC_FP64;
+    void *pipiv = nullptr, *plu = nullptr, *pB0 = nullptr, *pR = nullptr, *pS = nullptr, *pbe = nullptr;
+    GRIM_TRY(grim_workspace(h, "sv_ipiv", (size_t)n * sizeof(int), &pipiv));
+    GRIM_TRY(grim_workspace(h, "sv_lu64", (size_t)n * n * sizeof(double2), &plu));
+    GRIM_TRY(grim_workspace(h, "gd_B0", (size_t)n * nrhs * sizeof(double2), &pB0));
+    GRIM_TRY(grim_workspace(h, "gd_R", (size_t)n * nrhs * sizeof(double2), &pR));
+    GRIM_TRY(grim_workspace(h, "gd_scalars", 8 * sizeof(double), &pS));
+    if (!berr_dev) {
+        GRIM_TRY(grim_workspace(h, "gd_berr", (size_t)nrhs * sizeof(double), &pbe));
+        berr_dev = (double *)pbe;
+    }
+    int *ipiv = (int *)pipiv;
+    double2 *lu = (double2 *)plu, *B0 = (double2 *)pB0, *R = (double2 *)pR, *X = (double2 *)B;
+    double *sc = (double *)pS;  // [0] |A|_inf, [1] max berr, [2] max relres
+    GRIM_CHECK_CUDA(cudaMemcpy2DAsync(B0, n * sizeof(double2), B, ldb * sizeof(double2), n * sizeof(double2), nrhs,
+                                      cudaMemcpyDeviceToDevice, h->stream));
+    GRIM_TRY(inf_norm(h, n, (const double2 *)A, lda, sc));
+    dim3 eg(ceil_div(n, 256), nrhs);
+    const int keep = h->pivot_mode;
+    double berr = INFINITY;
+    int status = GRIM_OK;
+    for (int attempt = 0; attempt < 2 && status == GRIM_OK; ++attempt) {
+        // attempt 0: the requested pivots; attempt 1: certified (LAPACK getrf's pivots)
+        h->pivot_mode = attempt == 0 ? pivot : GRIM_PIVOT_CERTIFIED;
+        int linfo = 0;
+        GRIM_CHECK_CUDA(cudaMemcpy2DAsync(lu, n * sizeof(double2), A, lda * sizeof(double2), n * sizeof(double2), n,
+                                          cudaMemcpyDeviceToDevice, h->stream));
+        StreamTimer tf(h->stream);
+        status = getrf_impl<double2>(h, n, lu, n, ipiv, &linfo);
+        h->pivot_mode = keep;
+        if (status != GRIM_OK) break;
+        st.ms_factor += tf.stop_ms();
+        // after a fallback, -1 - (panels that pivoted) records it
+        st.pivoted_panels = attempt == 0 ? h->last.pivoted_panels : -1 - h->last.pivoted_panels;
+        if (linfo > 0) {
+            if (attempt == 0) continue;  // an exact zero pivot: the pivoted factorization decides
+            st.info = linfo;
+            h->last = st;
+            if (info) *info = linfo;
+            return grim_fail(GRIM_ERR_SINGULAR, "grim_zgesv_guarded: matrix is exactly singular");
+        }
+        StreamTimer ts(h->stream);
+        if (attempt == 1)
+            GRIM_CHECK_CUDA(cudaMemcpy2DAsync(X, ldb * sizeof(double2), B0, n * sizeof(double2), n * sizeof(double2),
+                                              nrhs, cudaMemcpyDeviceToDevice, h->stream));
+        GRIM_TRY(getrs_impl<double2>(h, n, nrhs, lu, n, ipiv, X, ldb));
+        GRIM_TRY(residual_and_berr(h, n, nrhs, (const double2 *)A, lda, X, ldb, B0, n, R, n, sc, berr_dev, nullptr,
+                                   sc + 1));
+        double hv = INFINITY;
+        GRIM_CHECK_CUDA(cudaMemcpyAsync(&hv, sc + 1, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        GRIM_CHECK_CUDA(cudaStreamSynchronize(h->stream));
+        berr = hv;
+        if (attempt == 0) st.initial_backward_error = berr;
+        for (int it = 0; it < max_refine && std::isfinite(berr) && berr > tol; ++it) {
+            // candidate x + solve(r): kept only if it lowers the largest backward error
+            void *pc = nullptr, *pcb = nullptr;
+            GRIM_TRY(grim_workspace(h, "gd_cand", (size_t)n * nrhs * sizeof(double2), &pc));
+            GRIM_TRY(grim_workspace(h, "gd_cand_berr", (size_t)nrhs * sizeof(double), &pcb));
+            double2 *Xc = (double2 *)pc;
+            GRIM_TRY(getrs_impl<double2>(h, n, nrhs, lu, n, ipiv, R, n));
+            GRIM_CHECK_CUDA(cudaMemcpy2DAsync(Xc, n * sizeof(double2), X, ldb * sizeof(double2), n * sizeof(double2),
+                                              nrhs, cudaMemcpyDeviceToDevice, h->stream));
+            k_add_update<double2><<<eg, 256, 0, h->stream>>>(n, nrhs, Xc, n, R, n);
+            GRIM_CHECK_LAUNCH(h, "k_add_update");
+            GRIM_TRY(residual_and_berr(h, n, nrhs, (const double2 *)A, lda, Xc, n, B0, n, R, n, sc,
+                                       (double *)pcb, nullptr, sc + 2));
+            GRIM_CHECK_CUDA(cudaMemcpyAsync(&hv, sc + 2, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+            GRIM_CHECK_CUDA(cudaStreamSynchronize(h->stream));
+            if (!(hv < berr)) break;
+            berr = hv;
+            GRIM_CHECK_CUDA(cudaMemcpy2DAsync(X, ldb * sizeof(double2), Xc, n * sizeof(double2), n * sizeof(double2),
+                                              nrhs, cudaMemcpyDeviceToDevice, h->stream));
+            GRIM_CHECK_CUDA(cudaMemcpyAsync(berr_dev, pcb, nrhs * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+            st.refinement_steps += 1;
+        }
+        st.ms_solve += ts.stop_ms();
+        if (std::isfinite(berr) && berr <= tol) break;
+    }
+    h->pivot_mode = keep;
+    GRIM_TRY(status);
+    st.backward_error = berr;
+    h->last = st;
+    if (stats) *stats = st;
+    if (info) *info = 0;
+    if (!std::isfinite(berr)) return grim_fail(GRIM_ERR_NONFINITE, "grim_zgesv_guarded: non-finite backward error");
     return GRIM_OK;
 }
 
@@ -1756,6 +1986,7 @@ static int grp_getrf(grim_context *h, int count, const int *n, void *const *A, c
         S.flags = f;
         f += 2 + 3 * S.npan;
         S.pa_hi = S.pa_lo = S.pb_hi = S.pb_lo = nullptr;
+        S.static_pivot = h->pivot_mode == GRIM_PIVOT_STATIC;
         if (sizeof(C) == sizeof(float2) && m > NB) {
             const size_t ra = (size_t)grp_rows_a(m - NB) * GRP_KP, rb = (size_t)grp_rows_b(m - NB) * GRP_KP;
             S.pa_hi = (float *)w;

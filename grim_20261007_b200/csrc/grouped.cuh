@@ -37,6 +37,7 @@ struct GrpSys {
     void *brow;     // n x NB backup of the U12 strip
     int *flags;     // [0] info, [1] pivoted panels, cert[npan], swapped[npan], counter[npan]
     float *pa_hi, *pa_lo, *pb_hi, *pb_lo;  // packed L21 / U12 (complex64 systems)
+    int static_pivot;  // 1: no partial-pivoting fallback (the caller guards the solution)
 };
 
 // Packed operand rows of a complex64 update with `rest` trailing rows / columns.
@@ -78,7 +79,8 @@ __global__ void __launch_bounds__(256, sizeof(C) == 8 ? 3 : 2) k_grp_apply(const
         pk.b_rows = grp_rows_b(rest);
     }
     panel_apply_cta<C>(S.n, (C *)S.A, S.lda, j, NB, nL, blockIdx.x - __ldg(prefix + s), 2 * nL, (C *)S.bcol,
-                       (C *)S.brow, cert + p, counter + p, swapped + p, S.ipiv, S.flags, S.flags + 1, pk);
+                       (C *)S.brow, cert + p, counter + p, swapped + p, S.ipiv, S.flags, S.flags + 1, pk,
+                       S.static_pivot);
 }
 
 // Systems first..first+gridDim.x-1 end at step p.
@@ -88,7 +90,7 @@ __global__ void __launch_bounds__(256) k_grp_last(const GrpSys *__restrict__ sys
     const int j = NB * p;
     int *cert = S.flags + 2, *swapped = cert + S.npan;
     panel_last_cta<C>(S.n, (C *)S.A, S.lda, j, S.n - j, (C *)S.bcol, cert + p, swapped + p, S.ipiv, S.flags,
-                      S.flags + 1);
+                      S.flags + 1, S.static_pivot);
 }
 
 // A22 -= L21 U12 for every updating complex64 system: (Mp / 128) x (Np / BN) tiles each.

@@ -68,6 +68,10 @@ __global__ void k_max_reduce(int n, const double *v, double *out) {
 }
 
 // Per-column max modulus of up to three column blocks (R, X, B) -> out[3*ncol].
+// max that propagates NaN (fmax drops it): a non-finite residual or solution must not
+// read as a small backward error.
+__device__ __forceinline__ double max_nan(double a, double b) { return (a > b || a != a) ? a : b; }
+
 template <typename TX>
 __global__ void k_col_absmax3(int m, const double2 *R, int64_t ldr, const TX *X, int64_t ldx, const double2 *B,
                               int64_t ldb, double *out) {
@@ -77,14 +81,14 @@ __global__ void k_col_absmax3(int m, const double2 *R, int64_t ldr, const TX *X,
         const double2 a = R[(int64_t)c * ldr + r];
         const TX x = X[(int64_t)c * ldx + r];
         const double2 b = B[(int64_t)c * ldb + r];
-        mr = fmax(mr, hypot(a.x, a.y));
-        mx = fmax(mx, hypot((double)x.x, (double)x.y));
-        mb = fmax(mb, hypot(b.x, b.y));
+        mr = max_nan(mr, hypot(a.x, a.y));
+        mx = max_nan(mx, hypot((double)x.x, (double)x.y));
+        mb = max_nan(mb, hypot(b.x, b.y));
     }
     for (int off = 16; off > 0; off >>= 1) {
-        mr = fmax(mr, __shfl_down_sync(0xffffffffu, mr, off));
-        mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, off));
-        mb = fmax(mb, __shfl_down_sync(0xffffffffu, mb, off));
+        mr = max_nan(mr, __shfl_down_sync(0xffffffffu, mr, off));
+        mx = max_nan(mx, __shfl_down_sync(0xffffffffu, mx, off));
+        mb = max_nan(mb, __shfl_down_sync(0xffffffffu, mb, off));
     }
     __shared__ double w[3][32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -96,9 +100,9 @@ __global__ void k_col_absmax3(int m, const double2 *R, int64_t ldr, const TX *X,
         mx = lane < nw ? w[1][lane] : 0.0;
         mb = lane < nw ? w[2][lane] : 0.0;
         for (int off = 16; off > 0; off >>= 1) {
-            mr = fmax(mr, __shfl_down_sync(0xffffffffu, mr, off));
-            mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, off));
-            mb = fmax(mb, __shfl_down_sync(0xffffffffu, mb, off));
+            mr = max_nan(mr, __shfl_down_sync(0xffffffffu, mr, off));
+            mx = max_nan(mx, __shfl_down_sync(0xffffffffu, mx, off));
+            mb = max_nan(mb, __shfl_down_sync(0xffffffffu, mb, off));
         }
         if (lane == 0) { out[3 * c] = mr; out[3 * c + 1] = mx; out[3 * c + 2] = mb; }
     }
@@ -112,7 +116,7 @@ __global__ void k_berr_finish(int ncol, const double *absmax3, const double *ano
         const double r = absmax3[3 * c], x = absmax3[3 * c + 1], b = absmax3[3 * c + 2];
         const double den = (*anorm) * x + b;
         double e = den > 0 ? r / den : (r > 0 ? INFINITY : 0.0);
-        if (!(e == e)) e = INFINITY;
+        if (!(e == e) || r != r || den != den) e = INFINITY;  // any NaN: no backward error
         double rr = r / (b > 0 ? b : 1.0);
         if (!(rr == rr)) rr = INFINITY;
         if (berr) berr[c] = e;

@@ -10,6 +10,9 @@
 //                 (U12 = inv(L11) A12), both with backups; the last CTA to finish
 //                 refactors the panel with partial pivoting if any certificate failed;
 //   k_gemm_rt     A22 -= L21 U12.
+// Static pivoting (no_fallback): the certificate is still computed but never acted on, so
+// the factors are the unpivoted ones; callers that ask for it check the solution's
+// backward error and refactor with partial pivoting when it fails (grim_zgesv_guarded).
 // Partial pivoting picks the diagonal at step c exactly when |a_ic^(c)|_1 <= |a_cc^(c)|_1
 // for every i > c (LAPACK izamax: |re|+|im|, first index on ties), and a_ic^(c) = l_ic u_cc,
 // so a passing certificate proves the unpivoted factors equal getrf's
@@ -437,7 +440,8 @@ __device__ void pivoted_panel(int n, C *A, int64_t lda, int j, int nbj, int *ipi
 template <typename C>
 __device__ __forceinline__ void panel_apply_cta(int n, C *A, int64_t lda, int j, int nbj, int nL, int b, int nblocks,
                                                 C *backup_col, C *backup_row, int *cert, int *counter, int *swapped,
-                                                int *ipiv, int *info, int *pivoted, PanelPack pk = PanelPack()) {
+                                                int *ipiv, int *info, int *pivoted, PanelPack pk = PanelPack(),
+                                                int no_fallback = 0) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C *T = reinterpret_cast<C *>(smem_raw);
     C *rd = T + NB * NBP;
@@ -525,7 +529,7 @@ __device__ __forceinline__ void panel_apply_cta(int n, C *A, int64_t lda, int j,
     __syncthreads();
     if (!s_last) return;
     __threadfence();
-    if (atomicAdd(cert, 0) == 0) return;
+    if (no_fallback || atomicAdd(cert, 0) == 0) return;
     for (int c = 0; c < nbj; ++c)
         for (int r = t; r < n - j; r += 256) A[(int64_t)(j + c) * lda + j + r] = backup_col[(int64_t)c * n + r];
     for (int c = j + nbj; c < n; ++c)
@@ -551,16 +555,17 @@ __device__ __forceinline__ void panel_apply_cta(int n, C *A, int64_t lda, int j,
 template <typename C>
 __global__ void __launch_bounds__(256)
 k_panel_apply(int n, C *A, int64_t lda, int j, int nbj, int nL, C *backup_col, C *backup_row, int *cert,
-              int *counter, int *swapped, int *ipiv, int *info, int *pivoted, PanelPack pk) {
+              int *counter, int *swapped, int *ipiv, int *info, int *pivoted, PanelPack pk, int no_fallback) {
     panel_apply_cta<C>(n, A, lda, j, nbj, nL, blockIdx.x, gridDim.x, backup_col, backup_row, cert, counter, swapped,
-                       ipiv, info, pivoted, pk);
+                       ipiv, info, pivoted, pk, no_fallback);
 }
 
 // Single-CTA fallback driver when there is no trailing strip (last panel).
 template <typename C>
 __device__ __forceinline__ void panel_last_cta(int n, C *A, int64_t lda, int j, int nbj, C *backup_col, int *cert,
-                                               int *swapped, int *ipiv, int *info, int *pivoted) {
-    if (*cert == 0) return;
+                                               int *swapped, int *ipiv, int *info, int *pivoted,
+                                               int no_fallback = 0) {
+    if (no_fallback || *cert == 0) return;
     for (int c = 0; c < nbj; ++c)
         for (int r = threadIdx.x; r < n - j; r += 256) A[(int64_t)(j + c) * lda + j + r] = backup_col[(int64_t)c * n + r];
     __syncthreads();
@@ -571,8 +576,8 @@ __device__ __forceinline__ void panel_last_cta(int n, C *A, int64_t lda, int j, 
 template <typename C>
 __global__ void __launch_bounds__(256)
 k_panel_last(int n, C *A, int64_t lda, int j, int nbj, C *backup_col, int *cert, int *swapped, int *ipiv, int *info,
-             int *pivoted) {
-    panel_last_cta<C>(n, A, lda, j, nbj, backup_col, cert, swapped, ipiv, info, pivoted);
+             int *pivoted, int no_fallback) {
+    panel_last_cta<C>(n, A, lda, j, nbj, backup_col, cert, swapped, ipiv, info, pivoted, no_fallback);
 }
 
 // Apply interchanges of later panels to the columns left of them.

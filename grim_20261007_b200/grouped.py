@@ -21,13 +21,15 @@ from . import _lib
 from .device import context, ptr, run_pool
 
 
-def getrf_grouped(mats, use_graph=True, ctx=None):
+def getrf_grouped(mats, use_graph=True, ctx=None, static_pivot=False):
     """Factor the square column-major device matrices ``mats`` in place (all complex64 or all
     complex128, contiguous, leading dimension = order) with one grouped LU.
 
     Returns (ipivs, infos, pivoted): 1-based int32 pivots per system, LAPACK-style info per
     system (0, or k+1 for an exactly zero U(k,k)) and the number of panels that fell back to
     partial pivoting.  The factors equal ``grim_cgetrf`` / ``grim_zgetrf`` of each matrix.
+    With ``static_pivot`` every system keeps its diagonal pivots (no partial-pivoting
+    fallback); the caller guards the solutions.
     """
     ctx = ctx or context()
     mats = list(mats)
@@ -47,8 +49,13 @@ def getrf_grouped(mats, use_graph=True, ctx=None):
     pps = (ctypes.c_void_p * count)(*[p.data_ptr() for p in ipivs])
     info = (ctypes.c_int * count)()
     piv = (ctypes.c_int * count)()
-    _lib.check(ctx.lib.grim_getrf_grouped(ctx.h, count, ns, aps, lds, pps, int(dt == torch.complex64), int(use_graph),
-                                          info, piv), 'grim_getrf_grouped')
+    _lib.check(ctx.lib.grim_set_tuning(ctx.h, _lib.TUNE_PIVOT, _lib.PIVOT_STATIC if static_pivot else
+                                       _lib.PIVOT_CERTIFIED), 'grim_set_tuning')
+    try:
+        _lib.check(ctx.lib.grim_getrf_grouped(ctx.h, count, ns, aps, lds, pps, int(dt == torch.complex64),
+                                              int(use_graph), info, piv), 'grim_getrf_grouped')
+    finally:
+        ctx.lib.grim_set_tuning(ctx.h, _lib.TUNE_PIVOT, _lib.PIVOT_CERTIFIED)
     return ipivs, list(info), list(piv)
 
 

@@ -30,7 +30,7 @@ import torch
 
 from .. import _lib
 from ..device import Context, ptr, require_cuda
-from ..twod import geometry as geo, operators as ops
+from ..twod import galerkin, operators as ops
 
 
 class Request:
@@ -68,7 +68,8 @@ class Request:
         r = max(1, len(self.angles))
         if self.kind == '2d':
             esz = 8 if self.precision == 'mixed' else 16
-            fixed = 0 if cached else 2 * self.n * self.n * esz + 2 * self.n * 64 * esz
+            # matrix, factors, panel backups and the fill's element-pair blocks (4 per pair)
+            fixed = 0 if cached else 6 * self.n * self.n * esz + 2 * self.n * 64 * esz
             return fixed + 8 * self.n * r * 16 + (1 << 20)
         ne = len(self.geometry) - 1
         mm = (self.n_modes or 40) + 2
@@ -241,27 +242,35 @@ class ServingEngine:
             return {'id': req.id, 'amp_vv': F[:nth], 'amp_hh': F[nth:], 'telemetry': tele}
 
     def _run_2d(self, slot, req):
+        """A 2-D request in the reference's linear-Galerkin combined formulation: fill and a
+        partial-pivoting factorization (kept in the cache), then the angles' solves guarded by
+        the backward error (refinement for mixed precision, the FP64 gate for FP64)."""
         ctx, s = slot.ctx, slot.stream
-        v = req.geometry
-        body = ops.DeviceBody(geo.panel_geometry([v]), geo.te_curvature_correction([v]) if req.pol == 'TE' else None)
         ang = torch.as_tensor(req.angles, device='cuda')
-        n = body.n
         key = req.cache_key()
         entry = self.cache.get(key)
         req.cache_hit = entry is not None
         mixed = req.precision == 'mixed'
         if entry is None:
+            body = galerkin.GalerkinBody([req.geometry], ctx=ctx)
+            n = body.n
             z = ops.fill(body, req.k, req.pol, complex64=mixed, ctx=ctx)
             lu = z.clone()
             ipiv = torch.empty(n, dtype=torch.int32, device='cuda')
             info = ctypes.c_int(0)
             fn = ctx.lib.grim_cgetrf if mixed else ctx.lib.grim_zgetrf
-            _lib.check(fn(ctx.h, n, ptr(lu), n, ptr(ipiv), ctypes.byref(info)), 'getrf')
+            _lib.check(ctx.lib.grim_set_tuning(ctx.h, _lib.TUNE_PIVOT, _lib.PIVOT_PARTIAL), 'grim_set_tuning')
+            try:
+                _lib.check(fn(ctx.h, n, ptr(lu), n, ptr(ipiv), ctypes.byref(info)), 'getrf')
+            finally:
+                ctx.lib.grim_set_tuning(ctx.h, _lib.TUNE_PIVOT, _lib.PIVOT_CERTIFIED)
             if info.value:
                 raise _lib.GrimError(_lib.GRIM_ERR_SINGULAR, f'request {req.id}: singular system (info={info.value})')
-            entry = {'z': z, 'lu': lu, 'ipiv': ipiv}
+            entry = {'z': z, 'lu': lu, 'ipiv': ipiv, 'body': body}
             self.cache.put(key, entry, 2 * z.numel() * z.element_size())
         else:
+            body = entry['body']
+            n = body.n
             for t in (entry['z'], entry['lu'], entry['ipiv']):
                 t.record_stream(s)
         b = ops.rhs(body, req.k, req.pol, ang, ctx=ctx)
@@ -276,7 +285,7 @@ class ServingEngine:
                 # stalled refinement: solve this request in FP64 (reference mixed -> double ladder)
                 z64 = ops.fill(body, req.k, req.pol, ctx=ctx)
                 x = b0
-                ops.solve_inplace(z64, x, 'double', ctx=ctx)
+                ops.solve_guarded(z64, x, pivot='partial', ctx=ctx)
                 tele['fp64_fallback'] = True
             else:
                 _lib.check(status, 'grim_zgesv_mixed_factored')
@@ -288,6 +297,12 @@ class ServingEngine:
                                            n), 'grim_zgetrs')
             berr = ops.backward_error(entry['z'], x, b, ctx=ctx)
             tele['backward_error'] = float(berr.max().item())
+            if not tele['backward_error'] <= ops.DOUBLE_GATE_TOL:
+                # the cached factor misses the FP64 gate: the gated solve of this request
+                x = b.clone()
+                st_g, berr = ops.solve_guarded(entry['z'], x, pivot='partial', ctx=ctx)
+                tele['backward_error'] = float(berr.max().item())
+                tele['gate_fallback'] = st_g['gate_fallback']
         amp = ops.farfield(body, req.k, ang, x, ctx=ctx)
         return amp.cpu().numpy(), tele
 

@@ -103,6 +103,16 @@ class GalerkinBody:
         self.route = torch.empty(max(1, self.nnz), dtype=torch.int32, device=dev)
         _lib.check(ctx.lib.grim_gal_near_list(ctx.h, self.ne, ptr(self.elem), ptr(self.nodes), ptr(self.row_off),
                                               ptr(self.col), ptr(self.route)), 'grim_gal_near_list')
+        # the adaptive (route 3) pairs get a CTA each: their indices, in list order
+        routes = self.route[:self.nnz].cpu().numpy()
+        adapt = np.flatnonzero(routes == 3).astype(np.int32)
+        self.nadapt = int(adapt.size)
+        self.adapt_idx = torch.from_numpy(adapt if adapt.size else np.zeros(1, np.int32)).to(dev)
+        self.route_counts = np.bincount(routes, minlength=4)
+
+    # partial pivoting leaves the diagonal on these systems (and unpivoted elimination grows
+    # by up to 1e10 on cosine-spaced airfoils): their factorizations pivot throughout
+    pivot = 'partial'
 
     def far_min_order(self, k, pol):
         return w_far_order(k, self.lengths) if pol == 'TE' else 0
@@ -115,7 +125,8 @@ class GalerkinBody:
         z = out if out is not None else torch.empty((n, n), dtype=dt, device=self.elem.device)
         _lib.check(ctx.lib.grim_gal_fill(ctx.h, _lib.POL_TM if pol == 'TM' else _lib.POL_TE, self.ne, n,
                                          ptr(self.elem), ptr(self.nodes), ptr(self.start_of), ptr(self.end_of),
-                                         ptr(self.row_off), ptr(self.col), ptr(self.route), self.nnz, float(k),
+                                         ptr(self.row_off), ptr(self.col), ptr(self.route), self.nnz,
+                                         ptr(self.adapt_idx), self.nadapt, float(k),
                                          int(self.far_min_order(k, pol)), ptr(z), n, int(complex64)), 'grim_gal_fill')
         return z
 

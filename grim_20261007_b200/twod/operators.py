@@ -24,6 +24,7 @@ POL_CODE = {'TM': _lib.POL_TM, 'TE': _lib.POL_TE}
 # hook keeps the reference RefinedLU's relative-residual test at 2e-12.
 MIXED_RCS_TOL = 1e-10
 MIXED_DROPIN_TOL = 2e-12
+DOUBLE_GATE_TOL = 1e-12   # the reference's FP64 normwise backward-error gate (twod/solver.py:694-760)
 
 
 def canonical_pol(pol):
@@ -86,7 +87,31 @@ def farfield(body, k, angles_dev, x, out=None, ctx=None):
     return amp
 
 
-def solve_inplace(z, b, precision='double', tol=None, max_iter=10, z32=None, ctx=None, stop='relres', tuned=True):
+PIVOTS = {'certified': _lib.PIVOT_CERTIFIED, 'static': _lib.PIVOT_STATIC, 'partial': _lib.PIVOT_PARTIAL}
+
+
+def solve_guarded(z, b, pivot='partial', tol=DOUBLE_GATE_TOL, max_refine=2, ctx=None):
+    """FP64 solve of Z X = B with the reference's dense gate (``grim_zgesv_guarded``): LU in
+    the ``pivot`` mode ('partial', 'certified' or 'static'), the per-column normwise
+    backward error, at most ``max_refine`` refinement steps while it exceeds ``tol`` and a
+    certified factorization when the gate still fails.  X overwrites ``b``; returns
+    (telemetry dict, per-column backward errors on the device)."""
+    ctx = ctx or context()
+    n, nrhs = int(b.shape[1]), int(b.shape[0])
+    berr = torch.empty(nrhs, dtype=torch.float64, device=b.device)
+    info = ctypes.c_int(0)
+    st = _lib.GrimSolveInfo()
+    _lib.check(ctx.lib.grim_zgesv_guarded(ctx.h, n, nrhs, ptr(z), n, ptr(b), n, PIVOTS[pivot], float(tol),
+                                          int(max_refine), ptr(berr), ctypes.byref(info), ctypes.byref(st)),
+               'grim_zgesv_guarded')
+    tele = st.as_dict()
+    tele['pivot'] = pivot
+    tele['gate_fallback'] = tele['pivoted_panels'] < 0
+    return tele, berr
+
+
+def solve_inplace(z, b, precision='double', tol=None, max_iter=10, z32=None, ctx=None, stop='relres', tuned=True,
+                  pivot='certified'):
     """Solve Z X = B on the device; X overwrites ``b`` (complex128, shape (nrhs, n)).
 
     precision 'double': FP64 LU + triangular solves.  'mixed': complex64 LU of ``z32``
@@ -95,6 +120,10 @@ def solve_inplace(z, b, precision='double', tol=None, max_iter=10, z32=None, ctx
     every column's relative residual (``stop='relres'``, the reference RefinedLU test) or
     normwise backward error (``stop='berr'``) is <= ``tol``.  With ``tuned`` the handle's
     tile shapes come from the autotuner's cache (``tuning.apply``).
+    ``pivot``: the factorization's pivot mode -- 'certified' (diagonal pivots, certified per
+    panel, partial pivoting where they fail), 'partial' (partial pivoting throughout) or
+    'static' (diagonal pivots; the refinement guards the solution, a stall raises
+    ``GrimNotConverged``).
     Returns the solve telemetry dict.
     """
     ctx = ctx or context()
@@ -109,6 +138,10 @@ def solve_inplace(z, b, precision='double', tol=None, max_iter=10, z32=None, ctx
             tuning.apply(ctx, n, nrhs)
     else:
         mode = _lib.PREC_FP64
+    if pivot == 'partial':
+        mode |= _lib.PREC_PARTIAL_PIVOT
+    elif pivot == 'static':
+        mode |= _lib.PREC_STATIC_PIVOT
     tol = MIXED_DROPIN_TOL if tol is None else float(tol)
     status = ctx.lib.grim_zgesv_mixed(ctx.h, n, nrhs, ptr(z), n, ptr(z32), n, ptr(b), n, mode, tol, int(max_iter),
                                       ctypes.byref(info), ctypes.byref(st))
@@ -140,6 +173,10 @@ def monostatic_solve(body, k, angles_deg, pol, precision='double', tol=None, che
     dev = body.geom.device
     if angles_dev is None:
         angles_dev = torch.as_tensor(np.asarray(angles_deg, dtype=np.float64), device=dev)
+    # linear-Galerkin systems: partial pivoting leaves the diagonal, so they factor with
+    # partial pivoting throughout and the FP64 path applies the reference's gate
+    pivot = getattr(body, 'pivot', 'certified')
+    static = pivot != 'certified'
     tele = {}
     if precision == 'mixed':
         z32 = fill(body, k, pol, complex64=True, ctx=ctx)
@@ -147,7 +184,7 @@ def monostatic_solve(body, k, angles_deg, pol, precision='double', tol=None, che
         b0 = b.clone()
         try:
             st = solve_inplace(None, b, 'mixed', tol=MIXED_RCS_TOL if tol is None else tol, z32=z32, ctx=ctx,
-                               stop='berr')
+                               stop='berr', pivot=pivot)
             x = b
             z = z32
         except _lib.GrimNotConverged:
@@ -155,9 +192,18 @@ def monostatic_solve(body, k, angles_deg, pol, precision='double', tol=None, che
             # reference's mixed -> double ladder does (linalg/dense.py:74-98)
             z = fill(body, k, pol, ctx=ctx)
             x = b0
-            st = solve_inplace(z, x, 'double', ctx=ctx)
+            if static:
+                st, _berr = solve_guarded(z, x, pivot=pivot, ctx=ctx)
+            else:
+                st = solve_inplace(z, x, 'double', ctx=ctx)
             st['fp64_fallback'] = True
         tele.update(st)
+    elif static:
+        z = fill(body, k, pol, ctx=ctx)
+        x = rhs(body, k, pol, angles_dev, ctx=ctx)
+        st, berr = solve_guarded(z, x, pivot=pivot, ctx=ctx)
+        tele.update(st)
+        tele['backward_error_dev'] = berr
     else:
         z = fill(body, k, pol, ctx=ctx)
         b = rhs(body, k, pol, angles_dev, ctx=ctx)
@@ -208,10 +254,17 @@ def monostatic_solves_grouped(bodies, ks, angles_deg, pol, precision='mixed', to
             return {'z': z, 'lu': z.clone(), 'b': b}
         return run
 
+    if any(getattr(b, 'pivot', 'certified') == 'partial' for b in bodies):
+        # the grouped factorization keeps diagonal pivots; systems that need partial
+        # pivoting are factored one by one on the pool instead
+        jobs = [(lambda i=i: monostatic_solve(bodies[i], ks[i], angles_deg, pols[i], precision=precision, tol=tol,
+                                              angles_dev=angles_dev)) for i in range(len(bodies))]
+        return run_pool(jobs, workers=workers, costs=costs)
+    static = all(getattr(b, 'pivot', 'certified') == 'static' for b in bodies)
     parts = run_pool([prep(i) for i in range(len(bodies))], workers=workers, costs=costs)
-    ipivs, infos, piv = getrf_grouped([p['lu'] for p in parts], use_graph=use_graph)
+    ipivs, infos, piv = getrf_grouped([p['lu'] for p in parts], use_graph=use_graph, static_pivot=static)
     for i, inf in enumerate(infos):
-        if inf:
+        if inf and not static:
             raise _lib.GrimError(_lib.GRIM_ERR_SINGULAR, f'system {i} (n={bodies[i].n}) is exactly singular '
                                                          f'(info={inf})')
 
@@ -229,13 +282,22 @@ def monostatic_solves_grouped(bodies, ks, angles_deg, pol, precision='mixed', to
                 except _lib.GrimNotConverged:
                     z64 = fill(bodies[i], ks[i], pols[i], ctx=c)
                     x = b0
-                    st = solve_inplace(z64, x, 'double', ctx=c)
+                    if static:
+                        st, _berr = solve_guarded(z64, x, pivot='static', ctx=c)
+                    else:
+                        st = solve_inplace(z64, x, 'double', ctx=c)
                     st['fp64_fallback'] = True
             else:
                 x = p['b'].clone()
                 n = bodies[i].n
                 _lib.check(c.lib.grim_zgetrs(c.h, n, nang, ptr(p['lu']), n, ptr(ipivs[i]), ptr(x), n), 'grim_zgetrs')
-                st = {'precision_mode': _lib.PREC_FP64, 'backward_error_dev': backward_error(p['z'], x, p['b'], ctx=c)}
+                berr = backward_error(p['z'], x, p['b'], ctx=c)
+                st = {'precision_mode': _lib.PREC_FP64, 'backward_error_dev': berr}
+                if static and (infos[i] or not float(berr.max()) <= DOUBLE_GATE_TOL):
+                    # the static-pivot factor missed the gate: the guarded solve of this system
+                    x = p['b'].clone()
+                    st, berr = solve_guarded(p['z'], x, pivot='static', ctx=c)
+                    st['backward_error_dev'] = berr
             tele.update(st)
             amp = farfield(bodies[i], ks[i], angles_dev, x, ctx=c)
             # release this system's matrices as soon as its work is queued: they were

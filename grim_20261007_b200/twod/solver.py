@@ -12,11 +12,13 @@ Public API (same names, arguments and result-dict keys as the reference):
   then the FP64 normwise backward-error gate (1e-12) with at most two refinement
   steps, raising ``RuntimeError`` when the gate fails.
 
-Physics: pulse basis, point-matched TM EFIE and TE MFIE on the straight panels of
-closed PEC contours (see ``operators.py``).  The reference discretises with linear
-Galerkin elements and a combined S + gamma D potential, so results agree with it to
-discretisation error (hundredths of a dB at 20 panels per wavelength), and with the
-analytic Mie series for the circular cylinder.
+Physics: the reference's own discretisation of closed PEC contours (``galerkin.py``):
+linear Galerkin elements, combined rows S + gamma (D + M/2) (TM) and K' - M/2 - gamma W
+(TE), so the amplitudes equal the reference solver's to rounding and conditioning
+(1e-10 on its C1 cylinder) and neither channel has interior resonances.  The
+pulse-basis, point-matched TM EFIE / TE MFIE of ``operators.DeviceBody`` remains
+selectable with ``GRIM_2D_FORMULATION=pulse`` (it agrees with the reference only to
+discretisation error).
 """
 from __future__ import annotations
 
@@ -32,6 +34,7 @@ from .. import _lib
 from ..device import context, require_cuda, run_pool
 from ..execution import require_gpu_dense_backend, requested_precision
 from . import certify
+from . import galerkin
 from . import geometry as geo
 from . import operators as ops
 
@@ -46,6 +49,17 @@ MAX_PANELS_DEFAULT = 20_000
 DEFAULT_PANELS_PER_WAVELENGTH = 20
 
 _DENSE_BACKEND_LOCAL = threading.local()
+
+FORMULATION_ENV = 'GRIM_2D_FORMULATION'
+_FORMULATIONS = {'galerkin', 'pulse'}
+
+
+def requested_formulation():
+    """'galerkin' (default: the reference's linear-Galerkin combined rows) or 'pulse'."""
+    value = os.environ.get(FORMULATION_ENV, 'galerkin').strip().lower()
+    if value not in _FORMULATIONS:
+        raise ValueError(f'{FORMULATION_ENV} must be galerkin or pulse.')
+    return value
 
 
 # ------------------------------------------------------------------ telemetry
@@ -256,6 +270,21 @@ class _MeshCache:
         self.lock = threading.Lock()
         self.locks = {}
         self.meshes = {}
+        self.bodies = {}
+
+    def galerkin_body(self, f):
+        """The frequency's linear-Galerkin device body, built once and shared by both
+        polarisations (its near-pair structure depends on the mesh only)."""
+        polys, _geom = self.get(f)
+        with self.lock:
+            lk = self.locks.setdefault(('galerkin', f), threading.Lock())
+        with lk:
+            if f not in self.bodies:
+                dev = torch.device('cuda', torch.cuda.current_device())
+                body = galerkin.GalerkinBody(polys, device=dev)
+                torch.cuda.current_stream().synchronize()  # other workers' streams read it next
+                self.bodies[f] = body
+            return self.bodies[f]
 
     def get(self, f):
         with self.lock:
@@ -274,6 +303,8 @@ def _frequency_body(meshes, f, pol, abort_event):
     if abort_event is not None and abort_event.is_set():
         raise InterruptedError('Solve canceled by user.')
     k = 2.0 * math.pi * f * 1e9 / C0
+    if requested_formulation() == 'galerkin':
+        return k, meshes.galerkin_body(f)
     polys, geom = meshes.get(f)
     te_diag = geo.te_curvature_correction(polys) if pol == 'TE' else None
     dev = torch.device('cuda', torch.cuda.current_device())
@@ -305,8 +336,9 @@ def _frequency_record(f, elevs, pol, precision, k, body, res, t0):
     } for e, sl, sd, ar, ai, ph, rr in zip(elevs, np.asarray(sig, dtype=float).tolist(),
                                            np.asarray(sdb, dtype=float).tolist(), amp.real.tolist(),
                                            amp.imag.tolist(), phase.tolist(), np.asarray(resid, float).tolist())]
+    kind = 'galerkin' if isinstance(body, galerkin.GalerkinBody) else 'pulse'
     event = dict(requested='gpu', used='gpu_grim', factorizations=1, rhs_columns=len(elevs), n=body.n,
-                 label=f'{pol} pulse {f:g} GHz', gpu_device=context().device_name, precision=precision,
+                 label=f'{pol} {kind} {f:g} GHz', gpu_device=context().device_name, precision=precision,
                  pivoted_panels=tele.get('pivoted_panels', 0), refinement_steps=tele.get('refinement_steps', 0),
                  grouped_factorization=bool(tele.get('grouped', False)))
     return dict(samples=samples, residuals=[float(r) for r in resid], event=event, n=body.n,
@@ -362,9 +394,15 @@ def _channel_result(pol, outs, precision, stage_seconds):
         residuals.extend(o['residuals'])
         counts.append(o['n'])
         _record_dense_backend_event(**o['event'])
+    if requested_formulation() == 'galerkin':
+        formulation = ('2D combined-field BIE, linear Galerkin (TM: S + gamma (D + M/2))' if pol == 'TM'
+                       else "2D combined-field BIE, linear Galerkin (TE: K' - M/2 - gamma W)")
+    else:
+        formulation = 'pulse_point_matched_efie' if pol == 'TM' else 'pulse_point_matched_mfie'
     metadata = {
         'solver_method': 'direct',
-        'formulation': 'pulse_point_matched_efie' if pol == 'TM' else 'pulse_point_matched_mfie',
+        'formulation': formulation,
+        'formulation_kind': 'multi_region' if requested_formulation() == 'galerkin' else 'pulse',
         'precision': precision,
         'device': context().device_name,
         'panel_count_max': max(counts),

@@ -54,6 +54,20 @@ extern "C" {
 #define GRIM_PREC_FP64 0         /* plain FP64 drop-in                               */
 #define GRIM_PREC_MIXED 1        /* FP32 factor, FP64 residual / update refinement   */
 #define GRIM_PREC_MIXED_BERR 2   /* as MIXED, stopping on the normwise backward error */
+#define GRIM_PREC_STATIC_PIVOT 8   /* or-ed into a mode: this factorization keeps the
+                                      diagonal pivots (no partial-pivoting fallback)  */
+#define GRIM_PREC_PARTIAL_PIVOT 16 /* or-ed into a mode: partial pivoting throughout    */
+/* Pivot modes of a factorization (grim_set_tuning GRIM_TUNE_PIVOT, grim_zgesv_guarded):
+ * CERTIFIED  diagonal pivots, each 64-column panel certified to be what partial pivoting
+ *            picks and refactored with partial pivoting when it is not (fast for
+ *            diagonally dominant systems: the pulse-basis matrices, the BoR modes);
+ * STATIC     diagonal pivots, no fallback (callers guard the solution);
+ * PARTIAL    partial pivoting of every panel on a thread-block cluster (the
+ *            linear-Galerkin combined-field systems, whose pivots leave the diagonal).
+ * CERTIFIED and PARTIAL give LAPACK getrf's pivots (|re| + |im|, first row on ties). */
+#define GRIM_PIVOT_CERTIFIED 0
+#define GRIM_PIVOT_STATIC 1
+#define GRIM_PIVOT_PARTIAL 2
 
 typedef struct grim_context *grim_handle_t;
 
@@ -116,6 +130,8 @@ int grim_farfield2d(grim_handle_t h, int n, const double *geom, int nang, const 
  *                        *nnz_host = row_off[ne] (synchronises the stream);
  *   grim_gal_near_list   col (nnz ints, ascending per row) and route (nnz ints: 0 self,
  *                        1 touching, 2 16-point tensor rule, 3 adaptive bisection).
+ * adapt_idx: the nadapt indices (into col / route) of the route-3 pairs, each integrated
+ *   by its own CTA.
  * grim_gal_fill writes the n x n node matrix: TM (pol 0) S + gamma (D + M/2), TE (pol 1)
  * K' - M/2 - gamma W, gamma = 1/(j k).  far_min_order: floor on the far Gauss order (the
  * TE rows' W rule: 8, or 16 outside its calibration; 0 for TM).  Near pairs in FP64;
@@ -131,8 +147,8 @@ int grim_gal_near_list(grim_handle_t h, int ne, const double *elem, const int *n
                        int *col, int *route);
 int grim_gal_fill(grim_handle_t h, int pol, int ne, int n, const double *elem, const int *nodes,
                   const int *start_of, const int *end_of, const int *row_off, const int *col,
-                  const int *route, int nnz, double k, int far_min_order, void *Z, int64_t ldz,
-                  int out_complex64);
+                  const int *route, int nnz, const int *adapt_idx, int nadapt, double k, int far_min_order,
+                  void *Z, int64_t ldz, int out_complex64);
 int grim_gal_status(grim_handle_t h, int *flag_host);
 int grim_gal_rhs(grim_handle_t h, int pol, int n, const double *elem, const int *start_of,
                  const int *end_of, int nang, const double *angles_deg, double k, void *B, int64_t ldb,
@@ -200,10 +216,23 @@ int grim_backward_error_noalloc(grim_handle_t h, int n, int nrhs, const void *A,
  * stopping when the normwise backward error |r| / (|A| |x| + |b|) of every column is
  * <= tol (the form of test LAPACK's zcgesv uses), for callers whose accuracy target
  * is a backward error (the RCS solves).  A is preserved.  info: LAPACK-style.  stats
- * may be NULL. */
+ * may be NULL.  GRIM_PREC_STATIC_PIVOT or GRIM_PREC_PARTIAL_PIVOT or-ed into the mode
+ * picks the factorization's pivot mode (GRIM_PIVOT_STATIC / GRIM_PIVOT_PARTIAL; the
+ * default is CERTIFIED); with static pivots the refinement guards the solution (a stall
+ * returns GRIM_ERR_NOT_CONVERGED). */
 int grim_zgesv_mixed(grim_handle_t h, int n, int nrhs, const void *A, int64_t lda, const void *A32,
                      int64_t lda32, void *B, int64_t ldb, int precision_mode, double tol, int max_iter,
                      int *info, grim_solve_info *stats);
+
+/* FP64 solve with the reference's backward-error gate (twod/solver.py:694-760): LU in the
+ * given pivot mode (GRIM_PIVOT_*), getrs, the per-column normwise backward error
+ * |r| / (|A|_inf |x| + |b|) into berr_dev (nrhs doubles, may be NULL), at most max_refine
+ * FP64 refinement steps with the same factors while the largest exceeds tol (each kept
+ * only if it lowers it), and, when the gate still fails, a CERTIFIED factorization and
+ * solve (stats->pivoted_panels = -1 - its pivoted panel count then records the
+ * fallback).  X overwrites B; A is preserved; synchronises the stream. */
+int grim_zgesv_guarded(grim_handle_t h, int n, int nrhs, const void *A, int64_t lda, void *B, int64_t ldb,
+                       int pivot, double tol, int max_refine, double *berr_dev, int *info, grim_solve_info *stats);
 
 /* Mixed solve reusing a complex64 factorization (LU32 and ipiv from grim_cgetrf, leading
  * dimension n) with FP64 refinement against A or the promotion of A32; for resident
@@ -341,10 +370,12 @@ int grim_mem_info(grim_handle_t h, size_t *free_bytes, size_t *total_bytes);
 /* Tile-shape overrides chosen by the autotuner (grim_20261007_b200.tuning), per handle;
  * value 0 restores the built-in rule.  GRIM_TUNE_SOLVE_BN: output-tile width (64 or 128)
  * of the tensor-core GEMMs of the packed-panel solve; GRIM_TUNE_GS_BLOCK: row block (256
- * or 512) of the packed-panel solve.  No counterpart in the reference (its BLAS picks its
- * own blocking). */
+ * or 512) of the packed-panel solve; GRIM_TUNE_PIVOT: the pivot mode (GRIM_PIVOT_*) of
+ * later factorizations on the handle (grim_getrf_grouped takes CERTIFIED or STATIC).  No
+ * counterpart in the reference (its BLAS picks its own blocking and always pivots). */
 #define GRIM_TUNE_SOLVE_BN 1
 #define GRIM_TUNE_GS_BLOCK 2
+#define GRIM_TUNE_PIVOT 3
 int grim_set_tuning(grim_handle_t h, int key, int value);
 
 #ifdef __cplusplus

@@ -1,4 +1,6 @@
-"""GPU 2-D fill / excitation / far field / end-to-end solve against the FP64 oracle."""
+"""GPU 2-D pulse-basis fill / excitation / far field / end-to-end solve against the FP64 pulse
+oracle, and the public entry points' concurrency, sweep and certification behaviour (the
+default linear-Galerkin formulation; its parity tests are in test_gpu_galerkin.py)."""
 import os
 
 import numpy as np
@@ -82,8 +84,10 @@ def test_rhs_and_farfield_match_oracle(ctx, pol):
     assert np.max(np.abs(amp - ampr)) <= 1e-12 * np.max(np.abs(ampr))
 
 
-def test_end_to_end_c1_cylinder_fp64(ctx):
-    """Config 1: PEC cylinder a=1 m, ka=10, 200 panels, 360 angles, TM, FP64."""
+def test_end_to_end_c1_cylinder_fp64(ctx, monkeypatch):
+    """Config 1 in the pulse formulation: PEC cylinder a=1 m, ka=10, 200 panels, 360 angles,
+    TM, FP64, against the pulse oracle (and the reference / Mie to discretisation error)."""
+    monkeypatch.setenv('GRIM_2D_FORMULATION', 'pulse')
     from grim_20261007_b200.twod.solver import solve_monostatic_rcs_2d_single_polarization
     g = np.load(os.path.join(GOLDEN, 'ref_cylinder_c1.npz'))
     snap = S.snapshot_from_polygons([S.circle(1.0, 200)])
@@ -99,7 +103,8 @@ def test_end_to_end_c1_cylinder_fp64(ctx):
     assert res['metadata']['device']
 
 
-def test_end_to_end_co_polarized_and_mixed(ctx):
+def test_end_to_end_co_polarized_and_mixed(ctx, monkeypatch):
+    monkeypatch.setenv('GRIM_2D_FORMULATION', 'pulse')
     from grim_20261007_b200.execution import linear_precision
     from grim_20261007_b200.twod.solver import solve_monostatic_rcs_2d
     v, k, f, _ = S.airfoil_case(1, 512)

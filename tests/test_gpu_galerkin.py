@@ -191,3 +191,98 @@ def test_two_contours_are_one_system(ctx):
     for pol, A in (('TM', S_ + gamma * (K_.T + 0.5 * M)), ('TE', K_ - 0.5 * M - gamma * W_)):
         z = _gpu_matrix(body, k, pol)
         assert np.max(np.abs(z - A)) <= 1e-12 * np.max(np.abs(A))
+
+
+AIRFOIL = np.load(os.path.join(GOLDEN, 'ref_airfoil.npz'))
+
+
+def _amplitudes(res, export=None):
+    rows = [r for r in res['samples'] if export is None or r.get('polarization') == export]
+    return (np.array([complex(r['rcs_amp_real'], r['rcs_amp_imag']) for r in rows]),
+            np.array([r['rcs_linear'] for r in rows]))
+
+
+def test_c1_cylinder_through_the_public_entry(ctx):
+    """Config 1 through solve_monostatic_rcs_2d_single_polarization: the reference's own
+    amplitudes (1e-10), the Mie series (1e-3 dB) and the FP64 gate."""
+    from oracle import mie
+    from grim_20261007_b200.twod.solver import solve_monostatic_rcs_2d_single_polarization
+    g = np.load(os.path.join(GOLDEN, 'ref_cylinder_c1.npz'))
+    snap = S.snapshot_from_polygons([S.circle(1.0, 200)])
+    for pol in ('TM', 'TE'):
+        res = solve_monostatic_rcs_2d_single_polarization(snap, [float(g['frequency_ghz'])], list(g['angles']), pol,
+                                                          geometry_units='meters', strict_quality_gate=True)
+        amp, sig = _amplitudes(res)
+        assert np.max(np.abs(amp - g[f'amp_{pol}']) / np.abs(g[f'amp_{pol}'])) <= 1e-10
+        assert abs(10 * np.log10(sig[0] / mie.cylinder_sigma(1.0, float(g['k']), pol))) <= 1e-3
+        assert max(r['linear_residual'] for r in res['samples']) <= 1e-12
+        assert 'Galerkin' in res['metadata']['formulation']
+
+
+@pytest.mark.parametrize('n', [int(x) for x in AIRFOIL['sizes']])
+def test_airfoil_matches_the_reference_solver(ctx, n):
+    """The headline geometry (seeded NACA 00tt, blunt trailing edge, cosine spacing, lambda/10,
+    720 angles) through solve_monostatic_rcs_2d: both channels' complex amplitudes equal the
+    reference solver's (tests/golden/ref_airfoil.npz) to 1e-9 of the peak amplitude in FP64;
+    the mixed-precision path is within 0.05 dB of the reference wherever sigma is within
+    40 dB of its peak."""
+    from grim_20261007_b200.execution import linear_precision
+    from grim_20261007_b200.twod.solver import solve_monostatic_rcs_2d
+    v, k, f, _t = S.airfoil_case(0, n)
+    assert abs(k - float(AIRFOIL[f'n{n}_k'])) <= 1e-12 * k
+    snap = S.snapshot_from_polygons([v])
+    ang = list(AIRFOIL['angles'])
+    r64 = solve_monostatic_rcs_2d(snap, [f / 1e9], ang, geometry_units='meters')
+    with linear_precision('mixed'):
+        r32 = solve_monostatic_rcs_2d(snap, [f / 1e9], ang, geometry_units='meters')
+    for pol, export in (('TE', 'VV'), ('TM', 'HH')):
+        ref_amp, ref_sig = AIRFOIL[f'n{n}_amp_{pol}'], AIRFOIL[f'n{n}_sigma_{pol}']
+        a64, s64 = _amplitudes(r64, export)
+        _a32, s32 = _amplitudes(r32, export)
+        assert np.max(np.abs(a64 - ref_amp)) <= 1e-9 * np.max(np.abs(ref_amp)), pol
+        db = 10 * np.log10(ref_sig)
+        mask = db > db.max() - 40
+        assert np.max(np.abs(10 * np.log10(s64[mask] / ref_sig[mask]))) <= 1e-6, pol
+        assert np.max(np.abs(10 * np.log10(s32[mask] / ref_sig[mask]))) <= 0.05, pol
+
+
+@pytest.mark.parametrize('pol', ['TM', 'TE'])
+def test_gated_solve_pivots_like_lapack_and_falls_back(ctx, pol):
+    """The airfoil's combined-field matrix factors with partial pivoting into LAPACK's pivots
+    and meets the reference's 1e-12 backward-error gate without refinement; a static-pivot
+    solve of a system whose leading entry is zero falls back to the certified factorization."""
+    import ctypes
+    import scipy.linalg as sla
+    from grim_20261007_b200 import _lib
+    from grim_20261007_b200.device import context, ptr, to_device_colmajor, to_host_matrix
+    from grim_20261007_b200.twod import operators as ops
+    from grim_20261007_b200.twod.galerkin import GalerkinBody
+    v, k, _f, _t = S.airfoil_case(2, 512)
+    body = GalerkinBody([v])
+    z = body.fill_matrix(k, pol)
+    ang = torch.as_tensor(np.arange(0.0, 360.0, 3.0), device='cuda')
+    x = body.rhs_matrix(k, pol, ang)
+    b = x.clone()
+    st, berr = ops.solve_guarded(z, x, pivot='partial')
+    assert float(berr.max()) <= 1e-12 and st['refinement_steps'] == 0 and not st['gate_fallback']
+    assert float(ops.backward_error(z, x, b).max()) <= 1e-12
+    c = context()
+    lu = z.clone()
+    ipiv = torch.zeros(body.n, dtype=torch.int32, device='cuda')
+    info = ctypes.c_int(-1)
+    _lib.check(c.lib.grim_set_tuning(c.h, _lib.TUNE_PIVOT, _lib.PIVOT_PARTIAL))
+    try:
+        _lib.check(c.lib.grim_zgetrf(c.h, body.n, ptr(lu), body.n, ptr(ipiv), ctypes.byref(info)))
+    finally:
+        c.lib.grim_set_tuning(c.h, _lib.TUNE_PIVOT, _lib.PIVOT_CERTIFIED)
+    lu_ref, piv_ref = sla.lu_factor(to_host_matrix(z))
+    np.testing.assert_array_equal(ipiv.cpu().numpy(), piv_ref + 1)
+    assert np.max(np.abs(to_host_matrix(lu) - lu_ref)) <= 1e-11 * np.max(np.abs(lu_ref))
+    rng = np.random.default_rng(1)
+    a = rng.standard_normal((96, 96)) + 1j * rng.standard_normal((96, 96))
+    a[0, 0] = 0.0
+    rhs = rng.standard_normal((96, 3)) + 0j
+    x2 = to_device_colmajor(rhs)
+    st2, berr2 = ops.solve_guarded(to_device_colmajor(a), x2, pivot='static')
+    assert st2['gate_fallback'] and float(berr2.max()) <= 1e-12
+    np.testing.assert_allclose(x2.cpu().numpy().T, np.linalg.solve(a, rhs), rtol=1e-10, atol=1e-12)

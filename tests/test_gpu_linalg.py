@@ -39,7 +39,7 @@ def _rand(n, m, seed, dominant=False):
     return a
 
 
-def _getrf(ctx, a, complex64=False):
+def _getrf(ctx, a, complex64=False, pivot=0):
     from grim_20261007_b200 import _lib
     from grim_20261007_b200.device import ptr
     n = a.shape[0]
@@ -47,8 +47,55 @@ def _getrf(ctx, a, complex64=False):
     ipiv = torch.zeros(n, dtype=torch.int32, device='cuda')
     info = ctypes.c_int(-1)
     fn = ctx.lib.grim_cgetrf if complex64 else ctx.lib.grim_zgetrf
-    _lib.check(fn(ctx.h, n, ptr(t), n, ptr(ipiv), ctypes.byref(info)))
+    _lib.check(ctx.lib.grim_set_tuning(ctx.h, _lib.TUNE_PIVOT, pivot))
+    try:
+        _lib.check(fn(ctx.h, n, ptr(t), n, ptr(ipiv), ctypes.byref(info)))
+    finally:
+        ctx.lib.grim_set_tuning(ctx.h, _lib.TUNE_PIVOT, _lib.PIVOT_CERTIFIED)
     return t, ipiv, info.value
+
+
+@pytest.mark.parametrize('n', [1, 7, 64, 97, 200, 333, 1100, 3500])
+def test_partial_pivoting_getrf_matches_lapack(ctx, n):
+    """Partial pivoting on a thread-block cluster: LAPACK's pivots and factors, for cluster
+    sizes 1 to 16 and (n = 3500, complex128) panel rows past a CTA's shared memory."""
+    from grim_20261007_b200 import _lib
+    a = _rand(n, n, 300 + n)
+    t, ipiv, info = _getrf(ctx, a, pivot=_lib.PIVOT_PARTIAL)
+    lu_ref, piv_ref = sla.lu_factor(a)
+    assert info == 0
+    np.testing.assert_array_equal(ipiv.cpu().numpy(), piv_ref + 1)
+    lu = _host(t)
+    assert np.max(np.abs(lu - lu_ref)) <= 1e-10 * max(1.0, np.max(np.abs(lu_ref)))
+
+
+@pytest.mark.parametrize('n', [160, 700])
+def test_partial_pivoting_cgetrf_matches_lapack(ctx, n):
+    from grim_20261007_b200 import _lib
+    a = _rand(n, n, 31 + n).astype(np.complex64)
+    t, ipiv, info = _getrf(ctx, a, complex64=True, pivot=_lib.PIVOT_PARTIAL)
+    lu_ref, piv_ref = sla.lu_factor(a)
+    assert info == 0
+    np.testing.assert_array_equal(ipiv.cpu().numpy(), piv_ref + 1)
+    assert np.max(np.abs(_host(t) - lu_ref)) <= 2e-3 * np.max(np.abs(lu_ref))
+
+
+def test_partial_pivoting_reports_exact_singularity_and_solves(ctx):
+    from grim_20261007_b200 import _lib
+    from grim_20261007_b200.device import ptr
+    a = _rand(150, 150, 9)
+    a[:, 70] = 0.0
+    _t, ipiv, info = _getrf(ctx, a, pivot=_lib.PIVOT_PARTIAL)
+    lu_ref, piv_ref, info_ref = sla.lapack.zgetrf(a)
+    assert info == info_ref == 71
+    np.testing.assert_array_equal(ipiv.cpu().numpy(), piv_ref + 1)
+    a = _rand(300, 300, 10)
+    b = _rand(300, 40, 11)
+    t, ipiv, info = _getrf(ctx, a, pivot=_lib.PIVOT_PARTIAL)
+    bt = _dev(b)
+    _lib.check(ctx.lib.grim_zgetrs(ctx.h, 300, 40, ptr(t), 300, ptr(ipiv), ptr(bt), 300))
+    x_ref = np.linalg.solve(a, b)
+    assert np.max(np.abs(_host(bt) - x_ref)) <= 1e-10 * np.max(np.abs(x_ref))
 
 
 @pytest.mark.parametrize('n', [1, 7, 64, 97, 200, 333])
@@ -174,3 +221,20 @@ def test_mixed_falls_back_to_fp64_when_refinement_stalls(ctx):
     berr = np.max(np.abs(r), axis=0) / (np.max(np.sum(np.abs(a), axis=1)) * np.max(np.abs(x), axis=0)
                                         + np.max(np.abs(b), axis=0))
     assert np.max(berr) < 1e-14
+
+
+def test_backward_error_reports_nonfinite_solutions_as_infinite():
+    """A NaN anywhere in a column's solution or residual makes that column's backward error
+    infinite (a max that dropped NaN would report it as tiny)."""
+    if not torch.cuda.is_available():
+        pytest.skip('no CUDA device')
+    from grim_20261007_b200.device import to_device_colmajor
+    from grim_20261007_b200.twod import operators as ops
+    rng = np.random.default_rng(4)
+    a = rng.standard_normal((80, 80)) + 1j * rng.standard_normal((80, 80))
+    x = rng.standard_normal((80, 3)) + 0j
+    b = a @ x
+    x[5, 1] = np.nan
+    berr = ops.backward_error(to_device_colmajor(a), to_device_colmajor(x), to_device_colmajor(b)).cpu().numpy()
+    assert berr[0] < 1e-14 and berr[2] < 1e-14
+    assert np.isinf(berr[1])
