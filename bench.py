@@ -1,11 +1,15 @@
 """Benchmark: RCS solves/s at N=2048 (mixed vs FP64 GPU), the 2-D airfoil workload.
 
 Workload (one "step"): the seeded NACA 00tt airfoil (chord 1 m, tt ~ U[8,15] %, cosine
-spacing, sharp trailing edge) with N = 2048 panels at lambda/10 (~30 GHz), 720
-monostatic angles (0..359.5 deg by 0.5), both polarisations (TM = HH EFIE, TE = VV
-MFIE): two solves per step, each = fill + LU + 720-RHS solve + refinement + far field.
-The headline arm is the mixed-precision path (complex64 fill/LU, FP64 refinement);
-the plain FP64 GPU path is timed on the same inputs for the ratio and the dB error.
+spacing, blunt trailing edge closed by two base elements) with N = 2048 elements at
+lambda/10 on average (~30 GHz), 720 monostatic angles (0..359.5 deg by 0.5), both
+polarisations (TM = HH, TE = VV) in the reference's own linear-Galerkin combined-field
+formulation: two solves per step, each = fill + partial-pivoting LU + 720-RHS solve +
+refinement + far field.  The headline arm is the mixed-precision path (complex64 fill and
+LU, FP64 refinement); the FP64 GPU path is timed on the same inputs for the ratio; both
+are compared with the reference solver's own amplitudes for this airfoil (the committed
+fixture tests/golden/ref_airfoil.npz).  ``--formulation pulse`` times the pulse-basis
+point-matched EFIE / MFIE instead.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl grim|reference]
 
@@ -297,7 +301,7 @@ def run_sweep(args, rank=0, world=1):
     from grim_20261007_b200 import synthetic as S
     from grim_20261007_b200.device import run_pool
     from grim_20261007_b200.sharding import max_over_ranks, my_units
-    from grim_20261007_b200.twod import geometry as geo, operators as ops
+    from grim_20261007_b200.twod import galerkin, geometry as geo, operators as ops
     from grim_20261007_b200.twod.solver import sweep_workers
     cases, thick = S.airfoil_sweep_case(args.seed + 3, args.sweep)
     ang = np.arange(181) * 1.0
@@ -305,7 +309,10 @@ def run_sweep(args, rank=0, world=1):
     all_n = [len(v) for v, _k, _f in cases]
     costs_all = [float(n) ** 3 + 181.0 * n * n for n in all_n]
     mine = my_units(costs_all, rank, world)
-    bodies = {i: ops.DeviceBody(geo.panel_geometry([cases[i][0]]), None) for i in mine}
+    if args.formulation == 'galerkin':
+        bodies = {i: galerkin.GalerkinBody([cases[i][0]]) for i in mine}
+    else:
+        bodies = {i: ops.DeviceBody(geo.panel_geometry([cases[i][0]]), None) for i in mine}
     ns = [bodies[i].n for i in mine]
 
     def jobs(prec, idx):
@@ -351,11 +358,80 @@ def run_sweep(args, rank=0, world=1):
         err = max(err, float(np.max(np.abs(10 * np.log10(s32[mask] / s64[mask])))))
     return {'systems': len(cases), 'band': '20:1', 'frequency_ghz': [cases[0][2] / 1e9, cases[-1][2] / 1e9],
             'n_min': min(all_n), 'n_max': max(all_n), 'angles': 181, 'polarization': 'TM', 'thickness': thick,
-            'ranks': world, 'workers_per_rank': workers, 'path': 'grouped LU (one CUDA graph) + pooled solves',
+            'ranks': world, 'workers_per_rank': workers,
+            'path': ('per-system partial-pivoting solves on the device worker pool (linear Galerkin)'
+                     if args.formulation == 'galerkin' else 'grouped LU (one CUDA graph) + pooled solves'),
             'seconds': sec, 'solves_per_s': len(cases) / sec,
             'per_system_pool': {'seconds': sec_pool, 'solves_per_s': len(cases) / sec_pool},
             'fp64_fallbacks': sum(1 for o in outs if o['telemetry'].get('fp64_fallback')),
             'max_db_error_vs_fp64_sampled': err, 'sampled_frequencies': len(sample)}
+
+
+def reference_far_block_fn():
+    """The reference's own far pass (``twod/assembly/native/far.c`` compiled from its sources
+    into oracle/_ref) as ``fn(mb, nb, q, obs_pts, src_pts, qw, phi, obs_norm, src_norm, far,
+    table)``, or None where it was not built."""
+    import ctypes
+    path = os.path.join(ROOT, 'oracle', '_ref', 'libghost_far_ref.so')
+    if not os.path.exists(path):
+        return None
+    lib = ctypes.CDLL(path)
+    fun = lib.ghost_far_block
+    p = ctypes.c_void_p
+    fun.argtypes = [ctypes.c_int64, ctypes.c_int64, ctypes.c_int, ctypes.c_int] + [p] * 7 + [ctypes.c_int] * 4 + \
+        [ctypes.c_double] * 2 + [ctypes.c_int, p, ctypes.c_int, p, p, p, p]
+    fun.restype = ctypes.c_int
+
+    def run(mb, nb, q, obs_pts, src_pts, qw, phi, obs_norm, src_norm, far, table):
+        accs = [np.zeros((4, mb, nb), complex) for _ in range(3)]
+        pw = np.ascontiguousarray(table.normalized_power)
+        st = fun(mb, nb, q, 2, obs_pts.ctypes.data, src_pts.ctypes.data, qw.ctypes.data, phi.ctypes.data,
+                 obs_norm.ctypes.data, src_norm.ctypes.data, far.ctypes.data, 1, 1, 1, 1, table.k, 0.0,
+                 len(table.bounds) - 1, table.bounds.ctypes.data, pw.shape[1] - 1, pw.ctypes.data,
+                 *(a_.ctypes.data for a_ in accs))
+        if st not in (0, 2):
+            raise RuntimeError(f'ghost_far_block returned {st}')
+        return accs
+    return run
+
+
+def cpu_solve_seconds(v, k, ang, rows, near=True):
+    """One solve of the workload by the CPU port (oracle/galerkin_cpu.py) on this process:
+    the far pass of element rows ``rows`` (None: all), the near pass, LU / solve / loads /
+    far field at full size."""
+    from oracle import galerkin_cpu as GC
+    fn, table = reference_far_pass(v, k)
+    return GC.time_solve(v, k, ang, rows, far_block_fn=fn, table=table, near=near)
+
+
+_FAR_PASS = {}
+
+
+def reference_far_pass(v, k):
+    """(compiled far-block function, its kernel table) for the contour v, or (None, None);
+    built once per process and wavenumber, as the reference keeps its table per solve."""
+    key = (float(k), np.asarray(v).tobytes())
+    if key not in _FAR_PASS:
+        fn = reference_far_block_fn()
+        table = None
+        if fn is not None:
+            from grim_20261007_b200.twod.farblock import KernelTable
+            table = KernelTable(k, 1.2 * float(np.max(np.ptp(v, axis=0))) * math.sqrt(2.0))
+            table.k = k
+        _FAR_PASS.clear()
+        _FAR_PASS[key] = (fn, table)
+    return _FAR_PASS[key]
+
+
+def cpu_baseline_sample(args, v, k, ang):
+    """The CPU port timed on one host core: one full TM solve of the workload (every
+    element row's far pass, every near pair, LAPACK LU and solve, loads, far field)."""
+    sec, parts = cpu_solve_seconds(v, k, ang, None)
+    return {'value': 1.0 / sec, 'unit': UNIT, 'cores': 1, 'kind': 'port',
+            'sample': f'one full TM solve of the workload (N={args.n}, {len(ang)} angles): far pairs by the '
+                      'reference\'s own compiled far.c (upper triangle, mirrored), near pairs by the oracle\'s '
+                      'Galerkin rules batched in NumPy as the reference batches them, LAPACK LU and solve',
+            'parts': parts}
 
 
 def workload(seed, n, nang):
@@ -365,54 +441,149 @@ def workload(seed, n, nang):
     return v, k, f, t, ang
 
 
-def cpu_oracle_solve(v, k, ang, pol):
-    from oracle import pulse2d as P
-    return P.solve(k, [v], ang, pol)['amplitude']
+def _ref_far_worker(payload):
+    """One spawned process of the reference arm: the far pass of its element rows."""
+    v, k, rows = payload
+    sys.path.insert(0, ROOT)
+    from oracle import galerkin_cpu as GC
+    fn, table = reference_far_pass(v, k)
+    t0 = time.perf_counter()
+    if fn is not None:
+        GC.far_all_compiled(v, k, fn, table, rows)
+    else:
+        GC.far_rows_numpy(v, k, rows)
+    return time.perf_counter() - t0
 
 
 def run_reference_arm(args, rank, world):
-    """Reference CPU implementation of the path (the oracle port), all host threads."""
+    """The reference's CPU path for this workload on all host cores (rank 0 only): the CPU
+    port of oracle/galerkin_cpu.py -- the far pass by the reference's own compiled far.c,
+    its element rows split over spawned processes, the batched near pass in the main process
+    meanwhile, then LAPACK LU and the 720-angle solve on all cores; one step = TM + TE."""
     if rank != 0:
         return
     import concurrent.futures as cf
     import multiprocessing as mp
-    from oracle import pulse2d as P
-    import scipy.linalg as sla
+    from oracle import galerkin_cpu as GC
     cores = os.cpu_count() or 1
     v, k, f, t, ang = workload(args.seed, args.n, args.angles)
-    c, tt, h, nn = P.panel_arrays([v])
-    ted = P.te_curvature_correction([v])
-    rows = np.array_split(np.arange(len(c)), cores)
+    chunks = [np.arange(i, args.n, cores) for i in range(cores)]
     ctx = mp.get_context('spawn')
 
-    def one_step(pool):
-        for pol in ('TM', 'TE'):
-            futs = [pool.submit(P.fill, k, c, tt, h, nn, pol, r, ted if pol == 'TE' else None) for r in rows]
-            z = np.concatenate([fu.result() for fu in futs], axis=0)
-            b = P.rhs(k, c, nn, ang, pol)
-            x = sla.lu_solve(sla.lu_factor(z, check_finite=False), b, check_finite=False)
-            P.monostatic_amplitude(P.farfield_weights(k, c, tt, h, ang), x)
+    def one_solve(pool):
+        t0 = time.perf_counter()
+        futs = [pool.submit(_ref_far_worker, (v, k, c)) for c in chunks]
+        GC.near_all(v, k)
+        for fu in futs:
+            fu.result()
+        _total, parts = cpu_solve_seconds(v, k, ang, [], near=False)   # LU, solve, loads, far field
+        return time.perf_counter() - t0 - parts['far_fill_s']
 
     with cf.ProcessPoolExecutor(max_workers=cores, mp_context=ctx) as pool:
         for _ in range(args.warmup):
-            one_step(pool)
-        t0 = time.perf_counter()
-        for _ in range(args.steps):
-            one_step(pool)
-        dt = time.perf_counter() - t0
+            one_solve(pool)
+        secs = [one_solve(pool) + one_solve(pool) for _ in range(args.steps)]
+    dt = float(np.sum(secs))
     value = 2 * args.steps / dt
     line = {
         'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': world, 'steps': args.steps, 'warmup': args.warmup,
         'ms_per_step': dt / args.steps * 1e3, 'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
         'dtype': 'f64', 'data': 'synthetic (seeded NACA 00tt airfoil)', 'impl': 'reference',
-        'config': {'workload': f'2-D airfoil N={args.n}, {args.angles} angles, TM+TE, FP64 CPU oracle port',
-                   'n_panels': args.n, 'angles': args.angles, 'seed': args.seed},
+        'config': {'workload': f'2-D airfoil N={args.n}, {args.angles} angles, TM+TE, linear-Galerkin combined '
+                               'formulation, FP64 CPU', 'n_elements': args.n, 'angles': args.angles, 'seed': args.seed},
         'cpu_baseline': {'value': value, 'unit': UNIT, 'cores': cores, 'kind': 'port',
-                         'sample': f'full TM+TE solve of the workload per step ({args.steps} steps), fill split over '
-                                   f'{cores} spawned processes, LAPACK LU/solve'},
+                         'sample': f'full TM + TE solves per step: the far pass by the reference\'s compiled far.c '
+                                   f'over {cores} spawned processes, the oracle\'s batched near pass, LAPACK LU and '
+                                   'solve on all cores'},
         'e2e': {'value': value, 'unit': UNIT, 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def reference_parity(args, rank, k, amp64, amp32):
+    """Max dB and relative amplitude differences of both arms from the reference solver's
+    own amplitudes (tests/golden/ref_airfoil.npz: its solve_monostatic_rcs_2d_single_
+    polarization on synthetic.airfoil_case(0, n), 720 angles) where sigma is within 40 dB
+    of its peak; None when this rank's workload is not the fixture's."""
+    path = os.path.join(ROOT, 'tests', 'golden', 'ref_airfoil.npz')
+    if not os.path.exists(path) or args.seed + rank != 0 or args.angles != 720:
+        return None
+    g = np.load(path)
+    if args.n not in [int(x) for x in g['sizes']] or abs(float(g[f'n{args.n}_k']) - k) > 1e-12 * k:
+        return None
+    out = {'reference': 'GHOST solve_monostatic_rcs_2d_single_polarization (its own stored amplitudes)'}
+    for pol in ('TM', 'TE'):
+        ref = g[f'n{args.n}_amp_{pol}']
+        db_ref = 10 * np.log10(np.abs(ref) ** 2)
+        mask = db_ref > db_ref.max() - 40
+        for arm, amp in (('fp64', amp64[pol]), ('mixed', amp32[pol])):
+            db = 10 * np.log10(np.abs(amp) ** 2)
+            out[f'{pol}_{arm}_max_db'] = float(np.max(np.abs(db - db_ref)[mask]))
+            out[f'{pol}_{arm}_max_rel_amp'] = float(np.max(np.abs(amp - ref)) / np.max(np.abs(ref)))
+    return out
+
+
+def kernel_roofline(prof):
+    """Roofline of the kernel with the largest share of one profiled mixed step."""
+    hbm, bf16, src = _peaks()
+    dom_name, dom = max(prof.items(), key=lambda kv: kv[1]['ms'])
+    step_ms = sum(v['ms'] for v in prof.values())
+    base = {'kernel': dom_name, 'launches': dom['launches'], 'avg_launch_ms': dom['ms'] / dom['launches'],
+            'share_of_step': dom['ms'] / step_ms, 'peak_source': src, 'traffic': None}
+    if 'gepp' in dom_name:
+        # the partial-pivoting panel is a chain of 64 dependent column steps per launch:
+        # latency-bound; its algorithmic rate is reported against the FP64 / FP32 pipe
+        achieved = dom['flops'] / (dom['ms'] * 1e-3) / 1e12
+        base.update(bound='latency (column-step chain)', achieved=achieved, peak=bf16, unit='TFLOP/s',
+                    frac=achieved / bf16, note='algorithmic 8 m 64^2 / 2 flops per panel; one cluster barrier '
+                    'per column; peak = measured dense bf16 tensor rate (the only measured compute peak)')
+        return base
+    if dom['flops'] > 0:
+        achieved = dom['flops'] / (dom['ms'] * 1e-3) / 1e12
+        base.update(bound='tensor', achieved=achieved, peak=bf16, unit='TFLOP/s', frac=achieved / bf16)
+        if dom_name in NCU_TRAFFIC:
+            nbytes, nflops = NCU_TRAFFIC[dom_name]
+            base['traffic'] = nbytes * (dom['flops'] / dom['launches']) / nflops
+        return base
+    achieved = dom['bytes'] / (dom['ms'] * 1e-3) / 1e9
+    base.update(bound='hbm', achieved=achieved, peak=hbm, unit='GB/s', frac=achieved / hbm)
+    return base
+
+
+def top_kernels(prof, count=6):
+    step_ms = sum(v['ms'] for v in prof.values())
+    top = sorted(prof.items(), key=lambda kv: -kv[1]['ms'])[:count]
+    return {name: {'ms': round(v['ms'], 4), 'launches': v['launches'], 'share': round(v['ms'] / step_ms, 4)}
+            for name, v in top}
+
+
+def summarize(d, keys):
+    if not d:
+        return d
+    return {k_: d[k_] for k_ in keys if k_ in d}
+
+
+def summarize_bor(bor):
+    if not bor:
+        return bor
+    out = {k_: bor[k_] for k_ in ('segments', 'modes', 'aspects', 'formulation', 'max_db_error_mixed_vs_fp64')
+           if k_ in bor}
+    for prec in ('double', 'mixed'):
+        if prec in bor:
+            out[prec] = {k_: bor[prec][k_] for k_ in ('seconds', 'solves_per_s', 'fp64_fallback_modes')
+                         if k_ in bor[prec]}
+    return out
+
+
+def write_detail(detail):
+    """Telemetry, per-kernel profiles and the secondary legs' full records, beside the line."""
+    folder = os.path.join(ROOT, 'gpurun_out')
+    if not os.path.isdir(folder):
+        return None
+    path = os.path.join(folder, 'bench_detail.json')
+    with open(path, 'w') as fh:
+        json.dump(detail, fh, default=str)
+    return os.path.relpath(path, ROOT)
 
 
 def main():
@@ -424,7 +595,7 @@ def main():
     ap.add_argument('--n', type=int, default=2048)
     ap.add_argument('--angles', type=int, default=720)
     ap.add_argument('--seed', type=int, default=0)
-    ap.add_argument('--cpu-sample', type=int, default=1, help='oracle solves timed for cpu_baseline (0 = skip)')
+    ap.add_argument('--cpu-sample', type=int, default=1, help='time one full CPU-port solve for cpu_baseline (0 = skip)')
     ap.add_argument('--serving', type=int, default=1, help='run the mixed request stream (p50/p99 latency)')
     ap.add_argument('--serving-requests', type=int, default=32)
     ap.add_argument('--bor', type=int, default=1, help='time the body-of-revolution ogive workload')
@@ -432,6 +603,8 @@ def main():
     ap.add_argument('--sweep', type=int, default=256, help='frequencies of the airfoil sweep leg (0 = skip)')
     ap.add_argument('--autotune', type=int, default=1, help='tune the solve tile shapes for the workload first')
     ap.add_argument('--far-block', type=int, default=1, help='time the Galerkin far-block pass (boundary B2)')
+    ap.add_argument('--formulation', default='galerkin', choices=['galerkin', 'pulse'],
+                    help="2-D discretisation: the reference's linear Galerkin (default) or pulse basis")
     args = ap.parse_args()
 
     world = int(os.environ.get('WORLD_SIZE', '1'))
@@ -451,14 +624,20 @@ def main():
 
     from grim_20261007_b200.device import all_contexts, context, run_concurrent
     from grim_20261007_b200.execution import linear_precision
-    from grim_20261007_b200.twod import geometry as geo, operators as ops
+    from grim_20261007_b200.twod import galerkin, geometry as geo, operators as ops
     from grim_20261007_b200.twod.solver import solve_monostatic_rcs_2d
     from grim_20261007_b200 import synthetic as S
 
     ctx = context()
     v, k, f, thick, ang = workload(args.seed + rank, args.n, args.angles)
-    geom = geo.panel_geometry([v])
-    bodies = {'TM': ops.DeviceBody(geom, None), 'TE': ops.DeviceBody(geom, geo.te_curvature_correction([v]))}
+    if args.formulation == 'galerkin':
+        gal = galerkin.GalerkinBody([v])
+        bodies = {'TM': gal, 'TE': gal}
+        h2d_body = gal.h2d_bytes
+    else:
+        geom = geo.panel_geometry([v])
+        bodies = {'TM': ops.DeviceBody(geom, None), 'TE': ops.DeviceBody(geom, geo.te_curvature_correction([v]))}
+        h2d_body = 2 * geom.nbytes + geom.shape[0] * 8
     ang_dev = torch.as_tensor(ang, device='cuda')
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device='cuda')
 
@@ -543,8 +722,14 @@ def main():
     tele64 = {p: {kk: vv for kk, vv in out64[p]['telemetry'].items() if not hasattr(vv, 'cpu')} for p in ('TM', 'TE')}
     berr64 = max(float(out64[p]['telemetry']['backward_error_dev'].max()) for p in ('TM', 'TE'))
 
+    # the same amplitudes against the reference solver's own (its stored complex amplitudes
+    # for this airfoil, tests/golden/ref_airfoil.npz), where the workload is the fixture's
+    parity = reference_parity(args, rank, k, {p: out64[p]['amplitude'].cpu().numpy() for p in ('TM', 'TE')},
+                              {p: out32[p]['amplitude'].cpu().numpy() for p in ('TM', 'TE')})
+
     # end-to-end through the public API (host geometry in, host amplitudes out)
     snap = S.snapshot_from_polygons([v])
+    os.environ['GRIM_2D_FORMULATION'] = args.formulation
     with linear_precision('mixed'):
         solve_monostatic_rcs_2d(snap, [f / 1e9], list(ang), geometry_units='meters', strict_quality_gate=False)
         torch.cuda.synchronize()
@@ -559,7 +744,7 @@ def main():
     if world > 1:
         dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
     e2e_value = 2 * e2e_steps * world / float(e2e_t[0])
-    h2d = 2 * (geom.nbytes + len(ang) * 8) + geom.shape[0] * 8
+    h2d = h2d_body + 2 * len(ang) * 8
     d2h = 2 * len(ang) * 16
 
     def settle():
@@ -583,64 +768,45 @@ def main():
     step_serial('double')
     prof = profile_step([ctx], lambda: step_serial('mixed'))
     prof64 = profile_step([ctx], lambda: step_serial('double'))
-    hbm, bf16, src = _peaks()
-    dom_name, dom = max(prof.items(), key=lambda kv: kv[1]['ms'])
-    step_ms = sum(v['ms'] for v in prof.values())
-    if dom['flops'] > 0:
-        achieved = dom['flops'] / (dom['ms'] * 1e-3) / 1e12
-        roofline = {'bound': 'tensor', 'achieved': achieved, 'peak': bf16, 'unit': 'TFLOP/s', 'frac': achieved / bf16,
-                    'traffic': None, 'kernel': dom_name, 'launches': dom['launches'],
-                    'avg_launch_ms': dom['ms'] / dom['launches'], 'flops_per_launch': dom['flops'] / dom['launches'],
-                    'share_of_step': dom['ms'] / step_ms, 'peak_source': src,
-                    'peak_note': 'measured dense bf16 tensor peak; the kernel computes complex64 as split TF32 '
-                                 '(3 tcgen05 TF32 products, 8 M N K algorithmic flops counted once) and the dense '
-                                 'TF32 rate is half the bf16 rate'}
-        if dom_name in NCU_TRAFFIC:
-            nbytes, nflops = NCU_TRAFFIC[dom_name]
-            roofline['traffic'] = nbytes * (dom['flops'] / dom['launches']) / nflops
-            roofline['traffic_note'] = 'bytes per launch: one ncu capture scaled by the launch flops'
-    else:
-        achieved = dom['bytes'] / (dom['ms'] * 1e-3) / 1e9
-        roofline = {'bound': 'hbm', 'achieved': achieved, 'peak': hbm, 'unit': 'GB/s', 'frac': achieved / hbm,
-                    'traffic': None, 'kernel': dom_name, 'launches': dom['launches'], 'peak_source': src}
+    roofline = kernel_roofline(prof)
 
     cpu_baseline = None
     if rank == 0 and world == 1 and args.cpu_sample > 0:
-        t0 = time.perf_counter()
-        for _ in range(args.cpu_sample):
-            cpu_oracle_solve(v, k, ang, 'TM')
-        dt = time.perf_counter() - t0
-        cpu_baseline = {'value': args.cpu_sample / dt, 'unit': UNIT, 'cores': 1, 'kind': 'port',
-                        'sample': f'{args.cpu_sample} full TM solve(s) of the workload by the FP64 NumPy/SciPy oracle '
-                                  '(single-threaded SciPy Bessel fill, LAPACK LU)'}
+        cpu_baseline = cpu_baseline_sample(args, v, k, ang)
 
     if rank == 0:
+        detail = {'telemetry_mixed': tele32, 'telemetry_fp64': tele64, 'kernel_profile_mixed': prof,
+                  'kernel_profile_fp64': prof64, 'serving': serving, 'bor_ogive': bor, 'frequency_sweep': sweep,
+                  'far_block': farblk, 'autotune': autotune}
+        detail_path = write_detail(detail)
         line = {
             'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': world, 'steps': args.steps,
             'warmup': args.warmup, 'ms_per_step': ms_step32, 'higher_is_better': True, 'scaling': 'weak',
             'vs_baseline': None, 'dtype': 'c64+f64', 'data': 'synthetic (seeded NACA 00tt airfoil)',
             'config': {'workload': f'2-D airfoil N={n}, {args.angles} monostatic angles, TM+TE (2 solves/step), '
-                                   'mixed precision', 'n_panels': n, 'angles': args.angles, 'seed': args.seed,
-                       'frequency_ghz': f / 1e9, 'thickness': thick,
+                                   f'mixed precision, {args.formulation} formulation', 'n_elements': n,
+                       'angles': args.angles, 'seed': args.seed, 'frequency_ghz': f / 1e9, 'thickness': thick,
+                       'formulation': args.formulation,
                        'l2': 'flushed between steps (256 MiB write outside each step\'s event window)',
                        'parallelism': f'replicas x{world}'},
             'fp64_gpu': {'value': fp64_value, 'ms_per_step': ms_step64, 'max_backward_error': berr64},
             'speedup_vs_fp64': value / fp64_value if fp64_value else None,
             'max_db_error_vs_fp64': err_db,
-            'telemetry_mixed': tele32, 'telemetry_fp64': tele64,
+            'parity_vs_reference': parity,
             'e2e': {'value': e2e_value, 'unit': UNIT, 'h2d_bytes_per_step': int(h2d), 'd2h_bytes_per_step': int(d2h),
                     'path': 'solve_monostatic_rcs_2d (public API), linear_precision("mixed")'},
             'gpu_launches': int(launches32),
             'roofline': roofline,
-            'serving': serving,
-            'bor_ogive': bor,
-            'frequency_sweep': sweep,
-            'far_block': farblk,
-            'autotune': autotune,
-            'kernel_profile_mixed': prof,
-            'kernel_profile_fp64': prof64,
+            'top_kernels_mixed': top_kernels(prof),
+            'serving': summarize(serving, ('requests', 'completed', 'solves_per_s', 'p50_s', 'p99_s', 'cache_hits')),
+            'bor_ogive': summarize_bor(bor),
+            'frequency_sweep': summarize(sweep, ('systems', 'seconds', 'solves_per_s', 'n_min', 'n_max',
+                                                 'max_db_error_vs_fp64_sampled', 'path')),
+            'far_block': summarize(farblk, ('gpu_pairs_per_s', 'gpu_host_buffers_pairs_per_s',
+                                            'reference_cpu_pairs_per_s', 'bitwise_equal_to_reference_on_sample')),
             'cpu_baseline': cpu_baseline,
             'clocks': clocks,
+            'detail_file': detail_path,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

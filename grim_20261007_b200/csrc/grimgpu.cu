@@ -668,6 +668,8 @@ static int smem_opt_in() {
     const int tri = (NB * NBP + NB) * (int)sizeof(C);
     GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_panel_apply<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, tri));
     GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_panel_u_moves<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, tri));
+    GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_apply_moves<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         GEPP_MOVES_SMEM_MAX));
     GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_trsm_diag<C, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, tri));
     GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_trsm_diag<C, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, tri));
     done.mark();
@@ -942,7 +944,22 @@ static int getrf_impl(grim_context *h, int n, C *A, int64_t lda, int *ipiv, int 
             status = grim_launch_status(h, kname("k_panel_last", sizeof(C)), 0, 0);
         }
     }
-    if (status == GRIM_OK) {
+    if (status == GRIM_OK && moves && (size_t)n * sizeof(C) <= GEPP_MOVES_SMEM_MAX && n > NB) {
+        // partial pivoting: every panel's row moves, then each factored column takes those of
+        // the panels after it (one CTA per column, in shared memory)
+        void *pm = nullptr;
+        status = grim_workspace(h, "lu_moves_all", (size_t)npan * GEPP_MOVES_STRIDE * sizeof(int), &pm);
+        if (status == GRIM_OK) {
+            k_ipiv_moves<<<ceil_div(npan, 4), 128, 0, h->stream>>>(n, ipiv, (int *)pm);
+            status = grim_launch_status(h, "k_ipiv_moves", 0, 0);
+        }
+        if (status == GRIM_OK) {
+            const int ncols = (npan - 1) * NB;
+            k_apply_moves<C><<<ncols, 256, (size_t)n * sizeof(C), h->stream>>>(n, A, lda, 0, 1, (const int *)pm,
+                                                                                nullptr);
+            status = grim_launch_status(h, kname("k_apply_moves_left", sizeof(C)), 0, 0);
+        }
+    } else if (status == GRIM_OK) {
         k_laswp_left<C><<<ceil_div(n, 128), 128, 0, h->stream>>>(n, A, lda, NB, swapped, ipiv);
         status = grim_launch_status(h, kname("k_laswp_left", sizeof(C)), 0, 0);
     }
@@ -983,6 +1000,13 @@ static int getrf_read_flags(grim_context *h, int *info, int *pivoted) {
 
 // getrs: interchanges (skipped when ipiv is the identity), then per 64-row block an
 // in-place diagonal triangular solve and a GEMM update of the remaining rows.
+static int rs_moves(grim_context *h, int n, int **out) {
+    void *p = nullptr;
+    GRIM_TRY(grim_workspace(h, "rs_moves", (size_t)ceil_div(n, NB) * GEPP_MOVES_STRIDE * sizeof(int), &p));
+    *out = (int *)p;
+    return GRIM_OK;
+}
+
 template <typename C>
 static int getrs_prepare(grim_context *h, int n, const int *ipiv, int **ident_out) {
     void *p_id = nullptr;
@@ -991,7 +1015,31 @@ static int getrs_prepare(grim_context *h, int n, const int *ipiv, int **ident_ou
     GRIM_CHECK_CUDA(cudaMemsetAsync(ident, 0xff, sizeof(int), h->stream));
     k_ipiv_identity<<<ceil_div(n, 256), 256, 0, h->stream>>>(n, ipiv, ident);
     GRIM_CHECK_LAUNCH(h, "k_ipiv_identity");
+    if ((size_t)n * sizeof(C) <= GEPP_MOVES_SMEM_MAX) {
+        // the row moves of every panel, for the right-hand sides' interchanges
+        int *mv = nullptr;
+        GRIM_TRY(rs_moves(h, n, &mv));
+        k_ipiv_moves<<<ceil_div(ceil_div(n, NB), 4), 128, 0, h->stream>>>(n, ipiv, mv);
+        GRIM_CHECK_LAUNCH(h, "k_ipiv_moves");
+    }
     *ident_out = ident;
+    return GRIM_OK;
+}
+
+// Right-hand-side interchanges of getrs: the panels' row moves applied in shared memory, one
+// CTA per column (the rows moves of getrs_prepare), or LAPACK's sequential swaps when a
+// column does not fit.
+template <typename C>
+static int rhs_interchanges(grim_context *h, int n, int nrhs, C *B, int64_t ldb, const int *ipiv, const int *ident) {
+    if ((size_t)n * sizeof(C) <= GEPP_MOVES_SMEM_MAX) {
+        int *mv = nullptr;
+        GRIM_TRY(rs_moves(h, n, &mv));
+        k_apply_moves<C><<<nrhs, 256, (size_t)n * sizeof(C), h->stream>>>(n, B, ldb, 0, 0, mv, ident);
+        GRIM_CHECK_LAUNCH(h, kname("k_apply_moves_rhs", sizeof(C)));
+        return GRIM_OK;
+    }
+    k_laswp_rhs<C><<<ceil_div(nrhs, 128), 128, 0, h->stream>>>(n, nrhs, B, ldb, ipiv, ident);
+    GRIM_CHECK_LAUNCH(h, kname("k_laswp_rhs", sizeof(C)));
     return GRIM_OK;
 }
 
@@ -1000,8 +1048,7 @@ static int getrs_apply(grim_context *h, int n, int nrhs, const C *LU, int64_t ld
                        C *B, int64_t ldb) {
     const int npan = ceil_div(n, NB);
     const size_t tri = (size_t)(NB * NBP + NB) * sizeof(C);
-    k_laswp_rhs<C><<<ceil_div(nrhs, 128), 128, 0, h->stream>>>(n, nrhs, B, ldb, ipiv, ident);
-    GRIM_CHECK_LAUNCH(h, kname("k_laswp_rhs", sizeof(C)));
+    GRIM_TRY(rhs_interchanges<C>(h, n, nrhs, B, ldb, ipiv, ident));
     const int ctiles = ceil_div(nrhs, TRSM_COLS);
     for (int p = 0; p < npan; ++p) {
         const int j = p * NB, nbj = std::min(NB, n - j);
@@ -1214,8 +1261,7 @@ static int gs_build(grim_context *h, int n, const float2 *LU, int64_t lda, int n
 static int gs_apply(grim_context *h, const GsPanels &P, int nrhs, const int *ipiv, const int *ident, float2 *B,
                     int64_t ldb) {
     const int n = P.n, nb = P.nb;
-    k_laswp_rhs<float2><<<ceil_div(nrhs, 128), 128, 0, h->stream>>>(n, nrhs, B, ldb, ipiv, ident);
-    GRIM_CHECK_LAUNCH(h, "k_laswp_rhs<c64>");
+    GRIM_TRY(rhs_interchanges<float2>(h, n, nrhs, B, ldb, ipiv, ident));
     const int bn = h->tune_solve_bn ? h->tune_solve_bn : tc_bn(nrhs), np = ceil_div(nrhs, bn) * bn;
     TcPacked pb;
     GRIM_TRY(tc_ws(h, "gs_b", np, tc_kp(GS_NB_MAX), &pb));
@@ -1480,7 +1526,11 @@ static int mixed_refine(grim_context *h, int n, int nrhs, const TA *Ares, int64_
     GRIM_TRY(smem_opt_in<float2>());
     GRIM_TRY(getrs_prepare<float2>(h, n, ipiv, &ident));
     GsPanels panels;
-    const bool use_gs = gs_wanted(n, nrhs);
+    // the packed-panel solve multiplies by explicitly inverted 512-row triangular blocks: fast,
+    // and accurate for diagonally dominant factors; partial-pivoting factors (the
+    // combined-field systems) keep the substitution solve, whose first backward error is
+    // two orders of magnitude smaller there (one refinement step saved)
+    const bool use_gs = gs_wanted(n, nrhs) && h->pivot_mode != GRIM_PIVOT_PARTIAL;
     if (use_gs) GRIM_TRY(gs_build(h, n, lu32, n, h->tune_gs_block ? h->tune_gs_block : gs_block(n, nrhs), &panels));
     auto solve32 = [&](float2 *X32) -> int {
         if (use_gs) return gs_apply(h, panels, nrhs, ipiv, ident, X32, n);

@@ -4,13 +4,15 @@
 // The 64-column panel rows j..n-1 are spread over the CS CTAs of one cluster, CTA c holding
 // panel rows [c rpc, (c+1) rpc) in shared memory (rows past its capacity in a global
 // scratch, which stays in L2).  Column step k:
-//   1. every CTA finds its best candidate for column k among its rows >= k, and publishes
-//      the candidate's whole row (and row k, if it owns it) in a double-buffered slot;
-//   2. one cluster barrier;
-//   3. every CTA reads the CS candidates through distributed shared memory, takes the
-//      largest (first row on ties), copies the winning row p, and the owners of rows k
-//      and p swap them (from the published copies);
-//   4. l = a_rk / a_kk and a_rc -= l a_kc on the CTA's own rows.
+//   1. every CTA reduces its best candidate for column k among its rows >= k and publishes
+//      the candidate's whole row (and row k, if it owns it) in a double-buffered slot,
+//      with step k - 1's rank-1 update (still pending on columns > k) applied on the fly;
+//   2. it arrives at the cluster barrier, finishes that pending update on its own rows
+//      while the other CTAs arrive, and waits;
+//   3. one warp reads the CS candidates through distributed shared memory, then the
+//      winner's row and row k; the owners of rows k and p swap them;
+//   4. one thread per row forms l = a_rk / a_kk, updates column k + 1 at once and finds
+//      the candidates of step k + 1.
 // One cluster barrier per column: a slot is rewritten two steps later, after every CTA
 // has passed the barrier that follows its reads.  Every CTA runs the same steps, barriers
 // included, whatever its rows.
@@ -42,7 +44,7 @@ struct GeppPub {
 // Fixed shared memory of the panel kernel (the rows follow it).
 template <typename C>
 __host__ __device__ constexpr size_t gepp_fixed_smem() {
-    return (2 * sizeof(GeppPub<C>) + NB * sizeof(C) /* prow */ + (size_t)GEPP_THREADS / 32 * 16 /* reduce */ +
+    return (2 * sizeof(GeppPub<C>) + 2 * NB * sizeof(C) /* prow */ + (size_t)GEPP_THREADS / 32 * 16 /* reduce */ +
             4 * NB * sizeof(int) /* ipiv, first, slot, content */ + 2 * NB * sizeof(int) /* extras */ + 64 + 15) /
            16 * 16;
 }
@@ -52,6 +54,111 @@ __device__ __forceinline__ bool gepp_better(double v, int i, double bv, int bi) 
     return v > bv || (v == bv && i < bi);
 }
 
+// Row moves of one panel's interchanges (one warp): ipiv_s[k] is the panel row that step k
+// swapped with row k (k < nbj).  Simulating the swaps on the touched rows -- the panel's
+// first nbj rows and the targets below them -- gives, for each touched row, the row whose
+// content ends there: moves[0] = count, then count destination rows and, GEPP_MAX_MOVES
+// entries on, count source rows (absolute: + j).  Scratch (shared): first, slot (NB ints),
+// content (2 NB), extra (NB).  Returns the count (every lane).
+__device__ __forceinline__ int panel_moves(const int *ipiv_s, int nbj, int j, int *moves, int *first, int *slot,
+                                           int *content, int *extra) {
+    const int lane = threadIdx.x & 31;
+    // first[k]: the first interchange with the same target row; extra targets (rows >= nbj)
+    // get slots nbj, nbj + 1, ... in order of first appearance
+    for (int k = lane; k < nbj; k += 32) {
+        int f = k;
+        for (int q = 0; q < k; ++q)
+            if (ipiv_s[q] == ipiv_s[k]) { f = q; break; }
+        first[k] = f;
+    }
+    __syncwarp();
+    int base = 0;
+    for (int k0 = 0; k0 < nbj; k0 += 32) {
+        const int k = k0 + lane;
+        const bool is_new = k < nbj && ipiv_s[k] >= nbj && first[k] == k;
+        const unsigned bal = __ballot_sync(0xffffffffu, is_new);
+        if (is_new) {
+            const int at = base + __popc(bal & ((1u << lane) - 1u));
+            slot[k] = nbj + at;
+            extra[at] = ipiv_s[k];
+        }
+        base += __popc(bal);
+    }
+    __syncwarp();
+    int cnt = 0;
+    if (lane == 0) {
+        for (int s = 0; s < nbj + base; ++s) content[s] = s < nbj ? s : extra[s - nbj];
+        for (int k = 0; k < nbj; ++k) {
+            const int pk_ = ipiv_s[k];
+            if (pk_ == k) continue;
+            const int sp = pk_ < nbj ? pk_ : slot[first[k]];
+            const int t = content[k];
+            content[k] = content[sp];
+            content[sp] = t;
+        }
+        for (int s = 0; s < nbj + base; ++s) {
+            const int pos = s < nbj ? s : extra[s - nbj];
+            if (content[s] != pos) {
+                moves[1 + cnt] = j + pos;                        // destination row
+                moves[1 + GEPP_MAX_MOVES + cnt] = j + content[s];  // source row
+                ++cnt;
+            }
+        }
+        moves[0] = cnt;
+    }
+    return __shfl_sync(0xffffffffu, cnt, 0);
+}
+
+// Row moves of every panel of a factorization, from its ipiv (1-based, absolute): one warp
+// per panel, moves of panel p at moves_all + p * GEPP_MOVES_STRIDE.
+#define GEPP_MOVES_STRIDE (1 + 2 * GEPP_MAX_MOVES)
+__global__ void __launch_bounds__(128) k_ipiv_moves(int n, const int *__restrict__ ipiv, int *__restrict__ moves_all) {
+    __shared__ int sc[4][NB * 6];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int p = blockIdx.x * 4 + warp;
+    const int npan = (n + NB - 1) / NB;
+    if (p >= npan) return;
+    const int j = p * NB, nbj = min(NB, n - j);
+    int *ip = sc[warp], *first = ip + NB, *slot = first + NB, *content = slot + NB, *extra = content + 2 * NB;
+    for (int k = lane; k < nbj; k += 32) ip[k] = ipiv[j + k] - 1 - j;
+    __syncwarp();
+    panel_moves(ip, nbj, j, moves_all + (size_t)p * GEPP_MOVES_STRIDE, first, slot, content, extra);
+}
+
+// Applies the row moves of panels first.. npan-1 to columns of B (one CTA per column, the
+// rows it can change staged in shared memory): the interchanges of getrs' right-hand
+// sides (left = 0: every panel, every row) and of the factored columns left of later
+// panels (left = 1: column c of panel c / NB takes the panels after it, rows from the next
+// panel on).  ident (may be NULL): nothing to do when *ident is set.  Dynamic smem: n
+// elements (n * sizeof(C) <= GEPP_MOVES_SMEM_MAX).
+#define GEPP_MOVES_SMEM_MAX (200 * 1024)
+template <typename C>
+__global__ void __launch_bounds__(256)
+k_apply_moves(int n, C *__restrict__ B, int64_t ldb, int col0, int left, const int *__restrict__ moves_all,
+              const int *__restrict__ ident) {
+    extern __shared__ __align__(16) unsigned char mv_smem[];
+    C *col = reinterpret_cast<C *>(mv_smem);
+    const int c = col0 + blockIdx.x;
+    const int npan = (n + NB - 1) / NB;
+    const int first = left ? c / NB + 1 : 0;
+    if (first >= npan || (ident && *ident)) return;
+    const int row0 = first * NB;
+    C *b = B + (int64_t)c * ldb;
+    for (int r = row0 + threadIdx.x; r < n; r += blockDim.x) col[r - row0] = b[r];
+    __syncthreads();
+    for (int p = first; p < npan; ++p) {
+        const int *mv = moves_all + (size_t)p * GEPP_MOVES_STRIDE;
+        const int cnt = min(mv[0], GEPP_MAX_MOVES);
+        C v = czero<C>();
+        const bool act = threadIdx.x < cnt;
+        if (act) v = col[mv[1 + GEPP_MAX_MOVES + threadIdx.x] - row0];
+        __syncthreads();
+        if (act) col[mv[1 + threadIdx.x] - row0] = v;
+        __syncthreads();
+    }
+    for (int r = row0 + threadIdx.x; r < n; r += blockDim.x) b[r] = col[r - row0];
+}
+
 template <typename C>
 __global__ void __launch_bounds__(GEPP_THREADS)
 k_panel_gepp(int n, C *__restrict__ A, int64_t lda, int j, int nbj, int rpc, int rows_smem, C *__restrict__ gscratch,
@@ -59,15 +166,16 @@ k_panel_gepp(int n, C *__restrict__ A, int64_t lda, int j, int nbj, int rpc, int
              PanelPack pk) {
     cg::cluster_group cluster = cg::this_cluster();
     const int rank = (int)cluster.block_rank();
+    const int cs = (int)cluster.num_blocks();
     extern __shared__ __align__(16) unsigned char gepp_smem[];
     GeppPub<C> *pub = reinterpret_cast<GeppPub<C> *>(gepp_smem);
-    C *prow = reinterpret_cast<C *>(pub + 2);
-    double *red_v = reinterpret_cast<double *>(prow + NB);
+    C *prow = reinterpret_cast<C *>(pub + 2);  // [2][NB]: the pivot rows of the last two steps
+    double *red_v = reinterpret_cast<double *>(prow + 2 * NB);
     int *red_i = reinterpret_cast<int *>(red_v + GEPP_THREADS / 32);
     int *ipiv_s = red_i + GEPP_THREADS / 32;
     int *first = ipiv_s + NB, *slot = first + NB, *content = slot + NB, *extra = content + 2 * NB;
     C *rows = reinterpret_cast<C *>(gepp_smem + gepp_fixed_smem<C>());
-    __shared__ int s_p, s_w, s_zero, s_nextra;
+    __shared__ int s_p, s_zero;
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int m = n - j;
@@ -83,18 +191,19 @@ k_panel_gepp(int n, C *__restrict__ A, int64_t lda, int j, int nbj, int rpc, int
     }
     __syncthreads();
 
+    // Step k starts with column k up to date on every row g >= k and the rank-1 update of
+    // step k - 1 still pending on columns > k (multipliers in column k - 1, pivot row in
+    // prow[(k - 1) & 1]); it finishes it while the cluster barrier completes.
+    double bv = -1.0;
+    int bi = 0x7fffffff;
+    for (int r = tid; r < nr; r += GEPP_THREADS) {
+        const double v = (double)cabs1(rowp(r)[0]);
+        if (gepp_better(v, r0 + r, bv, bi)) { bv = v; bi = r0 + r; }
+    }
     for (int k = 0; k < nbj; ++k) {
         const int par = k & 1;
-        // 1. local candidate for column k among rows >= k
-        double bv = -1.0;
-        int bi = 0x7fffffff;
-        for (int r = tid; r < nr; r += GEPP_THREADS) {
-            const int g = r0 + r;
-            if (g >= k) {
-                const double v = (double)cabs1(rowp(r)[k]);
-                if (gepp_better(v, g, bv, bi)) { bv = v; bi = g; }
-            }
-        }
+        const C *uprev = prow + (par ^ 1) * NB;
+        // 1. the CTA's candidate for column k, published with the pending update applied
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             const double ov = __shfl_down_sync(0xffffffffu, bv, o);
@@ -103,26 +212,59 @@ k_panel_gepp(int n, C *__restrict__ A, int64_t lda, int j, int nbj, int rpc, int
         }
         if (lane == 0) { red_v[warp] = bv; red_i[warp] = bi; }
         __syncthreads();
-        if (tid == 0) {
-            for (int w = 1; w < GEPP_THREADS / 32; ++w)
-                if (gepp_better(red_v[w], red_i[w], bv, bi)) { bv = red_v[w]; bi = red_i[w]; }
-            pub[par].val = bv;
-            pub[par].idx = bi;
-            red_i[0] = bi;
+        if (warp == 0) {
+            bv = lane < GEPP_THREADS / 32 ? red_v[lane] : -1.0;
+            bi = lane < GEPP_THREADS / 32 ? red_i[lane] : 0x7fffffff;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
+                const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+                if (gepp_better(ov, oi, bv, bi)) { bv = ov; bi = oi; }
+            }
+            const bool own_k = k >= r0 && k < r0 + nr;
+            for (int c = lane; c < NB; c += 32) {
+                if (bi != 0x7fffffff) {
+                    const C *a = rowp(bi - r0);
+                    C x = a[c];
+                    if (k > 0 && c > k) cfms(x, a[k - 1], uprev[c]);
+                    pub[par].row[c] = x;
+                }
+                if (own_k) {
+                    const C *a = rowp(k - r0);
+                    C x = a[c];
+                    if (k > 0 && c > k) cfms(x, a[k - 1], uprev[c]);
+                    pub[par].krow[c] = x;
+                }
+            }
+            if (lane == 0) {
+                pub[par].val = bv;
+                pub[par].idx = bi;
+            }
         }
+        // the published rows are read before any warp applies the pending update to them
         __syncthreads();
-        const int best = red_i[0];
-        if (tid < NB) {
-            if (best != 0x7fffffff) pub[par].row[tid] = rowp(best - r0)[tid];
-            if (k >= r0 && k < r0 + nr) pub[par].krow[tid] = rowp(k - r0)[tid];
+        cluster.barrier_arrive();
+        // 2. the pending update of step k - 1 on the CTA's rows >= k, columns > k: one thread
+        //    per row along its contiguous columns
+        if (k > 0) {
+            for (int r = tid; r < nr; r += GEPP_THREADS) {
+                if (r0 + r >= k) {
+                    C *a = rowp(r);
+                    const C l = a[k - 1];
+#pragma unroll 8
+                    for (int c = k + 1; c < NB; ++c) cfms(a[c], l, uprev[c]);
+                }
+            }
         }
-        // 2. every CTA's candidate is published
-        cluster.sync();
-        // 3. the winner: largest |re| + |im|, first row on ties
+        cluster.barrier_wait();
+        __syncthreads();
+        // 3. warp 0: the winner (largest |re| + |im|, first row on ties) from the CS published
+        //    candidates, then its row and row k, two columns per lane; the owners of rows k
+        //    and p swap them
         if (warp == 0) {
             double v = -1.0;
             int i = 0x7fffffff, w = 0;
-            if (lane < (int)cluster.num_blocks()) {
+            if (lane < cs) {
                 const GeppPub<C> *rp = cluster.map_shared_rank(&pub[par], lane);
                 v = rp->val;
                 i = rp->idx;
@@ -130,56 +272,59 @@ k_panel_gepp(int n, C *__restrict__ A, int64_t lda, int j, int nbj, int rpc, int
             }
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) {
-                const double ov = __shfl_down_sync(0xffffffffu, v, o);
-                const int oi = __shfl_down_sync(0xffffffffu, i, o);
-                const int ow = __shfl_down_sync(0xffffffffu, w, o);
+                const double ov = __shfl_xor_sync(0xffffffffu, v, o);
+                const int oi = __shfl_xor_sync(0xffffffffu, i, o);
+                const int ow = __shfl_xor_sync(0xffffffffu, w, o);
                 if (gepp_better(ov, oi, v, i)) { v = ov; i = oi; w = ow; }
+            }
+            const bool zero = !(v > 0.0);
+            const int ck = k / rpc;
+            const GeppPub<C> *wp = cluster.map_shared_rank(&pub[par], w);
+            const GeppPub<C> *kp = cluster.map_shared_rank(&pub[par], ck);
+            const C x0 = wp->row[lane], x1 = wp->row[lane + 32];
+            const C k0 = kp->krow[lane], k1 = kp->krow[lane + 32];
+            prow[par * NB + lane] = x0;
+            prow[par * NB + lane + 32] = x1;
+            if (i != k && !zero) {
+                if (rank == ck) {
+                    C *a = rowp(k - r0);
+                    a[lane] = x0;
+                    a[lane + 32] = x1;
+                }
+                if (rank == i / rpc) {
+                    C *a = rowp(i - r0);
+                    a[lane] = k0;
+                    a[lane + 32] = k1;
+                }
             }
             if (lane == 0) {
                 s_p = i;
-                s_w = w;
-                s_zero = !(v > 0.0);
-                if (rank == 0) ipiv_s[k] = i;
+                s_zero = zero;
+                if (rank == 0) ipiv_s[k] = zero ? k : i;
             }
         }
         __syncthreads();
-        const int p = s_p;
         const bool zero = s_zero;
-        const int ck = k / rpc, cp = p / rpc;
-        if (tid < NB) {
-            const C pv = cluster.map_shared_rank(&pub[par], s_w)->row[tid];
-            prow[tid] = pv;
-            if (p != k && !zero) {
-                if (rank == ck) rowp(k - r0)[tid] = pv;
-                if (rank == cp) rowp(p - r0)[tid] = cluster.map_shared_rank(&pub[par], ck)->krow[tid];
-            }
-        }
-        __syncthreads();
-        if (zero) {
-            // LAPACK getf2: a zero pivot column is left as it is, info records its first
-            if (rank == 0 && tid == 0) atomicCAS(info, 0, j + k + 1);
-            continue;
-        }
-        // 4. multipliers, then the rank-1 update of the CTA's rows below k
-        const C rp = crecip(prow[k]);
+        if (zero && rank == 0 && tid == 0) atomicCAS(info, 0, j + k + 1);
+        // 4. multipliers of the CTA's rows below k (LAPACK leaves a zero pivot column
+        //    unscaled), column k + 1 updated at once, and the candidates of step k + 1
+        const C *u = prow + par * NB;
+        const C rp = zero ? one_c<C>() : crecip(u[k]);
+        bv = -1.0;
+        bi = 0x7fffffff;
         for (int r = tid; r < nr; r += GEPP_THREADS) {
-            if (r0 + r > k) {
+            const int g = r0 + r;
+            if (g > k) {
                 C *a = rowp(r);
-                a[k] = cmul(a[k], rp);
-            }
-        }
-        __syncthreads();
-        const int c = tid & (NB - 1), rg = tid >> 6;
-        if (c > k) {
-            const C u = prow[c];
-            for (int r = rg; r < nr; r += GEPP_THREADS / NB) {
-                if (r0 + r > k) {
-                    C *a = rowp(r);
-                    cfms(a[c], a[k], u);
+                const C l = zero ? a[k] : cmul(a[k], rp);
+                a[k] = l;
+                if (k + 1 < NB) {
+                    cfms(a[k + 1], l, u[k + 1]);
+                    const double v = (double)cabs1(a[k + 1]);
+                    if (gepp_better(v, g, bv, bi)) { bv = v; bi = g; }
                 }
             }
         }
-        __syncthreads();
     }
     // every CTA has finished reading every other CTA's slots before any CTA exits
     cluster.sync();
@@ -223,54 +368,8 @@ k_panel_gepp(int n, C *__restrict__ A, int64_t lda, int j, int nbj, int rpc, int
     if (rank != 0) return;
     if (tid < nbj) ipiv[j + tid] = j + ipiv_s[tid] + 1;
     if (warp == 0) {
-        // first[k]: the first interchange with the same target row; extra targets (rows >= nbj)
-        // get slots nbj, nbj + 1, ... in order of first appearance
-        for (int k = lane; k < nbj; k += 32) {
-            int f = k;
-            for (int q = 0; q < k; ++q)
-                if (ipiv_s[q] == ipiv_s[k]) { f = q; break; }
-            first[k] = f;
-        }
-        __syncwarp();
-        int base = 0;
-        for (int k0 = 0; k0 < nbj; k0 += 32) {
-            const int k = k0 + lane;
-            const bool is_new = k < nbj && ipiv_s[k] >= nbj && first[k] == k;
-            const unsigned bal = __ballot_sync(0xffffffffu, is_new);
-            if (is_new) {
-                const int at = base + __popc(bal & ((1u << lane) - 1u));
-                slot[k] = nbj + at;
-                extra[at] = ipiv_s[k];
-            }
-            base += __popc(bal);
-        }
-        __syncwarp();
-        if (lane == 0) {
-            s_nextra = base;
-            // simulate the interchanges on the touched rows: content[s] = original row now at slot s
-            for (int s = 0; s < nbj + base; ++s) content[s] = s < nbj ? s : extra[s - nbj];
-            int any = 0;
-            for (int k = 0; k < nbj; ++k) {
-                const int pk_ = ipiv_s[k];
-                if (pk_ == k) continue;
-                any = 1;
-                const int sp = pk_ < nbj ? pk_ : slot[first[k]];
-                const int t = content[k];
-                content[k] = content[sp];
-                content[sp] = t;
-            }
-            *swapped = any;
-            int cnt = 0;
-            for (int s = 0; s < nbj + base; ++s) {
-                const int pos = s < nbj ? s : extra[s - nbj];
-                if (content[s] != pos) {
-                    moves[1 + cnt] = j + pos;                        // destination row
-                    moves[1 + GEPP_MAX_MOVES + cnt] = j + content[s];  // source row
-                    ++cnt;
-                }
-            }
-            moves[0] = cnt;
-        }
+        const int cnt = panel_moves(ipiv_s, nbj, j, moves, first, slot, content, extra);
+        if (lane == 0) *swapped = cnt > 0;
     }
 }
 

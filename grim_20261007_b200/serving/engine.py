@@ -278,9 +278,12 @@ class ServingEngine:
         st = _lib.GrimSolveInfo()
         if mixed:
             b0 = b.clone()
+            # the cached factor pivots partially: its solves keep the substitution kernels
+            ctx.lib.grim_set_tuning(ctx.h, _lib.TUNE_PIVOT, _lib.PIVOT_PARTIAL)
             status = ctx.lib.grim_zgesv_mixed_factored(ctx.h, n, int(b.shape[0]), None, 0, ptr(entry['z']), n,
                                                        ptr(entry['lu']), ptr(entry['ipiv']), ptr(b), n, self.tol, 10,
                                                        ctypes.byref(st))
+            ctx.lib.grim_set_tuning(ctx.h, _lib.TUNE_PIVOT, _lib.PIVOT_CERTIFIED)
             if status == _lib.GRIM_ERR_NOT_CONVERGED:
                 # stalled refinement: solve this request in FP64 (reference mixed -> double ladder)
                 z64 = ops.fill(body, req.k, req.pol, ctx=ctx)
