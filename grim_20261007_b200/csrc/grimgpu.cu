@@ -765,7 +765,7 @@ static int gepp_rows_target(size_t csize) {
         return e ? atoi(e) : 0;
     }();
     if (env >= 32) return env;
-    return csize == sizeof(double2) ? 128 : 256;
+    return 128;
 }
 
 // Partial-pivoting factorization of the panel (j, nbj) of A on one thread-block cluster.

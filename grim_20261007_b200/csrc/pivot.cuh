@@ -4,17 +4,18 @@
 // The 64-column panel rows j..n-1 are spread over the CS CTAs of one cluster, CTA c holding
 // panel rows [c rpc, (c+1) rpc) in shared memory (rows past its capacity in a global
 // scratch, which stays in L2).  Column step k:
-//   1. every CTA reduces its best candidate for column k among its rows >= k and publishes
-//      the candidate's whole row (and row k, if it owns it) in a double-buffered slot,
-//      with step k - 1's rank-1 update (still pending on columns > k) applied on the fly;
+//   1. every CTA reduces its best candidate for column k among its rows >= k, pushes its
+//      (value, row) into every CTA's shared memory and publishes the candidate's whole row
+//      (and row k, if it owns it) in a double-buffered slot, with step k - 1's rank-1
+//      update (still pending on columns > k) applied on the fly;
 //   2. it arrives at the cluster barrier, finishes that pending update on its own rows
 //      while the other CTAs arrive, and waits;
-//   3. one warp reads the CS candidates through distributed shared memory, then the
-//      winner's row and row k; the owners of rows k and p swap them;
+//   3. one warp finds the winner among the pushed candidates, then reads its row and row
+//      k through distributed shared memory; the owners of rows k and p swap them;
 //   4. one thread per row forms l = a_rk / a_kk, updates column k + 1 at once and finds
 //      the candidates of step k + 1.
-// One cluster barrier per column: a slot is rewritten two steps later, after every CTA
-// has passed the barrier that follows its reads.  Every CTA runs the same steps, barriers
+// One cluster barrier per column: a slot (pushed or published) is rewritten two steps
+// later, after every CTA has passed the barrier that follows its reads.  Every CTA runs the same steps, barriers
 // included, whatever its rows.
 //
 // The panel's interchanges reach the other columns in two ways: the trailing columns take
@@ -159,6 +160,21 @@ k_apply_moves(int n, C *__restrict__ B, int64_t ldb, int col0, int left, const i
     for (int r = row0 + threadIdx.x; r < n; r += blockDim.x) b[r] = col[r - row0];
 }
 
+// A CTA's candidate of one step, pushed into every CTA of the cluster.
+struct GeppCand {
+    double val;
+    int idx;
+    int pad;
+};
+
+// Cluster barrier halves: the arrive of threads whose writes other CTAs read carries release
+// semantics, the others' is relaxed; the wait acquires.
+__device__ __forceinline__ void gepp_arrive(bool release) {
+    if (release) asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
+    else asm volatile("barrier.cluster.arrive.relaxed.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void gepp_wait() { asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory"); }
+
 template <typename C>
 __global__ void __launch_bounds__(GEPP_THREADS)
 k_panel_gepp(int n, C *__restrict__ A, int64_t lda, int j, int nbj, int rpc, int rows_smem, C *__restrict__ gscratch,
@@ -175,7 +191,9 @@ k_panel_gepp(int n, C *__restrict__ A, int64_t lda, int j, int nbj, int rpc, int
     int *ipiv_s = red_i + GEPP_THREADS / 32;
     int *first = ipiv_s + NB, *slot = first + NB, *content = slot + NB, *extra = content + 2 * NB;
     C *rows = reinterpret_cast<C *>(gepp_smem + gepp_fixed_smem<C>());
+    __shared__ GeppCand cand[2][16];  // [parity][rank]: every CTA's candidate, pushed here
     __shared__ int s_p, s_zero;
+    __shared__ C s_rp;
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int m = n - j;
@@ -203,7 +221,8 @@ k_panel_gepp(int n, C *__restrict__ A, int64_t lda, int j, int nbj, int rpc, int
     for (int k = 0; k < nbj; ++k) {
         const int par = k & 1;
         const C *uprev = prow + (par ^ 1) * NB;
-        // 1. the CTA's candidate for column k, published with the pending update applied
+        // 1. the CTA's candidate for column k: warp maxima, then every thread takes the
+        //    largest of the 8 (first row on ties)
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             const double ov = __shfl_down_sync(0xffffffffu, bv, o);
@@ -212,86 +231,72 @@ k_panel_gepp(int n, C *__restrict__ A, int64_t lda, int j, int nbj, int rpc, int
         }
         if (lane == 0) { red_v[warp] = bv; red_i[warp] = bi; }
         __syncthreads();
-        if (warp == 0) {
-            bv = lane < GEPP_THREADS / 32 ? red_v[lane] : -1.0;
-            bi = lane < GEPP_THREADS / 32 ? red_i[lane] : 0x7fffffff;
+        bv = red_v[0];
+        bi = red_i[0];
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) {
-                const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
-                const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-                if (gepp_better(ov, oi, bv, bi)) { bv = ov; bi = oi; }
+        for (int w = 1; w < GEPP_THREADS / 32; ++w)
+            if (gepp_better(red_v[w], red_i[w], bv, bi)) { bv = red_v[w]; bi = red_i[w]; }
+        //    published with the pending update applied: its row (threads 0-63), row k if this
+        //    CTA owns it (64-127); its (value, row) pushed into every CTA (warp 4)
+        if (tid < 2 * NB) {
+            const int c = tid & (NB - 1);
+            const int src = tid < NB ? bi : k;
+            const bool want = tid < NB ? bi != 0x7fffffff : (k >= r0 && k < r0 + nr);
+            if (want) {
+                const C *a = rowp(src - r0);
+                C x = a[c];
+                if (k > 0 && c > k) cfms(x, a[k - 1], uprev[c]);
+                if (tid < NB) pub[par].row[c] = x;
+                else pub[par].krow[c] = x;
             }
-            const bool own_k = k >= r0 && k < r0 + nr;
-            for (int c = lane; c < NB; c += 32) {
-                if (bi != 0x7fffffff) {
-                    const C *a = rowp(bi - r0);
-                    C x = a[c];
-                    if (k > 0 && c > k) cfms(x, a[k - 1], uprev[c]);
-                    pub[par].row[c] = x;
-                }
-                if (own_k) {
-                    const C *a = rowp(k - r0);
-                    C x = a[c];
-                    if (k > 0 && c > k) cfms(x, a[k - 1], uprev[c]);
-                    pub[par].krow[c] = x;
-                }
-            }
-            if (lane == 0) {
-                pub[par].val = bv;
-                pub[par].idx = bi;
-            }
+        } else if (warp == 4 && lane < cs) {
+            GeppCand *dst = cluster.map_shared_rank(&cand[par][rank], lane);
+            dst->val = bv;
+            dst->idx = bi;
         }
         // the published rows are read before any warp applies the pending update to them
         __syncthreads();
-        cluster.barrier_arrive();
-        // 2. the pending update of step k - 1 on the CTA's rows >= k, columns > k: one thread
-        //    per row along its contiguous columns
+        gepp_arrive(warp <= 4);
+        // 2. the pending update of step k - 1 on the CTA's rows >= k, columns > k: two
+        //    threads per row, alternate columns
         if (k > 0) {
-            for (int r = tid; r < nr; r += GEPP_THREADS) {
+            const int half = tid & 1;
+            for (int r = tid >> 1; r < nr; r += GEPP_THREADS / 2) {
                 if (r0 + r >= k) {
                     C *a = rowp(r);
                     const C l = a[k - 1];
-#pragma unroll 8
-                    for (int c = k + 1; c < NB; ++c) cfms(a[c], l, uprev[c]);
+#pragma unroll 4
+                    for (int c = k + 1 + half; c < NB; c += 2) cfms(a[c], l, uprev[c]);
                 }
             }
         }
-        cluster.barrier_wait();
+        gepp_wait();
         __syncthreads();
-        // 3. warp 0: the winner (largest |re| + |im|, first row on ties) from the CS published
-        //    candidates, then its row and row k, two columns per lane; the owners of rows k
-        //    and p swap them
+        // 3. warp 0: the winner from the pushed candidates (local), then its row and row k
+        //    through distributed shared memory; the owners of rows k and p swap them
         if (warp == 0) {
             double v = -1.0;
-            int i = 0x7fffffff, w = 0;
-            if (lane < cs) {
-                const GeppPub<C> *rp = cluster.map_shared_rank(&pub[par], lane);
-                v = rp->val;
-                i = rp->idx;
-                w = lane;
-            }
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) {
-                const double ov = __shfl_xor_sync(0xffffffffu, v, o);
-                const int oi = __shfl_xor_sync(0xffffffffu, i, o);
-                const int ow = __shfl_xor_sync(0xffffffffu, w, o);
-                if (gepp_better(ov, oi, v, i)) { v = ov; i = oi; w = ow; }
+            int i = 0x7fffffff;
+            for (int w = 0; w < cs; ++w) {
+                const GeppCand cw = cand[par][w];
+                if (gepp_better(cw.val, cw.idx, v, i)) { v = cw.val; i = cw.idx; }
             }
             const bool zero = !(v > 0.0);
-            const int ck = k / rpc;
-            const GeppPub<C> *wp = cluster.map_shared_rank(&pub[par], w);
+            const int ck = k / rpc, cw = i == 0x7fffffff ? 0 : i / rpc;
+            const GeppPub<C> *wp = cluster.map_shared_rank(&pub[par], cw);
             const GeppPub<C> *kp = cluster.map_shared_rank(&pub[par], ck);
             const C x0 = wp->row[lane], x1 = wp->row[lane + 32];
             const C k0 = kp->krow[lane], k1 = kp->krow[lane + 32];
             prow[par * NB + lane] = x0;
             prow[par * NB + lane + 32] = x1;
+            if (lane == (k & 31)) s_rp = zero ? one_c<C>() : crecip(k < 32 ? x0 : x1);
             if (i != k && !zero) {
                 if (rank == ck) {
                     C *a = rowp(k - r0);
                     a[lane] = x0;
                     a[lane + 32] = x1;
                 }
-                if (rank == i / rpc) {
+                if (rank == cw) {
                     C *a = rowp(i - r0);
                     a[lane] = k0;
                     a[lane + 32] = k1;
@@ -309,7 +314,7 @@ k_panel_gepp(int n, C *__restrict__ A, int64_t lda, int j, int nbj, int rpc, int
         // 4. multipliers of the CTA's rows below k (LAPACK leaves a zero pivot column
         //    unscaled), column k + 1 updated at once, and the candidates of step k + 1
         const C *u = prow + par * NB;
-        const C rp = zero ? one_c<C>() : crecip(u[k]);
+        const C rp = s_rp;
         bv = -1.0;
         bi = 0x7fffffff;
         for (int r = tid; r < nr; r += GEPP_THREADS) {

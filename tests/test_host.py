@@ -142,3 +142,45 @@ def test_cpu_dense_backend_is_refused_not_run_on_the_gpu(monkeypatch):
         solver.solve_monostatic_rcs_2d_single_polarization(snap, [0.3], [0.0], 'TM', geometry_units='meters')
     monkeypatch.setenv('GHOST_DENSE_BACKEND', 'auto')
     assert require_gpu_dense_backend() == 'auto'
+
+
+def _snap(polys):
+    return S.snapshot_from_polygons(polys)
+
+
+def test_geometry_validation_rejects_what_the_reference_rejects():
+    """The reference's fatal solver-side checks (twod/geometry.py:1121-1457, geometry/io.py:712)
+    restated: the sharp-trailing-edge airfoil at 2048 elements is a crack (its upper and lower
+    vertices next to the tip are 7e-7 m apart), the blunt one is accepted; duplicate,
+    crossing and wrongly wound contours are refused."""
+    t = 0.12458731811250179
+    with pytest.raises(ValueError, match='Geometry crack'):
+        geo.contours_from_snapshot(_snap([S.naca_symmetric(t, 2048, closed_te=True)]), 'meters')
+    polys = geo.contours_from_snapshot(_snap([S.naca_symmetric(t, 2048)]), 'meters')
+    assert len(polys) == 1 and len(polys[0]) == 2048
+    geo.contours_from_snapshot(_snap([S.naca_symmetric(t, 1024, closed_te=True)]), 'meters')  # as the reference
+    with pytest.raises(ValueError, match='orientation'):
+        geo.contours_from_snapshot(_snap([S.circle(1.0, 40)[::-1]]), 'meters')
+    # a body inside a void inside a body: the void runs counter-clockwise
+    geo.contours_from_snapshot(_snap([S.circle(2.0, 60), S.circle(1.0, 40)[::-1], S.circle(0.5, 30)]), 'meters')
+    with pytest.raises(ValueError, match='Duplicate primitive'):
+        geo.contours_from_snapshot(_snap([S.circle(1.0, 40), S.circle(1.0, 40)]), 'meters')
+    bow = np.array([[0.0, 0.0], [1.0, 1.0], [1.0, 0.0], [0.0, 1.0]])
+    with pytest.raises(ValueError, match='intersection'):
+        geo.contours_from_snapshot(_snap([bow]), 'meters')
+    with pytest.raises(ValueError, match='Collinear overlapping'):
+        geo.contours_from_snapshot(_snap([np.array([[0.0, 0.0], [0.0, 1.0], [1.0, 1.0], [1.0, 0.0], [0.5, 0.0],
+                                                     [0.7, 0.0]])]), 'meters')
+    snap = _snap([S.circle(1.0, 40)])
+    snap['segments'][0]['point_pairs'][5]['x2'] += 1e-3
+    with pytest.raises(ValueError, match='disconnected primitive chain'):
+        geo.contours_from_snapshot(snap, 'meters')
+
+
+def test_geometry_validation_is_cheap_on_the_headline_airfoil():
+    import time
+    snap = _snap([S.airfoil_case(0, 2048)[0]])
+    geo.contours_from_snapshot(snap, 'meters')
+    t0 = time.perf_counter()
+    geo.contours_from_snapshot(snap, 'meters')
+    assert time.perf_counter() - t0 < 0.05
