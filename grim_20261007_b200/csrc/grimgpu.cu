@@ -244,7 +244,7 @@ extern "C" int grim_set_tuning(grim_handle_t h, int key, int value) {
         h->tune_solve_bn = value;
         return GRIM_OK;
     }
-    if (key == GRIM_TUNE_GS_BLOCK && (value == 0 || value == 256 || value == 512)) {
+    if (key == GRIM_TUNE_GS_BLOCK && (value == 0 || value == 64 || value == 128 || value == 256 || value == 512)) {
         h->tune_gs_block = value;
         return GRIM_OK;
     }
@@ -768,11 +768,47 @@ static int gepp_rows_target(size_t csize) {
     return 128;
 }
 
+// Register-resident panel rows (k_panel_gepp_reg) for panels of at most 16 x GEPPR_ROWS rows;
+// GRIM_GEPP_REG=0 keeps every panel on the shared-memory kernel.
+static bool gepp_reg_enabled() {
+    static const bool on = [] {
+        const char *e = getenv("GRIM_GEPP_REG");
+        return !(e && atoi(e) == 0);
+    }();
+    return on;
+}
+
 // Partial-pivoting factorization of the panel (j, nbj) of A on one thread-block cluster.
 template <typename C>
 static int gepp_launch(grim_context *h, int n, C *A, int64_t lda, int j, int nbj, int *ipiv, int *d_info,
                        int *swapped, int *moves, PanelPack pk) {
     const int m = n - j;
+    if (gepp_reg_enabled() && m <= 16 * GEPPR_ROWS) {
+        // rows in registers: the fewest CTAs of at most GEPPR_ROWS rows each
+        const int cs = std::max(1, ceil_div(m, GEPPR_ROWS));
+        const int rpc = ceil_div(m, cs);
+        static PerDeviceOnce attr_reg;
+        if (attr_reg.needed()) {
+            GRIM_CHECK_CUDA(
+                cudaFuncSetAttribute(k_panel_gepp_reg<C>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+            attr_reg.mark();
+        }
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(cs);
+        cfg.blockDim = dim3(GEPP_THREADS);
+        cfg.dynamicSmemBytes = 0;
+        cfg.stream = h->stream;
+        cudaLaunchAttribute la[1];
+        la[0].id = cudaLaunchAttributeClusterDimension;
+        la[0].val.clusterDim.x = cs;
+        la[0].val.clusterDim.y = 1;
+        la[0].val.clusterDim.z = 1;
+        cfg.attrs = la;
+        cfg.numAttrs = 1;
+        GRIM_CHECK_CUDA(cudaLaunchKernelEx(&cfg, k_panel_gepp_reg<C>, n, A, lda, j, nbj, rpc, ipiv, d_info, swapped,
+                                           moves, pk));
+        return grim_launch_status(h, kname("k_panel_gepp_reg", sizeof(C)), 8.0 * m * nbj * nbj / 2.0, 0);
+    }
     const int target = gepp_rows_target(sizeof(C));
     int cs = 1;
     while (cs < 16 && ceil_div(m, cs) > target) cs <<= 1;
@@ -1530,7 +1566,10 @@ static int mixed_refine(grim_context *h, int n, int nrhs, const TA *Ares, int64_
     // and accurate for diagonally dominant factors; partial-pivoting factors (the
     // combined-field systems) keep the substitution solve, whose first backward error is
     // two orders of magnitude smaller there (one refinement step saved)
-    const bool use_gs = gs_wanted(n, nrhs) && h->pivot_mode != GRIM_PIVOT_PARTIAL;
+    // the explicit block inverses start the refinement at a larger backward error than
+    // substitution (2e-3 against 3e-5 at N=2048 on the combined-field systems) and still
+    // finish first: one more refinement step costs less than the substitution chain
+    const bool use_gs = gs_wanted(n, nrhs);
     if (use_gs) GRIM_TRY(gs_build(h, n, lu32, n, h->tune_gs_block ? h->tune_gs_block : gs_block(n, nrhs), &panels));
     auto solve32 = [&](float2 *X32) -> int {
         if (use_gs) return gs_apply(h, panels, nrhs, ipiv, ident, X32, n);

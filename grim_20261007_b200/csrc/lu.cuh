@@ -238,11 +238,24 @@ __device__ __forceinline__ void subst_col_upper(C (&v)[16], const C *T, const C 
 
 // Stage the nbj x nbj diagonal block at (j, j) into smem T (padded, zero outside) and
 // the reciprocals of its diagonal into rd (1 outside).
+// Sixteen loads per thread are in flight before their stores: a 64-thread CTA stages the
+// block in four round trips to memory instead of sixty-four.
 template <typename C>
 __device__ __forceinline__ void stage_diag(const C *A, int64_t lda, int j, int nbj, C *T, C *rd) {
-    for (int e = threadIdx.x; e < NB * NB; e += blockDim.x) {
-        const int r = e & 63, c = e >> 6;
-        T[c * NBP + r] = (r < nbj && c < nbj) ? A[(int64_t)(j + c) * lda + j + r] : czero<C>();
+    constexpr int U = 16;
+    for (int e0 = threadIdx.x; e0 < NB * NB; e0 += U * blockDim.x) {
+        C x[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int e = e0 + u * (int)blockDim.x;
+            const int r = e & 63, c = e >> 6;
+            x[u] = (e < NB * NB && r < nbj && c < nbj) ? A[(int64_t)(j + c) * lda + j + r] : czero<C>();
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int e = e0 + u * (int)blockDim.x;
+            if (e < NB * NB) T[(e >> 6) * NBP + (e & 63)] = x[u];
+        }
     }
     __syncthreads();
     for (int r = threadIdx.x; r < NB; r += blockDim.x) rd[r] = r < nbj ? crecip(T[r * NBP + r]) : one_c<C>();

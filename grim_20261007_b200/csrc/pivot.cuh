@@ -378,6 +378,312 @@ k_panel_gepp(int n, C *__restrict__ A, int64_t lda, int j, int nbj, int rpc, int
     }
 }
 
+// ------------------------------------------------------------ register-resident panel rows
+// The same column steps with every panel row in registers: two threads per row, the thread
+// of parity h holding columns h, h + 2, ..., h + 62.  The rank-1 updates then run from
+// registers and only pivot rows pass through shared memory.  Each CTA holds at most
+// GEPPR_ROWS rows, so the kernel takes panels of at most 16 x GEPPR_ROWS rows.  The
+// column steps are instantiated one by one (gepp_reg_step<K>), so every register index is a
+// compile-time constant.
+//
+// Candidates are compared as integer keys: the bits of |re| + |im| (a non-negative double)
+// plus one order like the values, 0 marks "no candidate" (and NaN, which LAPACK's search
+// never picks either).  Rows rise with the lane, the warp and the CTA, so the lowest holder
+// of the maximum key is LAPACK's first row on ties.  Per step, a CTA publishes its best
+// row and row k as they are in registers, with the row's multiplier of the previous step;
+// the CTAs that read a row apply that pending update to the columns they take.  The
+// candidate is pushed with its element in column k, so the winner's reciprocal is formed
+// while its row is in flight, and every CTA but the owner of row k fetches only the
+// columns right of k.
+#define GEPPR_ROWS (GEPP_THREADS / 2)
+
+template <typename C>
+struct GeppPushed {
+    C piv;                   // the candidate's element in column k
+    unsigned long long key;  // its key (0: the CTA has no row >= k)
+    int idx;                 // its panel row
+    int pad;
+};
+
+template <typename C>
+struct GeppRegShared {
+    C row[2][NB];   // [parity]: the CTA's best candidate row, as in registers
+    C krow[2][NB];  // [parity]: panel row k, from the CTA that owns it
+    C row_l[2];     // [parity]: their multipliers of the previous step
+    C krow_l[2];
+    C u[2][NB];     // [parity]: the pivot row of the step (local copy, columns > k)
+    C kin[NB];      // row k, in the CTA that owns the winner row
+    GeppPushed<C> cand[2][16];  // [parity][rank]: every CTA's candidate, pushed here
+    unsigned long long red_k[GEPP_THREADS / 32];
+    int red_l[GEPP_THREADS / 32];
+    int ipiv[NB], first[NB], slot[NB], content[2 * NB], extra[NB];
+    int p, zero;
+    C rp;
+};
+
+template <typename C>
+struct GeppRegThread {
+    C a[NB / 2];             // a[q]: column 2 q + half of the thread's row
+    C lp;                    // the row's multiplier of the previous step
+    unsigned long long key;  // candidate key for the current column (thread holding it)
+};
+
+struct GeppRegCtx {
+    int tid, lane, warp, half, pr, r0, rank, cs, rpc, nbj, j;
+    bool valid;
+    int *info;
+};
+
+__device__ __forceinline__ unsigned long long gepp_key(double v) {
+    return v == v ? (unsigned long long)__double_as_longlong(v) + 1ull : 0ull;
+}
+
+// Warp maximum of the keys (every lane) and the lowest lane that holds it (-1: all zero).
+__device__ __forceinline__ int gepp_warp_argmax(unsigned long long key, unsigned long long &kmax) {
+    const unsigned hi = (unsigned)(key >> 32), lo = (unsigned)key;
+    const unsigned mhi = __reduce_max_sync(0xffffffffu, hi);
+    const unsigned mlo = __reduce_max_sync(0xffffffffu, hi == mhi ? lo : 0u);
+    kmax = ((unsigned long long)mhi << 32) | mlo;
+    const unsigned bal = __ballot_sync(0xffffffffu, kmax != 0ull && key == kmax);
+    return bal ? __ffs(bal) - 1 : -1;
+}
+
+template <typename C, int K>
+__device__ __forceinline__ void gepp_reg_step(GeppRegThread<C> &st, GeppRegShared<C> &sh, const GeppRegCtx &cx) {
+    if (K >= cx.nbj) return;
+    cg::cluster_group cluster = cg::this_cluster();
+    constexpr int par = K & 1, hk = K & 1, qk = K >> 1;
+    const C *uprev = sh.u[par ^ 1];
+
+    // 1. the CTA's candidate for column K: the first warp holding the maximum key
+    unsigned long long wmax;
+    const int wl = gepp_warp_argmax(st.key, wmax);
+    if (cx.lane == 0) {
+        sh.red_k[cx.warp] = wmax;
+        sh.red_l[cx.warp] = wl;
+    }
+    __syncthreads();
+    unsigned long long cmax = sh.red_k[0];
+    int cwarp = 0;
+#pragma unroll
+    for (int w = 1; w < GEPP_THREADS / 32; ++w)
+        if (sh.red_k[w] > cmax) {
+            cmax = sh.red_k[w];
+            cwarp = w;
+        }
+    const int owner = cmax ? cwarp * 32 + sh.red_l[cwarp] : 0;  // thread holding the element
+    const int bi = cmax ? cx.r0 + (owner >> 1) : 0x7fffffff;
+    //    its row and row K published as they are, with their pending multipliers
+    const bool own_best = cx.valid && cx.pr == bi;
+    const bool own_k = cx.valid && cx.pr == K;
+    if (own_best || own_k) {
+#pragma unroll
+        for (int q = 0; q < NB / 2; ++q) {
+            const int c = 2 * q + cx.half;
+            if (own_best) sh.row[par][c] = st.a[q];
+            if (own_k) sh.krow[par][c] = st.a[q];
+        }
+        if (cx.half == 0) {
+            if (own_best) sh.row_l[par] = st.lp;
+            if (own_k) sh.krow_l[par] = st.lp;
+        }
+    }
+    //    (key, row, element) pushed into every CTA by the lanes of the owner's warp
+    const int pw = owner >> 5;
+    if (cx.warp == pw) {
+        const C piv = shfl_c(st.a[qk], owner & 31);
+        if (cx.lane < cx.cs) {
+            GeppPushed<C> pc;
+            pc.piv = piv;
+            pc.key = cmax;
+            pc.idx = bi;
+            pc.pad = 0;
+            *cluster.map_shared_rank(&sh.cand[par][cx.rank], cx.lane) = pc;
+        }
+    }
+    const int kw = (K >= cx.r0 && K < cx.r0 + cx.rpc) ? (2 * (K - cx.r0)) >> 5 : -1;
+    __syncwarp();
+    gepp_arrive(cx.warp == pw || cx.warp == kw);
+
+    // 2. the pending update of step K - 1 on the thread's row (rows >= K, columns > K)
+    if (K > 0 && cx.valid && cx.pr >= K) {
+#pragma unroll
+        for (int q = 0; q < NB / 2; ++q) {
+            const int c = 2 * q + cx.half;
+            if (c > K) cfms(st.a[q], st.lp, uprev[c]);
+        }
+    }
+    __syncwarp();
+    gepp_wait();
+
+    // 3. warp 0: the winner among the pushed candidates (the first CTA holding the maximum),
+    //    its columns > K (all of them in the CTA that owns row K), and row K in the CTA that
+    //    owns the winner, through distributed shared memory
+    if (cx.warp == 0) {
+        unsigned long long gmax;
+        const int wlane = gepp_warp_argmax(cx.lane < cx.cs ? sh.cand[par][cx.lane].key : 0ull, gmax);
+        const bool zero = gmax <= 1ull;  // every candidate 0 (or none finite): no interchange
+        const int i = wlane >= 0 ? sh.cand[par][wlane].idx : K;
+        const int ck = K / cx.rpc, cw = i / cx.rpc;
+        const bool in_ck = cx.rank == ck;
+        const C *wrow = wlane >= 0 ? cluster.map_shared_rank(&sh.row[par][0], cw)
+                                   : cluster.map_shared_rank(&sh.krow[par][0], ck);
+        const C *wlp = wlane >= 0 ? cluster.map_shared_rank(&sh.row_l[par], cw)
+                                  : cluster.map_shared_rank(&sh.krow_l[par], ck);
+        const int c0 = cx.lane, c1 = cx.lane + 32;
+        C x0 = czero<C>(), x1 = czero<C>();
+        if (in_ck || c0 > K) x0 = wrow[c0];
+        if (in_ck || c1 > K) x1 = wrow[c1];
+        const bool need_k = cx.rank == cw && i != K && !zero;
+        C k0 = czero<C>(), k1 = czero<C>(), kl = czero<C>();
+        if (need_k) {
+            const C *kr = cluster.map_shared_rank(&sh.krow[par][0], ck);
+            k0 = kr[c0];
+            k1 = kr[c1];
+            kl = *cluster.map_shared_rank(&sh.krow_l[par], ck);
+        }
+        if (cx.lane == 0) {
+            sh.rp = zero ? one_c<C>() : crecip(sh.cand[par][wlane].piv);
+            sh.p = i;
+            sh.zero = zero;
+            if (cx.rank == 0) sh.ipiv[K] = zero ? K : i;
+        }
+        if (K > 0) {
+            const C wl_ = *wlp;
+            if (c0 > K) cfms(x0, wl_, uprev[c0]);
+            if (c1 > K) cfms(x1, wl_, uprev[c1]);
+            if (need_k) {
+                if (c0 > K) cfms(k0, kl, uprev[c0]);
+                if (c1 > K) cfms(k1, kl, uprev[c1]);
+            }
+        }
+        sh.u[par][c0] = x0;
+        sh.u[par][c1] = x1;
+        if (need_k) {
+            sh.kin[c0] = k0;
+            sh.kin[c1] = k1;
+        }
+    }
+    __syncthreads();
+
+    // 4. rows K and p swap; multipliers of the rows below K (LAPACK leaves a zero pivot
+    //    column unscaled), column K + 1 updated at once, and the candidates of step K + 1
+    const bool zero = sh.zero;
+    const int p = sh.p;
+    const C *u = sh.u[par];
+    if (zero && cx.rank == 0 && cx.tid == 0) atomicCAS(cx.info, 0, cx.j + K + 1);
+    if (!zero && p != K && cx.valid) {
+        if (cx.pr == K) {
+#pragma unroll
+            for (int q = 0; q < NB / 2; ++q) st.a[q] = u[2 * q + cx.half];
+        } else if (cx.pr == p) {
+#pragma unroll
+            for (int q = 0; q < NB / 2; ++q) st.a[q] = sh.kin[2 * q + cx.half];
+        }
+    }
+    const bool below = cx.valid && cx.pr > K;
+    C l = czero<C>();
+    if (cx.half == hk) l = zero ? st.a[qk] : cmul(st.a[qk], sh.rp);
+    const C lo = shfl_xor_c(l, 1);
+    if (cx.half != hk) l = lo;
+    if (below && cx.half == hk) st.a[qk] = l;
+    st.lp = l;
+    st.key = 0ull;
+    if constexpr (K + 1 < NB) {
+        constexpr int hk1 = (K + 1) & 1, qk1 = (K + 1) >> 1;
+        if (below && cx.half == hk1) {
+            cfms(st.a[qk1], l, u[K + 1]);
+            st.key = gepp_key((double)cabs1(st.a[qk1]));
+        }
+        gepp_reg_step<C, K + 1>(st, sh, cx);
+    }
+}
+
+template <typename C>
+__global__ void __launch_bounds__(GEPP_THREADS, 1)
+k_panel_gepp_reg(int n, C *__restrict__ A, int64_t lda, int j, int nbj, int rpc, int *__restrict__ ipiv,
+                 int *__restrict__ info, int *__restrict__ swapped, int *__restrict__ moves, PanelPack pk) {
+    cg::cluster_group cluster = cg::this_cluster();
+    __shared__ GeppRegShared<C> sh;
+    GeppRegCtx cx;
+    cx.tid = threadIdx.x;
+    cx.lane = cx.tid & 31;
+    cx.warp = cx.tid >> 5;
+    cx.half = cx.tid & 1;
+    cx.rank = (int)cluster.block_rank();
+    cx.cs = (int)cluster.num_blocks();
+    cx.rpc = rpc;
+    cx.nbj = nbj;
+    cx.j = j;
+    cx.info = info;
+    const int m = n - j;
+    const int r0 = cx.rank * rpc, r = cx.tid >> 1;
+    cx.pr = r0 + r;
+    cx.r0 = r0;
+    cx.valid = r < rpc && cx.pr < m;
+
+    GeppRegThread<C> st;
+#pragma unroll
+    for (int q = 0; q < NB / 2; ++q) {
+        const int c = 2 * q + cx.half;
+        st.a[q] = (cx.valid && c < nbj) ? A[(int64_t)(j + c) * lda + j + cx.pr] : czero<C>();
+    }
+    st.lp = czero<C>();
+    st.key = (cx.valid && cx.half == 0) ? gepp_key((double)cabs1(st.a[0])) : 0ull;
+    gepp_reg_step<C, 0>(st, sh, cx);
+    // every CTA has finished reading every other CTA's slots before any CTA exits
+    cluster.sync();
+
+    // the factored rows back; complex64: the trailing update's packed A operand (L21)
+    if (cx.valid) {
+#pragma unroll
+        for (int q = 0; q < NB / 2; ++q) {
+            const int c = 2 * q + cx.half;
+            if (c < nbj) A[(int64_t)(j + c) * lda + j + cx.pr] = st.a[q];
+        }
+    }
+    if constexpr (sizeof(C) == sizeof(float2)) {
+        if (pk.a_hi) {
+            // L21 rows are panel rows >= nbj (= NB here); padding rows up to a_rows / 2 are zero
+            const int rest = m - nbj;
+            const int pad_rows = pk.a_rows / 2;
+            const int mrow = cx.pr - nbj;
+            if (r < rpc && mrow >= 0 && mrow < pad_rows) {
+                const bool live = mrow < rest;
+#pragma unroll
+                for (int q = 0; q < NB / 2; ++q) {
+                    const int c = 2 * q + cx.half;
+                    float xr = 0.f, xi = 0.f;
+                    if (live) {
+                        const float2 x = *reinterpret_cast<const float2 *>(&st.a[q]);
+                        xr = x.x;
+                        xi = x.y;
+                    }
+                    pack_pair(pk.a_hi, pk.a_lo, tc_tile_offset(2 * mrow, 2 * c, pk.a_rows), xr, -xi);
+                    pack_pair(pk.a_hi, pk.a_lo, tc_tile_offset(2 * mrow + 1, 2 * c, pk.a_rows), xi, xr);
+                }
+            }
+            // rows past the rows of every CTA (rpc * CS may not reach pad_rows): zero
+            const int covered = cx.cs * rpc - nbj;
+            if (cx.rank == 0)
+                for (int e = cx.tid; e < (pad_rows - covered) * NB; e += GEPP_THREADS) {
+                    const int mr = covered + e / NB, cc = e % NB;
+                    if (mr < 0) continue;
+                    pack_pair(pk.a_hi, pk.a_lo, tc_tile_offset(2 * mr, 2 * cc, pk.a_rows), 0.f, 0.f);
+                    pack_pair(pk.a_hi, pk.a_lo, tc_tile_offset(2 * mr + 1, 2 * cc, pk.a_rows), 0.f, 0.f);
+                }
+        }
+    }
+
+    // CTA 0: ipiv, the swapped flag and the row moves of the panel's interchanges
+    if (cx.rank != 0) return;
+    if (cx.tid < nbj) ipiv[j + cx.tid] = j + sh.ipiv[cx.tid] + 1;
+    if (cx.warp == 0) {
+        const int cnt = panel_moves(sh.ipiv, nbj, j, moves, sh.first, sh.slot, sh.content, sh.extra);
+        if (cx.lane == 0) *swapped = cnt > 0;
+    }
+}
+
 // U12 = inv(L11) A12 of the trailing columns after the panel's row moves: one CTA per 64
 // columns, 4 threads per column.  Each column gathers every move's source before writing
 // any destination.  complex64: also writes the trailing update's packed B operand.

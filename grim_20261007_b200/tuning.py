@@ -2,10 +2,11 @@
 
 Two shapes of the packed-panel triangular solves are tunable per handle
 (``grim_set_tuning``): the output-tile width of their tensor-core GEMMs (64 or 128
-right-hand-side columns per CTA) and the row block of the packed panels (256 or 512).
-Which pair is fastest depends on N, the number of right-hand sides and the GPU, so the
-tuner times a complete mixed solve of a seeded airfoil system of the requested size for
-every pair and keeps the fastest, per (device, N bucket, right-hand-side bucket), in a
+right-hand-side columns per CTA) and the row block of the packed panels (128, 256 or
+512).  Which pair is fastest depends on N, the number of right-hand sides and the GPU, so
+the tuner times a complete mixed solve (partial pivoting, refinement to the backward-error
+target) of the seeded airfoil's linear-Galerkin TM system of the requested size for every
+pair and keeps the fastest, per (device, N bucket, right-hand-side bucket), in a
 JSON cache (``GRIM_TUNING_CACHE``, default ``~/.cache/grim_20261007_b200/tuning.json``).
 ``apply`` sets a handle from the cache before a solve; without an entry the library's
 built-in rule applies.  With ``GRIM_AUTOTUNE=1`` a missing entry is tuned on first use.
@@ -19,7 +20,7 @@ import threading
 
 from . import _lib
 
-CANDIDATES = {'solve_bn': (64, 128), 'gs_block': (256, 512)}
+CANDIDATES = {'solve_bn': (64, 128), 'gs_block': (128, 256, 512)}
 _lock = threading.Lock()
 _table = None
 
@@ -97,11 +98,12 @@ def tune_dense(n, nrhs, ctx=None, reps=2, seed=0):
 
     from . import synthetic as S
     from .device import context
-    from .twod import geometry as geo, operators as ops
+    from .twod import operators as ops
+    from .twod.galerkin import GalerkinBody
     ctx = ctx or context()
     n = int(n) + (int(n) & 1)
     v, k, _f, _t = S.airfoil_case(seed, n)
-    body = ops.DeviceBody(geo.panel_geometry([v]), None)
+    body = GalerkinBody([v], ctx=ctx)
     ang = torch.as_tensor(np.arange(int(nrhs)) * (360.0 / int(nrhs)), device='cuda')
     z32 = ops.fill(body, k, 'TM', complex64=True, ctx=ctx)
     b0 = ops.rhs(body, k, 'TM', ang, ctx=ctx)
@@ -114,7 +116,7 @@ def tune_dense(n, nrhs, ctx=None, reps=2, seed=0):
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record()
             ops.solve_inplace(None, b, 'mixed', tol=ops.MIXED_RCS_TOL, z32=z32, ctx=ctx, stop='berr',
-                              tuned=False)
+                              tuned=False, pivot=body.pivot)
             e1.record()
             torch.cuda.synchronize()
             if r:  # the first run allocates the workspaces

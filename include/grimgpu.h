@@ -369,8 +369,8 @@ int grim_mem_info(grim_handle_t h, size_t *free_bytes, size_t *total_bytes);
 
 /* Tile-shape overrides chosen by the autotuner (grim_20261007_b200.tuning), per handle;
  * value 0 restores the built-in rule.  GRIM_TUNE_SOLVE_BN: output-tile width (64 or 128)
- * of the tensor-core GEMMs of the packed-panel solve; GRIM_TUNE_GS_BLOCK: row block (256
- * or 512) of the packed-panel solve; GRIM_TUNE_PIVOT: the pivot mode (GRIM_PIVOT_*) of
+ * of the tensor-core GEMMs of the packed-panel solve; GRIM_TUNE_GS_BLOCK: row block (64,
+ * 128, 256 or 512) of the packed-panel solve; GRIM_TUNE_PIVOT: the pivot mode (GRIM_PIVOT_*) of
  * later factorizations on the handle (grim_getrf_grouped takes CERTIFIED or STATIC).  No
  * counterpart in the reference (its BLAS picks its own blocking and always pivots). */
 #define GRIM_TUNE_SOLVE_BN 1

@@ -55,10 +55,12 @@ def _getrf(ctx, a, complex64=False, pivot=0):
     return t, ipiv, info.value
 
 
-@pytest.mark.parametrize('n', [1, 7, 64, 97, 200, 333, 1100, 3500])
+@pytest.mark.parametrize('n', [1, 7, 64, 97, 200, 333, 1100, 2048, 2100, 3500])
 def test_partial_pivoting_getrf_matches_lapack(ctx, n):
     """Partial pivoting on a thread-block cluster: LAPACK's pivots and factors, for cluster
-    sizes 1 to 16 and (n = 3500, complex128) panel rows past a CTA's shared memory."""
+    sizes 1 to 16, panels of up to 16 x 128 rows in registers (n = 2048 fills all 16 CTAs)
+    and taller panels in shared memory (n = 2100, 3500; 3500 also past a CTA's shared
+    memory)."""
     from grim_20261007_b200 import _lib
     a = _rand(n, n, 300 + n)
     t, ipiv, info = _getrf(ctx, a, pivot=_lib.PIVOT_PARTIAL)
@@ -67,6 +69,32 @@ def test_partial_pivoting_getrf_matches_lapack(ctx, n):
     np.testing.assert_array_equal(ipiv.cpu().numpy(), piv_ref + 1)
     lu = _host(t)
     assert np.max(np.abs(lu - lu_ref)) <= 1e-10 * max(1.0, np.max(np.abs(lu_ref)))
+
+
+def _lapack_perm(ipiv):
+    """Row order of LAPACK's sequential interchanges (1-based ipiv)."""
+    perm = np.arange(len(ipiv))
+    for i, p in enumerate(ipiv - 1):
+        perm[[i, p]] = perm[[p, i]]
+    return perm
+
+
+def test_partial_pivoting_cgetrf_large_is_a_partial_pivoting_lu(ctx):
+    """complex64 at n = 2048 (16 CTAs of 128 register-resident rows): LAPACK's FP32 blocked
+    order rounds differently, so near-ties may pick other rows; the factors must still be a
+    partial-pivoting LU of A: P A = L U to FP32 accuracy, and no multiplier larger than the
+    pivot search allows (|re| + |im| of the pivot is the column's largest, so |l| <= sqrt 2)."""
+    from grim_20261007_b200 import _lib
+    n = 2048
+    a = _rand(n, n, 4242).astype(np.complex64)
+    t, ipiv, info = _getrf(ctx, a, complex64=True, pivot=_lib.PIVOT_PARTIAL)
+    assert info == 0
+    lu = _host(t).astype(np.complex128)
+    low = np.tril(lu, -1) + np.eye(n)
+    up = np.triu(lu)
+    assert np.max(np.abs(low)) <= np.sqrt(2.0) * (1.0 + 1e-5)
+    pa = a.astype(np.complex128)[_lapack_perm(ipiv.cpu().numpy())]
+    assert np.max(np.abs(pa - low @ up)) <= 1e-4 * np.max(np.abs(a))
 
 
 @pytest.mark.parametrize('n', [160, 700])
