@@ -149,10 +149,11 @@ def test_concurrent_channels_match_single_channel_solves(ctx):
 
 @pytest.mark.parametrize('grouped', ['1', '0'])
 def test_frequency_sweep_pool_matches_single_frequency_solves(ctx, grouped, monkeypatch):
-    """A multi-frequency request factors its systems with one grouped LU (GRIM_GROUPED_SWEEP=1,
-    the default) or each on the device worker pool (0); either way every frequency's samples
-    equal a one-frequency solve, in request order."""
+    """Pulse-basis systems: a multi-frequency request factors them with one grouped LU
+    (GRIM_GROUPED_SWEEP=1, the default) or each on the device worker pool (0); either way every
+    frequency's samples equal a one-frequency solve, in request order."""
     monkeypatch.setenv('GRIM_GROUPED_SWEEP', grouped)
+    monkeypatch.setenv('GRIM_2D_FORMULATION', 'pulse')
     from grim_20261007_b200.execution import linear_precision
     from grim_20261007_b200.twod.solver import solve_monostatic_rcs_2d_single_polarization as solve1
     v = S.naca_symmetric(0.1, 160)
@@ -175,10 +176,38 @@ def test_frequency_sweep_pool_matches_single_frequency_solves(ctx, grouped, monk
     assert counts['dense_grouped_factorization_count'] == (len(freqs) if grouped == '1' else 0)
 
 
-def test_certified_entry_publishes_the_refined_mesh(ctx):
-    """The certified production entry solves the base and refined meshes of both channels in
-    one grouped factorization and publishes the refined result: equal to a plain solve of the
+def test_galerkin_frequency_sweep_matches_single_frequency_solves(ctx, monkeypatch):
+    """Linear-Galerkin systems (the default formulation) pivot throughout, so a multi-frequency
+    request solves each on the device worker pool, never grouped; every frequency's samples
+    equal a one-frequency solve, in request order."""
+    monkeypatch.delenv('GRIM_2D_FORMULATION', raising=False)
+    from grim_20261007_b200.execution import linear_precision
+    from grim_20261007_b200.twod.solver import solve_monostatic_rcs_2d_single_polarization as solve1
+    v = S.naca_symmetric(0.1, 160)
+    snap = S.snapshot_from_polygons([v])
+    for sg in snap['segments']:
+        sg['properties'][1] = '-10'
+    freqs = [0.9, 2.4, 1.7]
+    ang = list(np.arange(0.0, 180.0, 3.0))
+    with linear_precision('mixed'):
+        swept = solve1(snap, freqs, ang, 'TE', geometry_units='meters', strict_quality_gate=False)
+        for i, f in enumerate(freqs):
+            one = solve1(snap, [f], ang, 'TE', geometry_units='meters', strict_quality_gate=False)
+            a1 = np.array([complex(s['rcs_amp_real'], s['rcs_amp_imag']) for s in one['samples']])
+            block = swept['samples'][i * len(ang):(i + 1) * len(ang)]
+            a2 = np.array([complex(s['rcs_amp_real'], s['rcs_amp_imag']) for s in block])
+            np.testing.assert_allclose(a2, a1, rtol=1e-13, atol=1e-13 * np.max(np.abs(a1)))
+    assert swept['metadata']['dense_grouped_factorization_count'] == 0
+    assert swept['metadata']['dense_gpu_solve_count'] == len(freqs)
+
+
+@pytest.mark.parametrize('formulation', ['pulse', 'galerkin'])
+def test_certified_entry_publishes_the_refined_mesh(ctx, formulation, monkeypatch):
+    """The certified production entry solves the base and refined meshes of both channels --
+    pulse systems in one grouped factorization, linear-Galerkin ones (partial pivoting) each
+    on the worker pool -- and publishes the refined result: equal to a plain solve of the
     refined snapshot, with the reference-shaped certificate; limits it cannot meet raise."""
+    monkeypatch.setenv('GRIM_2D_FORMULATION', formulation)
     from grim_20261007_b200.twod import certify
     from grim_20261007_b200.twod.solver import solve_monostatic_rcs_2d, solve_monostatic_rcs_2d_certified
     th = -2.0 * np.pi * np.arange(200) / 200.0
@@ -200,7 +229,7 @@ def test_certified_entry_publishes_the_refined_mesh(ctx):
         gates = meta['mesh_convergence']
         assert len(gates) == 2 and all(gt['passed'] for gt in gates)
         assert all(gt['fine_panel_count'] > gt['base_panel_count'] for gt in gates)
-        assert meta['dense_grouped_factorization_count'] == 2
+        assert meta['dense_grouped_factorization_count'] == (2 if formulation == 'pulse' else 0)
     with pytest.raises(ValueError, match='mesh convergence failed'):
         solve_monostatic_rcs_2d_certified(snap, [0.55], ang, geometry_units='meters',
                                           mesh_convergence_policy={'complex_max_limit': 1e-9})

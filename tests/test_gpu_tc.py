@@ -170,7 +170,8 @@ def test_autotuner_times_every_candidate_and_keeps_results(tmp_path, monkeypatch
     monkeypatch.setattr(tuning, '_table', None)
     ctx = context()
     entry = tuning.tune_dense(640, 200, ctx=ctx, reps=1)
-    assert len(entry['timings_ms']) == 4 and entry['choice']['solve_bn'] in (64, 128)
+    ncand = len(tuning.CANDIDATES['solve_bn']) * len(tuning.CANDIDATES['gs_block'])
+    assert len(entry['timings_ms']) == ncand and entry['choice']['solve_bn'] in (64, 128)
     assert tuning.lookup(ctx.device_name, 640, 200)['choice'] == entry['choice']
     v, k, _f, _t = S.airfoil_case(0, 640)
     body = ops.DeviceBody(geo.panel_geometry([v]), None)
