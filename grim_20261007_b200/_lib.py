@@ -93,6 +93,7 @@ SIGNATURES = [
                                  c_int, c_double, c_int, P_int, ctypes.POINTER(GrimSolveInfo)]),
     ('grim_zgesv_guarded', c_int, [c_void_p, c_int, c_int, c_void_p, c_int64, c_void_p, c_int64, c_int, c_double,
                                    c_int, c_void_p, P_int, ctypes.POINTER(GrimSolveInfo)]),
+    ('grim_zcond1_equilibrated', c_int, [c_void_p, c_int, c_void_p, c_int64, ctypes.POINTER(c_double)]),
     ('grim_zgesv_mixed_factored', c_int, [c_void_p, c_int, c_int, c_void_p, c_int64, c_void_p, c_int64, c_void_p,
                                           c_void_p, c_void_p, c_int64, c_double, c_int, ctypes.POINTER(GrimSolveInfo)]),
     ('grim_zgesv_refine_factored', c_int, [c_void_p, c_int, c_int, c_void_p, c_int64, c_void_p, c_int64, c_void_p,

@@ -24,6 +24,7 @@
 #include "farblock.cuh"
 #include "galerkin.cuh"
 #include "pivot.cuh"
+#include "condest.cuh"
 
 // ============================================================== errors
 static thread_local std::string g_last_error;
@@ -1872,6 +1873,136 @@ extern "C" int grim_zgesv_mixed_factored(grim_handle_t h, int n, int nrhs, const
     h->last = st;
     if (stats) *stats = st;
     return s;
+}
+
+// ============================================================== condition estimate
+// cond_1 of the row/column-equilibrated matrix (the reference's condition_est; kernels and
+// the estimator's description in condest.cuh).  B^-1 v = C A^-1 R v and B^-H v = R A^-H C v
+// run on partial-pivoting LUs of A and of A^H; the iteration is LAPACK zlacn2's.
+extern "C" int grim_zcond1_equilibrated(grim_handle_t h, int n, const void *A, int64_t lda, double *cond) {
+    if (!h || n <= 0 || !A || lda < n || !cond) return grim_fail(GRIM_ERR_ARGUMENT, "grim_zcond1_equilibrated: bad arguments");
+    DeviceGuard g(h->device);
+    struct PivotScope {
+        grim_context *h;
+        int keep;
+        explicit PivotScope(grim_context *hh) : h(hh), keep(hh->pivot_mode) { h->pivot_mode = GRIM_PIVOT_PARTIAL; }
+        ~PivotScope() { h->pivot_mode = keep; }
+    } scope(h);
+    void *plu = nullptr, *pluh = nullptr, *pip = nullptr, *pr = nullptr, *pc = nullptr, *pv = nullptr, *ps = nullptr;
+    GRIM_TRY(grim_workspace(h, "cond_lu", (size_t)n * n * sizeof(double2), &plu));
+    GRIM_TRY(grim_workspace(h, "cond_luh", (size_t)n * n * sizeof(double2), &pluh));
+    GRIM_TRY(grim_workspace(h, "cond_ipiv", (size_t)2 * n * sizeof(int), &pip));
+    GRIM_TRY(grim_workspace(h, "cond_rmax", (size_t)n * sizeof(unsigned long long), &pr));
+    GRIM_TRY(grim_workspace(h, "cond_cols", (size_t)2 * n * sizeof(double), &pc));
+    GRIM_TRY(grim_workspace(h, "cond_vec", (size_t)2 * n * sizeof(double2), &pv));
+    GRIM_TRY(grim_workspace(h, "cond_scal", 64, &ps));
+    double2 *lu = (double2 *)plu, *luh = (double2 *)pluh, *x = (double2 *)pv;
+    int *ipiv = (int *)pip, *ipivh = ipiv + n;
+    unsigned long long *rmax = (unsigned long long *)pr;
+    double *cscale = (double *)pc, *colsum = cscale + n;
+    double *sd = (double *)ps;
+    int *si = (int *)(sd + 4);
+    const double2 *a = (const double2 *)A;
+
+    // equilibration and ||B||_1
+    GRIM_CHECK_CUDA(cudaMemsetAsync(rmax, 0, (size_t)n * sizeof(unsigned long long), h->stream));
+    const int chunk = 64;
+    k_cond_rowmax<<<dim3(ceil_div(n, 256), ceil_div(n, chunk)), 256, 0, h->stream>>>(n, a, lda, chunk, rmax);
+    GRIM_CHECK_LAUNCH(h, "k_cond_rowmax");
+    k_cond_cols<<<n, 256, 0, h->stream>>>(n, a, lda, rmax, cscale, colsum);
+    GRIM_CHECK_LAUNCH(h, "k_cond_cols");
+    k_cond_max<<<1, 1024, 0, h->stream>>>(n, colsum, sd);
+    GRIM_CHECK_LAUNCH(h, "k_cond_max");
+
+    // LUs of A and A^H
+    GRIM_CHECK_CUDA(cudaMemcpy2DAsync(lu, n * sizeof(double2), a, lda * sizeof(double2), n * sizeof(double2), n,
+                                      cudaMemcpyDeviceToDevice, h->stream));
+    int info = 0, infoh = 0;
+    GRIM_TRY(getrf_impl<double2>(h, n, lu, n, ipiv, &info));
+    k_conj_transpose<<<dim3(ceil_div(n, 32), ceil_div(n, 32)), dim3(32, 8), 0, h->stream>>>(n, a, lda, luh, n);
+    GRIM_CHECK_LAUNCH(h, "k_conj_transpose");
+    GRIM_TRY(getrf_impl<double2>(h, n, luh, n, ipivh, &infoh));
+    double norm_b = 0.0;
+    GRIM_CHECK_CUDA(cudaMemcpyAsync(&norm_b, sd, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    GRIM_CHECK_CUDA(cudaStreamSynchronize(h->stream));
+    if (info > 0 || infoh > 0 || !std::isfinite(norm_b)) {
+        *cond = INFINITY;  // exactly singular (or non-finite entries)
+        return GRIM_OK;
+    }
+
+    const int vb = ceil_div(n, 256);
+    auto binv = [&](bool adjoint) -> int {  // x <- B^-1 x or B^-H x
+        k_cond_scale<<<vb, 256, 0, h->stream>>>(n, x, adjoint ? cscale : nullptr, adjoint ? nullptr : rmax);
+        GRIM_CHECK_LAUNCH(h, "k_cond_scale");
+        GRIM_TRY(getrs_impl<double2>(h, n, 1, adjoint ? luh : lu, n, adjoint ? ipivh : ipiv, x, n));
+        k_cond_scale<<<vb, 256, 0, h->stream>>>(n, x, adjoint ? nullptr : cscale, adjoint ? rmax : nullptr);
+        GRIM_CHECK_LAUNCH(h, "k_cond_scale");
+        return GRIM_OK;
+    };
+    auto fill = [&](int mode, int j) {
+        k_cond_fill<<<vb, 256, 0, h->stream>>>(n, x, mode, j);
+        return grim_launch_status(h, "k_cond_fill", 0, 0);
+    };
+    auto norm_sign = [&](bool sign, double *out) -> int {  // ||x||_1 (x <- sign(x) when asked)
+        k_cond_norm_sign<<<1, 1024, 0, h->stream>>>(n, x, sign ? x : nullptr, sd + 1);
+        GRIM_CHECK_LAUNCH(h, "k_cond_norm_sign");
+        GRIM_CHECK_CUDA(cudaMemcpyAsync(out, sd + 1, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        GRIM_CHECK_CUDA(cudaStreamSynchronize(h->stream));
+        return GRIM_OK;
+    };
+    auto argmax = [&](int jlast, int *j, double *zj, double *zlast) -> int {
+        k_cond_argmax<<<1, 1024, 0, h->stream>>>(n, x, jlast, si, sd + 2);
+        GRIM_CHECK_LAUNCH(h, "k_cond_argmax");
+        double d[2];
+        GRIM_CHECK_CUDA(cudaMemcpyAsync(j, si, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+        GRIM_CHECK_CUDA(cudaMemcpyAsync(d, sd + 2, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        GRIM_CHECK_CUDA(cudaStreamSynchronize(h->stream));
+        *zj = d[0];
+        *zlast = d[1];
+        return GRIM_OK;
+    };
+
+    // zlacn2: x = (1/n) e; y = B^-1 x
+    double est = 0.0;
+    GRIM_TRY(fill(0, 0));
+    GRIM_TRY(binv(false));
+    if (n == 1) {
+        GRIM_TRY(norm_sign(false, &est));
+    } else {
+        GRIM_TRY(norm_sign(true, &est));  // x = sign(y)
+        GRIM_TRY(binv(true));              // z = B^-H x
+        int j = 0, iter = 2;
+        double zj = 0.0, zl = 0.0;
+        GRIM_TRY(argmax(-1, &j, &zj, &zl));
+        for (;;) {
+            GRIM_TRY(fill(1, j));  // x = e_j
+            GRIM_TRY(binv(false));
+            const double old = est;
+            GRIM_TRY(norm_sign(true, &est));
+            if (!(est > old)) {
+                est = std::max(est, old);
+                break;
+            }
+            GRIM_TRY(binv(true));
+            const int jlast = j;
+            GRIM_TRY(argmax(jlast, &j, &zj, &zl));
+            if (zl != zj && iter < 5) {
+                ++iter;
+                continue;
+            }
+            break;
+        }
+        // the alternating-sign test vector
+        GRIM_TRY(fill(2, 0));
+        GRIM_TRY(binv(false));
+        double alt = 0.0;
+        GRIM_TRY(norm_sign(false, &alt));
+        alt = 2.0 * alt / (3.0 * n);
+        if (alt > est) est = alt;
+    }
+    const double c = norm_b * est;
+    *cond = std::isfinite(c) ? c : INFINITY;
+    return GRIM_OK;
 }
 
 // ============================================================== grouped factorization

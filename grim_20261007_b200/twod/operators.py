@@ -149,6 +149,20 @@ def solve_inplace(z, b, precision='double', tol=None, max_iter=10, z32=None, ctx
     return st.as_dict()
 
 
+def condition_estimate(z, ctx=None):
+    """cond_1 of the row/column-equilibrated ``z`` (complex128 device matrix), the reference's
+    ``condition_est`` (twod/solver.py:529 ``_equilibrated_condition_from_lu``): ||B||_1 times
+    the Hager-Higham estimate of ||B^-1||_1 on the device (``grim_zcond1_equilibrated``);
+    ``inf`` for an exactly singular matrix."""
+    ctx = ctx or context()
+    if z.dtype != torch.complex128:
+        raise TypeError('condition_estimate needs the complex128 matrix')
+    out = ctypes.c_double(0.0)
+    n = int(z.shape[0])
+    _lib.check(ctx.lib.grim_zcond1_equilibrated(ctx.h, n, ptr(z), n, ctypes.byref(out)), 'grim_zcond1_equilibrated')
+    return float(out.value)
+
+
 def backward_error(z, x, b, ctx=None):
     """Per-column normwise backward error on the device (reference twod/solver.py:695-720)."""
     ctx = ctx or context()
@@ -160,14 +174,16 @@ def backward_error(z, x, b, ctx=None):
 
 
 def monostatic_solve(body, k, angles_deg, pol, precision='double', tol=None, check_backward_error=True,
-                     angles_dev=None, keep=False, ctx=None):
+                     angles_dev=None, keep=False, ctx=None, condition=False):
     """One (geometry, frequency, polarization) solve with all its angles, on the device.
 
     Returns dict(amplitude=<device complex128 (nang,)>, telemetry).  With precision
     'double' the system is filled in FP64, factored and solved in FP64 and its normwise
-    backward error computed (the reference's 1e-12 gate); with 'mixed' the system is
-    filled in complex64 (FP64 small-kR and self terms), factored in complex64 and
-    refined with FP64 residuals against that matrix.
+    backward error computed (the reference's 1e-12 gate); with 'mixed' a pulse-basis
+    system is filled in complex64 (FP64 small-kR and self terms), factored in complex64
+    and refined with FP64 residuals against that matrix, a linear-Galerkin system is
+    filled in FP64, its complex64 rounding factored and the refinement run against the
+    FP64 matrix.
     """
     pol = canonical_pol(pol)
     dev = body.geom.device
@@ -179,18 +195,28 @@ def monostatic_solve(body, k, angles_deg, pol, precision='double', tol=None, che
     static = pivot != 'certified'
     tele = {}
     if precision == 'mixed':
-        z32 = fill(body, k, pol, complex64=True, ctx=ctx)
         b = rhs(body, k, pol, angles_dev, ctx=ctx)
         b0 = b.clone()
+        if static:
+            # linear-Galerkin systems fill in FP64 arithmetic whatever the output type, so
+            # the refinement runs against the FP64 matrix (its complex64 rounding is
+            # factored): the solution converges to the FP64 system's, not to the rounded one's
+            z = fill(body, k, pol, ctx=ctx)
+            z32 = None
+        else:
+            z = None
+            z32 = fill(body, k, pol, complex64=True, ctx=ctx)
         try:
-            st = solve_inplace(None, b, 'mixed', tol=MIXED_RCS_TOL if tol is None else tol, z32=z32, ctx=ctx,
+            st = solve_inplace(z, b, 'mixed', tol=MIXED_RCS_TOL if tol is None else tol, z32=z32, ctx=ctx,
                                stop='berr', pivot=pivot)
             x = b
-            z = z32
+            if z is None:
+                z = z32
         except _lib.GrimNotConverged:
             # refinement stalled (ill-conditioned system): fall back to the FP64 path, as the
             # reference's mixed -> double ladder does (linalg/dense.py:74-98)
-            z = fill(body, k, pol, ctx=ctx)
+            if z is None or z.dtype != torch.complex128:
+                z = fill(body, k, pol, ctx=ctx)
             x = b0
             if static:
                 st, _berr = solve_guarded(z, x, pivot=pivot, ctx=ctx)
@@ -213,6 +239,10 @@ def monostatic_solve(body, k, angles_deg, pol, precision='double', tol=None, che
         if check_backward_error:
             berr = backward_error(z, x, b, ctx=ctx)
             tele['backward_error_dev'] = berr
+    if condition:
+        # the estimate is of the FP64 system (filled again when the solve kept only complex64)
+        z64 = z if z.dtype == torch.complex128 else fill(body, k, pol, ctx=ctx)
+        tele['condition_est'] = condition_estimate(z64, ctx=ctx)
     amp = farfield(body, k, angles_dev, x, ctx=ctx)
     out = dict(amplitude=amp, telemetry=tele)
     if keep:
@@ -221,7 +251,7 @@ def monostatic_solve(body, k, angles_deg, pol, precision='double', tol=None, che
 
 
 def monostatic_solves_grouped(bodies, ks, angles_deg, pol, precision='mixed', tol=None, angles_dev=None,
-                              use_graph=True, workers=4):
+                              use_graph=True, workers=4, condition=False):
     """Many (geometry, frequency, polarization) systems with one angle set -- the systems
     of a frequency sweep; ``pol`` is one polarization or one per system -- solved
     together: fills and excitations on the device
@@ -258,7 +288,8 @@ def monostatic_solves_grouped(bodies, ks, angles_deg, pol, precision='mixed', to
         # the grouped factorization keeps diagonal pivots; systems that need partial
         # pivoting are factored one by one on the pool instead
         jobs = [(lambda i=i: monostatic_solve(bodies[i], ks[i], angles_deg, pols[i], precision=precision, tol=tol,
-                                              angles_dev=angles_dev)) for i in range(len(bodies))]
+                                              angles_dev=angles_dev, condition=condition))
+                for i in range(len(bodies))]
         return run_pool(jobs, workers=workers, costs=costs)
     static = all(getattr(b, 'pivot', 'certified') == 'static' for b in bodies)
     parts = run_pool([prep(i) for i in range(len(bodies))], workers=workers, costs=costs)
@@ -299,6 +330,9 @@ def monostatic_solves_grouped(bodies, ks, angles_deg, pol, precision='mixed', to
                     st, berr = solve_guarded(p['z'], x, pivot='static', ctx=c)
                     st['backward_error_dev'] = berr
             tele.update(st)
+            if condition:
+                z64 = p['z'] if p['z'].dtype == torch.complex128 else fill(bodies[i], ks[i], pols[i], ctx=c)
+                tele['condition_est'] = condition_estimate(z64, ctx=c)
             amp = farfield(bodies[i], ks[i], angles_dev, x, ctx=c)
             # release this system's matrices as soon as its work is queued: they were
             # allocated on another worker's stream, so the allocator must wait for this one

@@ -33,7 +33,7 @@ import torch
 from .. import _lib
 from ..device import context, require_cuda, run_pool
 from ..execution import require_gpu_dense_backend, requested_precision
-from . import certify
+from . import certify, quality
 from . import galerkin
 from . import geometry as geo
 from . import operators as ops
@@ -242,7 +242,7 @@ def _canonical_user_polarization_label(label):
 
 
 # ------------------------------------------------------------------ public solves
-def _validate_request(frequencies_ghz, elevations_deg, cfie_alpha, compute_condition_number):
+def _validate_request(frequencies_ghz, elevations_deg, cfie_alpha, compute_condition_number, quality_thresholds=None):
     if not frequencies_ghz:
         raise ValueError('At least one frequency is required.')
     if not elevations_deg:
@@ -255,9 +255,7 @@ def _validate_request(frequencies_ghz, elevations_deg, cfie_alpha, compute_condi
         raise ValueError('Elevation angles must all be finite.')
     if not math.isfinite(float(cfie_alpha)) or float(cfie_alpha) != 0.0:
         raise ValueError('cfie_alpha is not implemented by any active 2-D formulation; use cfie_alpha=0.')
-    if compute_condition_number:
-        raise NotImplementedError('Condition estimates run on the reference CPU path; the GPU path reports '
-                                  'backward errors instead.')
+    quality.merged_thresholds(quality_thresholds)  # unknown or invalid limits fail before any solve
     return freqs, elevs
 
 
@@ -342,21 +340,22 @@ def _frequency_record(f, elevs, pol, precision, k, body, res, t0):
                  pivoted_panels=tele.get('pivoted_panels', 0), refinement_steps=tele.get('refinement_steps', 0),
                  grouped_factorization=bool(tele.get('grouped', False)))
     return dict(samples=samples, residuals=[float(r) for r in resid], event=event, n=body.n,
-                seconds=time.perf_counter() - t0)
+                seconds=time.perf_counter() - t0, condition_est=tele.get('condition_est'))
 
 
-def _solve_frequency(meshes, f, elevs, pol, precision, abort_event):
+def _solve_frequency(meshes, f, elevs, pol, precision, abort_event, condition=False):
     """One (frequency, polarisation) system on the current device worker: mesh, fill,
-    solve, far field; returns host samples and telemetry."""
+    solve, far field (and, with ``condition``, the condition estimate of its FP64 matrix);
+    returns host samples and telemetry."""
     t0 = time.perf_counter()
     k, body = _frequency_body(meshes, f, pol, abort_event)
     angles = np.asarray(elevs, dtype=np.float64)
     angles_dev = torch.as_tensor(angles, device=body.geom.device)
-    res = ops.monostatic_solve(body, k, angles, pol, precision=precision, angles_dev=angles_dev)
+    res = ops.monostatic_solve(body, k, angles, pol, precision=precision, angles_dev=angles_dev, condition=condition)
     return _frequency_record(f, elevs, pol, precision, k, body, res, t0)
 
 
-def _solve_frequencies_grouped(items, elevs, precision, abort_event, workers):
+def _solve_frequencies_grouped(items, elevs, precision, abort_event, workers, condition=False):
     """Every (mesh, polarisation, frequency) system of a request through one grouped
     factorization (``operators.monostatic_solves_grouped``); returns the per-system outputs of
     ``_solve_frequency`` in ``items`` order."""
@@ -368,7 +367,7 @@ def _solve_frequencies_grouped(items, elevs, precision, abort_event, workers):
     angles_dev = torch.as_tensor(angles, device=built[0][1].geom.device)
     res = ops.monostatic_solves_grouped([b for _k, b in built], [k for k, _b in built], angles,
                                         [pol for pol, _f in keys], precision=precision, angles_dev=angles_dev,
-                                        workers=workers)
+                                        workers=workers, condition=condition)
     if abort_event is not None and abort_event.is_set():
         raise InterruptedError('Solve canceled by user.')
     return [_frequency_record(f, elevs, pol, precision, k, body, r, t0)
@@ -385,15 +384,19 @@ def _frequency_cost(geometry_snapshot, geometry_units, f, n_angles):
     return float(n) ** 3 + float(n) ** 2 * n_angles
 
 
-def _channel_result(pol, outs, precision, stage_seconds):
-    """Assemble one polarisation's reference-shaped result from its per-frequency outputs."""
+def _channel_result(pol, outs, precision, stage_seconds, condition=False, thresholds=None):
+    """Assemble one polarisation's reference-shaped result from its per-frequency outputs,
+    with the reference's quality gate (``quality.evaluate_quality_gate``) on its metadata."""
     _reset_dense_backend_telemetry()
-    samples, residuals, counts = [], [], []
+    samples, residuals, counts, conds = [], [], [], []
     for o in outs:
         samples.extend(o['samples'])
         residuals.extend(o['residuals'])
         counts.append(o['n'])
+        if o.get('condition_est') is not None:
+            conds.append(float(o['condition_est']))
         _record_dense_backend_event(**o['event'])
+    finite = [r for r in residuals if math.isfinite(r)]
     if requested_formulation() == 'galerkin':
         formulation = ('2D combined-field BIE, linear Galerkin (TM: S + gamma (D + M/2))' if pol == 'TM'
                        else "2D combined-field BIE, linear Galerkin (TE: K' - M/2 - gamma W)")
@@ -407,15 +410,29 @@ def _channel_result(pol, outs, precision, stage_seconds):
         'device': context().device_name,
         'panel_count_max': max(counts),
         'panel_count_min': min(counts),
-        'residual_norm_max': max(residuals) if residuals else 0.0,
+        'residual_norm_max': max(finite) if finite else float('nan'),
+        'residual_norm_mean': float(np.mean(finite)) if finite else float('nan'),
+        'residual_nonfinite_count': len(residuals) - len(finite),
+        'constraint_residual_norm_max': 0.0,
+        'junction_constraints_applied': False,
+        'condition_est_max': max(conds) if conds else float('nan'),
+        'condition_est_mean': float(np.mean(conds)) if conds else float('nan'),
+        'condition_est_computed': bool(condition),
+        'condition_estimator': 'equilibrated_1norm_lu_hager_higham' if condition else 'not_requested',
+        'warnings': [],
         'runtime_profile': {'stage_seconds': stage_seconds},
         'amplitude_version': RCS_AMPLITUDE_VERSION,
         **_dense_backend_summary(),
     }
-    metadata['quality_gate'] = {'passed': bool(max(residuals) <= (DENSE_LINEAR_BACKWARD_ERROR_MAX
-                                                                  if precision == 'double'
-                                                                  else ops.MIXED_RCS_TOL * 10)),
-                                'reason': 'backward error gate'}
+    gate = quality.evaluate_quality_gate(metadata, thresholds)
+    # the solve's own backward-error gate (FP64: the reference's 1e-12; mixed: 10x its target)
+    berr_limit = DENSE_LINEAR_BACKWARD_ERROR_MAX if precision == 'double' else ops.MIXED_RCS_TOL * 10
+    if not (finite and max(finite) <= berr_limit):
+        gate['violations'].append(f'backward error {max(finite) if finite else float("nan"):.6g} exceeds '
+                                  f'{berr_limit:.6g}')
+        gate['passed'] = False
+        gate['reason'] = '; '.join(gate['violations'])
+    metadata['quality_gate'] = gate
     return {
         'solver': '2d_bie_mom_rcs',
         'scattering_mode': 'monostatic',
@@ -429,25 +446,27 @@ def _channel_result(pol, outs, precision, stage_seconds):
 
 
 def _sweep(geometry_snapshot, frequencies_ghz, elevations_deg, pols, geometry_units, progress_callback,
-           cfie_alpha, compute_condition_number, max_panels, mesh_reference_ghz, abort_event):
+           cfie_alpha, compute_condition_number, max_panels, mesh_reference_ghz, abort_event, quality_thresholds=None):
     """Solve every (polarisation, frequency) system of a request on the device worker pool;
     returns {pol: reference-shaped channel result}."""
     channels = _sweep_many([geometry_snapshot], frequencies_ghz, elevations_deg, pols, geometry_units,
                            progress_callback, cfie_alpha, compute_condition_number, max_panels, mesh_reference_ghz,
-                           abort_event)[0]
+                           abort_event, quality_thresholds)[0]
     for ch in channels.values():
         ch.pop('_outs', None)
     return channels
 
 
 def _sweep_many(snapshots, frequencies_ghz, elevations_deg, pols, geometry_units, progress_callback, cfie_alpha,
-                compute_condition_number, max_panels, mesh_reference_ghz, abort_event):
+                compute_condition_number, max_panels, mesh_reference_ghz, abort_event, quality_thresholds=None):
     """Every (snapshot, polarisation, frequency) system of a request: one grouped
     factorization of all of them when there is more than one frequency or snapshot (a
     sweep, a certified base/refined pair), else the device worker pool.  Returns, per
     snapshot, {pol: reference-shaped channel result} (with the per-system outputs under
     ``'_outs'``)."""
-    freqs, elevs = _validate_request(frequencies_ghz, elevations_deg, cfie_alpha, compute_condition_number)
+    freqs, elevs = _validate_request(frequencies_ghz, elevations_deg, cfie_alpha, compute_condition_number,
+                                     quality_thresholds)
+    condition = bool(compute_condition_number)
     require_gpu_dense_backend()
     require_cuda()
     precision = requested_precision()
@@ -457,7 +476,8 @@ def _sweep_many(snapshots, frequencies_ghz, elevations_deg, pols, geometry_units
         for pol in pols:
             for f in freqs:
                 items.append((si, pol, f))
-                jobs.append(lambda m=meshes, f=f, pol=pol: _solve_frequency(m, f, elevs, pol, precision, abort_event))
+                jobs.append(lambda m=meshes, f=f, pol=pol: _solve_frequency(m, f, elevs, pol, precision, abort_event,
+                                                                           condition))
     # longest-processing-time order needs costs only when the systems differ (more than one
     # frequency or snapshot); each distinct (snapshot, frequency) is costed once
     costs = None
@@ -483,7 +503,7 @@ def _sweep_many(snapshots, frequencies_ghz, elevations_deg, pols, geometry_units
     if (len(freqs) > 1 or len(snapshots) > 1) and _grouped_sweeps():
         # every system through one grouped factorization (one CUDA graph)
         outs = _solve_frequencies_grouped([(mesh_list[si], pol, f) for si, pol, f in items], elevs, precision,
-                                          abort_event, sweep_workers(len(jobs)))
+                                          abort_event, sweep_workers(len(jobs)), condition)
         for i, o in enumerate(outs):
             on_done(i, o)
     else:
@@ -496,7 +516,7 @@ def _sweep_many(snapshots, frequencies_ghz, elevations_deg, pols, geometry_units
             mine = [o for (sj, p, _f), o in zip(items, outs) if sj == si and p == pol]
             stage = {'operators': 0.0, 'linear_solve': sum(o['seconds'] for o in mine), 'far_field': 0.0,
                      'wall': wall}
-            channels[pol] = _channel_result(pol, mine, precision, stage)
+            channels[pol] = _channel_result(pol, mine, precision, stage, condition, quality_thresholds)
             channels[pol]['_outs'] = mine
         results.append(channels)
     return results
@@ -535,9 +555,10 @@ def solve_monostatic_rcs_2d_single_polarization(
     if pol not in ('TM', 'TE'):
         raise ValueError(f'Unknown polarization {polarization!r}.')
     out = _sweep(geometry_snapshot, frequencies_ghz, elevations_deg, [pol], geometry_units, progress_callback,
-                 cfie_alpha, compute_condition_number, max_panels, mesh_reference_ghz, abort_event)[pol]
+                 cfie_alpha, compute_condition_number, max_panels, mesh_reference_ghz, abort_event,
+                 quality_thresholds)[pol]
     if strict_quality_gate and not out['metadata']['quality_gate']['passed']:
-        raise ValueError('Quality gate failed: backward error gate')
+        raise ValueError('Quality gate failed: ' + out['metadata']['quality_gate']['reason'])
     return out
 
 
@@ -558,10 +579,13 @@ def solve_monostatic_rcs_2d(geometry_snapshot, frequencies_ghz, elevations_deg, 
     """
     channels_by_pol = _sweep(geometry_snapshot, frequencies_ghz, elevations_deg,
                              [pol for _export, pol in _CO_POLARIZED_2D_CHANNELS], geometry_units, progress_callback,
-                             0.0, compute_condition_number, max_panels, mesh_reference_ghz, abort_event)
+                             0.0, compute_condition_number, max_panels, mesh_reference_ghz, abort_event,
+                             quality_thresholds)
     channels = {export: channels_by_pol[pol] for export, pol in _CO_POLARIZED_2D_CHANNELS}
-    if strict_quality_gate and not all(c['metadata']['quality_gate']['passed'] for c in channels.values()):
-        raise ValueError('Quality gate failed: backward error gate')
+    failed = [f"{k}: {c['metadata']['quality_gate']['reason']}" for k, c in channels.items()
+              if not c['metadata']['quality_gate']['passed']]
+    if strict_quality_gate and failed:
+        raise ValueError('Quality gate failed: ' + '; '.join(failed))
     samples = []
     for export, _pol in _CO_POLARIZED_2D_CHANNELS:
         for row in channels[export]['samples']:  # this call's own records: labelled in place
@@ -583,16 +607,19 @@ def solve_monostatic_rcs_2d(geometry_snapshot, frequencies_ghz, elevations_deg, 
 
 # ------------------------------------------------------------------ certified (base + refined mesh)
 def _certified_channels(geometry_snapshot, frequencies_ghz, elevations_deg, pols, geometry_units, progress_callback,
-                        mesh_convergence_policy, max_panels, mesh_reference_ghz, cfie_alpha, abort_event):
+                        mesh_convergence_policy, max_panels, mesh_reference_ghz, cfie_alpha, abort_event,
+                        quality_thresholds=None):
     """Base and refined-mesh solves of every (polarisation, frequency) system in ONE grouped
     factorization, then per polarisation and frequency the reference's certificate
     (``twod/solver.py:3663-3880``): the refined result is published only where it agrees
     with the base one within the policy, else ValueError."""
     policy = certify.validate_policy(mesh_convergence_policy)
     fine_snapshot = certify.scale_snapshot_panel_density(geometry_snapshot, policy['fine_factor'])
+    # the production entry reports the condition estimate, as the reference's does
+    # (twod/solver.py:3734 sets compute_condition_number for its certified pair)
     base, fine = _sweep_many([geometry_snapshot, fine_snapshot], frequencies_ghz, elevations_deg, pols,
-                             geometry_units, progress_callback, cfie_alpha, False, max_panels, mesh_reference_ghz,
-                             abort_event)
+                             geometry_units, progress_callback, cfie_alpha, True, max_panels, mesh_reference_ghz,
+                             abort_event, quality_thresholds)
     out = {}
     for pol in pols:
         b, f = base[pol], fine[pol]
@@ -629,7 +656,7 @@ def solve_monostatic_rcs_2d_certified_single_polarization(
         raise ValueError(f'Unknown polarization {polarization!r}.')
     return _certified_channels(geometry_snapshot, frequencies_ghz, elevations_deg, [pol], geometry_units,
                                progress_callback, mesh_convergence_policy, max_panels, mesh_reference_ghz, cfie_alpha,
-                               abort_event)[pol]
+                               abort_event, quality_thresholds)[pol]
 
 
 def solve_monostatic_rcs_2d_certified(geometry_snapshot, frequencies_ghz, elevations_deg, geometry_units="inches",
@@ -644,7 +671,7 @@ def solve_monostatic_rcs_2d_certified(geometry_snapshot, frequencies_ghz, elevat
     pols = [pol for _export, pol in _CO_POLARIZED_2D_CHANNELS]
     by_pol = _certified_channels(geometry_snapshot, frequencies_ghz, elevations_deg, pols, geometry_units,
                                  progress_callback, mesh_convergence_policy, max_panels, mesh_reference_ghz, 0.0,
-                                 abort_event)
+                                 abort_event, quality_thresholds)
     channels = {export: by_pol[pol] for export, pol in _CO_POLARIZED_2D_CHANNELS}
     samples = []
     for export, _pol in _CO_POLARIZED_2D_CHANNELS:

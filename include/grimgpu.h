@@ -234,6 +234,15 @@ int grim_zgesv_mixed(grim_handle_t h, int n, int nrhs, const void *A, int64_t ld
 int grim_zgesv_guarded(grim_handle_t h, int n, int nrhs, const void *A, int64_t lda, void *B, int64_t ldb,
                        int pivot, double tol, int max_refine, double *berr_dev, int *info, grim_solve_info *stats);
 
+/* Condition estimate of A (complex128, preserved): cond_1 of the row/column-equilibrated
+ * matrix B = R^-1 A C^-1 (r_i = max_j |a_ij|, c_j = max_i |a_ij| / r_i), ||B||_1 times a
+ * Hager-Higham estimate of ||B^-1||_1 (LAPACK zlacn2's iteration on partial-pivoting LUs of
+ * A and A^H, at most 11 single-vector solves); *cond on the host, INFINITY for an exactly
+ * singular or non-finite A.  Replaces the reference's _equilibrated_condition_from_lu
+ * (twod/solver.py:472-577, linalg/dense.py:157-198: the same matrix B, SciPy's block
+ * estimator).  Synchronises the stream. */
+int grim_zcond1_equilibrated(grim_handle_t h, int n, const void *A, int64_t lda, double *cond);
+
 /* Mixed solve reusing a complex64 factorization (LU32 and ipiv from grim_cgetrf, leading
  * dimension n) with FP64 refinement against A or the promotion of A32; for resident
  * factor caches (reference linalg/refined_lu.py:41-61 RefinedLU.solve on a kept factor). */

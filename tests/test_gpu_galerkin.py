@@ -286,3 +286,27 @@ def test_gated_solve_pivots_like_lapack_and_falls_back(ctx, pol):
     st2, berr2 = ops.solve_guarded(to_device_colmajor(a), x2, pivot='static')
     assert st2['gate_fallback'] and float(berr2.max()) <= 1e-12
     np.testing.assert_allclose(x2.cpu().numpy().T, np.linalg.solve(a, rhs), rtol=1e-10, atol=1e-12)
+
+
+def test_condition_number_and_quality_gate_through_the_public_entry(ctx):
+    """compute_condition_number=True reports the equilibrated condition estimate of every
+    system (condition_est_max / mean, the estimator's name) and the reference's quality gate
+    checks it: a limit below it fails the strict gate with the reference's message."""
+    import pytest as _pt
+    from grim_20261007_b200 import synthetic as S
+    from grim_20261007_b200.twod.solver import solve_monostatic_rcs_2d_single_polarization as solve1
+    v = S.naca_symmetric(0.12, 120)
+    snap = S.snapshot_from_polygons([v])
+    ang = list(np.arange(0.0, 180.0, 10.0))
+    out = solve1(snap, [0.9, 1.4], ang, 'TE', geometry_units='meters', compute_condition_number=True)
+    meta = out['metadata']
+    assert meta['condition_est_computed'] and meta['condition_estimator'] == 'equilibrated_1norm_lu_hager_higham'
+    assert 1.0 <= meta['condition_est_max'] < 1e6 and meta['condition_est_mean'] <= meta['condition_est_max']
+    gate = meta['quality_gate']
+    assert gate['passed'] and gate['certification_scope'] == 'discrete_linear_system_residual_and_condition'
+    with _pt.raises(ValueError, match='condition_est_max'):
+        solve1(snap, [0.9], ang, 'TE', geometry_units='meters', compute_condition_number=True,
+               quality_thresholds={'condition_est_max': 1.0})
+    plain = solve1(snap, [0.9], ang, 'TE', geometry_units='meters')
+    assert not plain['metadata']['condition_est_computed']
+    assert plain['metadata']['quality_gate']['certification_scope'] == 'discrete_linear_system_residual_only'

@@ -266,3 +266,32 @@ def test_backward_error_reports_nonfinite_solutions_as_infinite():
     berr = ops.backward_error(to_device_colmajor(a), to_device_colmajor(x), to_device_colmajor(b)).cpu().numpy()
     assert berr[0] < 1e-14 and berr[2] < 1e-14
     assert np.isinf(berr[1])
+
+
+def _golden_matrices():
+    import importlib.util
+    path = os.path.join(GOLDEN, 'make_quality_gate_golden.py')
+    spec = importlib.util.spec_from_file_location('make_quality_gate_golden', path)
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod.matrices()
+
+
+def test_condition_estimate_matches_the_exact_equilibrated_condition_and_the_reference(ctx):
+    """grim_zcond1_equilibrated (Hager-Higham on the device) against the exact cond_1 of the
+    row/column-equilibrated matrix and the reference's own estimate (SciPy's block estimator,
+    tests/golden/quality_gate.json): a lower bound, within a factor 3 of both (equal to
+    rounding on these matrices when the iteration finds the maximising column)."""
+    import json
+    from grim_20261007_b200.twod import operators as ops
+    with open(os.path.join(GOLDEN, 'quality_gate.json')) as f:
+        conds = json.load(f)['conditions']
+    for a, ref in zip(_golden_matrices(), conds):
+        est = ops.condition_estimate(_dev(a), ctx=ctx)
+        assert est <= ref['exact'] * (1 + 1e-9), (a.shape, est, ref)
+        assert est >= ref['exact'] / 3.0, (a.shape, est, ref)
+        assert ref['reference_estimate'] / 3.0 <= est <= 3.0 * ref['reference_estimate']
+    sing = _rand(50, 50, 77)
+    sing[:, 20] = 0.0
+    assert ops.condition_estimate(_dev(sing), ctx=ctx) == float('inf')
+    assert ops.condition_estimate(_dev(np.array([[2.0 + 1.0j]])), ctx=ctx) == pytest.approx(1.0)
