@@ -798,7 +798,7 @@ def main():
             'gpu_launches': int(launches32),
             'roofline': roofline,
             'top_kernels_mixed': top_kernels(prof),
-            'serving': summarize(serving, ('requests', 'completed', 'solves_per_s', 'p50_s', 'p99_s', 'cache_hits')),
+            'serving': summarize(serving, ('requests', 'completed', 'solves_per_s', 'p50_ms', 'p99_ms', 'cache_hits')),
             'bor_ogive': summarize_bor(bor),
             'frequency_sweep': summarize(sweep, ('systems', 'seconds', 'solves_per_s', 'n_min', 'n_max',
                                                  'max_db_error_vs_fp64_sampled', 'path')),

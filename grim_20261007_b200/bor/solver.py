@@ -21,8 +21,9 @@ import numpy as np
 import torch
 
 from .. import _lib
+from .. import sharding
 from ..device import context, ptr, require_cuda, run_pool
-from ..execution import requested_precision
+from ..execution import requested_precision, requested_shard_group
 from ..twod import operators as ops2d
 from .rules import near_rules, pair_classes
 
@@ -428,14 +429,30 @@ def solve_bor_device(points, k, thetas_deg, mmax, precision='double', tol=None, 
     t_moments = time.perf_counter() - tm
     th = torch.as_tensor(np.asarray(thetas_deg, dtype=np.float64), device='cuda')
     modes = list(range(0, mmax + 1)) if signed_mode_symmetry else list(range(-mmax, mmax + 1))
-    if ctx is not None:
-        outs = [_solve_mode(dev, m, th, precision, tol, ctx=ctx) for m in modes]
-    elif grouped:
-        outs = _solve_modes_grouped(dev, modes, th, precision, tol,
-                                    sweep_workers(len(modes)) if workers is None else workers)
+
+    def solve_local(idx):
+        sub = [modes[i] for i in idx]
+        if not sub:
+            return []
+        if ctx is not None:
+            return [_solve_mode(dev, m, th, precision, tol, ctx=ctx) for m in sub]
+        if grouped:
+            return _solve_modes_grouped(dev, sub, th, precision, tol,
+                                        sweep_workers(len(sub)) if workers is None else workers)
+        jobs = [(lambda m=m: _solve_mode(dev, m, th, precision, tol)) for m in sub]
+        return run_pool(jobs, workers=sweep_workers(len(jobs)) if workers is None else workers)
+
+    shard, group = requested_shard_group()
+    if shard and ctx is None:
+        # every rank holds the moments; the mode systems are split over the ranks (equal
+        # cost per mode) and their far-field contributions gathered on the host
+        def run_local(idx):
+            return [(part.cpu().numpy(), {kk: vv for kk, vv in t.items() if not hasattr(vv, 'cpu')})
+                    for part, t in solve_local(idx)]
+        outs = [(torch.as_tensor(part, device='cuda'), t)
+                for part, t in sharding.run_sharded([1.0] * len(modes), run_local, group)]
     else:
-        jobs = [(lambda m=m: _solve_mode(dev, m, th, precision, tol)) for m in modes]
-        outs = run_pool(jobs, workers=sweep_workers(len(jobs)) if workers is None else workers)
+        outs = solve_local(range(len(modes)))
     amp = torch.zeros(2 * int(th.numel()), dtype=torch.complex128, device='cuda')
     modes_used, tail = mmax, None
     if mode_tol is not None and signed_mode_symmetry:

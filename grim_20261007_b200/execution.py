@@ -7,6 +7,13 @@ Mirrors the reference's scoped options:
   backend and has no CPU solver, so ``cpu`` (a request for the reference's CPU LAPACK
   path) is refused with ``RuntimeError`` by every solve instead of running on the GPU
   unasked; ``auto`` and ``gpu`` both run on the GPU.
+
+One scope has no counterpart in the reference, whose frequency workers are processes of
+one host: ``shard_over_ranks(group)`` makes the public solves of every rank of a
+``torch.distributed`` process group (one process per GPU) split the independent systems
+of each request -- frequencies and polarisations of a 2-D request, Fourier modes of a
+body of revolution -- between the ranks and gather the host results, so each rank
+returns the whole result.
 """
 from __future__ import annotations
 
@@ -19,6 +26,7 @@ DENSE_GPU_MIN_N_ENV = 'GHOST_DENSE_GPU_MIN_N'
 DENSE_GPU_MIN_N_DEFAULT = 768
 
 _PRECISION = contextvars.ContextVar('grim_lu_precision', default='double')
+_SHARD = contextvars.ContextVar('grim_shard_group', default=None)
 
 
 @contextmanager
@@ -34,6 +42,31 @@ def linear_precision(value):
 
 def requested_precision():
     return _PRECISION.get()
+
+
+class _WholeWorld:
+    """Marker: shard over the default process group."""
+
+
+@contextmanager
+def shard_over_ranks(group=None):
+    """Split the systems of every public solve inside the scope over the ranks of
+    ``group`` (the default process group when None).  Every rank of the group must make
+    the same calls with the same arguments inside the scope (the gathers are collective)."""
+    token = _SHARD.set(_WholeWorld if group is None else group)
+    try:
+        yield
+    finally:
+        _SHARD.reset(token)
+
+
+def requested_shard_group():
+    """(active, group) of the innermost ``shard_over_ranks`` scope; group None means the
+    default process group."""
+    g = _SHARD.get()
+    if g is None:
+        return False, None
+    return True, (None if g is _WholeWorld else g)
 
 
 def requested_dense_backend():

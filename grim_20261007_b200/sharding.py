@@ -68,3 +68,36 @@ def max_over_ranks(value, group=None, device=None):
     t = torch.tensor([float(value)], dtype=torch.float64, device=device or 'cpu')
     dist.all_reduce(t, op=dist.ReduceOp.MAX, group=group)
     return float(t.item())
+
+
+def run_sharded(costs, run_local, group=None):
+    """Run units over the ranks of ``group``: this rank calls ``run_local(indices)`` on its
+    LPT share (unit indices in unit order; it returns one host result per index, in that
+    order), then every rank receives all results in unit order.  Without an initialised
+    process group, or with one rank, ``run_local`` gets every unit.  Collective: every rank
+    calls it with the same costs.  A rank whose share raised still joins the gather, and
+    then every rank raises ``RuntimeError`` naming the failed ranks (no rank is left
+    waiting in the collective)."""
+    if not dist.is_initialized() or dist.get_world_size(group) == 1:
+        return list(run_local(list(range(len(costs)))))
+    world = dist.get_world_size(group)
+    rank = dist.get_rank(group)
+    owner, _ = lpt_partition(costs, world)
+    mine = [i for i, r in enumerate(owner) if r == rank]
+    try:
+        local = list(run_local(mine)) if mine else []
+        if len(local) != len(mine):
+            raise RuntimeError(f'run_local returned {len(local)} results for {len(mine)} units')
+        part = (None, local)
+    except Exception as exc:  # noqa: BLE001 - reported to every rank below
+        part = (f'{type(exc).__name__}: {exc}', [])
+    parts = [None] * world
+    dist.all_gather_object(parts, part, group=group)
+    failed = [(r, p[0]) for r, p in enumerate(parts) if p[0] is not None]
+    if failed:
+        raise RuntimeError('sharded solve failed on rank(s) ' + '; '.join(f'{r}: {m}' for r, m in failed))
+    out, taken = [None] * len(costs), [0] * world
+    for i, r in enumerate(owner):
+        out[i] = parts[r][1][taken[r]]
+        taken[r] += 1
+    return out

@@ -32,7 +32,8 @@ import torch
 
 from .. import _lib
 from ..device import context, require_cuda, run_pool
-from ..execution import require_gpu_dense_backend, requested_precision
+from .. import sharding
+from ..execution import require_gpu_dense_backend, requested_precision, requested_shard_group
 from . import certify, quality
 from . import galerkin
 from . import geometry as geo
@@ -479,9 +480,11 @@ def _sweep_many(snapshots, frequencies_ghz, elevations_deg, pols, geometry_units
                 jobs.append(lambda m=meshes, f=f, pol=pol: _solve_frequency(m, f, elevs, pol, precision, abort_event,
                                                                            condition))
     # longest-processing-time order needs costs only when the systems differ (more than one
-    # frequency or snapshot); each distinct (snapshot, frequency) is costed once
+    # frequency or snapshot) or when they are split over ranks; each distinct (snapshot,
+    # frequency) is costed once
+    shard, group = requested_shard_group()
     costs = None
-    if len(freqs) > 1 or len(snapshots) > 1:
+    if len(freqs) > 1 or len(snapshots) > 1 or shard:
         per = {}
         for si, _pol, f in items:
             if (si, f) not in per:
@@ -499,15 +502,26 @@ def _sweep_many(snapshots, frequencies_ghz, elevations_deg, pols, geometry_units
             except Exception:  # noqa: BLE001 - progress reporting never fails a solve
                 pass
 
+    def run_local(idx):
+        # the systems ``idx`` (indices into items) on this process's device
+        idx = list(idx)
+        if len(idx) > 1 and (len(freqs) > 1 or len(snapshots) > 1) and _grouped_sweeps():
+            # every system through one grouped factorization (one CUDA graph)
+            outs = _solve_frequencies_grouped([(mesh_list[items[i][0]], items[i][1], items[i][2]) for i in idx],
+                                              elevs, precision, abort_event, sweep_workers(len(idx)), condition)
+            for i, o in zip(idx, outs):
+                on_done(i, o)
+            return outs
+        return run_pool([jobs[i] for i in idx], workers=sweep_workers(len(idx)),
+                        costs=None if costs is None else [costs[i] for i in idx],
+                        on_done=lambda li, o: on_done(idx[li], o))
+
     t0 = time.perf_counter()
-    if (len(freqs) > 1 or len(snapshots) > 1) and _grouped_sweeps():
-        # every system through one grouped factorization (one CUDA graph)
-        outs = _solve_frequencies_grouped([(mesh_list[si], pol, f) for si, pol, f in items], elevs, precision,
-                                          abort_event, sweep_workers(len(jobs)), condition)
-        for i, o in enumerate(outs):
-            on_done(i, o)
+    if shard:
+        # this rank's LPT share of the systems, then every rank's host records
+        outs = sharding.run_sharded(costs, run_local, group)
     else:
-        outs = run_pool(jobs, workers=sweep_workers(len(jobs)), costs=costs, on_done=on_done)
+        outs = run_local(range(len(items)))
     wall = time.perf_counter() - t0
     results = []
     for si in range(len(snapshots)):
