@@ -21,8 +21,8 @@ GRIM_ERR_NOT_CONVERGED = 7
 GRIM_ERR_NONFINITE = 8
 POL_TM, POL_TE = 0, 1
 PREC_FP64, PREC_MIXED, PREC_MIXED_BERR = 0, 1, 2
-PREC_STATIC_PIVOT, PREC_PARTIAL_PIVOT = 8, 16
-PIVOT_CERTIFIED, PIVOT_STATIC, PIVOT_PARTIAL = 0, 1, 2
+PREC_STATIC_PIVOT, PREC_PARTIAL_PIVOT, PREC_TOURNAMENT_PIVOT = 8, 16, 32
+PIVOT_CERTIFIED, PIVOT_STATIC, PIVOT_PARTIAL, PIVOT_TOURNAMENT = 0, 1, 2, 3
 TUNE_SOLVE_BN, TUNE_GS_BLOCK, TUNE_PIVOT = 1, 2, 3
 
 c_int, c_int64, c_double, c_void_p, c_char_p = ctypes.c_int, ctypes.c_int64, ctypes.c_double, ctypes.c_void_p, ctypes.c_char_p

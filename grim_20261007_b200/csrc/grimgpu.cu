@@ -24,6 +24,7 @@
 #include "farblock.cuh"
 #include "galerkin.cuh"
 #include "pivot.cuh"
+#include "tslu.cuh"
 #include "condest.cuh"
 
 // ============================================================== errors
@@ -249,7 +250,7 @@ extern "C" int grim_set_tuning(grim_handle_t h, int key, int value) {
         h->tune_gs_block = value;
         return GRIM_OK;
     }
-    if (key == GRIM_TUNE_PIVOT && value >= GRIM_PIVOT_CERTIFIED && value <= GRIM_PIVOT_PARTIAL) {
+    if (key == GRIM_TUNE_PIVOT && value >= GRIM_PIVOT_CERTIFIED && value <= GRIM_PIVOT_TOURNAMENT) {
         h->pivot_mode = value;
         return GRIM_OK;
     }
@@ -669,6 +670,7 @@ static int smem_opt_in() {
     const int tri = (NB * NBP + NB) * (int)sizeof(C);
     GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_panel_apply<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, tri));
     GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_panel_u_moves<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, tri));
+    GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_tslu_finish<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, tri));
     GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_apply_moves<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          GEPP_MOVES_SMEM_MAX));
     GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_trsm_diag<C, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, tri));
@@ -849,6 +851,47 @@ static int gepp_launch(grim_context *h, int n, C *A, int64_t lda, int j, int nbj
     return grim_launch_status(h, kname("k_panel_gepp", sizeof(C)), 8.0 * m * nbj * nbj / 2.0, 0);
 }
 
+// Tournament-pivoting panel (tslu.cuh): the selection tree, then L21 and the row moves.
+// ws: the factorization's tournament workspace (TsluWs, sized for its n).
+struct TsluWs {
+    int *cand = nullptr, *ccount = nullptr, *arrive = nullptr, *winners = nullptr;
+    void *top = nullptr;
+    int gmax = 0;  // CTAs of the first panel: arrive holds 2 gmax + 32 counters per panel
+};
+
+template <typename C>
+static int tslu_workspace(grim_context *h, int n, TsluWs *ws) {
+    const int npan = ceil_div(n, NB);
+    ws->gmax = ceil_div(n, TSLU_ROWS);
+    void *p = nullptr;
+    // nodes of one tree: sum over levels of ceil(g / 2^l) <= 2 g + log2(g)
+    const size_t nodes = (size_t)2 * ws->gmax + 32;
+    GRIM_TRY(grim_workspace(h, "tslu_nodes", nodes * (NB + 1) * sizeof(int) + NB * sizeof(int), &p));
+    ws->cand = (int *)p;
+    ws->ccount = ws->cand + nodes * NB;
+    ws->winners = ws->ccount + nodes;
+    GRIM_TRY(grim_workspace(h, sizeof(C) == 16 ? "tslu_top64" : "tslu_top32", (size_t)NB * NB * sizeof(C), &p));
+    ws->top = p;
+    GRIM_TRY(grim_workspace(h, "tslu_arrive", (size_t)npan * nodes * sizeof(int), &p));
+    ws->arrive = (int *)p;
+    GRIM_CHECK_CUDA(cudaMemsetAsync(ws->arrive, 0, (size_t)npan * nodes * sizeof(int), h->stream));
+    return GRIM_OK;
+}
+
+template <typename C>
+static int tslu_launch(grim_context *h, int n, C *A, int64_t lda, int p, int j, int nbj, int *ipiv, int *d_info,
+                       int *swapped, int *moves, PanelPack pk, const TsluWs &ws) {
+    const int m = n - j;
+    const int g = ceil_div(m, TSLU_ROWS);
+    int *arrive = ws.arrive + (size_t)p * (2 * ws.gmax + 32);
+    k_tslu_tree<C><<<g, TSLU_THREADS, 0, h->stream>>>(n, A, lda, j, nbj, ws.cand, ws.ccount, arrive, (C *)ws.top,
+                                                     ws.winners, ipiv, d_info, swapped, moves);
+    GRIM_TRY(grim_launch_status(h, kname("k_tslu_tree", sizeof(C)), 8.0 * m * nbj * nbj / 2.0, 0));
+    const size_t tri = (size_t)(NB * NBP + NB) * sizeof(C);
+    k_tslu_finish<C><<<g, 256, tri, h->stream>>>(n, A, lda, j, nbj, (const C *)ws.top, ws.winners, moves, pk);
+    return grim_launch_status(h, kname("k_tslu_finish", sizeof(C)), 8.0 * m * nbj * nbj / 2.0, 0);
+}
+
 // Device flag layout for one factorization: [0] info, [1] pivoted panels, then per panel
 // cert[npan], swapped[npan], counter[npan].
 //
@@ -893,10 +936,13 @@ static int getrf_impl(grim_context *h, int n, C *A, int64_t lda, int *ipiv, int 
     int status = GRIM_OK;
     bool wide_pending = false;
     int *moves = nullptr;
-    if (h->pivot_mode == GRIM_PIVOT_PARTIAL) {
+    const bool tournament = h->pivot_mode == GRIM_PIVOT_TOURNAMENT;
+    TsluWs tws;
+    if (h->pivot_mode == GRIM_PIVOT_PARTIAL || tournament) {
         void *pm = nullptr;
         GRIM_TRY(grim_workspace(h, "gepp_moves", (1 + 2 * GEPP_MAX_MOVES) * sizeof(int), &pm));
         moves = (int *)pm;
+        if (tournament) GRIM_TRY(tslu_workspace<C>(h, n, &tws));
     }
     for (int p = 0; p < npan && status == GRIM_OK && moves; ++p) {
         // partial pivoting: the panel on a cluster, then the trailing columns' row moves and
@@ -916,7 +962,8 @@ static int getrf_impl(grim_context *h, int n, C *A, int64_t lda, int *ipiv, int 
             pk.b_lo = pb.lo;
             pk.b_rows = pb.rows_p;
         }
-        status = gepp_launch<C>(h, n, A, lda, j, nbj, ipiv, d_info, swapped + p, moves, pk);
+        status = tournament ? tslu_launch<C>(h, n, A, lda, p, j, nbj, ipiv, d_info, swapped + p, moves, pk, tws)
+                            : gepp_launch<C>(h, n, A, lda, j, nbj, ipiv, d_info, swapped + p, moves, pk);
         if (status != GRIM_OK) break;
         if (wide_pending) {
             GRIM_CHECK_CUDA(cudaStreamWaitEvent(h->stream, h->events[2 + npan + p - 1], 0));
@@ -1658,9 +1705,11 @@ static int mixed_refine(grim_context *h, int n, int nrhs, const TA *Ares, int64_
 extern "C" int grim_zgesv_mixed(grim_handle_t h, int n, int nrhs, const void *A, int64_t lda, const void *A32,
                                 int64_t lda32, void *B, int64_t ldb, int precision_mode, double tol, int max_iter,
                                 int *info, grim_solve_info *stats) {
-    const int pivot_req = (precision_mode & GRIM_PREC_PARTIAL_PIVOT) ? GRIM_PIVOT_PARTIAL
-                          : (precision_mode & GRIM_PREC_STATIC_PIVOT) ? GRIM_PIVOT_STATIC : -1;
-    precision_mode &= ~(GRIM_PREC_STATIC_PIVOT | GRIM_PREC_PARTIAL_PIVOT);
+    const int pivot_req = (precision_mode & GRIM_PREC_TOURNAMENT_PIVOT) ? GRIM_PIVOT_TOURNAMENT
+                          : (precision_mode & GRIM_PREC_PARTIAL_PIVOT)  ? GRIM_PIVOT_PARTIAL
+                          : (precision_mode & GRIM_PREC_STATIC_PIVOT)   ? GRIM_PIVOT_STATIC
+                                                                        : -1;
+    precision_mode &= ~(GRIM_PREC_STATIC_PIVOT | GRIM_PREC_PARTIAL_PIVOT | GRIM_PREC_TOURNAMENT_PIVOT);
     if (!h || n <= 0 || nrhs <= 0 || !B || ldb < n || (!A && !A32) || (A && lda < n) || (A32 && lda32 < n) ||
         (precision_mode != GRIM_PREC_FP64 && precision_mode != GRIM_PREC_MIXED &&
          precision_mode != GRIM_PREC_MIXED_BERR))
@@ -1757,7 +1806,7 @@ extern "C" int grim_zgesv_guarded(grim_handle_t h, int n, int nrhs, const void *
                                   int pivot, double tol, int max_refine, double *berr_dev, int *info,
                                   grim_solve_info *stats) {
     if (!h || n <= 0 || nrhs <= 0 || !A || lda < n || !B || ldb < n || !(tol > 0) || max_refine < 0 ||
-        pivot < GRIM_PIVOT_CERTIFIED || pivot > GRIM_PIVOT_PARTIAL)
+        pivot < GRIM_PIVOT_CERTIFIED || pivot > GRIM_PIVOT_TOURNAMENT)
         return grim_fail(GRIM_ERR_ARGUMENT, "grim_zgesv_guarded: bad arguments");
     DeviceGuard g(h->device);
     grim_solve_info st{};

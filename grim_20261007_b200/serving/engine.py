@@ -259,7 +259,7 @@ class ServingEngine:
             ipiv = torch.empty(n, dtype=torch.int32, device='cuda')
             info = ctypes.c_int(0)
             fn = ctx.lib.grim_cgetrf if mixed else ctx.lib.grim_zgetrf
-            _lib.check(ctx.lib.grim_set_tuning(ctx.h, _lib.TUNE_PIVOT, _lib.PIVOT_PARTIAL), 'grim_set_tuning')
+            _lib.check(ctx.lib.grim_set_tuning(ctx.h, _lib.TUNE_PIVOT, ops.PIVOTS[body.pivot]), 'grim_set_tuning')
             try:
                 _lib.check(fn(ctx.h, n, ptr(lu), n, ptr(ipiv), ctypes.byref(info)), 'getrf')
             finally:
@@ -288,7 +288,7 @@ class ServingEngine:
                 # stalled refinement: solve this request in FP64 (reference mixed -> double ladder)
                 z64 = ops.fill(body, req.k, req.pol, ctx=ctx)
                 x = b0
-                ops.solve_guarded(z64, x, pivot='partial', ctx=ctx)
+                ops.solve_guarded(z64, x, pivot=body.pivot, ctx=ctx)
                 tele['fp64_fallback'] = True
             else:
                 _lib.check(status, 'grim_zgesv_mixed_factored')
@@ -303,7 +303,7 @@ class ServingEngine:
             if not tele['backward_error'] <= ops.DOUBLE_GATE_TOL:
                 # the cached factor misses the FP64 gate: the gated solve of this request
                 x = b.clone()
-                st_g, berr = ops.solve_guarded(entry['z'], x, pivot='partial', ctx=ctx)
+                st_g, berr = ops.solve_guarded(entry['z'], x, pivot=body.pivot, ctx=ctx)
                 tele['backward_error'] = float(berr.max().item())
                 tele['gate_fallback'] = st_g['gate_fallback']
         amp = ops.farfield(body, req.k, ang, x, ctx=ctx)

@@ -20,6 +20,8 @@ from __future__ import annotations
 
 import ctypes
 
+import os
+
 import numpy as np
 import torch
 
@@ -111,8 +113,9 @@ class GalerkinBody:
         self.route_counts = np.bincount(routes, minlength=4)
 
     # partial pivoting leaves the diagonal on these systems (and unpivoted elimination grows
-    # by up to 1e10 on cosine-spaced airfoils): their factorizations pivot throughout
-    pivot = 'partial'
+    # by up to 1e10 on cosine-spaced airfoils): their factorizations pivot throughout, with
+    # LAPACK's partial pivoting (GRIM_GALERKIN_PIVOT=tournament selects tournament pivoting)
+    pivot = 'tournament' if os.environ.get('GRIM_GALERKIN_PIVOT', 'partial') == 'tournament' else 'partial'
 
     def far_min_order(self, k, pol):
         return w_far_order(k, self.lengths) if pol == 'TE' else 0

@@ -87,12 +87,13 @@ def farfield(body, k, angles_dev, x, out=None, ctx=None):
     return amp
 
 
-PIVOTS = {'certified': _lib.PIVOT_CERTIFIED, 'static': _lib.PIVOT_STATIC, 'partial': _lib.PIVOT_PARTIAL}
+PIVOTS = {'certified': _lib.PIVOT_CERTIFIED, 'static': _lib.PIVOT_STATIC, 'partial': _lib.PIVOT_PARTIAL,
+          'tournament': _lib.PIVOT_TOURNAMENT}
 
 
 def solve_guarded(z, b, pivot='partial', tol=DOUBLE_GATE_TOL, max_refine=2, ctx=None):
     """FP64 solve of Z X = B with the reference's dense gate (``grim_zgesv_guarded``): LU in
-    the ``pivot`` mode ('partial', 'certified' or 'static'), the per-column normwise
+    the ``pivot`` mode ('partial', 'tournament', 'certified' or 'static'), the per-column normwise
     backward error, at most ``max_refine`` refinement steps while it exceeds ``tol`` and a
     certified factorization when the gate still fails.  X overwrites ``b``; returns
     (telemetry dict, per-column backward errors on the device)."""
@@ -121,7 +122,8 @@ def solve_inplace(z, b, precision='double', tol=None, max_iter=10, z32=None, ctx
     normwise backward error (``stop='berr'``) is <= ``tol``.  With ``tuned`` the handle's
     tile shapes come from the autotuner's cache (``tuning.apply``).
     ``pivot``: the factorization's pivot mode -- 'certified' (diagonal pivots, certified per
-    panel, partial pivoting where they fail), 'partial' (partial pivoting throughout) or
+    panel, partial pivoting where they fail), 'partial' (partial pivoting throughout),
+    'tournament' (tournament pivoting throughout) or
     'static' (diagonal pivots; the refinement guards the solution, a stall raises
     ``GrimNotConverged``).
     Returns the solve telemetry dict.
@@ -140,6 +142,8 @@ def solve_inplace(z, b, precision='double', tol=None, max_iter=10, z32=None, ctx
         mode = _lib.PREC_FP64
     if pivot == 'partial':
         mode |= _lib.PREC_PARTIAL_PIVOT
+    elif pivot == 'tournament':
+        mode |= _lib.PREC_TOURNAMENT_PIVOT
     elif pivot == 'static':
         mode |= _lib.PREC_STATIC_PIVOT
     tol = MIXED_DROPIN_TOL if tol is None else float(tol)
@@ -284,7 +288,7 @@ def monostatic_solves_grouped(bodies, ks, angles_deg, pol, precision='mixed', to
             return {'z': z, 'lu': z.clone(), 'b': b}
         return run
 
-    if any(getattr(b, 'pivot', 'certified') == 'partial' for b in bodies):
+    if any(getattr(b, 'pivot', 'certified') in ('partial', 'tournament') for b in bodies):
         # the grouped factorization keeps diagonal pivots; systems that need partial
         # pivoting are factored one by one on the pool instead
         jobs = [(lambda i=i: monostatic_solve(bodies[i], ks[i], angles_deg, pols[i], precision=precision, tol=tol,

@@ -57,17 +57,22 @@ extern "C" {
 #define GRIM_PREC_STATIC_PIVOT 8   /* or-ed into a mode: this factorization keeps the
                                       diagonal pivots (no partial-pivoting fallback)  */
 #define GRIM_PREC_PARTIAL_PIVOT 16 /* or-ed into a mode: partial pivoting throughout    */
+#define GRIM_PREC_TOURNAMENT_PIVOT 32 /* or-ed into a mode: tournament pivoting throughout */
 /* Pivot modes of a factorization (grim_set_tuning GRIM_TUNE_PIVOT, grim_zgesv_guarded):
  * CERTIFIED  diagonal pivots, each 64-column panel certified to be what partial pivoting
  *            picks and refactored with partial pivoting when it is not (fast for
  *            diagonally dominant systems: the pulse-basis matrices, the BoR modes);
  * STATIC     diagonal pivots, no fallback (callers guard the solution);
  * PARTIAL    partial pivoting of every panel on a thread-block cluster (the
- *            linear-Galerkin combined-field systems, whose pivots leave the diagonal).
+ *            linear-Galerkin combined-field systems, whose pivots leave the diagonal);
+ * TOURNAMENT tournament pivoting of every panel (communication-avoiding LU: each panel's
+ *            64 pivot rows chosen by a reduction tree of partial-pivoting selections on
+ *            128-row blocks; stable like partial pivoting in practice, other pivots).
  * CERTIFIED and PARTIAL give LAPACK getrf's pivots (|re| + |im|, first row on ties). */
 #define GRIM_PIVOT_CERTIFIED 0
 #define GRIM_PIVOT_STATIC 1
 #define GRIM_PIVOT_PARTIAL 2
+#define GRIM_PIVOT_TOURNAMENT 3
 
 typedef struct grim_context *grim_handle_t;
 

@@ -310,3 +310,26 @@ def test_condition_number_and_quality_gate_through_the_public_entry(ctx):
     plain = solve1(snap, [0.9], ang, 'TE', geometry_units='meters')
     assert not plain['metadata']['condition_est_computed']
     assert plain['metadata']['quality_gate']['certification_scope'] == 'discrete_linear_system_residual_only'
+
+
+@pytest.mark.parametrize('pol', ['TM', 'TE'])
+def test_tournament_pivoting_meets_the_gate_on_the_airfoil(ctx, pol):
+    """Tournament pivoting (tslu.cuh) of the linear-Galerkin systems: on the
+    2048-element airfoil the FP64 solve meets the reference's 1e-12 backward-error gate and
+    equals the partial-pivoting (LAPACK-pivot) solution to 1e-10; the mixed solve through a
+    complex64 tournament factorization refines to the same solution."""
+    from grim_20261007_b200.twod import operators as ops
+    from grim_20261007_b200.twod.galerkin import GalerkinBody
+    v, k, _f, _t = S.airfoil_case(0, 2048)
+    body = GalerkinBody([v])
+    z = body.fill_matrix(k, pol)
+    ang = torch.as_tensor(np.arange(0.0, 360.0, 2.0), device='cuda')
+    b = body.rhs_matrix(k, pol, ang)
+    xt, xp, xm = b.clone(), b.clone(), b.clone()
+    st, berr = ops.solve_guarded(z, xt, pivot='tournament')
+    assert float(berr.max()) <= 1e-12 and not st['gate_fallback'], st
+    _st, _b = ops.solve_guarded(z, xp, pivot='partial')
+    scale = float(xp.abs().max())
+    assert float((xt - xp).abs().max()) <= 1e-10 * scale
+    ops.solve_inplace(z, xm, 'mixed', tol=1e-12, stop='berr', pivot='tournament', tuned=False)
+    assert float((xm - xp).abs().max()) <= 1e-9 * scale

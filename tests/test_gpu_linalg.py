@@ -295,3 +295,111 @@ def test_condition_estimate_matches_the_exact_equilibrated_condition_and_the_ref
     sing[:, 20] = 0.0
     assert ops.condition_estimate(_dev(sing), ctx=ctx) == float('inf')
     assert ops.condition_estimate(_dev(np.array([[2.0 + 1.0j]])), ctx=ctx) == pytest.approx(1.0)
+
+
+def _tournament_pivots(a, nb=64, rows=128):
+    """NumPy model of the tournament (tslu.cuh): per panel, partial-pivoting selections on
+    128-row blocks, then on the concatenated choices of sibling pairs up to the root (first
+    row of the list on ties); the root's order is the panel's pivot order.  Returns the
+    LAPACK-style ipiv (1-based) of the whole factorization."""
+    a = np.array(a, dtype=np.complex128)
+    n = a.shape[0]
+    ipiv = np.zeros(n, dtype=np.int64)
+
+    def select(rows_idx, panel, w):
+        blk = panel[rows_idx].copy()
+        alive = np.ones(len(rows_idx), bool)
+        out = []
+        for k in range(min(w, len(rows_idx))):
+            v = np.where(alive, np.abs(blk[:, k].real) + np.abs(blk[:, k].imag), -1.0)
+            p = int(np.argmax(v))
+            out.append(rows_idx[p])
+            alive[p] = False
+            piv = blk[p, k]
+            if piv != 0:
+                l = np.where(alive, blk[:, k] / piv, 0)
+                blk[:, k + 1:] -= np.outer(l, blk[p, k + 1:])
+        return out
+
+    for j in range(0, n, nb):
+        w = min(nb, n - j)
+        panel = a[j:, j:j + w]
+        m = panel.shape[0]
+        lists = [select(list(range(s, min(m, s + rows))), panel, w) for s in range(0, m, rows)]
+        while len(lists) > 1:
+            lists = [select(lists[i] + (lists[i + 1] if i + 1 < len(lists) else []), panel, w)
+                     for i in range(0, len(lists), 2)]
+        win = lists[0][:w]
+        # swap sequence bringing win[s] to place s, applied to the whole matrix
+        order = list(range(m))
+        for s, r in enumerate(win):
+            p = order.index(r)
+            ipiv[j + s] = j + p + 1
+            order[s], order[p] = order[p], order[s]
+            a[[j + s, j + p]] = a[[j + p, j + s]]
+        # eliminate the panel without pivoting, then the trailing update
+        for k in range(w):
+            a[j + k + 1:, j + k] /= a[j + k, j + k]
+            a[j + k + 1:, j + k + 1:j + w] -= np.outer(a[j + k + 1:, j + k], a[j + k, j + k + 1:j + w])
+        if j + w < n:
+            l11 = np.tril(a[j:j + w, j:j + w], -1) + np.eye(w)
+            a[j:j + w, j + w:] = sla.solve_triangular(l11, a[j:j + w, j + w:], lower=True, unit_diagonal=True)
+            a[j + w:, j + w:] -= a[j + w:, j:j + w] @ a[j:j + w, j + w:]
+    return ipiv, a
+
+
+@pytest.mark.parametrize('n', [1, 5, 64, 130, 300, 1000, 2048, 2100, 4100])
+def test_tournament_getrf_is_an_lu_with_the_tournament_pivots(ctx, n):
+    """Tournament pivoting (tslu.cuh): P A = L U to FP64 accuracy, bounded multipliers, and
+    the pivots of the NumPy model of the same tree (one CTA, 16 and 33 leaves; a last panel
+    of 4 columns; 1 and 5 rows)."""
+    from grim_20261007_b200 import _lib
+    a = _rand(n, n, 900 + n)
+    t, ipiv, info = _getrf(ctx, a, pivot=_lib.PIVOT_TOURNAMENT)
+    assert info == 0
+    piv = ipiv.cpu().numpy()
+    assert np.all(piv >= np.arange(1, n + 1)) and np.all(piv <= n)
+    lu = _host(t)
+    low = np.tril(lu, -1) + np.eye(n)
+    up = np.triu(lu)
+    assert np.max(np.abs(low)) <= 10.0
+    pa = a[_lapack_perm(piv)]
+    assert np.max(np.abs(pa - low @ up)) <= 1e-11 * np.max(np.abs(a)) * max(1.0, n / 1000)
+    if n <= 1000:
+        ref_piv, ref_lu = _tournament_pivots(a)
+        np.testing.assert_array_equal(piv, ref_piv)
+        assert np.max(np.abs(lu - ref_lu)) <= 1e-10 * max(1.0, np.max(np.abs(ref_lu)))
+
+
+@pytest.mark.parametrize('n', [300, 2048])
+def test_tournament_cgetrf_and_mixed_solve(ctx, n):
+    """complex64 tournament LU (the trailing update's packed operands written by the L21
+    stage) is an LU of A to FP32 accuracy, and the mixed solve through it refines to FP64
+    (backward error <= 1e-12 against LAPACK's solution)."""
+    from grim_20261007_b200 import _lib
+    from grim_20261007_b200.twod import operators as ops
+    a = _rand(n, n, 77 + n)
+    a32 = a.astype(np.complex64)
+    t, ipiv, info = _getrf(ctx, a32, complex64=True, pivot=_lib.PIVOT_TOURNAMENT)
+    assert info == 0
+    lu = _host(t).astype(np.complex128)
+    low = np.tril(lu, -1) + np.eye(n)
+    up = np.triu(lu)
+    pa = a32.astype(np.complex128)[_lapack_perm(ipiv.cpu().numpy())]
+    assert np.max(np.abs(pa - low @ up)) <= 1e-4 * np.max(np.abs(a))
+    rhs = _rand(n, 40, 5 + n)
+    b = _dev(rhs)  # (40, n): the right-hand sides column-major
+    st = ops.solve_inplace(_dev(a), b, 'mixed', tol=1e-13, stop='berr', pivot='tournament', tuned=False)
+    xs = _host(b)
+    ref = np.linalg.solve(a, rhs)
+    assert np.max(np.abs(xs - ref)) <= 1e-9 * np.max(np.abs(ref))
+    assert st['backward_error'] <= 1e-12
+
+
+def test_tournament_singular_column_reports_info(ctx):
+    from grim_20261007_b200 import _lib
+    n = 300
+    a = _rand(n, n, 12)
+    a[:, 77] = 0.0
+    _t, _ipiv, info = _getrf(ctx, a, pivot=_lib.PIVOT_TOURNAMENT)
+    assert info == 78
