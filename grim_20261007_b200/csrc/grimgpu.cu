@@ -25,6 +25,7 @@
 #include "galerkin.cuh"
 #include "pivot.cuh"
 #include "tslu.cuh"
+#include "gepp_loop.cuh"
 #include "condest.cuh"
 
 // ============================================================== errors
@@ -781,11 +782,49 @@ static bool gepp_reg_enabled() {
     return on;
 }
 
+// Loop-resident partial-pivoting panel (k_panel_gepp_loop) for panels of at most
+// 16 x GEPPL_ROWS rows; GRIM_GEPP_LOOP=0 keeps them on the unrolled register kernel.
+static bool gepp_loop_enabled() {
+    static const bool on = [] {
+        const char *e = getenv("GRIM_GEPP_LOOP");
+        return !(e && atoi(e) == 0);
+    }();
+    return on;
+}
+
 // Partial-pivoting factorization of the panel (j, nbj) of A on one thread-block cluster.
 template <typename C>
 static int gepp_launch(grim_context *h, int n, C *A, int64_t lda, int j, int nbj, int *ipiv, int *d_info,
                        int *swapped, int *moves, PanelPack pk) {
     const int m = n - j;
+    if (gepp_loop_enabled() && m <= 16 * GEPPL_ROWS) {
+        const int cs = std::max(1, ceil_div(m, GEPPL_ROWS));
+        const int rpc = ceil_div(m, cs);
+        const size_t smem = (size_t)NB * GEPPL_ROWS * sizeof(C);
+        static PerDeviceOnce attr_loop;
+        if (attr_loop.needed()) {
+            GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_panel_gepp_loop<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)smem));
+            GRIM_CHECK_CUDA(
+                cudaFuncSetAttribute(k_panel_gepp_loop<C>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+            attr_loop.mark();
+        }
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(cs);
+        cfg.blockDim = dim3(GEPPL_THREADS);
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = h->stream;
+        cudaLaunchAttribute la[1];
+        la[0].id = cudaLaunchAttributeClusterDimension;
+        la[0].val.clusterDim.x = cs;
+        la[0].val.clusterDim.y = 1;
+        la[0].val.clusterDim.z = 1;
+        cfg.attrs = la;
+        cfg.numAttrs = 1;
+        GRIM_CHECK_CUDA(cudaLaunchKernelEx(&cfg, k_panel_gepp_loop<C>, n, A, lda, j, nbj, rpc, ipiv, d_info,
+                                           swapped, moves, pk));
+        return grim_launch_status(h, kname("k_panel_gepp_loop", sizeof(C)), 8.0 * m * nbj * nbj / 2.0, 0);
+    }
     if (gepp_reg_enabled() && m <= 16 * GEPPR_ROWS) {
         // rows in registers: the fewest CTAs of at most GEPPR_ROWS rows each
         const int cs = std::max(1, ceil_div(m, GEPPR_ROWS));

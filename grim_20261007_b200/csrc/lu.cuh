@@ -236,6 +236,137 @@ __device__ __forceinline__ void subst_col_upper(C (&v)[16], const C *T, const C 
     }
 }
 
+// x U = a for one 64-long row vector shared by 4 consecutive lanes (sub-lane s owns the
+// entries p = 4 i + s, i < 16, in v[i]; T is U in shared memory, leading dim NBP, rd its
+// reciprocal diagonal, entries past nbj zero with rd = 1).  The same result as
+// subst_row_upper, computed right-looking as a loop whose body stays in the instruction
+// cache: each column's value, once final, is broadcast to the group and subtracted from the
+// later entries; after each block of four columns the pending entries shift down one
+// register and the solved ones into x, so every register index is a compile-time constant.
+// Phase p (blocks 4 p .. 4 p + 3) keeps 16 - 4 p pending registers.
+template <typename C, int LIVE>
+__device__ __forceinline__ void subst_row_upper_blocks(C (&v)[16], C (&x)[16], const C *T, const C *rd, int nbj,
+                                                       int s, int b0) {
+    const int base = (int)(threadIdx.x & 31u) & ~3;
+#pragma unroll 1
+    for (int b = b0; b < b0 + 4; ++b) {
+#pragma unroll
+        for (int cc = 0; cc < 4; ++cc) {
+            const int c = 4 * b + cc;
+            C xc = czero<C>();
+            if (s == cc && c < nbj) xc = cmul(v[0], rd[c]);
+            xc = shfl_c(xc, base | cc);
+            if (s == cc) v[0] = xc;
+            if (s > cc) cfms(v[0], xc, T[(4 * b + s) * NBP + c]);
+#pragma unroll
+            for (int i = 1; i < LIVE; ++i)
+                if (b + i < 16) cfms(v[i], xc, T[(4 * (b + i) + s) * NBP + c]);
+        }
+#pragma unroll
+        for (int i = 0; i + 1 < 16; ++i) x[i] = x[i + 1];
+        x[15] = v[0];
+#pragma unroll
+        for (int i = 0; i + 1 < LIVE; ++i) v[i] = v[i + 1];
+        v[LIVE - 1] = czero<C>();
+    }
+}
+
+template <typename C>
+__device__ __forceinline__ void subst_row_upper_loop(C (&v)[16], const C *T, const C *rd, int nbj, int s) {
+    C x[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) x[i] = czero<C>();
+    subst_row_upper_blocks<C, 16>(v, x, T, rd, nbj, s, 0);
+    subst_row_upper_blocks<C, 12>(v, x, T, rd, nbj, s, 4);
+    subst_row_upper_blocks<C, 8>(v, x, T, rd, nbj, s, 8);
+    subst_row_upper_blocks<C, 4>(v, x, T, rd, nbj, s, 12);
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = x[i];
+}
+
+// T x = a (T unit lower) for one 64-long column vector shared by 4 lanes, the same result
+// as subst_col_lower1, right-looking in a loop whose body stays in the instruction cache:
+// entry r, once final, is broadcast to the group and subtracted from the later entries;
+// after each block of four entries the pending ones shift down a register and the solved
+// ones into x.  Phase p (blocks 4 p .. 4 p + 3) keeps 16 - 4 p pending registers.
+template <typename C, int LIVE>
+__device__ __forceinline__ void subst_col_lower1_blocks(C (&v)[16], C (&x)[16], const C *T, int s, int b0) {
+    const int base = (int)(threadIdx.x & 31u) & ~3;
+#pragma unroll 1
+    for (int b = b0; b < b0 + 4; ++b) {
+#pragma unroll
+        for (int cc = 0; cc < 4; ++cc) {
+            const int r = 4 * b + cc;
+            const C xr = shfl_c(v[0], base | cc);
+            if (s > cc) cfms(v[0], xr, T[r * NBP + 4 * b + s]);
+#pragma unroll
+            for (int i = 1; i < LIVE; ++i)
+                if (b + i < 16) cfms(v[i], xr, T[r * NBP + 4 * (b + i) + s]);
+        }
+#pragma unroll
+        for (int i = 0; i + 1 < 16; ++i) x[i] = x[i + 1];
+        x[15] = v[0];
+#pragma unroll
+        for (int i = 0; i + 1 < LIVE; ++i) v[i] = v[i + 1];
+        v[LIVE - 1] = czero<C>();
+    }
+}
+template <typename C>
+__device__ __forceinline__ void subst_col_lower1_loop(C (&v)[16], const C *T, int s) {
+    C x[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) x[i] = czero<C>();
+    subst_col_lower1_blocks<C, 16>(v, x, T, s, 0);
+    subst_col_lower1_blocks<C, 12>(v, x, T, s, 4);
+    subst_col_lower1_blocks<C, 8>(v, x, T, s, 8);
+    subst_col_lower1_blocks<C, 4>(v, x, T, s, 12);
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = x[i];
+}
+
+// T x = a (T upper, rd its reciprocal diagonal), the same result as subst_col_upper,
+// right-looking from the last entry down: the block being solved sits in v[15], pending
+// entries below it, and after each block everything shifts up a register (the solved entry
+// into x from the bottom).  Phase p (blocks 15 - 4 p .. 12 - 4 p) keeps 16 - 4 p registers.
+template <typename C, int LIVE>
+__device__ __forceinline__ void subst_col_upper_blocks(C (&v)[16], C (&x)[16], const C *T, const C *rd, int s,
+                                                       int b0) {
+    const int base = (int)(threadIdx.x & 31u) & ~3;
+#pragma unroll 1
+    for (int b = b0; b > b0 - 4; --b) {
+#pragma unroll
+        for (int cc = 3; cc >= 0; --cc) {
+            const int r = 4 * b + cc;
+            C xr = czero<C>();
+            if (s == cc) xr = cmul(v[15], rd[r]);
+            xr = shfl_c(xr, base | cc);
+            if (s == cc) v[15] = xr;
+            if (s < cc) cfms(v[15], xr, T[r * NBP + 4 * b + s]);
+#pragma unroll
+            for (int i = 16 - LIVE; i < 15; ++i)
+                if (b - 15 + i >= 0) cfms(v[i], xr, T[r * NBP + 4 * (b - 15 + i) + s]);
+        }
+#pragma unroll
+        for (int i = 15; i > 0; --i) x[i] = x[i - 1];
+        x[0] = v[15];
+#pragma unroll
+        for (int i = 15; i > 16 - LIVE; --i) v[i] = v[i - 1];
+        v[16 - LIVE] = czero<C>();
+    }
+}
+template <typename C>
+__device__ __forceinline__ void subst_col_upper_loop(C (&v)[16], const C *T, const C *rd, int s) {
+    C x[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) x[i] = czero<C>();
+    subst_col_upper_blocks<C, 16>(v, x, T, rd, s, 15);
+    subst_col_upper_blocks<C, 12>(v, x, T, rd, s, 11);
+    subst_col_upper_blocks<C, 8>(v, x, T, rd, s, 7);
+    subst_col_upper_blocks<C, 4>(v, x, T, rd, s, 3);
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = x[i];
+}
+
 // Stage the nbj x nbj diagonal block at (j, j) into smem T (padded, zero outside) and
 // the reciprocals of its diagonal into rd (1 outside).
 // Sixteen loads per thread are in flight before their stores: a 64-thread CTA stages the
@@ -476,7 +607,7 @@ __device__ __forceinline__ void panel_apply_cta(int n, C *A, int64_t lda, int j,
             }
             v[i] = x;
         }
-        subst_row_upper(v, T, rd, nbj, s);
+        subst_row_upper_loop(v, T, rd, nbj, s);
         if (ok) {
 #pragma unroll
             for (int i = 0; i < 16; ++i) {
@@ -513,7 +644,7 @@ __device__ __forceinline__ void panel_apply_cta(int n, C *A, int64_t lda, int j,
             }
             v[i] = x;
         }
-        subst_col_lower1(v, T, nbj, s);
+        subst_col_lower1_loop(v, T, s);
         if (ok) {
 #pragma unroll
             for (int i = 0; i < 16; ++i) {
@@ -667,8 +798,8 @@ k_trsm_diag(int nrhs, const C *__restrict__ LU, int64_t lda, C *B, int64_t ldb, 
         const int r = 4 * i + s;
         v[i] = (ok && r < nbj) ? B[(int64_t)col * ldb + j + r] : czero<C>();
     }
-    if (UPPER) subst_col_upper(v, T, rd, nbj, s);
-    else subst_col_lower1(v, T, nbj, s);
+    if (UPPER) subst_col_upper_loop(v, T, rd, s);
+    else subst_col_lower1_loop(v, T, s);
     if (ok) {
 #pragma unroll
         for (int i = 0; i < 16; ++i) {

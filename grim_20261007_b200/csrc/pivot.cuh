@@ -735,7 +735,7 @@ k_panel_u_moves(int n, C *__restrict__ A, int64_t lda, int j, int nbj, const int
         const int r = 4 * i + s;
         v[i] = (ok && r < nbj) ? A[(int64_t)col * lda + j + r] : czero<C>();
     }
-    subst_col_lower1(v, T, nbj, s);
+    subst_col_lower1_loop(v, T, s);
     if (ok) {
 #pragma unroll
         for (int i = 0; i < 16; ++i) {

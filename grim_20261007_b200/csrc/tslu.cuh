@@ -272,54 +272,6 @@ k_tslu_tree(int n, const C *__restrict__ A, int64_t lda, int j, int nbj, int *__
     if (lane == 0) *swapped = cntm > 0;
 }
 
-// x U = a for one 64-long row vector shared by 4 consecutive lanes (sub-lane s owns the
-// entries p = 4 i + s, i < 16, in v[i]; T is U in shared memory, leading dim NBP, rd its
-// reciprocal diagonal, entries past nbj zero with rd = 1).  The same result as
-// subst_row_upper, computed right-looking as a loop whose body stays in the instruction
-// cache: each column's value, once final, is broadcast to the group and subtracted from the
-// later entries; after each block of four columns the pending entries shift down one
-// register and the solved ones into x, so every register index is a compile-time constant.
-// Phase p (blocks 4 p .. 4 p + 3) keeps 16 - 4 p pending registers.
-template <typename C, int LIVE>
-__device__ __forceinline__ void subst_row_upper_blocks(C (&v)[16], C (&x)[16], const C *T, const C *rd, int nbj,
-                                                       int s, int b0) {
-    const int base = (int)(threadIdx.x & 31u) & ~3;
-#pragma unroll 1
-    for (int b = b0; b < b0 + 4; ++b) {
-#pragma unroll
-        for (int cc = 0; cc < 4; ++cc) {
-            const int c = 4 * b + cc;
-            C xc = czero<C>();
-            if (s == cc && c < nbj) xc = cmul(v[0], rd[c]);
-            xc = shfl_c(xc, base | cc);
-            if (s == cc) v[0] = xc;
-            if (s > cc) cfms(v[0], xc, T[(4 * b + s) * NBP + c]);
-#pragma unroll
-            for (int i = 1; i < LIVE; ++i)
-                if (b + i < 16) cfms(v[i], xc, T[(4 * (b + i) + s) * NBP + c]);
-        }
-#pragma unroll
-        for (int i = 0; i + 1 < 16; ++i) x[i] = x[i + 1];
-        x[15] = v[0];
-#pragma unroll
-        for (int i = 0; i + 1 < LIVE; ++i) v[i] = v[i + 1];
-        v[LIVE - 1] = czero<C>();
-    }
-}
-
-template <typename C>
-__device__ __forceinline__ void subst_row_upper_loop(C (&v)[16], const C *T, const C *rd, int nbj, int s) {
-    C x[16];
-#pragma unroll
-    for (int i = 0; i < 16; ++i) x[i] = czero<C>();
-    subst_row_upper_blocks<C, 16>(v, x, T, rd, nbj, s, 0);
-    subst_row_upper_blocks<C, 12>(v, x, T, rd, nbj, s, 4);
-    subst_row_upper_blocks<C, 8>(v, x, T, rd, nbj, s, 8);
-    subst_row_upper_blocks<C, 4>(v, x, T, rd, nbj, s, 12);
-#pragma unroll
-    for (int i = 0; i < 16; ++i) v[i] = x[i];
-}
-
 // After k_tslu_tree: every panel row gets x = a inv(U11) (its original panel row a, one row
 // substitution x U11 = a per row, four lanes per row).  A row that is not a pivot row is
 // L21's row x, written to its final place (the row moves' destination, else its own
