@@ -830,8 +830,10 @@ __device__ __forceinline__ int gal_far_order(double kl_max, double ratio_min, in
 // e < f only on diagonal tiles.  One set of Hankel evaluations per pair gives both
 // orientations: E[e][f] and E[f][e].  min_order: the floor on the tile order (the TE rows'
 // W rule: 8, or 16 outside its calibration; 0 for TM).
+// Two CTAs per SM (at most 128 registers a thread): 16 warps hide the FP64 latency of the
+// Hankel evaluations better than 8 (the accumulators of the pair spill a few words).
 template <int POL, typename C>
-__global__ void __launch_bounds__(GAL_FAR_THREADS)
+__global__ void __launch_bounds__(GAL_FAR_THREADS, 2)
 k_gal_far(int ne, const double *__restrict__ elem, const int2 *__restrict__ nodes, double k, int min_order,
           C *__restrict__ E) {
     const int ti = blockIdx.y, tj = blockIdx.x;
