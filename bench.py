@@ -186,12 +186,14 @@ def run_bor(args):
         res[prec] = F
         out[prec] = {'seconds': dt, 'solves_per_s': 1.0 / dt, 'refinement_steps': tele['refinement_steps'],
                      'fp64_fallback_modes': tele.get('fp64_fallback_modes', 0),
+                     'fp64_fallback_mode_list': tele.get('fp64_fallback_mode_list', []),
                      'stage_seconds': tele.get('stage_seconds')}
     s64 = 4 * np.pi * np.abs(res['double']) ** 2
     s32 = 4 * np.pi * np.abs(res['mixed']) ** 2
     db = 10 * np.log10(np.maximum(s64, 1e-30))
     mask = db > db.max() - 40
     out['max_db_error_mixed_vs_fp64'] = float(np.max(np.abs(10 * np.log10(s32[mask] / s64[mask]))))
+    out['k_rho_max'] = float(k * np.max(gen[:, 0]))
     return out
 
 
@@ -523,6 +525,67 @@ def reference_parity(args, rank, k, amp64, amp32):
     return out
 
 
+def own_gemm_rates():
+    """Large square GEMMs through this build's own tensor-core kernels, as the compute
+    denominators of the solve arms (no library GEMM is timed): the FP64 DMMA kernel
+    (complex128 residual R = B - A X at n = nrhs = 4096, 550 GFLOP) and the split-TF32
+    tcgen05 kernel (complex64 C -= A B at 8192^3, 4.4 TFLOP algorithmic 8 M N K), CUDA
+    events, one warm-up call, median of three."""
+    import torch
+    from grim_20261007_b200.device import context, ptr
+    ctx = context()
+    out = {}
+    n = 4096
+    g = torch.Generator(device='cuda').manual_seed(0)
+    a = torch.randn((n, n), dtype=torch.complex128, device='cuda', generator=g)
+    x = torch.randn((n, n), dtype=torch.complex128, device='cuda', generator=g)
+    b = torch.randn((n, n), dtype=torch.complex128, device='cuda', generator=g)
+    r = torch.empty_like(b)
+
+    def timed(fn, reps=3):
+        fn()
+        torch.cuda.synchronize()
+        ms = []
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        return float(np.median(ms))
+
+    ms = timed(lambda: ctx.lib.grim_residual(ctx.h, n, n, ptr(a), n, 0, ptr(x), n, ptr(b), n, ptr(r), n, 0))
+    out['fp64_dmma'] = {'kernel': 'k_gemm_dmma', 'm_n_k': [n, n, n], 'ms': ms, 'tflops': 8.0 * n ** 3 / (ms * 1e-3) / 1e12,
+                        'nominal_fp64_tensor_tflops': 40.0}
+    del a, x, b, r
+    m = 8192
+    a = torch.randn((m, m), dtype=torch.complex64, device='cuda', generator=g)
+    bb = torch.randn((m, m), dtype=torch.complex64, device='cuda', generator=g)
+    c = torch.zeros((m, m), dtype=torch.complex64, device='cuda')
+    ms = timed(lambda: ctx.lib.grim_cgemm_sub(ctx.h, m, m, m, ptr(a), m, ptr(bb), m, ptr(c), m, 1))
+    out['split_tf32'] = {'kernel': 'k_tc_gemm', 'm_n_k': [m, m, m], 'ms': ms,
+                         'tflops': 8.0 * m ** 3 / (ms * 1e-3) / 1e12}
+    del a, bb, c
+    torch.cuda.empty_cache()
+    return out
+
+
+def fp64_roofline(prof64, rates):
+    """The FP64 arm's GEMM kernel against the same kernel's large-square rate and the
+    nominal FP64 tensor rate."""
+    d = prof64.get('k_gemm_dmma')
+    if not d or not rates or not rates.get('fp64_dmma', {}).get('tflops'):
+        return None
+    achieved = d['flops'] / (d['ms'] * 1e-3) / 1e12
+    big = rates['fp64_dmma']['tflops']
+    return {'kernel': 'k_gemm_dmma', 'launches': d['launches'], 'achieved': achieved, 'unit': 'TFLOP/s',
+            'peak_own_large_gemm': big, 'frac_of_own_large_gemm': achieved / big,
+            'peak_nominal': 40.0, 'frac_of_nominal': achieved / 40.0,
+            'note': 'algorithmic 8 M N K per complex GEMM launch; denominators: the same kernel at 4096^3 '
+                    '(measured here) and the nominal FP64 tensor rate (not measured: no library FP64 GEMM is timed)'}
+
+
 def kernel_roofline(prof):
     """Roofline of the kernel with the largest share of one profiled mixed step."""
     hbm, bf16, src = _peaks()
@@ -769,6 +832,8 @@ def main():
     prof = profile_step([ctx], lambda: step_serial('mixed'))
     prof64 = profile_step([ctx], lambda: step_serial('double'))
     roofline = kernel_roofline(prof)
+    rates = own_gemm_rates() if rank == 0 else None
+    roof64 = fp64_roofline(prof64, rates) if rates else None
 
     cpu_baseline = None
     if rank == 0 and world == 1 and args.cpu_sample > 0:
@@ -776,6 +841,7 @@ def main():
 
     if rank == 0:
         detail = {'telemetry_mixed': tele32, 'telemetry_fp64': tele64, 'kernel_profile_mixed': prof,
+                  'own_gemm_rates': rates,
                   'kernel_profile_fp64': prof64, 'serving': serving, 'bor_ogive': bor, 'frequency_sweep': sweep,
                   'far_block': farblk, 'autotune': autotune}
         detail_path = write_detail(detail)
@@ -797,6 +863,8 @@ def main():
                     'path': 'solve_monostatic_rcs_2d (public API), linear_precision("mixed")'},
             'gpu_launches': int(launches32),
             'roofline': roofline,
+            'roofline_fp64': roof64,
+            'own_gemm_rates': {k_: {'tflops': v_['tflops'], 'kernel': v_['kernel']} for k_, v_ in (rates or {}).items()},
             'top_kernels_mixed': top_kernels(prof),
             'serving': summarize(serving, ('requests', 'completed', 'solves_per_s', 'p50_ms', 'p99_ms', 'cache_hits')),
             'bor_ogive': summarize_bor(bor),

@@ -288,54 +288,55 @@ def _mirror_modes(dev, modes, Zs):
     return [i for (i, _o), (d, a) in zip(checks, vals) if np.isfinite(d) and d <= MIRROR_ASYMMETRY_MAX * a]
 
 
-def _solve_mirror_grouped(dev, modes, Zs, Vs, workers):
-    """FP64 solves of mirror-symmetric mode systems through their even and odd halves
-    (reference ``bor/factor.py:37`` ``MirrorSplit``): the halves of every mode in one grouped
-    LU (a quarter of the LU work), then per mode the split right-hand sides, two half
-    solves and the join, on the worker pool.  The modes were checked symmetric to
-    MIRROR_ASYMMETRY_MAX, so the halves are the system itself to rounding and no
+def _solve_mirror_grouped(dev, modes, Zs, Vs, workers, precision='double', tol=None):
+    """Solves of mirror-symmetric mode systems through their even and odd halves (reference
+    ``bor/factor.py:37`` ``MirrorSplit``): the halves of every mode (FP64) and the split
+    right-hand sides, one grouped solve of all halves (``grouped.solve_grouped``: a quarter
+    of the LU work; mixed: complex64 factors refined against the FP64 halves, a half whose
+    refinement stalls re-solved in FP64), then the join.  The modes were checked symmetric
+    to MIRROR_ASYMMETRY_MAX, so the halves are the system itself to rounding and no
     refinement against the full matrix is needed."""
-    from ..grouped import getrf_grouped
+    from ..grouped import solve_grouped
     ctx = context()
-    halves = []
-    for m, Z in zip(modes, Zs):
+    halves, rhs, args_of = [], [], []
+    for m, Z, V in zip(modes, Zs, Vs):
         mp = dev.mirror(m)
         n = int(Z.shape[0])
+        nrhs = int(V.shape[0])
         ke, ko = mp['k'] + mp['nfe'], mp['k'] + mp['nfo']
         He = torch.empty((ke, ke), dtype=torch.complex128, device='cuda')
         Ho = torch.empty((ko, ko), dtype=torch.complex128, device='cuda')
         _lib.check(ctx.lib.grim_bor_mirror_halves(ctx.h, n, ptr(Z), n, mp['k'], ptr(mp['p1']), ptr(mp['p2']),
                                                   ptr(mp['s']), mp['nfe'], ptr(mp['fe']), mp['nfo'], ptr(mp['fo']),
                                                   ptr(He), ptr(Ho)), 'grim_bor_mirror_halves')
+        args = (mp['k'], ptr(mp['p1']), ptr(mp['p2']), ptr(mp['s']), mp['nfe'], ptr(mp['fe']), mp['nfo'], ptr(mp['fo']))
+        Be = torch.empty((nrhs, ke), dtype=torch.complex128, device='cuda')
+        Bo = torch.empty((nrhs, ko), dtype=torch.complex128, device='cuda')
+        _lib.check(ctx.lib.grim_bor_mirror_split(ctx.h, nrhs, ptr(V), n, *args, ptr(Be), ptr(Bo)),
+                   'grim_bor_mirror_split')
         halves += [He, Ho]
-    ipivs, infos, piv = getrf_grouped(halves)
-    for i, inf in enumerate(infos):
-        if inf:
-            raise _lib.GrimError(_lib.GRIM_ERR_SINGULAR, f'mirror half {i % 2} of mode {modes[i // 2]} is exactly '
-                                                         f'singular (info={inf})')
-
-    def job(j):
-        def run():
-            c = context()
-            mp = dev.mirror(modes[j])
-            V = Vs[j]
-            nrhs, n = int(V.shape[0]), int(V.shape[1])
-            ke, ko = mp['k'] + mp['nfe'], mp['k'] + mp['nfo']
-            Be = torch.empty((nrhs, ke), dtype=torch.complex128, device='cuda')
-            Bo = torch.empty((nrhs, ko), dtype=torch.complex128, device='cuda')
-            args = (mp['k'], ptr(mp['p1']), ptr(mp['p2']), ptr(mp['s']), mp['nfe'], ptr(mp['fe']), mp['nfo'],
-                    ptr(mp['fo']))
-            _lib.check(c.lib.grim_bor_mirror_split(c.h, nrhs, ptr(V), n, *args, ptr(Be), ptr(Bo)),
-                       'grim_bor_mirror_split')
-            for H, ipv, B, order in ((halves[2 * j], ipivs[2 * j], Be, ke), (halves[2 * j + 1], ipivs[2 * j + 1], Bo, ko)):
-                _lib.check(c.lib.grim_zgetrs(c.h, order, nrhs, ptr(H), order, ptr(ipv), ptr(B), order), 'grim_zgetrs')
-            _lib.check(c.lib.grim_bor_mirror_join(c.h, nrhs, ptr(Be), ptr(Bo), *args, ptr(V), n),
-                       'grim_bor_mirror_join')
-            return {'precision_mode': _lib.PREC_FP64, 'pivoted_panels': piv[2 * j] + piv[2 * j + 1], 'grouped': True,
-                    'mirror_halves': [ke, ko]}
-        return run
-
-    return run_pool([job(j) for j in range(len(modes))], workers=workers)
+        rhs += [Be, Bo]
+        args_of.append((args, nrhs, n, ke, ko))
+    mixed = precision == 'mixed'
+    rhs0 = [b.clone() for b in rhs] if mixed else None
+    sts = solve_grouped(halves, rhs, precision=precision, tol=tol, stop='berr', workers=workers)
+    stalled = [i for i, st in enumerate(sts) if st.get('not_converged')]
+    if stalled:
+        redo = solve_grouped([halves[i] for i in stalled], [rhs0[i] for i in stalled], precision='double',
+                             workers=workers)
+        for i, st in zip(stalled, redo):
+            sts[i] = dict(st, fp64_fallback=True)
+            rhs[i] = rhs0[i]
+    out = []
+    for j, (args, nrhs, n, ke, ko) in enumerate(args_of):
+        _lib.check(ctx.lib.grim_bor_mirror_join(ctx.h, nrhs, ptr(rhs[2 * j]), ptr(rhs[2 * j + 1]), *args, ptr(Vs[j]), n),
+                   'grim_bor_mirror_join')
+        se, so = sts[2 * j], sts[2 * j + 1]
+        out.append({'precision_mode': se.get('precision_mode', _lib.PREC_FP64),
+                    'pivoted_panels': se.get('pivoted_panels', 0) + so.get('pivoted_panels', 0), 'grouped': True,
+                    'mirror_halves': [ke, ko], 'fp64_fallback': bool(se.get('fp64_fallback') or so.get('fp64_fallback')),
+                    'refinement_steps': max(int(se.get('refinement_steps', 0)), int(so.get('refinement_steps', 0)))})
+    return out
 
 
 def _solve_modes_grouped(dev, modes, th, precision, tol, workers):
@@ -361,12 +362,12 @@ def _solve_modes_grouped(dev, modes, th, precision, tol, workers):
         tol = ops2d.MIXED_RCS_TOL
     torch.cuda.synchronize()
     t1 = time.perf_counter()
-    mirrored = _mirror_modes(dev, modes, Zs) if precision == 'double' else []
+    mirrored = _mirror_modes(dev, modes, Zs)
     sts = [None] * len(modes)
     if mirrored:
         for i, st in zip(mirrored, _solve_mirror_grouped(dev, [modes[i] for i in mirrored],
                                                          [Zs[i] for i in mirrored], [Vs[i] for i in mirrored],
-                                                         workers)):
+                                                         workers, precision=precision, tol=tol)):
             sts[i] = st
     rest = [i for i in range(len(modes)) if sts[i] is None]
     if rest:
@@ -467,9 +468,10 @@ def solve_bor_device(points, k, thetas_deg, mmax, precision='double', tol=None, 
             amp += part
     tele = {'modes': 2 * mmax + 1, 'mode_systems_solved': len(modes), 'max_backward_error': 0.0,
             'refinement_steps': max(t['refinement_steps'] for _p, t in outs)}
-    fallbacks = sum(1 for _p, t in outs if t['fp64_fallback'])
+    fallbacks = [m for m, (_p, t) in zip(modes, outs) if t['fp64_fallback']]
     if fallbacks:
-        tele['fp64_fallback_modes'] = fallbacks
+        tele['fp64_fallback_modes'] = len(fallbacks)
+        tele['fp64_fallback_mode_list'] = fallbacks
     tele['stage_seconds'] = dict(modal_moments=t_moments, **(outs[0][1].get('stage_seconds') or {}))
     F = amp.cpu().numpy() * (-1j * k * ETA0 / (4.0 * np.pi))
     tele['n_unknowns'] = 2 * (dev.ne + 1)

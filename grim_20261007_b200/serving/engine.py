@@ -10,7 +10,9 @@
   overlap on the device.
 * A resident factor cache keeps the system matrix and its LU factors of recent 2-D
   geometries on the device, keyed by (geometry hash, k, polarization, precision); a
-  repeat geometry skips the fill and the factorization and only solves its angles.
+  repeat geometry skips the fill and the factorization and only solves its angles.  The
+  cache's bytes count against the budget at admission (unpinned entries are evicted to
+  make room), and a request admitted as a cache hit pins its entry until it ends.
 * ``stats()`` reports completed solves, solves/s and p50/p99 latency (arrival to result).
 
 Results do not depend on what else runs: every kernel's reductions have a fixed order
@@ -50,6 +52,7 @@ class Request:
         self.pol = ops.canonical_pol(polarization) if kind == '2d' else 'VV+HH'
         self.precision = precision
         self.n_modes = n_modes
+        self.pinned = None  # cache key this request pinned at admission
         self.arrival = None
         self.started = None
         self.finished = None
@@ -77,12 +80,18 @@ class Request:
 
 
 class FactorCache:
-    """LRU cache of resident 2-D system matrices and factors, bounded in bytes."""
+    """LRU cache of resident 2-D system matrices and factors, bounded in bytes.
+
+    An entry can be pinned by the requests that will read it (``pin`` / ``unpin``): pinned
+    entries are never evicted, so a request admitted as a cache hit finds its factors when
+    it runs.  ``used`` counts every resident entry's bytes; the engine's admission counts
+    them against its memory budget next to the running requests."""
 
     def __init__(self, capacity_bytes):
         self.capacity = int(capacity_bytes)
         self.used = 0
         self.items = collections.OrderedDict()
+        self.pins = collections.Counter()
         self.lock = threading.Lock()
         self.hits = 0
         self.misses = 0
@@ -101,16 +110,53 @@ class FactorCache:
             self.hits += 1
             return e
 
+    def pin(self, key):
+        """Pin a resident entry; returns False (nothing pinned) when it is not resident."""
+        with self.lock:
+            if key not in self.items:
+                return False
+            self.pins[key] += 1
+            return True
+
+    def unpin(self, key):
+        with self.lock:
+            self.pins[key] -= 1
+            if self.pins[key] <= 0:
+                del self.pins[key]
+
+    def _evict_to(self, limit):
+        # least recently used unpinned entries first, until used <= limit (lock held); nothing
+        # is evicted when the pinned entries alone exceed the limit
+        pinned = sum(e['bytes'] for k, e in self.items.items() if self.pins.get(k, 0) > 0)
+        if pinned > limit:
+            return False
+        for k in [k for k in self.items if self.pins.get(k, 0) == 0]:
+            if self.used <= limit:
+                break
+            old = self.items.pop(k)
+            self.used -= old['bytes']
+        return self.used <= limit
+
+    def shrink_to(self, limit):
+        """Evict unpinned entries until at most ``limit`` bytes stay resident; True if reached."""
+        with self.lock:
+            return self._evict_to(max(0, int(limit)))
+
     def put(self, key, entry, nbytes):
         with self.lock:
-            if nbytes > self.capacity:
+            if nbytes > self.capacity or key in self.items:
                 return
-            while self.used + nbytes > self.capacity and self.items:
-                _k, old = self.items.popitem(last=False)
-                self.used -= old['bytes']
+            if not self._evict_to(self.capacity - nbytes):
+                return  # the rest is pinned: do not exceed the capacity
             entry['bytes'] = nbytes
             self.items[key] = entry
             self.used += nbytes
+
+
+def admission_fits(in_use, est, cache_used, budget, running):
+    """The engine's admission rule: a request fits when the running requests' estimates, its
+    own and the resident factor cache stay within the budget, or when nothing else runs."""
+    return in_use + est + cache_used <= budget or running == 0
 
 
 class _Slot:
@@ -187,11 +233,21 @@ class ServingEngine:
 
     # ------------------------------------------------------------------ scheduling
     def _take(self):
-        """Admit the oldest pending request that fits next to the running ones."""
-        for i, (req, fut, est) in enumerate(self.pending):
-            if self.in_use + est <= self.budget or self.running == 0:
+        """Admit the oldest pending request that fits next to the running ones and the
+        resident factor cache (unpinned cache entries are evicted to make room).  A request
+        whose factors are resident is estimated without them and pins them until it ends."""
+        for i, (req, fut, _est) in enumerate(self.pending):
+            key = req.cache_key()
+            cached = self.cache.pin(key)
+            est = req.estimate_bytes(cached=cached)
+            if not admission_fits(self.in_use, est, self.cache.used, self.budget, self.running):
+                self.cache.shrink_to(self.budget - self.in_use - est)
+            if admission_fits(self.in_use, est, self.cache.used, self.budget, self.running):
                 del self.pending[i]
+                req.pinned = key if cached else None
                 return req, fut, est
+            if cached:
+                self.cache.unpin(key)
         return None
 
     def _worker(self, slot):
@@ -218,6 +274,9 @@ class ServingEngine:
                 req.finished = time.perf_counter()
                 fut.set_exception(exc)
             finally:
+                if getattr(req, 'pinned', None) is not None:
+                    self.cache.unpin(req.pinned)
+                    req.pinned = None
                 with self.cv:
                     self.in_use -= est
                     self.running -= 1
