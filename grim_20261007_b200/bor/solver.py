@@ -238,6 +238,28 @@ class BorDevice:
         return V
 
 
+# Mixed precision pays on a mode system only when its LU dominates and complex64 can resolve
+# it: measured on the 400-segment ogive (k rho_max = 25, mode orders ~800, halves ~400), the
+# complex64 refinement stalls for every |m| >= 18 = 0.72 k rho_max (their FP64 re-solve then
+# doubles the work), and below that the complex64 grouped LU with its refinement takes longer
+# than the FP64 LU of the same small systems (64 ms against 24 ms for all 41 modes).  So a
+# mixed-precision request solves a mode in complex64 with FP64 refinement only when its
+# system has at least MIXED_MIN_ORDER unknowns and |m| < MIXED_MODE_FRACTION k rho_max; the
+# others are solved in FP64 (the mixed -> double ladder still guards the rest).
+MIXED_MIN_ORDER = 1536
+MIXED_MODE_FRACTION = 0.7
+
+
+def mode_precision(dev, m, order, precision):
+    """The precision one mode system is solved in under the request's ``precision``."""
+    if precision != 'mixed':
+        return precision
+    krho = dev.k * float(np.max(dev.nodes[:, 0]))
+    if order < MIXED_MIN_ORDER or abs(m) >= MIXED_MODE_FRACTION * krho:
+        return 'double'
+    return 'mixed'
+
+
 def _solve_mode(dev, m, th, precision, tol, ctx=None):
     """One Fourier mode on ``ctx`` (default: the current device worker): assemble, excite,
     solve and project; returns (this mode's far-field contribution [2 nth], telemetry)."""
@@ -248,6 +270,7 @@ def _solve_mode(dev, m, th, precision, tol, ctx=None):
     tele = {'fp64_fallback': False}
     if tol is None:
         tol = ops2d.MIXED_RCS_TOL  # an RCS solve: the same refinement target as the 2-D RCS path
+    precision = mode_precision(dev, m, int(Z.shape[0]), precision)
     if precision == 'mixed':
         V0 = V.clone()
         try:
@@ -362,18 +385,21 @@ def _solve_modes_grouped(dev, modes, th, precision, tol, workers):
         tol = ops2d.MIXED_RCS_TOL
     torch.cuda.synchronize()
     t1 = time.perf_counter()
-    mirrored = _mirror_modes(dev, modes, Zs)
+    mirrored = set(_mirror_modes(dev, modes, Zs))
     sts = [None] * len(modes)
-    if mirrored:
-        for i, st in zip(mirrored, _solve_mirror_grouped(dev, [modes[i] for i in mirrored],
-                                                         [Zs[i] for i in mirrored], [Vs[i] for i in mirrored],
-                                                         workers, precision=precision, tol=tol)):
-            sts[i] = st
-    rest = [i for i in range(len(modes)) if sts[i] is None]
-    if rest:
-        for i, st in zip(rest, solve_grouped([Zs[i] for i in rest], [Vs[i] for i in rest], precision=precision,
-                                             tol=tol, stop='berr', workers=workers)):
-            sts[i] = st
+    precs = [mode_precision(dev, m, int(Zs[i].shape[0]), precision) for i, m in enumerate(modes)]
+    for prec in ('double', 'mixed'):
+        mine = [i for i in range(len(modes)) if precs[i] == prec]
+        mir = [i for i in mine if i in mirrored]
+        if mir:
+            for i, st in zip(mir, _solve_mirror_grouped(dev, [modes[i] for i in mir], [Zs[i] for i in mir],
+                                                        [Vs[i] for i in mir], workers, precision=prec, tol=tol)):
+                sts[i] = st
+        rest = [i for i in mine if i not in mirrored]
+        if rest:
+            for i, st in zip(rest, solve_grouped([Zs[i] for i in rest], [Vs[i] for i in rest], precision=prec,
+                                                 tol=tol, stop='berr', workers=workers)):
+                sts[i] = st
     torch.cuda.synchronize()
     t2 = time.perf_counter()
     # stalled refinements (ill-conditioned modes): the reference's ladder to the double LU,

@@ -4,7 +4,8 @@ Public API (same names, arguments and result-dict keys as the reference):
 
 * ``solve_monostatic_rcs_2d(geometry_snapshot, frequencies_ghz, elevations_deg, ...)``
   -- ``twod/solver.py:3193``: both co-polarised channels (VV = TE, HH = TM), samples
-  VV first then HH (``_merge_co_polarized_2d_results`` ``:2778``);
+  interleaved VV then HH per physical sample, ``co_solved_samples`` per channel
+  (``_merge_co_polarized_2d_results`` ``:2778``);
 * ``solve_monostatic_rcs_2d_single_polarization(...)`` -- ``twod/solver.py:1988``;
 * ``_solve_dense_gpu(a_eval, rhs_eval) -> (x, device_name)`` -- ``twod/solver.py:355``,
   the ``GHOST_DENSE_BACKEND=gpu`` hook (CuPy cuSOLVER there, libgrimgpu here);
@@ -588,8 +589,8 @@ def solve_monostatic_rcs_2d(geometry_snapshot, frequencies_ghz, elevations_deg, 
 
     The channels' systems (one per polarisation and frequency) are independent; they are
     solved together on the device worker pool, so one system's latency-bound
-    factorization steps overlap another's tensor-core updates.  Samples and metadata
-    are those of the two single-polarisation solves, VV first.
+    factorization steps overlap another's tensor-core updates.  The result has the
+    reference's co-polarised shape (``_merge_co_polarized``).
     """
     channels_by_pol = _sweep(geometry_snapshot, frequencies_ghz, elevations_deg,
                              [pol for _export, pol in _CO_POLARIZED_2D_CHANNELS], geometry_units, progress_callback,
@@ -600,21 +601,81 @@ def solve_monostatic_rcs_2d(geometry_snapshot, frequencies_ghz, elevations_deg, 
               if not c['metadata']['quality_gate']['passed']]
     if strict_quality_gate and failed:
         raise ValueError('Quality gate failed: ' + '; '.join(failed))
-    samples = []
-    for export, _pol in _CO_POLARIZED_2D_CHANNELS:
-        for row in channels[export]['samples']:  # this call's own records: labelled in place
+    return _merge_co_polarized(channels)
+
+
+def _merge_co_polarized(channels, extra_metadata=None):
+    """The co-polarised result in the reference's shape (``twod/solver.py:2778``
+    ``_merge_co_polarized_2d_results``): ``samples`` interleave VV then HH per physical
+    sample (in the VV channel's order), each row labelled with its export and internal
+    polarisation; ``co_solved_samples`` keeps the two channels; the metadata carries the
+    channel metadata, the VV/HH mapping and the combined quality gate."""
+    co_solved = {}
+    for export, internal in _CO_POLARIZED_2D_CHANNELS:
+        rows = channels[export]['samples']  # this call's own records: labelled in place
+        for row in rows:
             row['polarization'] = export
-        samples.extend(channels[export]['samples'])
-    metadata = {'channels': {k: v['metadata'] for k, v in channels.items()},
-                'polarizations': [c[0] for c in _CO_POLARIZED_2D_CHANNELS]}
+            row['polarization_internal'] = internal
+        co_solved[export] = rows
+
+    def key(row):
+        return float(row['frequency_ghz']), float(row['theta_inc_deg']), float(row['theta_scat_deg'])
+
+    partners = {key(row): row for row in co_solved['HH']}
+    if set(partners) != {key(row) for row in co_solved['VV']}:
+        raise ValueError('TE/TM 2-D solves did not return the same physical grid.')
+    samples = []
+    for row in co_solved['VV']:
+        samples.append(row)
+        samples.append(partners[key(row)])
+    labels = [c[0] for c in _CO_POLARIZED_2D_CHANNELS]
+    meta = {k: channels[k]['metadata'] for k in labels}
+    gates = {k: dict(m.get('quality_gate', {}) or {}) for k, m in meta.items()}
+    passed = all(bool(g.get('passed', False)) for g in gates.values())
+
+    def worst(name, default=0.0):
+        vals = [float(m[name]) for m in meta.values() if name in m and math.isfinite(float(m[name]))]
+        return max(vals) if vals else default
+
+    metadata = {
+        'polarizations': labels,
+        'polarization_internal': [c[1] for c in _CO_POLARIZED_2D_CHANNELS],
+        'polarization_mapping': {'VV': 'TE', 'HH': 'TM'},
+        'formulation': 'co-polarized 2-D BIE/MoM',
+        'formulations': {k: m.get('formulation', '') for k, m in meta.items()},
+        'panel_count_min': int(worst('panel_count_min')),
+        'panel_count_max': int(worst('panel_count_max')),
+        'residual_norm_max': worst('residual_norm_max'),
+        'constraint_residual_norm_max': worst('constraint_residual_norm_max'),
+        'condition_est_max': worst('condition_est_max', float('nan')),
+        'condition_est_computed': all(bool(m.get('condition_est_computed', False)) for m in meta.values()),
+        'warnings': [w for m in meta.values() for w in (m.get('warnings', []) or [])],
+        'quality_gate': {'passed': passed, 'channels': gates,
+                         'reason': ('Both VV<-TE and HH<-TM discrete linear-system quality gates passed' if passed
+                                    else 'At least one co-polarized 2-D channel failed its quality gate')},
+        'channel_metadata': meta,
+        'channels': meta,
+        'amplitude_version': RCS_AMPLITUDE_VERSION,
+        'co_solve_shared_discretization': True,
+        'linear_backend': 'gpu_grim',
+        'dense_gpu_solve_count': int(sum(int(m.get('dense_gpu_solve_count', 0)) for m in meta.values())),
+        'dense_cpu_solve_count': 0,
+        'dense_gpu_devices': sorted({d for m in meta.values() for d in (m.get('dense_gpu_devices', []) or [])}),
+        'dense_largest_system': int(worst('dense_largest_system')),
+    }
+    if extra_metadata:
+        metadata.update(extra_metadata)
     return {
         'solver': '2d_bie_mom_rcs',
         'scattering_mode': 'monostatic',
         'amplitude_convention': RCS_AMPLITUDE_CONVENTION,
         'amplitude_version': RCS_AMPLITUDE_VERSION,
-        'polarization': 'VV+HH',
-        'polarization_export': 'VV+HH',
+        'rcs_log_unit': 'dBke',
+        'rcs_linear_quantity': 'sigma_2d',
+        'polarizations': labels,
+        'polarization_mapping': {'VV': 'TE', 'HH': 'TM'},
         'samples': samples,
+        'co_solved_samples': co_solved,
         'metadata': metadata,
     }
 
@@ -687,22 +748,6 @@ def solve_monostatic_rcs_2d_certified(geometry_snapshot, frequencies_ghz, elevat
                                  progress_callback, mesh_convergence_policy, max_panels, mesh_reference_ghz, 0.0,
                                  abort_event, quality_thresholds)
     channels = {export: by_pol[pol] for export, pol in _CO_POLARIZED_2D_CHANNELS}
-    samples = []
-    for export, _pol in _CO_POLARIZED_2D_CHANNELS:
-        for row in channels[export]['samples']:
-            row['polarization'] = export
-        samples.extend(channels[export]['samples'])
-    metadata = {'channels': {k: v['metadata'] for k, v in channels.items()},
-                'polarizations': [c[0] for c in _CO_POLARIZED_2D_CHANNELS],
-                'mesh_convergence_certified': True, 'certified_entry_point': True, 'published_mesh': 'fine',
-                'certification_solve_order': ['base_TE', 'base_TM', 'fine_TE', 'fine_TM']}
-    return {
-        'solver': '2d_bie_mom_rcs',
-        'scattering_mode': 'monostatic',
-        'amplitude_convention': RCS_AMPLITUDE_CONVENTION,
-        'amplitude_version': RCS_AMPLITUDE_VERSION,
-        'polarization': 'VV+HH',
-        'polarization_export': 'VV+HH',
-        'samples': samples,
-        'metadata': metadata,
-    }
+    return _merge_co_polarized(channels, {'mesh_convergence_certified': True, 'certified_entry_point': True,
+                                          'published_mesh': 'fine',
+                                          'certification_solve_order': ['base_TE', 'base_TM', 'fine_TE', 'fine_TM']})

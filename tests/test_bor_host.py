@@ -102,3 +102,15 @@ def test_validate_generatrix_rules():
     dup = np.vstack([pts[:3], pts[2:]])
     with pytest.raises(ValueError):
         B.validate_generatrix(dup)
+
+
+def test_mixed_requests_pick_the_precision_per_mode():
+    """Mixed precision only for mode systems of at least MIXED_MIN_ORDER unknowns below
+    MIXED_MODE_FRACTION k rho_max; FP64 requests stay FP64."""
+    from types import SimpleNamespace
+    from grim_20261007_b200.bor import solver as bs
+    dev = SimpleNamespace(k=25.0, nodes=np.array([[0.0, 1.0], [1.0, 0.0], [0.0, -1.0]]))
+    assert bs.mode_precision(dev, 3, 4000, 'double') == 'double'
+    assert bs.mode_precision(dev, 3, 4000, 'mixed') == 'mixed'
+    assert bs.mode_precision(dev, 18, 4000, 'mixed') == 'double'   # >= 0.7 k rho_max
+    assert bs.mode_precision(dev, 3, 800, 'mixed') == 'double'     # below the order threshold

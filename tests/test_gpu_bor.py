@@ -195,13 +195,17 @@ def test_signed_mode_symmetry_matches_all_modes():
 
 
 @pytest.mark.parametrize('precision', ['double', 'mixed'])
-def test_grouped_modes_match_per_mode_solves(precision):
+def test_grouped_modes_match_per_mode_solves(precision, monkeypatch):
     """The mode systems factored by one grouped LU give the same far field as each mode
-    factored on its own (identical factors, or for FP64 on this mirror-symmetric ogive the
-    even/odd halves; the mixed refinement stops at the same backward-error target)."""
+    factored on its own (identical factors, or on this mirror-symmetric ogive the even/odd
+    halves; the mixed refinement stops at the same backward-error target).  Mixed: every
+    mode is forced onto the complex64 path, whatever its order."""
     if not torch.cuda.is_available():
         pytest.skip('no CUDA device')
+    from grim_20261007_b200.bor import solver as bs
     from grim_20261007_b200.bor.solver import solve_bor_device
+    monkeypatch.setattr(bs, 'MIXED_MIN_ORDER', 0)
+    monkeypatch.setattr(bs, 'MIXED_MODE_FRACTION', 1e9)
     gen, _length, _half = S.ogive_case(8, n=60)
     k = 10.0 / float(np.max(gen[:, 0]))
     th = np.arange(0.0, 180.5, 5.0)

@@ -333,3 +333,27 @@ def test_tournament_pivoting_meets_the_gate_on_the_airfoil(ctx, pol):
     assert float((xt - xp).abs().max()) <= 1e-10 * scale
     ops.solve_inplace(z, xm, 'mixed', tol=1e-12, stop='berr', pivot='tournament', tuned=False)
     assert float((xm - xp).abs().max()) <= 1e-9 * scale
+
+
+def test_public_results_export_to_grim(ctx, tmp_path):
+    """A co-polarised and a single-polarisation solve of the C1 cylinder export to `.grim`
+    (the reference's archive format) and read back with their own amplitudes."""
+    from grim_20261007_b200 import grimfile
+    from grim_20261007_b200.twod.solver import (solve_monostatic_rcs_2d,
+                                                solve_monostatic_rcs_2d_single_polarization as solve1)
+    snap = S.snapshot_from_polygons([S.circle(1.0, 200)])
+    ang = list(np.arange(0.0, 360.0, 10.0))
+    both = solve_monostatic_rcs_2d(snap, [0.4, 0.5], ang, geometry_units='meters')
+    path = grimfile.export_result_to_grim(both, str(tmp_path / 'co'))[0]
+    back = grimfile.load_grim_npz(path)
+    assert list(back['polarizations']) == ['VV', 'HH'] and back['rcs_amp_real'].shape == (36, 1, 2, 2)
+    for p, pol in enumerate(('VV', 'HH')):
+        rows = [r for r in both['samples'] if r['polarization'] == pol]
+        for r in rows:
+            i = ang.index(r['theta_scat_deg'])
+            j = [0.4, 0.5].index(r['frequency_ghz'])
+            assert back['rcs_amp_real'][i, 0, j, p] == r['rcs_amp_real']
+            assert back['rcs_amp_imag'][i, 0, j, p] == r['rcs_amp_imag']
+    one = solve1(snap, [0.4], ang, 'TM', geometry_units='meters')
+    back1 = grimfile.load_grim_npz(grimfile.export_result_to_grim(one, str(tmp_path / 'tm.grim'), format_version=1)[0])
+    assert list(back1['polarizations']) == ['HH'] and back1['rcs_power'].dtype == np.float32

@@ -150,7 +150,7 @@ def _api_worker(rank, world, port, out):
 def test_public_2d_solve_splits_its_systems_over_two_gloo_ranks():
     """shard_over_ranks: each rank solves only its LPT share of the 10 (polarisation,
     frequency) systems, and both ranks return the same full result, in frequency order
-    per channel (VV then HH)."""
+    (VV then HH for each physical sample)."""
     import torch.multiprocessing as mp
     ctx = mp.get_context('spawn')
     q = ctx.Queue()
@@ -169,7 +169,8 @@ def test_public_2d_solve_splits_its_systems_over_two_gloo_ranks():
     assert not (s0 & s1) and len(s0) + len(s1) == 10 and s0 and s1
     assert got[0][1] == got[1][1]
     freqs = [0.5, 1.0, 1.5, 2.0, 2.5]
-    assert [(p, f) for p, f, _a in got[0][1]] == [(p, f) for p in ('VV', 'HH') for f in freqs for _e in (0, 1)]
+    # the reference's co-polarised order: VV then HH for each physical sample
+    assert [(p, f) for p, f, _a in got[0][1]] == [(p, f) for f in freqs for _e in (0, 1) for p in ('VV', 'HH')]
     # every system's samples come from the rank that solved it
     pol_of = {'VV': 'TE', 'HH': 'TM'}
     for p, f, a in got[0][1]:
