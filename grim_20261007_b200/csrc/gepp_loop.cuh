@@ -35,6 +35,7 @@
 template <typename C>
 struct GeppLCand {
     C piv;                   // the candidate's element in the step's column
+    C lp;                    // its pending multiplier (the previous step's)
     unsigned long long key;  // 0: no candidate
     int pos;                 // its current position in the panel
     int pad;
@@ -79,9 +80,13 @@ __device__ __forceinline__ int geppl_warp_best(unsigned long long key, int pos, 
     return bal ? __ffs(bal) - 1 : -1;
 }
 
-template <typename C, int H, int LIVE>
+// PUSH: every CTA pushes its candidate row (the live columns) into every CTA before the
+// cluster barrier, so the winner's row is read from local shared memory afterwards (crow:
+// [parity][rank][2 NB] elements of dynamic shared memory) instead of through a distributed
+// shared-memory load after it.
+template <typename C, int H, int LIVE, bool PUSH>
 __device__ __forceinline__ void geppl_col(GeppLRow<C> &st, GeppLShared<C> &sh, C *__restrict__ retired,
-                                          const GeppLCtx &cx, int t) {
+                                          C *__restrict__ crow, const GeppLCtx &cx, int t) {
     const int K = 2 * t + H;
     if (K >= cx.nbj) return;
     cg::cluster_group cluster = cg::this_cluster();
@@ -126,9 +131,19 @@ __device__ __forceinline__ void geppl_col(GeppLRow<C> &st, GeppLShared<C> &sh, C
     const int ow = ck != 0ull ? (2 * cslot) >> 5 : 0;
     if (cx.warp == ow) {
         const C piv = shfl_c(st.a[0], (2 * cslot + H) & 31);
+        const C plp = shfl_c(st.lp, (2 * cslot) & 31);
+        if (PUSH && ck != 0ull) {
+            // the row's live columns [2 t, 2 t + 2 LIVE) into every CTA's slot for this rank
+            __syncwarp();
+            for (int e = cx.lane; e < cx.cs * 2 * LIVE; e += 32) {
+                const int d = e / (2 * LIVE), c = 2 * t + e % (2 * LIVE);
+                *cluster.map_shared_rank(&crow[(H * 16 + cx.rank) * 2 * NB + c], d) = sh.pub[H][c];
+            }
+        }
         if (cx.lane < cx.cs) {
             GeppLCand<C> c;
             c.piv = piv;
+            c.lp = plp;
             c.key = ck;
             c.pos = cp;
             c.pad = 0;
@@ -161,8 +176,8 @@ __device__ __forceinline__ void geppl_col(GeppLRow<C> &st, GeppLShared<C> &sh, C
         const int c0 = cx.lane, c1 = cx.lane + 32;
         C x0 = czero<C>(), x1 = czero<C>();
         if (wr >= 0) {
-            const C *wrow = cluster.map_shared_rank(&sh.pub[H][0], wr);
-            const C wlp = *cluster.map_shared_rank(&sh.pub_lp[H], wr);
+            const C *wrow = PUSH ? crow + (H * 16 + wr) * 2 * NB : cluster.map_shared_rank(&sh.pub[H][0], wr);
+            const C wlp = PUSH ? sh.cand[H][wr].lp : *cluster.map_shared_rank(&sh.pub_lp[H], wr);
             if (c0 > K) {
                 x0 = wrow[c0];
                 if (K > 0) cfms(x0, wlp, uprev[c0]);
@@ -214,14 +229,14 @@ __device__ __forceinline__ void geppl_col(GeppLRow<C> &st, GeppLShared<C> &sh, C
     }
 }
 
-template <typename C, int LIVE>
+template <typename C, int LIVE, bool PUSH>
 __device__ __forceinline__ void geppl_phase(GeppLRow<C> &st, GeppLShared<C> &sh, C *__restrict__ retired,
-                                            const GeppLCtx &cx, int t0) {
+                                            C *__restrict__ crow, const GeppLCtx &cx, int t0) {
 #pragma unroll 1
     for (int t = t0; t < t0 + 8; ++t) {
         if (2 * t >= cx.nbj) return;  // the same in every thread
-        geppl_col<C, 0, LIVE>(st, sh, retired, cx, t);
-        geppl_col<C, 1, LIVE>(st, sh, retired, cx, t);
+        geppl_col<C, 0, LIVE, PUSH>(st, sh, retired, crow, cx, t);
+        geppl_col<C, 1, LIVE, PUSH>(st, sh, retired, crow, cx, t);
 #pragma unroll
         for (int q = 0; q + 1 < LIVE; ++q) st.a[q] = st.a[q + 1];
         st.a[LIVE - 1] = czero<C>();
@@ -230,10 +245,11 @@ __device__ __forceinline__ void geppl_phase(GeppLRow<C> &st, GeppLShared<C> &sh,
 
 // The panel (j, nbj) of A, rows j..n-1, on a cluster of gridDim.x CTAs, CTA c holding panel
 // rows [c rpc, (c + 1) rpc) (rpc <= GEPPL_ROWS).  Dynamic smem: NB * GEPPL_ROWS elements
-// (the retired columns, column-major by row slot).  Outputs as k_panel_gepp_reg: the factored
+// (the retired columns, column-major by row slot), then with PUSH 2 x 16 x 2 NB elements (the
+// pushed candidate rows).  Outputs as k_panel_gepp_reg: the factored
 // panel in place, ipiv (1-based, absolute), the first zero pivot in *info, *swapped, the
 // row moves, and (complex64, pk.a_hi) the trailing update's packed L21 operand.
-template <typename C>
+template <typename C, bool PUSH>
 __global__ void __launch_bounds__(GEPPL_THREADS, 1)
 k_panel_gepp_loop(int n, C *__restrict__ A, int64_t lda, int j, int nbj, int rpc, int *__restrict__ ipiv,
                   int *__restrict__ info, int *__restrict__ swapped, int *__restrict__ moves, PanelPack pk) {
@@ -241,6 +257,7 @@ k_panel_gepp_loop(int n, C *__restrict__ A, int64_t lda, int j, int nbj, int rpc
     __shared__ GeppLShared<C> sh;
     extern __shared__ __align__(16) unsigned char geppl_smem[];
     C *retired = reinterpret_cast<C *>(geppl_smem);
+    C *crow = retired + NB * GEPPL_ROWS;
     GeppLCtx cx;
     cx.tid = threadIdx.x;
     cx.lane = cx.tid & 31;
@@ -267,10 +284,10 @@ k_panel_gepp_loop(int n, C *__restrict__ A, int64_t lda, int j, int nbj, int rpc
     for (int e = cx.tid; e < NB * GEPPL_ROWS; e += GEPPL_THREADS) retired[e] = czero<C>();
     // every CTA's slots initialised before any CTA pushes into them
     cluster.sync();
-    geppl_phase<C, 32>(st, sh, retired, cx, 0);
-    geppl_phase<C, 24>(st, sh, retired, cx, 8);
-    geppl_phase<C, 16>(st, sh, retired, cx, 16);
-    geppl_phase<C, 8>(st, sh, retired, cx, 24);
+    geppl_phase<C, 32, PUSH>(st, sh, retired, crow, cx, 0);
+    geppl_phase<C, 24, PUSH>(st, sh, retired, crow, cx, 8);
+    geppl_phase<C, 16, PUSH>(st, sh, retired, crow, cx, 16);
+    geppl_phase<C, 8, PUSH>(st, sh, retired, crow, cx, 24);
     // every CTA has finished reading every other CTA's slots before any CTA exits; the rows'
     // final places may be in other CTAs' ranges, whose rows were all read at the start
     cluster.sync();

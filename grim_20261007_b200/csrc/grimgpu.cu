@@ -792,6 +792,18 @@ static bool gepp_loop_enabled() {
     return on;
 }
 
+// GRIM_GEPP_PUSH=1: candidate rows pushed into every CTA before the cluster barrier
+// (k_panel_gepp_loop PUSH).  Off by default: measured on the 2048-row panels it takes 132 us
+// against 119 us for reading only the winner's row through distributed shared memory after
+// the barrier (the pushes move 16 rows per CTA per column where the read moves one).
+static bool gepp_push_enabled() {
+    static const bool on = [] {
+        const char *e = getenv("GRIM_GEPP_PUSH");
+        return e && atoi(e) == 1;
+    }();
+    return on;
+}
+
 // Partial-pivoting factorization of the panel (j, nbj) of A on one thread-block cluster.
 template <typename C>
 static int gepp_launch(grim_context *h, int n, C *A, int64_t lda, int j, int nbj, int *ipiv, int *d_info,
@@ -800,13 +812,16 @@ static int gepp_launch(grim_context *h, int n, C *A, int64_t lda, int j, int nbj
     if (gepp_loop_enabled() && m <= 16 * GEPPL_ROWS) {
         const int cs = std::max(1, ceil_div(m, GEPPL_ROWS));
         const int rpc = ceil_div(m, cs);
-        const size_t smem = (size_t)NB * GEPPL_ROWS * sizeof(C);
+        const bool push = gepp_push_enabled();
+        const size_t smem = ((size_t)NB * GEPPL_ROWS + (push ? (size_t)2 * 16 * 2 * NB : 0)) * sizeof(C);
+        auto kern = push ? k_panel_gepp_loop<C, true> : k_panel_gepp_loop<C, false>;
         static PerDeviceOnce attr_loop;
         if (attr_loop.needed()) {
-            GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_panel_gepp_loop<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 (int)smem));
-            GRIM_CHECK_CUDA(
-                cudaFuncSetAttribute(k_panel_gepp_loop<C>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+            for (auto kf : {k_panel_gepp_loop<C, true>, k_panel_gepp_loop<C, false>}) {
+                const size_t sm = ((size_t)NB * GEPPL_ROWS + (size_t)2 * 16 * 2 * NB) * sizeof(C);
+                GRIM_CHECK_CUDA(cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+                GRIM_CHECK_CUDA(cudaFuncSetAttribute(kf, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+            }
             attr_loop.mark();
         }
         cudaLaunchConfig_t cfg = {};
@@ -821,8 +836,7 @@ static int gepp_launch(grim_context *h, int n, C *A, int64_t lda, int j, int nbj
         la[0].val.clusterDim.z = 1;
         cfg.attrs = la;
         cfg.numAttrs = 1;
-        GRIM_CHECK_CUDA(cudaLaunchKernelEx(&cfg, k_panel_gepp_loop<C>, n, A, lda, j, nbj, rpc, ipiv, d_info,
-                                           swapped, moves, pk));
+        GRIM_CHECK_CUDA(cudaLaunchKernelEx(&cfg, kern, n, A, lda, j, nbj, rpc, ipiv, d_info, swapped, moves, pk));
         return grim_launch_status(h, kname("k_panel_gepp_loop", sizeof(C)), 8.0 * m * nbj * nbj / 2.0, 0);
     }
     if (gepp_reg_enabled() && m <= 16 * GEPPR_ROWS) {
