@@ -114,8 +114,14 @@ def validate_primitives(a, b, seg_of, prim_of, names):
     tol = max(1e-8, 1e-6 * max(math.hypot(*span), 1.0))
     # vertices: weld endpoints within 1e-9 m into nodes
     key = np.round(pts / WELD_TOL).astype(np.int64)
-    _uniq, node = np.unique(key, axis=0, return_inverse=True)
-    node = node.reshape(-1)
+    # node of each endpoint: rows of key numbered in lexicographic order (np.unique(axis=0)
+    # numbers them the same way but sorts the rows as bytes, ten times slower)
+    order = np.lexsort((key[:, 1], key[:, 0]))
+    ks = key[order]
+    first_of_run = np.ones(len(ks), dtype=bool)
+    first_of_run[1:] = np.any(ks[1:] != ks[:-1], axis=1)
+    node = np.empty(len(ks), dtype=np.int64)
+    node[order] = np.cumsum(first_of_run) - 1
     nprim = len(a)
     feature = np.full(int(node.max()) + 1, np.inf)
     np.minimum.at(feature, node, np.concatenate([length, length]))
