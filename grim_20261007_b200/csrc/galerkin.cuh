@@ -245,31 +245,46 @@ __global__ void k_gal_near_list(int ne, const double *__restrict__ elem, const i
 //   P_nu = sum_m (-1)^m a_2m(nu) x^-2m, Q_nu = sum_m (-1)^m a_2m+1(nu) x^-2m-1 (DLMF 10.17.3),
 //   16 terms: the first omitted term is below 3e-16 of the sum at x = 25;
 //   below: CUDA's double-precision j0, y0, j1, y1.
-__device__ __forceinline__ void gal_hankel(double x, double k, double2 &g, double2 &hk) {
-    if (x >= GAL_X_ASYM) {
-        const double inv = 1.0 / x;
-        const double inv2 = inv * inv;
-        // Horner in inv2 from the highest even / odd coefficient down
-        double p0 = 0.0, q0 = 0.0, p1 = 0.0, q1 = 0.0;
+// Asymptotic branch with the first TERMS coefficients (TERMS even).
+template <int TERMS>
+__device__ __forceinline__ void gal_hankel_asym(double x, double k, double2 &g, double2 &hk) {
+    const double inv = 1.0 / x;
+    const double inv2 = inv * inv;
+    // Horner in inv2 from the highest even / odd coefficient down
+    double p0 = 0.0, q0 = 0.0, p1 = 0.0, q1 = 0.0;
 #pragma unroll
-        for (int m = GAL_ASYM64_TERMS / 2 - 1; m >= 0; --m) {
-            const double sg = (m & 1) ? -1.0 : 1.0;
-            p0 = fma(p0, inv2, sg * c_gal_a0[2 * m]);
-            q0 = fma(q0, inv2, sg * c_gal_a0[2 * m + 1]);
-            p1 = fma(p1, inv2, sg * c_gal_a1[2 * m]);
-            q1 = fma(q1, inv2, sg * c_gal_a1[2 * m + 1]);
-        }
-        q0 *= inv;
-        q1 *= inv;
-        double sx, cx;
-        sincos(x, &sx, &cx);
-        // C = sqrt(2/(pi x)) e^{-j(x - pi/4)}, e^{-j(x - pi/4)} = ((c + s) - j (s - c)) / sqrt(2)
-        const double amp = sqrt(inv * (1.0 / GRIM_PI));  // sqrt(2/(pi x)) / sqrt(2)
-        const double cr = amp * (cx + sx), ci = -amp * (sx - cx);
-        // g = (1/4)(Q0 + j P0) C ; hk = -(k/4)(P1 - j Q1) C
-        g = make_double2(0.25 * (q0 * cr - p0 * ci), 0.25 * (q0 * ci + p0 * cr));
-        const double kq = -0.25 * k;
-        hk = make_double2(kq * (p1 * cr + q1 * ci), kq * (p1 * ci - q1 * cr));
+    for (int m = TERMS / 2 - 1; m >= 0; --m) {
+        const double sg = (m & 1) ? -1.0 : 1.0;
+        p0 = fma(p0, inv2, sg * c_gal_a0[2 * m]);
+        q0 = fma(q0, inv2, sg * c_gal_a0[2 * m + 1]);
+        p1 = fma(p1, inv2, sg * c_gal_a1[2 * m]);
+        q1 = fma(q1, inv2, sg * c_gal_a1[2 * m + 1]);
+    }
+    q0 *= inv;
+    q1 *= inv;
+    double sx, cx;
+    sincos(x, &sx, &cx);
+    // C = sqrt(2/(pi x)) e^{-j(x - pi/4)}, e^{-j(x - pi/4)} = ((c + s) - j (s - c)) / sqrt(2)
+    const double amp = sqrt(inv * (1.0 / GRIM_PI));  // sqrt(2/(pi x)) / sqrt(2)
+    const double cr = amp * (cx + sx), ci = -amp * (sx - cx);
+    // g = (1/4)(Q0 + j P0) C ; hk = -(k/4)(P1 - j Q1) C
+    g = make_double2(0.25 * (q0 * cr - p0 * ci), 0.25 * (q0 * ci + p0 * cr));
+    const double kq = -0.25 * k;
+    hk = make_double2(kq * (p1 * cr + q1 * ci), kq * (p1 * ci - q1 * cr));
+}
+
+// G and its normal-derivative factor at x = k r.  Above GAL_X_ASYM the DLMF 10.17 expansion,
+// with as many terms as the argument needs for double precision (measured against SciPy's
+// Hankel functions, worst of orders 0 and 1: 16 terms 2.8e-15 at x = 25; 12 terms 3e-15 at
+// x = 35; 8 terms 8.5e-15 at x = 80, where the phase rounding already dominates); below it
+// CUDA's j0 / y0 / j1 / y1.
+__device__ __forceinline__ void gal_hankel(double x, double k, double2 &g, double2 &hk) {
+    if (x >= 80.0) {
+        gal_hankel_asym<8>(x, k, g, hk);
+    } else if (x >= 35.0) {
+        gal_hankel_asym<12>(x, k, g, hk);
+    } else if (x >= GAL_X_ASYM) {
+        gal_hankel_asym<GAL_ASYM64_TERMS>(x, k, g, hk);
     } else {
         const double j0v = j0(x), y0v = y0(x), j1v = j1(x), y1v = y1(x);
         // (j/4)(J0 - j Y0) = (Y0 + j J0)/4 ; (j/4) k (J1 - j Y1) = (k/4)(Y1 + j J1)

@@ -1023,7 +1023,8 @@ static int getrf_impl(grim_context *h, int n, C *A, int64_t lda, int *ipiv, int 
             wide_pending = false;
         }
         if (rest > 0) {
-            k_panel_u_moves<C><<<ceil_div(rest, NB), 256, tri, h->stream>>>(n, A, lda, j, nbj, moves, pk);
+            k_panel_u_moves<C><<<ceil_div(rest, UMOVES_THREADS / 4), UMOVES_THREADS, tri, h->stream>>>(n, A, lda, j,
+                                                                                                   nbj, moves, pk);
             status = grim_launch_status(h, kname("k_panel_u_moves", sizeof(C)), 8.0 * rest * nbj * nbj / 2.0, 0);
             if (status != GRIM_OK) break;
             status = trailing_update<C>(h, rest, nbj, A + (int64_t)j * lda + j + nbj, A + (int64_t)(j + nbj) * lda + j,

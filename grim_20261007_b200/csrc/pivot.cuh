@@ -684,12 +684,15 @@ k_panel_gepp_reg(int n, C *__restrict__ A, int64_t lda, int j, int nbj, int rpc,
     }
 }
 
-// U12 = inv(L11) A12 of the trailing columns after the panel's row moves: one CTA per 64
-// columns, 4 threads per column.  Each column gathers every move's source before writing
-// any destination.  complex64: also writes the trailing update's packed B operand.
-// Dynamic smem: NB * NBP + NB elements (the diagonal block and its reciprocals).
+// U12 = inv(L11) A12 of the trailing columns after the panel's row moves: one CTA per
+// blockDim.x / 4 columns (UMOVES_THREADS: 32 columns), 4 threads per column, so that the
+// 64-step substitution chains of a panel spread over about twice as many SMs as there are
+// 64-column blocks.  Each column gathers every move's source before writing any
+// destination.  complex64: also writes the trailing update's packed B operand.  Dynamic
+// smem: NB * NBP + NB elements (the diagonal block and its reciprocals).
+#define UMOVES_THREADS 128
 template <typename C>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(UMOVES_THREADS)
 k_panel_u_moves(int n, C *__restrict__ A, int64_t lda, int j, int nbj, const int *__restrict__ moves, PanelPack pk) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C *T = reinterpret_cast<C *>(smem_raw);
@@ -697,15 +700,16 @@ k_panel_u_moves(int n, C *__restrict__ A, int64_t lda, int j, int nbj, const int
     __shared__ int s_dst[GEPP_MAX_MOVES], s_src[GEPP_MAX_MOVES];
     __shared__ int s_cnt;
     const int t = threadIdx.x, s = t & 3, lane_vec = t >> 2;
+    const int cols_per_cta = (int)blockDim.x >> 2;
     if (t == 0) s_cnt = min(moves[0], GEPP_MAX_MOVES);
     __syncthreads();
     const int cnt = s_cnt;
-    for (int i = t; i < cnt; i += 256) {
+    for (int i = t; i < cnt; i += blockDim.x) {
         s_dst[i] = moves[1 + i];
         s_src[i] = moves[1 + GEPP_MAX_MOVES + i];
     }
     __syncthreads();
-    const int col = j + nbj + NB * blockIdx.x + lane_vec;
+    const int col = j + nbj + cols_per_cta * blockIdx.x + lane_vec;
     const bool ok = col < n;
     // every source of the column is read (by its 4 threads, one warp) before any destination
     // is written; the warp barriers stay outside the per-column condition, which differs
@@ -745,7 +749,7 @@ k_panel_u_moves(int n, C *__restrict__ A, int64_t lda, int j, int nbj, const int
     }
     if constexpr (sizeof(C) == sizeof(float2)) {
         if (pk.b_hi) {
-            const int nb_row = NB * blockIdx.x + lane_vec;
+            const int nb_row = cols_per_cta * blockIdx.x + lane_vec;
 #pragma unroll
             for (int i = 0; i < 16; ++i) {
                 const int r = 4 * i + s;
