@@ -226,9 +226,12 @@ def validate_winding(polygons, names):
                              f"{'clockwise' if want_cw else 'counter-clockwise'} so that its normals point into the air.")
 
 
-def contours_from_snapshot(snapshot, geometry_units='inches', wavelength=None, max_panels=20000):
+def contours_from_snapshot(snapshot, geometry_units='inches', wavelength=None, max_panels=20000, checks=None):
     """Return a list of closed polygons (vertex arrays, metres) ready for ``panel_geometry``,
-    after the reference's fatal geometry checks (``validate_primitives``, ``validate_winding``)."""
+    after the reference's fatal geometry checks (``validate_primitives``, ``validate_winding``).
+    With a list ``checks`` those two checks are not run here: a callable that runs them (and
+    raises their ValueError) is appended instead, for the caller to run alongside the solve
+    and before it returns anything."""
     scale = unit_scale(geometry_units)
     segs = list(snapshot.get('segments', []) or [])
     if not segs:
@@ -281,9 +284,15 @@ def contours_from_snapshot(snapshot, geometry_units='inches', wavelength=None, m
         polygons.append(poly)
         poly_names.append(names[-1])
     if prim_a:
-        validate_primitives(np.concatenate(prim_a), np.concatenate(prim_b), np.concatenate(seg_of),
-                            np.concatenate(prim_of), names)
-        validate_winding(polygons, poly_names)
+        args = (np.concatenate(prim_a), np.concatenate(prim_b), np.concatenate(seg_of), np.concatenate(prim_of), names)
+
+        def check(args=args, polygons=list(polygons), poly_names=list(poly_names)):
+            validate_primitives(*args)
+            validate_winding(polygons, poly_names)
+        if checks is None:
+            check()
+        else:
+            checks.append(check)
     return polygons
 
 

@@ -23,6 +23,7 @@ discretisation error).
 """
 from __future__ import annotations
 
+import concurrent.futures as cf
 import math
 import os
 import threading
@@ -265,12 +266,16 @@ class _MeshCache:
     """Meshes of one request, shared by the systems that use the same frequency (both
     polarisations of a co-polarised solve mesh the contour once)."""
 
-    def __init__(self, geometry_snapshot, geometry_units, max_panels, mesh_reference_ghz):
+    def __init__(self, geometry_snapshot, geometry_units, max_panels, mesh_reference_ghz, deferred_checks=False):
         self.args = (geometry_snapshot, geometry_units, max_panels, mesh_reference_ghz)
         self.lock = threading.Lock()
         self.locks = {}
         self.meshes = {}
         self.bodies = {}
+        # deferred_checks: the reference's geometry checks (they depend on the snapshot only) are
+        # not run while meshing; the first mesh keeps them in self.checks for the caller
+        self.deferred = bool(deferred_checks)
+        self.checks = []
 
     def galerkin_body(self, f):
         """The frequency's linear-Galerkin device body, built once and shared by both
@@ -293,7 +298,11 @@ class _MeshCache:
             if f not in self.meshes:
                 snapshot, units, max_panels, ref_ghz = self.args
                 mesh_lambda = C0 / (float(ref_ghz) * 1e9) if ref_ghz else C0 / (f * 1e9)
-                polys = geo.contours_from_snapshot(snapshot, units, mesh_lambda, max_panels)
+                pending = [] if self.deferred else None
+                polys = geo.contours_from_snapshot(snapshot, units, mesh_lambda, max_panels, checks=pending)
+                with self.lock:
+                    if pending and not self.checks:
+                        self.checks.extend(pending)
                 self.meshes[f] = (polys, geo.panel_geometry(polys))
             return self.meshes[f]
 
@@ -379,7 +388,8 @@ def _solve_frequencies_grouped(items, elevs, precision, abort_event, workers, co
 def _frequency_cost(geometry_snapshot, geometry_units, f, n_angles):
     """Relative cost of one frequency's system (N^3 + N^2 R, N from the panel density)."""
     try:
-        per = geo.contours_from_snapshot(geometry_snapshot, geometry_units, C0 / (f * 1e9), 10 ** 9)
+        # a cost estimate only: the geometry checks run once for the request elsewhere
+        per = geo.contours_from_snapshot(geometry_snapshot, geometry_units, C0 / (f * 1e9), 10 ** 9, checks=[])
         n = sum(len(p) for p in per)
     except Exception:  # noqa: BLE001 - a costing failure only changes the order
         n = 1
@@ -472,7 +482,16 @@ def _sweep_many(snapshots, frequencies_ghz, elevations_deg, pols, geometry_units
     require_gpu_dense_backend()
     require_cuda()
     precision = requested_precision()
-    mesh_list = [_MeshCache(snap, geometry_units, max_panels, mesh_reference_ghz) for snap in snapshots]
+    mesh_list = [_MeshCache(snap, geometry_units, max_panels, mesh_reference_ghz, deferred_checks=True)
+                 for snap in snapshots]
+    # each snapshot parsed and meshed here (its format errors raise now); the reference's geometry
+    # checks of every snapshot then run on a host thread while the systems are solved, and
+    # their error, if any, is raised before any result is returned
+    for meshes in mesh_list:
+        meshes.get(freqs[0])
+    checks = [c for meshes in mesh_list for c in meshes.checks]
+    check_pool = cf.ThreadPoolExecutor(max_workers=1) if checks else None
+    check_done = check_pool.submit(lambda: [c() for c in checks]) if checks else None
     items, jobs = [], []
     for si, meshes in enumerate(mesh_list):
         for pol in pols:
@@ -518,11 +537,18 @@ def _sweep_many(snapshots, frequencies_ghz, elevations_deg, pols, geometry_units
                         on_done=lambda li, o: on_done(idx[li], o))
 
     t0 = time.perf_counter()
-    if shard:
-        # this rank's LPT share of the systems, then every rank's host records
-        outs = sharding.run_sharded(costs, run_local, group)
-    else:
-        outs = run_local(range(len(items)))
+    try:
+        if shard:
+            # this rank's LPT share of the systems, then every rank's host records
+            outs = sharding.run_sharded(costs, run_local, group)
+        else:
+            outs = run_local(range(len(items)))
+    finally:
+        if check_done is not None:
+            try:
+                check_done.result()  # a geometry error takes precedence over anything the solve raised
+            finally:
+                check_pool.shutdown(wait=False)
     wall = time.perf_counter() - t0
     results = []
     for si in range(len(snapshots)):

@@ -184,3 +184,43 @@ def test_geometry_validation_is_cheap_on_the_headline_airfoil():
     t0 = time.perf_counter()
     geo.contours_from_snapshot(snap, 'meters')
     assert time.perf_counter() - t0 < 0.05
+
+
+def test_public_solve_raises_the_geometry_error_checked_beside_the_solve(monkeypatch):
+    """The reference's geometry checks run on a host thread while the systems are solved; a
+    rejected geometry still raises its ValueError from the public entry (before any result),
+    even when the solve itself fails on that geometry, and a valid one returns normally."""
+    from grim_20261007_b200.twod import solver
+
+    class _Ctx:
+        device_name = 'fake'
+
+    calls = []
+
+    def fake_solve(meshes, f, elevs, pol, precision, abort_event, condition=False):
+        calls.append((pol, f))
+        if fail['now']:
+            raise RuntimeError('solve failed')
+        samples = [{'frequency_ghz': f, 'theta_inc_deg': e, 'theta_scat_deg': e, 'rcs_linear': 1.0, 'rcs_db': 0.0,
+                    'rcs_amp_real': 1.0, 'rcs_amp_imag': 0.0, 'rcs_amp_phase_deg': 0.0, 'linear_residual': 1e-15}
+                   for e in elevs]
+        return dict(samples=samples, residuals=[1e-15] * len(elevs), event={'used': 'gpu_grim', 'n': 8}, n=8,
+                    seconds=0.0, condition_est=None)
+
+    fail = {'now': False}
+    monkeypatch.setenv('GRIM_SWEEP_WORKERS', '1')
+    monkeypatch.setenv('GRIM_GROUPED_SWEEP', '0')
+    monkeypatch.setattr(solver, '_solve_frequency', fake_solve)
+    monkeypatch.setattr(solver, 'require_cuda', lambda: None)
+    monkeypatch.setattr(solver, 'context', lambda: _Ctx())
+    t = 0.12458731811250179
+    cracked = _snap([S.naca_symmetric(t, 2048, closed_te=True)])
+    for failing in (False, True):
+        fail['now'] = failing
+        with pytest.raises(ValueError, match='Geometry crack'):
+            solver.solve_monostatic_rcs_2d_single_polarization(cracked, [1.0], [0.0, 10.0], 'TM',
+                                                               geometry_units='meters')
+    fail['now'] = False
+    good = solver.solve_monostatic_rcs_2d_single_polarization(_snap([S.naca_symmetric(t, 2048)]), [1.0, 2.0],
+                                                              [0.0, 10.0], 'TM', geometry_units='meters')
+    assert len(good['samples']) == 4 and ('TM', 2.0) in calls
