@@ -187,6 +187,9 @@ def run_bor(args):
         out[prec] = {'seconds': dt, 'solves_per_s': 1.0 / dt, 'refinement_steps': tele['refinement_steps'],
                      'fp64_fallback_modes': tele.get('fp64_fallback_modes', 0),
                      'fp64_fallback_mode_list': tele.get('fp64_fallback_mode_list', []),
+                     'max_backward_error': tele.get('max_backward_error'),
+                     'max_relative_residual': tele.get('max_relative_residual'),
+                     'gate_refined_modes': tele.get('gate_refined_modes', []),
                      'stage_seconds': tele.get('stage_seconds')}
     s64 = 4 * np.pi * np.abs(res['double']) ** 2
     s32 = 4 * np.pi * np.abs(res['mixed']) ** 2
@@ -633,8 +636,8 @@ def summarize_bor(bor):
            if k_ in bor}
     for prec in ('double', 'mixed'):
         if prec in bor:
-            out[prec] = {k_: bor[prec][k_] for k_ in ('seconds', 'solves_per_s', 'fp64_fallback_modes')
-                         if k_ in bor[prec]}
+            out[prec] = {k_: bor[prec][k_] for k_ in ('seconds', 'solves_per_s', 'fp64_fallback_modes',
+                                                      'max_backward_error') if k_ in bor[prec]}
     return out
 
 

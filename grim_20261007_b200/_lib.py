@@ -87,6 +87,8 @@ SIGNATURES = [
                                c_int64, c_int]),
     ('grim_residual', c_int, [c_void_p, c_int, c_int, c_void_p, c_int64, c_int, c_void_p, c_int64, c_void_p, c_int64,
                               c_void_p, c_int64, c_int]),
+    ('grim_solution_errors', c_int, [c_void_p, c_int, c_int, c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_int64,
+                                     c_void_p, c_int64, c_int, c_void_p, c_void_p, c_void_p]),
     ('grim_backward_error_noalloc', c_int, [c_void_p, c_int, c_int, c_void_p, c_int64, c_int, c_void_p, c_int64,
                                             c_void_p, c_int64, c_void_p]),
     ('grim_zgesv_mixed', c_int, [c_void_p, c_int, c_int, c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_int64,

@@ -105,6 +105,119 @@ def pole_map(nodes, m):
 MIRROR_NODE_TOLERANCE = 1e-9
 MIRROR_ASYMMETRY_MAX = 1e-12
 
+# The per-mode release gate (reference bor/solver.py constants, applied in bor/factor.py:302-355):
+# every mode solution is refined against its full FP64 matrix while its 2-norm relative
+# residual exceeds BOR_LINEAR_RESIDUAL_MAX or its normwise backward error exceeds
+# BOR_LINEAR_BACKWARD_ERROR_MAX, and a backward error still above the latter is an error.
+BOR_LINEAR_BACKWARD_ERROR_MAX = 1.0e-12
+BOR_LINEAR_RESIDUAL_MAX = 1.0e-8
+GATE_REFINEMENT_STEPS = 2
+GATE_SLICES = 8  # the gate's residual: int8 slices on the tensor cores at FP64 GEMM accuracy
+
+
+def solution_errors(Z, X, B, R, maxes, ctx=None, berr=None, relres=None):
+    """R = B - Z X and the release measures of the solution X (rows of the (nrhs, n) device
+    arrays are the right-hand sides): per-column backward error / 2-norm relative residual
+    into ``berr`` / ``relres`` when given, their maxima into the 2-element float64 device
+    view ``maxes`` (``grim_solution_errors``; reference bor/factor.py:289-300)."""
+    ctx = ctx or context()
+    n, nrhs = int(B.shape[1]), int(B.shape[0])
+    _lib.check(ctx.lib.grim_solution_errors(ctx.h, n, nrhs, ptr(Z), n, ptr(X), n, ptr(B), n, ptr(R), n, GATE_SLICES,
+                                            ptr(berr), ptr(relres), ptr(maxes)), 'grim_solution_errors')
+
+
+def release_limit(prec, tol):
+    """Backward error a mode solved in ``prec`` is released at without gate refinement: the
+    reference's limit for FP64, the refinement target ``tol`` (never tighter) for mixed."""
+    if prec == 'double':
+        return BOR_LINEAR_BACKWARD_ERROR_MAX
+    return max(float(tol), BOR_LINEAR_BACKWARD_ERROR_MAX)
+
+
+def gate_decision(berr, relres, limit):
+    """Whether a solution with these maxima is released as it stands."""
+    return bool(np.isfinite(berr) and np.isfinite(relres) and berr <= limit and relres <= BOR_LINEAR_RESIDUAL_MAX)
+
+
+def refinement_continues(prev, cand):
+    """The reference's stop rule (bor/factor.py:312-316): a refinement step is kept unless
+    neither the relative residual nor the backward error (``(berr, relres)`` maxima) fell."""
+    return not (cand[1] >= prev[1] and cand[0] >= prev[0])
+
+
+def _gate_modes(modes, Zs, Xs, B0s, precs, direct, tol, ctx=None):
+    """The per-mode release gate over solved mode systems, in place on ``Xs``.
+
+    ``Zs`` are the full FP64 mode matrices, ``B0s`` the right-hand sides and ``direct[i]``
+    says the solution came from the FP64 LU of the full matrix (not from the mirror halves
+    or a mixed-precision factor).  The residuals of all modes are measured first, then read
+    in one go.  A mode that misses the gate is factored (FP64, one grouped LU of all such
+    modes): a direct solution is refined from where it stands, any other one is replaced by
+    the LU solution (the reference's LU fallback for a mirror factor), then up to
+    GATE_REFINEMENT_STEPS refinement steps run under the reference's stop rule.  A mode
+    whose backward error still exceeds BOR_LINEAR_BACKWARD_ERROR_MAX raises RuntimeError.
+    Returns per-mode dicts (backward_error, relative_residual, gate_refinement_steps,
+    gate_lu_fallback)."""
+    from ..grouped import getrf_grouped
+    ctx = ctx or context()
+    count = len(modes)
+    if not count:
+        return []
+    size = max(int(B.numel()) for B in B0s)
+    scratch = torch.empty(size, dtype=torch.complex128, device='cuda')
+    maxes = torch.empty((count, 2), dtype=torch.float64, device='cuda')
+    for i in range(count):
+        R = scratch[:B0s[i].numel()].view(B0s[i].shape)
+        solution_errors(Zs[i], Xs[i], B0s[i], R, maxes[i], ctx=ctx)
+    vals = maxes.cpu().numpy()
+    out = [{'backward_error': float(vals[i, 0]), 'relative_residual': float(vals[i, 1]), 'gate_refinement_steps': 0}
+           for i in range(count)]
+    bad = [i for i in range(count) if not gate_decision(vals[i, 0], vals[i, 1], release_limit(precs[i], tol))]
+    if not bad:
+        return out
+    lus = [Zs[i].clone() for i in bad]
+    ipivs, infos, _piv = getrf_grouped(lus, ctx=ctx)
+    one = torch.empty(2, dtype=torch.float64, device='cuda')
+
+    def lu_solve(j, rhs):
+        n, nrhs = int(rhs.shape[1]), int(rhs.shape[0])
+        _lib.check(ctx.lib.grim_zgetrs(ctx.h, n, nrhs, ptr(lus[j]), n, ptr(ipivs[j]), ptr(rhs), n), 'grim_zgetrs')
+
+    def measure(i, X, R):
+        solution_errors(Zs[i], X, B0s[i], R, one, ctx=ctx)
+        b, r = one.cpu().numpy()
+        return float(b), float(r)
+
+    for j, i in enumerate(bad):
+        m = modes[i]
+        if infos[j]:
+            raise RuntimeError(f'BoR mode m={m} LU factorization failed (info={infos[j]}).')
+        if not direct[i]:
+            out[i]['gate_lu_fallback'] = ('mirror' if precs[i] == 'double' else 'mixed') + \
+                f' solution stopped at backward error {out[i]["backward_error"]:.3g}'
+            Xs[i].copy_(B0s[i])
+            lu_solve(j, Xs[i])
+        R, Rc = torch.empty_like(B0s[i]), torch.empty_like(B0s[i])
+        cur = measure(i, Xs[i], R)  # R: the residual of the current solution
+        for _step in range(GATE_REFINEMENT_STEPS):
+            if cur[0] <= BOR_LINEAR_BACKWARD_ERROR_MAX and cur[1] <= BOR_LINEAR_RESIDUAL_MAX:
+                break
+            cand = R.clone()
+            lu_solve(j, cand)
+            cand += Xs[i]
+            new = measure(i, cand, Rc)
+            if not refinement_continues(cur, new):
+                break
+            Xs[i].copy_(cand)
+            R, Rc = Rc, R
+            cur = new
+            out[i]['gate_refinement_steps'] += 1
+        out[i]['backward_error'], out[i]['relative_residual'] = cur
+        if not (np.isfinite(cur[0]) and np.isfinite(cur[1])) or cur[0] > BOR_LINEAR_BACKWARD_ERROR_MAX:
+            raise RuntimeError(f'BoR mode m={m} normwise linear backward error {cur[0]} exceeds the release limit '
+                               f'{BOR_LINEAR_BACKWARD_ERROR_MAX}.')
+    return out
+
 
 def mirror_map(nodes, m):
     """(target, sign) of the reduced unknowns of mode m when the generatrix is symmetric about
@@ -271,18 +384,20 @@ def _solve_mode(dev, m, th, precision, tol, ctx=None):
     if tol is None:
         tol = ops2d.MIXED_RCS_TOL  # an RCS solve: the same refinement target as the 2-D RCS path
     precision = mode_precision(dev, m, int(Z.shape[0]), precision)
+    V0 = V.clone()
     if precision == 'mixed':
-        V0 = V.clone()
         try:
             st = ops2d.solve_inplace(Z, V, 'mixed', tol=tol, ctx=ctx, stop='berr')
         except _lib.GrimNotConverged:
             # ill-conditioned mode: the reference's ladder falls back to the double LU
             tele['fp64_fallback'] = True
-            V = V0
+            V.copy_(V0)
+            precision = 'double'
             st = ops2d.solve_inplace(Z, V, 'double', ctx=ctx)
     else:
         st = ops2d.solve_inplace(Z, V, precision, tol=tol, ctx=ctx)
     tele['refinement_steps'] = int(st.get('refinement_steps', 0))
+    tele.update(_gate_modes([m], [Z], [V], [V0], [precision], [precision == 'double'], tol, ctx=ctx)[0])
     nth = int(th.numel())
     part = torch.zeros(2 * nth, dtype=torch.complex128, device='cuda')
     nred = int(Z.shape[0])
@@ -317,8 +432,9 @@ def _solve_mirror_grouped(dev, modes, Zs, Vs, workers, precision='double', tol=N
     right-hand sides, one grouped solve of all halves (``grouped.solve_grouped``: a quarter
     of the LU work; mixed: complex64 factors refined against the FP64 halves, a half whose
     refinement stalls re-solved in FP64), then the join.  The modes were checked symmetric
-    to MIRROR_ASYMMETRY_MAX, so the halves are the system itself to rounding and no
-    refinement against the full matrix is needed."""
+    to MIRROR_ASYMMETRY_MAX, so the halves are the system itself to rounding; the release
+    gate (``_gate_modes``) then checks every joined solution against the full matrix and
+    replaces one that misses it by the LU solution."""
     from ..grouped import solve_grouped
     ctx = context()
     halves, rhs, args_of = [], [], []
@@ -380,7 +496,7 @@ def _solve_modes_grouped(dev, modes, th, precision, tol, workers):
     parts = run_pool([prep(m) for m in modes], workers=workers)
     Zs = [p[0] for p in parts]
     Vs = [p[1] for p in parts]
-    V0s = [v.clone() for v in Vs] if precision == 'mixed' else None
+    V0s = [v.clone() for v in Vs]
     if tol is None:
         tol = ops2d.MIXED_RCS_TOL
     torch.cuda.synchronize()
@@ -412,12 +528,21 @@ def _solve_modes_grouped(dev, modes, th, precision, tol, workers):
             sts[i] = dict(st, fp64_fallback=True)
             Vs[i] = V0s[i]
     torch.cuda.synchronize()
-    stage = {'assembly': t1 - t0, 'grouped_factor_and_solves': t2 - t1, 'fp64_fallbacks': time.perf_counter() - t2}
+    t3 = time.perf_counter()
+    # the release gate against every full mode matrix: a solution from the FP64 LU of the
+    # full matrix is direct; mirror halves and mixed factors are not
+    fell_back = [bool(st.get('fp64_fallback')) for st in sts]
+    eff = ['double' if fb and i not in mirrored else precs[i] for i, fb in enumerate(fell_back)]
+    direct = [i not in mirrored and eff[i] == 'double' for i in range(len(modes))]
+    gate = _gate_modes(modes, Zs, Vs, V0s, eff, direct, tol)
+    torch.cuda.synchronize()
+    stage = {'assembly': t1 - t0, 'grouped_factor_and_solves': t2 - t1, 'fp64_fallbacks': t3 - t2,
+             'release_gate': time.perf_counter() - t3}
     ctx = context()
     nth = int(th.numel())
     outs = []
     for i, st in enumerate(sts):
-        tele = {'fp64_fallback': bool(st.get('fp64_fallback')), 'grouped': True, 'stage_seconds': stage}
+        tele = {'fp64_fallback': fell_back[i], 'grouped': True, 'stage_seconds': stage, **gate[i]}
         V = Vs[i]
         tele['refinement_steps'] = int(st.get('refinement_steps', 0))
         part = torch.zeros(2 * nth, dtype=torch.complex128, device='cuda')
@@ -492,8 +617,15 @@ def solve_bor_device(points, k, thetas_deg, mmax, precision='double', tol=None, 
             amp += 2.0 * part
         else:
             amp += part
-    tele = {'modes': 2 * mmax + 1, 'mode_systems_solved': len(modes), 'max_backward_error': 0.0,
+    tele = {'modes': 2 * mmax + 1, 'mode_systems_solved': len(modes),
+            'max_backward_error': max(t['backward_error'] for _p, t in outs),
+            'max_relative_residual': max(t['relative_residual'] for _p, t in outs),
+            'backward_error_max': BOR_LINEAR_BACKWARD_ERROR_MAX, 'residual_norm_refinement_advisory': BOR_LINEAR_RESIDUAL_MAX,
             'refinement_steps': max(t['refinement_steps'] for _p, t in outs)}
+    gated = [m for m, (_p, t) in zip(modes, outs) if t.get('gate_refinement_steps') or t.get('gate_lu_fallback')]
+    if gated:
+        tele['gate_refined_modes'] = gated
+        tele['gate_lu_fallback_modes'] = [m for m, (_p, t) in zip(modes, outs) if t.get('gate_lu_fallback')]
     fallbacks = [m for m, (_p, t) in zip(modes, outs) if t['fp64_fallback']]
     if fallbacks:
         tele['fp64_fallback_modes'] = len(fallbacks)

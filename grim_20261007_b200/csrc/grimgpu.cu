@@ -1640,6 +1640,41 @@ extern "C" int grim_residual(grim_handle_t h, int n, int nrhs, const void *A, in
     return tc_err_check(h, "grim_residual");
 }
 
+// Residual and release measures of one modal solution (reference bor/factor.py:289-300,
+// ModalFactor.errors): R = B - A X, per-column backward error and 2-norm relative
+// residual, their maxima in maxes[0..1].  On the handle's stream; slices > 0 (the int8
+// tensor-core residual) reads the kernels' error flag, one stream synchronisation.
+extern "C" int grim_solution_errors(grim_handle_t h, int n, int nrhs, const void *A, int64_t lda, const void *X,
+                                    int64_t ldx, const void *B, int64_t ldb, void *R, int64_t ldr, int slices,
+                                    double *berr_dev, double *relres_dev, double *maxes_dev) {
+    if (!h || n <= 0 || nrhs <= 0 || !A || !X || !B || !R || !maxes_dev || lda < n || ldx < n || ldb < n ||
+        ldr < n || (slices != 0 && !oz_supported(slices)) || (slices && !oz_fits(n, slices)))
+        return grim_fail(GRIM_ERR_ARGUMENT, "grim_solution_errors: bad arguments");
+    DeviceGuard g(h->device);
+    const double2 *Ad = (const double2 *)A, *Xd = (const double2 *)X, *Bd = (const double2 *)B;
+    double2 *Rd = (double2 *)R;
+    void *ps = nullptr, *pe = nullptr;
+    GRIM_TRY(grim_workspace(h, "se_scalars", 8 * sizeof(double), &ps));
+    GRIM_TRY(grim_workspace(h, "se_errs5", (size_t)5 * nrhs * sizeof(double), &pe));
+    double *anorm = (double *)ps;
+    GRIM_TRY(inf_norm(h, n, Ad, lda, anorm));
+    if (slices == 0) {
+        GRIM_CHECK_CUDA(cudaMemcpy2DAsync(Rd, ldr * sizeof(double2), Bd, ldb * sizeof(double2), n * sizeof(double2),
+                                          nrhs, cudaMemcpyDeviceToDevice, h->stream));
+        GRIM_TRY((gemm<double2, double2, double2, double2, true, true>(h, n, nrhs, n, Ad, lda, Xd, ldx, Rd, ldr)));
+    } else {
+        OzA qa;
+        GRIM_TRY(oz_prepare_a(h, n, Ad, lda, slices, &qa));
+        GRIM_TRY(oz_residual(h, qa, nrhs, Xd, ldx, Bd, ldb, Rd, ldr));
+        GRIM_TRY(tc_err_check(h, "grim_solution_errors"));
+    }
+    k_col_errs5<<<nrhs, 256, 0, h->stream>>>(n, Rd, ldr, Xd, ldx, Bd, ldb, (double *)pe);
+    GRIM_CHECK_LAUNCH(h, "k_col_errs5");
+    k_errs_finish<<<1, 1024, 0, h->stream>>>(nrhs, (const double *)pe, anorm, berr_dev, relres_dev, maxes_dev);
+    GRIM_CHECK_LAUNCH(h, "k_errs_finish");
+    return GRIM_OK;
+}
+
 // ============================================================== solve (FP64 or mixed)
 template <typename TA>
 static int mixed_refine(grim_context *h, int n, int nrhs, const TA *Ares, int64_t ldres, float2 *lu32, const int *ipiv,

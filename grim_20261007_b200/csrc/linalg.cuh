@@ -108,6 +108,94 @@ __global__ void k_col_absmax3(int m, const double2 *R, int64_t ldr, const TX *X,
     }
 }
 
+// Per-column error measures of a solution X of A X = B with residual R = B - A X:
+// out[5c..5c+4] = max|R|, max|X|, max|B|, sum |R|^2, sum |B|^2 (one CTA per column;
+// NaN propagates through every entry).
+__global__ void k_col_errs5(int m, const double2 *R, int64_t ldr, const double2 *X, int64_t ldx, const double2 *B,
+                            int64_t ldb, double *out) {
+    const int c = blockIdx.x;
+    double v[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    for (int r = threadIdx.x; r < m; r += blockDim.x) {
+        const double2 a = R[(int64_t)c * ldr + r];
+        const double2 x = X[(int64_t)c * ldx + r];
+        const double2 b = B[(int64_t)c * ldb + r];
+        v[0] = max_nan(v[0], hypot(a.x, a.y));
+        v[1] = max_nan(v[1], hypot(x.x, x.y));
+        v[2] = max_nan(v[2], hypot(b.x, b.y));
+        v[3] += a.x * a.x + a.y * a.y;
+        v[4] += b.x * b.x + b.y * b.y;
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+#pragma unroll
+        for (int q = 0; q < 3; ++q) v[q] = max_nan(v[q], __shfl_down_sync(0xffffffffu, v[q], off));
+        v[3] += __shfl_down_sync(0xffffffffu, v[3], off);
+        v[4] += __shfl_down_sync(0xffffffffu, v[4], off);
+    }
+    __shared__ double w[5][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) {
+#pragma unroll
+        for (int q = 0; q < 5; ++q) w[q][warp] = v[q];
+    }
+    __syncthreads();
+    if (warp == 0) {
+        const int nw = blockDim.x >> 5;
+#pragma unroll
+        for (int q = 0; q < 5; ++q) v[q] = lane < nw ? w[q][lane] : 0.0;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+#pragma unroll
+            for (int q = 0; q < 3; ++q) v[q] = max_nan(v[q], __shfl_down_sync(0xffffffffu, v[q], off));
+            v[3] += __shfl_down_sync(0xffffffffu, v[3], off);
+            v[4] += __shfl_down_sync(0xffffffffu, v[4], off);
+        }
+        if (lane == 0) {
+#pragma unroll
+            for (int q = 0; q < 5; ++q) out[5 * c + q] = v[q];
+        }
+    }
+}
+
+// From k_col_errs5: berr[c] = max|R| / (anorm max|X| + max|B|) (inf where the denominator
+// is 0 and the residual is not, or anything is NaN) and relres[c] = ||R||_2 / ||B||_2 (the
+// bare ||R||_2 for a zero column); maxes[0..1] = their maxima (NaN-propagating).
+__global__ void k_errs_finish(int ncol, const double *errs5, const double *anorm, double *berr, double *relres,
+                              double *maxes) {
+    double mb = 0.0, mr = 0.0;
+    for (int c = threadIdx.x; c < ncol; c += blockDim.x) {
+        const double r = errs5[5 * c], x = errs5[5 * c + 1], b = errs5[5 * c + 2];
+        const double r2 = sqrt(errs5[5 * c + 3]), b2 = sqrt(errs5[5 * c + 4]);
+        const double den = (*anorm) * x + b;
+        double e = den > 0 ? r / den : (r > 0 ? INFINITY : 0.0);
+        if (!(e == e) || r != r || den != den) e = INFINITY;
+        double rr = r2 / (b2 > 0 ? b2 : 1.0);
+        if (!(rr == rr)) rr = INFINITY;
+        if (berr) berr[c] = e;
+        if (relres) relres[c] = rr;
+        mb = fmax(mb, e);
+        mr = fmax(mr, rr);
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+        mb = fmax(mb, __shfl_down_sync(0xffffffffu, mb, off));
+        mr = fmax(mr, __shfl_down_sync(0xffffffffu, mr, off));
+    }
+    __shared__ double w[2][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) { w[0][warp] = mb; w[1][warp] = mr; }
+    __syncthreads();
+    if (warp == 0) {
+        const int nw = blockDim.x >> 5;
+        mb = lane < nw ? w[0][lane] : 0.0;
+        mr = lane < nw ? w[1][lane] : 0.0;
+        for (int off = 16; off > 0; off >>= 1) {
+            mb = fmax(mb, __shfl_down_sync(0xffffffffu, mb, off));
+            mr = fmax(mr, __shfl_down_sync(0xffffffffu, mr, off));
+        }
+        if (lane == 0) { maxes[0] = mb; maxes[1] = mr; }
+    }
+}
+
 // berr[c] = r / (anorm x + b); relres[c] = r / b (reference RefinedLU measure).
 __global__ void k_berr_finish(int ncol, const double *absmax3, const double *anorm, double *berr, double *relres,
                               double *maxes) {

@@ -23,6 +23,7 @@
  *                        scatter.py:282-368 (linear-Galerkin S + gamma(D + M/2) / K' - M/2 - gamma W fill),
  *                        twod/assembly/kernels.py:223-294 loads, twod/operators.py:2925-3030 far field
  *   grim_backward_error  twod/solver.py:695-720  backward_metrics (normwise backward error)
+ *   grim_solution_errors bor/factor.py:289-300  ModalFactor.errors (BoR release measures)
  *   grim_bor_*           bor/solver.py:1769-1962,2558-2608  per-mode assembly, excitation, far field
  *   ghost_far_block      twod/assembly/native/far.c:193-207  ghost_far_block (same signature, GPU)
  *   grim_far_block       the same on device pointers
@@ -197,6 +198,19 @@ int grim_residual(grim_handle_t h, int n, int nrhs, const void *A, int64_t lda, 
  * berr[j] = max_i |A x_j - b_j|_i / (||A||_inf max|x_j| + max|b_j|), A complex128 or complex64. */
 int grim_backward_error(grim_handle_t h, int n, int nrhs, const void *A, int64_t lda, int a_complex64,
                         const void *X, int64_t ldx, const void *B, int64_t ldb, double *berr_dev);
+
+/* Residual and release measures of a computed solution X of A X = B (reference
+ * bor/factor.py:289-300, ModalFactor.errors, used by the BoR per-mode gate of
+ * bor/factor.py:302-355): R = B - A X; per column berr[j] = max_i |R_ij| / (||A||_inf
+ * max_i |X_ij| + max_i |B_ij|) (inf for a zero denominator under a non-zero residual, or
+ * any NaN) and relres[j] = ||R_j||_2 / ||B_j||_2 (||R_j||_2 for a zero column); maxes[0]
+ * and maxes[1] = their maxima.  A, X, B, R complex128; berr_dev / relres_dev may be NULL.
+ * slices = 0 computes R with the FP64 GEMM, 8 on the integer tensor cores (8 int8 slices:
+ * FP64 GEMM accuracy; reads the kernels' error flag, one stream synchronisation).  R must
+ * not overlap B. */
+int grim_solution_errors(grim_handle_t h, int n, int nrhs, const void *A, int64_t lda, const void *X, int64_t ldx,
+                         const void *B, int64_t ldb, void *R, int64_t ldr, int slices, double *berr_dev,
+                         double *relres_dev, double *maxes_dev);
 
 /* Allocation-free grim_backward_error (no counterpart in the reference).  For callers
  * that cannot allocate device memory when they call it (memory owned by another

@@ -114,3 +114,22 @@ def test_mixed_requests_pick_the_precision_per_mode():
     assert bs.mode_precision(dev, 3, 4000, 'mixed') == 'mixed'
     assert bs.mode_precision(dev, 18, 4000, 'mixed') == 'double'   # >= 0.7 k rho_max
     assert bs.mode_precision(dev, 3, 800, 'mixed') == 'double'     # below the order threshold
+
+
+def test_release_gate_decisions():
+    """The per-mode release gate's host rules (reference bor/factor.py:302-355): limits per
+    precision, the pass test, and the refinement stop rule."""
+    from grim_20261007_b200.bor import solver as B
+    assert B.BOR_LINEAR_BACKWARD_ERROR_MAX == 1e-12 and B.BOR_LINEAR_RESIDUAL_MAX == 1e-8
+    assert B.release_limit('double', 1e-10) == 1e-12
+    assert B.release_limit('mixed', 1e-10) == 1e-10
+    assert B.release_limit('mixed', 1e-14) == 1e-12
+    assert B.gate_decision(1e-13, 1e-9, 1e-12)
+    assert not B.gate_decision(2e-12, 1e-9, 1e-12)
+    assert not B.gate_decision(1e-13, 2e-8, 1e-12)  # the relative residual alone sends it to refinement
+    assert not B.gate_decision(float('nan'), 0.0, 1e-12)
+    assert not B.gate_decision(0.0, float('inf'), 1e-12)
+    assert B.refinement_continues((1e-10, 1e-6), (1e-11, 1e-6))   # backward error fell
+    assert B.refinement_continues((1e-10, 1e-6), (1e-9, 1e-7))    # residual fell
+    assert not B.refinement_continues((1e-10, 1e-6), (1e-10, 1e-6))
+    assert not B.refinement_continues((1e-10, 1e-6), (2e-10, 2e-6))

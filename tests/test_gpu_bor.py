@@ -215,6 +215,11 @@ def test_grouped_modes_match_per_mode_solves(precision, monkeypatch):
     # double: the grouped path solves the symmetric ogive's modes through their mirror halves
     rtol = 1e-11 if precision == 'double' else 1e-8
     np.testing.assert_allclose(f_g, f_1, rtol=rtol, atol=rtol * np.max(np.abs(f_1)))
+    # the release gate measured every mode against its full matrix
+    limit = bs.release_limit(precision, 1e-10)
+    for t in (t_g, t_1):
+        assert 0.0 < t['max_backward_error'] <= limit
+        assert 0.0 < t['max_relative_residual'] <= bs.BOR_LINEAR_RESIDUAL_MAX
 
 
 def test_adaptive_mode_tail_matches_reference(ctx):
@@ -228,3 +233,82 @@ def test_adaptive_mode_tail_matches_reference(ctx):
     for pol in ('vv', 'hh'):
         amp = np.asarray(res['amp_' + pol])
         assert np.max(np.abs(amp - g['amp_%s_efie' % pol]) / np.abs(g['amp_%s_efie' % pol])) < 2e-3
+
+
+@pytest.mark.parametrize('slices', [0, 8])
+def test_solution_errors_match_numpy(ctx, slices):
+    """grim_solution_errors: R = B - A X, the normwise backward error and the 2-norm
+    relative residual per column (a zero right-hand side included) against NumPy."""
+    from grim_20261007_b200.device import ptr
+    rng = np.random.default_rng(17)
+    n, nrhs = 300, 37
+    A = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    X = rng.standard_normal((n, nrhs)) + 1j * rng.standard_normal((n, nrhs))
+    Bm = A @ X + 1e-9 * (rng.standard_normal((n, nrhs)) + 1j * rng.standard_normal((n, nrhs)))
+    Bm[:, 5] = 0.0
+    dev = lambda a: torch.as_tensor(np.ascontiguousarray(a.T), device='cuda')  # column-major storage
+    Ad, Xd, Bd = dev(A), dev(X), dev(Bm)
+    R = torch.empty_like(Bd)
+    berr = torch.empty(nrhs, dtype=torch.float64, device='cuda')
+    relres = torch.empty_like(berr)
+    maxes = torch.empty(2, dtype=torch.float64, device='cuda')
+    assert ctx.lib.grim_solution_errors(ctx.h, n, nrhs, ptr(Ad), n, ptr(Xd), n, ptr(Bd), n, ptr(R), n, slices,
+                                        ptr(berr), ptr(relres), ptr(maxes)) == 0
+    Rn = Bm - A @ X
+    scale = np.max(np.abs(A)) * np.max(np.abs(X)) * n
+    assert np.max(np.abs(R.cpu().numpy().T - Rn)) <= 1e-15 * scale
+    anorm = np.max(np.sum(np.abs(A), axis=1))
+    be = np.max(np.abs(Rn), axis=0) / (anorm * np.max(np.abs(X), axis=0) + np.max(np.abs(Bm), axis=0))
+    bn = np.linalg.norm(Bm, axis=0)
+    rr = np.linalg.norm(Rn, axis=0) / np.where(bn > 0, bn, 1.0)
+    np.testing.assert_allclose(berr.cpu().numpy(), be, rtol=1e-4)
+    np.testing.assert_allclose(relres.cpu().numpy(), rr, rtol=1e-4)
+    np.testing.assert_allclose(maxes.cpu().numpy(), [be.max(), rr.max()], rtol=1e-4)
+
+
+def _gate_case():
+    from grim_20261007_b200.bor import solver as B
+    pts = S.sphere_generatrix(1.0, 14)
+    dev = B.BorDevice(pts, 2.5, 4, alpha=0.5)
+    th = torch.as_tensor(np.arange(0.0, 181.0, 10.0), device='cuda')
+    modes = [0, 1, 2]
+    Zs = [dev.matrix(m) for m in modes]
+    B0s = [dev.excitation(m, th, far=False) for m in modes]
+    exact = [np.linalg.solve(Z.cpu().numpy().T, b.cpu().numpy().T) for Z, b in zip(Zs, B0s)]
+    return B, modes, Zs, B0s, exact
+
+
+def test_release_gate_refines_and_falls_back(ctx):
+    """The per-mode release gate: a direct FP64 solution off by 1e-7 is refined from where it
+    stands, a mirror / mixed one off by as much is replaced by the LU solution, an exact
+    one is released untouched; every mode ends at the reference's limits."""
+    B, modes, Zs, B0s, exact = _gate_case()
+    rng = np.random.default_rng(3)
+    Xs = []
+    for i, x in enumerate(exact):
+        noise = 1e-7 * np.max(np.abs(x)) * (rng.standard_normal(x.shape) + 1j * rng.standard_normal(x.shape))
+        Xs.append(torch.as_tensor(np.ascontiguousarray((x + (noise if i < 2 else 0.0)).T), device='cuda'))
+    out = B._gate_modes(modes, Zs, Xs, B0s, ['double', 'double', 'double'], [True, False, True], 1e-10)
+    assert out[0]['gate_refinement_steps'] >= 1 and 'gate_lu_fallback' not in out[0]
+    assert 'gate_lu_fallback' in out[1]
+    assert out[2]['gate_refinement_steps'] == 0 and 'gate_lu_fallback' not in out[2]
+    for o, X, x in zip(out, Xs, exact):
+        assert o['backward_error'] <= B.BOR_LINEAR_BACKWARD_ERROR_MAX
+        assert o['relative_residual'] <= B.BOR_LINEAR_RESIDUAL_MAX
+        assert np.max(np.abs(X.cpu().numpy().T - x)) <= 1e-10 * np.max(np.abs(x))
+    # a mixed solution is released at its refinement target, not at the FP64 limit
+    x = exact[0]
+    noise = 1e-13 * np.max(np.abs(x)) * (rng.standard_normal(x.shape) + 1j * rng.standard_normal(x.shape))
+    Xm = torch.as_tensor(np.ascontiguousarray((x + noise).T), device='cuda')
+    om = B._gate_modes([0], [Zs[0]], [Xm], [B0s[0]], ['mixed'], [False], 1e-10)[0]
+    assert 'gate_lu_fallback' not in om and om['gate_refinement_steps'] == 0
+
+
+def test_release_gate_raises_above_the_limit(ctx, monkeypatch):
+    """A backward error that refinement cannot bring under the limit raises (the limit is
+    set to zero here, so no solution can reach it)."""
+    B, modes, Zs, B0s, exact = _gate_case()
+    monkeypatch.setattr(B, 'BOR_LINEAR_BACKWARD_ERROR_MAX', 0.0)
+    X = torch.as_tensor(np.ascontiguousarray(exact[0].T), device='cuda')
+    with pytest.raises(RuntimeError, match='exceeds the release limit'):
+        B._gate_modes([0], [Zs[0]], [X], [B0s[0]], ['double'], [True], 1e-10)
