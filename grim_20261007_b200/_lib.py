@@ -30,6 +30,14 @@ c_size_t = ctypes.c_size_t
 P_int = ctypes.POINTER(ctypes.c_int)
 
 
+class GrimCondSystem(ctypes.Structure):
+    """``grim_cond_system`` of include/grimgpu.h (one factored system for grim_zcond1_factored)."""
+    _fields_ = [('n', c_int), ('A', c_void_p), ('lda', c_int64), ('halves', c_int), ('lu_complex64', c_int),
+                ('lu', c_void_p * 2), ('ldlu', c_int64 * 2), ('ipiv', c_void_p * 2), ('k', c_int), ('nfe', c_int),
+                ('nfo', c_int), ('p1', c_void_p), ('p2', c_void_p), ('fe', c_void_p), ('fo', c_void_p),
+                ('s', c_void_p)]
+
+
 class GrimSolveInfo(ctypes.Structure):
     _fields_ = [('backward_error', c_double), ('initial_backward_error', c_double), ('refinement_steps', c_int),
                 ('pivoted_panels', c_int), ('precision_mode', c_int), ('info', c_int), ('ms_factor', c_double),
@@ -87,6 +95,7 @@ SIGNATURES = [
                                c_int64, c_int]),
     ('grim_residual', c_int, [c_void_p, c_int, c_int, c_void_p, c_int64, c_int, c_void_p, c_int64, c_void_p, c_int64,
                               c_void_p, c_int64, c_int]),
+    ('grim_zcond1_factored', c_int, [c_void_p, c_int, c_void_p, c_void_p]),
     ('grim_solution_errors', c_int, [c_void_p, c_int, c_int, c_void_p, c_int64, c_void_p, c_int64, c_void_p, c_int64,
                                      c_void_p, c_int64, c_int, c_void_p, c_void_p, c_void_p]),
     ('grim_backward_error_noalloc', c_int, [c_void_p, c_int, c_int, c_void_p, c_int64, c_int, c_void_p, c_int64,

@@ -15,6 +15,7 @@ the CFIE with alpha = 0.5).  Impedance and sheet models are rejected.
 """
 from __future__ import annotations
 
+import ctypes
 import math
 
 import numpy as np
@@ -145,7 +146,7 @@ def refinement_continues(prev, cand):
     return not (cand[1] >= prev[1] and cand[0] >= prev[0])
 
 
-def _gate_modes(modes, Zs, Xs, B0s, precs, direct, tol, ctx=None):
+def _gate_modes(modes, Zs, Xs, B0s, precs, direct, tol, ctx=None, factors=None):
     """The per-mode release gate over solved mode systems, in place on ``Xs``.
 
     ``Zs`` are the full FP64 mode matrices, ``B0s`` the right-hand sides and ``direct[i]``
@@ -157,7 +158,8 @@ def _gate_modes(modes, Zs, Xs, B0s, precs, direct, tol, ctx=None):
     GATE_REFINEMENT_STEPS refinement steps run under the reference's stop rule.  A mode
     whose backward error still exceeds BOR_LINEAR_BACKWARD_ERROR_MAX raises RuntimeError.
     Returns per-mode dicts (backward_error, relative_residual, gate_refinement_steps,
-    gate_lu_fallback)."""
+    gate_lu_fallback); with ``factors`` (a list, one entry per mode) the LU of every mode
+    factored here replaces its entry."""
     from ..grouped import getrf_grouped
     ctx = ctx or context()
     count = len(modes)
@@ -216,7 +218,56 @@ def _gate_modes(modes, Zs, Xs, B0s, precs, direct, tol, ctx=None):
         if not (np.isfinite(cur[0]) and np.isfinite(cur[1])) or cur[0] > BOR_LINEAR_BACKWARD_ERROR_MAX:
             raise RuntimeError(f'BoR mode m={m} normwise linear backward error {cur[0]} exceeds the release limit '
                                f'{BOR_LINEAR_BACKWARD_ERROR_MAX}.')
+        if factors is not None:
+            factors[i] = {'halves': None, 'lu': [lus[j]], 'ipiv': [ipivs[j]]}
     return out
+
+
+# The per-mode condition gate (reference bor/solver.py BOR_CONDITION_EST_MAX, applied by
+# bor/factor.py:205-229 whenever the public solve_bor runs, monitor_cond=True there).
+BOR_CONDITION_EST_MAX = 1.0e12
+
+
+def condition_estimates(Zs, factors, ctx=None):
+    """1-norm condition estimates ||Z||_1 est(||inv(Z)||_1) of factored mode systems, all in
+    one launch (``grim_zcond1_factored``: LAPACK zgecon's estimator on the device).
+    ``factors[i]``: {'halves': None or the mirror map, 'lu': [LU] or [even, odd],
+    'ipiv': [...]}; complex64 factors (mixed precision) are read as such.  Returns a float64
+    NumPy array (NaN for a system holding a NaN, inf where zgecon's rcond is 0)."""
+    ctx = ctx or context()
+    count = len(Zs)
+    if not count:
+        return np.zeros(0)
+    arr = (_lib.GrimCondSystem * count)()
+    for q, Z, f in zip(arr, Zs, factors):
+        n = int(Z.shape[0])
+        q.n, q.A, q.lda = n, Z.data_ptr(), n
+        c64 = 0
+        for h, lu in enumerate(f['lu']):
+            q.lu[h] = lu.data_ptr()
+            q.ldlu[h] = int(lu.shape[0])
+            c64 |= int(lu.dtype == torch.complex64) << h
+        q.lu_complex64 = c64
+        mp = f['halves']
+        if mp is not None:
+            q.halves = 1
+            q.ipiv[0], q.ipiv[1] = f['ipiv'][0].data_ptr(), f['ipiv'][1].data_ptr()
+            q.k, q.nfe, q.nfo = int(mp['k']), int(mp['nfe']), int(mp['nfo'])
+            q.p1, q.p2, q.s = mp['p1'].data_ptr(), mp['p2'].data_ptr(), mp['s'].data_ptr()
+            q.fe, q.fo = mp['fe'].data_ptr(), mp['fo'].data_ptr()
+    cond = torch.empty(count, dtype=torch.float64, device='cuda')
+    _lib.check(ctx.lib.grim_zcond1_factored(ctx.h, count, ctypes.byref(arr), ptr(cond)), 'grim_zcond1_factored')
+    return cond.cpu().numpy()
+
+
+def condition_gate(modes, conds):
+    """The reference's release test of the mode condition estimates (bor/factor.py:224-229)."""
+    for m, c in zip(modes, conds):
+        if not (np.isfinite(c) and c > 0.0):
+            raise RuntimeError(f'BoR mode m={m} condition estimation failed.')
+        if c > BOR_CONDITION_EST_MAX:
+            raise RuntimeError(f'BoR mode m={m} estimated 1-norm condition {c} exceeds the release limit '
+                               f'{BOR_CONDITION_EST_MAX}.')
 
 
 def mirror_map(nodes, m):
@@ -373,9 +424,34 @@ def mode_precision(dev, m, order, precision):
     return 'mixed'
 
 
-def _solve_mode(dev, m, th, precision, tol, ctx=None):
+def _factor_solve(Z, V, precision, tol, ctx):
+    """LU of the mode matrix Z (complex64 with FP64 refinement for 'mixed', else complex128)
+    and the solve of V in place; returns (solve telemetry, factor for condition_estimates).
+    A mixed refinement that stalls raises GrimNotConverged."""
+    from ..grouped import refine_factored
+    n, nrhs = int(Z.shape[0]), int(V.shape[0])
+    ipiv = torch.empty(n, dtype=torch.int32, device='cuda')
+    info = ctypes.c_int(0)
+    if precision == 'mixed':
+        lu = Z.to(torch.complex64, copy=True)
+        _lib.check(ctx.lib.grim_cgetrf(ctx.h, n, ptr(lu), n, ptr(ipiv), ctypes.byref(info)), 'grim_cgetrf')
+    else:
+        lu = Z.clone()
+        _lib.check(ctx.lib.grim_zgetrf(ctx.h, n, ptr(lu), n, ptr(ipiv), ctypes.byref(info)), 'grim_zgetrf')
+    if info.value:
+        raise _lib.GrimError(_lib.GRIM_ERR_SINGULAR, f'BoR mode matrix is exactly singular (info={info.value})')
+    if precision == 'mixed':
+        st = refine_factored(Z, lu, ipiv, V, tol, stop='berr', ctx=ctx)
+    else:
+        _lib.check(ctx.lib.grim_zgetrs(ctx.h, n, nrhs, ptr(lu), n, ptr(ipiv), ptr(V), n), 'grim_zgetrs')
+        st = {'precision_mode': _lib.PREC_FP64}
+    return st, {'halves': None, 'lu': [lu], 'ipiv': [ipiv]}
+
+
+def _solve_mode(dev, m, th, precision, tol, ctx=None, monitor_cond=True):
     """One Fourier mode on ``ctx`` (default: the current device worker): assemble, excite,
-    solve and project; returns (this mode's far-field contribution [2 nth], telemetry)."""
+    factor, solve and project, with the condition gate (``monitor_cond``) and the release
+    gate; returns (this mode's far-field contribution [2 nth], telemetry)."""
     ctx = ctx or context()
     Z = dev.matrix(m, ctx=ctx)
     V = dev.excitation(m, th, far=False, ctx=ctx)
@@ -385,19 +461,26 @@ def _solve_mode(dev, m, th, precision, tol, ctx=None):
         tol = ops2d.MIXED_RCS_TOL  # an RCS solve: the same refinement target as the 2-D RCS path
     precision = mode_precision(dev, m, int(Z.shape[0]), precision)
     V0 = V.clone()
-    if precision == 'mixed':
-        try:
-            st = ops2d.solve_inplace(Z, V, 'mixed', tol=tol, ctx=ctx, stop='berr')
-        except _lib.GrimNotConverged:
-            # ill-conditioned mode: the reference's ladder falls back to the double LU
-            tele['fp64_fallback'] = True
-            V.copy_(V0)
-            precision = 'double'
-            st = ops2d.solve_inplace(Z, V, 'double', ctx=ctx)
-    else:
-        st = ops2d.solve_inplace(Z, V, precision, tol=tol, ctx=ctx)
+    try:
+        st, factor = _factor_solve(Z, V, precision, tol, ctx)
+    except _lib.GrimNotConverged:
+        # ill-conditioned mode: the reference's ladder falls back to the double LU
+        tele['fp64_fallback'] = True
+        V.copy_(V0)
+        precision = 'double'
+        st, factor = _factor_solve(Z, V, precision, tol, ctx)
     tele['refinement_steps'] = int(st.get('refinement_steps', 0))
-    tele.update(_gate_modes([m], [Z], [V], [V0], [precision], [precision == 'double'], tol, ctx=ctx)[0])
+    factors = [factor]
+    if monitor_cond:
+        cond = condition_estimates([Z], factors, ctx=ctx)
+        condition_gate([m], cond)
+    tele.update(_gate_modes([m], [Z], [V], [V0], [precision], [precision == 'double'], tol, ctx=ctx,
+                            factors=factors)[0])
+    if monitor_cond:
+        if tele.get('gate_lu_fallback'):
+            cond = condition_estimates([Z], factors, ctx=ctx)
+            condition_gate([m], cond)
+        tele['condition_est'] = float(cond[0])
     nth = int(th.numel())
     part = torch.zeros(2 * nth, dtype=torch.complex128, device='cuda')
     nred = int(Z.shape[0])
@@ -426,7 +509,7 @@ def _mirror_modes(dev, modes, Zs):
     return [i for (i, _o), (d, a) in zip(checks, vals) if np.isfinite(d) and d <= MIRROR_ASYMMETRY_MAX * a]
 
 
-def _solve_mirror_grouped(dev, modes, Zs, Vs, workers, precision='double', tol=None):
+def _solve_mirror_grouped(dev, modes, Zs, Vs, workers, precision='double', tol=None, keep_factors=False):
     """Solves of mirror-symmetric mode systems through their even and odd halves (reference
     ``bor/factor.py:37`` ``MirrorSplit``): the halves of every mode (FP64) and the split
     right-hand sides, one grouped solve of all halves (``grouped.solve_grouped``: a quarter
@@ -434,7 +517,8 @@ def _solve_mirror_grouped(dev, modes, Zs, Vs, workers, precision='double', tol=N
     refinement stalls re-solved in FP64), then the join.  The modes were checked symmetric
     to MIRROR_ASYMMETRY_MAX, so the halves are the system itself to rounding; the release
     gate (``_gate_modes``) then checks every joined solution against the full matrix and
-    replaces one that misses it by the LU solution."""
+    replaces one that misses it by the LU solution.  With ``keep_factors`` returns
+    (telemetry, factors): per mode the halves' LUs for ``condition_estimates``."""
     from ..grouped import solve_grouped
     ctx = context()
     halves, rhs, args_of = [], [], []
@@ -458,15 +542,17 @@ def _solve_mirror_grouped(dev, modes, Zs, Vs, workers, precision='double', tol=N
         args_of.append((args, nrhs, n, ke, ko))
     mixed = precision == 'mixed'
     rhs0 = [b.clone() for b in rhs] if mixed else None
-    sts = solve_grouped(halves, rhs, precision=precision, tol=tol, stop='berr', workers=workers)
+    sts = solve_grouped(halves, rhs, precision=precision, tol=tol, stop='berr', workers=workers,
+                        keep_factors=keep_factors)
     stalled = [i for i, st in enumerate(sts) if st.get('not_converged')]
     if stalled:
         redo = solve_grouped([halves[i] for i in stalled], [rhs0[i] for i in stalled], precision='double',
-                             workers=workers)
+                             workers=workers, keep_factors=keep_factors)
         for i, st in zip(stalled, redo):
             sts[i] = dict(st, fp64_fallback=True)
             rhs[i] = rhs0[i]
-    out = []
+    facs = [(st.pop('lu', None), st.pop('ipiv', None)) for st in sts]
+    out, factors = [], []
     for j, (args, nrhs, n, ke, ko) in enumerate(args_of):
         _lib.check(ctx.lib.grim_bor_mirror_join(ctx.h, nrhs, ptr(rhs[2 * j]), ptr(rhs[2 * j + 1]), *args, ptr(Vs[j]), n),
                    'grim_bor_mirror_join')
@@ -475,14 +561,21 @@ def _solve_mirror_grouped(dev, modes, Zs, Vs, workers, precision='double', tol=N
                     'pivoted_panels': se.get('pivoted_panels', 0) + so.get('pivoted_panels', 0), 'grouped': True,
                     'mirror_halves': [ke, ko], 'fp64_fallback': bool(se.get('fp64_fallback') or so.get('fp64_fallback')),
                     'refinement_steps': max(int(se.get('refinement_steps', 0)), int(so.get('refinement_steps', 0)))})
-    return out
+        if keep_factors:
+            (lue, pe), (luo, po) = facs[2 * j], facs[2 * j + 1]
+            factors.append({'halves': dev.mirror(modes[j]), 'lu': [lue, luo], 'ipiv': [pe, po]})
+    return (out, factors) if keep_factors else out
 
 
-def _solve_modes_grouped(dev, modes, th, precision, tol, workers):
+def _solve_modes_grouped(dev, modes, th, precision, tol, workers, monitor_cond=True):
     """All mode systems through one grouped LU (``grouped.solve_grouped``): assembly and
     excitations on the worker pool, one grouped factorization of every mode matrix, then
     the per-mode solves / refinement on the pool and the far-field projections here.  A
-    mode whose refinement stalls is re-solved in FP64 (the reference's ladder)."""
+    mode whose refinement stalls is re-solved in FP64 (the reference's ladder).  With
+    ``monitor_cond`` (the reference's public solve_bor) the factors are kept and every
+    mode's condition estimate is taken and gated before the release gate, as the
+    reference's ModalFactor does at construction; a mode the release gate refactors is
+    estimated again from its new LU."""
     from ..grouped import solve_grouped
 
     def prep(m):
@@ -503,46 +596,65 @@ def _solve_modes_grouped(dev, modes, th, precision, tol, workers):
     t1 = time.perf_counter()
     mirrored = set(_mirror_modes(dev, modes, Zs))
     sts = [None] * len(modes)
+    factors = [None] * len(modes)
     precs = [mode_precision(dev, m, int(Zs[i].shape[0]), precision) for i, m in enumerate(modes)]
     for prec in ('double', 'mixed'):
         mine = [i for i in range(len(modes)) if precs[i] == prec]
         mir = [i for i in mine if i in mirrored]
         if mir:
-            for i, st in zip(mir, _solve_mirror_grouped(dev, [modes[i] for i in mir], [Zs[i] for i in mir],
-                                                        [Vs[i] for i in mir], workers, precision=prec, tol=tol)):
-                sts[i] = st
+            res = _solve_mirror_grouped(dev, [modes[i] for i in mir], [Zs[i] for i in mir], [Vs[i] for i in mir],
+                                        workers, precision=prec, tol=tol, keep_factors=monitor_cond)
+            outs_m, facs = res if monitor_cond else (res, [None] * len(mir))
+            for i, st, f in zip(mir, outs_m, facs):
+                sts[i], factors[i] = st, f
         rest = [i for i in mine if i not in mirrored]
         if rest:
             for i, st in zip(rest, solve_grouped([Zs[i] for i in rest], [Vs[i] for i in rest], precision=prec,
-                                                 tol=tol, stop='berr', workers=workers)):
+                                                 tol=tol, stop='berr', workers=workers, keep_factors=monitor_cond)):
                 sts[i] = st
+                factors[i] = {'halves': None, 'lu': [st.pop('lu', None)], 'ipiv': [st.pop('ipiv', None)]}
     torch.cuda.synchronize()
     t2 = time.perf_counter()
     # stalled refinements (ill-conditioned modes): the reference's ladder to the double LU,
-    # here one grouped FP64 factorization of all of them
+    # here one grouped FP64 factorization of all of them (into copies: V0s stay the
+    # right-hand sides of the release gate)
     stalled = [i for i, st in enumerate(sts) if st.get('not_converged')]
     if stalled:
-        redo = solve_grouped([Zs[i] for i in stalled], [V0s[i] for i in stalled], precision='double',
-                             workers=workers)
-        for i, st in zip(stalled, redo):
+        xs = [V0s[i].clone() for i in stalled]
+        redo = solve_grouped([Zs[i] for i in stalled], xs, precision='double', workers=workers,
+                             keep_factors=monitor_cond)
+        for i, st, x in zip(stalled, redo, xs):
+            factors[i] = {'halves': None, 'lu': [st.pop('lu', None)], 'ipiv': [st.pop('ipiv', None)]}
             sts[i] = dict(st, fp64_fallback=True)
-            Vs[i] = V0s[i]
+            Vs[i] = x
     torch.cuda.synchronize()
     t3 = time.perf_counter()
+    conds = None
+    if monitor_cond:
+        conds = condition_estimates(Zs, factors)
+        condition_gate(modes, conds)
+    t4 = time.perf_counter()
     # the release gate against every full mode matrix: a solution from the FP64 LU of the
     # full matrix is direct; mirror halves and mixed factors are not
     fell_back = [bool(st.get('fp64_fallback')) for st in sts]
     eff = ['double' if fb and i not in mirrored else precs[i] for i, fb in enumerate(fell_back)]
     direct = [i not in mirrored and eff[i] == 'double' for i in range(len(modes))]
-    gate = _gate_modes(modes, Zs, Vs, V0s, eff, direct, tol)
+    gate = _gate_modes(modes, Zs, Vs, V0s, eff, direct, tol, factors=factors if monitor_cond else None)
+    redone = [i for i in range(len(modes)) if gate[i].get('gate_lu_fallback')]
+    if monitor_cond and redone:
+        again = condition_estimates([Zs[i] for i in redone], [factors[i] for i in redone])
+        condition_gate([modes[i] for i in redone], again)
+        conds[redone] = again
     torch.cuda.synchronize()
     stage = {'assembly': t1 - t0, 'grouped_factor_and_solves': t2 - t1, 'fp64_fallbacks': t3 - t2,
-             'release_gate': time.perf_counter() - t3}
+             'condition_estimates': t4 - t3, 'release_gate': time.perf_counter() - t4}
     ctx = context()
     nth = int(th.numel())
     outs = []
     for i, st in enumerate(sts):
         tele = {'fp64_fallback': fell_back[i], 'grouped': True, 'stage_seconds': stage, **gate[i]}
+        if conds is not None:
+            tele['condition_est'] = float(conds[i])
         V = Vs[i]
         tele['refinement_steps'] = int(st.get('refinement_steps', 0))
         part = torch.zeros(2 * nth, dtype=torch.complex128, device='cuda')
@@ -554,7 +666,8 @@ def _solve_modes_grouped(dev, modes, th, precision, tol, workers):
 
 
 def solve_bor_device(points, k, thetas_deg, mmax, precision='double', tol=None, ctx=None, workers=None,
-                     signed_mode_symmetry=True, grouped=True, mode_tol=None, tail_start=0, alpha=1.0):
+                     signed_mode_symmetry=True, grouped=True, mode_tol=None, tail_start=0, alpha=1.0,
+                     monitor_cond=True):
     """Device path: returns (F[2 nth] complex128 on the host, telemetry).
 
     The modal moments are built once; the per-mode systems are independent and run on the
@@ -569,7 +682,9 @@ def solve_bor_device(points, k, thetas_deg, mmax, precision='double', tol=None, 
     grouped LU (``grouped.py``); otherwise each mode is factored on its own worker.  With
     ``mode_tol`` the modal sum stops at the reference's adaptive tail (two consecutive
     modes at or above ``tail_start`` below the tolerance; ``_adaptive_tail``); all modes up
-    to ``mmax`` are solved together first, so the truncation decides only the sum.
+    to ``mmax`` are solved together first, so the truncation decides only the sum.  Every
+    mode passes the reference's release gates: its condition estimate (``monitor_cond``,
+    on in the reference's public solve_bor) and its backward error against the full matrix.
     """
     from ..twod.solver import sweep_workers
     import time
@@ -587,11 +702,12 @@ def solve_bor_device(points, k, thetas_deg, mmax, precision='double', tol=None, 
         if not sub:
             return []
         if ctx is not None:
-            return [_solve_mode(dev, m, th, precision, tol, ctx=ctx) for m in sub]
+            return [_solve_mode(dev, m, th, precision, tol, ctx=ctx, monitor_cond=monitor_cond) for m in sub]
         if grouped:
             return _solve_modes_grouped(dev, sub, th, precision, tol,
-                                        sweep_workers(len(sub)) if workers is None else workers)
-        jobs = [(lambda m=m: _solve_mode(dev, m, th, precision, tol)) for m in sub]
+                                        sweep_workers(len(sub)) if workers is None else workers,
+                                        monitor_cond=monitor_cond)
+        jobs = [(lambda m=m: _solve_mode(dev, m, th, precision, tol, monitor_cond=monitor_cond)) for m in sub]
         return run_pool(jobs, workers=sweep_workers(len(jobs)) if workers is None else workers)
 
     shard, group = requested_shard_group()
@@ -622,6 +738,14 @@ def solve_bor_device(points, k, thetas_deg, mmax, precision='double', tol=None, 
             'max_relative_residual': max(t['relative_residual'] for _p, t in outs),
             'backward_error_max': BOR_LINEAR_BACKWARD_ERROR_MAX, 'residual_norm_refinement_advisory': BOR_LINEAR_RESIDUAL_MAX,
             'refinement_steps': max(t['refinement_steps'] for _p, t in outs)}
+    tele['linear_refinement_steps'] = int(sum(t.get('gate_refinement_steps', 0) for _p, t in outs))
+    tele['condition_est_computed'] = bool(monitor_cond)
+    tele['condition_est_limit'] = BOR_CONDITION_EST_MAX
+    if monitor_cond:
+        conds = [t['condition_est'] for _p, t in outs]
+        tele['condition_est_method'] = 'lapack_gecon_1norm'
+        tele['max_cond'] = float(max(conds))
+        tele['median_cond'] = float(np.median(conds))
     gated = [m for m, (_p, t) in zip(modes, outs) if t.get('gate_refinement_steps') or t.get('gate_lu_fallback')]
     if gated:
         tele['gate_refined_modes'] = gated
@@ -725,4 +849,16 @@ def solve_bor(points, freq_hz, thetas_deg, formulation="auto", cfie_alpha=0.5, z
         'precision': requested_precision(),
         'warnings': [],
         'mode_bandwidth': int(bandwidth),
+        # the reference's release statistics (bor/solver.py:3195-3240)
+        'linear_residual': float(tele['max_relative_residual']),
+        'linear_backward_error': float(tele['max_backward_error']),
+        'linear_refinement_steps': int(tele['linear_refinement_steps']),
+        'linear_residual_limit': BOR_LINEAR_RESIDUAL_MAX,
+        'linear_residual_limit_kind': 'iterative_refinement_advisory',
+        'linear_backward_error_limit': BOR_LINEAR_BACKWARD_ERROR_MAX,
+        'condition_est_computed': True,
+        'condition_est_method': 'lapack_gecon_1norm',
+        'condition_est_limit': BOR_CONDITION_EST_MAX,
+        'max_cond': float(tele['max_cond']),
+        'median_cond': float(tele['median_cond']),
     }

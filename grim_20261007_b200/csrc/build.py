@@ -17,7 +17,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 PKG = os.path.dirname(HERE)
 SOURCES = ['grimgpu.cu']
 HEADERS = ['common.cuh', 'hankel.cuh', 'fill2d.cuh', 'linalg.cuh', 'lu.cuh', 'tc_gemm.cuh', 'ozaki.cuh', 'dmma.cuh',
-           'grouped.cuh', 'farblock.cuh', 'galerkin.cuh', 'pivot.cuh', 'condest.cuh', 'bor.cuh', 'noalloc.cu']
+           'grouped.cuh', 'farblock.cuh', 'galerkin.cuh', 'pivot.cuh', 'condest.cuh', 'bor.cuh', 'noalloc.cu',
+           'tslu.cuh', 'gepp_loop.cuh', 'modecond.cuh']
 OUT = os.path.join(PKG, 'libgrimgpu.so')
 ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
 

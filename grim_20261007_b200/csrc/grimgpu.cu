@@ -27,6 +27,7 @@
 #include "tslu.cuh"
 #include "gepp_loop.cuh"
 #include "condest.cuh"
+#include "modecond.cuh"
 
 // ============================================================== errors
 static thread_local std::string g_last_error;
@@ -2140,6 +2141,76 @@ extern "C" int grim_zcond1_equilibrated(grim_handle_t h, int n, const void *A, i
     }
     const double c = norm_b * est;
     *cond = std::isfinite(c) ? c : INFINITY;
+    return GRIM_OK;
+}
+
+// ------------------------------------------------ condition estimates of factored systems
+extern "C" int grim_zcond1_factored(grim_handle_t h, int count, const grim_cond_system *sys, double *cond_dev) {
+    if (!h || count <= 0 || count > 65535 || !sys || !cond_dev)
+        return grim_fail(GRIM_ERR_ARGUMENT, "grim_zcond1_factored: bad arguments");
+    DeviceGuard g(h->device);
+    std::vector<CondSysDev> d(count);
+    size_t tot = 0;
+    int nmax = 0;
+    for (int i = 0; i < count; ++i) {
+        const grim_cond_system &q = sys[i];
+        bool ok = q.n > 0 && q.A && q.lda >= q.n && q.lu[0];
+        if (ok && q.halves) {
+            const int ke = q.k + q.nfe, ko = q.k + q.nfo;
+            ok = q.k >= 0 && q.nfe >= 0 && q.nfo >= 0 && ke > 0 && ko > 0 && 2 * q.k + q.nfe + q.nfo == q.n &&
+                 q.lu[1] && q.ipiv[0] && q.ipiv[1] && q.ldlu[0] >= ke && q.ldlu[1] >= ko &&
+                 (q.k == 0 || (q.p1 && q.p2 && q.s)) && (q.nfe == 0 || q.fe) && (q.nfo == 0 || q.fo);
+        } else if (ok) {
+            ok = q.ldlu[0] >= q.n;
+        }
+        if (!ok) return grim_fail(GRIM_ERR_ARGUMENT, "grim_zcond1_factored: bad system description");
+        tot += (size_t)q.n;
+        nmax = std::max(nmax, q.n);
+    }
+    void *ps = nullptr, *pv = nullptr, *pc = nullptr;
+    GRIM_TRY(grim_workspace(h, "mc_sys", (size_t)count * sizeof(CondSysDev), &ps));
+    GRIM_TRY(grim_workspace(h, "mc_vec", 2 * tot * sizeof(double2), &pv));
+    GRIM_TRY(grim_workspace(h, "mc_colsum", tot * sizeof(double), &pc));
+    double2 *vec = (double2 *)pv;
+    double *colsum = (double *)pc;
+    size_t off = 0;
+    for (int i = 0; i < count; ++i) {
+        const grim_cond_system &q = sys[i];
+        CondSysDev &e = d[i];
+        e.n = q.n;
+        e.halves = q.halves ? 1 : 0;
+        e.lu_c64[0] = q.lu_complex64 & 1;
+        e.lu_c64[1] = q.halves ? (q.lu_complex64 >> 1) & 1 : 0;
+        e.order[0] = q.halves ? q.k + q.nfe : q.n;
+        e.order[1] = q.halves ? q.k + q.nfo : 0;
+        e.lu[0] = q.lu[0];
+        e.lu[1] = q.halves ? q.lu[1] : nullptr;
+        e.ld[0] = q.ldlu[0];
+        e.ld[1] = q.halves ? q.ldlu[1] : 0;
+        e.ipiv[0] = q.halves ? q.ipiv[0] : nullptr;
+        e.ipiv[1] = q.halves ? q.ipiv[1] : nullptr;
+        e.k = q.halves ? q.k : 0;
+        e.nfe = q.halves ? q.nfe : 0;
+        e.nfo = q.halves ? q.nfo : 0;
+        e.p1 = q.p1;
+        e.p2 = q.p2;
+        e.fe = q.fe;
+        e.fo = q.fo;
+        e.s = q.s;
+        e.a = (const double2 *)q.A;
+        e.lda = q.lda;
+        e.colsum = colsum + off;
+        e.x = vec + 2 * off;
+        e.w = vec + 2 * off + q.n;
+        off += (size_t)q.n;
+    }
+    CondSysDev *dsys = (CondSysDev *)ps;
+    GRIM_CHECK_CUDA(cudaMemcpyAsync(dsys, d.data(), (size_t)count * sizeof(CondSysDev), cudaMemcpyHostToDevice,
+                                    h->stream));
+    k_cond_colsum<<<dim3(ceil_div(nmax, 8), count), 256, 0, h->stream>>>(dsys);
+    GRIM_CHECK_LAUNCH(h, "k_cond_colsum");
+    k_cond_lacn2<<<count, CS_THREADS, 0, h->stream>>>(dsys, cond_dev);
+    GRIM_CHECK_LAUNCH(h, "k_cond_lacn2");
     return GRIM_OK;
 }
 

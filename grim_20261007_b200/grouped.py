@@ -75,7 +75,8 @@ def refine_factored(z, lu32, ipiv, b, tol, stop='berr', max_iter=10, ctx=None):
     return st.as_dict()
 
 
-def solve_grouped(zs, bs, precision='mixed', tol=None, stop='berr', use_graph=True, workers=4, costs=None):
+def solve_grouped(zs, bs, precision='mixed', tol=None, stop='berr', use_graph=True, workers=4, costs=None,
+                  keep_factors=False):
     """Solve Z_i X_i = B_i for every system: one grouped LU of all matrices, then the
     triangular solves (and, mixed, the FP64 refinement) per system on the worker pool.
 
@@ -83,7 +84,9 @@ def solve_grouped(zs, bs, precision='mixed', tol=None, stop='berr', use_graph=Tr
     promotion is the system); the LU runs in complex64 (mixed) or complex128 (double);
     ``bs``: complex128 (nrhs_i, n_i) right-hand sides, overwritten by the solutions.
     Returns per-system telemetry dicts; a mixed system whose refinement stalls carries
-    ``not_converged=True`` and its ``bs`` entry is left as the partial solution.
+    ``not_converged=True`` and its ``bs`` entry is left as the partial solution.  With
+    ``keep_factors`` every dict also holds its factor: ``lu`` (complex64 for mixed, else
+    complex128, LAPACK layout) and ``ipiv`` (1-based int32), both on the device.
     """
     from .twod.operators import MIXED_RCS_TOL
     lus = [z.to(torch.complex64, copy=True) if precision == 'mixed' else z.clone() for z in zs]
@@ -108,6 +111,8 @@ def solve_grouped(zs, bs, precision='mixed', tol=None, stop='berr', use_graph=Tr
                 st = {'precision_mode': _lib.PREC_FP64}
             st['pivoted_panels'] = piv[i]
             st['grouped'] = True
+            if keep_factors:
+                st['lu'], st['ipiv'] = lus[i], ipivs[i]
             return st
         return run
 

@@ -24,6 +24,7 @@
  *                        twod/assembly/kernels.py:223-294 loads, twod/operators.py:2925-3030 far field
  *   grim_backward_error  twod/solver.py:695-720  backward_metrics (normwise backward error)
  *   grim_solution_errors bor/factor.py:289-300  ModalFactor.errors (BoR release measures)
+ *   grim_zcond1_factored bor/factor.py:205-229  ModalFactor._condition (zgecon per BoR mode)
  *   grim_bor_*           bor/solver.py:1769-1962,2558-2608  per-mode assembly, excitation, far field
  *   ghost_far_block      twod/assembly/native/far.c:193-207  ghost_far_block (same signature, GPU)
  *   grim_far_block       the same on device pointers
@@ -261,6 +262,35 @@ int grim_zgesv_guarded(grim_handle_t h, int n, int nrhs, const void *A, int64_t 
  * (twod/solver.py:472-577, linalg/dense.py:157-198: the same matrix B, SciPy's block
  * estimator).  Synchronises the stream. */
 int grim_zcond1_equilibrated(grim_handle_t h, int n, const void *A, int64_t lda, double *cond);
+
+/* One factored system for grim_zcond1_factored: the full matrix A (complex128, column-major,
+ * for ||A||_1) and either its LU (halves = 0: LAPACK layout, lu[0] / ldlu[0]; the row
+ * interchanges are not needed) or the LUs of its mirror halves (halves = 1: lu[0] / ipiv[0]
+ * of the even half of order k + nfe, lu[1] / ipiv[1] of the odd half of order k + nfo, with
+ * 2k + nfe + nfo = n, and the split of grim_bor_mirror_split: pairs p1[k], p2[k] with
+ * signs s[k] = +-1, fixed unknowns fe[nfe] / fo[nfo]; every pointer on the device). */
+typedef struct grim_cond_system {
+    int n;
+    const void *A;
+    int64_t lda;
+    int halves;
+    int lu_complex64;  /* bit h set: lu[h] stored in complex64 (else complex128) */
+    const void *lu[2];
+    int64_t ldlu[2];
+    const int *ipiv[2];
+    int k, nfe, nfo;
+    const int *p1, *p2, *fe, *fo;
+    const double *s;
+} grim_cond_system;
+
+/* 1-norm condition estimates of already factored systems (reference bor/factor.py:205-229,
+ * ModalFactor._condition: LAPACK zgecon on each BoR mode's LU with ||A||_1 of the mode
+ * matrix, rcond^-1 = ||A||_1 est(||A^-1||_1)).  The estimate is zgecon's: the zlacn2
+ * iteration on inv(U) inv(L) (adjoint inv(L^H) inv(U^H)); a mirror-split system uses the
+ * true inverse through its halves.  One CTA per system, all systems in one launch:
+ * cond_dev[count] on the device, NaN for a system holding a NaN, INFINITY where zgecon
+ * returns rcond = 0 (zero norm or estimate, or overflow).  No host synchronisation. */
+int grim_zcond1_factored(grim_handle_t h, int count, const grim_cond_system *systems, double *cond_dev);
 
 /* Mixed solve reusing a complex64 factorization (LU32 and ipiv from grim_cgetrf, leading
  * dimension n) with FP64 refinement against A or the promotion of A32; for resident

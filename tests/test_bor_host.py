@@ -133,3 +133,15 @@ def test_release_gate_decisions():
     assert B.refinement_continues((1e-10, 1e-6), (1e-9, 1e-7))    # residual fell
     assert not B.refinement_continues((1e-10, 1e-6), (1e-10, 1e-6))
     assert not B.refinement_continues((1e-10, 1e-6), (2e-10, 2e-6))
+
+
+def test_condition_gate_messages():
+    """The reference's condition release test (bor/factor.py:224-229) on host values."""
+    from grim_20261007_b200.bor import solver as B
+    assert B.BOR_CONDITION_EST_MAX == 1e12
+    B.condition_gate([0, 1], [1.0, 9e11])
+    with pytest.raises(RuntimeError, match='m=3 estimated 1-norm condition .* exceeds the release limit'):
+        B.condition_gate([2, 3], [5.0, 2e12])
+    for bad in (float('nan'), float('inf'), 0.0):
+        with pytest.raises(RuntimeError, match='m=4 condition estimation failed'):
+            B.condition_gate([4], [bad])

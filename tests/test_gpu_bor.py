@@ -286,7 +286,9 @@ def test_release_gate_refines_and_falls_back(ctx):
     rng = np.random.default_rng(3)
     Xs = []
     for i, x in enumerate(exact):
-        noise = 1e-7 * np.max(np.abs(x)) * (rng.standard_normal(x.shape) + 1j * rng.standard_normal(x.shape))
+        # per-column noise: a column whose right-hand side vanishes (no excitation of this mode
+        # at that aspect) keeps its exact zero solution, the only one with a small backward error
+        noise = 1e-7 * np.max(np.abs(x), axis=0) * (rng.standard_normal(x.shape) + 1j * rng.standard_normal(x.shape))
         Xs.append(torch.as_tensor(np.ascontiguousarray((x + (noise if i < 2 else 0.0)).T), device='cuda'))
     out = B._gate_modes(modes, Zs, Xs, B0s, ['double', 'double', 'double'], [True, False, True], 1e-10)
     assert out[0]['gate_refinement_steps'] >= 1 and 'gate_lu_fallback' not in out[0]
@@ -298,7 +300,7 @@ def test_release_gate_refines_and_falls_back(ctx):
         assert np.max(np.abs(X.cpu().numpy().T - x)) <= 1e-10 * np.max(np.abs(x))
     # a mixed solution is released at its refinement target, not at the FP64 limit
     x = exact[0]
-    noise = 1e-13 * np.max(np.abs(x)) * (rng.standard_normal(x.shape) + 1j * rng.standard_normal(x.shape))
+    noise = 1e-13 * np.max(np.abs(x), axis=0) * (rng.standard_normal(x.shape) + 1j * rng.standard_normal(x.shape))
     Xm = torch.as_tensor(np.ascontiguousarray((x + noise).T), device='cuda')
     om = B._gate_modes([0], [Zs[0]], [Xm], [B0s[0]], ['mixed'], [False], 1e-10)[0]
     assert 'gate_lu_fallback' not in om and om['gate_refinement_steps'] == 0
@@ -312,3 +314,79 @@ def test_release_gate_raises_above_the_limit(ctx, monkeypatch):
     X = torch.as_tensor(np.ascontiguousarray(exact[0].T), device='cuda')
     with pytest.raises(RuntimeError, match='exceeds the release limit'):
         B._gate_modes([0], [Zs[0]], [X], [B0s[0]], ['double'], [True], 1e-10)
+
+
+def _plain_factor(lu):
+    """A scipy LU (logical (i, j) indexing) as the device factor entry of condition_estimates."""
+    dt = torch.complex64 if lu.dtype == np.complex64 else torch.complex128
+    t = torch.as_tensor(np.ascontiguousarray(lu.T), dtype=dt, device='cuda')
+    return {'halves': None, 'lu': [t], 'ipiv': [None]}
+
+
+def test_condition_estimates_match_lapack_zgecon(ctx):
+    """grim_zcond1_factored on LAPACK's own LU factors equals 1 / zgecon (the reference's
+    per-mode estimate) on random systems of ragged orders, all in one launch; complex64
+    factors against cgecon to single precision."""
+    import scipy.linalg as sl
+    from scipy.linalg import lapack
+    from grim_20261007_b200.bor import solver as B
+    rng = np.random.default_rng(11)
+    orders = [1, 2, 5, 31, 32, 33, 100, 257]
+    mats, facs, ref = [], [], []
+    for n in orders:
+        A = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n)) + 3.0 * np.eye(n) * (n % 3 == 0)
+        lu, _piv = sl.lu_factor(A)
+        anorm = float(np.max(np.sum(np.abs(A), axis=0)))
+        rcond, info = lapack.zgecon(lu, anorm, norm='1')
+        assert info == 0
+        mats.append(torch.as_tensor(np.ascontiguousarray(A.T), device='cuda'))
+        facs.append(_plain_factor(lu))
+        ref.append(1.0 / rcond)
+    got = B.condition_estimates(mats, facs)
+    np.testing.assert_allclose(got, ref, rtol=1e-9)
+    # complex64 factors (the mixed path) against cgecon
+    A = rng.standard_normal((120, 120)) + 1j * rng.standard_normal((120, 120))
+    lu32, _piv = sl.lu_factor(A.astype(np.complex64))
+    anorm = float(np.max(np.sum(np.abs(A), axis=0)))
+    rc32, _info = lapack.cgecon(lu32, anorm, norm='1')
+    got32 = B.condition_estimates([torch.as_tensor(np.ascontiguousarray(A.T), device='cuda')], [_plain_factor(lu32)])
+    np.testing.assert_allclose(got32, [1.0 / rc32], rtol=1e-4)
+
+
+def test_condition_estimates_of_mirror_halves_and_modes(ctx):
+    """A mirror-split ogive mode: the estimate through its halves' LUs is a lower bound of the
+    exact 1-norm condition number within a factor 3, as zgecon's on the full LU; the grouped
+    mode solve reports the same estimates for its modes."""
+    from grim_20261007_b200.bor import solver as B
+    pts = S.ogive_generatrix(3.0, 22.0, 30)
+    dev = B.BorDevice(pts, 5.0, 4, alpha=0.5)
+    th = torch.as_tensor(np.array([10.0, 60.0, 120.0]), device='cuda')
+    modes = [0, 1, 2, 3]
+    Zs = [dev.matrix(m) for m in modes]
+    Vs = [dev.excitation(m, th, far=False) for m in modes]
+    outs, facs = B._solve_mirror_grouped(dev, modes, [z.clone() for z in Zs], Vs, workers=1, keep_factors=True)
+    got = B.condition_estimates(Zs, facs)
+    for Z, c in zip(Zs, got):
+        z = Z.cpu().numpy().T
+        exact = np.linalg.norm(z, 1) * np.linalg.norm(np.linalg.inv(z), 1)
+        assert exact / 3.0 <= c <= exact * (1 + 1e-9), (c, exact)
+    gen, _l, _h = S.ogive_case(8, n=60)
+    k = 10.0 / float(np.max(gen[:, 0]))
+    _f, tele = B.solve_bor_device(gen, k, np.arange(0.0, 180.5, 5.0), 6, alpha=0.5)
+    assert tele['condition_est_computed'] and 1.0 < tele['median_cond'] <= tele['max_cond'] < B.BOR_CONDITION_EST_MAX
+    _f1, tele1 = B.solve_bor_device(gen, k, np.arange(0.0, 180.5, 5.0), 6, alpha=0.5, grouped=False)
+    # mirror halves (grouped) and full LUs (per mode) estimate the same condition numbers
+    assert tele1['max_cond'] / 3.0 <= tele['max_cond'] <= 3.0 * tele1['max_cond']
+
+
+def test_condition_gate_raises_above_the_limit(monkeypatch):
+    """The reference's condition release limit: a mode estimated above it raises (the limit is
+    lowered to 1 here, below every condition number)."""
+    if not torch.cuda.is_available():
+        pytest.skip('no CUDA device')
+    from grim_20261007_b200.bor import solver as B
+    monkeypatch.setattr(B, 'BOR_CONDITION_EST_MAX', 1.0)
+    pts = S.sphere_generatrix(1.0, 14)
+    for grouped in (True, False):
+        with pytest.raises(RuntimeError, match='condition .* exceeds the release limit'):
+            B.solve_bor_device(pts, 2.5, [0.0, 45.0, 90.0], 3, alpha=0.5, grouped=grouped)

@@ -21,6 +21,28 @@ def test_library_loads_and_exports_every_declared_symbol():
     assert lib.grim_version() >= 1
 
 
+def test_cond_system_struct_matches_the_c_layout(tmp_path):
+    """_lib.GrimCondSystem has grim_cond_system's size and field offsets (compiled here
+    against include/grimgpu.h)."""
+    import os
+    import shutil
+    import subprocess
+    cc = shutil.which('gcc') or shutil.which('cc')
+    if cc is None:
+        pytest.skip('no C compiler')
+    inc = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), 'include')
+    fields = [f[0] for f in _lib.GrimCondSystem._fields_]
+    src = tmp_path / 'layout.c'
+    body = ''.join(f'    printf("%zu\\n", offsetof(grim_cond_system, {f}));\n' for f in fields)
+    src.write_text('#include <stddef.h>\n#include <stdio.h>\n#include "grimgpu.h"\nint main(void) {\n'
+                   '    printf("%zu\\n", sizeof(grim_cond_system));\n' + body + '    return 0;\n}\n')
+    exe = tmp_path / 'layout'
+    subprocess.run([cc, '-I', inc, str(src), '-o', str(exe)], check=True)
+    got = [int(v) for v in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()]
+    want = [ctypes.sizeof(_lib.GrimCondSystem)] + [getattr(_lib.GrimCondSystem, f).offset for f in fields]
+    assert got == want
+
+
 def test_library_reports_errors_without_device():
     import torch
     if torch.cuda.is_available():
