@@ -189,6 +189,7 @@ def run_bor(args):
                      'fp64_fallback_mode_list': tele.get('fp64_fallback_mode_list', []),
                      'max_backward_error': tele.get('max_backward_error'),
                      'max_relative_residual': tele.get('max_relative_residual'),
+                     'max_cond': tele.get('max_cond'),
                      'gate_refined_modes': tele.get('gate_refined_modes', []),
                      'stage_seconds': tele.get('stage_seconds')}
     s64 = 4 * np.pi * np.abs(res['double']) ** 2

@@ -120,7 +120,9 @@ def solution_errors(Z, X, B, R, maxes, ctx=None, berr=None, relres=None):
     """R = B - Z X and the release measures of the solution X (rows of the (nrhs, n) device
     arrays are the right-hand sides): per-column backward error / 2-norm relative residual
     into ``berr`` / ``relres`` when given, their maxima into the 2-element float64 device
-    view ``maxes`` (``grim_solution_errors``; reference bor/factor.py:289-300)."""
+    view ``maxes`` (``grim_solution_errors``; reference bor/factor.py:289-300).  Queued on
+    the handle's stream: call ``grim_synchronize`` (it reports the tensor-core error flag)
+    before reading the results."""
     ctx = ctx or context()
     n, nrhs = int(B.shape[1]), int(B.shape[0])
     _lib.check(ctx.lib.grim_solution_errors(ctx.h, n, nrhs, ptr(Z), n, ptr(X), n, ptr(B), n, ptr(R), n, GATE_SLICES,
@@ -171,6 +173,7 @@ def _gate_modes(modes, Zs, Xs, B0s, precs, direct, tol, ctx=None, factors=None):
     for i in range(count):
         R = scratch[:B0s[i].numel()].view(B0s[i].shape)
         solution_errors(Zs[i], Xs[i], B0s[i], R, maxes[i], ctx=ctx)
+    _lib.check(ctx.lib.grim_synchronize(ctx.h), 'grim_synchronize')  # one wait (and error check) for all modes
     vals = maxes.cpu().numpy()
     out = [{'backward_error': float(vals[i, 0]), 'relative_residual': float(vals[i, 1]), 'gate_refinement_steps': 0}
            for i in range(count)]
@@ -187,6 +190,7 @@ def _gate_modes(modes, Zs, Xs, B0s, precs, direct, tol, ctx=None, factors=None):
 
     def measure(i, X, R):
         solution_errors(Zs[i], X, B0s[i], R, one, ctx=ctx)
+        _lib.check(ctx.lib.grim_synchronize(ctx.h), 'grim_synchronize')
         b, r = one.cpu().numpy()
         return float(b), float(r)
 
@@ -228,12 +232,13 @@ def _gate_modes(modes, Zs, Xs, B0s, precs, direct, tol, ctx=None, factors=None):
 BOR_CONDITION_EST_MAX = 1.0e12
 
 
-def condition_estimates(Zs, factors, ctx=None):
+def condition_estimates(Zs, factors, ctx=None, read=True):
     """1-norm condition estimates ||Z||_1 est(||inv(Z)||_1) of factored mode systems, all in
     one launch (``grim_zcond1_factored``: LAPACK zgecon's estimator on the device).
     ``factors[i]``: {'halves': None or the mirror map, 'lu': [LU] or [even, odd],
     'ipiv': [...]}; complex64 factors (mixed precision) are read as such.  Returns a float64
-    NumPy array (NaN for a system holding a NaN, inf where zgecon's rcond is 0)."""
+    NumPy array (NaN for a system holding a NaN, inf where zgecon's rcond is 0); with
+    ``read=False`` the float64 device tensor, not waited for."""
     ctx = ctx or context()
     count = len(Zs)
     if not count:
@@ -257,7 +262,7 @@ def condition_estimates(Zs, factors, ctx=None):
             q.fe, q.fo = mp['fe'].data_ptr(), mp['fo'].data_ptr()
     cond = torch.empty(count, dtype=torch.float64, device='cuda')
     _lib.check(ctx.lib.grim_zcond1_factored(ctx.h, count, ctypes.byref(arr), ptr(cond)), 'grim_zcond1_factored')
-    return cond.cpu().numpy()
+    return cond.cpu().numpy() if read else cond
 
 
 def condition_gate(modes, conds):
@@ -450,8 +455,9 @@ def _factor_solve(Z, V, precision, tol, ctx):
 
 def _solve_mode(dev, m, th, precision, tol, ctx=None, monitor_cond=True):
     """One Fourier mode on ``ctx`` (default: the current device worker): assemble, excite,
-    factor, solve and project, with the condition gate (``monitor_cond``) and the release
-    gate; returns (this mode's far-field contribution [2 nth], telemetry)."""
+    factor, solve and project.  The release measures (and with ``monitor_cond`` the
+    condition estimate) are queued on the device, not read: returns (this mode's far-field
+    contribution [2 nth], telemetry, pending device results for ``_finish_modes``)."""
     ctx = ctx or context()
     Z = dev.matrix(m, ctx=ctx)
     V = dev.excitation(m, th, far=False, ctx=ctx)
@@ -470,23 +476,79 @@ def _solve_mode(dev, m, th, precision, tol, ctx=None, monitor_cond=True):
         precision = 'double'
         st, factor = _factor_solve(Z, V, precision, tol, ctx)
     tele['refinement_steps'] = int(st.get('refinement_steps', 0))
-    factors = [factor]
+    pending = {'precision': precision, 'maxes': torch.empty(2, dtype=torch.float64, device='cuda'), 'cond': None}
+    solution_errors(Z, V, V0, torch.empty_like(V0), pending['maxes'], ctx=ctx)
     if monitor_cond:
-        cond = condition_estimates([Z], factors, ctx=ctx)
-        condition_gate([m], cond)
-    tele.update(_gate_modes([m], [Z], [V], [V0], [precision], [precision == 'double'], tol, ctx=ctx,
-                            factors=factors)[0])
-    if monitor_cond:
-        if tele.get('gate_lu_fallback'):
-            cond = condition_estimates([Z], factors, ctx=ctx)
-            condition_gate([m], cond)
-        tele['condition_est'] = float(cond[0])
+        pending['cond'] = condition_estimates([Z], [factor], ctx=ctx, read=False)
     nth = int(th.numel())
     part = torch.zeros(2 * nth, dtype=torch.complex128, device='cuda')
     nred = int(Z.shape[0])
     _lib.check(ctx.lib.grim_bor_farfield_accumulate(ctx.h, nred, 2 * nth, ptr(W), nred, ptr(V), nred, ptr(part)),
                'grim_bor_farfield_accumulate')
-    return part, tele
+    return part, tele, pending
+
+
+def _pool_mode(dev, m, th, precision, tol, monitor_cond):
+    """``_solve_mode`` on a device worker, its handle's tensor-core error flag checked."""
+    out = _solve_mode(dev, m, th, precision, tol, monitor_cond=monitor_cond)
+    c = context()
+    _lib.check(c.lib.grim_synchronize(c.h), 'grim_synchronize')
+    return out
+
+
+def _redo_mode(dev, m, th, tol, ctx, monitor_cond):
+    """A mode that missed the release gate, again from its FP64 LU: assemble, factor, solve,
+    then the gate's refinement (``_gate_modes``, which raises when the backward error stays
+    above the limit) and, with ``monitor_cond``, the condition gate on the new factor.
+    Returns (far-field contribution, gate telemetry)."""
+    Z = dev.matrix(m, ctx=ctx)
+    V = dev.excitation(m, th, far=False, ctx=ctx)
+    W = dev.excitation(m, th, far=True, ctx=ctx)
+    V0 = V.clone()
+    _st, factor = _factor_solve(Z, V, 'double', tol, ctx)
+    factors = [factor]
+    gate = _gate_modes([m], [Z], [V], [V0], ['double'], [True], tol, ctx=ctx, factors=factors)[0]
+    if monitor_cond:
+        cond = condition_estimates([Z], factors, ctx=ctx)
+        condition_gate([m], cond)
+        gate['condition_est'] = float(cond[0])
+    nth = int(th.numel())
+    part = torch.zeros(2 * nth, dtype=torch.complex128, device='cuda')
+    nred = int(Z.shape[0])
+    _lib.check(ctx.lib.grim_bor_farfield_accumulate(ctx.h, nred, 2 * nth, ptr(W), nred, ptr(V), nred, ptr(part)),
+               'grim_bor_farfield_accumulate')
+    return part, gate
+
+
+def _finish_modes(dev, modes, th, results, tol, ctx, monitor_cond):
+    """The gates over modes solved by ``_solve_mode``: one read of every mode's queued
+    condition estimate and release measures, the condition gate in mode order, then each
+    mode that missed the release limits solved again from its FP64 LU with refinement
+    (``_redo_mode``; a mixed solution that misses them is replaced by the LU solution, as
+    the grouped path does).  Returns [(part, telemetry)]."""
+    ctx = ctx or context()
+    if tol is None:
+        tol = ops2d.MIXED_RCS_TOL
+    if not results:
+        return []
+    _lib.check(ctx.lib.grim_synchronize(ctx.h), 'grim_synchronize')
+    vals = torch.stack([p['maxes'] for _part, _t, p in results]).cpu().numpy()
+    conds = None
+    if monitor_cond:
+        conds = torch.cat([p['cond'] for _part, _t, p in results]).cpu().numpy()
+        condition_gate(modes, conds)
+    outs = []
+    for i, (m, (part, tele, p)) in enumerate(zip(modes, results)):
+        tele.update(backward_error=float(vals[i, 0]), relative_residual=float(vals[i, 1]), gate_refinement_steps=0)
+        if conds is not None:
+            tele['condition_est'] = float(conds[i])
+        if not gate_decision(vals[i, 0], vals[i, 1], release_limit(p['precision'], tol)):
+            part, gate = _redo_mode(dev, m, th, tol, ctx, monitor_cond)
+            if p['precision'] != 'double':
+                gate['gate_lu_fallback'] = f'mixed solution stopped at backward error {vals[i, 0]:.3g}'
+            tele.update(gate)
+        outs.append((part, tele))
+    return outs
 
 
 def _mirror_modes(dev, modes, Zs):
@@ -702,13 +764,15 @@ def solve_bor_device(points, k, thetas_deg, mmax, precision='double', tol=None, 
         if not sub:
             return []
         if ctx is not None:
-            return [_solve_mode(dev, m, th, precision, tol, ctx=ctx, monitor_cond=monitor_cond) for m in sub]
+            res = [_solve_mode(dev, m, th, precision, tol, ctx=ctx, monitor_cond=monitor_cond) for m in sub]
+            return _finish_modes(dev, sub, th, res, tol, ctx, monitor_cond)
         if grouped:
             return _solve_modes_grouped(dev, sub, th, precision, tol,
                                         sweep_workers(len(sub)) if workers is None else workers,
                                         monitor_cond=monitor_cond)
-        jobs = [(lambda m=m: _solve_mode(dev, m, th, precision, tol, monitor_cond=monitor_cond)) for m in sub]
-        return run_pool(jobs, workers=sweep_workers(len(jobs)) if workers is None else workers)
+        jobs = [(lambda m=m: _pool_mode(dev, m, th, precision, tol, monitor_cond)) for m in sub]
+        res = run_pool(jobs, workers=sweep_workers(len(jobs)) if workers is None else workers)
+        return _finish_modes(dev, sub, th, res, tol, None, monitor_cond)
 
     shard, group = requested_shard_group()
     if shard and ctx is None:

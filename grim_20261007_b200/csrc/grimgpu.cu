@@ -222,11 +222,12 @@ extern "C" int grim_set_stream(grim_handle_t h, void *stream) {
     return GRIM_OK;
 }
 extern "C" void *grim_get_stream(grim_handle_t h) { return h ? (void *)h->stream : nullptr; }
+static int tc_err_check(grim_context *h, const char *what);
 extern "C" int grim_synchronize(grim_handle_t h) {
     if (!h) return grim_fail(GRIM_ERR_ARGUMENT, "null handle");
     DeviceGuard g(h->device);
     GRIM_CHECK_CUDA(cudaStreamSynchronize(h->stream));
-    return GRIM_OK;
+    return tc_err_check(h, "a tensor-core kernel since the last check");
 }
 extern "C" int64_t grim_launch_count(grim_handle_t h) { return h ? h->launches : 0; }
 extern "C" int grim_device_name(grim_handle_t h, char *buf, int len) {
@@ -1643,8 +1644,8 @@ extern "C" int grim_residual(grim_handle_t h, int n, int nrhs, const void *A, in
 
 // Residual and release measures of one modal solution (reference bor/factor.py:289-300,
 // ModalFactor.errors): R = B - A X, per-column backward error and 2-norm relative
-// residual, their maxima in maxes[0..1].  On the handle's stream; slices > 0 (the int8
-// tensor-core residual) reads the kernels' error flag, one stream synchronisation.
+// residual, their maxima in maxes[0..1].  On the handle's stream, no host synchronisation:
+// the int8 tensor-core residual (slices > 0) leaves its error flag to grim_synchronize.
 extern "C" int grim_solution_errors(grim_handle_t h, int n, int nrhs, const void *A, int64_t lda, const void *X,
                                     int64_t ldx, const void *B, int64_t ldb, void *R, int64_t ldr, int slices,
                                     double *berr_dev, double *relres_dev, double *maxes_dev) {
@@ -1667,7 +1668,6 @@ extern "C" int grim_solution_errors(grim_handle_t h, int n, int nrhs, const void
         OzA qa;
         GRIM_TRY(oz_prepare_a(h, n, Ad, lda, slices, &qa));
         GRIM_TRY(oz_residual(h, qa, nrhs, Xd, ldx, Bd, ldb, Rd, ldr));
-        GRIM_TRY(tc_err_check(h, "grim_solution_errors"));
     }
     k_col_errs5<<<nrhs, 256, 0, h->stream>>>(n, Rd, ldr, Xd, ldx, Bd, ldb, (double *)pe);
     GRIM_CHECK_LAUNCH(h, "k_col_errs5");

@@ -97,6 +97,8 @@ int grim_destroy(grim_handle_t h);
  * A new handle runs on its own non-blocking stream until this is called. */
 int grim_set_stream(grim_handle_t h, void *stream);
 void *grim_get_stream(grim_handle_t h);
+/* Waits for the handle's stream; also reports (GRIM_ERR_CUDA, then cleared) a bounded wait
+ * that ran out in a tensor-core kernel queued without a host check (grim_solution_errors). */
 int grim_synchronize(grim_handle_t h);
 const char *grim_last_error(void);
 int grim_device_name(grim_handle_t h, char *buf, int len);
@@ -207,8 +209,8 @@ int grim_backward_error(grim_handle_t h, int n, int nrhs, const void *A, int64_t
  * any NaN) and relres[j] = ||R_j||_2 / ||B_j||_2 (||R_j||_2 for a zero column); maxes[0]
  * and maxes[1] = their maxima.  A, X, B, R complex128; berr_dev / relres_dev may be NULL.
  * slices = 0 computes R with the FP64 GEMM, 8 on the integer tensor cores (8 int8 slices:
- * FP64 GEMM accuracy; reads the kernels' error flag, one stream synchronisation).  R must
- * not overlap B. */
+ * FP64 GEMM accuracy).  No host synchronisation: the tensor-core kernels' error flag is
+ * reported by the next grim_synchronize.  R must not overlap B. */
 int grim_solution_errors(grim_handle_t h, int n, int nrhs, const void *A, int64_t lda, const void *X, int64_t ldx,
                          const void *B, int64_t ldb, void *R, int64_t ldr, int slices, double *berr_dev,
                          double *relres_dev, double *maxes_dev);

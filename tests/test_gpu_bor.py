@@ -254,6 +254,7 @@ def test_solution_errors_match_numpy(ctx, slices):
     maxes = torch.empty(2, dtype=torch.float64, device='cuda')
     assert ctx.lib.grim_solution_errors(ctx.h, n, nrhs, ptr(Ad), n, ptr(Xd), n, ptr(Bd), n, ptr(R), n, slices,
                                         ptr(berr), ptr(relres), ptr(maxes)) == 0
+    assert ctx.lib.grim_synchronize(ctx.h) == 0
     Rn = Bm - A @ X
     scale = np.max(np.abs(A)) * np.max(np.abs(X)) * n
     assert np.max(np.abs(R.cpu().numpy().T - Rn)) <= 1e-15 * scale
@@ -390,3 +391,24 @@ def test_condition_gate_raises_above_the_limit(monkeypatch):
     for grouped in (True, False):
         with pytest.raises(RuntimeError, match='condition .* exceeds the release limit'):
             B.solve_bor_device(pts, 2.5, [0.0, 45.0, 90.0], 3, alpha=0.5, grouped=grouped)
+
+
+def test_release_gate_paths_when_every_mode_misses_the_limits(monkeypatch):
+    """With the relative-residual limit at zero every mode misses the release limits: the
+    grouped path replaces each mirror-halves solution by its full LU solution (and takes
+    its condition estimate again), the per-mode path solves each mode again from its FP64
+    LU; both far fields equal the ordinary solve's."""
+    if not torch.cuda.is_available():
+        pytest.skip('no CUDA device')
+    from grim_20261007_b200.bor import solver as B
+    gen, _l, _h = S.ogive_case(5, n=40)
+    k = 8.0 / float(np.max(gen[:, 0]))
+    th = np.arange(0.0, 180.5, 15.0)
+    f0, t0 = B.solve_bor_device(gen, k, th, 6, alpha=0.5)
+    monkeypatch.setattr(B, 'BOR_LINEAR_RESIDUAL_MAX', 0.0)
+    f1, t1 = B.solve_bor_device(gen, k, th, 6, alpha=0.5)
+    assert len(t1.get('gate_lu_fallback_modes', [])) >= 1  # the mirror-split modes of this symmetric body
+    f2, _t2 = B.solve_bor_device(gen, k, th, 6, alpha=0.5, grouped=False)
+    for f in (f1, f2):
+        np.testing.assert_allclose(f, f0, rtol=1e-10, atol=1e-10 * np.max(np.abs(f0)))
+    assert t1['max_cond'] / 3.0 <= t0['max_cond'] <= 3.0 * t1['max_cond']
