@@ -148,7 +148,41 @@ def refinement_continues(prev, cand):
     return not (cand[1] >= prev[1] and cand[0] >= prev[0])
 
 
-def _gate_modes(modes, Zs, Xs, B0s, precs, direct, tol, ctx=None, factors=None):
+def _measure_modes(Zs, Xs, B0s, ctx=None, workers=None, side=None):
+    """The release measures of every mode solution, read in one go: a (count, 2) NumPy array
+    of (backward error, relative residual) maxima.  With ``workers`` (and no ``ctx``) the
+    modes run on that many device workers, so that one mode's residual overlaps the next
+    one's; ``side`` (a callable taking a handle) runs beside them, first, and its result is
+    returned too (None without it)."""
+    count = len(Zs)
+    maxes = torch.empty((count, 2), dtype=torch.float64, device='cuda')
+    side_out = None
+    if workers and workers > 1 and count > 1 and ctx is None:
+        def job(i):
+            def run():
+                c = context()
+                solution_errors(Zs[i], Xs[i], B0s[i], torch.empty_like(B0s[i]), maxes[i], ctx=c)
+                _lib.check(c.lib.grim_synchronize(c.h), 'grim_synchronize')
+            return run
+        jobs = [job(i) for i in range(count)]
+        if side is not None:
+            jobs.insert(0, lambda: side(context()))
+        res = run_pool(jobs, workers=min(int(workers), len(jobs)))
+        side_out = res[0] if side is not None else None
+    else:
+        ctx = ctx or context()
+        if side is not None:
+            side_out = side(ctx)
+        size = max(int(B.numel()) for B in B0s)
+        scratch = torch.empty(size, dtype=torch.complex128, device='cuda')
+        for i in range(count):
+            R = scratch[:B0s[i].numel()].view(B0s[i].shape)
+            solution_errors(Zs[i], Xs[i], B0s[i], R, maxes[i], ctx=ctx)
+        _lib.check(ctx.lib.grim_synchronize(ctx.h), 'grim_synchronize')  # one wait (and error check) for all
+    return maxes.cpu().numpy(), side_out
+
+
+def _gate_modes(modes, Zs, Xs, B0s, precs, direct, tol, ctx=None, factors=None, measured=None):
     """The per-mode release gate over solved mode systems, in place on ``Xs``.
 
     ``Zs`` are the full FP64 mode matrices, ``B0s`` the right-hand sides and ``direct[i]``
@@ -161,20 +195,14 @@ def _gate_modes(modes, Zs, Xs, B0s, precs, direct, tol, ctx=None, factors=None):
     whose backward error still exceeds BOR_LINEAR_BACKWARD_ERROR_MAX raises RuntimeError.
     Returns per-mode dicts (backward_error, relative_residual, gate_refinement_steps,
     gate_lu_fallback); with ``factors`` (a list, one entry per mode) the LU of every mode
-    factored here replaces its entry."""
+    factored here replaces its entry.  ``measured``: the first measurements when the caller
+    took them (``_measure_modes``)."""
     from ..grouped import getrf_grouped
     ctx = ctx or context()
     count = len(modes)
     if not count:
         return []
-    size = max(int(B.numel()) for B in B0s)
-    scratch = torch.empty(size, dtype=torch.complex128, device='cuda')
-    maxes = torch.empty((count, 2), dtype=torch.float64, device='cuda')
-    for i in range(count):
-        R = scratch[:B0s[i].numel()].view(B0s[i].shape)
-        solution_errors(Zs[i], Xs[i], B0s[i], R, maxes[i], ctx=ctx)
-    _lib.check(ctx.lib.grim_synchronize(ctx.h), 'grim_synchronize')  # one wait (and error check) for all modes
-    vals = maxes.cpu().numpy()
+    vals = _measure_modes(Zs, Xs, B0s, ctx=ctx)[0] if measured is None else measured
     out = [{'backward_error': float(vals[i, 0]), 'relative_residual': float(vals[i, 1]), 'gate_refinement_steps': 0}
            for i in range(count)]
     bad = [i for i in range(count) if not gate_decision(vals[i, 0], vals[i, 1], release_limit(precs[i], tol))]
@@ -691,9 +719,14 @@ def _solve_modes_grouped(dev, modes, th, precision, tol, workers, monitor_cond=T
             Vs[i] = x
     torch.cuda.synchronize()
     t3 = time.perf_counter()
+    # the condition estimates (one launch, a CTA per mode) run beside the release measures
+    # of every mode on the worker pool; the condition gate is applied first, as the
+    # reference's factor construction does
+    side = (lambda c: condition_estimates(Zs, factors, ctx=c, read=False)) if monitor_cond else None
+    vals, cond_dev = _measure_modes(Zs, Vs, V0s, workers=workers, side=side)
     conds = None
     if monitor_cond:
-        conds = condition_estimates(Zs, factors)
+        conds = cond_dev.cpu().numpy()
         condition_gate(modes, conds)
     t4 = time.perf_counter()
     # the release gate against every full mode matrix: a solution from the FP64 LU of the
@@ -701,7 +734,8 @@ def _solve_modes_grouped(dev, modes, th, precision, tol, workers, monitor_cond=T
     fell_back = [bool(st.get('fp64_fallback')) for st in sts]
     eff = ['double' if fb and i not in mirrored else precs[i] for i, fb in enumerate(fell_back)]
     direct = [i not in mirrored and eff[i] == 'double' for i in range(len(modes))]
-    gate = _gate_modes(modes, Zs, Vs, V0s, eff, direct, tol, factors=factors if monitor_cond else None)
+    gate = _gate_modes(modes, Zs, Vs, V0s, eff, direct, tol, factors=factors if monitor_cond else None,
+                       measured=vals)
     redone = [i for i in range(len(modes)) if gate[i].get('gate_lu_fallback')]
     if monitor_cond and redone:
         again = condition_estimates([Zs[i] for i in redone], [factors[i] for i in redone])
@@ -709,7 +743,7 @@ def _solve_modes_grouped(dev, modes, th, precision, tol, workers, monitor_cond=T
         conds[redone] = again
     torch.cuda.synchronize()
     stage = {'assembly': t1 - t0, 'grouped_factor_and_solves': t2 - t1, 'fp64_fallbacks': t3 - t2,
-             'condition_estimates': t4 - t3, 'release_gate': time.perf_counter() - t4}
+             'condition_and_release_measures': t4 - t3, 'release_gate': time.perf_counter() - t4}
     ctx = context()
     nth = int(th.numel())
     outs = []
