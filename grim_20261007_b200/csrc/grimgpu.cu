@@ -360,32 +360,60 @@ static int gal_err_flag(grim_context *h, int **out) {
     return GRIM_OK;
 }
 
+static int lookahead_streams(grim_context *h, int nevents);
+
 template <typename C>
 static int gal_fill_impl(grim_context *h, int pol, int ne, int n, const double *elem, const int2 *nodes,
                          const int *start_of, const int *end_of, const int *row_off, const int *col, const int *route,
                          int nnz, const int *adapt_idx, int nadapt, double k, int far_min_order, C *Z, int64_t ldz) {
-    void *pnb = nullptr, *pe = nullptr;
+    void *pnb = nullptr, *pe = nullptr, *pst = nullptr;
     int *err = nullptr;
     GRIM_TRY(gal_err_flag(h, &err));
     GRIM_TRY(grim_workspace(h, "gal_nb", (size_t)nnz * 8 * sizeof(double2), &pnb));
     GRIM_TRY(grim_workspace(h, "gal_e", (size_t)ne * ne * 4 * sizeof(C), &pe));
+    if (nadapt > 0)
+        GRIM_TRY(grim_workspace(h, "gal_adapt_stack", (size_t)nadapt * GAL_ADAPT_GCAP * sizeof(GalBox), &pst));
     double2 *nbk = (double2 *)pnb;
     C *E = (C *)pe;
+    // The near pairs (k_gal_near, k_gal_adapt: NBK) and the far pairs (k_gal_far: E) write
+    // disjoint buffers, so the near work -- the adaptive close pairs are a few hundred
+    // long-running CTAs -- runs on the handle's high-priority stream beside the far tiles
+    // (not when profiling per launch); the near routing waits for both.
+    const bool split = !h->profiling;
+    const cudaStream_t caller = h->stream;
+    if (split) {
+        GRIM_TRY(lookahead_streams(h, 2));
+        GRIM_CHECK_CUDA(cudaEventRecord(h->events[0], caller));
+        GRIM_CHECK_CUDA(cudaStreamWaitEvent(h->chain, h->events[0], 0));
+        h->stream = h->chain;
+    }
+    int status = GRIM_OK;
     k_gal_near<<<ceil_div(nnz, GAL_NEAR_WARPS), GAL_NEAR_WARPS * 32, 0, h->stream>>>(ne, nnz, elem, nodes, row_off,
                                                                                      col, route, k, nbk, err);
-    GRIM_CHECK_LAUNCH(h, "k_gal_near");
-    if (nadapt > 0) {
+    status = grim_launch_status(h, "k_gal_near", 0, 0);
+    if (status == GRIM_OK && nadapt > 0) {
         static PerDeviceOnce attr;
         if (attr.needed()) {
-            GRIM_CHECK_CUDA(cudaFuncSetAttribute(k_gal_adapt, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 (int)GAL_ADAPT_SMEM));
-            attr.mark();
+            cudaError_t e = cudaFuncSetAttribute(k_gal_adapt, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)GAL_ADAPT_SMEM);
+            if (e != cudaSuccess) status = grim_cuda_check(e, "k_gal_adapt attribute");
+            else attr.mark();
         }
-        void *pst = nullptr;
-        GRIM_TRY(grim_workspace(h, "gal_adapt_stack", (size_t)nadapt * GAL_ADAPT_GCAP * sizeof(GalBox), &pst));
-        k_gal_adapt<<<nadapt, GAL_ADAPT_WARPS * 32, GAL_ADAPT_SMEM, h->stream>>>(ne, nadapt, adapt_idx, elem, row_off,
-                                                                                   col, k, (GalBox *)pst, nbk, err);
-        GRIM_CHECK_LAUNCH(h, "k_gal_adapt");
+        if (status == GRIM_OK) {
+            k_gal_adapt<<<nadapt, GAL_ADAPT_WARPS * 32, GAL_ADAPT_SMEM, h->stream>>>(ne, nadapt, adapt_idx, elem,
+                                                                                       row_off, col, k, (GalBox *)pst,
+                                                                                       nbk, err);
+            status = grim_launch_status(h, "k_gal_adapt", 0, 0);
+        }
+    }
+    if (split) {
+        // the caller's stream carries on with the far tiles, then waits for the near work
+        cudaEventRecord(h->events[1], h->chain);
+        h->stream = caller;
+    }
+    if (status != GRIM_OK) {
+        if (split) cudaStreamWaitEvent(caller, h->events[1], 0);
+        return status;
     }
     const int tiles = ceil_div(ne, GAL_TILE);
     dim3 fg(tiles, tiles);
@@ -393,7 +421,9 @@ static int gal_fill_impl(grim_context *h, int pol, int ne, int n, const double *
         k_gal_far<GRIM_POL_TM, C><<<fg, GAL_FAR_THREADS, 0, h->stream>>>(ne, elem, nodes, k, far_min_order, E);
     else
         k_gal_far<GRIM_POL_TE, C><<<fg, GAL_FAR_THREADS, 0, h->stream>>>(ne, elem, nodes, k, far_min_order, E);
-    GRIM_CHECK_LAUNCH(h, "k_gal_far");
+    status = grim_launch_status(h, "k_gal_far", 0, 0);
+    if (split) GRIM_CHECK_CUDA(cudaStreamWaitEvent(caller, h->events[1], 0));
+    GRIM_TRY(status);
     if (pol == GRIM_POL_TM)
         k_gal_near_route<GRIM_POL_TM, C><<<ceil_div(nnz, 128), 128, 0, h->stream>>>(ne, nnz, elem, row_off, col, nbk, k, E);
     else
