@@ -145,3 +145,49 @@ def test_condition_gate_messages():
     for bad in (float('nan'), float('inf'), 0.0):
         with pytest.raises(RuntimeError, match='m=4 condition estimation failed'):
             B.condition_gate([4], [bad])
+
+
+def test_finish_modes_decisions_without_a_device(monkeypatch):
+    """The per-mode path's gate bookkeeping (``_finish_modes``) on host stand-ins: the
+    condition gate is applied to every mode first, then exactly the modes whose measures
+    miss their release limits are solved again (``_redo_mode``), a mixed one marked as an
+    LU fallback."""
+    import torch
+
+    class Lib:
+        @staticmethod
+        def grim_synchronize(h):
+            return 0
+
+    class Ctx:
+        lib, h = Lib(), None
+
+    redone = []
+
+    def fake_redo(dev, m, th, tol, ctx, monitor_cond):
+        redone.append(m)
+        return torch.full((2,), float(m)), {'backward_error': 1e-15, 'relative_residual': 1e-14,
+                                            'gate_refinement_steps': 1, 'condition_est': 10.0}
+
+    monkeypatch.setattr(B, '_redo_mode', fake_redo)
+
+    def res(m, berr, rel, prec, cond):
+        return (torch.zeros(2), {'fp64_fallback': False},
+                {'precision': prec, 'maxes': torch.tensor([berr, rel], dtype=torch.float64),
+                 'cond': torch.tensor([cond], dtype=torch.float64)})
+
+    results = [res(0, 1e-15, 1e-12, 'double', 5.0),      # released
+               res(1, 2e-12, 1e-12, 'double', 5.0),      # backward error above 1e-12: redone
+               res(2, 5e-11, 1e-12, 'mixed', 5.0),       # mixed at its 1e-10 target: released
+               res(3, 1e-15, 3e-8, 'mixed', 5.0)]        # relative residual above 1e-8: redone
+    outs = B._finish_modes(None, [0, 1, 2, 3], None, results, 1e-10, Ctx(), True)
+    assert redone == [1, 3]
+    assert [float(p[0]) for p, _t in outs] == [0.0, 1.0, 0.0, 3.0]
+    assert 'gate_lu_fallback' in outs[3][1] and 'gate_lu_fallback' not in outs[1][1]
+    assert outs[0][1]['backward_error'] == 1e-15 and outs[0][1]['condition_est'] == 5.0
+    # the condition gate comes first: a mode over the limit raises before any re-solve
+    redone.clear()
+    bad = [res(0, 2e-12, 1e-12, 'double', 5.0), res(1, 1e-15, 1e-12, 'double', 2e12)]
+    with pytest.raises(RuntimeError, match='m=1 estimated 1-norm condition'):
+        B._finish_modes(None, [0, 1], None, bad, 1e-10, Ctx(), True)
+    assert redone == []
